@@ -1,0 +1,404 @@
+"""Benchmark of the B200 rigid-body step (sphere-steps/s).
+
+Default workload: the large DEM scene -- 1,048,576 spheres, log-normal radii (median 0.5,
+sigma_log 0.2, clipped to [0.3, 0.9]) in a random packing at 30% solid fraction at the bottom of a
+200x200x400 box of planes, linear spring-dashpot k_n=1e5, c_n=50, mu=0.4, dt=5e-5 -- advanced by
+the mixed-precision path (FP64 positions, FP32 velocities/forces).  Beside it, on the same scene,
+the plain all-FP64 GPU path, the 32,768-sphere hard-contact (NBGS) scene, and the compiled pe
+reference on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dem_large_1m|dem_lattice_4096|nbgs_box_32768|ensemble_512]
+
+Under torchrun each rank advances its own replica of the scene (one scene does not shard
+without spatial decomposition; the batched ensemble shards by scene): weak scaling, whole-job
+throughput = spheres x steps x ranks / max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from pe_b200 import scenes  # noqa: E402
+
+METRIC = "sphere-steps/s (1M DEM, 32k NBGS) mixed+batched vs plain FP64 GPU at stated err"
+UNIT = "sphere-steps/s"
+# algorithmic bytes per sphere-step of the DEM step (positions, velocities, radius/mass, grid
+# key+id read and written once): FP64 176 B, mixed 120 B
+ALGO_BYTES = {"fp64": 176.0, "mixed": 120.0}
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dem_large_1m",
+                    choices=["dem_large_1m", "dem_lattice_4096", "nbgs_box_32768", "ensemble_512"])
+    ap.add_argument("--no-extras", action="store_true", help="headline measurement only")
+    return ap.parse_args()
+
+
+def build_workload(name, seed=0):
+    if name == "dem_large_1m":
+        return [scenes.dem_large(seed)], "dem"
+    if name == "dem_lattice_4096":
+        return [scenes.dem_lattice(seed)], "dem"
+    if name == "nbgs_box_32768":
+        return [scenes.nbgs_box(seed)], "hcsits"
+    if name == "ensemble_512":
+        return scenes.batched_ensemble(seed), "dem"
+    raise ValueError(name)
+
+
+# ------------------------------------------------------------------------------------------
+# reference (pe compiled from its own sources, oracle/_ref) on the host cores
+# ------------------------------------------------------------------------------------------
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def ref_sample_scene(workload):
+    """Bounded sample of the workload for the single-threaded reference: the same packing,
+    radii, materials and time step, on a smaller footprint (pe's body setup grows faster than
+    linearly with the body count)."""
+    if workload == "dem_large_1m":
+        n = 262144
+        side = 200.0 * (n / 1048576) ** 0.5
+        return scenes.dem_large(0, n=n, dims=(side, side, 400.0)), "ref_dem", \
+            f"{n} spheres of the 1M DEM scene's packing on a {side:.0f}x{side:.0f} footprint"
+    if workload == "dem_lattice_4096":
+        return scenes.dem_lattice(0), "ref_dem", "the full 4096-sphere lattice scene"
+    if workload == "nbgs_box_32768":
+        return scenes.nbgs_box(0), "ref_hcsits", "the full 32768-sphere NBGS scene"
+    if workload == "ensemble_512":
+        ss = scenes.batched_ensemble(0)
+        k = int(np.argsort([s.n for s in ss])[len(ss) // 2])
+        return ss[k], "ref_dem", f"one median-size scene ({ss[k].n} spheres) of the ensemble"
+    raise ValueError(workload)
+
+
+def run_reference(workload, steps, warmup=1, budget_s=60.0):
+    exe_scene, exe, sample = ref_sample_scene(workload)
+    path = os.path.join(REF_DIR, exe)
+    if not os.path.exists(path):
+        return None, f"compiled reference missing ({path}); build with make -C oracle/ref"
+    with tempfile.TemporaryDirectory() as tmp:
+        sp = os.path.join(tmp, "scene.bin")
+        exe_scene.save(sp)
+        extra = ["0", "100"] if exe == "ref_hcsits" else []
+        # probe one step to size the timed sample within the budget
+        t0 = time.perf_counter()
+        r = subprocess.run([path, "time", sp, "0", "1", *extra], capture_output=True, text=True)
+        if r.returncode != 0:
+            return None, "reference run failed: " + r.stderr.strip()[-200:]
+        one = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
+        k = max(1, min(steps, int(budget_s / max(one, 1e-6))))
+        r = subprocess.run([path, "time", sp, str(warmup), str(k), *extra], capture_output=True,
+                           text=True)
+        if r.returncode != 0:
+            return None, "reference run failed: " + r.stderr.strip()[-200:]
+        res = json.loads(r.stdout.strip().splitlines()[-1])
+        res["wall_s"] = time.perf_counter() - t0
+        res["sample"] = f"{sample}; {k} timed steps after {warmup} warm-up"
+        res["cores"] = 1
+        return res, None
+
+
+# ------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                   "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+def make_engine(ss, kind, precision, iters=100):
+    from pe_b200 import _abi
+    from pe_b200.engine import Engine
+    solver = _abi.DEM if kind == "dem" else _abi.HCSITS
+    model = _abi.INELASTIC_FRICTIONLESS
+    if kind == "hcsits" and float(ss[0].materials[0, 2]) > 0:
+        model = _abi.APPROX_INELASTIC_COULOMB_DECOUPLING
+    e = Engine(solver=solver, precision=precision, relaxation_model=model, max_iterations=iters)
+    if len(ss) == 1:
+        e.load_scene(ss[0])
+    else:
+        e.load_scenes(ss)
+    return e
+
+
+def timed_steps(e, dt, steps, warmup, torch, flush_buf, stream, dist=None):
+    """Per-step CUDA events on the library's stream; the L2 flush between steps is untimed."""
+    for _ in range(warmup):
+        e.step(dt)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e.set_profiling(True)
+    launches0 = e.kernel_launches()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush_buf.add_(1)          # writes 256 MiB: evicts the previous step's data from L2
+            evs[k][0].record(stream)
+            e.step(dt)
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    launches = e.kernel_launches() - launches0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    prof = e.profile()
+    e.set_profiling(False)
+    return ms, launches, prof
+
+
+def our_arm(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+    from pe_b200 import _abi
+    from pe_b200.engine import Engine
+
+    ss, kind = build_workload(args.workload)
+    nsph = sum(s.n for s in ss)
+    dt = ss[0].dt
+    dev = torch.device("cuda", local)
+    flush = torch.zeros(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    precision = _abi.MIXED
+    e = make_engine(ss, kind, precision)
+    stream = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        uuid = None
+    clocks = Clocks(uuid)
+    clocks.start()
+    ms, launches, prof = timed_steps(e, dt, args.steps, args.warmup, torch, flush, stream, dist)
+    clk = clocks.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = nsph * args.steps * world / (ms_max / 1e3)
+
+    # end to end through the public API: host arrays in, K steps, host arrays out
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    host = [(np.ascontiguousarray(s.x), np.ascontiguousarray(s.v), np.ascontiguousarray(s.w))
+            for s in ss]
+    t0 = time.perf_counter()
+    e2 = make_engine(ss, kind, precision)
+    e2.step(dt, args.steps)
+    out = e2.download()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(s.x.nbytes + s.v.nbytes + s.w.nbytes + s.r.nbytes + s.mat.nbytes for s in ss)
+    d2h = sum(a.nbytes for a in out if a is not None)
+    e2.close()
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_value = nsph * args.steps * world / float(te.item())
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        e.close()
+        return None
+
+    # dominant kernel roofline (the fused DEM step kernel or the NBGS sweeps)
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    if kind == "dem":
+        kms, kcnt = prof.get("dem_step", (0.0, 0))
+        per = ALGO_BYTES["mixed"]
+        algo = per * nsph
+        kname = "k_dem_step<float>"
+    else:
+        kms, kcnt = prof.get("sweeps", (0.0, 0))
+        st = e.stats()
+        algo = 100 * (128.0 * st["contacts"] + 80.0 * nsph)
+        kname = "k_sweep<float> (100 sweeps)"
+    kavg = kms / max(kcnt, 1)
+    achieved = algo / (kavg / 1e3) / 1e9 if kavg > 0 else None
+    traffic = read_traffic(args.workload)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": kavg}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (f64 positions)", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "spheres": nsph, "scenes": len(ss),
+                       "precision": "mixed", "dt": dt,
+                       "l2": "flushed between timed steps (256 MiB write, untimed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "clocks": clk, "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": d2h / args.steps,
+                    "note": "upload + steps + download through the C ABI, wall clock"},
+            "roofline": roofline,
+            "stages_ms_per_step": {k: v[0] / args.steps for k, v in prof.items() if v[1]}}
+    e.close()
+    if not args.no_extras:
+        line.update(extras(args, torch, flush, dev, ss, kind, value))
+    return line
+
+
+def extras(args, torch, flush, dev, ss, kind, mixed_value):
+    """FP64 path on the same scene, the NBGS scene, and the compiled reference."""
+    from pe_b200 import _abi
+    out = {}
+    nsph = sum(s.n for s in ss)
+    dt = ss[0].dt
+    k64 = max(10, args.steps // 2)
+    e = make_engine(ss, kind, _abi.FP64)
+    stream = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+    ms, _, prof = timed_steps(e, dt, k64, 3, torch, flush, stream)
+    v64 = nsph * k64 / (ms / 1e3)
+    out["fp64"] = {"value": v64, "ms_per_step": ms / k64,
+                   "mixed_over_fp64": mixed_value / v64,
+                   "stages_ms_per_step": {k: v[0] / k64 for k, v in prof.items() if v[1]}}
+    e.close()
+    if kind == "dem" and args.workload != "nbgs_box_32768":
+        s = scenes.nbgs_box(0)
+        for prec, name in ((_abi.MIXED, "mixed"), (_abi.FP64, "fp64")):
+            e = make_engine([s], "hcsits", prec)
+            st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+            ksteps = 20
+            ms, _, prof = timed_steps(e, s.dt, ksteps, 3, torch, flush, st)
+            stt = e.stats()
+            out.setdefault("nbgs_32k", {})[name] = {
+                "value": s.n * ksteps / (ms / 1e3), "ms_per_step": ms / ksteps,
+                "contacts": stt["contacts"], "colors": stt["colors"],
+                "stages_ms_per_step": {k: v[0] / ksteps for k, v in prof.items() if v[1]}}
+            e.close()
+    ref, why = run_reference(args.workload, steps=10, budget_s=20.0)
+    if ref:
+        out["cpu_baseline"] = {"value": ref["sphere_steps_per_s"], "unit": UNIT,
+                               "cores": ref["cores"], "kind": "reference",
+                               "sample": ref["sample"]}
+    else:
+        out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                               "sample": why}
+    return out
+
+
+def read_traffic(workload):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{workload}_launch_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    ref, why = run_reference(args.workload, steps=max(1, args.steps), warmup=max(1, min(args.warmup, 3)),
+                             budget_s=90.0)
+    if not ref:
+        return {"impl": "reference", "unavailable": why}
+    v = ref["sphere_steps_per_s"]
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": ref["steps"],
+            "warmup": args.warmup, "ms_per_step": 1e3 * ref["seconds"] / ref["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "precision": "fp64 (pe compiled -O3 -DNDEBUG)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ref["cores"], "kind": "reference",
+                             "sample": ref["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    line = reference_arm(args) if args.impl == "reference" else our_arm(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

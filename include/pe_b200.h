@@ -1,0 +1,173 @@
+/*
+ * pe_b200.h -- C ABI of the B200 rigid-body time step (libpe_b200.so).
+ *
+ * The library owns device memory and one CUDA stream per context.  Host arrays passed in are
+ * copied; the caller keeps ownership.  Every entry point returns a pe_b200_status; no C++
+ * exception crosses this boundary.  A context is used by one host thread at a time.
+ *
+ * Each entry point replaces a piece of pe's compile-time plugin boundary (the
+ * CollisionSystem<Config> specialisation selected by pe_CONSTRAINT_SOLVER,
+ * pe/config/Collisions.h:90, pe/core/Configuration.h:84) and of the body/world API that feeds
+ * it; the reference interface is cited beside each declaration (paths relative to pe's root).
+ *
+ * Body order: spheres are identified by their index in the arrays given to
+ * pe_b200_upload_bodies (pe's creation order, hence pe's system-id order).  Walls (planes, then
+ * boxes) follow the spheres in the id space used for contacts: id n + k for wall k.
+ */
+#ifndef PE_B200_H
+#define PE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PE_B200_OK = 0,
+    PE_B200_ERR_ARG = 1,       /* invalid argument (pe: std::invalid_argument) */
+    PE_B200_ERR_CAPACITY = 2,  /* a buffer capacity was exceeded */
+    PE_B200_ERR_NAN = 3,       /* non-finite state detected */
+    PE_B200_ERR_TIMEOUT = 4,   /* a bounded device wait gave up */
+    PE_B200_ERR_CUDA = 5,      /* CUDA runtime error */
+    PE_B200_ERR_STATE = 6,     /* call out of order (e.g. step before upload) */
+    PE_B200_ERR_NOMEM = 7,     /* device or host allocation failed */
+    PE_B200_ERR_UNSUPPORTED = 8 /* model not supported (pe: std::runtime_error,
+                                   HardContactSemiImplicitTimesteppingSolvers.h:1926) */
+} pe_b200_status;
+
+typedef enum {
+    PE_B200_DEM = 0,    /* pe::response::DEMSolver (pe/core/collisionsystem/DEMSolver.h) */
+    PE_B200_HCSITS = 1  /* pe::response::HardContactSemiImplicitTimesteppingSolvers */
+} pe_b200_solver;
+
+typedef enum {
+    PE_B200_FP64 = 0,   /* everything in FP64, as pe's default real (pe/config/Precision.h) */
+    PE_B200_MIXED = 1   /* FP64 positions; FP32 velocities, detection, forces and NBGS updates */
+} pe_b200_precision;
+
+typedef enum {
+    /* HardContactSemiImplicitTimesteppingSolvers.h:172-179 (the first two models) */
+    PE_B200_INELASTIC_FRICTIONLESS = 0,
+    PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING = 1
+} pe_b200_relaxation_model;
+
+typedef struct {
+    int32_t solver;            /* pe_b200_solver */
+    int32_t precision;         /* pe_b200_precision */
+    int32_t relaxation_model;  /* pe_b200_relaxation_model (HCSITS only) */
+    int32_t max_iterations;    /* HCSITS sweeps per step; pe default 100 (HCSITS.h:421) */
+    double erp;                /* HCSITS error reduction; pe default 0.7 (HCSITS.h:420) */
+    double gravity[3];         /* World::setGravity (pe/core/World.h:754); default 0 */
+    double damping;            /* World::setDamping, 1 = no drag (src/core/Settings.cpp:47) */
+    int32_t device;            /* CUDA device ordinal */
+    int32_t track_orientation; /* 1: integrate sphere quaternions (Default.h:190-193) */
+    int64_t max_contacts;      /* HCSITS contact capacity; 0 = automatic (8 per sphere) */
+} pe_b200_params;
+
+/* createMaterial argument list, src/core/Materials.cpp:175 */
+typedef struct {
+    double density, cor, csf, cdf, poisson, young, stiffness, dampingN, dampingT;
+} pe_b200_material;
+
+typedef struct pe_b200_ctx pe_b200_ctx;
+
+/* Fills *p with pe's defaults (zero gravity, no drag, DEM, FP64, 100 sweeps, erp 0.7).
+ * Replaces: the compile-time defaults of the collision system constructors
+ * (pe/core/collisionsystem/DEMSolver.h:340ff, HCSITS.h:408-426) and Settings (Settings.cpp:46-48). */
+void pe_b200_default_params(pe_b200_params *p);
+
+/* Creates a context (device buffers are allocated on upload).
+ * Replaces: CollisionSystem<Config>::CollisionSystem() / theCollisionSystem()
+ * (pe/core/CollisionSystem.h, DEMSolver.h:340, HCSITS.h:408). */
+int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out);
+
+/* Releases the context and all its device memory.
+ * Replaces: CollisionSystem<Config>::~CollisionSystem (DEMSolver.h:441). */
+int pe_b200_destroy(pe_b200_ctx *ctx);
+
+/* Human-readable text of the last error on this context ("" if none). */
+const char *pe_b200_last_error(const pe_b200_ctx *ctx);
+
+/* Updates gravity and drag.  Replaces: World::setGravity / World::setDamping
+ * (pe/core/World.h:736-767). */
+int pe_b200_set_gravity(pe_b200_ctx *ctx, const double g[3]);
+int pe_b200_set_damping(pe_b200_ctx *ctx, double damping);
+
+/* HCSITS runtime setters.  Replace: setMaxIterations / setRelaxationModel /
+ * setErrorReductionParameter (HardContactSemiImplicitTimesteppingSolvers.h:793, 814, 835). */
+int pe_b200_set_max_iterations(pe_b200_ctx *ctx, int32_t n);
+int pe_b200_set_relaxation_model(pe_b200_ctx *ctx, int32_t model);
+int pe_b200_set_error_reduction(pe_b200_ctx *ctx, double erp);
+
+/* Material table (validated like createMaterial, src/core/Materials.cpp:180-207).
+ * Replaces: createMaterial / Material::get*(m1, m2) composition (pe/core/Materials.h:468-715). */
+int pe_b200_set_materials(pe_b200_ctx *ctx, int32_t n, const pe_b200_material *m);
+
+/* Fixed walls of scene `scene`: planes (4 doubles each: unit normal, displacement d with
+ * n.x = d on the plane) and boxes (15 doubles each: centre, side lengths, row-major rotation).
+ * Replaces: createPlane (src/core/rigidbody/Plane.cpp:1202) and createBox + setFixed
+ * (src/core/rigidbody/Box.cpp:1312). */
+int pe_b200_set_walls(pe_b200_ctx *ctx, int32_t scene, int32_t nplanes, const double *planes,
+                      const int32_t *plane_mat, int32_t nboxes, const double *boxes,
+                      const int32_t *box_mat);
+
+/* Uploads the spheres of every scene at once: n spheres, interleaved xyz vectors, radii,
+ * material ids and scene ids (scene may be NULL: all in scene 0).  nscenes scenes.
+ * Replaces: createSphere (src/core/rigidbody/Sphere.cpp:1187) + setLinearVel/setAngularVel,
+ * World::add -> CollisionSystem::add (src/core/World.cpp:262-277, DEMSolver.h:988-1008). */
+int pe_b200_upload_bodies(pe_b200_ctx *ctx, int64_t n, const double *x, const double *v,
+                          const double *w, const double *r, const int32_t *mat,
+                          const int32_t *scene, int32_t nscenes);
+
+/* Overwrites positions/velocities of the uploaded spheres (same order; any pointer may be NULL
+ * to keep that field).  Replaces: RigidBody::setPosition / setLinearVel / setAngularVel. */
+int pe_b200_set_state(pe_b200_ctx *ctx, const double *x, const double *v, const double *w);
+
+/* Advances every scene by nsteps steps of size dt.
+ * Replaces: World::simulationStep (src/core/World.cpp:330-357) ->
+ * CollisionSystem::simulationStep (DEMSolver.h:1155-1262, HCSITS.h:1472-1520).
+ * dt <= 0 is rejected with PE_B200_ERR_ARG as World.cpp:333-334 throws. */
+int pe_b200_step(pe_b200_ctx *ctx, int32_t nsteps, double dt);
+
+/* Downloads sphere state in upload order (any pointer may be NULL).
+ * Replaces: RigidBody::getPosition / getLinearVel / getAngularVel / getQuaternion. */
+int pe_b200_download_bodies(pe_b200_ctx *ctx, double *x, double *v, double *w, double *q);
+
+/* Contacts of the current state (detection only, no response), sorted by (b1, b2):
+ * ids (2 per contact, wall k has id n + k of its scene's wall list), and 7 doubles per contact
+ * (contact point xyz, normal xyz from body 2 to body 1, signed distance).  *n_out receives the
+ * total count; at most cap records are written (ids/geom may be NULL when cap is 0).
+ * Replaces: HashGrids::findContacts + MaxContacts::collide
+ * (pe/core/detection/coarse/HashGrids.h:1121, pe/core/detection/fine/MaxContacts.h:242). */
+int pe_b200_find_contacts(pe_b200_ctx *ctx, int64_t cap, int64_t *ids, double *geom,
+                          int64_t *n_out);
+
+/* Statistics of the last step: number of contacts, number of colours (HCSITS), the L-inf
+ * impulse change of the last sweep (pe's delta_max, HCSITS.h:1893-1946) and the complementarity
+ * residual of the final impulses in velocity units (computed in FP64 when requested by
+ * pe_b200_set_residual(ctx, 1); otherwise -1). */
+int pe_b200_last_step_stats(pe_b200_ctx *ctx, int64_t *ncontacts, int32_t *ncolors,
+                            double *delta_max, double *residual);
+int pe_b200_set_residual(pe_b200_ctx *ctx, int32_t enabled);
+
+/* Stage timers (CUDA events on the context's stream around each stage; off by default).
+ * Replaces: pe's profiling sections and logProfilingSummary (pe/config/ProfilingMode.h:40,
+ * pe/core/collisionsystem/DEMSolver.h:698-960).  Enabling resets the totals. */
+int pe_b200_set_profiling(pe_b200_ctx *ctx, int32_t enabled);
+/* Per stage: name, total milliseconds and number of timed launches since profiling was
+ * enabled; *n_out receives the number of stages (at most cap are written). */
+int pe_b200_profile(pe_b200_ctx *ctx, int32_t cap, const char **names, double *total_ms,
+                    int64_t *count, int32_t *n_out);
+
+/* Number of kernels this context launched since creation (device-side work accounting). */
+int64_t pe_b200_kernel_launches(const pe_b200_ctx *ctx);
+
+/* The CUDA stream (cudaStream_t) this context launches on, for event timing by the caller. */
+void *pe_b200_stream(pe_b200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PE_B200_H */

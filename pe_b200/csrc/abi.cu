@@ -1,0 +1,689 @@
+// abi.cu -- the extern "C" entry points of libpe_b200.so (declared in include/pe_b200.h).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+
+#include "internal.cuh"
+
+namespace peb {
+
+int set_err(Ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_err(Ctx *c, cudaError_t e, const char *where) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "CUDA error %d (%s) at %s", (int)e, cudaGetErrorString(e), where);
+    return set_err(c, PE_B200_ERR_CUDA, buf);
+}
+
+const char *kStageNames[ST_COUNT] = {"sort", "dem_step", "permute", "detect", "color",
+                                     "contact_cache", "sweeps", "integrate"};
+
+static cudaEvent_t take_event(Ctx *c) {
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+void prof_begin(Ctx *c, int stage) {
+    if (!c->prof) return;
+    cudaEvent_t e = take_event(c);
+    if (!e) return;
+    cudaEventRecord(e, c->stream);
+    c->ev_pending[stage] = e;
+}
+
+void prof_end(Ctx *c, int stage) {
+    if (!c->prof || !c->ev_pending[stage]) return;
+    cudaEvent_t e = take_event(c);
+    if (!e) return;
+    cudaEventRecord(e, c->stream);
+    c->ev_open[stage].push_back({c->ev_pending[stage], e});
+    c->ev_pending[stage] = nullptr;
+}
+
+static void prof_collect(Ctx *c) {
+    cudaStreamSynchronize(c->stream);
+    for (int s = 0; s < ST_COUNT; ++s) {
+        for (auto &pr : c->ev_open[s]) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+                c->prof_ms[s] += ms;
+                c->prof_count[s] += 1;
+            }
+            c->ev_pool.push_back(pr.first);
+            c->ev_pool.push_back(pr.second);
+        }
+        c->ev_open[s].clear();
+    }
+}
+
+namespace {
+
+void free_bodies(BodyBuf &b) {
+    cudaFree(b.pr);
+    cudaFree(b.vw);
+    cudaFree(b.tag);
+    cudaFree(b.uid);
+    cudaFree(b.q);
+    b = BodyBuf();
+}
+
+void free_device(Ctx *c) {
+    free_bodies(c->cur);
+    free_bodies(c->nxt);
+    cudaFree(c->key);
+    cudaFree(c->rank);
+    cudaFree(c->sorted);
+    cudaFree(c->cell_count);
+    cudaFree(c->cell_start);
+    cudaFree(c->scan_tmp);
+    cudaFree(c->d_scenes);
+    cudaFree(c->d_mats);
+    cudaFree(c->d_planes);
+    cudaFree(c->d_plane_mat);
+    cudaFree(c->d_boxes);
+    cudaFree(c->d_box_mat);
+    c->key = c->rank = c->sorted = c->cell_count = c->cell_start = c->scan_tmp = nullptr;
+    c->scan_tmp_cap = 0;
+    c->d_scenes = nullptr;
+    c->d_mats = nullptr;
+    c->d_planes = nullptr;
+    c->d_plane_mat = nullptr;
+    c->d_boxes = nullptr;
+    c->d_box_mat = nullptr;
+    nbgs_free(c);
+    c->uploaded = false;
+    c->binned = false;
+}
+
+int alloc_bodies(Ctx *c, BodyBuf &b) {
+    const size_t n = (size_t)std::max<int64_t>(c->n, 1);
+    PEB_CUDA(c, cudaMalloc(&b.pr, n * sizeof(double4)));
+    PEB_CUDA(c, cudaMalloc(&b.vw, n * (size_t)c->vw_bytes));
+    PEB_CUDA(c, cudaMalloc(&b.tag, n * sizeof(uint32_t)));
+    PEB_CUDA(c, cudaMalloc(&b.uid, n * sizeof(int32_t)));
+    if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&b.q, n * sizeof(double4)));
+    return PE_B200_OK;
+}
+
+int check_material(const pe_b200_material &m, std::string &why) {
+    // createMaterial argument checks, src/core/Materials.cpp:189-207
+    if (!(m.density > 0)) { why = "Invalid material density!"; return 1; }
+    if (m.cor < 0 || m.cor > 1) { why = "Invalid coefficient of restitution!"; return 1; }
+    if (m.csf < 0) { why = "Invalid coefficient of static friction!"; return 1; }
+    if (m.cdf < 0) { why = "Invalid coefficient of dynamic friction!"; return 1; }
+    if (m.poisson < -1 || m.poisson > 0.5) { why = "Invalid Poisson's ratio"; return 1; }
+    if (!(m.young > 0)) { why = "Invalid Young's modulus"; return 1; }
+    if (!(m.stiffness > 0)) { why = "Invalid stiffness"; return 1; }
+    if (m.dampingN < 0 || m.dampingT < 0) { why = "Invalid damping coefficients"; return 1; }
+    return 0;
+}
+
+int upload_tables(Ctx *c) {
+    // materials
+    std::vector<MatDev> md(c->mats.size());
+    for (size_t k = 0; k < c->mats.size(); ++k) {
+        const pe_b200_material &m = c->mats[k];
+        md[k].density = m.density;
+        md[k].rk = 1.0 / m.stiffness;
+        md[k].rcn = 1.0 / m.dampingN;
+        md[k].rct = 1.0 / m.dampingT;
+        md[k].csf = m.csf;
+        md[k].cdf = m.cdf;
+    }
+    cudaFree(c->d_mats);
+    c->d_mats = nullptr;
+    PEB_CUDA(c, cudaMalloc(&c->d_mats, std::max<size_t>(md.size(), 1) * sizeof(MatDev)));
+    if (!md.empty())
+        PEB_CUDA(c, cudaMemcpy(c->d_mats, md.data(), md.size() * sizeof(MatDev),
+                               cudaMemcpyHostToDevice));
+    // walls, concatenated per scene
+    c->planes.clear();
+    c->plane_mat.clear();
+    c->boxes.clear();
+    c->box_mat.clear();
+    for (int s = 0; s < c->nscenes; ++s) {
+        SceneInfo &si = c->scenes[s];
+        si.plane_begin = (int32_t)(c->planes.size() / 4);
+        si.nplanes = (int32_t)(c->scene_planes[s].size() / 4);
+        si.box_begin = (int32_t)(c->boxes.size() / 15);
+        si.nboxes = (int32_t)(c->scene_boxes[s].size() / 15);
+        c->planes.insert(c->planes.end(), c->scene_planes[s].begin(), c->scene_planes[s].end());
+        c->plane_mat.insert(c->plane_mat.end(), c->scene_plane_mat[s].begin(),
+                            c->scene_plane_mat[s].end());
+        c->boxes.insert(c->boxes.end(), c->scene_boxes[s].begin(), c->scene_boxes[s].end());
+        c->box_mat.insert(c->box_mat.end(), c->scene_box_mat[s].begin(),
+                          c->scene_box_mat[s].end());
+    }
+    cudaFree(c->d_planes);
+    cudaFree(c->d_plane_mat);
+    cudaFree(c->d_boxes);
+    cudaFree(c->d_box_mat);
+    c->d_planes = nullptr;
+    c->d_plane_mat = nullptr;
+    c->d_boxes = nullptr;
+    c->d_box_mat = nullptr;
+    const size_t np = c->planes.size() / 4, nb = c->boxes.size() / 15;
+    PEB_CUDA(c, cudaMalloc(&c->d_planes, std::max<size_t>(np, 1) * sizeof(double4)));
+    PEB_CUDA(c, cudaMalloc(&c->d_plane_mat, std::max<size_t>(np, 1) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&c->d_boxes, std::max<size_t>(nb, 1) * 15 * sizeof(double)));
+    PEB_CUDA(c, cudaMalloc(&c->d_box_mat, std::max<size_t>(nb, 1) * sizeof(int32_t)));
+    if (np) {
+        PEB_CUDA(c, cudaMemcpy(c->d_planes, c->planes.data(), np * sizeof(double4),
+                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpy(c->d_plane_mat, c->plane_mat.data(), np * sizeof(int32_t),
+                               cudaMemcpyHostToDevice));
+    }
+    if (nb) {
+        PEB_CUDA(c, cudaMemcpy(c->d_boxes, c->boxes.data(), nb * 15 * sizeof(double),
+                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpy(c->d_box_mat, c->box_mat.data(), nb * sizeof(int32_t),
+                               cudaMemcpyHostToDevice));
+    }
+    cudaFree(c->d_scenes);
+    c->d_scenes = nullptr;
+    PEB_CUDA(c, cudaMalloc(&c->d_scenes, std::max<size_t>(c->scenes.size(), 1) * sizeof(SceneInfo)));
+    if (!c->scenes.empty())
+        PEB_CUDA(c, cudaMemcpy(c->d_scenes, c->scenes.data(), c->scenes.size() * sizeof(SceneInfo),
+                               cudaMemcpyHostToDevice));
+    return PE_B200_OK;
+}
+
+// grid geometry of each scene: bounding box of its spheres, extended to axis-aligned planes
+// that close the scene, with cells of the largest AABB extent (grown if the grid would be much
+// larger than the body count; bodies that leave the grid are clamped into the border cells,
+// which keeps the search exact and only costs speed)
+void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int64_t> &order,
+                const std::vector<int64_t> &begin, const std::vector<int64_t> &count) {
+    int64_t base = 0;
+    for (int s = 0; s < c->nscenes; ++s) {
+        SceneInfo &si = c->scenes[s];
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        double rmax = 0.0;
+        for (int64_t k = begin[s]; k < begin[s] + count[s]; ++k) {
+            const int64_t i = order[k];
+            rmax = std::max(rmax, r[i]);
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = std::min(lo[a], x[3 * i + a] - r[i]);
+                hi[a] = std::max(hi[a], x[3 * i + a] + r[i]);
+            }
+        }
+        if (count[s] == 0) {
+            for (int a = 0; a < 3; ++a) { lo[a] = 0; hi[a] = 1; }
+            rmax = 0.5;
+        }
+        const std::vector<double> &pl = c->scene_planes[s];
+        for (size_t p = 0; p + 3 < pl.size(); p += 4) {
+            for (int a = 0; a < 3; ++a) {
+                const double na = pl[p + a];
+                const bool axis = fabs(fabs(na) - 1.0) < 1e-12;
+                if (!axis) continue;
+                // n.x >= d: lower bound along +axis, or upper bound along -axis
+                if (na > 0) lo[a] = std::min(lo[a], pl[p + 3]);
+                else hi[a] = std::max(hi[a], -pl[p + 3]);
+                // only extend towards the plane, never shrink below the bodies' extent
+            }
+        }
+        double h = 2.0 * (rmax + kContactThreshold) * (1.0 + 1e-9);
+        int64_t dim[3], nc;
+        const int64_t cap = 8 * std::max<int64_t>(count[s], 1) + 4096;
+        for (;;) {
+            nc = 1;
+            for (int a = 0; a < 3; ++a) {
+                dim[a] = (int64_t)floor((hi[a] - lo[a]) / h) + 1;
+                nc *= dim[a];
+            }
+            if (nc <= cap) break;
+            h *= 1.26;
+        }
+        for (int a = 0; a < 3; ++a) {
+            si.lo[a] = lo[a];
+            si.dim[a] = (int32_t)dim[a];
+        }
+        si.h = h;
+        si.inv_h = 1.0 / h;
+        si.cell_base = base;
+        si.body_begin = begin[s];
+        si.nbodies = count[s];
+        base += nc;
+    }
+    c->ncell = base;
+}
+
+}  // namespace
+
+}  // namespace peb
+
+using namespace peb;
+
+extern "C" {
+
+void pe_b200_default_params(pe_b200_params *p) {
+    if (!p) return;
+    memset(p, 0, sizeof *p);
+    p->solver = PE_B200_DEM;
+    p->precision = PE_B200_FP64;
+    p->relaxation_model = PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING;
+    p->max_iterations = 100;
+    p->erp = 0.7;
+    p->damping = 1.0;
+    p->device = 0;
+    p->track_orientation = 0;
+    p->max_contacts = 0;
+}
+
+int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
+    if (!p || !out) return PE_B200_ERR_ARG;
+    *out = nullptr;
+    if (p->solver != PE_B200_DEM && p->solver != PE_B200_HCSITS) return PE_B200_ERR_ARG;
+    if (p->precision != PE_B200_FP64 && p->precision != PE_B200_MIXED) return PE_B200_ERR_ARG;
+    if (p->relaxation_model != PE_B200_INELASTIC_FRICTIONLESS &&
+        p->relaxation_model != PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING)
+        return PE_B200_ERR_UNSUPPORTED;
+    if (p->max_iterations < 0 || p->damping < 0 || p->damping > 1) return PE_B200_ERR_ARG;
+    Ctx *c = new (std::nothrow) Ctx();
+    if (!c) return PE_B200_ERR_NOMEM;
+    c->p = *p;
+    c->device = p->device;
+    c->vw_bytes = 6 * (p->precision == PE_B200_FP64 ? 8 : 4);
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_err, sizeof(int32_t));
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, p->device);
+    if (e != cudaSuccess) {
+        int rc = cuda_err(c, e, "pe_b200_create");
+        if (c->stream) cudaStreamDestroy(c->stream);
+        cudaFree(c->d_err);
+        if (c->h_err) cudaFreeHost(c->h_err);
+        delete c;
+        return rc;
+    }
+    *out = reinterpret_cast<pe_b200_ctx *>(c);
+    return PE_B200_OK;
+}
+
+int pe_b200_destroy(pe_b200_ctx *h) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    prof_collect(c);
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    c->ev_pool.clear();
+    free_device(c);
+    cudaFree(c->d_err);
+    if (c->h_err) cudaFreeHost(c->h_err);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PE_B200_OK;
+}
+
+const char *pe_b200_last_error(const pe_b200_ctx *h) {
+    const Ctx *c = reinterpret_cast<const Ctx *>(h);
+    return c ? c->err.c_str() : "null context";
+}
+
+int pe_b200_set_gravity(pe_b200_ctx *h, const double g[3]) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !g) return PE_B200_ERR_ARG;
+    for (int a = 0; a < 3; ++a) c->p.gravity[a] = g[a];
+    return PE_B200_OK;
+}
+
+int pe_b200_set_damping(pe_b200_ctx *h, double d) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    // World::setDamping, pe/core/World.h:767 (valid range [0, 1])
+    if (d < 0.0 || d > 1.0) return set_err(c, PE_B200_ERR_ARG, "Invalid damping value");
+    c->p.damping = d;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_max_iterations(pe_b200_ctx *h, int32_t n) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || n < 0) return PE_B200_ERR_ARG;
+    c->p.max_iterations = n;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_relaxation_model(pe_b200_ctx *h, int32_t m) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    if (m != PE_B200_INELASTIC_FRICTIONLESS && m != PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING)
+        return set_err(c, PE_B200_ERR_UNSUPPORTED, "Unsupported relaxation model.");
+    c->p.relaxation_model = m;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_error_reduction(pe_b200_ctx *h, double erp) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !(erp >= 0.0 && erp <= 1.0)) return PE_B200_ERR_ARG;
+    c->p.erp = erp;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_residual(pe_b200_ctx *h, int32_t enabled) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    c->want_residual = enabled ? 1 : 0;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_materials(pe_b200_ctx *h, int32_t n, const pe_b200_material *m) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || n <= 0 || n > kMaxMaterials || !m) return PE_B200_ERR_ARG;
+    std::string why;
+    for (int32_t k = 0; k < n; ++k)
+        if (check_material(m[k], why)) return set_err(c, PE_B200_ERR_ARG, why);
+    c->mats.assign(m, m + n);
+    if (c->uploaded) {
+        cudaSetDevice(c->device);
+        return upload_tables(c);
+    }
+    return PE_B200_OK;
+}
+
+int pe_b200_set_walls(pe_b200_ctx *h, int32_t scene, int32_t nplanes, const double *planes,
+                      const int32_t *plane_mat, int32_t nboxes, const double *boxes,
+                      const int32_t *box_mat) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || scene < 0 || scene >= kMaxScenes || nplanes < 0 || nboxes < 0) return PE_B200_ERR_ARG;
+    if ((nplanes > 0 && (!planes || !plane_mat)) || (nboxes > 0 && (!boxes || !box_mat)))
+        return PE_B200_ERR_ARG;
+    if ((size_t)scene >= c->scene_planes.size()) {
+        c->scene_planes.resize(scene + 1);
+        c->scene_plane_mat.resize(scene + 1);
+        c->scene_boxes.resize(scene + 1);
+        c->scene_box_mat.resize(scene + 1);
+    }
+    std::vector<double> pl(planes, planes + 4 * (size_t)nplanes);
+    for (int32_t p = 0; p < nplanes; ++p) {
+        double *q = &pl[4 * p];
+        const double l2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+        // createPlane: zero normals are rejected, others normalised (Plane.cpp:1206-1219)
+        if (!(l2 > 0.0)) return set_err(c, PE_B200_ERR_ARG, "Invalid plane normal!");
+        const double len = sqrt(l2), il = 1.0 / len;
+        q[0] *= il; q[1] *= il; q[2] *= il;
+        if (plane_mat[p] < 0 || (size_t)plane_mat[p] >= c->mats.size())
+            return set_err(c, PE_B200_ERR_ARG, "Invalid material ID");
+    }
+    for (int32_t b = 0; b < nboxes; ++b) {
+        const double *q = boxes + 15 * b;
+        // createBox: side lengths must be positive (Box.cpp:1316-1317)
+        if (!(q[3] > 0 && q[4] > 0 && q[5] > 0))
+            return set_err(c, PE_B200_ERR_ARG, "Invalid side length");
+        if (box_mat[b] < 0 || (size_t)box_mat[b] >= c->mats.size())
+            return set_err(c, PE_B200_ERR_ARG, "Invalid material ID");
+    }
+    c->scene_planes[scene] = pl;
+    c->scene_plane_mat[scene].assign(plane_mat, plane_mat + nplanes);
+    c->scene_boxes[scene].assign(boxes, boxes + 15 * (size_t)nboxes);
+    c->scene_box_mat[scene].assign(box_mat, box_mat + nboxes);
+    if (c->uploaded) {
+        cudaSetDevice(c->device);
+        return upload_tables(c);
+    }
+    return PE_B200_OK;
+}
+
+int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const double *v,
+                          const double *w, const double *r, const int32_t *mat,
+                          const int32_t *scene, int32_t nscenes) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || n < 0 || n > (int64_t)INT32_MAX / 2 || nscenes <= 0 || nscenes > kMaxScenes)
+        return PE_B200_ERR_ARG;
+    if (n > 0 && (!x || !v || !w || !r || !mat)) return PE_B200_ERR_ARG;
+    if (c->mats.empty()) return set_err(c, PE_B200_ERR_STATE, "materials must be set before bodies");
+    cudaSetDevice(c->device);
+    for (int64_t i = 0; i < n; ++i) {
+        // createSphere: the radius must be positive (Sphere.cpp:1193-1194)
+        if (!(r[i] > 0.0)) return set_err(c, PE_B200_ERR_ARG, "Invalid sphere radius");
+        if (mat[i] < 0 || (size_t)mat[i] >= c->mats.size())
+            return set_err(c, PE_B200_ERR_ARG, "Invalid material ID");
+        if (scene && (scene[i] < 0 || scene[i] >= nscenes))
+            return set_err(c, PE_B200_ERR_ARG, "Invalid scene ID");
+        for (int a = 0; a < 3; ++a)
+            if (!isfinite(x[3 * i + a]) || !isfinite(v[3 * i + a]) || !isfinite(w[3 * i + a]))
+                return set_err(c, PE_B200_ERR_NAN, "non-finite body state");
+    }
+    free_device(c);
+    c->n = n;
+    c->nscenes = nscenes;
+    c->scenes.assign(nscenes, SceneInfo());
+    c->scene_planes.resize(std::max<size_t>(c->scene_planes.size(), nscenes));
+    c->scene_plane_mat.resize(c->scene_planes.size());
+    c->scene_boxes.resize(c->scene_planes.size());
+    c->scene_box_mat.resize(c->scene_planes.size());
+    // group bodies by scene (stable) for the grid plan
+    std::vector<int64_t> count(nscenes, 0), begin(nscenes, 0), order(n);
+    for (int64_t i = 0; i < n; ++i) count[scene ? scene[i] : 0]++;
+    for (int s = 1; s < nscenes; ++s) begin[s] = begin[s - 1] + count[s - 1];
+    {
+        std::vector<int64_t> fill(begin);
+        for (int64_t i = 0; i < n; ++i) order[fill[scene ? scene[i] : 0]++] = i;
+    }
+    plan_grids(c, x, r, order, begin, count);
+    if (c->ncell > (int64_t)INT32_MAX / 2) return set_err(c, PE_B200_ERR_CAPACITY, "grid too large");
+    int rc = upload_tables(c);
+    if (rc) return rc;
+    rc = alloc_bodies(c, c->cur);
+    if (rc) return rc;
+    rc = alloc_bodies(c, c->nxt);
+    if (rc) return rc;
+    rc = grid_alloc(c);
+    if (rc) return rc;
+    // pack the host arrays into the device layout (upload order)
+    std::vector<double> pr(4 * (size_t)std::max<int64_t>(n, 1));
+    std::vector<uint32_t> tag(std::max<int64_t>(n, 1));
+    std::vector<int32_t> uid(std::max<int64_t>(n, 1));
+    std::vector<char> vw((size_t)std::max<int64_t>(n, 1) * c->vw_bytes);
+    const bool f64 = c->p.precision == PE_B200_FP64;
+    for (int64_t i = 0; i < n; ++i) {
+        pr[4 * i] = x[3 * i];
+        pr[4 * i + 1] = x[3 * i + 1];
+        pr[4 * i + 2] = x[3 * i + 2];
+        pr[4 * i + 3] = r[i];
+        tag[i] = (uint32_t)mat[i] | ((uint32_t)(scene ? scene[i] : 0) << 16);
+        uid[i] = (int32_t)i;
+        for (int a = 0; a < 3; ++a) {
+            if (f64) {
+                ((double *)vw.data())[6 * i + a] = v[3 * i + a];
+                ((double *)vw.data())[6 * i + 3 + a] = w[3 * i + a];
+            } else {
+                ((float *)vw.data())[6 * i + a] = (float)v[3 * i + a];
+                ((float *)vw.data())[6 * i + 3 + a] = (float)w[3 * i + a];
+            }
+        }
+    }
+    if (n > 0) {
+        PEB_CUDA(c, cudaMemcpy(c->cur.pr, pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpy(c->cur.vw, vw.data(), n * c->vw_bytes, cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpy(c->cur.tag, tag.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpy(c->cur.uid, uid.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        if (c->p.track_orientation) {
+            std::vector<double> q(4 * (size_t)n, 0.0);
+            for (int64_t i = 0; i < n; ++i) q[4 * i] = 1.0;
+            PEB_CUDA(c, cudaMemcpy(c->cur.q, q.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+        }
+    }
+    c->uploaded = true;
+    c->binned = false;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_state(pe_b200_ctx *h, const double *x, const double *v, const double *w) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    cudaSetDevice(c->device);
+    const int64_t n = c->n;
+    if (n == 0) return PE_B200_OK;
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    // current order -> upload order map
+    std::vector<int32_t> uid(n);
+    std::vector<double> pr(4 * (size_t)n);
+    std::vector<char> vw((size_t)n * c->vw_bytes);
+    PEB_CUDA(c, cudaMemcpy(uid.data(), c->cur.uid, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    PEB_CUDA(c, cudaMemcpy(pr.data(), c->cur.pr, n * sizeof(double4), cudaMemcpyDeviceToHost));
+    PEB_CUDA(c, cudaMemcpy(vw.data(), c->cur.vw, n * c->vw_bytes, cudaMemcpyDeviceToHost));
+    const bool f64 = c->p.precision == PE_B200_FP64;
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t i = uid[k];
+        for (int a = 0; a < 3; ++a) {
+            if (x) pr[4 * k + a] = x[3 * i + a];
+            if (f64) {
+                if (v) ((double *)vw.data())[6 * k + a] = v[3 * i + a];
+                if (w) ((double *)vw.data())[6 * k + 3 + a] = w[3 * i + a];
+            } else {
+                if (v) ((float *)vw.data())[6 * k + a] = (float)v[3 * i + a];
+                if (w) ((float *)vw.data())[6 * k + 3 + a] = (float)w[3 * i + a];
+            }
+        }
+    }
+    PEB_CUDA(c, cudaMemcpy(c->cur.pr, pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+    PEB_CUDA(c, cudaMemcpy(c->cur.vw, vw.data(), n * c->vw_bytes, cudaMemcpyHostToDevice));
+    c->binned = false;
+    return PE_B200_OK;
+}
+
+int pe_b200_step(pe_b200_ctx *h, int32_t nsteps, double dt) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    // World::simulationStep rejects non-positive time steps (src/core/World.cpp:333-334)
+    if (!(dt > 0.0)) return set_err(c, PE_B200_ERR_ARG, "Invalid time step size");
+    if (nsteps < 0) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    cudaSetDevice(c->device);
+    for (int32_t k = 0; k < nsteps; ++k) {
+        const int rc = (c->p.solver == PE_B200_DEM) ? dem_step(c, dt) : nbgs_step(c, dt);
+        if (rc) return rc;
+    }
+    return PE_B200_OK;
+}
+
+static int check_device_errors(Ctx *c) {
+    PEB_CUDA(c, cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int32_t e = *c->h_err;
+    if (e) {
+        PEB_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(int32_t), c->stream));
+        if (e & DERR_NAN) return set_err(c, PE_B200_ERR_NAN, "non-finite body state after step");
+        if (e & DERR_TIMEOUT) return set_err(c, PE_B200_ERR_TIMEOUT, "device wait timed out");
+        return set_err(c, PE_B200_ERR_CAPACITY, "device capacity exceeded");
+    }
+    return PE_B200_OK;
+}
+
+int pe_b200_download_bodies(pe_b200_ctx *h, double *x, double *v, double *w, double *q) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    if (q && !c->p.track_orientation)
+        return set_err(c, PE_B200_ERR_STATE, "orientations are not tracked");
+    cudaSetDevice(c->device);
+    const int64_t n = c->n;
+    if (n == 0) return PE_B200_OK;
+    std::vector<int32_t> uid(n);
+    std::vector<double> pr(4 * (size_t)n);
+    std::vector<char> vw((size_t)n * c->vw_bytes);
+    std::vector<double> qq(q ? 4 * (size_t)n : 0);
+    PEB_CUDA(c, cudaMemcpyAsync(uid.data(), c->cur.uid, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaMemcpyAsync(pr.data(), c->cur.pr, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaMemcpyAsync(vw.data(), c->cur.vw, n * c->vw_bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (q) PEB_CUDA(c, cudaMemcpyAsync(qq.data(), c->cur.q, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+    int rc = check_device_errors(c);
+    const bool f64 = c->p.precision == PE_B200_FP64;
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t i = uid[k];
+        if (i < 0 || i >= n) return set_err(c, PE_B200_ERR_STATE, "corrupt body permutation");
+        for (int a = 0; a < 3; ++a) {
+            if (x) x[3 * i + a] = pr[4 * k + a];
+            if (f64) {
+                if (v) v[3 * i + a] = ((double *)vw.data())[6 * k + a];
+                if (w) w[3 * i + a] = ((double *)vw.data())[6 * k + 3 + a];
+            } else {
+                if (v) v[3 * i + a] = ((float *)vw.data())[6 * k + a];
+                if (w) w[3 * i + a] = ((float *)vw.data())[6 * k + 3 + a];
+            }
+        }
+        if (q)
+            for (int a = 0; a < 4; ++a) q[4 * i + a] = qq[4 * k + a];
+    }
+    return rc;
+}
+
+int pe_b200_find_contacts(pe_b200_ctx *h, int64_t cap, int64_t *ids, double *geom,
+                          int64_t *n_out) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || cap < 0 || !n_out || (cap > 0 && (!ids || !geom))) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    cudaSetDevice(c->device);
+    return find_contacts(c, cap, ids, geom, n_out);
+}
+
+int pe_b200_last_step_stats(pe_b200_ctx *h, int64_t *ncontacts, int32_t *ncolors,
+                            double *delta_max, double *residual) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    if (ncontacts) *ncontacts = c->last_ncontacts;
+    if (ncolors) *ncolors = c->last_ncolors;
+    if (delta_max) *delta_max = c->last_delta;
+    if (residual) *residual = c->last_residual;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_profiling(pe_b200_ctx *h, int32_t enabled) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    cudaSetDevice(c->device);
+    prof_collect(c);
+    c->prof = enabled != 0;
+    for (int s = 0; s < ST_COUNT; ++s) {
+        c->prof_ms[s] = 0.0;
+        c->prof_count[s] = 0;
+    }
+    return PE_B200_OK;
+}
+
+int pe_b200_profile(pe_b200_ctx *h, int32_t cap, const char **names, double *total_ms,
+                    int64_t *count, int32_t *n_out) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || cap < 0 || !n_out) return PE_B200_ERR_ARG;
+    cudaSetDevice(c->device);
+    prof_collect(c);
+    const int m = cap < ST_COUNT ? cap : ST_COUNT;
+    for (int s = 0; s < m; ++s) {
+        if (names) names[s] = kStageNames[s];
+        if (total_ms) total_ms[s] = c->prof_ms[s];
+        if (count) count[s] = c->prof_count[s];
+    }
+    *n_out = ST_COUNT;
+    return PE_B200_OK;
+}
+
+int64_t pe_b200_kernel_launches(const pe_b200_ctx *h) {
+    const Ctx *c = reinterpret_cast<const Ctx *>(h);
+    return c ? c->launches : -1;
+}
+
+void *pe_b200_stream(pe_b200_ctx *h) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    return c ? (void *)c->stream : nullptr;
+}
+
+}  // extern "C"

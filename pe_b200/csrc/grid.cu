@@ -1,0 +1,215 @@
+// grid.cu -- uniform-grid build as a counting sort of cell keys.
+//
+// pe's coarse detector (pe/core/detection/coarse/HashGrids.h:1121-1314) re-hashes every body
+// into hierarchical hash grids and walks cell pairs with pointer-chasing.  Here the grid is a
+// dense per-scene array of int32 cells with a cell at least the largest AABB extent, so every
+// AABB-overlapping pair lies in neighbouring cells.  The sort is:
+//   count  (atomic histogram; the producing step kernel already did this for the next step)
+//   scan   (exclusive prefix sum over cells -> cell_start)
+//   scatter(slot of body i = cell_start[key[i]] + rank[i])
+//   fixup  (order each cell by body index, so the result is independent of atomic order)
+#include "internal.cuh"
+
+namespace peb {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int warp_incl_scan(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// exclusive scan of one tile; block total to tile_sums[blockIdx.x]
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile(const int32_t *__restrict__ in,
+                                                            int32_t *__restrict__ out, int64_t n,
+                                                            int32_t *__restrict__ tile_sums) {
+    __shared__ int warp_tot[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k;
+        v[k] = (i < n) ? in[i] : 0;
+        s += v[k];
+    }
+    const int incl = warp_incl_scan(s);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int t = (lane < kScanThreads / 32) ? warp_tot[lane] : 0;
+        t = warp_incl_scan(t);
+        if (lane < kScanThreads / 32) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    int run = incl - s + (warp > 0 ? warp_tot[warp - 1] : 0);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kScanThreads - 1) tile_sums[blockIdx.x] = run;
+}
+
+__global__ void k_scan_add(int32_t *__restrict__ out, int64_t n,
+                           const int32_t *__restrict__ tile_off) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_off[i / kScanTile];
+}
+
+__global__ void k_set_total(int32_t *out, int64_t n, const int32_t *last_in,
+                            const int32_t *last_out) {
+    out[n] = (n > 0) ? (*last_out + *last_in) : 0;
+}
+
+__global__ void k_bin(int64_t n, const double4 *__restrict__ pr, const uint32_t *__restrict__ tag,
+                      const SceneInfo *__restrict__ scenes, int32_t *__restrict__ key,
+                      int32_t *__restrict__ rank, int32_t *__restrict__ cell_count) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = pr[i];
+    const SceneInfo &s = scenes[tag[i] >> 16];
+    int cx, cy, cz;
+    cell_coords(s, p.x, p.y, p.z, cx, cy, cz);
+    const int32_t k = (int32_t)cell_key(s, cx, cy, cz);
+    key[i] = k;
+    rank[i] = atomicAdd(&cell_count[k], 1);
+}
+
+__global__ void k_scatter(int64_t n, const int32_t *__restrict__ key,
+                          const int32_t *__restrict__ rank, const int32_t *__restrict__ start,
+                          int32_t *__restrict__ sorted) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    sorted[start[key[i]] + rank[i]] = (int32_t)i;
+}
+
+// insertion sort of each cell's slots by body index (cells hold a handful of bodies)
+__global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
+                        int32_t *__restrict__ sorted) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const int b = start[c], e = start[c + 1];
+    if (e - b < 2) return;
+    for (int i = b + 1; i < e; ++i) {
+        const int32_t v = sorted[i];
+        int j = i - 1;
+        while (j >= b && sorted[j] > v) {
+            sorted[j + 1] = sorted[j];
+            --j;
+        }
+        sorted[j + 1] = v;
+    }
+}
+
+}  // namespace
+
+int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n) {
+    // recursive reduce-then-scan; scratch holds every level's tile sums
+    std::vector<int64_t> sizes;
+    int64_t m = n;
+    int64_t need = 0;
+    while (true) {
+        const int64_t tiles = (m + kScanTile - 1) / kScanTile;
+        sizes.push_back(m);
+        need += tiles + 1;
+        if (tiles <= 1) break;
+        m = tiles;
+    }
+    if (need + 1 > c->scan_tmp_cap) {
+        if (c->scan_tmp) cudaFree(c->scan_tmp);
+        c->scan_tmp = nullptr;
+        PEB_CUDA(c, cudaMalloc(&c->scan_tmp, (size_t)(need + 1) * sizeof(int32_t)));
+        c->scan_tmp_cap = need + 1;
+    }
+    // the last input element, kept for the total (the scan may run in place)
+    int32_t *last_in = c->scan_tmp + need;
+    if (n > 0)
+        PEB_CUDA(c, cudaMemcpyAsync(last_in, in + n - 1, sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    // level 0 ... L-1: scan, recording tile sums in scan_tmp
+    std::vector<int32_t *> lvl_in, lvl_out, lvl_sums;
+    const int32_t *cur_in = in;
+    int32_t *cur_out = out;
+    int32_t *tmp = c->scan_tmp;
+    for (size_t l = 0; l < sizes.size(); ++l) {
+        const int64_t len = sizes[l];
+        const int64_t tiles = (len + kScanTile - 1) / kScanTile;
+        int32_t *sums = tmp;
+        tmp += tiles + 1;
+        if (len > 0) {
+            k_scan_tile<<<(unsigned)tiles, kScanThreads, 0, c->stream>>>(cur_in, cur_out, len, sums);
+            PEB_LAUNCHED(c);
+        }
+        lvl_out.push_back(cur_out);
+        lvl_sums.push_back(sums);
+        if (tiles <= 1) break;
+        cur_in = sums;
+        cur_out = sums;  // scanned in place at the next level (the tile kernel reads before writing)
+    }
+    // propagate offsets downwards
+    for (int l = (int)lvl_out.size() - 2; l >= 0; --l) {
+        const int64_t len = sizes[l];
+        k_scan_add<<<grid_for(len, 256), 256, 0, c->stream>>>(lvl_out[l], len, lvl_sums[l]);
+        PEB_LAUNCHED(c);
+    }
+    k_set_total<<<1, 1, 0, c->stream>>>(out, n, last_in, out + (n > 0 ? n - 1 : 0));
+    PEB_LAUNCHED(c);
+    return PE_B200_OK;
+}
+
+int grid_alloc(Ctx *c) {
+    const size_t n = (size_t)c->n;
+    PEB_CUDA(c, cudaMalloc(&c->key, n * sizeof(int32_t) + 16));
+    PEB_CUDA(c, cudaMalloc(&c->rank, n * sizeof(int32_t) + 16));
+    PEB_CUDA(c, cudaMalloc(&c->sorted, n * sizeof(int32_t) + 16));
+    PEB_CUDA(c, cudaMalloc(&c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
+    return PE_B200_OK;
+}
+
+int grid_bin_current(Ctx *c) {
+    PEB_CUDA(c, cudaMemsetAsync(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t),
+                                c->stream));
+    if (c->n > 0) {
+        k_bin<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->n, c->cur.pr, c->cur.tag,
+                                                          c->d_scenes, c->key, c->rank,
+                                                          c->cell_count);
+        PEB_LAUNCHED(c);
+    }
+    c->binned = true;
+    return PE_B200_OK;
+}
+
+// cell_count/key/rank describe the current body order -> cell_start + sorted;
+// cell_count is cleared for the producing kernel of this step.
+int grid_sort(Ctx *c) {
+    prof_begin(c, ST_SORT);
+    int rc = scan_exclusive(c, c->cell_count, c->cell_start, c->ncell);
+    if (rc) return rc;
+    if (c->n > 0) {
+        k_scatter<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->n, c->key, c->rank,
+                                                              c->cell_start, c->sorted);
+        PEB_LAUNCHED(c);
+        k_fixup<<<grid_for(c->ncell, 256), 256, 0, c->stream>>>(c->ncell, c->cell_start,
+                                                                c->sorted);
+        PEB_LAUNCHED(c);
+    }
+    PEB_CUDA(c, cudaMemsetAsync(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t),
+                                c->stream));
+    prof_end(c, ST_SORT);
+    return PE_B200_OK;
+}
+
+}  // namespace peb

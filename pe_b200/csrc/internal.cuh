@@ -1,0 +1,284 @@
+// internal.cuh -- shared state, layouts and device helpers of libpe_b200.
+//
+// HBM layout (one context; all arrays in the internal body order, which is re-sorted by grid
+// cell every step, so a CTA's bodies and their neighbours sit in a few cache lines):
+//   pr   double4  (x, y, z, r)                        32 B / body, double-buffered
+//   vw   VT[6]    (vx, vy, vz, wx, wy, wz)             48 B (FP64) or 24 B (mixed) / body
+//   tag  uint32   material id | scene id << 16          4 B / body
+//   uid  int32    upload index (pe creation order)      4 B / body
+//   q    double4  orientation (only when tracked)      32 B / body
+// Uniform grid per scene (cell >= largest AABB extent, pe/core/detection/coarse/HashGrids.h
+// finds the same pair set): cell_count/cell_start are dense int32 arrays over all scenes' cells;
+// key/rank hold every body's cell and its slot inside that cell for the next sort.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pe_b200.h"
+
+namespace peb {
+
+constexpr double kContactThreshold = 1e-8;   // pe/core/Thresholds.h:151 (double)
+constexpr float kContactThresholdF = 5e-7f;  // pe/core/Thresholds.h:103 (float)
+constexpr double kFrictionThreshold = 1e-8;  // pe/core/Thresholds.h:161
+constexpr int kMaxScenes = 65535;
+constexpr int kMaxMaterials = 65535;
+
+struct SceneInfo {
+    double lo[3];
+    double h, inv_h;
+    int32_t dim[3];
+    int32_t pad0;
+    int64_t cell_base;
+    int32_t plane_begin, nplanes, box_begin, nboxes;
+    int64_t body_begin, nbodies;   // in upload order
+};
+
+// per-material constants; reciprocals so a composed value is one division (Materials.h:633)
+struct MatDev {
+    double density;
+    double rk, rcn, rct;   // 1/stiffness, 1/dampingN, 1/dampingT
+    double csf, cdf;
+};
+
+struct BodyBuf {
+    double4 *pr = nullptr;
+    void *vw = nullptr;
+    uint32_t *tag = nullptr;
+    int32_t *uid = nullptr;
+    double4 *q = nullptr;
+};
+
+struct NbgsBuf {
+    int64_t cap = 0;          // contact capacity
+    // contact records (FP64 or FP32 by precision), struct-of-arrays in a single allocation
+    void *cache = nullptr;
+    int32_t *b1 = nullptr, *b2 = nullptr;     // internal slots; b2 < 0: wall
+    int32_t *color = nullptr;                 // colour per contact
+    int32_t *order = nullptr;                 // contacts sorted by colour
+    int32_t *color_start = nullptr;           // host-visible after colouring
+    int32_t *cnt = nullptr;                   // per-slot contact counts / offsets (N+1)
+    int32_t *body_cnt = nullptr;              // per-body incident dynamic contacts (N+1)
+    int32_t *body_adj = nullptr;              // body -> contacts CSR (2 * cap)
+    uint64_t *used = nullptr;                 // colours used per body (bitmask)
+    int32_t *flags = nullptr;                 // device counters (uncoloured, overflow, ...)
+    void *vel = nullptr;                      // v', w', dv, dw per body (VT[12])
+    double *red = nullptr;                    // reduction scratch
+    int64_t red_cap = 0;
+};
+
+// stage timers (pe's profiling sections, e.g. DEMSolver.h:1159-1260): CUDA events around each
+// stage on the context's stream, summed when queried
+enum Stage : int {
+    ST_SORT = 0, ST_DEM, ST_PERMUTE, ST_DETECT, ST_COLOR, ST_CACHE, ST_SWEEP, ST_INTEGRATE,
+    ST_COUNT
+};
+extern const char *kStageNames[ST_COUNT];
+
+struct Ctx;
+void prof_begin(Ctx *c, int stage);
+void prof_end(Ctx *c, int stage);
+
+struct Ctx {
+    pe_b200_params p;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int sm_count = 148;
+    int64_t launches = 0;
+
+    // host copies
+    std::vector<pe_b200_material> mats;
+    std::vector<double> planes;     // 4 per plane, concatenated over scenes
+    std::vector<int32_t> plane_mat;
+    std::vector<double> boxes;      // 15 per box
+    std::vector<int32_t> box_mat;
+    std::vector<std::vector<double>> scene_planes, scene_boxes;
+    std::vector<std::vector<int32_t>> scene_plane_mat, scene_box_mat;
+    std::vector<SceneInfo> scenes;
+
+    // device
+    int64_t n = 0;                  // bodies
+    int32_t nscenes = 0;
+    int64_t ncell = 0;              // total cells over scenes
+    BodyBuf cur, nxt;
+    int32_t *key = nullptr, *rank = nullptr, *sorted = nullptr;
+    int32_t *cell_count = nullptr, *cell_start = nullptr;
+    int32_t *scan_tmp = nullptr;
+    int64_t scan_tmp_cap = 0;
+    SceneInfo *d_scenes = nullptr;
+    MatDev *d_mats = nullptr;
+    double4 *d_planes = nullptr;    // (n, d)
+    int32_t *d_plane_mat = nullptr;
+    double *d_boxes = nullptr;
+    int32_t *d_box_mat = nullptr;
+    int32_t *d_err = nullptr;       // device error word (bit flags)
+    int32_t *h_err = nullptr;       // pinned mirror
+    bool uploaded = false;
+    bool binned = false;
+    int64_t vw_bytes = 0;
+
+    NbgsBuf nb;
+    // profiling
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_open[ST_COUNT];
+    cudaEvent_t ev_pending[ST_COUNT] = {};
+    double prof_ms[ST_COUNT] = {};
+    int64_t prof_count[ST_COUNT] = {};
+    int64_t last_ncontacts = 0;
+    int32_t last_ncolors = 0;
+    double last_delta = -1.0, last_residual = -1.0;
+    int32_t want_residual = 0;
+};
+
+// device error flags
+enum : int32_t {
+    DERR_CAPACITY = 1,
+    DERR_NAN = 2,
+    DERR_TIMEOUT = 4,
+    DERR_CELL_OVERFLOW = 8,
+    DERR_COLORS = 16,
+};
+
+int set_err(Ctx *c, int code, const std::string &msg);
+int cuda_err(Ctx *c, cudaError_t e, const char *where);
+
+#define PEB_CUDA(ctx, call)                                            \
+    do {                                                               \
+        cudaError_t e__ = (call);                                      \
+        if (e__ != cudaSuccess) return ::peb::cuda_err(ctx, e__, #call); \
+    } while (0)
+
+#define PEB_LAUNCHED(ctx)                                                          \
+    do {                                                                           \
+        (ctx)->launches++;                                                         \
+        cudaError_t e__ = cudaGetLastError();                                      \
+        if (e__ != cudaSuccess) return ::peb::cuda_err(ctx, e__, "kernel launch"); \
+    } while (0)
+
+inline unsigned grid_for(int64_t n, int block) {
+    return (unsigned)((n + block - 1) / block);
+}
+
+// grid build: (re)bins bodies and sorts them by cell (grid.cu)
+int grid_alloc(Ctx *c);
+int grid_bin_current(Ctx *c);
+int grid_sort(Ctx *c);
+int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n);  // out[n] = total
+
+// solvers
+int dem_step(Ctx *c, double dt);
+int nbgs_step(Ctx *c, double dt);
+int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out);
+void nbgs_free(Ctx *c);
+
+// ------------------------------------------------------------------------------------------
+// device helpers
+// ------------------------------------------------------------------------------------------
+template <typename T>
+struct V3 {
+    T x, y, z;
+};
+
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> v3(T x, T y, T z) {
+    return V3<T>{x, y, z};
+}
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> operator+(V3<T> a, V3<T> b) {
+    return v3(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> operator-(V3<T> a, V3<T> b) {
+    return v3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> operator-(V3<T> a) {
+    return v3(-a.x, -a.y, -a.z);
+}
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> operator*(V3<T> a, T s) {
+    return v3(a.x * s, a.y * s, a.z * s);
+}
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> operator*(T s, V3<T> a) {
+    return v3(s * a.x, s * a.y, s * a.z);
+}
+template <typename T>
+__host__ __device__ __forceinline__ T dot(V3<T> a, V3<T> b) {
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename T>
+__host__ __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <typename T>
+__device__ __forceinline__ T vsqrt(T a);
+template <>
+__device__ __forceinline__ double vsqrt<double>(double a) { return sqrt(a); }
+template <>
+__device__ __forceinline__ float vsqrt<float>(float a) { return sqrtf(a); }
+
+template <typename T>
+__device__ __forceinline__ T length(V3<T> a) {
+    return vsqrt<T>(a.x * a.x + a.y * a.y + a.z * a.z);
+}
+// Vector3::getNormalized (pe/math/Vector3.h:1025-1037)
+template <typename T>
+__device__ __forceinline__ V3<T> normalized(V3<T> a) {
+    const T len = vsqrt<T>(a.x * a.x + a.y * a.y + a.z * a.z);
+    if (len == T(0)) return a;
+    const T il = T(1) / len;
+    return v3(a.x * il, a.y * il, a.z * il);
+}
+
+// Length without fused multiply-adds, so a pair predicate evaluates exactly as pe's FP64 code
+// (pe/math/Vector3.h:958) and the detected pair set matches bit for bit.
+__device__ __forceinline__ double length_rn(double x, double y, double z) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+__device__ __forceinline__ double dot_rn(double ax, double ay, double az, double bx, double by,
+                                         double bz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
+}
+
+template <typename T>
+__device__ __forceinline__ V3<T> ld_vw(const T *vw, int64_t i, int which) {
+    const T *p = vw + 6 * i + 3 * which;
+    return v3(p[0], p[1], p[2]);
+}
+
+__device__ __forceinline__ void sphere_mass(double r, double density, double &im, double &ii,
+                                            double &I) {
+    // SphereBase.h:169-171, SphereBase.cpp:79-80, SphereBase.h:230-234 + Matrix3x3::getInverse
+    const double mass = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(4.0 / 3.0, 3.14159265358979323846), r), r), r);
+    const double m2 = __dmul_rn(mass, density);
+    const double Iv = __dmul_rn(__dmul_rn(__dmul_rn(0.4, m2), r), r);
+    const double I2 = __dmul_rn(Iv, Iv);
+    const double det = __ddiv_rn(1.0, __dmul_rn(Iv, I2));
+    im = __ddiv_rn(1.0, m2);
+    ii = __dmul_rn(det, I2);
+    I = Iv;
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+__device__ __forceinline__ void cell_coords(const SceneInfo &s, double x, double y, double z,
+                                            int &cx, int &cy, int &cz) {
+    cx = clampi((int)floor((x - s.lo[0]) * s.inv_h), 0, s.dim[0] - 1);
+    cy = clampi((int)floor((y - s.lo[1]) * s.inv_h), 0, s.dim[1] - 1);
+    cz = clampi((int)floor((z - s.lo[2]) * s.inv_h), 0, s.dim[2] - 1);
+}
+
+__device__ __forceinline__ int64_t cell_key(const SceneInfo &s, int cx, int cy, int cz) {
+    return s.cell_base + ((int64_t)cz * s.dim[1] + cy) * s.dim[0] + cx;
+}
+
+}  // namespace peb

@@ -1,0 +1,920 @@
+// nbgs.cu -- hard-contact step (pe's HardContactSemiImplicitTimesteppingSolvers, "HCSITS") and
+// the explicit contact list behind pe_b200_find_contacts.
+//
+// Step (HCSITS.h:1472-2019), one sorted pass per stage:
+//   permute + body cache    state to cell-sorted slot order; v' = v + g dt,
+//                           w' = w + dt I^-1 ((I w) x w), dv = dw = 0 (HCSITS.h:1834-1880, 4094-4110)
+//   detect                  per-body count, exclusive scan, write (deterministic order)
+//   colour                  body-conflict-free edge colouring of the contact graph: rounds of
+//                           Jones-Plassmann selection, each winner takes the smallest colour
+//                           unused at both of its bodies (walls never conflict: infinite mass)
+//   contact cache           frame n,t,o; ERP-scaled distance; Delassus block D, D^-1, 1/D_nn,
+//                           (D_to)^-1 (HCSITS.h:1741-1820), stored in colour-sorted order
+//   sweeps                  max_iterations x colours: each colour is a conflict-free parallel
+//                           Gauss-Seidel sweep (relaxInelasticFrictionlessContacts :2039-2105,
+//                           relaxApproximateInelasticCoulombContactsByDecoupling :2129-2304)
+//   integrate               x += (v'+dv) dt, quaternion, drag, store v, w (HCSITS.h:4135-4190)
+// Colour order replaces pe's detection order; only converged frictionless velocities are
+// order-independent, which is what the parity tests compare.
+#include <algorithm>
+#include <vector>
+
+#include "contacts.cuh"
+
+namespace peb {
+
+namespace {
+
+constexpr int kBlk = 256;
+
+struct CountF {
+    int n = 0;
+    __device__ void operator()(const ContactGeom &) { ++n; }
+};
+
+// --------------------------------------------------------------------------------------------
+// contact list for pe_b200_find_contacts (uses the sort of the current state, no permutation)
+// --------------------------------------------------------------------------------------------
+__global__ void k_count(int64_t n, VisitArgs a, int32_t *cnt) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    CountF f;
+    visit_contacts(a, a.sorted ? a.sorted[t] : (int32_t)t, f);
+    cnt[t] = f.n;
+}
+
+struct ListF {
+    int64_t pos;
+    int64_t cap;
+    int64_t n_total;
+    int32_t uid_self;
+    int64_t *ids;
+    double *geom;
+    const int32_t *uid;
+    __device__ void operator()(const ContactGeom &g) {
+        if (pos < cap) {
+            ids[2 * pos] = uid_self;
+            ids[2 * pos + 1] = g.other >= 0 ? (int64_t)uid[g.other] : n_total + g.wall;
+            double *o = geom + 7 * pos;
+            o[0] = g.gx; o[1] = g.gy; o[2] = g.gz;
+            o[3] = g.nx; o[4] = g.ny; o[5] = g.nz;
+            o[6] = g.dist;
+        }
+        ++pos;
+    }
+};
+
+__global__ void k_list(int64_t n, VisitArgs a, const int32_t *off, int64_t cap, int64_t *ids,
+                       double *geom) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t b = a.sorted ? a.sorted[t] : (int32_t)t;
+    ListF f;
+    f.pos = off[t];
+    f.cap = cap;
+    f.n_total = n;
+    f.uid_self = a.uid[b];
+    f.ids = ids;
+    f.geom = geom;
+    f.uid = a.uid;
+    visit_contacts(a, b, f);
+}
+
+VisitArgs visit_args(Ctx *c, const int32_t *sorted) {
+    VisitArgs a;
+    a.sorted = sorted;
+    a.cell_start = c->cell_start;
+    a.scenes = c->d_scenes;
+    a.planes = c->d_planes;
+    a.boxes = c->d_boxes;
+    a.pr = c->cur.pr;
+    a.tag = c->cur.tag;
+    a.uid = c->cur.uid;
+    a.total_planes = (int32_t)(c->planes.size() / 4);
+    return a;
+}
+
+// --------------------------------------------------------------------------------------------
+// hard-contact step
+// --------------------------------------------------------------------------------------------
+template <typename T>
+struct Raw {  // detection output, detection order
+    int32_t *b1, *b2;
+    T *r1, *r2, *n;   // 3 x cap each, component-major
+    T *dist, *mu;
+};
+
+template <typename T>
+struct Cache {  // colour-sorted solver records (component-major SoA)
+    int32_t *b1, *b2;
+    T *r1, *r2, *n, *t, *o;  // 3 x cap
+    T *dist, *mu, *dn_inv, *dnn;
+    T *dinv;                 // 6 x cap: xx xy xz yy yz zz (contact frame)
+    T *dto_inv;              // 3 x cap: tt to oo
+    T *p;                    // 3 x cap, contact frame
+};
+
+template <typename T>
+struct BodyV {  // per body, slot order
+    T *v, *w, *dv, *dw;   // 3 x n each, component-major
+    T *im, *ii;
+};
+
+template <typename T>
+__device__ __forceinline__ V3<T> ld3c(const T *a, int64_t i, int64_t s) {
+    return v3(a[i], a[i + s], a[i + 2 * s]);
+}
+template <typename T>
+__device__ __forceinline__ void st3c(T *a, int64_t i, int64_t s, V3<T> v) {
+    a[i] = v.x; a[i + s] = v.y; a[i + 2 * s] = v.z;
+}
+
+// permute to slot order and fill the body cache
+template <typename VT, bool TRACKQ>
+__global__ void k_permute_cache(int64_t n, const int32_t *sorted, const double4 *pr,
+                                const VT *vw, const uint32_t *tag, const int32_t *uid,
+                                const double4 *q, double4 *pr_o, VT *vw_o, uint32_t *tag_o,
+                                int32_t *uid_o, double4 *q_o, const MatDev *mats, double gx,
+                                double gy, double gz, double dt, BodyV<VT> bv) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t b = sorted[t];
+    const double4 p = pr[b];
+    const uint32_t tg = tag[b];
+    pr_o[t] = p;
+    tag_o[t] = tg;
+    uid_o[t] = uid[b];
+    if (TRACKQ) q_o[t] = q[b];
+    const VT *src = vw + 6 * (int64_t)b;
+    VT *dst = vw_o + 6 * t;
+    V3<VT> v = v3(src[0], src[1], src[2]), w = v3(src[3], src[4], src[5]);
+    dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; dst[3] = w.x; dst[4] = w.y; dst[5] = w.z;
+    double im, ii, I;
+    sphere_mass(p.w, mats[tg & 0xffffu].density, im, ii, I);
+    const V3<VT> vp = v + v3(VT(gx), VT(gy), VT(gz)) * VT(dt);
+    const V3<VT> Iw = VT(I) * w;
+    const V3<VT> wp = w + VT(dt) * (VT(ii) * cross(Iw, w));
+    st3c(bv.v, t, n, vp);
+    st3c(bv.w, t, n, wp);
+    const V3<VT> z = v3(VT(0), VT(0), VT(0));
+    st3c(bv.dv, t, n, z);
+    st3c(bv.dw, t, n, z);
+    bv.im[t] = VT(im);
+    bv.ii[t] = VT(ii);
+}
+
+template <typename T>
+struct RawF {
+    int64_t pos, cap, n;
+    int32_t self;
+    double4 ps;
+    V3<double> vs, ws;
+    const MatDev *mats;
+    uint32_t tag_self;
+    const uint32_t *tag;
+    const int32_t *plane_mat, *box_mat;
+    int32_t total_planes;
+    const double4 *pr;
+    const T *vw;
+    double erp;
+    Raw<T> raw;
+    __device__ void operator()(const ContactGeom &g) {
+        if (pos >= cap) { ++pos; return; }
+        // relative velocity at the contact point for the friction pick (Contact.cpp:82-105)
+        const V3<double> gp = v3(g.gx, g.gy, g.gz);
+        const V3<double> r1 = gp - v3(ps.x, ps.y, ps.z);
+        V3<double> rvel = vs + cross(ws, r1);
+        V3<double> r2 = v3(0.0, 0.0, 0.0);
+        int32_t m2;
+        if (g.other >= 0) {
+            const double4 pj = pr[g.other];
+            r2 = gp - v3(pj.x, pj.y, pj.z);
+            const T *o = vw + 6 * (int64_t)g.other;
+            const V3<double> vj = v3(double(o[0]), double(o[1]), double(o[2]));
+            const V3<double> wj = v3(double(o[3]), double(o[4]), double(o[5]));
+            rvel = rvel - (vj + cross(wj, r2));
+            m2 = (int32_t)(tag[g.other] & 0xffffu);
+        } else {
+            m2 = g.wall < total_planes ? plane_mat[g.wall] : box_mat[g.wall - total_planes];
+        }
+        const V3<double> n = v3(g.nx, g.ny, g.nz);
+        const double nvel = dot(n, rvel);
+        const double tvel = dot(n, rvel - n * nvel);
+        const MatDev &a = mats[tag_self & 0xffffu], &b = mats[m2];
+        const double mu = (fabs(tvel) > kFrictionThreshold) ? a.cdf + b.cdf : a.csf + b.csf;
+        double dist = g.dist;
+        if (dist < 0.0) dist *= erp;   // HCSITS.h:1797-1800
+        raw.b1[pos] = self;
+        raw.b2[pos] = g.other;
+        st3c(raw.r1, pos, cap, v3(T(r1.x), T(r1.y), T(r1.z)));
+        st3c(raw.r2, pos, cap, v3(T(r2.x), T(r2.y), T(r2.z)));
+        st3c(raw.n, pos, cap, v3(T(n.x), T(n.y), T(n.z)));
+        raw.dist[pos] = T(dist);
+        raw.mu[pos] = T(mu);
+        ++pos;
+    }
+};
+
+template <typename T>
+__global__ void k_raw(int64_t n, VisitArgs a, const int32_t *off, int64_t cap, const T *vw,
+                      const MatDev *mats, const int32_t *plane_mat, const int32_t *box_mat,
+                      double erp, Raw<T> raw, int32_t *err) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    RawF<T> f;
+    f.pos = off[t];
+    f.cap = cap;
+    f.n = n;
+    f.self = (int32_t)t;
+    f.ps = a.pr[t];
+    const T *o = vw + 6 * t;
+    f.vs = v3(double(o[0]), double(o[1]), double(o[2]));
+    f.ws = v3(double(o[3]), double(o[4]), double(o[5]));
+    f.mats = mats;
+    f.tag_self = a.tag[t];
+    f.tag = a.tag;
+    f.plane_mat = plane_mat;
+    f.box_mat = box_mat;
+    f.total_planes = a.total_planes;
+    f.pr = a.pr;
+    f.vw = vw;
+    f.erp = erp;
+    f.raw = raw;
+    visit_contacts(a, (int32_t)t, f);
+    if (f.pos > cap) atomicOr(err, DERR_CAPACITY);
+}
+
+// ---- colouring --------------------------------------------------------------------------------
+__global__ void k_degree(int64_t nc, const int32_t *b1, const int32_t *b2, int32_t *deg) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    atomicAdd(&deg[b1[c]], 1);
+    if (b2[c] >= 0) atomicAdd(&deg[b2[c]], 1);
+}
+
+__global__ void k_adj_fill(int64_t nc, const int32_t *b1, const int32_t *b2, int32_t *fill,
+                           int32_t *adj) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    adj[atomicAdd(&fill[b1[c]], 1)] = (int32_t)c;
+    if (b2[c] >= 0) adj[atomicAdd(&fill[b2[c]], 1)] = (int32_t)c;
+}
+
+__device__ __forceinline__ uint32_t prio(uint32_t c) {
+    uint32_t h = c * 0x9E3779B1u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ bool beats(uint32_t c, uint32_t e) {
+    const uint32_t pc = prio(c), pe_ = prio(e);
+    return pc > pe_ || (pc == pe_ && c > e);
+}
+
+// one Jones-Plassmann round: an uncoloured contact whose priority beats every uncoloured
+// neighbour (contacts sharing a dynamic body) takes the smallest colour free at both bodies
+__global__ void k_color_round(int64_t nc, int round, const int32_t *b1, const int32_t *b2,
+                              const int32_t *adj_start, const int32_t *adj, int32_t *color,
+                              uint64_t *used, int32_t *remaining, int32_t *err) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc || color[c] >= 0) return;
+    const int32_t bodies[2] = {b1[c], b2[c]};
+    for (int k = 0; k < 2; ++k) {
+        const int32_t b = bodies[k];
+        if (b < 0) continue;
+        for (int s = adj_start[b]; s < adj_start[b + 1]; ++s) {
+            const int32_t e = adj[s];
+            if (e == c) continue;
+            const int32_t ce = color[e];
+            // neighbours coloured in an earlier round no longer compete
+            if (ce >= 0 && ce < (1 << 20) && ((ce >> 8) < round)) continue;
+            if (beats((uint32_t)e, (uint32_t)c)) {
+                atomicAdd(remaining, 1);
+                return;
+            }
+        }
+    }
+    const uint64_t u = used[bodies[0]] | (bodies[1] >= 0 ? used[bodies[1]] : 0ull);
+    const int col = __ffsll((long long)~u) - 1;
+    if (col < 0) {
+        atomicOr(err, DERR_COLORS);
+        return;
+    }
+    // colour and round packed: low 8 bits colour, upper bits the round it was chosen in
+    color[c] = (round << 8) | col;
+    used[bodies[0]] |= (1ull << col);
+    if (bodies[1] >= 0) used[bodies[1]] |= (1ull << col);
+}
+
+__global__ void k_color_hist(int64_t nc, int32_t *color, int32_t *hist, int32_t *ncolors) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int col = color[c] & 0xff;
+    color[c] = col;
+    atomicAdd(&hist[col], 1);
+    atomicMax(ncolors, col + 1);
+}
+
+__global__ void k_color_pos(int64_t nc, const int32_t *color, int32_t *fill, int32_t *pos) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    pos[c] = atomicAdd(&fill[color[c]], 1);
+}
+
+// ---- contact cache (HCSITS.h:1767-1815) --------------------------------------------------------
+template <typename T>
+__global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos, BodyV<T> bv,
+                        int64_t nb, Cache<T> cc) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int64_t k = pos[c];
+    const int32_t b1 = raw.b1[c], b2 = raw.b2[c];
+    const V3<T> r1 = ld3c(raw.r1, c, cap), r2 = ld3c(raw.r2, c, cap), n = ld3c(raw.n, c, cap);
+    V3<T> t;
+    if (fabs(n.x) < fabs(n.y)) {
+        if (fabs(n.x) < fabs(n.z)) t = v3(T(0), n.z, -n.y);
+        else t = v3(n.y, -n.x, T(0));
+    } else {
+        if (fabs(n.y) < fabs(n.z)) t = v3(-n.z, T(0), n.x);
+        else t = v3(n.y, -n.x, T(0));
+    }
+    t = normalized(t);
+    const V3<T> o = cross(n, t);
+    const T im1 = bv.im[b1], ii1 = bv.ii[b1];
+    const T im2 = b2 >= 0 ? bv.im[b2] : T(0), ii2 = b2 >= 0 ? bv.ii[b2] : T(0);
+    // D = -(r1^x I1^-1 r1^x + r2^x I2^-1 r2^x) + (1/m1 + 1/m2) 1 with scalar sphere inertia:
+    // -r^x r^x = |r|^2 1 - r r^T
+    T D[9];
+    const T a1 = dot(r1, r1), a2 = dot(r2, r2);
+    const T rr1[3] = {r1.x, r1.y, r1.z}, rr2[3] = {r2.x, r2.y, r2.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const T d1 = (i == j ? a1 : T(0)) - rr1[i] * rr1[j];
+            const T d2 = (i == j ? a2 : T(0)) - rr2[i] * rr2[j];
+            D[3 * i + j] = ii1 * d1 + ii2 * d2 + (i == j ? im1 + im2 : T(0));
+        }
+    // rotate into the contact frame: Dc = C^T D C with C = [n t o]
+    const V3<T> C[3] = {n, t, o};
+    T Dc[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const V3<T> DCi = v3(D[0] * C[i].x + D[1] * C[i].y + D[2] * C[i].z,
+                             D[3] * C[i].x + D[4] * C[i].y + D[5] * C[i].z,
+                             D[6] * C[i].x + D[7] * C[i].y + D[8] * C[i].z);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Dc[j][i] = dot(C[j], DCi);
+    }
+    // symmetric inverse
+    const T xx = Dc[0][0], xy = Dc[0][1], xz = Dc[0][2], yy = Dc[1][1], yz = Dc[1][2],
+            zz = Dc[2][2];
+    const T c00 = yy * zz - yz * yz, c01 = xz * yz - xy * zz, c02 = xy * yz - xz * yy;
+    const T det = xx * c00 + xy * c01 + xz * c02;
+    const T id = T(1) / det;
+    cc.dinv[k] = c00 * id;
+    cc.dinv[k + cap] = c01 * id;
+    cc.dinv[k + 2 * cap] = c02 * id;
+    cc.dinv[k + 3 * cap] = (xx * zz - xz * xz) * id;
+    cc.dinv[k + 4 * cap] = (xy * xz - xx * yz) * id;
+    cc.dinv[k + 5 * cap] = (xx * yy - xy * xy) * id;
+    cc.dn_inv[k] = T(1) / xx;
+    cc.dnn[k] = xx;
+    const T d2 = yy * zz - yz * yz;
+    const T id2 = T(1) / d2;
+    cc.dto_inv[k] = zz * id2;
+    cc.dto_inv[k + cap] = -yz * id2;
+    cc.dto_inv[k + 2 * cap] = yy * id2;
+    cc.b1[k] = b1;
+    cc.b2[k] = b2;
+    st3c(cc.r1, k, cap, r1);
+    st3c(cc.r2, k, cap, r2);
+    st3c(cc.n, k, cap, n);
+    st3c(cc.t, k, cap, t);
+    st3c(cc.o, k, cap, o);
+    cc.dist[k] = raw.dist[c];
+    cc.mu[k] = raw.mu[c];
+    st3c(cc.p, k, cap, v3(T(0), T(0), T(0)));
+    (void)nb;
+}
+
+// ---- one colour of one sweep ----------------------------------------------------------------
+template <typename T, bool FRICTION>
+__global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int64_t cap, T dtinv,
+                                                Cache<T> cc, BodyV<T> bv, int64_t nb,
+                                                int track_delta, unsigned long long *delta) {
+    const int64_t k = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= end) return;
+    const int32_t b1 = cc.b1[k], b2 = cc.b2[k];
+    const V3<T> r1 = ld3c(cc.r1, k, cap), r2 = ld3c(cc.r2, k, cap);
+    const V3<T> n = ld3c(cc.n, k, cap);
+    const V3<T> pc = ld3c(cc.p, k, cap);  // contact-frame impulse
+    const T im1 = bv.im[b1], ii1 = bv.ii[b1];
+    V3<T> dv1 = ld3c(bv.dv, b1, nb), dw1 = ld3c(bv.dw, b1, nb);
+    const V3<T> v1 = ld3c(bv.v, b1, nb), w1 = ld3c(bv.w, b1, nb);
+    V3<T> dv2 = v3(T(0), T(0), T(0)), dw2 = dv2, v2 = dv2, w2 = dv2;
+    T im2 = T(0), ii2 = T(0);
+    if (b2 >= 0) {
+        im2 = bv.im[b2];
+        ii2 = bv.ii[b2];
+        dv2 = ld3c(bv.dv, b2, nb);
+        dw2 = ld3c(bv.dw, b2, nb);
+        v2 = ld3c(bv.v, b2, nb);
+        w2 = ld3c(bv.w, b2, nb);
+    }
+    V3<T> t, o;
+    V3<T> pold;
+    if (FRICTION) {
+        t = ld3c(cc.t, k, cap);
+        o = ld3c(cc.o, k, cap);
+        pold = n * pc.x + t * pc.y + o * pc.z;
+    } else {
+        pold = n * pc.x;
+    }
+    // remove this contact's impulse (HCSITS.h:2050-2053)
+    dv1 = dv1 - im1 * pold;
+    dw1 = dw1 - ii1 * cross(r1, pold);
+    if (b2 >= 0) {
+        dv2 = dv2 + im2 * pold;
+        dw2 = dw2 + ii2 * cross(r2, pold);
+    }
+    const V3<T> gdot = ((v1 + dv1) - (v2 + dv2) + cross(w1 + dw1, r1)) - cross(w2 + dw2, r2);
+    T gn = dot(n, gdot) + cc.dist[k] * dtinv;
+    V3<T> pnew = v3(T(0), T(0), T(0));
+    V3<T> pcf = pnew;
+    if (gn < T(0)) {
+        if (!FRICTION) {
+            pcf.x = -cc.dn_inv[k] * gn;
+            pnew = n * pcf.x;
+        } else {
+            const T gt = dot(t, gdot), go = dot(o, gdot);
+            const T *di = cc.dinv;
+            const T dxx = di[k], dxy = di[k + cap], dxz = di[k + 2 * cap], dyy = di[k + 3 * cap],
+                    dyz = di[k + 4 * cap], dzz = di[k + 5 * cap];
+            pcf = v3(-(dxx * gn + dxy * gt + dxz * go), -(dxy * gn + dyy * gt + dyz * go),
+                     -(dxz * gn + dyz * gt + dzz * go));
+            const T mu = cc.mu[k];
+            T flimit = mu * pcf.x;
+            T fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+            if (fsq > flimit * flimit || pcf.x < T(0)) {
+                // decoupled relaxation (HCSITS.h:2187-2228)
+                V3<T> ptmp = t * pc.y + o * pc.z;
+                const V3<T> e1 = cross(ii1 * cross(r1, ptmp), r1);
+                const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
+                const T gdot_n = gn + dot(n, e1 + e2);
+                pcf.x = -(cc.dn_inv[k] * gdot_n);
+                pcf.x = pcf.x > T(0) ? pcf.x : T(0);
+                ptmp = n * pcf.x;
+                const V3<T> f1 = cross(ii1 * cross(r1, ptmp), r1);
+                const V3<T> f2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
+                const V3<T> gdot2 = (gdot + f1) + f2;
+                const T g2t = dot(t, gdot2), g2o = dot(o, gdot2);
+                const T *ti = cc.dto_inv;
+                pcf.y = -(ti[k] * g2t + ti[k + cap] * g2o);
+                pcf.z = -(ti[k + cap] * g2t + ti[k + 2 * cap] * g2o);
+                flimit = mu * pcf.x;
+                fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+                if (fsq > flimit * flimit) {
+                    const T f = flimit / sqrt(fsq);
+                    pcf.y *= f;
+                    pcf.z *= f;
+                }
+            }
+            pnew = n * pcf.x + t * pcf.y + o * pcf.z;
+        }
+        dv1 = dv1 + im1 * pnew;
+        dw1 = dw1 + ii1 * cross(r1, pnew);
+        if (b2 >= 0) {
+            dv2 = dv2 - im2 * pnew;
+            dw2 = dw2 - ii2 * cross(r2, pnew);
+        }
+    }
+    st3c(cc.p, k, cap, pcf);
+    st3c(bv.dv, b1, nb, dv1);
+    st3c(bv.dw, b1, nb, dw1);
+    if (b2 >= 0) {
+        st3c(bv.dv, b2, nb, dv2);
+        st3c(bv.dw, b2, nb, dw2);
+    }
+    if (track_delta) {
+        const V3<T> dp = pold - pnew;
+        const double m = fmax(fabs(double(dp.x)), fmax(fabs(double(dp.y)), fabs(double(dp.z))));
+        atomicMax(delta, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// complementarity residual of the final impulses (same definition as the oracle), in FP64
+template <typename T, bool FRICTION>
+__global__ void k_residual(int64_t nc, int64_t cap, double dtinv, Cache<T> cc, BodyV<T> bv,
+                           int64_t nb, unsigned long long *res) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nc) return;
+    const int32_t b1 = cc.b1[k], b2 = cc.b2[k];
+    auto L = [&](const T *a, int32_t b) { return v3(double(a[b]), double(a[b + nb]), double(a[b + 2 * nb])); };
+    auto C3 = [&](const T *a) { return v3(double(a[k]), double(a[k + cap]), double(a[k + 2 * cap])); };
+    const V3<double> r1 = C3(cc.r1), r2 = C3(cc.r2), n = C3(cc.n), t = C3(cc.t), o = C3(cc.o);
+    V3<double> a = L(bv.v, b1) + L(bv.dv, b1), wa = L(bv.w, b1) + L(bv.dw, b1);
+    V3<double> b = v3(0.0, 0.0, 0.0), wb = b;
+    if (b2 >= 0) {
+        b = L(bv.v, b2) + L(bv.dv, b2);
+        wb = L(bv.w, b2) + L(bv.dw, b2);
+    }
+    const V3<double> gdot = ((a - b) + cross(wa, r1)) - cross(wb, r2);
+    const double gn = dot(n, gdot) + double(cc.dist[k]) * dtinv;
+    const V3<double> pc = C3(cc.p);
+    const double pn = pc.x, Dnn = double(cc.dnn[k]);
+    double r = fabs(fmin(pn * Dnn, gn));
+    if (FRICTION) {
+        const double pt = pc.y, po = pc.z, gt = dot(t, gdot), go = dot(o, gdot);
+        const double pto = sqrt(pt * pt + po * po), gto = sqrt(gt * gt + go * go);
+        const double mu = double(cc.mu[k]);
+        r = fmax(r, fmax(0.0, pto - mu * pn) * Dnn);
+        if (pn > 0.0) {
+            if (pto < mu * pn * (1.0 - 1e-9)) r = fmax(r, gto);
+            else if (pto > 0.0) r = fmax(r, gto + (pt * gt + po * go) / pto);
+        }
+    }
+    atomicMax(res, (unsigned long long)__double_as_longlong(r));
+}
+
+template <typename VT, bool TRACKQ>
+__global__ void k_integrate(int64_t n, double dt, double drag, int has_drag, BodyV<VT> bv,
+                            const SceneInfo *scenes, const double4 *pr, const uint32_t *tag,
+                            const int32_t *uid, const double4 *q, double4 *pr_o, VT *vw_o,
+                            uint32_t *tag_o, int32_t *uid_o, double4 *q_o, int32_t *key,
+                            int32_t *rank, int32_t *cell_count, int32_t *err) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    V3<VT> v = ld3c(bv.v, t, n) + ld3c(bv.dv, t, n);
+    V3<VT> w = ld3c(bv.w, t, n) + ld3c(bv.dw, t, n);
+    const double4 p = pr[t];
+    const double nx = p.x + double(v.x) * dt, ny = p.y + double(v.y) * dt, nz = p.z + double(v.z) * dt;
+    if (TRACKQ) {
+        const double phx = double(w.x) * dt, phy = double(w.y) * dt, phz = double(w.z) * dt;
+        const double ang = sqrt(phx * phx + phy * phy + phz * phz);
+        double d0 = 1.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
+        if (!(fabs(ang) < 1e-15)) {
+            double sa, ca;
+            sincos(ang * 0.5, &sa, &ca);
+            const double il = 1.0 / ang;
+            d0 = ca; d1 = sa * (phx * il); d2 = sa * (phy * il); d3 = sa * (phz * il);
+        }
+        const double4 qq = q[t];
+        double4 r;
+        r.x = d0 * qq.x - d1 * qq.y - d2 * qq.z - d3 * qq.w;
+        r.y = d0 * qq.y + d1 * qq.x + d2 * qq.w - d3 * qq.z;
+        r.z = d0 * qq.z + d2 * qq.x + d3 * qq.y - d1 * qq.w;
+        r.w = d0 * qq.w + d3 * qq.x + d1 * qq.z - d2 * qq.y;
+        q_o[t] = r;
+    }
+    if (has_drag) {
+        v = v * VT(drag);
+        w = w * VT(drag);
+    }
+    pr_o[t] = make_double4(nx, ny, nz, p.w);
+    VT *o = vw_o + 6 * t;
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = w.x; o[4] = w.y; o[5] = w.z;
+    const uint32_t tg = tag[t];
+    tag_o[t] = tg;
+    uid_o[t] = uid[t];
+    if (!isfinite(nx) || !isfinite(ny) || !isfinite(nz)) atomicOr(err, DERR_NAN);
+    const SceneInfo &s = scenes[tg >> 16];
+    int cx, cy, cz;
+    cell_coords(s, nx, ny, nz, cx, cy, cz);
+    const int32_t kk = (int32_t)cell_key(s, cx, cy, cz);
+    key[t] = kk;
+    rank[t] = atomicAdd(&cell_count[kk], 1);
+}
+
+// ---- buffers -------------------------------------------------------------------------------
+int nbgs_alloc(Ctx *c, int64_t cap) {
+    NbgsBuf &b = c->nb;
+    const size_t es = (c->p.precision == PE_B200_FP64) ? 8 : 4;
+    const int64_t n = std::max<int64_t>(c->n, 1);
+    if (b.cap < cap) {
+        cudaFree(b.cache);
+        b.cache = nullptr;
+        cudaFree(b.order);
+        b.order = nullptr;
+        cudaFree(b.color);
+        b.color = nullptr;
+        cudaFree(b.body_adj);
+        b.body_adj = nullptr;
+        // raw: 2 int + 11 T; cache: 2 int + 27 T  (per contact)
+        const size_t bytes = (size_t)cap * (4 * sizeof(int32_t) + 42 * es) + 64 * 256;
+        PEB_CUDA(c, cudaMalloc(&b.cache, bytes));
+        PEB_CUDA(c, cudaMalloc(&b.order, (size_t)cap * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.color, (size_t)cap * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.body_adj, (size_t)2 * cap * sizeof(int32_t)));
+        b.cap = cap;
+    }
+    if (!b.cnt) {
+        PEB_CUDA(c, cudaMalloc(&b.cnt, ((size_t)n + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.body_cnt, ((size_t)n + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.used, (size_t)n * sizeof(uint64_t)));
+        PEB_CUDA(c, cudaMalloc(&b.vel, (size_t)n * 14 * es));
+        PEB_CUDA(c, cudaMalloc(&b.flags, 256 * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMallocHost(&b.color_start, 260 * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.red, 4 * sizeof(double)));
+    }
+    return PE_B200_OK;
+}
+
+template <typename T>
+void layout(Ctx *c, Raw<T> &raw, Cache<T> &cc, BodyV<T> &bv) {
+    NbgsBuf &b = c->nb;
+    const int64_t cap = b.cap;
+    char *p = (char *)b.cache;
+    auto take = [&](size_t bytes) {
+        char *q = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return q;
+    };
+    raw.b1 = (int32_t *)take(cap * 4);
+    raw.b2 = (int32_t *)take(cap * 4);
+    raw.r1 = (T *)take(3 * cap * sizeof(T));
+    raw.r2 = (T *)take(3 * cap * sizeof(T));
+    raw.n = (T *)take(3 * cap * sizeof(T));
+    raw.dist = (T *)take(cap * sizeof(T));
+    raw.mu = (T *)take(cap * sizeof(T));
+    cc.b1 = (int32_t *)take(cap * 4);
+    cc.b2 = (int32_t *)take(cap * 4);
+    cc.r1 = (T *)take(3 * cap * sizeof(T));
+    cc.r2 = (T *)take(3 * cap * sizeof(T));
+    cc.n = (T *)take(3 * cap * sizeof(T));
+    cc.t = (T *)take(3 * cap * sizeof(T));
+    cc.o = (T *)take(3 * cap * sizeof(T));
+    cc.dist = (T *)take(cap * sizeof(T));
+    cc.mu = (T *)take(cap * sizeof(T));
+    cc.dn_inv = (T *)take(cap * sizeof(T));
+    cc.dnn = (T *)take(cap * sizeof(T));
+    cc.dinv = (T *)take(6 * cap * sizeof(T));
+    cc.dto_inv = (T *)take(3 * cap * sizeof(T));
+    cc.p = (T *)take(3 * cap * sizeof(T));
+    const int64_t n = std::max<int64_t>(c->n, 1);
+    T *v = (T *)b.vel;
+    bv.v = v;
+    bv.w = v + 3 * n;
+    bv.dv = v + 6 * n;
+    bv.dw = v + 9 * n;
+    bv.im = v + 12 * n;
+    bv.ii = v + 13 * n;
+}
+
+template <typename VT>
+int nbgs_step_t(Ctx *c, double dt) {
+    NbgsBuf &nb = c->nb;
+    const int64_t n = c->n;
+    const int64_t auto_cap = c->p.max_contacts > 0 ? c->p.max_contacts : std::max<int64_t>(8 * n, 1024);
+    int rc = nbgs_alloc(c, auto_cap);
+    if (rc) return rc;
+    // 1. sort, permute to slot order, body cache
+    if (!c->binned) {
+        rc = grid_bin_current(c);
+        if (rc) return rc;
+    }
+    rc = grid_sort(c);
+    if (rc) return rc;
+    Raw<VT> raw;
+    Cache<VT> cc;
+    BodyV<VT> bv;
+    layout(c, raw, cc, bv);
+    {
+        prof_begin(c, ST_PERMUTE);
+        const bool tq = c->p.track_orientation != 0;
+        auto kern = tq ? k_permute_cache<VT, true> : k_permute_cache<VT, false>;
+        kern<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(
+            n, c->sorted, c->cur.pr, (const VT *)c->cur.vw, c->cur.tag, c->cur.uid, c->cur.q,
+            c->nxt.pr, (VT *)c->nxt.vw, c->nxt.tag, c->nxt.uid, c->nxt.q, c->d_mats,
+            c->p.gravity[0], c->p.gravity[1], c->p.gravity[2], dt, bv);
+        PEB_LAUNCHED(c);
+        prof_end(c, ST_PERMUTE);
+        std::swap(c->cur, c->nxt);
+    }
+    // 2. detection: count, scan, write (state is in slot order now: sorted == identity)
+    VisitArgs va = visit_args(c, nullptr);
+    prof_begin(c, ST_DETECT);
+    k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
+    PEB_LAUNCHED(c);
+    rc = scan_exclusive(c, nb.cnt, nb.cnt, n);
+    if (rc) return rc;
+    int32_t total = 0;
+    PEB_CUDA(c, cudaMemcpyAsync(&total, nb.cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (total > nb.cap) {
+        if (c->p.max_contacts > 0)
+            return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
+        rc = nbgs_alloc(c, (int64_t)total * 5 / 4 + 1024);
+        if (rc) return rc;
+        layout(c, raw, cc, bv);
+    }
+    const int64_t nc = total;
+    const int64_t cap = nb.cap;
+    c->last_ncontacts = nc;
+    k_raw<VT><<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt, cap, (const VT *)c->cur.vw,
+                                                         c->d_mats, c->d_plane_mat, c->d_box_mat,
+                                                         c->p.erp, raw, c->d_err);
+    PEB_LAUNCHED(c);
+    prof_end(c, ST_DETECT);
+    // 3. colouring
+    int32_t ncolors = 0;
+    if (nc > 0) {
+        prof_begin(c, ST_COLOR);
+        PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)n + 1) * sizeof(int32_t), c->stream));
+        k_degree<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, raw.b1, raw.b2, nb.body_cnt);
+        PEB_LAUNCHED(c);
+        rc = scan_exclusive(c, nb.body_cnt, nb.body_cnt, n);
+        if (rc) return rc;
+        int32_t *fill = nb.cnt;  // reuse: counts are consumed
+        PEB_CUDA(c, cudaMemcpyAsync(fill, nb.body_cnt, ((size_t)n + 1) * sizeof(int32_t),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        k_adj_fill<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, raw.b1, raw.b2, fill, nb.body_adj);
+        PEB_LAUNCHED(c);
+        PEB_CUDA(c, cudaMemsetAsync(nb.color, 0xff, (size_t)nc * sizeof(int32_t), c->stream));
+        PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)n * sizeof(uint64_t), c->stream));
+        int round = 0;
+        for (;;) {
+            const int batch = 8;
+            PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, batch * sizeof(int32_t), c->stream));
+            for (int k = 0; k < batch; ++k, ++round) {
+                k_color_round<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(
+                    nc, round, raw.b1, raw.b2, nb.body_cnt, nb.body_adj, nb.color, nb.used,
+                    nb.flags + k, c->d_err);
+                PEB_LAUNCHED(c);
+            }
+            int32_t rem[8];
+            PEB_CUDA(c, cudaMemcpyAsync(rem, nb.flags, sizeof rem, cudaMemcpyDeviceToHost, c->stream));
+            PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+            if (rem[batch - 1] == 0) break;
+            if (round > 4096) return set_err(c, PE_B200_ERR_TIMEOUT, "colouring did not finish");
+        }
+        // counting sort by colour
+        PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, 256 * sizeof(int32_t), c->stream));
+        int32_t *hist = nb.flags, *nco = nb.flags + 128;
+        k_color_hist<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, nb.color, hist, nco);
+        PEB_LAUNCHED(c);
+        PEB_CUDA(c, cudaMemcpyAsync(nb.color_start, nb.flags, 130 * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+        ncolors = nb.color_start[128];
+        std::vector<int32_t> start(ncolors + 1, 0);
+        for (int k = 0; k < ncolors; ++k) start[k + 1] = start[k] + nb.color_start[k];
+        for (int k = 0; k <= ncolors; ++k) nb.color_start[k] = start[k];
+        PEB_CUDA(c, cudaMemcpyAsync(nb.flags, start.data(), (ncolors + 1) * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, c->stream));
+        k_color_pos<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, nb.color, nb.flags, nb.order);
+        PEB_LAUNCHED(c);
+        prof_end(c, ST_COLOR);
+        prof_begin(c, ST_CACHE);
+        // 4. contact cache in colour-sorted order
+        k_cache<VT><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+        PEB_LAUNCHED(c);
+        prof_end(c, ST_CACHE);
+    }
+    c->last_ncolors = ncolors;
+    // 5. sweeps
+    const bool fr = c->p.relaxation_model == PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING;
+    const int iters = c->p.max_iterations;
+    unsigned long long *dl = (unsigned long long *)nb.red;
+    if (c->want_residual) PEB_CUDA(c, cudaMemsetAsync(nb.red, 0, 2 * sizeof(double), c->stream));
+    if (nc > 0) {
+        prof_begin(c, ST_SWEEP);
+        for (int it = 0; it < iters; ++it) {
+            const int track = (c->want_residual && it == iters - 1) ? 1 : 0;
+            for (int col = 0; col < ncolors; ++col) {
+                const int64_t b = nb.color_start[col], e = nb.color_start[col + 1];
+                if (e <= b) continue;
+                if (fr)
+                    k_sweep<VT, true><<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
+                        b, e, cap, VT(1.0 / dt), cc, bv, n, track, dl);
+                else
+                    k_sweep<VT, false><<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
+                        b, e, cap, VT(1.0 / dt), cc, bv, n, track, dl);
+                PEB_LAUNCHED(c);
+            }
+        }
+        prof_end(c, ST_SWEEP);
+        if (c->want_residual) {
+            if (fr)
+                k_residual<VT, true><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, 1.0 / dt, cc, bv, n, dl + 1);
+            else
+                k_residual<VT, false><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, 1.0 / dt, cc, bv, n, dl + 1);
+            PEB_LAUNCHED(c);
+        }
+    }
+    // 6. integrate into the other buffer and bin for the next step
+    {
+        prof_begin(c, ST_INTEGRATE);
+        const bool tq = c->p.track_orientation != 0;
+        const int has_drag = c->p.damping < 1.0;
+        const double drag = has_drag ? pow(c->p.damping, dt) : 1.0;
+        auto kern = tq ? k_integrate<VT, true> : k_integrate<VT, false>;
+        kern<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(
+            n, dt, drag, has_drag, bv, c->d_scenes, c->cur.pr, c->cur.tag, c->cur.uid, c->cur.q,
+            c->nxt.pr, (VT *)c->nxt.vw, c->nxt.tag, c->nxt.uid, c->nxt.q, c->key, c->rank,
+            c->cell_count, c->d_err);
+        PEB_LAUNCHED(c);
+        prof_end(c, ST_INTEGRATE);
+        std::swap(c->cur, c->nxt);
+    }
+    if (c->want_residual) {
+        double r[2];
+        PEB_CUDA(c, cudaMemcpyAsync(r, nb.red, sizeof r, cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->last_delta = nc > 0 ? r[0] : 0.0;
+        c->last_residual = nc > 0 ? r[1] : 0.0;
+    } else {
+        c->last_delta = -1.0;
+        c->last_residual = -1.0;
+    }
+    return PE_B200_OK;
+}
+
+}  // namespace
+
+void nbgs_free(Ctx *c) {
+    NbgsBuf &b = c->nb;
+    cudaFree(b.cache);
+    cudaFree(b.order);
+    cudaFree(b.color);
+    cudaFree(b.body_adj);
+    cudaFree(b.cnt);
+    cudaFree(b.body_cnt);
+    cudaFree(b.used);
+    cudaFree(b.vel);
+    cudaFree(b.flags);
+    cudaFree(b.red);
+    if (b.color_start) cudaFreeHost(b.color_start);
+    b = NbgsBuf();
+}
+
+int nbgs_step(Ctx *c, double dt) {
+    if (c->n == 0) return PE_B200_OK;
+    return (c->p.precision == PE_B200_FP64) ? nbgs_step_t<double>(c, dt) : nbgs_step_t<float>(c, dt);
+}
+
+int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out) {
+    const int64_t n = c->n;
+    *n_out = 0;
+    if (n == 0) return PE_B200_OK;
+    // make the sort describe the current state (keeps key/rank/counts valid for the next step)
+    if (!c->binned) {
+        int rc = grid_bin_current(c);
+        if (rc) return rc;
+    }
+    // the sort consumes cell_count; rebuild it afterwards from the same state
+    int rc = grid_sort(c);
+    if (rc) return rc;
+    int32_t *cnt = nullptr;
+    PEB_CUDA(c, cudaMalloc(&cnt, ((size_t)n + 2) * sizeof(int32_t)));
+    VisitArgs va = visit_args(c, c->sorted);
+    k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, cnt);
+    PEB_LAUNCHED(c);
+    rc = scan_exclusive(c, cnt, cnt, n);
+    if (rc) { cudaFree(cnt); return rc; }
+    int32_t total = 0;
+    PEB_CUDA(c, cudaMemcpyAsync(&total, cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::vector<int64_t> hid(2 * (size_t)std::max(total, 1));
+    std::vector<double> hg(7 * (size_t)std::max(total, 1));
+    int64_t *d_ids = nullptr;
+    double *d_geom = nullptr;
+    cudaError_t e = cudaMalloc(&d_ids, hid.size() * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d_geom, hg.size() * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(cnt); cudaFree(d_ids); cudaFree(d_geom);
+        return cuda_err(c, e, "find_contacts alloc");
+    }
+    k_list<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, cnt, total, d_ids, d_geom);
+    c->launches++;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hid.data(), d_ids, hid.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hg.data(), d_geom, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(cnt);
+    cudaFree(d_ids);
+    cudaFree(d_geom);
+    if (e != cudaSuccess) return cuda_err(c, e, "find_contacts");
+    // canonical order (b1, b2)
+    std::vector<int64_t> idx(total);
+    for (int64_t k = 0; k < total; ++k) idx[k] = k;
+    std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+        if (hid[2 * a] != hid[2 * b]) return hid[2 * a] < hid[2 * b];
+        return hid[2 * a + 1] < hid[2 * b + 1];
+    });
+    const int64_t m = std::min<int64_t>(cap, total);
+    for (int64_t k = 0; k < m; ++k) {
+        ids[2 * k] = hid[2 * idx[k]];
+        ids[2 * k + 1] = hid[2 * idx[k] + 1];
+        for (int a = 0; a < 7; ++a) geom[7 * k + a] = hg[7 * idx[k] + a];
+    }
+    *n_out = total;
+    // restore the binning of the current state for the next step
+    return grid_bin_current(c);
+}
+
+}  // namespace peb

@@ -1,0 +1,76 @@
+"""Generates the golden vectors of tests/golden/ by running the compiled pe reference.
+
+The reference is built from its own sources by oracle/ref/Makefile (into oracle/_ref/); this
+script feeds it seeded scenes (pe_b200.scenes) through its public API (oracle/ref/ref_driver.cpp)
+and stores inputs and outputs as compressed .npz files.  Run from the repository root:
+
+    make -C oracle/ref -j8 && python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from pe_b200 import scenes  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref")
+OUT = os.path.dirname(os.path.abspath(__file__))
+CONTACT_DTYPE = np.dtype([("b1", "<i8"), ("b2", "<i8"), ("gpos", "<f8", 3), ("n", "<f8", 3),
+                          ("dist", "<f8")])
+
+
+def run_pairs(exe, scene_path, tmp):
+    out = os.path.join(tmp, "pairs.bin")
+    subprocess.run([os.path.join(REF, exe), "pairs", scene_path, out], check=True)
+    b = open(out, "rb").read()
+    n = int(np.frombuffer(b[:8], "<i8")[0])
+    return np.frombuffer(b[8:], CONTACT_DTYPE, count=n).copy()
+
+
+def run_steps(exe, scene_path, n, steps, tmp, extra=()):
+    out = os.path.join(tmp, "state.bin")
+    subprocess.run([os.path.join(REF, exe), "step", scene_path, str(steps), out,
+                    *[str(e) for e in extra]], check=True)
+    a = np.fromfile(out, "<f8")
+    return (a[:3 * n].reshape(n, 3), a[3 * n:6 * n].reshape(n, 3), a[6 * n:9 * n].reshape(n, 3),
+            a[9 * n:].reshape(n, 4))
+
+
+def golden(name, scene, dem_steps=(1, 10), hc=True, hc_converged=False):
+    with tempfile.TemporaryDirectory() as tmp:
+        sp = os.path.join(tmp, "scene.bin")
+        scene.save(sp)
+        rec = {"scene": np.frombuffer(scene.to_bytes(), np.uint8)}
+        rec["pairs"] = run_pairs("ref_dem", sp, tmp)
+        for k in dem_steps:
+            x, v, w, q = run_steps("ref_dem", sp, scene.n, k, tmp)
+            rec[f"dem{k}_x"], rec[f"dem{k}_v"], rec[f"dem{k}_w"], rec[f"dem{k}_q"] = x, v, w, q
+        if hc:
+            rec["hc_pairs"] = run_pairs("ref_hcsits", sp, tmp)
+            for model in (0, 1):
+                x, v, w, q = run_steps("ref_hcsits", sp, scene.n, 1, tmp, (model, 100))
+                rec[f"hc{model}_x"], rec[f"hc{model}_v"], rec[f"hc{model}_w"] = x, v, w
+                rec[f"hc{model}_q"] = q
+        if hc_converged:
+            x, v, w, q = run_steps("ref_hcsits", sp, scene.n, 1, tmp, (0, 40000))
+            rec["hc0conv_x"], rec["hc0conv_v"], rec["hc0conv_w"] = x, v, w
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **rec)
+    print(path, os.path.getsize(path), "bytes,", len(rec["pairs"]), "contacts")
+
+
+if __name__ == "__main__":
+    golden("small64_boxes", scenes.small_random(1, n=64, with_boxes=True))
+    golden("small64_planes", scenes.small_random(2, n=64, with_boxes=False))
+    golden("lattice512", scenes.dem_lattice(0, side=8), dem_steps=(1, 10, 100))
+    golden("dense512", scenes.nbgs_box(0, n=512, dims=(8.0, 8.0, 20.0), dense=True),
+           dem_steps=(1,))
+    # loose packings whose frictionless solve converges (contacts form short chains)
+    golden("loose125_planes", scenes.small_random(3, n=125, overlap=0.0, with_boxes=False),
+           dem_steps=(1,), hc_converged=True)
+    golden("loose125_boxes", scenes.small_random(4, n=125, overlap=0.0, with_boxes=True),
+           dem_steps=(1,), hc_converged=True)

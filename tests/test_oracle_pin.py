@@ -1,0 +1,84 @@
+"""Pins the CPU restatement (oracle/) against golden vectors produced by the compiled pe
+reference (tests/golden/make_golden.py) and, when the reference build is present, against a
+live run of it."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import CONVERGED_NAMES, GOLDEN_NAMES, load_golden, pair_set, rel_err, rel_err_w
+from oracle.pe_oracle import APPROX_COULOMB_DECOUPLING, CONTACT_DTYPE, FRICTIONLESS, OracleWorld
+from pe_b200 import scenes
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_pairs_match_reference(name):
+    g = load_golden(name)
+    o = OracleWorld(g["scene"])
+    c = o.contacts()
+    ref = g["pairs"]
+    assert pair_set(np.stack([c["b1"], c["b2"]], 1)) == pair_set(np.stack([ref["b1"], ref["b2"]], 1))
+    # geometry of each contact (in canonical order)
+    order = np.lexsort((ref["b2"], ref["b1"]))
+    r = ref[order]
+    if len(r):
+        assert rel_err(c["gpos"], r["gpos"]) < 1e-15
+        assert rel_err(c["n"], r["n"]) < 1e-15
+        assert np.abs(c["dist"] - r["dist"]).max() < 1e-15
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_dem_steps_match_reference(name):
+    g = load_golden(name)
+    for key in sorted(k for k in g if k.startswith("dem") and k.endswith("_x")):
+        k = int(key[3:-2])
+        o = OracleWorld(g["scene"], track_orientation=True)
+        o.dem_step(g["scene"].dt, k)
+        tol = 1e-13 if k <= 10 else 1e-11
+        assert rel_err(o.x, g[f"dem{k}_x"]) < tol
+        assert rel_err(o.v, g[f"dem{k}_v"]) < tol
+        assert rel_err_w(o.w, g[f"dem{k}_w"], g[f"dem{k}_v"], g["scene"].r) < tol
+        assert rel_err(o.q, g[f"dem{k}_q"]) < tol
+
+
+@pytest.mark.parametrize("name", [n for n in GOLDEN_NAMES if n != "lattice512"])
+@pytest.mark.parametrize("model", [FRICTIONLESS, APPROX_COULOMB_DECOUPLING])
+def test_hcsits_step_bit_exact_in_reference_order(name, model):
+    """Replaying pe's own contact order, the restated sweep reproduces pe's step exactly."""
+    g = load_golden(name)
+    o = OracleWorld(g["scene"], track_orientation=True)
+    o.hcsits_step(g["scene"].dt, model, 100, contacts=g["hc_pairs"])
+    assert np.array_equal(o.x, g[f"hc{model}_x"])
+    assert np.array_equal(o.v, g[f"hc{model}_v"])
+    assert np.array_equal(o.w, g[f"hc{model}_w"])
+
+
+@pytest.mark.parametrize("name", CONVERGED_NAMES)
+def test_hcsits_converged_frictionless_any_order(name):
+    """Converged frictionless velocities do not depend on the sweep order."""
+    g = load_golden(name)
+    o = OracleWorld(g["scene"])
+    o.hcsits_step(g["scene"].dt, FRICTIONLESS, 40000)
+    assert rel_err(o.v, g["hc0conv_v"]) < 1e-6
+    assert rel_err(o.x, g["hc0conv_x"]) < 1e-9
+
+
+REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "ref_dem")),
+                    reason="compiled reference not built (make -C oracle/ref)")
+def test_live_reference_random_scenes(tmp_path):
+    for seed in range(3):
+        s = scenes.small_random(10 + seed, n=125, with_boxes=bool(seed % 2))
+        p = tmp_path / "s.bin"
+        s.save(str(p))
+        out = tmp_path / "o.bin"
+        subprocess.run([os.path.join(REF, "ref_dem"), "step", str(p), "5", str(out)], check=True)
+        a = np.fromfile(out, "<f8")
+        n = s.n
+        o = OracleWorld(s)
+        o.dem_step(s.dt, 5)
+        assert rel_err(o.x, a[:3 * n].reshape(n, 3)) < 1e-13
+        assert rel_err(o.v, a[3 * n:6 * n].reshape(n, 3)) < 1e-12
