@@ -161,6 +161,38 @@ int pe_b200_set_profiling(pe_b200_ctx *ctx, int32_t enabled);
 int pe_b200_profile(pe_b200_ctx *ctx, int32_t cap, const char **names, double *total_ms,
                     int64_t *count, int32_t *n_out);
 
+/* Allocation-free DEM step.  This entry point has no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory -- an application that owns all device memory
+ * through its own arena or pool, or a real-time loop that must not pay for an allocation's
+ * implicit synchronisation -- it advances one scene by one FP64 DEM step (the same kernel as
+ * pe_b200_step with PE_B200_DEM/PE_B200_FP64) without calling cudaMalloc, cudaFree or any
+ * allocating routine.  Its scratch lives in one fixed __device__ array inside the library
+ * (about 7.3 MB, held on every GPU that loads the library until the process exits).
+ *
+ *   x, v, w (3n doubles each, interleaved xyz), r (n), mat (n): device inputs;
+ *   x_out, v_out, w_out: device outputs (may alias nothing of the inputs);
+ *   mats/planes/boxes: host tables (as pe_b200_set_materials / pe_b200_set_walls);
+ *   domain_lo/hi: box the grid covers (bodies outside are clamped into border cells, still
+ *   exact); max_radius: no sphere may be larger (checked, PE_B200_ERR_ARG otherwise);
+ *   stream: cudaStream_t to run on (NULL: the legacy default stream).  Returns after the step
+ *   has finished on the device.
+ * Limits: n <= PE_B200_STATIC_MAX_SPHERES, <= 64 materials, <= 64 planes, <= 64 boxes (larger
+ * requests return PE_B200_ERR_ARG before any work); the grid is coarsened to at most
+ * PE_B200_STATIC_MAX_CELLS cells.  All calls on a device share the array: calls whose work
+ * overlaps on the GPU race and corrupt each other.  The first call on each device looks up the
+ * array's address; make it before any stream capture. */
+#define PE_B200_STATIC_MAX_SPHERES 32768
+#define PE_B200_STATIC_MAX_CELLS 131072
+int pe_b200_dem_step_static(int64_t n, const double *x, const double *v, const double *w,
+                            const double *r, const int32_t *mat, int32_t nmat,
+                            const pe_b200_material *mats, int32_t nplanes, const double *planes,
+                            const int32_t *plane_mat, int32_t nboxes, const double *boxes,
+                            const int32_t *box_mat, const double gravity[3], double damping,
+                            double dt, const double domain_lo[3], const double domain_hi[3],
+                            double max_radius, double *x_out, double *v_out, double *w_out,
+                            void *stream);
+
 /* Number of kernels this context launched since creation (device-side work accounting). */
 int64_t pe_b200_kernel_launches(const pe_b200_ctx *ctx);
 

@@ -351,4 +351,40 @@ int dem_step(Ctx *c, double dt) {
     return PE_B200_OK;
 }
 
+// Launches the FP64 step kernel on caller-provided buffers (used by the allocation-free entry
+// point in noalloc.cu); every pointer is device memory the caller owns.
+cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream) {
+    DemArgs<double> a;
+    a.n = r.n;
+    a.dt = r.dt;
+    for (int k = 0; k < 3; ++k) a.g[k] = r.g[k];
+    a.has_drag = r.damping < 1.0;
+    a.drag = a.has_drag ? pow(r.damping, r.dt) : 1.0;
+    a.sorted = r.sorted;
+    a.cell_start = r.cell_start;
+    a.scenes = r.scenes;
+    a.mats = r.mats;
+    a.planes = r.planes;
+    a.plane_mat = r.plane_mat;
+    a.boxes = r.boxes;
+    a.box_mat = r.box_mat;
+    a.pr = r.pr;
+    a.vw = r.vw;
+    a.tag = r.tag;
+    a.uid = r.uid;
+    a.q = nullptr;
+    a.pr_out = r.pr_out;
+    a.vw_out = r.vw_out;
+    a.tag_out = r.tag_out;
+    a.uid_out = r.uid_out;
+    a.q_out = nullptr;
+    a.key = r.key;
+    a.rank = r.rank;
+    a.cell_count = r.cell_count;
+    a.err = r.err;
+    if (r.n > 0)
+        k_dem_step<double, false><<<grid_for(r.n, kDemBlock), kDemBlock, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace peb

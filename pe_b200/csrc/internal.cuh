@@ -171,6 +171,30 @@ int grid_bin_current(Ctx *c);
 int grid_sort(Ctx *c);
 int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n);  // out[n] = total
 
+// FP64 DEM step kernel on raw device buffers (layout as above; single launch, no allocation)
+struct DemRawArgs {
+    int64_t n;
+    double dt, damping;
+    double g[3];
+    const int32_t *sorted, *cell_start;
+    const SceneInfo *scenes;
+    const MatDev *mats;
+    const double4 *planes;
+    const int32_t *plane_mat;
+    const double *boxes;
+    const int32_t *box_mat;
+    const double4 *pr;
+    const double *vw;
+    const uint32_t *tag;
+    const int32_t *uid;
+    double4 *pr_out;
+    double *vw_out;
+    uint32_t *tag_out;
+    int32_t *uid_out;
+    int32_t *key, *rank, *cell_count, *err;
+};
+cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream);
+
 // solvers
 int dem_step(Ctx *c, double dt);
 int nbgs_step(Ctx *c, double dt);
