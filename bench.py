@@ -287,7 +287,7 @@ def our_arm(args):
         kms, kcnt = prof.get("dem_step", (0.0, 0))
         per = ALGO_BYTES["mixed"]
         algo = per * nsph
-        kname = "k_dem_step<float>"
+        kname = "k_dem_list<float> (neighbour-list force + integration)"
     else:
         kms, kcnt = prof.get("sweeps", (0.0, 0))
         st = e.stats()

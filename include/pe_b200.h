@@ -64,6 +64,10 @@ typedef struct {
     int32_t device;            /* CUDA device ordinal */
     int32_t track_orientation; /* 1: integrate sphere quaternions (Default.h:190-193) */
     int64_t max_contacts;      /* HCSITS contact capacity; 0 = automatic (8 per sphere) */
+    double skin;               /* DEM neighbour-list skin; <= 0: 0.1 x the smallest radius */
+    int32_t neighbor_lists;    /* DEM: 1 = Verlet lists rebuilt on demand (default),
+                                  0 = grid search every step */
+    int32_t reserved;
 } pe_b200_params;
 
 /* createMaterial argument list, src/core/Materials.cpp:175 */

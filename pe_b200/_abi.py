@@ -37,7 +37,8 @@ class Params(C.Structure):
     _fields_ = [("solver", C.c_int32), ("precision", C.c_int32), ("relaxation_model", C.c_int32),
                 ("max_iterations", C.c_int32), ("erp", C.c_double),
                 ("gravity", C.c_double * 3), ("damping", C.c_double), ("device", C.c_int32),
-                ("track_orientation", C.c_int32), ("max_contacts", C.c_int64)]
+                ("track_orientation", C.c_int32), ("max_contacts", C.c_int64),
+                ("skin", C.c_double), ("neighbor_lists", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Material(C.Structure):

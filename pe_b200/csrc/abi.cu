@@ -10,6 +10,12 @@
 
 namespace peb {
 
+unsigned capped_grid(const Ctx *c, int64_t n, int block) {
+    const int64_t g = (n + block - 1) / block;
+    const int64_t cap = 8 * (int64_t)c->sm_count;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
 int set_err(Ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;
     return code;
@@ -22,7 +28,7 @@ int cuda_err(Ctx *c, cudaError_t e, const char *where) {
 }
 
 const char *kStageNames[ST_COUNT] = {"sort", "dem_step", "permute", "detect", "color",
-                                     "contact_cache", "sweeps", "integrate"};
+                                     "contact_cache", "sweeps", "integrate", "list_rebuild"};
 
 static cudaEvent_t take_event(Ctx *c) {
     if (!c->ev_pool.empty()) {
@@ -103,6 +109,7 @@ void free_device(Ctx *c) {
     c->d_boxes = nullptr;
     c->d_box_mat = nullptr;
     nbgs_free(c);
+    dem_list_free(c);
     c->uploaded = false;
     c->binned = false;
 }
@@ -281,6 +288,8 @@ void pe_b200_default_params(pe_b200_params *p) {
     p->device = 0;
     p->track_orientation = 0;
     p->max_contacts = 0;
+    p->skin = 0.0;
+    p->neighbor_lists = 1;
 }
 
 int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
@@ -522,6 +531,13 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
     }
     c->uploaded = true;
     c->binned = false;
+    if (c->p.solver == PE_B200_DEM && c->p.neighbor_lists && n > 0) {
+        double rmin = INFINITY;
+        for (int64_t i = 0; i < n; ++i) rmin = std::min(rmin, r[i]);
+        c->nl.skin = c->p.skin > 0.0 ? c->p.skin : 0.1 * rmin;
+        rc = dem_list_alloc(c);
+        if (rc) return rc;
+    }
     return PE_B200_OK;
 }
 
@@ -557,6 +573,10 @@ int pe_b200_set_state(pe_b200_ctx *h, const double *x, const double *v, const do
     PEB_CUDA(c, cudaMemcpy(c->cur.pr, pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
     PEB_CUDA(c, cudaMemcpy(c->cur.vw, vw.data(), n * c->vw_bytes, cudaMemcpyHostToDevice));
     c->binned = false;
+    if (c->nl.enabled) {
+        const int rc = dem_list_request_rebuild(c);
+        if (rc) return rc;
+    }
     return PE_B200_OK;
 }
 
@@ -569,7 +589,8 @@ int pe_b200_step(pe_b200_ctx *h, int32_t nsteps, double dt) {
     if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
     cudaSetDevice(c->device);
     for (int32_t k = 0; k < nsteps; ++k) {
-        const int rc = (c->p.solver == PE_B200_DEM) ? dem_step(c, dt) : nbgs_step(c, dt);
+        const int rc = (c->p.solver != PE_B200_DEM) ? nbgs_step(c, dt)
+                       : (c->nl.enabled ? dem_list_step(c, dt) : dem_step(c, dt));
         if (rc) return rc;
     }
     return PE_B200_OK;

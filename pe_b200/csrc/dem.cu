@@ -1,5 +1,4 @@
-// dem.cu -- fused DEM step: neighbour search, contact law, force accumulation and integration
-// in one kernel per step.
+// dem.cu -- the DEM step: neighbour search, contact law, force accumulation and integration.
 //
 // Restates, per body:
 //   detection    HashGrids::findContacts + MaxContacts::collideSphere{Sphere,Plane,Box}
@@ -15,10 +14,22 @@
 // both partners, in pe's orientation -- body 1 = smaller id -- so both see bitwise-opposite
 // forces) and no atomics or contact list are needed.
 //
-// Each thread owns one slot of the cell-sorted order and writes the integrated body to that
-// slot of the other buffer, so the state is re-sorted by cell as a side effect; it also bins
-// the integrated position for the next step's counting sort.
+// Two neighbour sources:
+//   grid   (k_dem_step) every step: the counting-sorted uniform grid, 27 cells per sphere; the
+//          thread owning sorted slot t writes its body to slot t of the other buffer, so the
+//          state is re-sorted by cell as a side effect, and it bins the result for the next sort.
+//   lists  (k_dem_list) Verlet lists: all pairs closer than r_i + r_j + skin when the list was
+//          built.  A sphere's accumulated path length is tracked; once any sphere has moved
+//          skin/2 the device requests a rebuild, which the next step performs (sort, permute to
+//          cell order, count/scan/write the lists) before its force kernel.  Every pair that can
+//          come within the contact threshold is therefore in the list, and the pair set is the
+//          grid's, exactly.  The rebuild kernels run every step and return at once unless
+//          requested, so the host never waits on the device to decide.  If a rebuild overflows
+//          the list capacity, that step's force kernel searches the fresh grid instead (exact)
+//          and the host grows the capacity at its next check.
 #include <math_constants.h>
+
+#include <algorithm>
 
 #include "internal.cuh"
 
@@ -84,7 +95,7 @@ struct DemArgs {
     double g[3];
     double drag;      // damping^dt
     int has_drag;
-    const int32_t *sorted;
+    const int32_t *sorted;   // grid kernel: slot -> body; nullptr: identity
     const int32_t *cell_start;
     const SceneInfo *scenes;
     const MatDev *mats;
@@ -106,84 +117,62 @@ struct DemArgs {
     int32_t *rank;
     int32_t *cell_count;
     int32_t *err;
+    // lists
+    const int32_t *nl_start;
+    const int32_t *nl_idx;
+    float *disp;
+    int32_t *nl_flags;
+    float half_skin;
 };
 
-template <typename VT, bool TRACKQ>
-__global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
-    using T = VT;  // arithmetic type of the contact law (double or float)
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
-    const int32_t b = a.sorted[t];
-    const double4 pi = a.pr[b];
-    const uint32_t tagi = a.tag[b];
-    const int32_t uidi = a.uid[b];
-    const SceneInfo &s = a.scenes[tagi >> 16];
-    const MatDev mi = a.mats[tagi & 0xffffu];
-    const V3<T> vi = ld_vw(a.vw, b, 0), wi = ld_vw(a.vw, b, 1);
-    Acc<T> acc;
-    acc.F = v3(T(0), T(0), T(0));
-    acc.T_ = acc.F;
-
-    int cx, cy, cz;
-    cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= s.dim[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= s.dim[1]) continue;
-            const int64_t c0 = cell_key(s, x0, y, z);
-            const int64_t c1 = c0 + (x1 - x0) + 1;
-            const int e = a.cell_start[c1];
-            for (int slot = a.cell_start[c0]; slot < e; ++slot) {
-                const int32_t j = a.sorted[slot];
-                if (j == b) continue;
-                const double4 pj = a.pr[j];
-                const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-                const double rs = pi.w + pj.w;
-                // only penetrating contacts (dist < -contactThreshold) produce a force
-                // (ContactBase.h:307-310); this bound is conservative for them
-                if (ddx * ddx + ddy * ddy + ddz * ddz >= rs * rs) continue;
-                const int32_t uidj = a.uid[j];
-                const bool self1 = uidi < uidj;
-                // pe orientation: body 1 = smaller system id (MaxContacts.h:550-551)
-                const double4 p1 = self1 ? pi : pj;
-                const double4 p2 = self1 ? pj : pi;
-                const double nx = p1.x - p2.x, ny = p1.y - p2.y, nz = p1.z - p2.z;
-                const double len = length_rn(nx, ny, nz);
-                const double dist = __dsub_rn(__dsub_rn(len, p1.w), p2.w);
-                if (!(dist < -kContactThreshold)) continue;
-                const MatDev mj = a.mats[a.tag[j] & 0xffffu];
-                const V3<T> vj = ld_vw(a.vw, j, 0), wj = ld_vw(a.vw, j, 1);
-                V3<T> n, r1, r2;
-                if (sizeof(T) == 8) {
-                    // FP64: the contact point in absolute coordinates, as pe computes it
-                    const double il = 1.0 / len;
-                    const double nnx = nx * il, nny = ny * il, nnz = nz * il;
-                    const double k = p2.w + 0.5 * dist;
-                    const double gx = p2.x + nnx * k, gy = p2.y + nny * k, gz = p2.z + nnz * k;
-                    n = v3(T(nnx), T(nny), T(nnz));
-                    r1 = v3(T(gx - p1.x), T(gy - p1.y), T(gz - p1.z));
-                    r2 = v3(T(gx - p2.x), T(gy - p2.y), T(gz - p2.z));
-                } else {
-                    // mixed: relative vectors only (the absolute point needs FP64)
-                    const V3<T> d = v3(T(nx), T(ny), T(nz));
-                    const T il = T(1) / T(len);
-                    n = d * il;
-                    const T k = T(p2.w) + T(0.5) * T(dist);
-                    r2 = n * k;
-                    r1 = r2 - d;
-                }
-                if (self1)
-                    dem_contact<T>(n, T(dist), r1, r2, vi, wi, vj, wj, mi, mj, true, acc);
-                else
-                    dem_contact<T>(n, T(dist), r1, r2, vj, wj, vi, wi, mj, mi, false, acc);
-            }
-        }
+// one sphere pair (body b and neighbour j), both in the buffers of `a`
+template <typename T, typename VT>
+__device__ __forceinline__ void pair_force(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
+                                           V3<T> wi, int32_t uidi, const MatDev &mi,
+                                           int32_t j, const double4 &pj, Acc<T> &acc) {
+    const int32_t uidj = a.uid[j];
+    const bool self1 = uidi < uidj;
+    // pe orientation: body 1 = smaller system id (MaxContacts.h:550-551)
+    const double4 p1 = self1 ? pi : pj;
+    const double4 p2 = self1 ? pj : pi;
+    const double nx = p1.x - p2.x, ny = p1.y - p2.y, nz = p1.z - p2.z;
+    const double len = length_rn(nx, ny, nz);
+    const double dist = __dsub_rn(__dsub_rn(len, p1.w), p2.w);
+    // only penetrating contacts produce a force (ContactBase.h:307-310)
+    if (!(dist < -kContactThreshold)) return;
+    const MatDev mj = a.mats[a.tag[j] & 0xffffu];
+    const V3<T> vj = ld_vw(a.vw, j, 0), wj = ld_vw(a.vw, j, 1);
+    V3<T> n, r1, r2;
+    if (sizeof(T) == 8) {
+        // FP64: the contact point in absolute coordinates, as pe computes it
+        const double il = 1.0 / len;
+        const double nnx = nx * il, nny = ny * il, nnz = nz * il;
+        const double k = p2.w + 0.5 * dist;
+        const double gx = p2.x + nnx * k, gy = p2.y + nny * k, gz = p2.z + nnz * k;
+        n = v3(T(nnx), T(nny), T(nnz));
+        r1 = v3(T(gx - p1.x), T(gy - p1.y), T(gz - p1.z));
+        r2 = v3(T(gx - p2.x), T(gy - p2.y), T(gz - p2.z));
+    } else {
+        // mixed: relative vectors only (the absolute point needs FP64)
+        const V3<T> d = v3(T(nx), T(ny), T(nz));
+        const T il = T(1) / T(len);
+        n = d * il;
+        const T k = T(p2.w) + T(0.5) * T(dist);
+        r2 = n * k;
+        r1 = r2 - d;
     }
-    // walls: planes (MaxContacts.h:777-790), then boxes (MaxContacts.h:589-668); the sphere is
-    // body 1 and the fixed wall has zero velocity
+    if (self1)
+        dem_contact<T>(n, T(dist), r1, r2, vi, wi, vj, wj, mi, mj, true, acc);
+    else
+        dem_contact<T>(n, T(dist), r1, r2, vj, wj, vi, wi, mj, mi, false, acc);
+}
+
+// walls of the sphere's scene: planes (MaxContacts.h:777-790), then boxes
+// (MaxContacts.h:589-668); the sphere is body 1 and the fixed wall has zero velocity
+template <typename T, typename VT>
+__device__ __forceinline__ void wall_forces(const DemArgs<VT> &a, const SceneInfo &s,
+                                            const double4 &pi, V3<T> vi, V3<T> wi,
+                                            const MatDev &mi, Acc<T> &acc) {
     const V3<T> zero = v3(T(0), T(0), T(0));
     for (int p = 0; p < s.nplanes; ++p) {
         const double4 pl = a.planes[s.plane_begin + p];
@@ -204,33 +193,33 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     }
     for (int k = 0; k < s.nboxes; ++k) {
         const double *B = a.boxes + 15 * (int64_t)(s.box_begin + k);
-        const double l[3] = {0.5 * B[3], 0.5 * B[4], 0.5 * B[5]};
+        const double l0 = 0.5 * B[3], l1 = 0.5 * B[4], l2 = 0.5 * B[5];
         const double *R = B + 6;
         const double dx = pi.x - B[0], dy = pi.y - B[1], dz = pi.z - B[2];
-        double p[3] = {dx * R[0] + dy * R[3] + dz * R[6], dx * R[1] + dy * R[4] + dz * R[7],
-                       dx * R[2] + dy * R[5] + dz * R[8]};
+        double p0 = dx * R[0] + dy * R[3] + dz * R[6];
+        double p1 = dx * R[1] + dy * R[4] + dz * R[7];
+        double p2 = dx * R[2] + dy * R[5] + dz * R[8];
         bool outside = false;
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            if (p[ax] < -l[ax]) { p[ax] = -l[ax]; outside = true; }
-            else if (p[ax] > l[ax]) { p[ax] = l[ax]; outside = true; }
-        }
+        if (p0 < -l0) { p0 = -l0; outside = true; } else if (p0 > l0) { p0 = l0; outside = true; }
+        if (p1 < -l1) { p1 = -l1; outside = true; } else if (p1 > l1) { p1 = l1; outside = true; }
+        if (p2 < -l2) { p2 = -l2; outside = true; } else if (p2 > l2) { p2 = l2; outside = true; }
         double nx, ny, nz, dist, gx, gy, gz;
         if (!outside) {
-            dist = fabs(p[0]) - l[0];
+            dist = fabs(p0) - l0;
             int face = 0;
-            for (int ax = 1; ax < 3; ++ax) {
-                const double tmp = fabs(p[ax]) - l[ax];
-                if (dist < tmp) { dist = tmp; face = ax; }
-            }
-            const double sg = (p[face] > 0.0) ? 1.0 : -1.0;
+            double pf = p0;
+            const double t1 = fabs(p1) - l1;
+            if (dist < t1) { dist = t1; face = 1; pf = p1; }
+            const double t2 = fabs(p2) - l2;
+            if (dist < t2) { dist = t2; face = 2; pf = p2; }
+            const double sg = (pf > 0.0) ? 1.0 : -1.0;
             nx = R[face] * sg; ny = R[3 + face] * sg; nz = R[6 + face] * sg;
             dist -= pi.w;
             gx = pi.x; gy = pi.y; gz = pi.z;
         } else {
-            const double qx = R[0] * p[0] + R[1] * p[1] + R[2] * p[2];
-            const double qy = R[3] * p[0] + R[4] * p[1] + R[5] * p[2];
-            const double qz = R[6] * p[0] + R[7] * p[1] + R[8] * p[2];
+            const double qx = R[0] * p0 + R[1] * p1 + R[2] * p2;
+            const double qy = R[3] * p0 + R[4] * p1 + R[5] * p2;
+            const double qz = R[6] * p0 + R[7] * p1 + R[8] * p2;
             const double mx = dx - qx, my = dy - qy, mz = dz - qz;
             const double len = length_rn(mx, my, mz);
             dist = len - pi.w;
@@ -244,15 +233,21 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
         const V3<T> r1 = v3(T(gx - pi.x), T(gy - pi.y), T(gz - pi.z));
         dem_contact<T>(n, T(dist), r1, zero, vi, wi, zero, zero, mi, mw, true, acc);
     }
+}
 
-    // SphereTrait::move, Default.h:166-216
+// SphereTrait::move, Default.h:166-216: returns the new position; writes v, w (and q)
+template <typename VT, bool TRACKQ>
+__device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, int64_t t,
+                                             const double4 &pi, V3<VT> vi, V3<VT> wi,
+                                             const MatDev &mi, const Acc<VT> &acc, V3<VT> &v) {
+    using T = VT;
     double im, ii, I;
     sphere_mass(pi.w, mi.density, im, ii, I);
     (void)I;
     const V3<T> gg = v3(T(a.g[0]), T(a.g[1]), T(a.g[2]));
     const V3<T> vdot = acc.F * T(im) + gg;
     const V3<T> wdot = T(ii) * acc.T_;
-    V3<T> v = vi + vdot * T(a.dt);
+    v = vi + vdot * T(a.dt);
     V3<T> w = wi + wdot * T(a.dt);
     const double nxp = pi.x + double(v.x) * a.dt;
     const double nyp = pi.y + double(v.y) * a.dt;
@@ -280,22 +275,115 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
         v = v * T(a.drag);
         w = w * T(a.drag);
     }
-    a.pr_out[t] = make_double4(nxp, nyp, nzp, pi.w);
+    const double4 out = make_double4(nxp, nyp, nzp, pi.w);
+    a.pr_out[t] = out;
     VT *o = a.vw_out + 6 * t;
     o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = w.x; o[4] = w.y; o[5] = w.z;
+    if (!isfinite(nxp) || !isfinite(nyp) || !isfinite(nzp)) atomicOr(a.err, DERR_NAN);
+    return out;
+}
+
+// all grid neighbours of body b (slot cells of the sphere's scene); the bound is conservative
+// for penetrating contacts
+template <typename T, typename VT>
+__device__ __forceinline__ void grid_forces(const DemArgs<VT> &a, const SceneInfo &s, int32_t b,
+                                            const double4 &pi, V3<T> vi, V3<T> wi, int32_t uidi,
+                                            const MatDev &mi, Acc<T> &acc) {
+    int cx, cy, cz;
+    cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= s.dim[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= s.dim[1]) continue;
+            const int64_t c0 = cell_key(s, x0, y, z);
+            const int64_t c1 = c0 + (x1 - x0) + 1;
+            const int e = a.cell_start[c1];
+            for (int slot = a.cell_start[c0]; slot < e; ++slot) {
+                const int32_t j = a.sorted ? a.sorted[slot] : slot;
+                if (j == b) continue;
+                const double4 pj = a.pr[j];
+                const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+                const double rs = pi.w + pj.w;
+                if (ddx * ddx + ddy * ddy + ddz * ddz >= rs * rs) continue;
+                pair_force<T, VT>(a, pi, vi, wi, uidi, mi, j, pj, acc);
+            }
+        }
+    }
+}
+
+template <typename VT, bool TRACKQ>
+__global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
+    using T = VT;  // arithmetic type of the contact law (double or float)
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int32_t b = a.sorted[t];
+    const double4 pi = a.pr[b];
+    const uint32_t tagi = a.tag[b];
+    const int32_t uidi = a.uid[b];
+    const SceneInfo &s = a.scenes[tagi >> 16];
+    const MatDev mi = a.mats[tagi & 0xffffu];
+    const V3<T> vi = ld_vw(a.vw, b, 0), wi = ld_vw(a.vw, b, 1);
+    Acc<T> acc;
+    acc.F = v3(T(0), T(0), T(0));
+    acc.T_ = acc.F;
+    grid_forces<T, VT>(a, s, b, pi, vi, wi, uidi, mi, acc);
+    wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
+    V3<T> v;
+    const double4 o = integrate<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v);
     a.tag_out[t] = tagi;
     a.uid_out[t] = uidi;
-    if (!isfinite(nxp) || !isfinite(nyp) || !isfinite(nzp)) atomicOr(a.err, DERR_NAN);
     // bin for the next step's counting sort
     int ncx, ncy, ncz;
-    cell_coords(s, nxp, nyp, nzp, ncx, ncy, ncz);
+    cell_coords(s, o.x, o.y, o.z, ncx, ncy, ncz);
     const int32_t kk = (int32_t)cell_key(s, ncx, ncy, ncz);
     a.key[t] = kk;
     a.rank[t] = atomicAdd(&a.cell_count[kk], 1);
 }
 
+// list step: body t stays at index t (the order changes only at rebuilds)
+template <typename VT, bool TRACKQ>
+__global__ void __launch_bounds__(kDemBlock) k_dem_list(DemArgs<VT> a) {
+    using T = VT;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool use_grid = a.nl_flags[1] != 0;   // this step's rebuild overflowed the lists
+    bool moved = false;
+    if (t < a.n) {
+        const double4 pi = a.pr[t];
+        const uint32_t tagi = a.tag[t];
+        const int32_t uidi = a.uid[t];
+        const SceneInfo &s = a.scenes[tagi >> 16];
+        const MatDev mi = a.mats[tagi & 0xffffu];
+        const V3<T> vi = ld_vw(a.vw, t, 0), wi = ld_vw(a.vw, t, 1);
+        Acc<T> acc;
+        acc.F = v3(T(0), T(0), T(0));
+        acc.T_ = acc.F;
+        if (!use_grid) {
+            const int e = a.nl_start[t + 1];
+            for (int k = a.nl_start[t]; k < e; ++k) {
+                const int32_t j = a.nl_idx[k];
+                pair_force<T, VT>(a, pi, vi, wi, uidi, mi, j, a.pr[j], acc);
+            }
+        } else {
+            grid_forces<T, VT>(a, s, (int32_t)t, pi, vi, wi, uidi, mi, acc);
+        }
+        wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
+        V3<T> v;
+        integrate<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v);
+        const float step = float(sqrt(double(v.x) * double(v.x) + double(v.y) * double(v.y) +
+                                      double(v.z) * double(v.z)) * a.dt);
+        const float d = a.disp[t] + step;
+        a.disp[t] = d;
+        moved = !(d < a.half_skin);   // also catches NaN
+    }
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(&a.nl_flags[0], 1);
+    if (use_grid && t == 0) atomicOr(&a.nl_flags[0], 1);
+}
+
 template <typename VT>
-int launch_dem(Ctx *c, double dt) {
+DemArgs<VT> dem_args(Ctx *c, double dt) {
     DemArgs<VT> a;
     a.n = c->n;
     a.dt = dt;
@@ -324,6 +412,17 @@ int launch_dem(Ctx *c, double dt) {
     a.rank = c->rank;
     a.cell_count = c->cell_count;
     a.err = c->d_err;
+    a.nl_start = c->nl.start;
+    a.nl_idx = c->nl.idx;
+    a.disp = c->nl.disp;
+    a.nl_flags = c->nl.flags;
+    a.half_skin = float(0.5 * c->nl.skin * (1.0 - 1e-5));
+    return a;
+}
+
+template <typename VT>
+int launch_dem(Ctx *c, double dt) {
+    DemArgs<VT> a = dem_args<VT>(c, dt);
     prof_begin(c, ST_DEM);
     if (c->p.track_orientation)
         k_dem_step<VT, true><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
@@ -333,6 +432,294 @@ int launch_dem(Ctx *c, double dt) {
     prof_end(c, ST_DEM);
     return PE_B200_OK;
 }
+
+// ---- list rebuild (every kernel returns at once unless a rebuild was requested) -------------
+__global__ void k_zero_c(int32_t *p, int64_t n, const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(i, n) p[i] = 0;
+}
+
+__global__ void k_bin_c(int64_t n, const double4 *pr, const uint32_t *tag,
+                        const SceneInfo *scenes, int32_t *key, int32_t *rank,
+                        int32_t *cell_count, const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(i, n) {
+        const double4 p = pr[i];
+        const SceneInfo &s = scenes[tag[i] >> 16];
+        int cx, cy, cz;
+        cell_coords(s, p.x, p.y, p.z, cx, cy, cz);
+        const int32_t k = (int32_t)cell_key(s, cx, cy, cz);
+        key[i] = k;
+        rank[i] = atomicAdd(&cell_count[k], 1);
+    }
+}
+
+__global__ void k_scatter_c(int64_t n, const int32_t *key, const int32_t *rank,
+                            const int32_t *start, int32_t *sorted, const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(i, n) sorted[start[key[i]] + rank[i]] = (int32_t)i;
+}
+
+__global__ void k_fixup_c(int64_t ncell, const int32_t *start, int32_t *sorted,
+                          const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(c, ncell) {
+        const int b = start[c], e = start[c + 1];
+        for (int i = b + 1; i < e; ++i) {
+            const int32_t v = sorted[i];
+            int j = i - 1;
+            while (j >= b && sorted[j] > v) {
+                sorted[j + 1] = sorted[j];
+                --j;
+            }
+            sorted[j + 1] = v;
+        }
+    }
+}
+
+// gather into cell order (tmp), resetting the path lengths
+template <typename VT>
+__global__ void k_permute_c(int64_t n, const int32_t *sorted, BodyBuf src, BodyBuf dst,
+                            float *disp, const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(t, n) {
+        const int32_t b = sorted[t];
+        dst.pr[t] = src.pr[b];
+        const VT *s6 = (const VT *)src.vw + 6 * (int64_t)b;
+        VT *d6 = (VT *)dst.vw + 6 * t;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) d6[k] = s6[k];
+        dst.tag[t] = src.tag[b];
+        dst.uid[t] = src.uid[b];
+        if (src.q) dst.q[t] = src.q[b];
+        disp[t] = 0.f;
+    }
+}
+
+template <typename VT>
+__global__ void k_copy_c(int64_t n, BodyBuf src, BodyBuf dst, const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(t, n) {
+        dst.pr[t] = src.pr[t];
+        const VT *s6 = (const VT *)src.vw + 6 * t;
+        VT *d6 = (VT *)dst.vw + 6 * t;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) d6[k] = s6[k];
+        dst.tag[t] = src.tag[t];
+        dst.uid[t] = src.uid[t];
+        if (src.q) dst.q[t] = src.q[t];
+    }
+}
+
+// neighbours of body t (state in cell order, so slot == index): pairs closer than
+// r_i + r_j + skin.  mode 0 counts, mode 1 writes.
+template <int MODE>
+__global__ void k_list(int64_t n, const double4 *pr, const uint32_t *tag,
+                       const SceneInfo *scenes, const int32_t *cell_start, double skin,
+                       int32_t *cnt, const int32_t *start, int64_t cap, int32_t *idx,
+                       const int32_t *cond) {
+    if (!*cond) return;
+    if (MODE == 1 && start[n] > cap) return;  // overflow: the force kernel searches the grid
+    GRID_STRIDE(t, n) {
+    const double4 pi = pr[t];
+    const SceneInfo &s = scenes[tag[t] >> 16];
+    int cx, cy, cz;
+    cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    int pos = (MODE == 1) ? start[t] : 0;
+    int count = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= s.dim[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= s.dim[1]) continue;
+            const int64_t c0 = cell_key(s, x0, y, z);
+            const int64_t c1 = c0 + (x1 - x0) + 1;
+            const int e = cell_start[c1];
+            for (int j = cell_start[c0]; j < e; ++j) {
+                if (j == t) continue;
+                const double4 pj = pr[j];
+                const double dx = pi.x - pj.x, dy2 = pi.y - pj.y, dz2 = pi.z - pj.z;
+                const double rc = pi.w + pj.w + skin;
+                if (dx * dx + dy2 * dy2 + dz2 * dz2 < rc * rc) {
+                    if (MODE == 1) idx[pos++] = j;
+                    ++count;
+                }
+            }
+        }
+    }
+    if (MODE == 0) cnt[t] = count;
+    }
+}
+
+__global__ void k_rebuild_done(int64_t n, const int32_t *start, int64_t cap, int32_t *flags) {
+    if (!flags[0]) return;
+    flags[0] = 0;
+    flags[1] = start[n] > cap ? 1 : 0;
+    flags[2] = start[n];
+    flags[3] += 1;
+}
+
+template <typename VT>
+int list_rebuild(Ctx *c) {
+    ListBuf &L = c->nl;
+    const int64_t n = c->n;
+    const int32_t *cond = L.flags;
+    prof_begin(c, ST_REBUILD);
+    k_zero_c<<<capped_grid(c, c->ncell + 1, 256), 256, 0, c->stream>>>(c->cell_count, c->ncell + 1, cond);
+    PEB_LAUNCHED(c);
+    k_bin_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+                                                     c->key, c->rank, c->cell_count, cond);
+    PEB_LAUNCHED(c);
+    int rc = scan_exclusive_cond(c, c->cell_count, c->cell_start, c->ncell, cond);
+    if (rc) return rc;
+    k_scatter_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->key, c->rank, c->cell_start,
+                                                         c->sorted, cond);
+    PEB_LAUNCHED(c);
+    k_fixup_c<<<capped_grid(c, c->ncell, 256), 256, 0, c->stream>>>(c->ncell, c->cell_start, c->sorted,
+                                                             cond);
+    PEB_LAUNCHED(c);
+    k_permute_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->sorted, c->cur, L.tmp, L.disp,
+                                                             cond);
+    PEB_LAUNCHED(c);
+    k_copy_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.tmp, c->cur, cond);
+    PEB_LAUNCHED(c);
+    k_list<0><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+                                                       c->cell_start, L.skin, L.cnt, nullptr, 0,
+                                                       nullptr, cond);
+    PEB_LAUNCHED(c);
+    rc = scan_exclusive_cond(c, L.cnt, L.start, n, cond);
+    if (rc) return rc;
+    k_list<1><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+                                                       c->cell_start, L.skin, nullptr, L.start,
+                                                       L.cap, L.idx, cond);
+    PEB_LAUNCHED(c);
+    k_rebuild_done<<<1, 1, 0, c->stream>>>(n, L.start, L.cap, L.flags);
+    PEB_LAUNCHED(c);
+    prof_end(c, ST_REBUILD);
+    return PE_B200_OK;
+}
+
+__global__ void k_cond_set(cudaGraphConditionalHandle h, const int32_t *flags) {
+    cudaGraphSetConditional(h, flags[0] ? 1u : 0u);
+}
+
+void drop_graph(ListBuf &L, int k) {
+    if (L.gexec[k]) cudaGraphExecDestroy(L.gexec[k]);
+    if (L.graph[k]) cudaGraphDestroy(L.graph[k]);
+    L.gexec[k] = nullptr;
+    L.graph[k] = nullptr;
+    L.graph_pr[k] = nullptr;
+}
+
+// Captures the rebuild for the current position buffer into slot k: a kernel copies the
+// device-side request into the graph's condition, and the rebuild kernels form the body of an
+// IF node, so a step without a rebuild costs one tiny kernel.  Returns false on any failure
+// (the caller then launches the rebuild kernels directly, which return at once unless needed).
+template <typename VT>
+bool build_rebuild_graph(Ctx *c, int k) {
+    ListBuf &L = c->nl;
+    drop_graph(L, k);
+    if (scan_reserve(c, std::max<int64_t>(c->ncell, c->n)) != PE_B200_OK) return false;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h{};
+    ok = ok && cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t set_node = nullptr, cond_node = nullptr;
+    if (ok) {
+        cudaKernelNodeParams kp = {};
+        void *args[] = {&h, &L.flags};
+        kp.func = (void *)k_cond_set;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(1);
+        kp.kernelParams = args;
+        ok = cudaGraphAddKernelNode(&set_node, g, nullptr, 0, &kp) == cudaSuccess;
+    }
+    cudaGraph_t body = nullptr;
+    if (ok) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&cond_node, g, &set_node, 1, &cp) == cudaSuccess;
+        if (ok) body = cp.conditional.phGraph_out[0];
+    }
+    if (ok) {
+        const bool prof = c->prof;
+        const int64_t launches = c->launches;
+        c->prof = false;  // event records are not allowed in a conditional body
+        ok = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeRelaxed) == cudaSuccess;
+        if (ok) {
+            const int rc = list_rebuild<VT>(c);
+            cudaGraph_t out = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &out);
+            ok = rc == PE_B200_OK && e == cudaSuccess;
+        }
+        c->prof = prof;
+        c->launches = launches;
+    }
+    if (ok) ok = cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
+    if (!ok) {
+        if (ge) cudaGraphExecDestroy(ge);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();  // clear the sticky-free error of the failed graph call
+        return false;
+    }
+    L.graph[k] = g;
+    L.gexec[k] = ge;
+    L.graph_pr[k] = c->cur.pr;
+    L.graph_cap = L.cap;
+    return true;
+}
+
+template <typename VT>
+int list_step(Ctx *c, double dt) {
+    ListBuf &L = c->nl;
+    if (L.graph_cap != L.cap) {
+        drop_graph(L, 0);
+        drop_graph(L, 1);
+        L.graph_cap = L.cap;
+    }
+    int slot = -1;
+    if (!L.graph_disabled) {
+        for (int k = 0; k < 2; ++k)
+            if (L.gexec[k] && L.graph_pr[k] == c->cur.pr) slot = k;
+        if (slot < 0) {
+            const int k = L.gexec[0] ? 1 : 0;
+            if (build_rebuild_graph<VT>(c, k)) slot = k;
+            else L.graph_disabled = true;
+        }
+    }
+    if (slot >= 0) {
+        prof_begin(c, ST_REBUILD);
+        PEB_CUDA(c, cudaGraphLaunch(L.gexec[slot], c->stream));
+        c->launches += 1;
+        prof_end(c, ST_REBUILD);
+    } else {
+        int rc = list_rebuild<VT>(c);
+        if (rc) return rc;
+    }
+    DemArgs<VT> a = dem_args<VT>(c, dt);
+    a.sorted = nullptr;   // the grid fallback sees the state in cell order
+    prof_begin(c, ST_DEM);
+    if (c->p.track_orientation)
+        k_dem_list<VT, true><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
+    else
+        k_dem_list<VT, false><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
+    PEB_LAUNCHED(c);
+    prof_end(c, ST_DEM);
+    // positions/velocities/orientations double-buffered; tag and uid stay where they are
+    std::swap(c->cur.pr, c->nxt.pr);
+    std::swap(c->cur.vw, c->nxt.vw);
+    std::swap(c->cur.q, c->nxt.q);
+    return PE_B200_OK;
+}
+
+__global__ void k_set_one(int32_t *p) { *p = 1; }
 
 }  // namespace
 
@@ -347,6 +734,87 @@ int dem_step(Ctx *c, double dt) {
         rc = (c->p.precision == PE_B200_FP64) ? launch_dem<double>(c, dt) : launch_dem<float>(c, dt);
         if (rc) return rc;
         std::swap(c->cur, c->nxt);
+    }
+    return PE_B200_OK;
+}
+
+// ---- list mode: buffers, rebuild requests, the capacity check ------------------------------
+int dem_list_alloc(Ctx *c) {
+    ListBuf &L = c->nl;
+    const size_t n = (size_t)std::max<int64_t>(c->n, 1);
+    L.cap = std::max<int64_t>(16 * c->n, 1024);
+    PEB_CUDA(c, cudaMalloc(&L.start, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.cnt, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.idx, (size_t)L.cap * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.disp, n * sizeof(float)));
+    PEB_CUDA(c, cudaMalloc(&L.flags, 8 * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemset(L.flags, 0, 8 * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemset(L.disp, 0, n * sizeof(float)));
+    if (!L.h_flags) PEB_CUDA(c, cudaMallocHost(&L.h_flags, 8 * sizeof(int32_t)));
+    if (!L.ev) PEB_CUDA(c, cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming));
+    PEB_CUDA(c, cudaMalloc(&L.tmp.pr, n * sizeof(double4)));
+    PEB_CUDA(c, cudaMalloc(&L.tmp.vw, n * (size_t)c->vw_bytes));
+    PEB_CUDA(c, cudaMalloc(&L.tmp.tag, n * sizeof(uint32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.tmp.uid, n * sizeof(int32_t)));
+    if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&L.tmp.q, n * sizeof(double4)));
+    L.enabled = true;
+    L.check_pending = false;
+    return dem_list_request_rebuild(c);
+}
+
+void dem_list_free(Ctx *c) {
+    ListBuf &L = c->nl;
+    if (L.check_pending && L.ev) cudaEventSynchronize(L.ev);
+    drop_graph(L, 0);
+    drop_graph(L, 1);
+    cudaFree(L.start);
+    cudaFree(L.cnt);
+    cudaFree(L.idx);
+    cudaFree(L.disp);
+    cudaFree(L.flags);
+    cudaFree(L.tmp.pr);
+    cudaFree(L.tmp.vw);
+    cudaFree(L.tmp.tag);
+    cudaFree(L.tmp.uid);
+    cudaFree(L.tmp.q);
+    if (L.h_flags) cudaFreeHost(L.h_flags);
+    if (L.ev) cudaEventDestroy(L.ev);
+    const double skin = L.skin;
+    L = ListBuf();
+    L.skin = skin;
+}
+
+int dem_list_request_rebuild(Ctx *c) {
+    k_set_one<<<1, 1, 0, c->stream>>>(c->nl.flags);
+    PEB_LAUNCHED(c);
+    return PE_B200_OK;
+}
+
+int dem_list_step(Ctx *c, double dt) {
+    ListBuf &L = c->nl;
+    if (c->n == 0) return PE_B200_OK;
+    // capacity check of an earlier step, without waiting for the device
+    if (L.check_pending && cudaEventQuery(L.ev) == cudaSuccess) {
+        L.check_pending = false;
+        if (L.h_flags[1]) {
+            PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+            const int64_t need = std::max<int64_t>(L.h_flags[2], 0);
+            const int64_t cap = std::max<int64_t>(2 * L.cap, need + need / 4 + 1024);
+            cudaFree(L.idx);
+            L.idx = nullptr;
+            PEB_CUDA(c, cudaMalloc(&L.idx, (size_t)cap * sizeof(int32_t)));
+            L.cap = cap;
+            int rc = dem_list_request_rebuild(c);
+            if (rc) return rc;
+        }
+    }
+    int rc = (c->p.precision == PE_B200_FP64) ? list_step<double>(c, dt) : list_step<float>(c, dt);
+    if (rc) return rc;
+    if (!L.check_pending) {
+        PEB_CUDA(c, cudaMemcpyAsync(L.h_flags, L.flags, 4 * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaEventRecord(L.ev, c->stream));
+        L.check_pending = true;
     }
     return PE_B200_OK;
 }
@@ -382,6 +850,11 @@ cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream) {
     a.rank = r.rank;
     a.cell_count = r.cell_count;
     a.err = r.err;
+    a.nl_start = nullptr;
+    a.nl_idx = nullptr;
+    a.disp = nullptr;
+    a.nl_flags = nullptr;
+    a.half_skin = 0.f;
     if (r.n > 0)
         k_dem_step<double, false><<<grid_for(r.n, kDemBlock), kDemBlock, 0, stream>>>(a);
     return cudaGetLastError();

@@ -31,7 +31,9 @@ __device__ __forceinline__ int warp_incl_scan(int v) {
 // exclusive scan of one tile; block total to tile_sums[blockIdx.x]
 __global__ void __launch_bounds__(kScanThreads) k_scan_tile(const int32_t *__restrict__ in,
                                                             int32_t *__restrict__ out, int64_t n,
-                                                            int32_t *__restrict__ tile_sums) {
+                                                            int32_t *__restrict__ tile_sums,
+                                                            const int32_t *cond) {
+    if (cond && !*cond) return;
     __shared__ int warp_tot[kScanThreads / 32];
     const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
     int v[kScanItems];
@@ -63,13 +65,16 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile(const int32_t *__res
 }
 
 __global__ void k_scan_add(int32_t *__restrict__ out, int64_t n,
-                           const int32_t *__restrict__ tile_off) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] += tile_off[i / kScanTile];
+                           const int32_t *__restrict__ tile_off, const int32_t *cond) {
+    if (cond && !*cond) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] += tile_off[i / kScanTile];
 }
 
 __global__ void k_set_total(int32_t *out, int64_t n, const int32_t *last_in,
-                            const int32_t *last_out) {
+                            const int32_t *last_out, const int32_t *cond) {
+    if (cond && !*cond) return;
     out[n] = (n > 0) ? (*last_out + *last_in) : 0;
 }
 
@@ -115,7 +120,30 @@ __global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
 
 }  // namespace
 
+// sizes the scan scratch for inputs of up to n elements (so a later scan allocates nothing)
+int scan_reserve(Ctx *c, int64_t n) {
+    int64_t m = n, need = 0;
+    while (true) {
+        const int64_t tiles = (m + kScanTile - 1) / kScanTile;
+        need += tiles + 1;
+        if (tiles <= 1) break;
+        m = tiles;
+    }
+    if (need + 1 > c->scan_tmp_cap) {
+        if (c->scan_tmp) cudaFree(c->scan_tmp);
+        c->scan_tmp = nullptr;
+        PEB_CUDA(c, cudaMalloc(&c->scan_tmp, (size_t)(need + 1) * sizeof(int32_t)));
+        c->scan_tmp_cap = need + 1;
+    }
+    return PE_B200_OK;
+}
+
 int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n) {
+    return scan_exclusive_cond(c, in, out, n, nullptr);
+}
+
+// cond (device int, may be null): when it holds 0 every kernel of the scan returns at once
+int scan_exclusive_cond(Ctx *c, const int32_t *in, int32_t *out, int64_t n, const int32_t *cond) {
     // recursive reduce-then-scan; scratch holds every level's tile sums
     std::vector<int64_t> sizes;
     int64_t m = n;
@@ -149,7 +177,8 @@ int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n) {
         int32_t *sums = tmp;
         tmp += tiles + 1;
         if (len > 0) {
-            k_scan_tile<<<(unsigned)tiles, kScanThreads, 0, c->stream>>>(cur_in, cur_out, len, sums);
+            k_scan_tile<<<(unsigned)tiles, kScanThreads, 0, c->stream>>>(cur_in, cur_out, len, sums,
+                                                                          cond);
             PEB_LAUNCHED(c);
         }
         lvl_out.push_back(cur_out);
@@ -161,10 +190,10 @@ int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n) {
     // propagate offsets downwards
     for (int l = (int)lvl_out.size() - 2; l >= 0; --l) {
         const int64_t len = sizes[l];
-        k_scan_add<<<grid_for(len, 256), 256, 0, c->stream>>>(lvl_out[l], len, lvl_sums[l]);
+        k_scan_add<<<capped_grid(c, len, 256), 256, 0, c->stream>>>(lvl_out[l], len, lvl_sums[l], cond);
         PEB_LAUNCHED(c);
     }
-    k_set_total<<<1, 1, 0, c->stream>>>(out, n, last_in, out + (n > 0 ? n - 1 : 0));
+    k_set_total<<<1, 1, 0, c->stream>>>(out, n, last_in, out + (n > 0 ? n - 1 : 0), cond);
     PEB_LAUNCHED(c);
     return PE_B200_OK;
 }

@@ -71,11 +71,36 @@ struct NbgsBuf {
     int64_t red_cap = 0;
 };
 
+// Verlet neighbour lists of the DEM step (dem_list.cu): every pair closer than r_i + r_j + skin
+// at the last rebuild; valid while no sphere has moved more than skin/2 since then
+struct ListBuf {
+    bool enabled = false;
+    double skin = 0.0;
+    int64_t cap = 0;
+    int32_t *start = nullptr;   // n + 1 (CSR offsets)
+    int32_t *cnt = nullptr;     // n + 1
+    int32_t *idx = nullptr;     // cap
+    float *disp = nullptr;      // path length since the last rebuild
+    int32_t *flags = nullptr;   // [0] rebuild requested, [1] list overflowed at this rebuild,
+                                // [2] entries needed, [3] rebuild count
+    int32_t *h_flags = nullptr; // pinned mirror
+    cudaEvent_t ev = nullptr;
+    bool check_pending = false;
+    BodyBuf tmp;                // permutation target of a rebuild
+    // the rebuild as a CUDA graph whose body runs only when requested (a conditional node), one
+    // graph per position buffer; rebuilt when capacities change
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    const void *graph_pr[2] = {nullptr, nullptr};
+    int64_t graph_cap = -1;
+    bool graph_disabled = false;
+};
+
 // stage timers (pe's profiling sections, e.g. DEMSolver.h:1159-1260): CUDA events around each
 // stage on the context's stream, summed when queried
 enum Stage : int {
     ST_SORT = 0, ST_DEM, ST_PERMUTE, ST_DETECT, ST_COLOR, ST_CACHE, ST_SWEEP, ST_INTEGRATE,
-    ST_COUNT
+    ST_REBUILD, ST_COUNT
 };
 extern const char *kStageNames[ST_COUNT];
 
@@ -123,6 +148,7 @@ struct Ctx {
     int64_t vw_bytes = 0;
 
     NbgsBuf nb;
+    ListBuf nl;
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -165,11 +191,19 @@ inline unsigned grid_for(int64_t n, int block) {
     return (unsigned)((n + block - 1) / block);
 }
 
+// grid-stride launches: at most 8 blocks per SM
+unsigned capped_grid(const Ctx *c, int64_t n, int block);
+#define GRID_STRIDE(i, n)                                                              \
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n);         \
+         i += (int64_t)gridDim.x * blockDim.x)
+
 // grid build: (re)bins bodies and sorts them by cell (grid.cu)
 int grid_alloc(Ctx *c);
 int grid_bin_current(Ctx *c);
 int grid_sort(Ctx *c);
 int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n);  // out[n] = total
+int scan_exclusive_cond(Ctx *c, const int32_t *in, int32_t *out, int64_t n, const int32_t *cond);
+int scan_reserve(Ctx *c, int64_t n);
 
 // FP64 DEM step kernel on raw device buffers (layout as above; single launch, no allocation)
 struct DemRawArgs {
@@ -196,6 +230,10 @@ struct DemRawArgs {
 cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream);
 
 // solvers
+int dem_list_alloc(Ctx *c);
+void dem_list_free(Ctx *c);
+int dem_list_request_rebuild(Ctx *c);
+int dem_list_step(Ctx *c, double dt);
 int dem_step(Ctx *c, double dt);
 int nbgs_step(Ctx *c, double dt);
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out);

@@ -23,7 +23,7 @@ class Engine:
                  relaxation_model: int = _abi.APPROX_INELASTIC_COULOMB_DECOUPLING,
                  max_iterations: int = 100, erp: float = 0.7, gravity=(0.0, 0.0, 0.0),
                  damping: float = 1.0, device: int = 0, track_orientation: bool = False,
-                 max_contacts: int = 0):
+                 max_contacts: int = 0, neighbor_lists: bool = True, skin: float = 0.0):
         self._L = _abi.load()
         p = _abi.default_params()
         p.solver, p.precision = solver, precision
@@ -33,6 +33,8 @@ class Engine:
         p.damping, p.device = damping, device
         p.track_orientation = 1 if track_orientation else 0
         p.max_contacts = max_contacts
+        p.neighbor_lists = 1 if neighbor_lists else 0
+        p.skin = float(skin)
         h = C.c_void_p()
         self._check(self._L.pe_b200_create(C.byref(p), C.byref(h)), ctx=None)
         self._h = h

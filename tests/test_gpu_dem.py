@@ -140,3 +140,33 @@ def test_nan_state_is_reported():
     with pytest.raises(PeB200Error) as ei:
         e.download()
     assert ei.value.code == _abi.ERR_NAN
+
+
+@pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
+def test_neighbor_lists_match_grid_search(precision):
+    """Verlet lists (rebuilt whenever a sphere has moved skin/2) give the grid search's forces;
+    a tiny skin forces a rebuild nearly every step, a large one almost never."""
+    s = scenes.small_random(9, n=3000, overlap=0.03, with_boxes=True)
+    g = Engine(solver=_abi.DEM, precision=precision, neighbor_lists=False).load_scene(s)
+    g.step(s.dt, 60)
+    xg, vg, wg = g.download()
+    for skin in (1e-4, 0.05, 0.5):
+        e = Engine(solver=_abi.DEM, precision=precision, neighbor_lists=True, skin=skin)
+        e.load_scene(s)
+        for _ in range(3):
+            e.step(s.dt, 20)
+        x, v, w = e.download()
+        tol = 1e-12 if precision == _abi.FP64 else 1e-5
+        assert rel_err(x, xg) < tol
+        assert rel_err(v, vg) < (tol if precision == _abi.FP64 else 1e-3)
+
+
+def test_neighbor_lists_vs_oracle_long_run():
+    s = scenes.dem_lattice(1, side=10)
+    o = OracleWorld(s)
+    o.dem_step(s.dt, 300)
+    e = engine_for(s)
+    e.step(s.dt, 300)
+    x, v, w = e.download()
+    assert rel_err(x, o.x) < 1e-12
+    assert rel_err(v, o.v) < 1e-9
