@@ -156,6 +156,12 @@ int pe_b200_last_step_stats(pe_b200_ctx *ctx, int64_t *ncontacts, int32_t *ncolo
                             double *delta_max, double *residual);
 int pe_b200_set_residual(pe_b200_ctx *ctx, int32_t enabled);
 
+/* DEM neighbour-list state: rebuilds so far, entries at the last rebuild, capacity, skin
+ * (waits for the context's stream).  pe has no neighbour lists: its hash grids re-bin every
+ * body every step (HashGrids.h:1121-1258); this reports the device-side replacement. */
+int pe_b200_neighbor_list_stats(pe_b200_ctx *ctx, int64_t *rebuilds, int64_t *entries,
+                                int64_t *capacity, double *skin);
+
 /* Stage timers (CUDA events on the context's stream around each stage; off by default).
  * Replaces: pe's profiling sections and logProfilingSummary (pe/config/ProfilingMode.h:40,
  * pe/core/collisionsystem/DEMSolver.h:698-960).  Enabling resets the totals. */

@@ -48,15 +48,18 @@ def up_to_date() -> bool:
     return os.path.getmtime(LIB) >= _newest(sources() + headers() + [__file__])
 
 
-def build(force: bool = False, verbose: bool = False, extra_flags=()) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, extra_flags=(), out: str = None,
+          build_dir: str = None) -> str:
+    lib = out or LIB
+    bdir = build_dir or BUILD
+    if out is None and not force and up_to_date():
         return LIB
-    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(bdir, exist_ok=True)
     cc = nvcc()
     objs = []
 
     def compile_one(src):
-        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
         cmd = [cc, *ARCH, *NVCC_FLAGS, *extra_flags, "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
@@ -67,13 +70,13 @@ def build(force: bool = False, verbose: bool = False, extra_flags=()) -> str:
 
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, sources()))
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -510,11 +510,11 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
         uid[i] = (int32_t)i;
         for (int a = 0; a < 3; ++a) {
             if (f64) {
-                ((double *)vw.data())[6 * i + a] = v[3 * i + a];
-                ((double *)vw.data())[6 * i + 3 + a] = w[3 * i + a];
+                ((double *)vw.data())[a * n + i] = v[3 * i + a];
+                ((double *)vw.data())[(3 + a) * n + i] = w[3 * i + a];
             } else {
-                ((float *)vw.data())[6 * i + a] = (float)v[3 * i + a];
-                ((float *)vw.data())[6 * i + 3 + a] = (float)w[3 * i + a];
+                ((float *)vw.data())[a * n + i] = (float)v[3 * i + a];
+                ((float *)vw.data())[(3 + a) * n + i] = (float)w[3 * i + a];
             }
         }
     }
@@ -562,11 +562,11 @@ int pe_b200_set_state(pe_b200_ctx *h, const double *x, const double *v, const do
         for (int a = 0; a < 3; ++a) {
             if (x) pr[4 * k + a] = x[3 * i + a];
             if (f64) {
-                if (v) ((double *)vw.data())[6 * k + a] = v[3 * i + a];
-                if (w) ((double *)vw.data())[6 * k + 3 + a] = w[3 * i + a];
+                if (v) ((double *)vw.data())[a * n + k] = v[3 * i + a];
+                if (w) ((double *)vw.data())[(3 + a) * n + k] = w[3 * i + a];
             } else {
-                if (v) ((float *)vw.data())[6 * k + a] = (float)v[3 * i + a];
-                if (w) ((float *)vw.data())[6 * k + 3 + a] = (float)w[3 * i + a];
+                if (v) ((float *)vw.data())[a * n + k] = (float)v[3 * i + a];
+                if (w) ((float *)vw.data())[(3 + a) * n + k] = (float)w[3 * i + a];
             }
         }
     }
@@ -635,11 +635,11 @@ int pe_b200_download_bodies(pe_b200_ctx *h, double *x, double *v, double *w, dou
         for (int a = 0; a < 3; ++a) {
             if (x) x[3 * i + a] = pr[4 * k + a];
             if (f64) {
-                if (v) v[3 * i + a] = ((double *)vw.data())[6 * k + a];
-                if (w) w[3 * i + a] = ((double *)vw.data())[6 * k + 3 + a];
+                if (v) v[3 * i + a] = ((double *)vw.data())[a * n + k];
+                if (w) w[3 * i + a] = ((double *)vw.data())[(3 + a) * n + k];
             } else {
-                if (v) v[3 * i + a] = ((float *)vw.data())[6 * k + a];
-                if (w) w[3 * i + a] = ((float *)vw.data())[6 * k + 3 + a];
+                if (v) v[3 * i + a] = ((float *)vw.data())[a * n + k];
+                if (w) w[3 * i + a] = ((float *)vw.data())[(3 + a) * n + k];
             }
         }
         if (q)
@@ -665,6 +665,23 @@ int pe_b200_last_step_stats(pe_b200_ctx *h, int64_t *ncontacts, int32_t *ncolors
     if (ncolors) *ncolors = c->last_ncolors;
     if (delta_max) *delta_max = c->last_delta;
     if (residual) *residual = c->last_residual;
+    return PE_B200_OK;
+}
+
+int pe_b200_neighbor_list_stats(pe_b200_ctx *h, int64_t *rebuilds, int64_t *entries,
+                                int64_t *capacity, double *skin) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    int32_t f[4] = {0, 0, 0, 0};
+    if (c->nl.enabled) {
+        cudaSetDevice(c->device);
+        PEB_CUDA(c, cudaMemcpyAsync(f, c->nl.flags, sizeof f, cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    if (rebuilds) *rebuilds = f[3];
+    if (entries) *entries = f[2];
+    if (capacity) *capacity = c->nl.cap;
+    if (skin) *skin = c->nl.skin;
     return PE_B200_OK;
 }
 

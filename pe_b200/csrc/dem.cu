@@ -37,7 +37,13 @@ namespace peb {
 
 namespace {
 
-constexpr int kDemBlock = 128;
+#ifndef PEB_DEM_BLOCK
+#define PEB_DEM_BLOCK 128
+#endif
+#ifndef PEB_LIST_MIN_BLOCKS_F32
+#define PEB_LIST_MIN_BLOCKS_F32 7
+#endif
+constexpr int kDemBlock = PEB_DEM_BLOCK;
 
 template <typename T>
 struct Acc {
@@ -125,14 +131,12 @@ struct DemArgs {
     float half_skin;
 };
 
-// one sphere pair (body b and neighbour j), both in the buffers of `a`
+// one sphere pair (this body and neighbour j), both in the buffers of `a`; self1: this body is
+// pe's body 1, i.e. has the smaller system id (MaxContacts.h:550-551)
 template <typename T, typename VT>
-__device__ __forceinline__ void pair_force(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
-                                           V3<T> wi, int32_t uidi, const MatDev &mi,
-                                           int32_t j, const double4 &pj, Acc<T> &acc) {
-    const int32_t uidj = a.uid[j];
-    const bool self1 = uidi < uidj;
-    // pe orientation: body 1 = smaller system id (MaxContacts.h:550-551)
+__device__ __forceinline__ void pair_force_o(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
+                                             V3<T> wi, const MatDev &mi, int32_t j,
+                                             const double4 &pj, bool self1, Acc<T> &acc) {
     const double4 p1 = self1 ? pi : pj;
     const double4 p2 = self1 ? pj : pi;
     const double nx = p1.x - p2.x, ny = p1.y - p2.y, nz = p1.z - p2.z;
@@ -140,8 +144,8 @@ __device__ __forceinline__ void pair_force(const DemArgs<VT> &a, const double4 &
     const double dist = __dsub_rn(__dsub_rn(len, p1.w), p2.w);
     // only penetrating contacts produce a force (ContactBase.h:307-310)
     if (!(dist < -kContactThreshold)) return;
-    const MatDev mj = a.mats[a.tag[j] & 0xffffu];
-    const V3<T> vj = ld_vw(a.vw, j, 0), wj = ld_vw(a.vw, j, 1);
+    const MatDev &mj = a.mats[a.tag[j] & 0xffffu];
+    const V3<T> vj = ld_vw(a.vw, a.n, j, 0), wj = ld_vw(a.vw, a.n, j, 1);
     V3<T> n, r1, r2;
     if (sizeof(T) == 8) {
         // FP64: the contact point in absolute coordinates, as pe computes it
@@ -167,6 +171,13 @@ __device__ __forceinline__ void pair_force(const DemArgs<VT> &a, const double4 &
         dem_contact<T>(n, T(dist), r1, r2, vj, wj, vi, wi, mj, mi, false, acc);
 }
 
+template <typename T, typename VT>
+__device__ __forceinline__ void pair_force(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
+                                           V3<T> wi, int32_t uidi, const MatDev &mi,
+                                           int32_t j, const double4 &pj, Acc<T> &acc) {
+    pair_force_o<T, VT>(a, pi, vi, wi, mi, j, pj, uidi < a.uid[j], acc);
+}
+
 // walls of the sphere's scene: planes (MaxContacts.h:777-790), then boxes
 // (MaxContacts.h:589-668); the sphere is body 1 and the fixed wall has zero velocity
 template <typename T, typename VT>
@@ -174,12 +185,17 @@ __device__ __forceinline__ void wall_forces(const DemArgs<VT> &a, const SceneInf
                                             const double4 &pi, V3<T> vi, V3<T> wi,
                                             const MatDev &mi, Acc<T> &acc) {
     const V3<T> zero = v3(T(0), T(0), T(0));
+    const float pxf = float(pi.x), pyf = float(pi.y), pzf = float(pi.z), prf = float(pi.w);
     for (int p = 0; p < s.nplanes; ++p) {
         const double4 pl = a.planes[s.plane_begin + p];
+        // FP32 estimate first: spheres clearly off the plane skip the exact FP64 test (the
+        // estimate's error is far below the 1e-3 margin for coordinates up to ~1e4)
+        const float est = float(pl.x) * pxf + float(pl.y) * pyf + float(pl.z) * pzf - prf - float(pl.w);
+        if (est > 1e-3f * (1.0f + fabsf(float(pl.w)) + fabsf(pxf) + fabsf(pyf) + fabsf(pzf))) continue;
         const double kk = dot_rn(pl.x, pl.y, pl.z, pi.x, pi.y, pi.z);
         const double dist = __dsub_rn(__dsub_rn(kk, pi.w), pl.w);
         if (!(dist < -kContactThreshold)) continue;
-        const MatDev mw = a.mats[a.plane_mat[s.plane_begin + p]];
+        const MatDev &mw = a.mats[a.plane_mat[s.plane_begin + p]];
         const V3<T> n = v3(T(pl.x), T(pl.y), T(pl.z));
         V3<T> r1;
         if (sizeof(T) == 8) {
@@ -228,27 +244,38 @@ __device__ __forceinline__ void wall_forces(const DemArgs<VT> &a, const SceneInf
             gx = B[0] + qx; gy = B[1] + qy; gz = B[2] + qz;
         }
         if (!(dist < -kContactThreshold)) continue;
-        const MatDev mw = a.mats[a.box_mat[s.box_begin + k]];
+        const MatDev &mw = a.mats[a.box_mat[s.box_begin + k]];
         const V3<T> n = v3(T(nx), T(ny), T(nz));
         const V3<T> r1 = v3(T(gx - pi.x), T(gy - pi.y), T(gz - pi.z));
         dem_contact<T>(n, T(dist), r1, zero, vi, wi, zero, zero, mi, mw, true, acc);
     }
 }
 
-// SphereTrait::move, Default.h:166-216: returns the new position; writes v, w (and q)
+// SphereTrait::move, Default.h:166-216: new position (radius kept), v and w; writes q
 template <typename VT, bool TRACKQ>
-__device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, int64_t t,
-                                             const double4 &pi, V3<VT> vi, V3<VT> wi,
-                                             const MatDev &mi, const Acc<VT> &acc, V3<VT> &v) {
+__device__ __forceinline__ double4 integrate_core(const DemArgs<VT> &a, int64_t b, int64_t t,
+                                                  const double4 &pi, V3<VT> vi, V3<VT> wi,
+                                                  const MatDev &mi, const Acc<VT> &acc,
+                                                  V3<VT> &v, V3<VT> &w) {
     using T = VT;
-    double im, ii, I;
-    sphere_mass(pi.w, mi.density, im, ii, I);
-    (void)I;
+    T im, ii;
+    if (sizeof(T) == 8) {
+        double dim, dii, I;
+        sphere_mass(pi.w, mi.density, dim, dii, I);
+        im = T(dim);
+        ii = T(dii);
+    } else {
+        // mixed precision: the same formulas in FP32 (SphereBase.h:169-171, 230-234)
+        const float r = float(pi.w);
+        const float m = 4.0f / 3.0f * 3.14159265f * r * r * r * float(mi.density);
+        im = T(1.0f / m);
+        ii = T(1.0f / (0.4f * m * r * r));
+    }
     const V3<T> gg = v3(T(a.g[0]), T(a.g[1]), T(a.g[2]));
     const V3<T> vdot = acc.F * T(im) + gg;
     const V3<T> wdot = T(ii) * acc.T_;
     v = vi + vdot * T(a.dt);
-    V3<T> w = wi + wdot * T(a.dt);
+    w = wi + wdot * T(a.dt);
     const double nxp = pi.x + double(v.x) * a.dt;
     const double nyp = pi.y + double(v.y) * a.dt;
     const double nzp = pi.z + double(v.z) * a.dt;
@@ -275,11 +302,18 @@ __device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, in
         v = v * T(a.drag);
         w = w * T(a.drag);
     }
-    const double4 out = make_double4(nxp, nyp, nzp, pi.w);
-    a.pr_out[t] = out;
-    VT *o = a.vw_out + 6 * t;
-    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = w.x; o[4] = w.y; o[5] = w.z;
     if (!isfinite(nxp) || !isfinite(nyp) || !isfinite(nzp)) atomicOr(a.err, DERR_NAN);
+    return make_double4(nxp, nyp, nzp, pi.w);
+}
+
+template <typename VT, bool TRACKQ>
+__device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, int64_t t,
+                                             const double4 &pi, V3<VT> vi, V3<VT> wi,
+                                             const MatDev &mi, const Acc<VT> &acc, V3<VT> &v) {
+    V3<VT> w;
+    const double4 out = integrate_core<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v, w);
+    a.pr_out[t] = out;
+    st_vw(a.vw_out, a.n, t, v, w);
     return out;
 }
 
@@ -324,8 +358,8 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     const uint32_t tagi = a.tag[b];
     const int32_t uidi = a.uid[b];
     const SceneInfo &s = a.scenes[tagi >> 16];
-    const MatDev mi = a.mats[tagi & 0xffffu];
-    const V3<T> vi = ld_vw(a.vw, b, 0), wi = ld_vw(a.vw, b, 1);
+    const MatDev &mi = a.mats[tagi & 0xffffu];
+    const V3<T> vi = ld_vw(a.vw, a.n, b, 0), wi = ld_vw(a.vw, a.n, b, 1);
     Acc<T> acc;
     acc.F = v3(T(0), T(0), T(0));
     acc.T_ = acc.F;
@@ -345,7 +379,7 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
 
 // list step: body t stays at index t (the order changes only at rebuilds)
 template <typename VT, bool TRACKQ>
-__global__ void __launch_bounds__(kDemBlock) k_dem_list(DemArgs<VT> a) {
+__global__ void __launch_bounds__(kDemBlock, sizeof(VT) == 4 ? PEB_LIST_MIN_BLOCKS_F32 : 5) k_dem_list(DemArgs<VT> a) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool use_grid = a.nl_flags[1] != 0;   // this step's rebuild overflowed the lists
@@ -353,28 +387,40 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_list(DemArgs<VT> a) {
     if (t < a.n) {
         const double4 pi = a.pr[t];
         const uint32_t tagi = a.tag[t];
-        const int32_t uidi = a.uid[t];
         const SceneInfo &s = a.scenes[tagi >> 16];
-        const MatDev mi = a.mats[tagi & 0xffffu];
-        const V3<T> vi = ld_vw(a.vw, t, 0), wi = ld_vw(a.vw, t, 1);
+        const MatDev &mi = a.mats[tagi & 0xffffu];
+        const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
         Acc<T> acc;
         acc.F = v3(T(0), T(0), T(0));
         acc.T_ = acc.F;
         if (!use_grid) {
+            // entries: neighbour index, top bit set when this body is pe's body 1; two at a
+            // time so their loads overlap
+            int k = a.nl_start[t];
             const int e = a.nl_start[t + 1];
-            for (int k = a.nl_start[t]; k < e; ++k) {
-                const int32_t j = a.nl_idx[k];
-                pair_force<T, VT>(a, pi, vi, wi, uidi, mi, j, a.pr[j], acc);
+            for (; k + 1 < e; k += 2) {
+                const uint32_t e0 = (uint32_t)a.nl_idx[k], e1 = (uint32_t)a.nl_idx[k + 1];
+                const int32_t j0 = (int32_t)(e0 & 0x7fffffffu), j1 = (int32_t)(e1 & 0x7fffffffu);
+                const double4 p0 = a.pr[j0], p1 = a.pr[j1];
+                pair_force_o<T, VT>(a, pi, vi, wi, mi, j0, p0, (e0 >> 31) != 0u, acc);
+                pair_force_o<T, VT>(a, pi, vi, wi, mi, j1, p1, (e1 >> 31) != 0u, acc);
+            }
+            if (k < e) {
+                const uint32_t e0 = (uint32_t)a.nl_idx[k];
+                const int32_t j0 = (int32_t)(e0 & 0x7fffffffu);
+                pair_force_o<T, VT>(a, pi, vi, wi, mi, j0, a.pr[j0], (e0 >> 31) != 0u, acc);
             }
         } else {
-            grid_forces<T, VT>(a, s, (int32_t)t, pi, vi, wi, uidi, mi, acc);
+            grid_forces<T, VT>(a, s, (int32_t)t, pi, vi, wi, a.uid[t], mi, acc);
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
-        V3<T> v;
-        integrate<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v);
-        const float step = float(sqrt(double(v.x) * double(v.x) + double(v.y) * double(v.y) +
-                                      double(v.z) * double(v.z)) * a.dt);
-        const float d = a.disp[t] + step;
+        V3<T> v, w;
+        const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w);
+        // whole 32-byte records: a partial sector write would make L2 fetch the sector first
+        a.pr_out[t] = o;
+        st_vw(a.vw_out, a.n, t, v, w);
+        const float vx = float(v.x), vy = float(v.y), vz = float(v.z);
+        const float d = a.disp[t] + sqrtf(vx * vx + vy * vy + vz * vz) * float(a.dt) * 1.0001f;
         a.disp[t] = d;
         moved = !(d < a.half_skin);   // also catches NaN
     }
@@ -485,10 +531,7 @@ __global__ void k_permute_c(int64_t n, const int32_t *sorted, BodyBuf src, BodyB
     GRID_STRIDE(t, n) {
         const int32_t b = sorted[t];
         dst.pr[t] = src.pr[b];
-        const VT *s6 = (const VT *)src.vw + 6 * (int64_t)b;
-        VT *d6 = (VT *)dst.vw + 6 * t;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) d6[k] = s6[k];
+        cp_vw((VT *)dst.vw, t, (const VT *)src.vw, b, n);
         dst.tag[t] = src.tag[b];
         dst.uid[t] = src.uid[b];
         if (src.q) dst.q[t] = src.q[b];
@@ -497,14 +540,13 @@ __global__ void k_permute_c(int64_t n, const int32_t *sorted, BodyBuf src, BodyB
 }
 
 template <typename VT>
-__global__ void k_copy_c(int64_t n, BodyBuf src, BodyBuf dst, const int32_t *cond) {
+__global__ void k_copy_c(int64_t n, BodyBuf src, BodyBuf dst, double4 *other_pr,
+                         const int32_t *cond) {
     if (!*cond) return;
     GRID_STRIDE(t, n) {
         dst.pr[t] = src.pr[t];
-        const VT *s6 = (const VT *)src.vw + 6 * t;
-        VT *d6 = (VT *)dst.vw + 6 * t;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) d6[k] = s6[k];
+        other_pr[t] = src.pr[t];   // the other position buffer keeps the radius too
+        cp_vw((VT *)dst.vw, t, (const VT *)src.vw, t, n);
         dst.tag[t] = src.tag[t];
         dst.uid[t] = src.uid[t];
         if (src.q) dst.q[t] = src.q[t];
@@ -514,7 +556,7 @@ __global__ void k_copy_c(int64_t n, BodyBuf src, BodyBuf dst, const int32_t *con
 // neighbours of body t (state in cell order, so slot == index): pairs closer than
 // r_i + r_j + skin.  mode 0 counts, mode 1 writes.
 template <int MODE>
-__global__ void k_list(int64_t n, const double4 *pr, const uint32_t *tag,
+__global__ void k_list(int64_t n, const double4 *pr, const uint32_t *tag, const int32_t *uid,
                        const SceneInfo *scenes, const int32_t *cell_start, double skin,
                        int32_t *cnt, const int32_t *start, int64_t cap, int32_t *idx,
                        const int32_t *cond) {
@@ -543,7 +585,8 @@ __global__ void k_list(int64_t n, const double4 *pr, const uint32_t *tag,
                 const double dx = pi.x - pj.x, dy2 = pi.y - pj.y, dz2 = pi.z - pj.z;
                 const double rc = pi.w + pj.w + skin;
                 if (dx * dx + dy2 * dy2 + dz2 * dz2 < rc * rc) {
-                    if (MODE == 1) idx[pos++] = j;
+                    if (MODE == 1)
+                        idx[pos++] = (int32_t)((uint32_t)j | (uid[t] < uid[j] ? 0x80000000u : 0u));
                     ++count;
                 }
             }
@@ -583,15 +626,15 @@ int list_rebuild(Ctx *c) {
     k_permute_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->sorted, c->cur, L.tmp, L.disp,
                                                              cond);
     PEB_LAUNCHED(c);
-    k_copy_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.tmp, c->cur, cond);
+    k_copy_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.tmp, c->cur, c->nxt.pr, cond);
     PEB_LAUNCHED(c);
-    k_list<0><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+    k_list<0><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->cur.uid, c->d_scenes,
                                                        c->cell_start, L.skin, L.cnt, nullptr, 0,
                                                        nullptr, cond);
     PEB_LAUNCHED(c);
     rc = scan_exclusive_cond(c, L.cnt, L.start, n, cond);
     if (rc) return rc;
-    k_list<1><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+    k_list<1><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->cur.uid, c->d_scenes,
                                                        c->cell_start, L.skin, nullptr, L.start,
                                                        L.cap, L.idx, cond);
     PEB_LAUNCHED(c);
@@ -601,108 +644,26 @@ int list_rebuild(Ctx *c) {
     return PE_B200_OK;
 }
 
-__global__ void k_cond_set(cudaGraphConditionalHandle h, const int32_t *flags) {
-    cudaGraphSetConditional(h, flags[0] ? 1u : 0u);
-}
-
-void drop_graph(ListBuf &L, int k) {
-    if (L.gexec[k]) cudaGraphExecDestroy(L.gexec[k]);
-    if (L.graph[k]) cudaGraphDestroy(L.graph[k]);
-    L.gexec[k] = nullptr;
-    L.graph[k] = nullptr;
-    L.graph_pr[k] = nullptr;
-}
-
-// Captures the rebuild for the current position buffer into slot k: a kernel copies the
-// device-side request into the graph's condition, and the rebuild kernels form the body of an
-// IF node, so a step without a rebuild costs one tiny kernel.  Returns false on any failure
-// (the caller then launches the rebuild kernels directly, which return at once unless needed).
-template <typename VT>
-bool build_rebuild_graph(Ctx *c, int k) {
-    ListBuf &L = c->nl;
-    drop_graph(L, k);
-    if (scan_reserve(c, std::max<int64_t>(c->ncell, c->n)) != PE_B200_OK) return false;
-    cudaGraph_t g = nullptr;
-    cudaGraphExec_t ge = nullptr;
-    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
-    cudaGraphConditionalHandle h{};
-    ok = ok && cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
-    cudaGraphNode_t set_node = nullptr, cond_node = nullptr;
-    if (ok) {
-        cudaKernelNodeParams kp = {};
-        void *args[] = {&h, &L.flags};
-        kp.func = (void *)k_cond_set;
-        kp.gridDim = dim3(1);
-        kp.blockDim = dim3(1);
-        kp.kernelParams = args;
-        ok = cudaGraphAddKernelNode(&set_node, g, nullptr, 0, &kp) == cudaSuccess;
-    }
-    cudaGraph_t body = nullptr;
-    if (ok) {
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        ok = cudaGraphAddNode(&cond_node, g, &set_node, 1, &cp) == cudaSuccess;
-        if (ok) body = cp.conditional.phGraph_out[0];
-    }
-    if (ok) {
-        const bool prof = c->prof;
-        const int64_t launches = c->launches;
-        c->prof = false;  // event records are not allowed in a conditional body
-        ok = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
-                                           cudaStreamCaptureModeRelaxed) == cudaSuccess;
-        if (ok) {
-            const int rc = list_rebuild<VT>(c);
-            cudaGraph_t out = nullptr;
-            const cudaError_t e = cudaStreamEndCapture(c->stream, &out);
-            ok = rc == PE_B200_OK && e == cudaSuccess;
-        }
-        c->prof = prof;
-        c->launches = launches;
-    }
-    if (ok) ok = cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
-    if (!ok) {
-        if (ge) cudaGraphExecDestroy(ge);
-        if (g) cudaGraphDestroy(g);
-        cudaGetLastError();  // clear the sticky-free error of the failed graph call
-        return false;
-    }
-    L.graph[k] = g;
-    L.gexec[k] = ge;
-    L.graph_pr[k] = c->cur.pr;
-    L.graph_cap = L.cap;
-    return true;
-}
-
 template <typename VT>
 int list_step(Ctx *c, double dt) {
     ListBuf &L = c->nl;
-    if (L.graph_cap != L.cap) {
-        drop_graph(L, 0);
-        drop_graph(L, 1);
-        L.graph_cap = L.cap;
-    }
-    int slot = -1;
-    if (!L.graph_disabled) {
-        for (int k = 0; k < 2; ++k)
-            if (L.gexec[k] && L.graph_pr[k] == c->cur.pr) slot = k;
-        if (slot < 0) {
-            const int k = L.gexec[0] ? 1 : 0;
-            if (build_rebuild_graph<VT>(c, k)) slot = k;
-            else L.graph_disabled = true;
+    prof_begin(c, ST_REBUILD);
+    int rc = PE_B200_OK;
+    if (!L.coop_disabled) {
+        rc = dem_list_rebuild_persistent(c);
+        if (rc != PE_B200_OK) {
+            // no cooperative launch here: the rebuild kernels run one by one and return at
+            // once unless a rebuild was requested
+            L.coop_disabled = true;
+            cudaGetLastError();
+            c->err.clear();
+            rc = list_rebuild<VT>(c);
         }
-    }
-    if (slot >= 0) {
-        prof_begin(c, ST_REBUILD);
-        PEB_CUDA(c, cudaGraphLaunch(L.gexec[slot], c->stream));
-        c->launches += 1;
-        prof_end(c, ST_REBUILD);
     } else {
-        int rc = list_rebuild<VT>(c);
-        if (rc) return rc;
+        rc = list_rebuild<VT>(c);
     }
+    prof_end(c, ST_REBUILD);
+    if (rc) return rc;
     DemArgs<VT> a = dem_args<VT>(c, dt);
     a.sorted = nullptr;   // the grid fallback sees the state in cell order
     prof_begin(c, ST_DEM);
@@ -752,6 +713,8 @@ int dem_list_alloc(Ctx *c) {
     PEB_CUDA(c, cudaMemset(L.disp, 0, n * sizeof(float)));
     if (!L.h_flags) PEB_CUDA(c, cudaMallocHost(&L.h_flags, 8 * sizeof(int32_t)));
     if (!L.ev) PEB_CUDA(c, cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming));
+    PEB_CUDA(c, cudaMalloc(&L.rb_bar, 2 * sizeof(unsigned int)));
+    PEB_CUDA(c, cudaMemset(L.rb_bar, 0, 2 * sizeof(unsigned int)));
     PEB_CUDA(c, cudaMalloc(&L.tmp.pr, n * sizeof(double4)));
     PEB_CUDA(c, cudaMalloc(&L.tmp.vw, n * (size_t)c->vw_bytes));
     PEB_CUDA(c, cudaMalloc(&L.tmp.tag, n * sizeof(uint32_t)));
@@ -765,8 +728,8 @@ int dem_list_alloc(Ctx *c) {
 void dem_list_free(Ctx *c) {
     ListBuf &L = c->nl;
     if (L.check_pending && L.ev) cudaEventSynchronize(L.ev);
-    drop_graph(L, 0);
-    drop_graph(L, 1);
+    cudaFree(L.rb_bar);
+    cudaFree(L.rb_blk);
     cudaFree(L.start);
     cudaFree(L.cnt);
     cudaFree(L.idx);

@@ -87,13 +87,11 @@ struct ListBuf {
     cudaEvent_t ev = nullptr;
     bool check_pending = false;
     BodyBuf tmp;                // permutation target of a rebuild
-    // the rebuild as a CUDA graph whose body runs only when requested (a conditional node), one
-    // graph per position buffer; rebuilt when capacities change
-    cudaGraph_t graph[2] = {nullptr, nullptr};
-    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-    const void *graph_pr[2] = {nullptr, nullptr};
-    int64_t graph_cap = -1;
-    bool graph_disabled = false;
+    // persistent rebuild kernel (rebuild.cu): grid barrier words and per-block partial sums
+    unsigned int *rb_bar = nullptr;
+    int32_t *rb_blk = nullptr;
+    int64_t rb_blk_cap = 0;
+    bool coop_disabled = false;
 };
 
 // stage timers (pe's profiling sections, e.g. DEMSolver.h:1159-1260): CUDA events around each
@@ -233,6 +231,7 @@ cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream);
 int dem_list_alloc(Ctx *c);
 void dem_list_free(Ctx *c);
 int dem_list_request_rebuild(Ctx *c);
+int dem_list_rebuild_persistent(Ctx *c);
 int dem_list_step(Ctx *c, double dt);
 int dem_step(Ctx *c, double dt);
 int nbgs_step(Ctx *c, double dt);
@@ -309,10 +308,25 @@ __device__ __forceinline__ double dot_rn(double ax, double ay, double az, double
     return __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
 }
 
+// velocities are component-major: component c (vx vy vz wx wy wz) of body i at vw[c * n + i]
 template <typename T>
-__device__ __forceinline__ V3<T> ld_vw(const T *vw, int64_t i, int which) {
-    const T *p = vw + 6 * i + 3 * which;
-    return v3(p[0], p[1], p[2]);
+__device__ __forceinline__ V3<T> ld_vw(const T *vw, int64_t n, int64_t i, int which) {
+    const T *p = vw + 3 * which * n + i;
+    return v3(p[0], p[n], p[2 * n]);
+}
+template <typename T>
+__device__ __forceinline__ void st_vw(T *vw, int64_t n, int64_t i, V3<T> v, V3<T> w) {
+    vw[i] = v.x;
+    vw[n + i] = v.y;
+    vw[2 * n + i] = v.z;
+    vw[3 * n + i] = w.x;
+    vw[4 * n + i] = w.y;
+    vw[5 * n + i] = w.z;
+}
+template <typename T>
+__device__ __forceinline__ void cp_vw(T *dst, int64_t i, const T *src, int64_t j, int64_t n) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) dst[c * n + i] = src[c * n + j];
 }
 
 __device__ __forceinline__ void sphere_mass(double r, double density, double &im, double &ii,

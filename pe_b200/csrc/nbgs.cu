@@ -145,10 +145,8 @@ __global__ void k_permute_cache(int64_t n, const int32_t *sorted, const double4 
     tag_o[t] = tg;
     uid_o[t] = uid[b];
     if (TRACKQ) q_o[t] = q[b];
-    const VT *src = vw + 6 * (int64_t)b;
-    VT *dst = vw_o + 6 * t;
-    V3<VT> v = v3(src[0], src[1], src[2]), w = v3(src[3], src[4], src[5]);
-    dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; dst[3] = w.x; dst[4] = w.y; dst[5] = w.z;
+    V3<VT> v = ld_vw(vw, n, b, 0), w = ld_vw(vw, n, b, 1);
+    st_vw(vw_o, n, t, v, w);
     double im, ii, I;
     sphere_mass(p.w, mats[tg & 0xffffu].density, im, ii, I);
     const V3<VT> vp = v + v3(VT(gx), VT(gy), VT(gz)) * VT(dt);
@@ -189,9 +187,9 @@ struct RawF {
         if (g.other >= 0) {
             const double4 pj = pr[g.other];
             r2 = gp - v3(pj.x, pj.y, pj.z);
-            const T *o = vw + 6 * (int64_t)g.other;
-            const V3<double> vj = v3(double(o[0]), double(o[1]), double(o[2]));
-            const V3<double> wj = v3(double(o[3]), double(o[4]), double(o[5]));
+            const V3<T> vt = ld_vw(vw, n, g.other, 0), wt = ld_vw(vw, n, g.other, 1);
+            const V3<double> vj = v3(double(vt.x), double(vt.y), double(vt.z));
+            const V3<double> wj = v3(double(wt.x), double(wt.y), double(wt.z));
             rvel = rvel - (vj + cross(wj, r2));
             m2 = (int32_t)(tag[g.other] & 0xffffu);
         } else {
@@ -227,9 +225,9 @@ __global__ void k_raw(int64_t n, VisitArgs a, const int32_t *off, int64_t cap, c
     f.n = n;
     f.self = (int32_t)t;
     f.ps = a.pr[t];
-    const T *o = vw + 6 * t;
-    f.vs = v3(double(o[0]), double(o[1]), double(o[2]));
-    f.ws = v3(double(o[3]), double(o[4]), double(o[5]));
+    const V3<T> vt = ld_vw(vw, n, t, 0), wt = ld_vw(vw, n, t, 1);
+    f.vs = v3(double(vt.x), double(vt.y), double(vt.z));
+    f.ws = v3(double(wt.x), double(wt.y), double(wt.z));
     f.mats = mats;
     f.tag_self = a.tag[t];
     f.tag = a.tag;
@@ -576,8 +574,7 @@ __global__ void k_integrate(int64_t n, double dt, double drag, int has_drag, Bod
         w = w * VT(drag);
     }
     pr_o[t] = make_double4(nx, ny, nz, p.w);
-    VT *o = vw_o + 6 * t;
-    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = w.x; o[4] = w.y; o[5] = w.z;
+    st_vw(vw_o, n, t, v, w);
     const uint32_t tg = tag[t];
     tag_o[t] = tg;
     uid_o[t] = uid[t];

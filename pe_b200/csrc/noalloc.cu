@@ -102,8 +102,8 @@ __global__ void k_pack_bin(int64_t n, const double *x, const double *v, const do
     }
     pr[i] = make_double4(px, py, pz, ri);
     for (int a = 0; a < 3; ++a) {
-        vw[6 * i + a] = v[3 * i + a];
-        vw[6 * i + 3 + a] = w[3 * i + a];
+        vw[a * n + i] = v[3 * i + a];
+        vw[(3 + a) * n + i] = w[3 * i + a];
     }
     tag[i] = (uint32_t)m;
     uid[i] = (int32_t)i;
@@ -182,8 +182,8 @@ __global__ void k_unpack(int64_t n, const double4 *pr, const double *vw, const i
     x[3 * i + 1] = p.y;
     x[3 * i + 2] = p.z;
     for (int a = 0; a < 3; ++a) {
-        v[3 * i + a] = vw[6 * t + a];
-        w[3 * i + a] = vw[6 * t + 3 + a];
+        v[3 * i + a] = vw[a * n + t];
+        w[3 * i + a] = vw[(3 + a) * n + t];
     }
 }
 

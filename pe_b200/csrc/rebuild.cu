@@ -1,0 +1,315 @@
+// rebuild.cu -- the neighbour-list rebuild of the DEM step as one persistent kernel.
+//
+// One cooperative launch per step.  Unless the previous force kernel requested a rebuild (a
+// sphere has moved skin/2 since the last one) every block returns after reading one flag, so a
+// step without a rebuild pays a single short launch.  A rebuild runs its stages back to back,
+// separated by grid-wide barriers:
+//   clear cell counts | bin (cell key + slot, atomic histogram) | scan counts -> cell offsets |
+//   scatter | order each cell by body index | gather bodies into cell order | copy back |
+//   count neighbours closer than r_i + r_j + skin | scan counts -> list offsets | write lists
+// Every barrier wait is bounded: a block that waits too long sets an error flag and returns.
+#include <algorithm>
+
+#include "internal.cuh"
+
+namespace peb {
+
+namespace {
+
+constexpr int kRbBlock = 256;
+constexpr unsigned long long kSpinLimit = 1ull << 24;  // ~2 s with 100 ns sleeps
+
+template <typename VT>
+struct RebuildArgs {
+    int64_t n, ncell;
+    const SceneInfo *scenes;
+    BodyBuf cur, tmp;
+    double4 *other_pr;
+    int32_t *key, *rank, *sorted, *cell_count, *cell_start;
+    int32_t *cnt, *start, *idx;
+    int64_t cap;
+    double skin;
+    float *disp;
+    int32_t *flags;
+    unsigned int *bar;   // [0] arrivals, [1] generation
+    int32_t *blk;        // per-block partial sums (gridDim.x + 1)
+    int32_t *err;
+};
+
+// grid-wide barrier with a bounded wait; returns false (in every thread) after a timeout
+__device__ bool grid_sync(unsigned int *bar, int32_t *err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int *vgen = bar + 1;
+        const unsigned int gen = *vgen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*vgen == gen) {
+                __nanosleep(100);
+                if (++spins > kSpinLimit) {
+                    ok = 0;
+                    atomicOr(err, DERR_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ int block_sum(int v) {
+    __shared__ int ws[kRbBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int t = 0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kRbBlock / 32; ++k) t += ws[k];
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// inclusive scan across the block; *total receives the block total
+__device__ int block_incl_scan(int v, int *total) {
+    __shared__ int ws[kRbBlock / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) ws[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int x = (lane < kRbBlock / 32) ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += u;
+        }
+        if (lane < kRbBlock / 32) ws[lane] = x;
+    }
+    __syncthreads();
+    const int r = v + (w > 0 ? ws[w - 1] : 0);
+    *total = ws[kRbBlock / 32 - 1];
+    __syncthreads();
+    return r;
+}
+
+// exclusive scan of in[0, m) into out[0, m], out[m] = total; blocks own contiguous chunks
+template <typename VT>
+__device__ bool grid_scan(const RebuildArgs<VT> &a, const int32_t *in, int32_t *out, int64_t m) {
+    const int64_t per = (m + gridDim.x - 1) / gridDim.x;
+    const int64_t b0 = (int64_t)blockIdx.x * per;
+    const int64_t b1 = (b0 + per < m) ? b0 + per : m;
+    int s = 0;
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) s += in[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) a.blk[blockIdx.x] = s;
+    if (!grid_sync(a.bar, a.err)) return false;
+    if (blockIdx.x == 0) {
+        int run = 0;
+        for (int64_t base = 0; base < gridDim.x; base += blockDim.x) {
+            const int64_t i = base + threadIdx.x;
+            const int v = (i < gridDim.x) ? a.blk[i] : 0;
+            int tot;
+            const int incl = block_incl_scan(v, &tot);
+            if (i < gridDim.x) a.blk[i] = run + incl - v;
+            run += tot;
+        }
+        if (threadIdx.x == 0) out[m] = run;
+    }
+    if (!grid_sync(a.bar, a.err)) return false;
+    int run = a.blk[blockIdx.x];
+    for (int64_t base = b0; base < b1; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const int v = (i < b1) ? in[i] : 0;
+        int tot;
+        const int incl = block_incl_scan(v, &tot);
+        if (i < b1) out[i] = run + incl - v;
+        run += tot;
+    }
+    return true;
+}
+
+// neighbours of body t (state in cell order): count, or write with the orientation bit
+template <int MODE, typename VT>
+__device__ int list_neighbours(const RebuildArgs<VT> &a, int64_t t, int pos) {
+    const double4 pi = a.cur.pr[t];
+    const SceneInfo &s = a.scenes[a.cur.tag[t] >> 16];
+    const int32_t uidt = a.cur.uid[t];
+    int cx, cy, cz;
+    cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    int count = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int z = cz + dz;
+        if (z < 0 || z >= s.dim[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cy + dy;
+            if (y < 0 || y >= s.dim[1]) continue;
+            const int64_t c0 = cell_key(s, x0, y, z);
+            const int64_t c1 = c0 + (x1 - x0) + 1;
+            const int e = a.cell_start[c1];
+            for (int j = a.cell_start[c0]; j < e; ++j) {
+                if (j == t) continue;
+                const double4 pj = a.cur.pr[j];
+                const double dx = pi.x - pj.x, dy2 = pi.y - pj.y, dz2 = pi.z - pj.z;
+                const double rc = pi.w + pj.w + a.skin;
+                if (dx * dx + dy2 * dy2 + dz2 * dz2 < rc * rc) {
+                    if (MODE == 1)
+                        a.idx[pos++] = (int32_t)((uint32_t)j |
+                                                 (uidt < a.cur.uid[j] ? 0x80000000u : 0u));
+                    ++count;
+                }
+            }
+        }
+    }
+    return count;
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
+    if (!a.flags[0]) return;  // uniform: no rebuild requested
+    const int64_t n = a.n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // 1. clear the cell counts
+    for (int64_t i = g0; i <= a.ncell; i += stride) a.cell_count[i] = 0;
+    if (!grid_sync(a.bar, a.err)) return;
+    // 2. bin
+    for (int64_t i = g0; i < n; i += stride) {
+        const double4 p = a.cur.pr[i];
+        const SceneInfo &s = a.scenes[a.cur.tag[i] >> 16];
+        int cx, cy, cz;
+        cell_coords(s, p.x, p.y, p.z, cx, cy, cz);
+        const int32_t k = (int32_t)cell_key(s, cx, cy, cz);
+        a.key[i] = k;
+        a.rank[i] = atomicAdd(&a.cell_count[k], 1);
+    }
+    if (!grid_sync(a.bar, a.err)) return;
+    // 3. cell offsets
+    if (!grid_scan(a, a.cell_count, a.cell_start, a.ncell)) return;
+    if (!grid_sync(a.bar, a.err)) return;
+    // 4. scatter
+    for (int64_t i = g0; i < n; i += stride) a.sorted[a.cell_start[a.key[i]] + a.rank[i]] = (int32_t)i;
+    if (!grid_sync(a.bar, a.err)) return;
+    // 5. order each cell by body index (independent of the atomics' order)
+    for (int64_t c = g0; c < a.ncell; c += stride) {
+        const int b = a.cell_start[c], e = a.cell_start[c + 1];
+        for (int i = b + 1; i < e; ++i) {
+            const int32_t v = a.sorted[i];
+            int j = i - 1;
+            while (j >= b && a.sorted[j] > v) {
+                a.sorted[j + 1] = a.sorted[j];
+                --j;
+            }
+            a.sorted[j + 1] = v;
+        }
+    }
+    if (!grid_sync(a.bar, a.err)) return;
+    // 6. gather into cell order
+    for (int64_t t = g0; t < n; t += stride) {
+        const int32_t b = a.sorted[t];
+        a.tmp.pr[t] = a.cur.pr[b];
+        cp_vw((VT *)a.tmp.vw, t, (const VT *)a.cur.vw, b, n);
+        a.tmp.tag[t] = a.cur.tag[b];
+        a.tmp.uid[t] = a.cur.uid[b];
+        if (a.cur.q) a.tmp.q[t] = a.cur.q[b];
+        a.disp[t] = 0.f;
+    }
+    if (!grid_sync(a.bar, a.err)) return;
+    // 7. copy back (the other position buffer keeps the radius too)
+    for (int64_t t = g0; t < n; t += stride) {
+        const double4 p = a.tmp.pr[t];
+        a.cur.pr[t] = p;
+        a.other_pr[t] = p;
+        cp_vw((VT *)a.cur.vw, t, (const VT *)a.tmp.vw, t, n);
+        a.cur.tag[t] = a.tmp.tag[t];
+        a.cur.uid[t] = a.tmp.uid[t];
+        if (a.cur.q) a.cur.q[t] = a.tmp.q[t];
+    }
+    if (!grid_sync(a.bar, a.err)) return;
+    // 8. neighbour counts
+    for (int64_t t = g0; t < n; t += stride) a.cnt[t] = list_neighbours<0, VT>(a, t, 0);
+    if (!grid_sync(a.bar, a.err)) return;
+    // 9. list offsets
+    if (!grid_scan(a, a.cnt, a.start, n)) return;
+    if (!grid_sync(a.bar, a.err)) return;
+    const int64_t need = a.start[n];
+    if (g0 == 0) {
+        a.flags[1] = need > a.cap ? 1 : 0;
+        a.flags[2] = (int32_t)need;
+        a.flags[3] += 1;
+        a.flags[0] = 0;
+    }
+    // 10. write the lists (if they fit; otherwise the force kernel searches the fresh grid)
+    if (need <= a.cap)
+        for (int64_t t = g0; t < n; t += stride) list_neighbours<1, VT>(a, t, a.start[t]);
+}
+
+template <typename VT>
+int launch_rebuild(Ctx *c) {
+    ListBuf &L = c->nl;
+    static thread_local int occ_cache[2] = {0, 0};
+    int &occ = occ_cache[sizeof(VT) == 8 ? 1 : 0];
+    if (occ == 0) {
+        PEB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rebuild<VT>, kRbBlock, 0));
+        if (occ < 1) return set_err(c, PE_B200_ERR_CUDA, "rebuild kernel cannot be resident");
+    }
+    const int64_t want = std::max<int64_t>(1, (c->n + kRbBlock - 1) / kRbBlock);
+    const unsigned grid = (unsigned)std::min<int64_t>(want, (int64_t)occ * c->sm_count);
+    if (L.rb_blk_cap < (int64_t)grid + 1) {
+        cudaFree(L.rb_blk);
+        L.rb_blk = nullptr;
+        PEB_CUDA(c, cudaMalloc(&L.rb_blk, ((size_t)grid + 1) * sizeof(int32_t)));
+        L.rb_blk_cap = grid + 1;
+    }
+    RebuildArgs<VT> a;
+    a.n = c->n;
+    a.ncell = c->ncell;
+    a.scenes = c->d_scenes;
+    a.cur = c->cur;
+    a.tmp = L.tmp;
+    a.other_pr = c->nxt.pr;
+    a.key = c->key;
+    a.rank = c->rank;
+    a.sorted = c->sorted;
+    a.cell_count = c->cell_count;
+    a.cell_start = c->cell_start;
+    a.cnt = L.cnt;
+    a.start = L.start;
+    a.idx = L.idx;
+    a.cap = L.cap;
+    a.skin = L.skin;
+    a.disp = L.disp;
+    a.flags = L.flags;
+    a.bar = L.rb_bar;
+    a.blk = L.rb_blk;
+    a.err = c->d_err;
+    void *args[] = {&a};
+    PEB_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_rebuild<VT>, dim3(grid),
+                                            dim3(kRbBlock), args, 0, c->stream));
+    c->launches++;
+    return PE_B200_OK;
+}
+
+}  // namespace
+
+int dem_list_rebuild_persistent(Ctx *c) {
+    return (c->p.precision == PE_B200_FP64) ? launch_rebuild<double>(c) : launch_rebuild<float>(c);
+}
+
+}  // namespace peb

@@ -191,6 +191,13 @@ class Engine:
         self._check(self._L.pe_b200_profile(self._h, cap, names, ms, cnt, C.byref(n)))
         return {names[k].decode(): (ms[k], cnt[k]) for k in range(min(n.value, cap))}
 
+    def neighbor_list_stats(self) -> dict:
+        r, e, c = C.c_int64(), C.c_int64(), C.c_int64()
+        sk = C.c_double()
+        self._check(self._L.pe_b200_neighbor_list_stats(self._h, C.byref(r), C.byref(e),
+                                                        C.byref(c), C.byref(sk)))
+        return {"rebuilds": r.value, "entries": e.value, "capacity": c.value, "skin": sk.value}
+
     def kernel_launches(self) -> int:
         return int(self._L.pe_b200_kernel_launches(self._h))
 
