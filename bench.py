@@ -167,14 +167,15 @@ class Clocks:
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
-def make_engine(ss, kind, precision, iters=100):
+def make_engine(ss, kind, precision, iters=100, lists=True):
     from pe_b200 import _abi
     from pe_b200.engine import Engine
     solver = _abi.DEM if kind == "dem" else _abi.HCSITS
     model = _abi.INELASTIC_FRICTIONLESS
     if kind == "hcsits" and float(ss[0].materials[0, 2]) > 0:
         model = _abi.APPROX_INELASTIC_COULOMB_DECOUPLING
-    e = Engine(solver=solver, precision=precision, relaxation_model=model, max_iterations=iters)
+    e = Engine(solver=solver, precision=precision, relaxation_model=model, max_iterations=iters,
+               neighbor_lists=lists)
     if len(ss) == 1:
         e.load_scene(ss[0])
     else:
@@ -339,33 +340,67 @@ def our_arm(args):
 
 
 def extras(args, torch, flush, dev, ss, kind, mixed_value):
-    """FP64 path on the same scene, the NBGS scene, and the compiled reference."""
+    """Beside the headline: the plain FP64 GPU path (grid search every step, the first CUDA
+    form), the FP64 path with neighbour lists, the mixed-vs-FP64 position error after 1000 steps,
+    the batched ensemble, the NBGS scenes, and the compiled reference."""
     from pe_b200 import _abi
     out = {}
     nsph = sum(s.n for s in ss)
     dt = ss[0].dt
-    k64 = max(10, args.steps // 2)
-    e = make_engine(ss, kind, _abi.FP64)
-    stream = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
-    ms, _, prof = timed_steps(e, dt, k64, 3, torch, flush, stream)
-    v64 = nsph * k64 / (ms / 1e3)
-    out["fp64"] = {"value": v64, "ms_per_step": ms / k64,
-                   "mixed_over_fp64": mixed_value / v64,
-                   "stages_ms_per_step": {k: v[0] / k64 for k, v in prof.items() if v[1]}}
-    e.close()
-    if kind == "dem" and args.workload != "nbgs_box_32768":
-        s = scenes.nbgs_box(0)
-        for prec, name in ((_abi.MIXED, "mixed"), (_abi.FP64, "fp64")):
-            e = make_engine([s], "hcsits", prec)
-            st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
-            ksteps = 20
-            ms, _, prof = timed_steps(e, s.dt, ksteps, 3, torch, flush, st)
-            stt = e.stats()
-            out.setdefault("nbgs_32k", {})[name] = {
-                "value": s.n * ksteps / (ms / 1e3), "ms_per_step": ms / ksteps,
-                "contacts": stt["contacts"], "colors": stt["colors"],
-                "stages_ms_per_step": {k: v[0] / ksteps for k, v in prof.items() if v[1]}}
+
+    def timed(e, k, w=3):
+        st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+        ms, _, prof = timed_steps(e, dt if e is not None else dt, k, w, torch, flush, st)
+        return ms, prof
+
+    if kind == "dem":
+        for label, prec, lists in (("plain_fp64", _abi.FP64, False), ("fp64", _abi.FP64, True)):
+            k = max(10, min(args.steps, 200))
+            e = make_engine(ss, kind, prec, lists=lists)
+            ms, prof = timed(e, k)
+            v = nsph * k / (ms / 1e3)
+            out[label] = {"value": v, "ms_per_step": ms / k, "mixed_over_this": mixed_value / v,
+                          "neighbor_lists": lists,
+                          "stages_ms_per_step": {a: b[0] / k for a, b in prof.items() if b[1]}}
             e.close()
+        # stated error: mixed against FP64 positions after 1000 steps from the same state
+        em = make_engine(ss, kind, _abi.MIXED)
+        ef = make_engine(ss, kind, _abi.FP64)
+        em.step(dt, 1000)
+        ef.step(dt, 1000)
+        xm, xf = em.download()[0], ef.download()[0]
+        x0 = np.concatenate([s.x for s in ss])
+        out["error_after_1000_steps"] = {
+            "position_rel_linf": float(np.abs(xm - xf).max() / np.abs(xf).max()),
+            "displacement_rel_linf": float(np.abs(xm - xf).max() / max(np.abs(xf - x0).max(), 1e-300)),
+            "reference": "FP64 GPU path (itself within 1e-12 of pe's FP64 step)"}
+        em.close()
+        ef.close()
+    if args.workload == "dem_large_1m":
+        ens = scenes.batched_ensemble(0)
+        ne = sum(s.n for s in ens)
+        e = make_engine(ens, "dem", _abi.MIXED)
+        st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+        k = 50
+        ms, _, prof = timed_steps(e, ens[0].dt, k, 3, torch, flush, st)
+        out["ensemble_512"] = {"value": ne * k / (ms / 1e3), "ms_per_step": ms / k,
+                               "spheres": ne, "scenes": len(ens), "precision": "mixed",
+                               "stages_ms_per_step": {a: b[0] / k for a, b in prof.items() if b[1]}}
+        e.close()
+        for label, sc in (("nbgs_32k", scenes.nbgs_box(0)),
+                          ("nbgs_32k_dense", scenes.nbgs_box(0, n=32768, dims=(32.0, 32.0, 120.0),
+                                                            dense=True))):
+            for prec, name in ((_abi.MIXED, "mixed"), (_abi.FP64, "fp64")):
+                e = make_engine([sc], "hcsits", prec)
+                st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+                ksteps = 10
+                ms, _, prof = timed_steps(e, sc.dt, ksteps, 2, torch, flush, st)
+                stt = e.stats()
+                out.setdefault(label, {})[name] = {
+                    "value": sc.n * ksteps / (ms / 1e3), "ms_per_step": ms / ksteps,
+                    "contacts": stt["contacts"], "colors": stt["colors"], "sweeps": 100,
+                    "stages_ms_per_step": {a: b[0] / ksteps for a, b in prof.items() if b[1]}}
+                e.close()
     ref, why = run_reference(args.workload, steps=10, budget_s=20.0)
     if ref:
         out["cpu_baseline"] = {"value": ref["sphere_steps_per_s"], "unit": UNIT,

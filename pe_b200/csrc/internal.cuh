@@ -66,6 +66,9 @@ struct NbgsBuf {
     int32_t *body_adj = nullptr;              // body -> contacts CSR (2 * cap)
     uint64_t *used = nullptr;                 // colours used per body (bitmask)
     int32_t *flags = nullptr;                 // device counters (uncoloured, overflow, ...)
+    int32_t *cstart_dev = nullptr;            // colour offsets on the device
+    unsigned int *bar = nullptr;              // grid barrier of the persistent sweep
+    bool coop_disabled = false;
     void *vel = nullptr;                      // v', w', dv, dw per body (VT[12])
     double *red = nullptr;                    // reduction scratch
     int64_t red_cap = 0;
@@ -355,6 +358,43 @@ __device__ __forceinline__ void cell_coords(const SceneInfo &s, double x, double
 
 __device__ __forceinline__ int64_t cell_key(const SceneInfo &s, int cx, int cy, int cz) {
     return s.cell_base + ((int64_t)cz * s.dim[1] + cy) * s.dim[0] + cx;
+}
+
+// Grid-wide barrier for cooperative launches, with a bounded wait: a block that waits longer
+// than ~2 s records DERR_TIMEOUT and every thread of it sees false.  bar[0] counts arrivals,
+// bar[1] is the generation; both start at 0 and are left consistent after a completed barrier.
+constexpr unsigned long long kSpinLimit = 1ull << 24;  // polls of ~100 ns each
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, int32_t *err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int *vgen = bar + 1;
+        const unsigned int gen = *vgen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            // poll hot for the first few thousand rounds (barriers between short stages end
+            // within microseconds), then back off
+            unsigned long long spins = 0;
+            while (*vgen == gen) {
+                if (++spins > 4096) __nanosleep(128);
+                if (spins > kSpinLimit) {
+                    ok = 0;
+                    atomicOr(err, DERR_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
 }
 
 }  // namespace peb

@@ -401,26 +401,32 @@ __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos,
 }
 
 // ---- one colour of one sweep ----------------------------------------------------------------
-template <typename T, bool FRICTION>
-__global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int64_t cap, T dtinv,
-                                                Cache<T> cc, BodyV<T> bv, int64_t nb,
-                                                int track_delta, unsigned long long *delta) {
-    const int64_t k = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= end) return;
+// loads that bypass L1: in the persistent sweep, other SMs update these between colours
+template <typename T>
+__device__ __forceinline__ V3<T> ld3cg(const T *a, int64_t i, int64_t s) {
+    return v3(__ldcg(a + i), __ldcg(a + i + s), __ldcg(a + i + 2 * s));
+}
+
+// one contact of one sweep; COHERENT: read the velocity corrections and the impulse from L2
+template <typename T, bool FRICTION, bool COHERENT>
+__device__ __forceinline__ void sweep_contact(int64_t k, int64_t cap, T dtinv, const Cache<T> &cc,
+                                              const BodyV<T> &bv, int64_t nb, int track_delta,
+                                              unsigned long long *delta) {
     const int32_t b1 = cc.b1[k], b2 = cc.b2[k];
     const V3<T> r1 = ld3c(cc.r1, k, cap), r2 = ld3c(cc.r2, k, cap);
     const V3<T> n = ld3c(cc.n, k, cap);
-    const V3<T> pc = ld3c(cc.p, k, cap);  // contact-frame impulse
+    const V3<T> pc = COHERENT ? ld3cg(cc.p, k, cap) : ld3c(cc.p, k, cap);  // contact frame
     const T im1 = bv.im[b1], ii1 = bv.ii[b1];
-    V3<T> dv1 = ld3c(bv.dv, b1, nb), dw1 = ld3c(bv.dw, b1, nb);
+    V3<T> dv1 = COHERENT ? ld3cg(bv.dv, b1, nb) : ld3c(bv.dv, b1, nb);
+    V3<T> dw1 = COHERENT ? ld3cg(bv.dw, b1, nb) : ld3c(bv.dw, b1, nb);
     const V3<T> v1 = ld3c(bv.v, b1, nb), w1 = ld3c(bv.w, b1, nb);
     V3<T> dv2 = v3(T(0), T(0), T(0)), dw2 = dv2, v2 = dv2, w2 = dv2;
     T im2 = T(0), ii2 = T(0);
     if (b2 >= 0) {
         im2 = bv.im[b2];
         ii2 = bv.ii[b2];
-        dv2 = ld3c(bv.dv, b2, nb);
-        dw2 = ld3c(bv.dw, b2, nb);
+        dv2 = COHERENT ? ld3cg(bv.dv, b2, nb) : ld3c(bv.dv, b2, nb);
+        dw2 = COHERENT ? ld3cg(bv.dw, b2, nb) : ld3c(bv.dw, b2, nb);
         v2 = ld3c(bv.v, b2, nb);
         w2 = ld3c(bv.w, b2, nb);
     }
@@ -502,6 +508,38 @@ __global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int6
         const V3<T> dp = pold - pnew;
         const double m = fmax(fabs(double(dp.x)), fmax(fabs(double(dp.y)), fabs(double(dp.z))));
         atomicMax(delta, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+template <typename T, bool FRICTION>
+__global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int64_t cap, T dtinv,
+                                                Cache<T> cc, BodyV<T> bv, int64_t nb,
+                                                int track_delta, unsigned long long *delta) {
+    const int64_t k = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= end) return;
+    sweep_contact<T, FRICTION, false>(k, cap, dtinv, cc, bv, nb, track_delta, delta);
+}
+
+// All sweeps of a step in one cooperative launch: colour after colour, separated by bounded
+// grid barriers (each colour is conflict-free, so its contacts run in parallel).
+template <typename T, bool FRICTION>
+__global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolors,
+                                                            const int32_t *color_start,
+                                                            int64_t cap, T dtinv, Cache<T> cc,
+                                                            BodyV<T> bv, int64_t nb,
+                                                            int track_last,
+                                                            unsigned long long *delta,
+                                                            unsigned int *bar, int32_t *err) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t e = color_start[col + 1];
+            for (int64_t k = color_start[col] + g0; k < e; k += stride)
+                sweep_contact<T, FRICTION, true>(k, cap, dtinv, cc, bv, nb, track, delta);
+            if (!grid_sync(bar, err)) return;
+        }
     }
 }
 
@@ -617,6 +655,9 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         PEB_CUDA(c, cudaMalloc(&b.flags, 256 * sizeof(int32_t)));
         PEB_CUDA(c, cudaMallocHost(&b.color_start, 260 * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.red, 4 * sizeof(double)));
+        PEB_CUDA(c, cudaMalloc(&b.cstart_dev, 130 * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.bar, 2 * sizeof(unsigned int)));
+        PEB_CUDA(c, cudaMemset(b.bar, 0, 2 * sizeof(unsigned int)));
     }
     return PE_B200_OK;
 }
@@ -780,7 +821,40 @@ int nbgs_step_t(Ctx *c, double dt) {
     if (c->want_residual) PEB_CUDA(c, cudaMemsetAsync(nb.red, 0, 2 * sizeof(double), c->stream));
     if (nc > 0) {
         prof_begin(c, ST_SWEEP);
-        for (int it = 0; it < iters; ++it) {
+        bool done = iters == 0;
+        if (!done && !nb.coop_disabled) {
+            // all sweeps in one cooperative launch (colours separated by grid barriers); as few
+            // blocks as the largest colour needs, so the barriers stay short
+            int maxcol = 1;
+            for (int col = 0; col < ncolors; ++col)
+                maxcol = std::max(maxcol, nb.color_start[col + 1] - nb.color_start[col]);
+            auto kern = fr ? k_sweeps_persistent<VT, true> : k_sweeps_persistent<VT, false>;
+            int occ = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0);
+            if (e == cudaSuccess && occ > 0) {
+                const unsigned grid = (unsigned)std::min<int64_t>(
+                    (int64_t)occ * c->sm_count, std::max<int64_t>(1, (maxcol + kBlk - 1) / kBlk));
+                PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start,
+                                            (ncolors + 1) * sizeof(int32_t),
+                                            cudaMemcpyHostToDevice, c->stream));
+                int iters_a = iters, ncol_a = ncolors, track_a = c->want_residual ? 1 : 0;
+                int64_t cap_a = cap, n_a = n;
+                VT dtinv_a = VT(1.0 / dt);
+                int32_t *cs = nb.cstart_dev;
+                void *args[] = {&iters_a, &ncol_a, &cs, &cap_a, &dtinv_a, &cc, &bv, &n_a,
+                                &track_a, &dl, &nb.bar, &c->d_err};
+                e = cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(kBlk), args, 0,
+                                                c->stream);
+            }
+            if (e == cudaSuccess) {
+                done = true;
+                c->launches++;
+            } else {
+                cudaGetLastError();
+                nb.coop_disabled = true;
+            }
+        }
+        for (int it = 0; !done && it < iters; ++it) {
             const int track = (c->want_residual && it == iters - 1) ? 1 : 0;
             for (int col = 0; col < ncolors; ++col) {
                 const int64_t b = nb.color_start[col], e = nb.color_start[col + 1];
@@ -845,6 +919,8 @@ void nbgs_free(Ctx *c) {
     cudaFree(b.vel);
     cudaFree(b.flags);
     cudaFree(b.red);
+    cudaFree(b.cstart_dev);
+    cudaFree(b.bar);
     if (b.color_start) cudaFreeHost(b.color_start);
     b = NbgsBuf();
 }

@@ -17,7 +17,6 @@ namespace peb {
 namespace {
 
 constexpr int kRbBlock = 256;
-constexpr unsigned long long kSpinLimit = 1ull << 24;  // ~2 s with 100 ns sleeps
 
 template <typename VT>
 struct RebuildArgs {
@@ -35,38 +34,6 @@ struct RebuildArgs {
     int32_t *blk;        // per-block partial sums (gridDim.x + 1)
     int32_t *err;
 };
-
-// grid-wide barrier with a bounded wait; returns false (in every thread) after a timeout
-__device__ bool grid_sync(unsigned int *bar, int32_t *err) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int *vgen = bar + 1;
-        const unsigned int gen = *vgen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u);
-        int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned long long spins = 0;
-            while (*vgen == gen) {
-                __nanosleep(100);
-                if (++spins > kSpinLimit) {
-                    ok = 0;
-                    atomicOr(err, DERR_TIMEOUT);
-                    break;
-                }
-            }
-        }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
 
 __device__ int block_sum(int v) {
     __shared__ int ws[kRbBlock / 32];
