@@ -156,6 +156,20 @@ int pe_b200_last_step_stats(pe_b200_ctx *ctx, int64_t *ncontacts, int32_t *ncolo
                             double *delta_max, double *residual);
 int pe_b200_set_residual(pe_b200_ctx *ctx, int32_t enabled);
 
+/* Reverse-mode gradients of the FP64 DEM step (no counterpart in pe, which has no gradients).
+ * pe_b200_adjoint_forward runs nsteps steps of size dt from the current state (the grid-search
+ * DEM step, FP64, orientation tracking off), keeping a checkpoint every `checkpoint_every`
+ * steps; the context is left at the final state.  pe_b200_adjoint_backward takes the gradient
+ * of a loss with respect to the final state (gx, gv, gw: 3n doubles each, upload order),
+ * recomputes each segment from its checkpoint and returns the gradient with respect to the
+ * initial positions, velocities and angular velocities, and in gparams (4 doubles, may be NULL)
+ * the derivative with respect to the contact coefficients k_n, c_n, c_t and mu, each summed over
+ * all contacts (for one material: the derivative with respect to that composed coefficient). */
+int pe_b200_adjoint_forward(pe_b200_ctx *ctx, int32_t nsteps, double dt, int32_t checkpoint_every);
+int pe_b200_adjoint_backward(pe_b200_ctx *ctx, const double *gx, const double *gv,
+                             const double *gw, double *gx0, double *gv0, double *gw0,
+                             double *gparams);
+
 /* DEM neighbour-list state: rebuilds so far, entries at the last rebuild, capacity, skin
  * (waits for the context's stream).  pe has no neighbour lists: its hash grids re-bin every
  * body every step (HashGrids.h:1121-1258); this reports the device-side replacement. */

@@ -27,7 +27,8 @@ EXPORTS = ["pe_b200_default_params", "pe_b200_create", "pe_b200_destroy", "pe_b2
            "pe_b200_set_state", "pe_b200_step", "pe_b200_download_bodies",
            "pe_b200_find_contacts", "pe_b200_last_step_stats", "pe_b200_set_residual",
            "pe_b200_kernel_launches", "pe_b200_stream", "pe_b200_set_profiling",
-           "pe_b200_profile", "pe_b200_dem_step_static", "pe_b200_neighbor_list_stats"]
+           "pe_b200_profile", "pe_b200_dem_step_static", "pe_b200_neighbor_list_stats",
+           "pe_b200_adjoint_forward", "pe_b200_adjoint_backward"]
 
 STATIC_MAX_SPHERES = 32768
 STATIC_MAX_CELLS = 131072
@@ -87,6 +88,8 @@ def load() -> C.CDLL:
         "pe_b200_kernel_launches": (i64, [vp]),
         "pe_b200_set_profiling": (C.c_int, [vp, i32]),
         "pe_b200_neighbor_list_stats": (C.c_int, [vp, P(i64), P(i64), P(i64), P(dp)]),
+        "pe_b200_adjoint_forward": (C.c_int, [vp, i32, dp, i32]),
+        "pe_b200_adjoint_backward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "pe_b200_profile": (C.c_int, [vp, i32, P(C.c_char_p), P(dp), P(i64), P(i32)]),
         "pe_b200_stream": (vp, [vp]),
         "pe_b200_dem_step_static": (C.c_int, [i64, vp, vp, vp, vp, vp, i32, P(Material), i32, vp,

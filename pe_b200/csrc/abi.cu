@@ -110,6 +110,7 @@ void free_device(Ctx *c) {
     c->d_box_mat = nullptr;
     nbgs_free(c);
     dem_list_free(c);
+    adjoint_free(c);
     c->uploaded = false;
     c->binned = false;
 }
@@ -666,6 +667,22 @@ int pe_b200_last_step_stats(pe_b200_ctx *h, int64_t *ncontacts, int32_t *ncolors
     if (delta_max) *delta_max = c->last_delta;
     if (residual) *residual = c->last_residual;
     return PE_B200_OK;
+}
+
+int pe_b200_adjoint_forward(pe_b200_ctx *h, int32_t nsteps, double dt, int32_t every) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    cudaSetDevice(c->device);
+    return adjoint_forward(c, nsteps, dt, every);
+}
+
+int pe_b200_adjoint_backward(pe_b200_ctx *h, const double *gx, const double *gv, const double *gw,
+                             double *gx0, double *gv0, double *gw0, double *gparams) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !gx || !gv || !gw || !gx0 || !gv0 || !gw0) return PE_B200_ERR_ARG;
+    cudaSetDevice(c->device);
+    return adjoint_backward(c, gx, gv, gw, gx0, gv0, gw0, gparams);
 }
 
 int pe_b200_neighbor_list_stats(pe_b200_ctx *h, int64_t *rebuilds, int64_t *entries,

@@ -97,6 +97,14 @@ struct ListBuf {
     bool coop_disabled = false;
 };
 
+// checkpoints of the adjoint's forward run (adjoint.cu)
+struct AdjState {
+    int32_t nsteps = 0, every = 1;
+    double dt = 0.0;
+    std::vector<BodyBuf> ckpt;   // state before steps 0, every, 2*every, ...
+    std::vector<BodyBuf> seg;    // pre-step states of the segment being reversed
+};
+
 // stage timers (pe's profiling sections, e.g. DEMSolver.h:1159-1260): CUDA events around each
 // stage on the context's stream, summed when queried
 enum Stage : int {
@@ -150,6 +158,7 @@ struct Ctx {
 
     NbgsBuf nb;
     ListBuf nl;
+    AdjState adj;
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -237,6 +246,10 @@ int dem_list_request_rebuild(Ctx *c);
 int dem_list_rebuild_persistent(Ctx *c);
 int dem_list_step(Ctx *c, double dt);
 int dem_step(Ctx *c, double dt);
+int adjoint_forward(Ctx *c, int32_t nsteps, double dt, int32_t every);
+int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *gw, double *ox,
+                     double *ov, double *ow, double *gpar);
+void adjoint_free(Ctx *c);
 int nbgs_step(Ctx *c, double dt);
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out);
 void nbgs_free(Ctx *c);

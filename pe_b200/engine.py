@@ -191,6 +191,23 @@ class Engine:
         self._check(self._L.pe_b200_profile(self._h, cap, names, ms, cnt, C.byref(n)))
         return {names[k].decode(): (ms[k], cnt[k]) for k in range(min(n.value, cap))}
 
+    def adjoint_forward(self, nsteps: int, dt: float, checkpoint_every: int = 100):
+        """Runs nsteps FP64 DEM steps keeping checkpoints for adjoint_backward."""
+        self._check(self._L.pe_b200_adjoint_forward(self._h, int(nsteps), float(dt),
+                                                    int(checkpoint_every)))
+
+    def adjoint_backward(self, gx, gv, gw):
+        """Gradient of a loss w.r.t. the initial state and the contact coefficients, given its
+        gradient w.r.t. the final state. Returns (gx0, gv0, gw0, gparams[k_n, c_n, c_t, mu])."""
+        n = self.n
+        cv = lambda a: np.ascontiguousarray(a, np.float64).reshape(n, 3)
+        gx, gv, gw = cv(gx), cv(gv), cv(gw)
+        ox, ov, ow = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        gp = np.zeros(4)
+        self._check(self._L.pe_b200_adjoint_backward(self._h, _p(gx), _p(gv), _p(gw), _p(ox),
+                                                     _p(ov), _p(ow), _p(gp)))
+        return ox, ov, ow, gp
+
     def neighbor_list_stats(self) -> dict:
         r, e, c = C.c_int64(), C.c_int64(), C.c_int64()
         sk = C.c_double()

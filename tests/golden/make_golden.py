@@ -63,7 +63,44 @@ def golden(name, scene, dem_steps=(1, 10), hc=True, hc_converged=False):
     print(path, os.path.getsize(path), "bytes,", len(rec["pairs"]), "contacts")
 
 
+def adjoint_fd(name="adjoint_fd", seed=2, n=64, steps=40):
+    """Central differences (h as in the adjoint tests) of the loss of pe_b200.adjoint.LossSpec after
+    `steps` reference DEM steps, with respect to sampled initial velocities and to k_n, c_n, mu."""
+    from pe_b200.adjoint import LossSpec, make_single_material, set_params
+
+    p = {"k_n": 1e5, "c_n": 50.0, "c_t": 40.0, "mu": 0.3}
+    s = make_single_material(scenes.small_random(seed, n=n, overlap=0.04, with_boxes=False), **p)
+    spec = LossSpec.for_scene(s)
+    with tempfile.TemporaryDirectory() as tmp:
+        def loss(t):
+            sp = os.path.join(tmp, "scene.bin")
+            t.save(sp)
+            return spec.value(run_steps("ref_dem", sp, t.n, steps, tmp)[0])
+
+        rec = {"scene": np.frombuffer(s.to_bytes(), np.uint8), "loss": loss(s)}
+        rng = np.random.default_rng(0)
+        idx = np.stack([rng.integers(0, n, 8), rng.integers(0, 3, 8)], axis=1)
+        fd = []
+        for i, a in idx:
+            sp_, sm_ = s.copy(), s.copy()
+            sp_.v[i, a] += 1e-6
+            sm_.v[i, a] -= 1e-6
+            fd.append((loss(sp_) - loss(sm_)) / 2e-6)
+        rec["v_idx"], rec["fd_v"] = idx, np.array(fd)
+        for key, h in (("k_n", 1e-1), ("c_n", 1e-4), ("mu", 1e-6)):
+            pp, pm = dict(p), dict(p)
+            pp[key] += h
+            pm[key] -= h
+            rec["fd_" + key] = (loss(set_params(s, **pp)) - loss(set_params(s, **pm))) / (2 * h)
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **rec)
+    print(path, os.path.getsize(path), "bytes, loss", rec["loss"])
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["adjoint_fd"]:
+        adjoint_fd()
+        sys.exit(0)
     golden("small64_boxes", scenes.small_random(1, n=64, with_boxes=True))
     golden("small64_planes", scenes.small_random(2, n=64, with_boxes=False))
     golden("lattice512", scenes.dem_lattice(0, side=8), dem_steps=(1, 10, 100))
@@ -74,3 +111,4 @@ if __name__ == "__main__":
            dem_steps=(1,), hc_converged=True)
     golden("loose125_boxes", scenes.small_random(4, n=125, overlap=0.0, with_boxes=True),
            dem_steps=(1,), hc_converged=True)
+    adjoint_fd()

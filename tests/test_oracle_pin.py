@@ -82,3 +82,34 @@ def test_live_reference_random_scenes(tmp_path):
         o.dem_step(s.dt, 5)
         assert rel_err(o.x, a[:3 * n].reshape(n, 3)) < 1e-13
         assert rel_err(o.v, a[3 * n:6 * n].reshape(n, 3)) < 1e-12
+
+
+def test_oracle_finite_differences_match_reference():
+    """The oracle's 40-step loss and its central differences (the checks the adjoint is held to)
+    equal the compiled reference's."""
+    from pe_b200.adjoint import LossSpec, set_params
+
+    g = load_golden("adjoint_fd")
+    s = g["scene"]
+    spec = LossSpec.for_scene(s)
+
+    def loss(t):
+        o = OracleWorld(t)
+        o.dem_step(t.dt, 40)
+        return spec.value(o.x)
+
+    assert abs(loss(s) - float(g["loss"])) < 1e-13
+    fd = []
+    for i, a in g["v_idx"]:
+        sp, sm = s.copy(), s.copy()
+        sp.v[i, a] += 1e-6
+        sm.v[i, a] -= 1e-6
+        fd.append((loss(sp) - loss(sm)) / 2e-6)
+    assert np.abs(np.array(fd) - g["fd_v"]).max() < 1e-7 * np.abs(g["fd_v"]).max()
+    p = {"k_n": 1e5, "c_n": 50.0, "c_t": 40.0, "mu": 0.3}
+    for key, h in (("k_n", 1e-1), ("c_n", 1e-4), ("mu", 1e-6)):
+        pp, pm = dict(p), dict(p)
+        pp[key] += h
+        pm[key] -= h
+        f = (loss(set_params(s, **pp)) - loss(set_params(s, **pm))) / (2 * h)
+        assert abs(f - float(g["fd_" + key])) < 1e-7 * abs(float(g["fd_" + key])) + 1e-12, key
