@@ -1,0 +1,645 @@
+/* pe_b200_world.hpp -- pe's World / body-creation API on top of the C ABI of pe_b200.h.
+ *
+ * Header-only C++17.  A program written against pe's single-domain API
+ *
+ *     WorldID world = theWorld();
+ *     world->setGravity(0.0, 0.0, -9.81);
+ *     MaterialID m = createMaterial("granite2", 1.0, 0.0, 0.15, 0.15, 0.25, 1e9, 2e5, 100, 100);
+ *     createPlane(100, 0.0, 0.0, 1.0, 0.0, m);
+ *     SphereID s = createSphere(1, 0.0, 0.0, 0.5, 0.5, m);
+ *     world->run(1000, 1e-4);
+ *     Vec3 x = s->getPosition();
+ *
+ * compiles against this header with `namespace pe = pe_b200;` (or `using namespace pe_b200;`)
+ * and runs its time steps on the GPU.  It follows
+ *   - World (pe/core/World.h:159-295, src/core/World.cpp:262-357): setGravity, setDamping,
+ *     simulationStep, run, size, destroy;
+ *   - createMaterial and the predefined materials iron, copper, granite, oak, fir
+ *     (src/core/Materials.cpp:175-290, pe/core/Materials.h:831-1176);
+ *   - createSphere (src/core/rigidbody/Sphere.cpp:1187-1200), createPlane
+ *     (src/core/rigidbody/Plane.cpp:1202-1225), createBox (src/core/rigidbody/Box.cpp:1312-1330);
+ *   - the HCSITS setters of the collision system (HardContactSemiImplicitTimesteppingSolvers.h:
+ *     172-179 for the model names, 793-850 for the setters);
+ * with pe's exceptions: std::invalid_argument for invalid arguments, std::runtime_error for
+ * unsupported configurations and device errors.
+ *
+ * Differences from pe, all checked at the call that hits them:
+ *   - spheres move; planes and boxes are fixed walls (a box must be setFixed(true) before the
+ *     next time step, as pe's fixed boxes are);
+ *   - the solver is chosen at run time (theCollisionSystem()->setSolver) instead of by the
+ *     compile-time pe_CONSTRAINT_SOLVER; the default is PE_B200_CONSTRAINT_SOLVER
+ *     (PE_B200_DEM unless defined before including this header);
+ *   - state lives on the GPU: setters upload before the next step, getters download once after
+ *     each step (or batch of steps).
+ */
+#ifndef PE_B200_WORLD_HPP
+#define PE_B200_WORLD_HPP
+
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pe_b200.h"
+
+#ifndef PE_B200_CONSTRAINT_SOLVER
+#define PE_B200_CONSTRAINT_SOLVER PE_B200_DEM
+#endif
+
+namespace pe_b200 {
+
+typedef double real;
+typedef std::size_t id_t;
+
+// ---- vectors -----------------------------------------------------------------------------------
+class Vec3 {
+  public:
+    Vec3() : v_{0.0, 0.0, 0.0} {}
+    Vec3(real x, real y, real z) : v_{x, y, z} {}
+    real operator[](std::size_t i) const { return v_[i]; }
+    real &operator[](std::size_t i) { return v_[i]; }
+    Vec3 operator+(const Vec3 &b) const { return Vec3(v_[0] + b[0], v_[1] + b[1], v_[2] + b[2]); }
+    Vec3 operator-(const Vec3 &b) const { return Vec3(v_[0] - b[0], v_[1] - b[1], v_[2] - b[2]); }
+    Vec3 operator*(real s) const { return Vec3(v_[0] * s, v_[1] * s, v_[2] * s); }
+    real operator*(const Vec3 &b) const { return v_[0] * b[0] + v_[1] * b[1] + v_[2] * b[2]; }
+    real sqrLength() const { return (*this) * (*this); }
+    real length() const { return std::sqrt(sqrLength()); }
+    Vec3 getNormalized() const {
+        const real l = length();
+        return l > 0.0 ? (*this) * (1.0 / l) : *this;
+    }
+
+  private:
+    real v_[3];
+};
+
+// ---- materials ---------------------------------------------------------------------------------
+typedef std::size_t MaterialID;
+const MaterialID iron = 0;
+const MaterialID copper = 1;
+const MaterialID granite = 2;
+const MaterialID oak = 3;
+const MaterialID fir = 4;
+const MaterialID invalid_material = static_cast<MaterialID>(-1);
+
+class Material {
+  public:
+    Material(const std::string &name, const pe_b200_material &m) : name_(name), m_(m) {}
+    const std::string &getName() const { return name_; }
+    real getDensity() const { return m_.density; }
+    real getRestitution() const { return m_.cor; }
+    real getStaticFriction() const { return m_.csf; }
+    real getDynamicFriction() const { return m_.cdf; }
+    real getPoissonRatio() const { return m_.poisson; }
+    real getYoungModulus() const { return m_.young; }
+    real getStiffness() const { return m_.stiffness; }
+    real getDampingN() const { return m_.dampingN; }
+    real getDampingT() const { return m_.dampingT; }
+    const pe_b200_material &record() const { return m_; }
+
+  private:
+    std::string name_;
+    pe_b200_material m_;
+};
+
+namespace detail {
+inline std::vector<Material> &materials() {
+    // pe's predefined materials, in pe's order (pe/core/Materials.h:831, 896, 961, 1026, 1091)
+    static std::vector<Material> table = {
+        Material("iron", {7874, 0.5, 0.1, 0.1, 0.24, 200, 200, 0, 0}),
+        Material("copper", {8920, 0.5, 0.1, 0.1, 0.33, 117, 117, 0, 0}),
+        Material("granite", {2800, 0.5, 0.1, 0.1, 0.25, 55, 55, 0, 0}),
+        Material("oak", {800, 0.5, 0.1, 0.1, 0.35, 11, 11, 0, 0}),
+        Material("fir", {500, 0.5, 0.1, 0.1, 0.34, 13, 13, 0, 0}),
+    };
+    return table;
+}
+inline unsigned long &anonymous_materials() {
+    static unsigned long count = 0;
+    return count;
+}
+}  // namespace detail
+
+inline const Material &getMaterial(MaterialID id) {
+    if (id >= detail::materials().size()) throw std::invalid_argument("Invalid material ID");
+    return detail::materials()[id];
+}
+
+/* Material::find (src/core/Materials.cpp:302) */
+inline MaterialID findMaterial(const std::string &name) {
+    const std::vector<Material> &t = detail::materials();
+    for (std::size_t i = 0; i < t.size(); ++i)
+        if (t[i].getName() == name) return i;
+    return invalid_material;
+}
+
+inline void markMaterialsChanged();
+
+/* createMaterial with pe's argument checks and messages (src/core/Materials.cpp:175-223) */
+inline MaterialID createMaterial(const std::string &name, real density, real cor, real csf,
+                                 real cdf, real poisson, real young, real stiffness,
+                                 real dampingN, real dampingT) {
+    if (findMaterial(name) != invalid_material)
+        throw std::invalid_argument("Material of that name already exists!");
+    if (density <= 0.0) throw std::invalid_argument("Invalid material density!");
+    if (cor < 0.0 || cor > 1.0) throw std::invalid_argument("Invalid coefficient of restitution!");
+    if (csf < 0.0) throw std::invalid_argument("Invalid coefficient of static friction!");
+    if (cdf < 0.0) throw std::invalid_argument("Invalid coefficient of dynamic friction!");
+    if (poisson < -1.0 || poisson > 0.5) throw std::invalid_argument("Invalid Poisson's ratio");
+    if (young <= 0.0) throw std::invalid_argument("Invalid Young's modulus");
+    if (stiffness <= 0.0) throw std::invalid_argument("Invalid stiffness");
+    if (dampingN < 0.0 || dampingT < 0.0)
+        throw std::invalid_argument("Invalid damping coefficients");
+    detail::materials().emplace_back(
+        name, pe_b200_material{density, cor, csf, cdf, poisson, young, stiffness, dampingN, dampingT});
+    markMaterialsChanged();
+    return detail::materials().size() - 1;
+}
+
+/* anonymous material "Material<k>" (src/core/Materials.cpp:275-290) */
+inline MaterialID createMaterial(real density, real cor, real csf, real cdf, real poisson,
+                                 real young, real stiffness, real dampingN, real dampingT) {
+    std::string name;
+    do {
+        if (detail::anonymous_materials() + 1 == 0)
+            throw std::runtime_error("Index overflow for anonymous materials");
+        name = "Material" + std::to_string(++detail::anonymous_materials());
+    } while (findMaterial(name) != invalid_material);
+    return createMaterial(name, density, cor, csf, cdf, poisson, young, stiffness, dampingN,
+                          dampingT);
+}
+
+// ---- bodies ------------------------------------------------------------------------------------
+class World;
+
+class RigidBody {
+  public:
+    virtual ~RigidBody() {}
+    id_t getID() const { return uid_; }
+    id_t getSystemID() const { return sid_; }
+    MaterialID getMaterial() const { return mat_; }
+    bool isVisible() const { return visible_; }
+
+  protected:
+    RigidBody(World *w, id_t sid, id_t uid, MaterialID mat, bool visible)
+        : world_(w), sid_(sid), uid_(uid), mat_(mat), visible_(visible) {}
+    World *world_;
+    id_t sid_, uid_;
+    MaterialID mat_;
+    bool visible_;
+    friend class World;
+};
+
+class Sphere : public RigidBody {
+  public:
+    real getRadius() const { return r_; }
+    /* SphereBase::calcMass (pe/core/rigidbody/SphereBase.h:169-171) */
+    real getMass() const {
+        return 4.0 / 3.0 * M_PI * r_ * r_ * r_ * getMaterial_().getDensity();
+    }
+    Vec3 getPosition() const;
+    Vec3 getLinearVel() const;
+    Vec3 getAngularVel() const;
+    void setPosition(real x, real y, real z);
+    void setPosition(const Vec3 &p) { setPosition(p[0], p[1], p[2]); }
+    void setLinearVel(real x, real y, real z);
+    void setLinearVel(const Vec3 &v) { setLinearVel(v[0], v[1], v[2]); }
+    void setAngularVel(real x, real y, real z);
+    void setAngularVel(const Vec3 &w) { setAngularVel(w[0], w[1], w[2]); }
+
+  private:
+    Sphere(World *w, id_t sid, id_t uid, const Vec3 &x, real r, MaterialID m, bool visible)
+        : RigidBody(w, sid, uid, m, visible), x_(x), r_(r) {}
+    const Material &getMaterial_() const { return pe_b200::getMaterial(mat_); }
+    Vec3 x_, v_, w_;
+    real r_;
+    friend class World;
+};
+
+class Plane : public RigidBody {
+  public:
+    const Vec3 &getNormal() const { return n_; }
+    real getDisplacement() const { return d_; }
+
+  private:
+    Plane(World *w, id_t sid, id_t uid, const Vec3 &n, real d, MaterialID m, bool visible)
+        : RigidBody(w, sid, uid, m, visible), n_(n), d_(d) {}
+    Vec3 n_;
+    real d_;
+    friend class World;
+};
+
+class Box : public RigidBody {
+  public:
+    const Vec3 &getPosition() const { return x_; }
+    const Vec3 &getLengths() const { return l_; }
+    bool isFixed() const { return fixed_; }
+    void setFixed(bool fixed);
+    /* rotation matrix, row-major */
+    const real *getRotation() const { return R_; }
+    /* RigidBody::rotate(axis, angle): rotation about the box centre (Rodrigues' formula) */
+    void rotate(const Vec3 &axis, real angle);
+    void rotate(real x, real y, real z, real angle) { rotate(Vec3(x, y, z), angle); }
+
+  private:
+    Box(World *w, id_t sid, id_t uid, const Vec3 &x, const Vec3 &l, MaterialID m, bool visible)
+        : RigidBody(w, sid, uid, m, visible), x_(x), l_(l), R_{1, 0, 0, 0, 1, 0, 0, 0, 1} {}
+    Vec3 x_, l_;
+    real R_[9];
+    bool fixed_ = false;
+    friend class World;
+};
+
+typedef Sphere *SphereID;
+typedef Plane *PlaneID;
+typedef Box *BoxID;
+typedef RigidBody *BodyID;
+
+// ---- collision system (solver settings) --------------------------------------------------------
+class CollisionSystem {
+  public:
+    /* HardContactSemiImplicitTimesteppingSolvers.h:172-179 */
+    enum RelaxationModel {
+        InelasticFrictionlessContact,
+        ApproximateInelasticCoulombContactByDecoupling,
+        ApproximateInelasticCoulombContactByOrthogonalProjections,
+        InelasticCoulombContactByDecoupling,
+        InelasticCoulombContactByOrthogonalProjections,
+        InelasticGeneralizedMaximumDissipationContact
+    };
+    /* HCSITS.h:793-850; models other than the first two raise std::runtime_error at the next
+     * step, where pe raises it (HCSITS.h:1926) */
+    void setMaxIterations(std::size_t n);
+    void setRelaxationModel(RelaxationModel m);
+    void setErrorReductionParameter(real erp);
+    /* the relaxation parameter only enters the models this library does not implement */
+    void setRelaxationParameter(real omega) { omega_ = omega; }
+    real getRelaxationParameter() const { return omega_; }
+    std::size_t getMaxIterations() const { return (std::size_t)p_.max_iterations; }
+    RelaxationModel getRelaxationModel() const { return model_; }
+    /* run-time replacement of the compile-time pe_CONSTRAINT_SOLVER */
+    void setSolver(int solver);   /* PE_B200_DEM or PE_B200_HCSITS */
+    void setPrecision(int prec);  /* PE_B200_FP64 or PE_B200_MIXED */
+    void setDevice(int device);
+    int getSolver() const { return p_.solver; }
+    int getPrecision() const { return p_.precision; }
+    /* number of contacts and NBGS colours of the last step */
+    void lastStepStats(int64_t *ncontacts, int32_t *ncolors) const;
+
+  private:
+    CollisionSystem() {
+        pe_b200_default_params(&p_);
+        p_.solver = PE_B200_CONSTRAINT_SOLVER;
+    }
+    pe_b200_params p_;
+    RelaxationModel model_ = ApproximateInelasticCoulombContactByDecoupling;
+    real omega_ = 0.75;
+    World *world_ = nullptr;
+    friend class World;
+};
+
+// ---- world -------------------------------------------------------------------------------------
+class World {
+  public:
+    typedef std::size_t SizeType;
+
+    static World &instance() {
+        static World w;
+        return w;
+    }
+    ~World() { release(); }
+
+    void setGravity(real gx, real gy, real gz) { setGravity(Vec3(gx, gy, gz)); }
+    void setGravity(const Vec3 &g) {
+        g_ = g;
+        if (ctx_) check(pe_b200_set_gravity(ctx_, gravity_array()));
+    }
+    const Vec3 &getGravity() const { return g_; }
+    void setDamping(real damping) {
+        if (damping < 0.0 || damping > 1.0) throw std::invalid_argument("Invalid damping factor");
+        damping_ = damping;
+        if (ctx_) check(pe_b200_set_damping(ctx_, damping_));
+    }
+    real getDamping() const { return damping_; }
+
+    SizeType size() const { return spheres_.size() + planes_.size() + boxes_.size(); }
+    SizeType numSpheres() const { return spheres_.size(); }
+    SizeType numPlanes() const { return planes_.size(); }
+    SizeType numBoxes() const { return boxes_.size(); }
+    SphereID sphere(SizeType i) const { return spheres_.at(i).get(); }
+
+    /* World::simulationStep (src/core/World.cpp:330-357) */
+    void simulationStep(real timestep) { run(1, timestep); }
+    /* World::run: `steps` time steps in one call into the library */
+    void run(unsigned int steps, real timestep) {
+        if (!(timestep > 0.0)) throw std::invalid_argument("Invalid time step size");
+        prepare();
+        if (!spheres_.empty()) check(pe_b200_step(ctx_, (int32_t)steps, timestep));
+        host_stale_ = !spheres_.empty();
+    }
+
+    /* destroy(BodyID): removes and deletes a body */
+    void destroy(BodyID b) {
+        pull();
+        if (erase(spheres_, b) || erase(planes_, b) || erase(boxes_, b)) {
+            structure_dirty_ = true;
+            return;
+        }
+        throw std::invalid_argument("Body does not belong to this world");
+    }
+    /* removes every body (pe's World::destroy of all bodies / a fresh world) */
+    void clear() {
+        spheres_.clear();
+        planes_.clear();
+        boxes_.clear();
+        structure_dirty_ = true;
+        host_stale_ = false;
+    }
+
+    CollisionSystem &collisionSystem() { return cs_; }
+    pe_b200_ctx *context() { return ctx_; }
+
+    // -- used by the free functions and the body classes ----------------------------------------
+    SphereID addSphere(id_t uid, const Vec3 &x, real r, MaterialID m, bool visible) {
+        pull();
+        if (!(r > 0.0)) throw std::invalid_argument("Invalid sphere radius");
+        getMaterial(m);
+        spheres_.emplace_back(new Sphere(this, next_sid_++, uid, x, r, m, visible));
+        structure_dirty_ = true;
+        return spheres_.back().get();
+    }
+    PlaneID addPlane(id_t uid, Vec3 n, real d, MaterialID m, bool visible) {
+        if (n.sqrLength() == 0.0) throw std::invalid_argument("Invalid plane normal!");
+        getMaterial(m);
+        pull();
+        planes_.emplace_back(new Plane(this, next_sid_++, uid, n.getNormalized(), d, m, visible));
+        structure_dirty_ = true;
+        return planes_.back().get();
+    }
+    BoxID addBox(id_t uid, const Vec3 &x, const Vec3 &l, MaterialID m, bool visible) {
+        if (l[0] <= 0.0 || l[1] <= 0.0 || l[2] <= 0.0)
+            throw std::invalid_argument("Invalid side length");
+        getMaterial(m);
+        pull();
+        boxes_.emplace_back(new Box(this, next_sid_++, uid, x, l, m, visible));
+        structure_dirty_ = true;
+        return boxes_.back().get();
+    }
+    void pull() const {
+        if (!host_stale_ || !ctx_) return;
+        const std::size_t n = spheres_.size();
+        std::vector<double> x(3 * n), v(3 * n), w(3 * n);
+        check(pe_b200_download_bodies(ctx_, x.data(), v.data(), w.data(), nullptr));
+        for (std::size_t i = 0; i < n; ++i) {
+            Sphere &s = *spheres_[i];
+            s.x_ = Vec3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+            s.v_ = Vec3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+            s.w_ = Vec3(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
+        }
+        host_stale_ = false;
+    }
+    void markStateDirty() { state_dirty_ = true; }
+    void markStructureDirty() { structure_dirty_ = true; }
+    void markParamsDirty() { params_dirty_ = true; }
+    void check(int rc) const {
+        if (rc == PE_B200_OK) return;
+        const std::string msg = ctx_ ? pe_b200_last_error(ctx_) : "pe_b200 error";
+        if (rc == PE_B200_ERR_ARG) throw std::invalid_argument(msg);
+        throw std::runtime_error(msg + " (status " + std::to_string(rc) + ")");
+    }
+
+  private:
+    World() { cs_.world_ = this; }
+    World(const World &) = delete;
+    World &operator=(const World &) = delete;
+
+    template <typename T>
+    static bool erase(std::vector<std::unique_ptr<T>> &v, BodyID b) {
+        for (auto it = v.begin(); it != v.end(); ++it)
+            if (it->get() == b) {
+                v.erase(it);
+                return true;
+            }
+        return false;
+    }
+    const double *gravity_array() {
+        ga_[0] = g_[0];
+        ga_[1] = g_[1];
+        ga_[2] = g_[2];
+        return ga_;
+    }
+    void release() {
+        if (ctx_) pe_b200_destroy(ctx_);
+        ctx_ = nullptr;
+    }
+    // brings the device up to date with the host-side world before a step
+    void prepare() {
+        if (params_dirty_ || !ctx_) {
+            pull();
+            release();
+            pe_b200_params p = cs_.p_;
+            for (int k = 0; k < 3; ++k) p.gravity[k] = g_[k];
+            p.damping = damping_;
+            int rc = pe_b200_create(&p, &ctx_);
+            if (rc != PE_B200_OK) {
+                ctx_ = nullptr;
+                throw std::runtime_error("pe_b200_create failed (status " + std::to_string(rc) + ")");
+            }
+            params_dirty_ = false;
+            structure_dirty_ = true;
+        }
+        for (const auto &b : boxes_)
+            if (!b->isFixed())
+                throw std::runtime_error("Box " + std::to_string(b->getID()) +
+                                         " is not fixed: only fixed boxes are supported");
+        if (cs_.p_.solver == PE_B200_HCSITS &&
+            cs_.model_ > CollisionSystem::ApproximateInelasticCoulombContactByDecoupling)
+            throw std::runtime_error("Unsupported relaxation model.");
+        if (structure_dirty_) {
+            std::vector<pe_b200_material> mats;
+            for (const Material &m : detail::materials()) mats.push_back(m.record());
+            check(pe_b200_set_materials(ctx_, (int32_t)mats.size(), mats.data()));
+            std::vector<double> planes, boxes;
+            std::vector<int32_t> pm, bm;
+            for (const auto &p : planes_) {
+                planes.insert(planes.end(), {p->n_[0], p->n_[1], p->n_[2], p->d_});
+                pm.push_back((int32_t)p->mat_);
+            }
+            for (const auto &b : boxes_) {
+                boxes.insert(boxes.end(), {b->x_[0], b->x_[1], b->x_[2], b->l_[0], b->l_[1], b->l_[2]});
+                boxes.insert(boxes.end(), b->R_, b->R_ + 9);
+                bm.push_back((int32_t)b->mat_);
+            }
+            check(pe_b200_set_walls(ctx_, 0, (int32_t)planes_.size(), planes.data(), pm.data(),
+                                    (int32_t)boxes_.size(), boxes.data(), bm.data()));
+            const std::size_t n = spheres_.size();
+            std::vector<double> x, v, w, r;
+            std::vector<int32_t> mat;
+            for (const auto &s : spheres_) {
+                x.insert(x.end(), {s->x_[0], s->x_[1], s->x_[2]});
+                v.insert(v.end(), {s->v_[0], s->v_[1], s->v_[2]});
+                w.insert(w.end(), {s->w_[0], s->w_[1], s->w_[2]});
+                r.push_back(s->r_);
+                mat.push_back((int32_t)s->mat_);
+            }
+            if (n) check(pe_b200_upload_bodies(ctx_, (int64_t)n, x.data(), v.data(), w.data(),
+                                               r.data(), mat.data(), nullptr, 1));
+            structure_dirty_ = false;
+            state_dirty_ = false;
+        } else if (state_dirty_) {
+            const std::size_t n = spheres_.size();
+            std::vector<double> x(3 * n), v(3 * n), w(3 * n);
+            for (std::size_t i = 0; i < n; ++i)
+                for (int a = 0; a < 3; ++a) {
+                    x[3 * i + a] = spheres_[i]->x_[a];
+                    v[3 * i + a] = spheres_[i]->v_[a];
+                    w[3 * i + a] = spheres_[i]->w_[a];
+                }
+            if (n) check(pe_b200_set_state(ctx_, x.data(), v.data(), w.data()));
+            state_dirty_ = false;
+        }
+        check(pe_b200_set_gravity(ctx_, gravity_array()));
+        check(pe_b200_set_damping(ctx_, damping_));
+    }
+
+    CollisionSystem cs_;
+    pe_b200_ctx *ctx_ = nullptr;
+    std::vector<std::unique_ptr<Sphere>> spheres_;
+    std::vector<std::unique_ptr<Plane>> planes_;
+    std::vector<std::unique_ptr<Box>> boxes_;
+    Vec3 g_;
+    double ga_[3] = {0.0, 0.0, 0.0};
+    real damping_ = 1.0;
+    id_t next_sid_ = 0;
+    bool structure_dirty_ = true, state_dirty_ = false, params_dirty_ = true;
+    mutable bool host_stale_ = false;
+};
+
+typedef World *WorldID;
+
+/* theWorld() (pe/core/World.h:333) */
+inline WorldID theWorld() { return &World::instance(); }
+/* theCollisionSystem() */
+inline CollisionSystem *theCollisionSystem() { return &World::instance().collisionSystem(); }
+
+inline void markMaterialsChanged() { World::instance().markStructureDirty(); }
+
+// ---- body creation (pe's free functions) -------------------------------------------------------
+inline SphereID createSphere(id_t uid, const Vec3 &gpos, real radius, MaterialID material,
+                             bool visible = true) {
+    return World::instance().addSphere(uid, gpos, radius, material, visible);
+}
+inline SphereID createSphere(id_t uid, real x, real y, real z, real radius, MaterialID material,
+                             bool visible = true) {
+    return createSphere(uid, Vec3(x, y, z), radius, material, visible);
+}
+inline PlaneID createPlane(id_t uid, const Vec3 &normal, real d, MaterialID material,
+                           bool visible = true) {
+    return World::instance().addPlane(uid, normal, d, material, visible);
+}
+inline PlaneID createPlane(id_t uid, real a, real b, real c, real d, MaterialID material,
+                           bool visible = true) {
+    return createPlane(uid, Vec3(a, b, c), d, material, visible);
+}
+/* plane through gpos: d = normalised normal . gpos (Plane.cpp:1260-1320) */
+inline PlaneID createPlane(id_t uid, const Vec3 &normal, const Vec3 &gpos, MaterialID material,
+                           bool visible = true) {
+    if (normal.sqrLength() == 0.0) throw std::invalid_argument("Invalid plane normal!");
+    const Vec3 n = normal.getNormalized();
+    return createPlane(uid, n, n * gpos, material, visible);
+}
+inline BoxID createBox(id_t uid, const Vec3 &gpos, const Vec3 &lengths, MaterialID material,
+                       bool visible = true) {
+    return World::instance().addBox(uid, gpos, lengths, material, visible);
+}
+inline BoxID createBox(id_t uid, real x, real y, real z, real lx, real ly, real lz,
+                       MaterialID material, bool visible = true) {
+    return createBox(uid, Vec3(x, y, z), Vec3(lx, ly, lz), material, visible);
+}
+inline void destroy(BodyID body) { World::instance().destroy(body); }
+
+// ---- out-of-line members -----------------------------------------------------------------------
+inline Vec3 Sphere::getPosition() const { world_->pull(); return x_; }
+inline Vec3 Sphere::getLinearVel() const { world_->pull(); return v_; }
+inline Vec3 Sphere::getAngularVel() const { world_->pull(); return w_; }
+inline void Sphere::setPosition(real x, real y, real z) {
+    world_->pull();
+    x_ = Vec3(x, y, z);
+    world_->markStateDirty();
+}
+inline void Sphere::setLinearVel(real x, real y, real z) {
+    world_->pull();
+    v_ = Vec3(x, y, z);
+    world_->markStateDirty();
+}
+inline void Sphere::setAngularVel(real x, real y, real z) {
+    world_->pull();
+    w_ = Vec3(x, y, z);
+    world_->markStateDirty();
+}
+inline void Box::setFixed(bool fixed) {
+    fixed_ = fixed;
+    world_->markStructureDirty();
+}
+inline void Box::rotate(const Vec3 &axis, real angle) {
+    if (axis.sqrLength() == 0.0) throw std::invalid_argument("Invalid rotation axis");
+    const Vec3 u = axis.getNormalized();
+    const real c = std::cos(angle), s = std::sin(angle), t = 1.0 - c;
+    const real Q[9] = {t * u[0] * u[0] + c,        t * u[0] * u[1] - s * u[2], t * u[0] * u[2] + s * u[1],
+                       t * u[0] * u[1] + s * u[2], t * u[1] * u[1] + c,        t * u[1] * u[2] - s * u[0],
+                       t * u[0] * u[2] - s * u[1], t * u[1] * u[2] + s * u[0], t * u[2] * u[2] + c};
+    real out[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            out[3 * i + j] = Q[3 * i] * R_[j] + Q[3 * i + 1] * R_[3 + j] + Q[3 * i + 2] * R_[6 + j];
+    for (int k = 0; k < 9; ++k) R_[k] = out[k];
+    world_->markStructureDirty();
+}
+
+inline void CollisionSystem::setMaxIterations(std::size_t n) {
+    if (n > (std::size_t)INT32_MAX) throw std::invalid_argument("Invalid number of iterations");
+    p_.max_iterations = (int32_t)n;
+    if (world_->context()) world_->check(pe_b200_set_max_iterations(world_->context(), p_.max_iterations));
+}
+inline void CollisionSystem::setRelaxationModel(RelaxationModel m) {
+    model_ = m;
+    if (m <= ApproximateInelasticCoulombContactByDecoupling) {
+        p_.relaxation_model = (int32_t)m;
+        if (world_->context())
+            world_->check(pe_b200_set_relaxation_model(world_->context(), p_.relaxation_model));
+    }
+}
+inline void CollisionSystem::setErrorReductionParameter(real erp) {
+    p_.erp = erp;
+    if (world_->context()) world_->check(pe_b200_set_error_reduction(world_->context(), erp));
+}
+inline void CollisionSystem::setSolver(int solver) {
+    if (solver != PE_B200_DEM && solver != PE_B200_HCSITS) throw std::invalid_argument("Invalid solver");
+    p_.solver = solver;
+    world_->markParamsDirty();
+}
+inline void CollisionSystem::setPrecision(int prec) {
+    if (prec != PE_B200_FP64 && prec != PE_B200_MIXED) throw std::invalid_argument("Invalid precision");
+    p_.precision = prec;
+    world_->markParamsDirty();
+}
+inline void CollisionSystem::setDevice(int device) {
+    p_.device = device;
+    world_->markParamsDirty();
+}
+inline void CollisionSystem::lastStepStats(int64_t *ncontacts, int32_t *ncolors) const {
+    double dm, res;
+    if (!world_->context()) {
+        *ncontacts = 0;
+        *ncolors = 0;
+        return;
+    }
+    world_->check(pe_b200_last_step_stats(world_->context(), ncontacts, ncolors, &dm, &res));
+}
+
+}  // namespace pe_b200
+
+#endif  // PE_B200_WORLD_HPP

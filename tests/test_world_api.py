@@ -1,0 +1,83 @@
+"""pe's World / body-creation C++ API (include/pe_b200_world.hpp) driven by a C++ program
+(tests/cpp/world_driver.cpp): argument checks on the CPU, and on the GPU the same trajectories as
+the Engine binding and the oracle."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import load_golden, rel_err
+from oracle.pe_oracle import OracleWorld
+from pe_b200 import _abi
+from pe_b200.engine import Engine
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "pe_b200")
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    if not os.path.exists(os.path.join(LIBDIR, "libpe_b200.so")):
+        pytest.skip("libpe_b200.so not built")
+    exe = str(tmp_path_factory.mktemp("cpp") / "world_driver")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "world_driver.cpp"), "-L", LIBDIR,
+                    "-lpe_b200", "-Wl,-rpath," + LIBDIR, "-o", exe], check=True)
+    return exe
+
+
+def test_world_api_argument_checks(driver):
+    r = subprocess.run([driver, "errors"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "ok"
+
+
+def run_driver(driver, tmp_path, s, solver, prec, steps):
+    sp, out = str(tmp_path / "scene.bin"), str(tmp_path / "out.bin")
+    s.save(sp)
+    r = subprocess.run([driver, "run", sp, solver, prec, str(steps), out], capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    a = np.fromfile(out, "<f8").reshape(3, s.n, 3)
+    return a[0], a[1], a[2]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small64_boxes", "lattice512"])
+def test_world_api_dem_matches_engine_and_oracle(driver, tmp_path, name):
+    s = load_golden(name)["scene"]
+    x, v, w = run_driver(driver, tmp_path, s, "dem", "fp64", 10)
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(s)
+    e.step(s.dt, 10)
+    xe, ve, we = e.download()
+    e.close()
+    assert np.array_equal(x, xe) and np.array_equal(v, ve) and np.array_equal(w, we)
+    o = OracleWorld(s)
+    o.dem_step(s.dt, 10)
+    assert rel_err(x, o.x) < 1e-12
+    assert rel_err(v, o.v) < 1e-10
+
+
+@pytest.mark.gpu
+def test_world_api_hcsits_matches_engine(driver, tmp_path):
+    s = load_golden("loose125_boxes")["scene"]
+    x, v, w = run_driver(driver, tmp_path, s, "hcsits", "fp64", 4)
+    e = Engine(solver=_abi.HCSITS, precision=_abi.FP64, relaxation_model=1,
+               max_iterations=100).load_scene(s)
+    e.step(s.dt, 4)
+    xe, ve, we = e.download()
+    e.close()
+    assert np.array_equal(x, xe) and np.array_equal(v, ve) and np.array_equal(w, we)
+
+
+@pytest.mark.gpu
+def test_world_api_mixed_precision_runs(driver, tmp_path):
+    s = load_golden("lattice512")["scene"]
+    x, v, w = run_driver(driver, tmp_path, s, "dem", "mixed", 10)
+    o = OracleWorld(s)
+    o.dem_step(s.dt, 10)
+    assert rel_err(x, o.x) < 1e-6
