@@ -185,6 +185,32 @@ int pe_b200_set_profiling(pe_b200_ctx *ctx, int32_t enabled);
 int pe_b200_profile(pe_b200_ctx *ctx, int32_t cap, const char **names, double *total_ms,
                     int64_t *count, int32_t *n_out);
 
+/* CUDA graphs of the DEM neighbour-list step (no pe counterpart; pe's step is a serial loop).
+ * pe_b200_step(ctx, nsteps, dt) with nsteps >= steps captures `steps` consecutive steps once and
+ * then replays the graph, so a replay costs one launch instead of two per step; the remainder
+ * runs step by step.  Default 16; 0 (or 1) launches every step; odd values are rounded down.
+ * Graphs are not used while profiling is on.  The results are the same as without graphs. */
+int pe_b200_set_graph_steps(pe_b200_ctx *ctx, int32_t steps);
+/* 1 when the last pe_b200_step ran through a captured graph. */
+int pe_b200_graph_active(const pe_b200_ctx *ctx);
+
+/* Launch shapes of the DEM neighbour-list step (no pe counterpart). */
+typedef struct {
+    int32_t dem_variant;     /* launch shape of the force/integration kernel, 0..variants-1 */
+    int32_t rebuild_per_sm;  /* CTAs per SM of the persistent list rebuild; 0 = as many as fit */
+    double skin;             /* neighbour-list skin (cells are re-planned to 2 r_max + skin) */
+    double ms_per_step;      /* pe_b200_autotune: measured time of the winner; else -1 */
+    int32_t variants;        /* output: number of launch shapes */
+    int32_t reserved;
+} pe_b200_tuning;
+int pe_b200_get_tuning(pe_b200_ctx *ctx, pe_b200_tuning *out);
+int pe_b200_set_tuning(pe_b200_ctx *ctx, const pe_b200_tuning *t);
+/* Times the DEM list step under candidate tunings from the current state (each trial restores
+ * that state, forces one list rebuild and times trial_steps steps with CUDA events), applies the
+ * fastest and restores the state.  Shapes do not change results; the skin changes them only in
+ * the last bits (the summation order follows the re-sorted body order). */
+int pe_b200_autotune(pe_b200_ctx *ctx, double dt, int32_t trial_steps, pe_b200_tuning *out);
+
 /* Allocation-free DEM step.  This entry point has no counterpart in the reference.
  *
  * For callers that cannot allocate device memory -- an application that owns all device memory

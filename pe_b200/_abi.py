@@ -28,7 +28,9 @@ EXPORTS = ["pe_b200_default_params", "pe_b200_create", "pe_b200_destroy", "pe_b2
            "pe_b200_find_contacts", "pe_b200_last_step_stats", "pe_b200_set_residual",
            "pe_b200_kernel_launches", "pe_b200_stream", "pe_b200_set_profiling",
            "pe_b200_profile", "pe_b200_dem_step_static", "pe_b200_neighbor_list_stats",
-           "pe_b200_adjoint_forward", "pe_b200_adjoint_backward"]
+           "pe_b200_adjoint_forward", "pe_b200_adjoint_backward", "pe_b200_set_graph_steps",
+           "pe_b200_graph_active", "pe_b200_get_tuning", "pe_b200_set_tuning",
+           "pe_b200_autotune"]
 
 STATIC_MAX_SPHERES = 32768
 STATIC_MAX_CELLS = 131072
@@ -45,6 +47,11 @@ class Params(C.Structure):
 class Material(C.Structure):
     _fields_ = [(f, C.c_double) for f in ("density", "cor", "csf", "cdf", "poisson", "young",
                                           "stiffness", "dampingN", "dampingT")]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("dem_variant", C.c_int32), ("rebuild_per_sm", C.c_int32), ("skin", C.c_double),
+                ("ms_per_step", C.c_double), ("variants", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PeB200Error(RuntimeError):
@@ -90,6 +97,11 @@ def load() -> C.CDLL:
         "pe_b200_neighbor_list_stats": (C.c_int, [vp, P(i64), P(i64), P(i64), P(dp)]),
         "pe_b200_adjoint_forward": (C.c_int, [vp, i32, dp, i32]),
         "pe_b200_adjoint_backward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        "pe_b200_set_graph_steps": (C.c_int, [vp, i32]),
+        "pe_b200_graph_active": (C.c_int, [vp]),
+        "pe_b200_get_tuning": (C.c_int, [vp, P(Tuning)]),
+        "pe_b200_set_tuning": (C.c_int, [vp, P(Tuning)]),
+        "pe_b200_autotune": (C.c_int, [vp, dp, i32, P(Tuning)]),
         "pe_b200_profile": (C.c_int, [vp, i32, P(C.c_char_p), P(dp), P(i64), P(i32)]),
         "pe_b200_stream": (vp, [vp]),
         "pe_b200_dem_step_static": (C.c_int, [i64, vp, vp, vp, vp, vp, i32, P(Material), i32, vp,

@@ -138,6 +138,8 @@ int check_material(const pe_b200_material &m, std::string &why) {
     return 0;
 }
 
+}  // namespace
+
 int upload_tables(Ctx *c) {
     // materials
     std::vector<MatDev> md(c->mats.size());
@@ -208,15 +210,19 @@ int upload_tables(Ctx *c) {
     return PE_B200_OK;
 }
 
+namespace {
+
 // grid geometry of each scene: bounding box of its spheres, extended to axis-aligned planes
 // that close the scene, with cells of the largest AABB extent (grown if the grid would be much
 // larger than the body count; bodies that leave the grid are clamped into the border cells,
 // which keeps the search exact and only costs speed)
 void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int64_t> &order,
-                const std::vector<int64_t> &begin, const std::vector<int64_t> &count) {
-    int64_t base = 0;
+                const std::vector<int64_t> &begin, const std::vector<int64_t> &count,
+                double skin) {
+    c->plan_bounds.assign(6 * (size_t)c->nscenes, 0.0);
+    c->plan_rmax.assign(c->nscenes, 0.0);
+    c->plan_count.assign(c->nscenes, 0);
     for (int s = 0; s < c->nscenes; ++s) {
-        SceneInfo &si = c->scenes[s];
         double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         double rmax = 0.0;
         for (int64_t k = begin[s]; k < begin[s] + count[s]; ++k) {
@@ -243,9 +249,31 @@ void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int6
                 // only extend towards the plane, never shrink below the bodies' extent
             }
         }
-        double h = 2.0 * (rmax + kContactThreshold) * (1.0 + 1e-9);
+        for (int a = 0; a < 3; ++a) {
+            c->plan_bounds[6 * s + a] = lo[a];
+            c->plan_bounds[6 * s + 3 + a] = hi[a];
+        }
+        c->plan_rmax[s] = rmax;
+        c->plan_count[s] = count[s];
+        c->scenes[s].body_begin = begin[s];
+        c->scenes[s].nbodies = count[s];
+    }
+    plan_cells(c, skin);
+}
+
+}  // namespace
+
+// Cells of every scene for the bounds plan_grids recorded: edge 2 (r_max + contact threshold)
+// plus the neighbour-list skin, so that the 27 cells around a body hold every body closer than
+// r_i + r_j + skin; grown if the grid would be much larger than the body count.
+void plan_cells(Ctx *c, double skin) {
+    int64_t base = 0;
+    for (int s = 0; s < c->nscenes; ++s) {
+        SceneInfo &si = c->scenes[s];
+        const double *lo = &c->plan_bounds[6 * s], *hi = &c->plan_bounds[6 * s + 3];
+        double h = (2.0 * (c->plan_rmax[s] + kContactThreshold) + std::max(skin, 0.0)) * (1.0 + 1e-9);
         int64_t dim[3], nc;
-        const int64_t cap = 8 * std::max<int64_t>(count[s], 1) + 4096;
+        const int64_t cap = 8 * std::max<int64_t>(c->plan_count[s], 1) + 4096;
         for (;;) {
             nc = 1;
             for (int a = 0; a < 3; ++a) {
@@ -262,14 +290,29 @@ void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int6
         si.h = h;
         si.inv_h = 1.0 / h;
         si.cell_base = base;
-        si.body_begin = begin[s];
-        si.nbodies = count[s];
         base += nc;
     }
     c->ncell = base;
 }
 
-}  // namespace
+
+}  // namespace peb
+
+namespace peb {
+
+int run_steps(Ctx *c, int32_t nsteps, double dt) {
+    int32_t k = 0;
+    if (c->p.solver == PE_B200_DEM && c->nl.enabled && !c->prof) {
+        int rc = dem_list_graph_run(c, nsteps, dt, &k);
+        if (rc) return rc;
+    }
+    for (; k < nsteps; ++k) {
+        const int rc = (c->p.solver != PE_B200_DEM) ? nbgs_step(c, dt)
+                       : (c->nl.enabled ? dem_list_step(c, dt) : dem_step(c, dt));
+        if (rc) return rc;
+    }
+    return PE_B200_OK;
+}
 
 }  // namespace peb
 
@@ -351,6 +394,7 @@ int pe_b200_set_gravity(pe_b200_ctx *h, const double g[3]) {
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c || !g) return PE_B200_ERR_ARG;
     for (int a = 0; a < 3; ++a) c->p.gravity[a] = g[a];
+    c->epoch++;
     return PE_B200_OK;
 }
 
@@ -360,6 +404,7 @@ int pe_b200_set_damping(pe_b200_ctx *h, double d) {
     // World::setDamping, pe/core/World.h:767 (valid range [0, 1])
     if (d < 0.0 || d > 1.0) return set_err(c, PE_B200_ERR_ARG, "Invalid damping value");
     c->p.damping = d;
+    c->epoch++;
     return PE_B200_OK;
 }
 
@@ -400,6 +445,7 @@ int pe_b200_set_materials(pe_b200_ctx *h, int32_t n, const pe_b200_material *m) 
     for (int32_t k = 0; k < n; ++k)
         if (check_material(m[k], why)) return set_err(c, PE_B200_ERR_ARG, why);
     c->mats.assign(m, m + n);
+    c->epoch++;
     if (c->uploaded) {
         cudaSetDevice(c->device);
         return upload_tables(c);
@@ -443,6 +489,7 @@ int pe_b200_set_walls(pe_b200_ctx *h, int32_t scene, int32_t nplanes, const doub
     c->scene_plane_mat[scene].assign(plane_mat, plane_mat + nplanes);
     c->scene_boxes[scene].assign(boxes, boxes + 15 * (size_t)nboxes);
     c->scene_box_mat[scene].assign(box_mat, box_mat + nboxes);
+    c->epoch++;
     if (c->uploaded) {
         cudaSetDevice(c->device);
         return upload_tables(c);
@@ -471,6 +518,7 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
                 return set_err(c, PE_B200_ERR_NAN, "non-finite body state");
     }
     free_device(c);
+    c->epoch++;
     c->n = n;
     c->nscenes = nscenes;
     c->scenes.assign(nscenes, SceneInfo());
@@ -486,7 +534,13 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
         std::vector<int64_t> fill(begin);
         for (int64_t i = 0; i < n; ++i) order[fill[scene ? scene[i] : 0]++] = i;
     }
-    plan_grids(c, x, r, order, begin, count);
+    const bool lists = c->p.solver == PE_B200_DEM && c->p.neighbor_lists && n > 0;
+    if (lists) {
+        double rmin = INFINITY;
+        for (int64_t i = 0; i < n; ++i) rmin = std::min(rmin, r[i]);
+        c->nl.skin = c->p.skin > 0.0 ? c->p.skin : 0.1 * rmin;
+    }
+    plan_grids(c, x, r, order, begin, count, lists ? c->nl.skin : 0.0);
     if (c->ncell > (int64_t)INT32_MAX / 2) return set_err(c, PE_B200_ERR_CAPACITY, "grid too large");
     int rc = upload_tables(c);
     if (rc) return rc;
@@ -532,10 +586,7 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
     }
     c->uploaded = true;
     c->binned = false;
-    if (c->p.solver == PE_B200_DEM && c->p.neighbor_lists && n > 0) {
-        double rmin = INFINITY;
-        for (int64_t i = 0; i < n; ++i) rmin = std::min(rmin, r[i]);
-        c->nl.skin = c->p.skin > 0.0 ? c->p.skin : 0.1 * rmin;
+    if (lists) {
         rc = dem_list_alloc(c);
         if (rc) return rc;
     }
@@ -589,12 +640,52 @@ int pe_b200_step(pe_b200_ctx *h, int32_t nsteps, double dt) {
     if (nsteps < 0) return PE_B200_ERR_ARG;
     if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
     cudaSetDevice(c->device);
-    for (int32_t k = 0; k < nsteps; ++k) {
-        const int rc = (c->p.solver != PE_B200_DEM) ? nbgs_step(c, dt)
-                       : (c->nl.enabled ? dem_list_step(c, dt) : dem_step(c, dt));
-        if (rc) return rc;
-    }
+    return run_steps(c, nsteps, dt);
+}
+
+int pe_b200_set_graph_steps(pe_b200_ctx *h, int32_t steps) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || steps < 0) return PE_B200_ERR_ARG;
+    c->graph_steps = steps & ~1;
+    c->sg.failed = false;
+    dem_graph_free(c);
     return PE_B200_OK;
+}
+
+int pe_b200_graph_active(const pe_b200_ctx *h) {
+    const Ctx *c = reinterpret_cast<const Ctx *>(h);
+    return (c && c->sg.exec && !c->sg.failed) ? 1 : 0;
+}
+
+int pe_b200_get_tuning(pe_b200_ctx *h, pe_b200_tuning *out) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !out) return PE_B200_ERR_ARG;
+    out->dem_variant = c->tune.dem_variant;
+    out->rebuild_per_sm = c->tune.rebuild_per_sm;
+    out->skin = c->nl.skin;
+    out->ms_per_step = -1.0;
+    out->variants = dem_variant_count();
+    out->reserved = 0;
+    return PE_B200_OK;
+}
+
+int pe_b200_set_tuning(pe_b200_ctx *h, const pe_b200_tuning *t) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !t) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    cudaSetDevice(c->device);
+    Tuning tu;
+    tu.dem_variant = t->dem_variant;
+    tu.rebuild_per_sm = t->rebuild_per_sm;
+    return set_tuning(c, tu, c->nl.enabled ? t->skin : c->nl.skin);
+}
+
+int pe_b200_autotune(pe_b200_ctx *h, double dt, int32_t trial_steps, pe_b200_tuning *out) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    cudaSetDevice(c->device);
+    return autotune(c, dt, trial_steps, out);
 }
 
 static int check_device_errors(Ctx *c) {

@@ -1,0 +1,171 @@
+// autotune.cu -- launch-shape autotuner of the DEM list step (no pe counterpart: pe runs one
+// fixed serial loop).
+//
+// The tunables change only how the work is laid out on the GPU, never which pairs a body sums
+// or in which order, except for the skin, which changes when the state is re-sorted and so the
+// last bits of the forces:
+//   dem_variant     threads per block / resident blocks per SM of k_dem_list (dem.cu)
+//   rebuild_per_sm  CTAs per SM of the persistent rebuild kernel (rebuild.cu)
+//   skin            neighbour-list skin (cells are re-planned to 2 r_max + skin)
+// Each trial restores the state saved at entry, forces a list rebuild, runs a few untimed steps
+// (graph capture included), then times `trial` steps with CUDA events after forcing one more
+// rebuild, so a trial's time charges at least one rebuild per `trial` steps.  Coordinate
+// descent: skin first, then the force kernel's shape, then the rebuild grid.
+#include <algorithm>
+#include <cmath>
+
+#include "internal.cuh"
+
+namespace peb {
+
+namespace {
+
+void free_snap(BodyBuf &b) {
+    cudaFree(b.pr);
+    cudaFree(b.vw);
+    cudaFree(b.tag);
+    cudaFree(b.uid);
+    cudaFree(b.q);
+    b = BodyBuf();
+}
+
+int copy_bodies(Ctx *c, BodyBuf &dst, const BodyBuf &src) {
+    const size_t n = (size_t)c->n;
+    PEB_CUDA(c, cudaMemcpyAsync(dst.pr, src.pr, n * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+    PEB_CUDA(c, cudaMemcpyAsync(dst.vw, src.vw, n * (size_t)c->vw_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    PEB_CUDA(c, cudaMemcpyAsync(dst.tag, src.tag, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
+    PEB_CUDA(c, cudaMemcpyAsync(dst.uid, src.uid, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    if (src.q && dst.q)
+        PEB_CUDA(c, cudaMemcpyAsync(dst.q, src.q, n * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+    return PE_B200_OK;
+}
+
+}  // namespace
+
+// New skin: re-plans the cells so the 27-cell search still covers r_i + r_j + skin, and asks
+// for a list rebuild.
+int set_list_skin(Ctx *c, double skin) {
+    if (!(skin > 0.0) || !std::isfinite(skin)) return set_err(c, PE_B200_ERR_ARG, "invalid skin");
+    if (skin == c->nl.skin) return PE_B200_OK;
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->nl.skin = skin;
+    plan_cells(c, skin);
+    cudaFree(c->cell_count);
+    cudaFree(c->cell_start);
+    c->cell_count = c->cell_start = nullptr;
+    PEB_CUDA(c, cudaMalloc(&c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemset(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t)));
+    int rc = upload_tables(c);
+    if (rc) return rc;
+    c->binned = false;
+    c->epoch++;
+    return dem_list_request_rebuild(c);
+}
+
+int set_tuning(Ctx *c, const Tuning &t, double skin) {
+    if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < 0)
+        return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
+    if (t.dem_variant != c->tune.dem_variant || t.rebuild_per_sm != c->tune.rebuild_per_sm) {
+        c->tune = t;
+        c->epoch++;
+        // the rebuild grid may grow: its per-block buffer is allocated outside any capture
+        c->nl.warm = false;
+    }
+    if (c->nl.enabled) return set_list_skin(c, skin);
+    return PE_B200_OK;
+}
+
+int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
+    if (c->p.solver != PE_B200_DEM || !c->nl.enabled || c->n == 0)
+        return set_err(c, PE_B200_ERR_UNSUPPORTED, "the autotuner tunes the DEM neighbour-list step");
+    if (!(dt > 0.0) || trial < 2) return PE_B200_ERR_ARG;
+    BodyBuf snap;
+    const size_t n = (size_t)c->n;
+    cudaError_t e = cudaMalloc(&snap.pr, n * sizeof(double4));
+    if (e == cudaSuccess) e = cudaMalloc(&snap.vw, n * (size_t)c->vw_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&snap.tag, n * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&snap.uid, n * sizeof(int32_t));
+    if (e == cudaSuccess && c->cur.q) e = cudaMalloc(&snap.q, n * sizeof(double4));
+    if (e != cudaSuccess) {
+        free_snap(snap);
+        return cuda_err(c, e, "autotune snapshot");
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = copy_bodies(c, snap, c->cur);
+    const Tuning t0 = c->tune;
+    const double skin0 = c->nl.skin;
+    const bool prof0 = c->prof;
+    c->prof = false;
+    const int32_t warm = std::max<int32_t>(2, trial / 4);
+
+    auto measure = [&](const Tuning &t, double skin, double *ms) -> int {
+        int r = copy_bodies(c, c->cur, snap);
+        if (!r) r = set_tuning(c, t, skin);
+        if (!r) r = dem_list_request_rebuild(c);
+        if (!r) r = run_steps(c, warm, dt);
+        if (!r) r = dem_list_request_rebuild(c);
+        if (r) return r;
+        PEB_CUDA(c, cudaEventRecord(e0, c->stream));
+        r = run_steps(c, trial, dt);
+        if (r) return r;
+        PEB_CUDA(c, cudaEventRecord(e1, c->stream));
+        PEB_CUDA(c, cudaEventSynchronize(e1));
+        float f = 0.f;
+        PEB_CUDA(c, cudaEventElapsedTime(&f, e0, e1));
+        *ms = (double)f / trial;
+        return PE_B200_OK;
+    };
+
+    Tuning best = t0;
+    double best_skin = skin0, best_ms = INFINITY;
+    auto consider = [&](const Tuning &t, double skin) -> int {
+        double ms = INFINITY;
+        int r = measure(t, skin, &ms);
+        if (r) return r;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+            best_skin = skin;
+        }
+        return PE_B200_OK;
+    };
+    if (!rc) rc = consider(t0, skin0);
+    for (double f : {0.5, 1.5, 2.0, 3.0})
+        if (!rc) rc = consider(best, skin0 * f);
+    for (int v = 0; v < dem_variant_count() && !rc; ++v) {
+        if (v == best.dem_variant) continue;
+        Tuning t = best;
+        t.dem_variant = v;
+        rc = consider(t, best_skin);
+    }
+    for (int r : {1, 2, 4, 0}) {
+        if (rc || r == best.rebuild_per_sm) continue;
+        Tuning t = best;
+        t.rebuild_per_sm = r;
+        rc = consider(t, best_skin);
+    }
+    // leave the state as it was at entry, with the winning shapes
+    if (!rc) rc = copy_bodies(c, c->cur, snap);
+    if (!rc) rc = set_tuning(c, best, best_skin);
+    if (!rc) rc = dem_list_request_rebuild(c);
+    cudaStreamSynchronize(c->stream);
+    c->prof = prof0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    free_snap(snap);
+    if (rc) return rc;
+    if (out) {
+        out->dem_variant = best.dem_variant;
+        out->rebuild_per_sm = best.rebuild_per_sm;
+        out->skin = best_skin;
+        out->ms_per_step = best_ms;
+        out->variants = dem_variant_count();
+        out->reserved = 0;
+    }
+    return PE_B200_OK;
+}
+
+}  // namespace peb

@@ -377,9 +377,22 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     a.rank[t] = atomicAdd(&a.cell_count[kk], 1);
 }
 
+// launch shapes of the list step kernel: threads per block and the resident blocks per SM the
+// register allocation must allow, for FP32 and FP64 velocities (pe_b200_autotune picks one)
+struct DemShape {
+    int block, minb_f32, minb_f64;
+};
+constexpr DemShape kDemShapes[] = {{kDemBlock, PEB_LIST_MIN_BLOCKS_F32, 5},
+                                   {256, 3, 2},
+                                   {64, 14, 10},
+                                   {128, 8, 6},
+                                   {128, 6, 4},
+                                   {256, 4, 3}};
+constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]));
+
 // list step: body t stays at index t (the order changes only at rebuilds)
-template <typename VT, bool TRACKQ>
-__global__ void __launch_bounds__(kDemBlock, sizeof(VT) == 4 ? PEB_LIST_MIN_BLOCKS_F32 : 5) k_dem_list(DemArgs<VT> a) {
+template <typename VT, bool TRACKQ, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool use_grid = a.nl_flags[1] != 0;   // this step's rebuild overflowed the lists
@@ -644,6 +657,14 @@ int list_rebuild(Ctx *c) {
     return PE_B200_OK;
 }
 
+template <typename VT, bool TRACKQ, int V>
+void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
+    static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
+    constexpr int B = kDemShapes[V].block;
+    constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
+    k_dem_list<VT, TRACKQ, B, M><<<grid_for(c->n, B), B, 0, c->stream>>>(a);
+}
+
 template <typename VT>
 int list_step(Ctx *c, double dt) {
     ListBuf &L = c->nl;
@@ -668,9 +689,16 @@ int list_step(Ctx *c, double dt) {
     a.sorted = nullptr;   // the grid fallback sees the state in cell order
     prof_begin(c, ST_DEM);
     if (c->p.track_orientation)
-        k_dem_list<VT, true><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
+        launch_list_shape<VT, true, 0>(c, a);
     else
-        k_dem_list<VT, false><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
+        switch (c->tune.dem_variant) {
+            case 1: launch_list_shape<VT, false, 1>(c, a); break;
+            case 2: launch_list_shape<VT, false, 2>(c, a); break;
+            case 3: launch_list_shape<VT, false, 3>(c, a); break;
+            case 4: launch_list_shape<VT, false, 4>(c, a); break;
+            case 5: launch_list_shape<VT, false, 5>(c, a); break;
+            default: launch_list_shape<VT, false, 0>(c, a); break;
+        }
     PEB_LAUNCHED(c);
     prof_end(c, ST_DEM);
     // positions/velocities/orientations double-buffered; tag and uid stay where they are
@@ -722,11 +750,13 @@ int dem_list_alloc(Ctx *c) {
     if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&L.tmp.q, n * sizeof(double4)));
     L.enabled = true;
     L.check_pending = false;
+    L.warm = false;
     return dem_list_request_rebuild(c);
 }
 
 void dem_list_free(Ctx *c) {
     ListBuf &L = c->nl;
+    dem_graph_free(c);
     if (L.check_pending && L.ev) cudaEventSynchronize(L.ev);
     cudaFree(L.rb_bar);
     cudaFree(L.rb_blk);
@@ -753,10 +783,12 @@ int dem_list_request_rebuild(Ctx *c) {
     return PE_B200_OK;
 }
 
-int dem_list_step(Ctx *c, double dt) {
+namespace {
+
+// capacity check of an earlier step, without waiting for the device: a rebuild whose lists did
+// not fit (the step then searched the grid) grows the list buffer and asks for a new rebuild
+int list_capacity_check(Ctx *c) {
     ListBuf &L = c->nl;
-    if (c->n == 0) return PE_B200_OK;
-    // capacity check of an earlier step, without waiting for the device
     if (L.check_pending && cudaEventQuery(L.ev) == cudaSuccess) {
         L.check_pending = false;
         if (L.h_flags[1]) {
@@ -767,12 +799,17 @@ int dem_list_step(Ctx *c, double dt) {
             L.idx = nullptr;
             PEB_CUDA(c, cudaMalloc(&L.idx, (size_t)cap * sizeof(int32_t)));
             L.cap = cap;
+            c->epoch++;
             int rc = dem_list_request_rebuild(c);
             if (rc) return rc;
         }
     }
-    int rc = (c->p.precision == PE_B200_FP64) ? list_step<double>(c, dt) : list_step<float>(c, dt);
-    if (rc) return rc;
+    return PE_B200_OK;
+}
+
+// queues the read-back of the rebuild flags that list_capacity_check looks at
+int list_queue_check(Ctx *c) {
+    ListBuf &L = c->nl;
     if (!L.check_pending) {
         PEB_CUDA(c, cudaMemcpyAsync(L.h_flags, L.flags, 4 * sizeof(int32_t),
                                     cudaMemcpyDeviceToHost, c->stream));
@@ -781,6 +818,115 @@ int dem_list_step(Ctx *c, double dt) {
     }
     return PE_B200_OK;
 }
+
+int list_step_any(Ctx *c, double dt) {
+    return (c->p.precision == PE_B200_FP64) ? list_step<double>(c, dt) : list_step<float>(c, dt);
+}
+
+void graph_key(const Ctx *c, const void *key[12]) {
+    const void *k[12] = {c->cur.pr, c->cur.vw, c->cur.q, c->cur.tag, c->cur.uid, c->nxt.pr,
+                         c->nxt.vw, c->nxt.q, c->nl.idx, (const void *)(intptr_t)c->nl.cap,
+                         (const void *)(intptr_t)c->n, c->nl.rb_blk};
+    for (int i = 0; i < 12; ++i) key[i] = k[i];
+}
+
+// Captures steps list steps into c->sg.  Nothing runs on the device during a capture, so a
+// failed capture leaves the context exactly as it was and only switches graphs off.
+int capture_steps(Ctx *c, int32_t steps, double dt) {
+    StepGraph &G = c->sg;
+    dem_graph_free(c);
+    const BodyBuf cur0 = c->cur, nxt0 = c->nxt;
+    const bool coop0 = c->nl.coop_disabled;
+    const int64_t l0 = c->launches;
+    const void *key[12];
+    graph_key(c, key);
+    cudaGraph_t g = nullptr;
+    int rc = PE_B200_OK;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int32_t k = 0; k < steps && rc == PE_B200_OK; ++k) rc = list_step_any(c, dt);
+        const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+        if (e == cudaSuccess) e = e2;
+    }
+    const int64_t per_replay = c->launches - l0;
+    c->launches = l0;
+    bool ok = e == cudaSuccess && rc == PE_B200_OK && g != nullptr &&
+              c->nl.coop_disabled == coop0 && c->cur.pr == cur0.pr && c->cur.vw == cur0.vw;
+    if (ok) ok = cudaGraphInstantiate(&G.exec, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+        if (G.exec) cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
+        G.failed = true;
+        c->cur = cur0;
+        c->nxt = nxt0;
+        c->nl.coop_disabled = coop0;
+        cudaGetLastError();
+        c->err.clear();
+        return PE_B200_OK;
+    }
+    G.steps = steps;
+    G.dt = dt;
+    G.epoch = c->epoch;
+    for (int i = 0; i < 12; ++i) G.key[i] = key[i];
+    G.launches = per_replay;
+    return PE_B200_OK;
+}
+
+}  // namespace
+
+int dem_list_step(Ctx *c, double dt) {
+    if (c->n == 0) return PE_B200_OK;
+    int rc = list_capacity_check(c);
+    if (rc) return rc;
+    rc = list_step_any(c, dt);
+    if (rc) return rc;
+    c->nl.warm = true;
+    return list_queue_check(c);
+}
+
+void dem_graph_free(Ctx *c) {
+    if (c->sg.exec) cudaGraphExecDestroy(c->sg.exec);
+    c->sg.exec = nullptr;
+    c->sg.steps = 0;
+}
+
+int dem_list_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *done) {
+    *done = 0;
+    StepGraph &G = c->sg;
+    // an even count: the buffer swaps of one replay cancel, so every replay starts on the
+    // buffers the graph was captured on
+    const int32_t gs = c->graph_steps & ~1;
+    if (c->n == 0 || gs < 2 || G.failed) return PE_B200_OK;
+    while (nsteps - *done >= gs) {
+        int rc = list_capacity_check(c);
+        if (rc) return rc;
+        if (!c->nl.warm) {
+            // first step on fresh buffers: allocations happen outside any capture
+            rc = dem_list_step(c, dt);
+            if (rc) return rc;
+            ++*done;
+            continue;
+        }
+        const void *key[12];
+        graph_key(c, key);
+        bool match = G.exec && G.steps == gs && G.dt == dt && G.epoch == c->epoch;
+        for (int i = 0; i < 12 && match; ++i) match = G.key[i] == key[i];
+        if (!match) {
+            rc = capture_steps(c, gs, dt);
+            if (rc) return rc;
+            if (G.failed) return PE_B200_OK;
+        }
+        PEB_CUDA(c, cudaGraphLaunch(G.exec, c->stream));
+        c->launches += G.launches;
+        *done += gs;
+        rc = list_queue_check(c);
+        if (rc) return rc;
+    }
+    return PE_B200_OK;
+}
+
+int dem_variant_count() { return kDemShapeCount; }
 
 // Launches the FP64 step kernel on caller-provided buffers (used by the allocation-free entry
 // point in noalloc.cu); every pointer is device memory the caller owns.

@@ -95,6 +95,25 @@ struct ListBuf {
     int32_t *rb_blk = nullptr;
     int64_t rb_blk_cap = 0;
     bool coop_disabled = false;
+    bool warm = false;          // a list step has run since the buffers were (re)allocated
+};
+
+// launch shapes of the DEM list step, picked by pe_b200_autotune (autotune.cu)
+struct Tuning {
+    int32_t dem_variant = 0;    // index into the k_dem_list launch shapes (dem.cu)
+    int32_t rebuild_per_sm = 0; // persistent rebuild CTAs per SM; 0 = as many as fit
+};
+
+// a captured CUDA graph of `steps` DEM list steps (dem.cu); valid while the buffers it was
+// captured on and the context's parameter epoch are unchanged
+struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int32_t steps = 0;
+    double dt = 0.0;
+    uint64_t epoch = 0;
+    const void *key[12] = {};
+    int64_t launches = 0;       // kernels per replay
+    bool failed = false;        // capture not possible here: plain launches from now on
 };
 
 // checkpoints of the adjoint's forward run (adjoint.cu)
@@ -134,6 +153,9 @@ struct Ctx {
     std::vector<std::vector<double>> scene_planes, scene_boxes;
     std::vector<std::vector<int32_t>> scene_plane_mat, scene_box_mat;
     std::vector<SceneInfo> scenes;
+    std::vector<double> plan_bounds;  // per scene: lo xyz, hi xyz of the grid (plan_grids)
+    std::vector<double> plan_rmax;
+    std::vector<int64_t> plan_count;
 
     // device
     int64_t n = 0;                  // bodies
@@ -159,6 +181,10 @@ struct Ctx {
     NbgsBuf nb;
     ListBuf nl;
     AdjState adj;
+    Tuning tune;
+    StepGraph sg;
+    int32_t graph_steps = 16;       // DEM list steps per graph replay; 0 = no graphs
+    uint64_t epoch = 1;             // bumped by every change that captured kernels bake in
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -245,6 +271,20 @@ void dem_list_free(Ctx *c);
 int dem_list_request_rebuild(Ctx *c);
 int dem_list_rebuild_persistent(Ctx *c);
 int dem_list_step(Ctx *c, double dt);
+// runs whole graph replays of c->graph_steps list steps while they fit in nsteps; *done
+// receives the steps run (0 when graphs are off or not possible)
+int dem_list_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *done);
+void dem_graph_free(Ctx *c);
+int dem_variant_count();
+// cells of every scene for neighbour-list skin `skin` (abi.cu)
+void plan_cells(Ctx *c, double skin);
+int upload_tables(Ctx *c);
+// pe_b200_step's loop, shared with the autotuner
+int run_steps(Ctx *c, int32_t nsteps, double dt);
+// autotune.cu
+int set_list_skin(Ctx *c, double skin);
+int set_tuning(Ctx *c, const Tuning &t, double skin);
+int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out);
 int dem_step(Ctx *c, double dt);
 int adjoint_forward(Ctx *c, int32_t nsteps, double dt, int32_t every);
 int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *gw, double *ox,

@@ -237,7 +237,8 @@ int launch_rebuild(Ctx *c) {
         if (occ < 1) return set_err(c, PE_B200_ERR_CUDA, "rebuild kernel cannot be resident");
     }
     const int64_t want = std::max<int64_t>(1, (c->n + kRbBlock - 1) / kRbBlock);
-    const unsigned grid = (unsigned)std::min<int64_t>(want, (int64_t)occ * c->sm_count);
+    const int per_sm = c->tune.rebuild_per_sm > 0 ? std::min(occ, c->tune.rebuild_per_sm) : occ;
+    const unsigned grid = (unsigned)std::min<int64_t>(want, (int64_t)per_sm * c->sm_count);
     if (L.rb_blk_cap < (int64_t)grid + 1) {
         cudaFree(L.rb_blk);
         L.rb_blk = nullptr;

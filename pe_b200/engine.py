@@ -208,6 +208,29 @@ class Engine:
                                                      _p(ov), _p(ow), _p(gp)))
         return ox, ov, ow, gp
 
+    def set_graph_steps(self, steps: int):
+        """DEM list steps per CUDA-graph replay (0 = launch every step)."""
+        self._check(self._L.pe_b200_set_graph_steps(self._h, int(steps)))
+
+    def graph_active(self) -> bool:
+        return bool(self._L.pe_b200_graph_active(self._h))
+
+    def tuning(self) -> dict:
+        t = _abi.Tuning()
+        self._check(self._L.pe_b200_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_ if k != "reserved"}
+
+    def set_tuning(self, dem_variant: int, rebuild_per_sm: int, skin: float):
+        t = _abi.Tuning(dem_variant=dem_variant, rebuild_per_sm=rebuild_per_sm, skin=skin)
+        self._check(self._L.pe_b200_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, dt: float, trial_steps: int = 100) -> dict:
+        """Times candidate launch shapes and skins from the current state and keeps the fastest
+        (the state is restored)."""
+        t = _abi.Tuning()
+        self._check(self._L.pe_b200_autotune(self._h, float(dt), int(trial_steps), C.byref(t)))
+        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_ if k != "reserved"}
+
     def neighbor_list_stats(self) -> dict:
         r, e, c = C.c_int64(), C.c_int64(), C.c_int64()
         sk = C.c_double()

@@ -1,0 +1,105 @@
+"""CUDA-graph replay and the launch-shape autotuner of the DEM neighbour-list step: neither may
+change results (the skin may change the last bits), and the lists must hold every pair that can
+touch before the next rebuild."""
+import numpy as np
+import pytest
+
+from helpers import rel_err
+from pe_b200 import _abi, scenes
+from pe_b200.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def run(s, precision, steps, graph_steps=16, tuning=None, scenes_list=None):
+    e = Engine(solver=_abi.DEM, precision=precision)
+    if scenes_list:
+        e.load_scenes(scenes_list)
+    else:
+        e.load_scene(s)
+    e.set_graph_steps(graph_steps)
+    if tuning is not None:
+        e.set_tuning(*tuning)
+    e.step(s.dt, steps)
+    out = e.download()
+    active = e.graph_active()
+    e.close()
+    return out, active
+
+
+@pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
+def test_graph_replay_matches_step_by_step(precision):
+    s = scenes.dem_lattice(0, side=12)
+    (x0, v0, w0), a0 = run(s, precision, 53, graph_steps=0)
+    (x1, v1, w1), a1 = run(s, precision, 53, graph_steps=16)
+    assert not a0 and a1
+    assert np.array_equal(x0, x1) and np.array_equal(v0, v1) and np.array_equal(w0, w1)
+
+
+def test_graph_replay_batched_scenes():
+    ss = [scenes.small_random(s, n=64 + 16 * s, with_boxes=bool(s % 2)) for s in range(6)]
+    for s in ss:
+        s.dt = ss[0].dt
+    (x0, v0, w0), _ = run(ss[0], _abi.MIXED, 40, graph_steps=0, scenes_list=ss)
+    (x1, v1, w1), a1 = run(ss[0], _abi.MIXED, 40, graph_steps=8, scenes_list=ss)
+    assert a1
+    assert np.array_equal(x0, x1) and np.array_equal(v0, v1)
+
+
+def test_launch_shapes_do_not_change_results():
+    s = scenes.dem_lattice(1, side=10)
+    e = Engine(solver=_abi.DEM, precision=_abi.MIXED).load_scene(s)
+    skin = e.tuning()["skin"]
+    nvar = e.tuning()["variants"]
+    e.close()
+    ref, _ = run(s, _abi.MIXED, 30)
+    for v in range(nvar):
+        for rb in (0, 1, 3):
+            out, _ = run(s, _abi.MIXED, 30, tuning=(v, rb, skin))
+            for a, b in zip(out, ref):
+                assert np.array_equal(a, b), (v, rb)
+
+
+def test_autotune_restores_state_and_keeps_physics():
+    s = scenes.dem_lattice(2, side=12)
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(s)
+    e.step(s.dt, 20)
+    before = e.download()
+    t = e.autotune(s.dt, 40)
+    after = e.download()
+    for a, b in zip(before, after):
+        assert np.array_equal(a, b)
+    assert 0 <= t["dem_variant"] < t["variants"] and t["rebuild_per_sm"] >= 0
+    assert t["skin"] > 0 and t["ms_per_step"] > 0
+    e.step(s.dt, 60)
+    x, v, w = e.download()
+    e.close()
+    g = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(s)
+    g.step(s.dt, 80)
+    xg, vg, wg = g.download()
+    g.close()
+    assert rel_err(x, xg) < 1e-12
+    assert rel_err(v, vg) < 1e-9
+
+
+@pytest.mark.parametrize("skin", [0.0, 0.2])
+def test_lists_cover_pairs_beyond_one_cell(skin):
+    """Two spheres 0.04 apart sit two grid cells apart along x when the cells are only 2 r_max
+    wide; they close the gap before either has moved skin/2, so the list built at the start must
+    already hold the pair (the cells are 2 r_max + skin wide)."""
+    r = 0.5
+    x = np.array([[1.99, 5.0, 5.0], [3.03, 5.0, 5.0]])
+    v = np.array([[0.5, 0.0, 0.0], [-0.5, 0.0, 0.0]])
+    s = scenes._scene(x, v, np.full(2, r), np.zeros(2, np.int64), scenes.box_planes([0, 0, 0], [10, 10, 10]),
+                      np.zeros(6, np.int64), np.zeros((0, 15)), np.zeros(0), [scenes.material(1.0, 1e5, 50.0, 40.0, 0.3)],
+                      (0.0, 0.0, 0.0), 1e-4, 600, "gap_pair")
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64, skin=skin).load_scene(s)
+    e.step(s.dt, 600)
+    xl, vl, _ = e.download()
+    e.close()
+    g = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(s)
+    g.step(s.dt, 600)
+    xg, vg, _ = g.download()
+    g.close()
+    assert vg[0, 0] < 0.4   # the pair did collide
+    assert rel_err(xl, xg) < 1e-12 and rel_err(vl, vg) < 1e-10
