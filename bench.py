@@ -49,10 +49,15 @@ def parse():
     ap.add_argument("--workload", default="dem_large_1m",
                     choices=["dem_large_1m", "dem_lattice_4096", "nbgs_box_32768", "ensemble_512"])
     ap.add_argument("--no-extras", action="store_true", help="headline measurement only")
+    ap.add_argument("--tuning", default=None,
+                    help="dem_variant,rebuild_per_sm,skin instead of running the autotuner")
     return ap.parse_args()
 
 
-def build_workload(name, seed=0):
+def build_workload(name, seed=0, rank=0, world=1):
+    """The scenes this rank advances.  A single scene is replicated on every rank; the batched
+    ensemble is partitioned by scene (largest first onto the least-loaded rank), so the ranks
+    share one fixed job and exchange nothing."""
     if name == "dem_large_1m":
         return [scenes.dem_large(seed)], "dem"
     if name == "dem_lattice_4096":
@@ -60,8 +65,19 @@ def build_workload(name, seed=0):
     if name == "nbgs_box_32768":
         return [scenes.nbgs_box(seed)], "hcsits"
     if name == "ensemble_512":
-        return scenes.batched_ensemble(seed), "dem"
+        return shard_scenes(scenes.batched_ensemble(seed), rank, world), "dem"
     raise ValueError(name)
+
+
+def shard_scenes(ss, rank, world):
+    load = [0] * world
+    mine = []
+    for k in sorted(range(len(ss)), key=lambda k: (-ss[k].n, k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += ss[k].n
+        if r == rank:
+            mine.append(ss[k])
+    return mine
 
 
 # ------------------------------------------------------------------------------------------
@@ -115,6 +131,59 @@ def run_reference(workload, steps, warmup=1, budget_s=60.0):
         res["sample"] = f"{sample}; {k} timed steps after {warmup} warm-up"
         res["cores"] = 1
         return res, None
+
+
+def run_reference_parallel(workload, steps, budget_s=60.0):
+    """pe is single-threaded, so the host's throughput is that of independent processes, one
+    per core: each runs its own sample of the workload (as many as the cores and half the free
+    memory allow) and the sphere-steps/s add up."""
+    if workload == "dem_large_1m":
+        n = 65536
+        side = 200.0 * (n / 1048576) ** 0.5
+        samples = [scenes.dem_large(0, n=n, dims=(side, side, 400.0))]
+        exe, what = "ref_dem", f"{n} spheres of the 1M DEM scene's packing ({side:.0f}x{side:.0f} footprint)"
+    else:
+        sc, exe, what = ref_sample_scene(workload)
+        samples = [sc]
+    path = os.path.join(REF_DIR, exe)
+    if not os.path.exists(path):
+        return None, f"compiled reference missing ({path}); build with make -C oracle/ref"
+    cores = os.cpu_count() or 1
+    try:
+        avail = int([l for l in open("/proc/meminfo") if l.startswith("MemAvailable")][0].split()[1]) * 1024
+    except (OSError, IndexError, ValueError):
+        avail = 8 << 30
+    with tempfile.TemporaryDirectory() as tmp:
+        extra = ["0", "100"] if exe == "ref_hcsits" else []
+        files = []
+        for k, sc in enumerate(samples[:cores]):
+            sp = os.path.join(tmp, f"scene{k}.bin")
+            sc.save(sp)
+            files.append((sp, sc.n))
+        # probe: one step of the first sample, and its memory
+        import resource
+        t0 = time.perf_counter()
+        r = subprocess.run([path, "time", files[0][0], "0", "1", *extra], capture_output=True, text=True)
+        if r.returncode != 0:
+            return None, "reference run failed: " + r.stderr.strip()[-200:]
+        one = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
+        rss = resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss * 1024
+        procs = max(1, min(cores, int(0.5 * avail / max(rss, 1 << 20))))
+        k = max(1, min(steps, int(budget_s / max(one, 1e-6))))
+        jobs = [subprocess.Popen([path, "time", files[q % len(files)][0], "1", str(k), *extra],
+                                 stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+                for q in range(procs)]
+        res = []
+        for j in jobs:
+            out, err = j.communicate()
+            if j.returncode != 0:
+                return None, "reference run failed: " + err.strip()[-200:]
+            res.append(json.loads(out.strip().splitlines()[-1]))
+        total = sum(x["sphere_steps_per_s"] for x in res)
+        return {"sphere_steps_per_s": total, "steps": k, "seconds": max(x["seconds"] for x in res),
+                "cores": procs, "wall_s": time.perf_counter() - t0,
+                "sample": f"{procs} concurrent single-threaded processes, each {what}; {k} timed "
+                          f"steps after 1 warm-up; host has {cores} cores"}, None
 
 
 # ------------------------------------------------------------------------------------------
@@ -223,6 +292,127 @@ def timed_steps(e, dt, steps, warmup, torch, flush_buf, stream, dist=None):
     return ms, launches, prof
 
 
+def timed_chunks(e, dt, chunks, chunk, warmup, torch, flush_buf, stream):
+    """Steps in chunks of `chunk` (each one CUDA-graph replay), L2 flushed between chunks."""
+    e.set_graph_steps(chunk)
+    e.step(dt, chunk * max(1, warmup))
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(chunks)]
+    l0 = e.kernel_launches()
+    with torch.cuda.stream(stream):
+        for k in range(chunks):
+            flush_buf[0].add_(1)
+            flush_buf[2].add_(flush_buf[1].sum())
+            evs[k][0].record(stream)
+            e.step(dt, chunk)
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs), e.kernel_launches() - l0, e.graph_active()
+
+
+def adjoint_extra(torch):
+    """The differentiable-DEM workload: 16384 spheres in the hopper, 2000 FP64 steps with a
+    checkpoint every 100, gradient of final centre-of-mass height plus mass fraction below the
+    opening w.r.t. all initial velocities and k_n, c_n, mu; and the adjoint of the last 100-step
+    segment against central differences (h = 1e-6) of the GPU step and of the compiled pe."""
+    from pe_b200 import _abi
+    from pe_b200.adjoint import LossSpec, make_single_material, set_params
+    from pe_b200.engine import Engine
+    s0 = scenes.hopper(0)
+    m = s0.materials[0]
+    p = {"k_n": m[6] / 2, "c_n": m[7] / 2, "c_t": m[8] / 2, "mu": 2 * m[2]}
+    s = make_single_material(s0, **p)
+    spec = LossSpec.for_scene(s, z_open=10.0)
+    K, EVERY = s.steps, 100
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e.adjoint_forward(K, s.dt, EVERY)
+    x = e.download()[0]
+    t1 = time.perf_counter()
+    z = np.zeros_like(x)
+    _, gv0, _, gp = e.adjoint_backward(spec.grad(x), z, z)
+    t2 = time.perf_counter()
+    out = {"spheres": s.n, "steps": K, "checkpoint_every": EVERY, "loss": spec.value(x),
+           "forward_ms": 1e3 * (t1 - t0), "backward_ms": 1e3 * (t2 - t1),
+           "grad_params": {"k_n": gp[0], "c_n": gp[1], "c_t": gp[2], "mu": gp[3]},
+           "grad_v0_linf": float(np.abs(gv0).max())}
+    e.close()
+    # the last segment: state after K - 100 steps, adjoint of 100 steps vs central differences
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(s)
+    e.step(s.dt, K - EVERY)
+    xs, vs, ws = e.download()
+    e.close()
+    seg = s.copy()
+    seg.x, seg.v, seg.w = xs, vs, ws
+
+    def gpu_x(t):
+        g = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(t)
+        g.step(t.dt, EVERY)
+        x = g.download()[0]
+        g.close()
+        return x
+
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(seg)
+    e.adjoint_forward(EVERY, s.dt, 10)
+    xe = e.download()[0]
+    _, gvs, _, gps = e.adjoint_backward(spec.grad(xe), z, z)
+    e.close()
+    # velocity components of spheres with the largest adjoint (the ones in contact)
+    flat = np.argsort(-np.abs(gvs).ravel())[:4]
+    idx = [(int(f // 3), int(f % 3)) for f in flat]
+    h = 1e-6
+    fd, fdr = [], []
+    ref = os.path.join(REF_DIR, "ref_dem")
+    have_ref = os.path.exists(ref)
+
+    def ref_x(t, tmp):
+        sp = os.path.join(tmp, "seg.bin")
+        t.save(sp)
+        o = os.path.join(tmp, "o.bin")
+        subprocess.run([ref, "step", sp, str(EVERY), o], check=True)
+        a = np.fromfile(o, "<f8")
+        return a[:3 * t.n].reshape(t.n, 3)
+
+    with tempfile.TemporaryDirectory() as tmp:
+        for (i, a) in idx:
+            sp_, sm_ = seg.copy(), seg.copy()
+            sp_.v[i, a] += h
+            sm_.v[i, a] -= h
+            fd.append(spec.diff(gpu_x(sp_), gpu_x(sm_)) / (2 * h))
+            if have_ref:
+                fdr.append(spec.diff(ref_x(sp_, tmp), ref_x(sm_, tmp)) / (2 * h))
+        pfd, pfdr = {}, {}
+        for key, k, hp in (("k_n", 0, 1e-1), ("c_n", 1, 1e-4), ("mu", 3, 1e-6)):
+            pp, pm = dict(p), dict(p)
+            pp[key] += hp
+            pm[key] -= hp
+            pfd[key] = spec.diff(gpu_x(set_params(seg, **pp)), gpu_x(set_params(seg, **pm))) / (2 * hp)
+            if have_ref:
+                pfdr[key] = spec.diff(ref_x(set_params(seg, **pp), tmp),
+                                      ref_x(set_params(seg, **pm), tmp)) / (2 * hp)
+    ad = np.array([gvs[i, a] for i, a in idx])
+    fd = np.array(fd)
+    rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    segment = {"steps": EVERY, "from_step": K - EVERY, "h": h,
+               "v_components": idx, "adjoint": ad.tolist(), "fd_gpu": fd.tolist(),
+               "rel_err_vs_fd_gpu": rel(ad, fd),
+               "params_adjoint": {"k_n": gps[0], "c_n": gps[1], "mu": gps[3]},
+               "params_fd_gpu": pfd,
+               "params_rel_err_vs_fd_gpu": {k: abs(gps[j] - pfd[k]) / max(abs(pfd[k]), 1e-300)
+                                            for k, j in (("k_n", 0), ("c_n", 1), ("mu", 3))}}
+    if have_ref:
+        fdr = np.array(fdr)
+        segment.update({"fd_reference": fdr.tolist(), "rel_err_vs_fd_reference": rel(ad, fdr),
+                        "params_fd_reference": pfdr,
+                        "params_rel_err_vs_fd_reference": {
+                            k: abs(gps[j] - pfdr[k]) / max(abs(pfdr[k]), 1e-300)
+                            for k, j in (("k_n", 0), ("c_n", 1), ("mu", 3))}})
+    out["segment_check"] = segment
+    return out
+
+
 def our_arm(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -239,7 +429,7 @@ def our_arm(args):
     from pe_b200 import _abi
     from pe_b200.engine import Engine
 
-    ss, kind = build_workload(args.workload)
+    ss, kind = build_workload(args.workload, rank=rank, world=world)
     nsph = sum(s.n for s in ss)
     dt = ss[0].dt
     dev = torch.device("cuda", local)
@@ -248,6 +438,15 @@ def our_arm(args):
              torch.zeros(1, dtype=torch.float32, device=dev))
     precision = _abi.MIXED
     e = make_engine(ss, kind, precision)
+    # launch shapes and skin picked by the library's autotuner from the initial state (untimed;
+    # the state is restored)
+    tuning = None
+    if kind == "dem" and args.tuning:
+        v, r, sk = args.tuning.split(",")
+        e.set_tuning(int(v), int(r), float(sk))
+        tuning = dict(e.tuning(), source="--tuning")
+    elif kind == "dem":
+        tuning = e.autotune(dt, 100)
     stream = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
     uuid = None
     try:
@@ -260,10 +459,13 @@ def our_arm(args):
     ms, launches, prof = timed_steps(e, dt, args.steps, args.warmup, torch, flush, stream, dist)
     clk = clocks.stop()
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    tot = torch.tensor([float(nsph)], dtype=torch.float64, device=dev)
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
     ms_max = float(t.item())
-    value = nsph * args.steps * world / (ms_max / 1e3)
+    total_sph = float(tot.item())
+    value = total_sph * args.steps / (ms_max / 1e3)
 
     # end to end through the public API: host arrays in, K steps, host arrays out
     torch.cuda.synchronize()
@@ -273,6 +475,8 @@ def our_arm(args):
             for s in ss]
     t0 = time.perf_counter()
     e2 = make_engine(ss, kind, precision)
+    if tuning is not None:
+        e2.set_tuning(tuning["dem_variant"], tuning["rebuild_per_sm"], tuning["skin"])
     e2.step(dt, args.steps)
     out = e2.download()
     torch.cuda.synchronize()
@@ -284,7 +488,7 @@ def our_arm(args):
     if dist is not None:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
         dist.barrier()
-    e2e_value = nsph * args.steps * world / float(te.item())
+    e2e_value = total_sph * args.steps / float(te.item())
 
     if dist is not None:
         dist.destroy_process_group()
@@ -320,12 +524,17 @@ def our_arm(args):
                 "algorithmic_bytes_per_launch": algo, "avg_launch_ms": kavg}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong" if args.workload == "ensemble_512" else "weak",
             "vs_baseline": None, "dtype": "f32 (f64 positions)", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "spheres": nsph, "scenes": len(ss),
-                       "precision": "mixed", "dt": dt,
+            "config": {"workload": args.workload, "spheres": int(total_sph),
+                       "spheres_per_rank": nsph, "scenes": len(ss),
+                       "precision": "mixed", "dt": dt, "tuning": tuning,
                        "l2": "flushed between timed steps (256 MiB write + 256 MiB read, untimed)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                       "parallelism": ("1 GPU" if world == 1 else
+                                       f"scenes partitioned over {world} ranks"
+                                       if args.workload == "ensemble_512" else
+                                       f"replicas x{world}")},
             "clocks": clk, "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
@@ -376,17 +585,36 @@ def extras(args, torch, flush, dev, ss, kind, mixed_value):
             "reference": "FP64 GPU path (itself within 1e-12 of pe's FP64 step)"}
         em.close()
         ef.close()
+    if kind == "dem":
+        # the same tuned mixed step through CUDA-graph replays of 16 steps, flushed between
+        # replays (the scene's state and lists, > 126 MB, exceed L2 within a replay as well)
+        e = make_engine(ss, kind, _abi.MIXED)
+        tu = e.autotune(dt, 100)
+        st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+        chunks = max(2, min(args.steps, 400) // 16)
+        ms, launches, active = timed_chunks(e, dt, chunks, 16, 3, torch, flush, st)
+        out["graph_replay_16"] = {"value": nsph * chunks * 16 / (ms / 1e3),
+                                  "ms_per_step": ms / (chunks * 16), "steps": chunks * 16,
+                                  "graph_active": active, "gpu_launches": launches,
+                                  "tuning": tu}
+        e.close()
     if args.workload == "dem_large_1m":
         ens = scenes.batched_ensemble(0)
         ne = sum(s.n for s in ens)
         e = make_engine(ens, "dem", _abi.MIXED)
+        tu = e.autotune(ens[0].dt, 50)
         st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
-        k = 50
+        k = 48
         ms, _, prof = timed_steps(e, ens[0].dt, k, 3, torch, flush, st)
+        msg, _, active = timed_chunks(e, ens[0].dt, 3, 16, 1, torch, flush, st)
         out["ensemble_512"] = {"value": ne * k / (ms / 1e3), "ms_per_step": ms / k,
+                               "graph_replay_16_value": ne * 48 / (msg / 1e3),
+                               "graph_replay_16_ms_per_step": msg / 48, "graph_active": active,
                                "spheres": ne, "scenes": len(ens), "precision": "mixed",
+                               "tuning": tu,
                                "stages_ms_per_step": {a: b[0] / k for a, b in prof.items() if b[1]}}
         e.close()
+        out["adjoint_hopper_16384"] = adjoint_extra(torch)
         for label, sc in (("nbgs_32k", scenes.nbgs_box(0)),
                           ("nbgs_32k_dense", scenes.nbgs_box(0, n=32768, dims=(32.0, 32.0, 120.0),
                                                             dense=True))):
@@ -430,8 +658,7 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    ref, why = run_reference(args.workload, steps=max(1, args.steps), warmup=max(1, min(args.warmup, 3)),
-                             budget_s=90.0)
+    ref, why = run_reference_parallel(args.workload, steps=max(1, args.steps), budget_s=60.0)
     if not ref:
         return {"impl": "reference", "unavailable": why}
     v = ref["sphere_steps_per_s"]
