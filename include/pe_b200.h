@@ -63,7 +63,9 @@ typedef struct {
     double damping;            /* World::setDamping, 1 = no drag (src/core/Settings.cpp:47) */
     int32_t device;            /* CUDA device ordinal */
     int32_t track_orientation; /* 1: integrate sphere quaternions (Default.h:190-193) */
-    int64_t max_contacts;      /* HCSITS contact capacity; 0 = automatic (8 per sphere) */
+    int64_t max_contacts;      /* HCSITS contact capacity; 0 = automatic (8 per sphere).
+                                  DEM lists: initial capacity in entries (grown on demand);
+                                  0 = automatic (16 per sphere) */
     double skin;               /* DEM neighbour-list skin; <= 0: 0.1 x the smallest radius */
     int32_t neighbor_lists;    /* DEM: 1 = Verlet lists rebuilt on demand (default),
                                   0 = grid search every step */

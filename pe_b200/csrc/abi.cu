@@ -169,6 +169,28 @@ int upload_tables(Ctx *c) {
         si.nplanes = (int32_t)(c->scene_planes[s].size() / 4);
         si.box_begin = (int32_t)(c->boxes.size() / 15);
         si.nboxes = (int32_t)(c->scene_boxes[s].size() / 15);
+        // the box inside every plane of the scene, 1e-6 inside each of them
+        for (int a = 0; a < 3; ++a) {
+            si.wall_lo[a] = -INFINITY;
+            si.wall_hi[a] = INFINITY;
+        }
+        const std::vector<double> &sp = c->scene_planes[s];
+        for (size_t q = 0; q + 3 < sp.size(); q += 4) {
+            int axis = -1;
+            for (int a = 0; a < 3; ++a)
+                if (fabs(sp[q + a]) == 1.0 && sp[q + (a + 1) % 3] == 0.0 && sp[q + (a + 2) % 3] == 0.0)
+                    axis = a;
+            if (axis < 0) {
+                for (int a = 0; a < 3; ++a) {
+                    si.wall_lo[a] = INFINITY;
+                    si.wall_hi[a] = -INFINITY;
+                }
+                break;
+            }
+            // n.x = d on the plane, body side n.x > d
+            if (sp[q + axis] > 0) si.wall_lo[axis] = std::max(si.wall_lo[axis], sp[q + 3] + 1e-6);
+            else si.wall_hi[axis] = std::min(si.wall_hi[axis], -sp[q + 3] - 1e-6);
+        }
         c->planes.insert(c->planes.end(), c->scene_planes[s].begin(), c->scene_planes[s].end());
         c->plane_mat.insert(c->plane_mat.end(), c->scene_plane_mat[s].begin(),
                             c->scene_plane_mat[s].end());
@@ -181,16 +203,23 @@ int upload_tables(Ctx *c) {
     cudaFree(c->d_boxes);
     cudaFree(c->d_box_mat);
     c->d_planes = nullptr;
+    c->d_planes_f = nullptr;
     c->d_plane_mat = nullptr;
     c->d_boxes = nullptr;
     c->d_box_mat = nullptr;
     const size_t np = c->planes.size() / 4, nb = c->boxes.size() / 15;
-    PEB_CUDA(c, cudaMalloc(&c->d_planes, std::max<size_t>(np, 1) * sizeof(double4)));
+    // FP64 planes followed by an FP32 copy for the kernels' quick rejection test
+    PEB_CUDA(c, cudaMalloc(&c->d_planes, std::max<size_t>(np, 1) * (sizeof(double4) + sizeof(float4))));
+    c->d_planes_f = reinterpret_cast<float4 *>(c->d_planes + std::max<size_t>(np, 1));
     PEB_CUDA(c, cudaMalloc(&c->d_plane_mat, std::max<size_t>(np, 1) * sizeof(int32_t)));
     PEB_CUDA(c, cudaMalloc(&c->d_boxes, std::max<size_t>(nb, 1) * 15 * sizeof(double)));
     PEB_CUDA(c, cudaMalloc(&c->d_box_mat, std::max<size_t>(nb, 1) * sizeof(int32_t)));
     if (np) {
         PEB_CUDA(c, cudaMemcpy(c->d_planes, c->planes.data(), np * sizeof(double4),
+                               cudaMemcpyHostToDevice));
+        std::vector<float> pf(4 * np);
+        for (size_t k = 0; k < 4 * np; ++k) pf[k] = (float)c->planes[k];
+        PEB_CUDA(c, cudaMemcpy(c->d_planes_f, pf.data(), np * sizeof(float4),
                                cudaMemcpyHostToDevice));
         PEB_CUDA(c, cudaMemcpy(c->d_plane_mat, c->plane_mat.data(), np * sizeof(int32_t),
                                cudaMemcpyHostToDevice));
@@ -289,6 +318,7 @@ void plan_cells(Ctx *c, double skin) {
         }
         si.h = h;
         si.inv_h = 1.0 / h;
+        si.rmax = c->plan_rmax[s];
         si.cell_base = base;
         base += nc;
     }

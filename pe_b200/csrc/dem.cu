@@ -106,6 +106,7 @@ struct DemArgs {
     const SceneInfo *scenes;
     const MatDev *mats;
     const double4 *planes;
+    const float4 *planes_f;   // FP32 copy of planes (may be null: converted on the fly)
     const int32_t *plane_mat;
     const double *boxes;
     const int32_t *box_mat;
@@ -185,13 +186,25 @@ __device__ __forceinline__ void wall_forces(const DemArgs<VT> &a, const SceneInf
                                             const double4 &pi, V3<T> vi, V3<T> wi,
                                             const MatDev &mi, Acc<T> &acc) {
     const V3<T> zero = v3(T(0), T(0), T(0));
+    // a sphere clear of every (axis-aligned) plane tests none of them
+    const bool clear = pi.x - pi.w > s.wall_lo[0] && pi.x + pi.w < s.wall_hi[0] &&
+                       pi.y - pi.w > s.wall_lo[1] && pi.y + pi.w < s.wall_hi[1] &&
+                       pi.z - pi.w > s.wall_lo[2] && pi.z + pi.w < s.wall_hi[2];
     const float pxf = float(pi.x), pyf = float(pi.y), pzf = float(pi.z), prf = float(pi.w);
-    for (int p = 0; p < s.nplanes; ++p) {
-        const double4 pl = a.planes[s.plane_begin + p];
+    const float tol = 1e-3f * (1.0f + fabsf(pxf) + fabsf(pyf) + fabsf(pzf));
+    for (int p = 0; p < (clear ? 0 : s.nplanes); ++p) {
+        float4 pf;
+        if (a.planes_f) {
+            pf = a.planes_f[s.plane_begin + p];
+        } else {
+            const double4 q = a.planes[s.plane_begin + p];
+            pf = make_float4(float(q.x), float(q.y), float(q.z), float(q.w));
+        }
         // FP32 estimate first: spheres clearly off the plane skip the exact FP64 test (the
         // estimate's error is far below the 1e-3 margin for coordinates up to ~1e4)
-        const float est = float(pl.x) * pxf + float(pl.y) * pyf + float(pl.z) * pzf - prf - float(pl.w);
-        if (est > 1e-3f * (1.0f + fabsf(float(pl.w)) + fabsf(pxf) + fabsf(pyf) + fabsf(pzf))) continue;
+        const float est = pf.x * pxf + pf.y * pyf + pf.z * pzf - prf - pf.w;
+        if (est > tol + 1e-3f * fabsf(pf.w)) continue;
+        const double4 pl = a.planes[s.plane_begin + p];
         const double kk = dot_rn(pl.x, pl.y, pl.z, pi.x, pi.y, pi.z);
         const double dist = __dsub_rn(__dsub_rn(kk, pi.w), pl.w);
         if (!(dist < -kContactThreshold)) continue;
@@ -268,8 +281,8 @@ __device__ __forceinline__ double4 integrate_core(const DemArgs<VT> &a, int64_t 
         // mixed precision: the same formulas in FP32 (SphereBase.h:169-171, 230-234)
         const float r = float(pi.w);
         const float m = 4.0f / 3.0f * 3.14159265f * r * r * r * float(mi.density);
-        im = T(1.0f / m);
-        ii = T(1.0f / (0.4f * m * r * r));
+        im = T(__frcp_rn(m));
+        ii = T(__frcp_rn(0.4f * m * r * r));
     }
     const V3<T> gg = v3(T(a.g[0]), T(a.g[1]), T(a.g[2]));
     const V3<T> vdot = acc.F * T(im) + gg;
@@ -395,22 +408,28 @@ template <typename VT, bool TRACKQ, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool use_grid = a.nl_flags[1] != 0;   // this step's rebuild overflowed the lists
     bool moved = false;
     if (t < a.n) {
+        // every load of this body's own records first: they are independent, and none may
+        // wait behind this thread's stores
         const double4 pi = a.pr[t];
         const uint32_t tagi = a.tag[t];
+        const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
+        int k = a.nl_start[t];
+        const int e = a.nl_start[t + 1];
+        const float disp0 = a.disp[t];
         const SceneInfo &s = a.scenes[tagi >> 16];
         const MatDev &mi = a.mats[tagi & 0xffffu];
-        const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
         Acc<T> acc;
         acc.F = v3(T(0), T(0), T(0));
         acc.T_ = acc.F;
-        if (!use_grid) {
+        // a body without candidates at the last rebuild has no contact partner before the
+        // next one, lists or not; the others read whether that rebuild's lists fit
+        if (k < e && a.nl_flags[1] != 0) {
+            grid_forces<T, VT>(a, s, (int32_t)t, pi, vi, wi, a.uid[t], mi, acc);
+        } else if (k < e) {
             // entries: neighbour index, top bit set when this body is pe's body 1; two at a
             // time so their loads overlap
-            int k = a.nl_start[t];
-            const int e = a.nl_start[t + 1];
             for (; k + 1 < e; k += 2) {
                 const uint32_t e0 = (uint32_t)a.nl_idx[k], e1 = (uint32_t)a.nl_idx[k + 1];
                 const int32_t j0 = (int32_t)(e0 & 0x7fffffffu), j1 = (int32_t)(e1 & 0x7fffffffu);
@@ -423,8 +442,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
                 const int32_t j0 = (int32_t)(e0 & 0x7fffffffu);
                 pair_force_o<T, VT>(a, pi, vi, wi, mi, j0, a.pr[j0], (e0 >> 31) != 0u, acc);
             }
-        } else {
-            grid_forces<T, VT>(a, s, (int32_t)t, pi, vi, wi, a.uid[t], mi, acc);
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
         V3<T> v, w;
@@ -433,12 +450,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
         a.pr_out[t] = o;
         st_vw(a.vw_out, a.n, t, v, w);
         const float vx = float(v.x), vy = float(v.y), vz = float(v.z);
-        const float d = a.disp[t] + sqrtf(vx * vx + vy * vy + vz * vz) * float(a.dt) * 1.0001f;
+        const float d = disp0 + sqrtf(vx * vx + vy * vy + vz * vz) * float(a.dt) * 1.0001f;
         a.disp[t] = d;
         moved = !(d < a.half_skin);   // also catches NaN
     }
     if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(&a.nl_flags[0], 1);
-    if (use_grid && t == 0) atomicOr(&a.nl_flags[0], 1);
+    // after an overflow every step rebuilds until the host has grown the list buffer
+    if (t == 0 && a.nl_flags[1] != 0) atomicOr(&a.nl_flags[0], 1);
 }
 
 template <typename VT>
@@ -454,6 +472,7 @@ DemArgs<VT> dem_args(Ctx *c, double dt) {
     a.scenes = c->d_scenes;
     a.mats = c->d_mats;
     a.planes = c->d_planes;
+    a.planes_f = c->d_planes_f;
     a.plane_mat = c->d_plane_mat;
     a.boxes = c->d_boxes;
     a.box_mat = c->d_box_mat;
@@ -580,15 +599,16 @@ __global__ void k_list(int64_t n, const double4 *pr, const uint32_t *tag, const 
     const SceneInfo &s = scenes[tag[t] >> 16];
     int cx, cy, cz;
     cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    // only the cells within reach of the sphere (a partner is at most r_max + skin further)
+    const double reach = (pi.w + s.rmax + skin) * (1.0 + 1e-12) + 1e-12;
+    int x0, x1, y0, y1, z0, z1;
+    search_range(s, 0, pi.x, reach, cx, x0, x1);
+    search_range(s, 1, pi.y, reach, cy, y0, y1);
+    search_range(s, 2, pi.z, reach, cz, z0, z1);
     int pos = (MODE == 1) ? start[t] : 0;
     int count = 0;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= s.dim[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= s.dim[1]) continue;
+    for (int z = z0; z <= z1; ++z) {
+        for (int y = y0; y <= y1; ++y) {
             const int64_t c0 = cell_key(s, x0, y, z);
             const int64_t c1 = c0 + (x1 - x0) + 1;
             const int e = cell_start[c1];
@@ -731,7 +751,7 @@ int dem_step(Ctx *c, double dt) {
 int dem_list_alloc(Ctx *c) {
     ListBuf &L = c->nl;
     const size_t n = (size_t)std::max<int64_t>(c->n, 1);
-    L.cap = std::max<int64_t>(16 * c->n, 1024);
+    L.cap = c->p.max_contacts > 0 ? c->p.max_contacts : std::max<int64_t>(16 * c->n, 1024);
     PEB_CUDA(c, cudaMalloc(&L.start, (n + 2) * sizeof(int32_t)));
     PEB_CUDA(c, cudaMalloc(&L.cnt, (n + 2) * sizeof(int32_t)));
     PEB_CUDA(c, cudaMalloc(&L.idx, (size_t)L.cap * sizeof(int32_t)));
@@ -942,6 +962,7 @@ cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream) {
     a.scenes = r.scenes;
     a.mats = r.mats;
     a.planes = r.planes;
+    a.planes_f = nullptr;
     a.plane_mat = r.plane_mat;
     a.boxes = r.boxes;
     a.box_mat = r.box_mat;

@@ -36,6 +36,10 @@ struct SceneInfo {
     int64_t cell_base;
     int32_t plane_begin, nplanes, box_begin, nboxes;
     int64_t body_begin, nbodies;   // in upload order
+    // spheres whose extent lies inside [wall_lo, wall_hi] touch none of the scene's planes
+    // (axis-aligned planes only; a scene with another plane has an empty box)
+    double wall_lo[3], wall_hi[3];
+    double rmax;                   // largest sphere radius of the scene at upload
 };
 
 // per-material constants; reciprocals so a composed value is one division (Materials.h:633)
@@ -169,6 +173,7 @@ struct Ctx {
     SceneInfo *d_scenes = nullptr;
     MatDev *d_mats = nullptr;
     double4 *d_planes = nullptr;    // (n, d)
+    float4 *d_planes_f = nullptr;   // FP32 copy, inside the d_planes allocation
     int32_t *d_plane_mat = nullptr;
     double *d_boxes = nullptr;
     int32_t *d_box_mat = nullptr;
@@ -407,6 +412,17 @@ __device__ __forceinline__ void cell_coords(const SceneInfo &s, double x, double
     cx = clampi((int)floor((x - s.lo[0]) * s.inv_h), 0, s.dim[0] - 1);
     cy = clampi((int)floor((y - s.lo[1]) * s.inv_h), 0, s.dim[1] - 1);
     cz = clampi((int)floor((z - s.lo[2]) * s.inv_h), 0, s.dim[2] - 1);
+}
+
+// Cells along axis `a` that can hold a body closer than `reach` to coordinate p, whose own
+// (clamped) cell is c: the clamped cells of p - reach and p + reach, never more than one cell
+// either side of c since cell edges are at least 2 r_max + skin.
+__device__ __forceinline__ void search_range(const SceneInfo &s, int a, double p, double reach,
+                                             int c, int &lo, int &hi) {
+    const int l = clampi((int)floor((p - reach - s.lo[a]) * s.inv_h), 0, s.dim[a] - 1);
+    const int h = clampi((int)floor((p + reach - s.lo[a]) * s.inv_h), 0, s.dim[a] - 1);
+    lo = max(l, c - 1);
+    hi = min(h, c + 1);
 }
 
 __device__ __forceinline__ int64_t cell_key(const SceneInfo &s, int cx, int cy, int cz) {

@@ -119,14 +119,15 @@ __device__ int list_neighbours(const RebuildArgs<VT> &a, int64_t t, int pos) {
     const int32_t uidt = a.cur.uid[t];
     int cx, cy, cz;
     cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    // only the cells within reach of the sphere (a partner is at most r_max + skin further)
+    const double reach = (pi.w + s.rmax + a.skin) * (1.0 + 1e-12) + 1e-12;
+    int x0, x1, y0, y1, z0, z1;
+    search_range(s, 0, pi.x, reach, cx, x0, x1);
+    search_range(s, 1, pi.y, reach, cy, y0, y1);
+    search_range(s, 2, pi.z, reach, cz, z0, z1);
     int count = 0;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= s.dim[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= s.dim[1]) continue;
+    for (int z = z0; z <= z1; ++z) {
+        for (int y = y0; y <= y1; ++y) {
             const int64_t c0 = cell_key(s, x0, y, z);
             const int64_t c1 = c0 + (x1 - x0) + 1;
             const int e = a.cell_start[c1];

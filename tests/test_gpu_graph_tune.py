@@ -103,3 +103,23 @@ def test_lists_cover_pairs_beyond_one_cell(skin):
     g.close()
     assert vg[0, 0] < 0.4   # the pair did collide
     assert rel_err(xl, xg) < 1e-12 and rel_err(vl, vg) < 1e-10
+
+
+@pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
+def test_list_overflow_falls_back_to_the_grid(precision):
+    """A list buffer far too small for the first rebuild: that step searches the grid, the
+    library grows the buffer, and the trajectory is the grid path's."""
+    s = scenes.dem_lattice(3, side=8)
+    e = Engine(solver=_abi.DEM, precision=precision, max_contacts=64).load_scene(s)
+    e.step(s.dt, 30)
+    x, v, _ = e.download()
+    st = e.neighbor_list_stats()
+    e.close()
+    assert st["capacity"] > 64
+    g = Engine(solver=_abi.DEM, precision=precision, neighbor_lists=False).load_scene(s)
+    g.step(s.dt, 30)
+    xg, vg, _ = g.download()
+    g.close()
+    tol = 1e-12 if precision == _abi.FP64 else 1e-6
+    assert rel_err(x, xg) < tol
+    assert rel_err(v, vg) < (1e-9 if precision == _abi.FP64 else 1e-3)
