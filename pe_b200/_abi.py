@@ -51,7 +51,7 @@ class Material(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("dem_variant", C.c_int32), ("rebuild_per_sm", C.c_int32), ("skin", C.c_double),
-                ("ms_per_step", C.c_double), ("variants", C.c_int32), ("reserved", C.c_int32)]
+                ("ms_per_step", C.c_double), ("variants", C.c_int32), ("nbgs_sweeps", C.c_int32)]
 
 
 class PeB200Error(RuntimeError):

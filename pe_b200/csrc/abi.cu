@@ -695,7 +695,7 @@ int pe_b200_get_tuning(pe_b200_ctx *h, pe_b200_tuning *out) {
     out->skin = c->nl.skin;
     out->ms_per_step = -1.0;
     out->variants = dem_variant_count();
-    out->reserved = 0;
+    out->nbgs_sweeps = c->tune.nbgs_sweeps;
     return PE_B200_OK;
 }
 
@@ -707,6 +707,7 @@ int pe_b200_set_tuning(pe_b200_ctx *h, const pe_b200_tuning *t) {
     Tuning tu;
     tu.dem_variant = t->dem_variant;
     tu.rebuild_per_sm = t->rebuild_per_sm;
+    tu.nbgs_sweeps = t->nbgs_sweeps;
     return set_tuning(c, tu, c->nl.enabled ? t->skin : c->nl.skin);
 }
 

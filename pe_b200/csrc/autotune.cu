@@ -64,8 +64,10 @@ int set_list_skin(Ctx *c, double skin) {
 }
 
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
-    if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < 0)
+    if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < 0 ||
+        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 3)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
+    c->tune.nbgs_sweeps = t.nbgs_sweeps;
     if (t.dem_variant != c->tune.dem_variant || t.rebuild_per_sm != c->tune.rebuild_per_sm) {
         c->tune = t;
         c->epoch++;
@@ -163,7 +165,7 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
         out->skin = best_skin;
         out->ms_per_step = best_ms;
         out->variants = dem_variant_count();
-        out->reserved = 0;
+        out->nbgs_sweeps = best.nbgs_sweeps;
     }
     return PE_B200_OK;
 }

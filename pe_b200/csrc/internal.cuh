@@ -73,6 +73,7 @@ struct NbgsBuf {
     int32_t *cstart_dev = nullptr;            // colour offsets on the device
     unsigned int *bar = nullptr;              // grid barrier of the persistent sweep
     bool coop_disabled = false;
+    int cluster = -1;               // CTAs of the one-cluster sweep kernel (0: not available)
     void *vel = nullptr;                      // v', w', dv, dw per body (VT[12])
     double *red = nullptr;                    // reduction scratch
     int64_t red_cap = 0;
@@ -106,6 +107,7 @@ struct ListBuf {
 struct Tuning {
     int32_t dem_variant = 0;    // index into the k_dem_list launch shapes (dem.cu)
     int32_t rebuild_per_sm = 0; // persistent rebuild CTAs per SM; 0 = as many as fit
+    int32_t nbgs_sweeps = 0;    // 0 automatic, 1 one cluster, 2 cooperative grid, 3 per colour
 };
 
 // a captured CUDA graph of `steps` DEM list steps (dem.cu); valid while the buffers it was

@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "contacts.cuh"
 
 namespace peb {
@@ -104,20 +106,49 @@ struct Raw {  // detection output, detection order
     T *dist, *mu;
 };
 
-template <typename T>
-struct Cache {  // colour-sorted solver records (component-major SoA)
-    int32_t *b1, *b2;
-    T *r1, *r2, *n, *t, *o;  // 3 x cap
-    T *dist, *mu, *dn_inv, *dnn;
-    T *dinv;                 // 6 x cap: xx xy xz yy yz zz (contact frame)
-    T *dto_inv;              // 3 x cap: tt to oo
-    T *p;                    // 3 x cap, contact frame
-};
+// 4-vectors of the arithmetic type: the sweep reads whole 16/32-byte records
+template <typename T> struct Vec4;
+template <> struct Vec4<float> { typedef float4 type; };
+template <> struct Vec4<double> { typedef double4 type; };
+template <typename T> using T4 = typename Vec4<T>::type;
 
 template <typename T>
-struct BodyV {  // per body, slot order
-    T *v, *w, *dv, *dw;   // 3 x n each, component-major
-    T *im, *ii;
+__device__ __forceinline__ T4<T> mk4(T x, T y, T z, T w) {
+    T4<T> r;
+    r.x = x; r.y = y; r.z = z; r.w = w;
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ V3<T> xyz(const T4<T> &a) { return v3(a.x, a.y, a.z); }
+
+// loads that bypass L1: in the persistent sweeps, other SMs update these between colours
+__device__ __forceinline__ float4 ldcg4(const float4 *p) { return __ldcg(p); }
+__device__ __forceinline__ double4 ldcg4(const double4 *p) {
+    const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Colour-sorted solver records, one per contact.  rec holds kRec 4-vectors per contact, the
+// frictionless sweep reading only the first three:
+//   [n, dist] [r1, 1/D_nn] [r2, D_nn] [t, mu] [o, Dto^-1_tt] [D^-1 xx xy xz yy]
+//   [D^-1 yz zz, Dto^-1_to, Dto^-1_oo]
+constexpr int kRec = 7;
+template <typename T>
+struct Cache {
+    int2 *ids;    // body 1, body 2 (-1: wall)
+    T4<T> *rec;   // kRec per contact
+    T4<T> *p;     // impulse in the contact frame (n, t, o, -)
+};
+
+// Per body, slot order: velocities after the predictor with 1/m, 1/I (read-only in the sweeps)
+// and the velocity corrections (read and written by the sweeps).
+template <typename T>
+struct BodyV {
+    T4<T> *vr;    // v, 1/m
+    T4<T> *wr;    // w, 1/I
+    T4<T> *dv;    // dv, -
+    T4<T> *dw;    // dw, -
 };
 
 template <typename T>
@@ -152,13 +183,10 @@ __global__ void k_permute_cache(int64_t n, const int32_t *sorted, const double4 
     const V3<VT> vp = v + v3(VT(gx), VT(gy), VT(gz)) * VT(dt);
     const V3<VT> Iw = VT(I) * w;
     const V3<VT> wp = w + VT(dt) * (VT(ii) * cross(Iw, w));
-    st3c(bv.v, t, n, vp);
-    st3c(bv.w, t, n, wp);
-    const V3<VT> z = v3(VT(0), VT(0), VT(0));
-    st3c(bv.dv, t, n, z);
-    st3c(bv.dw, t, n, z);
-    bv.im[t] = VT(im);
-    bv.ii[t] = VT(ii);
+    bv.vr[t] = mk4<VT>(vp.x, vp.y, vp.z, VT(im));
+    bv.wr[t] = mk4<VT>(wp.x, wp.y, wp.z, VT(ii));
+    bv.dv[t] = mk4<VT>(VT(0), VT(0), VT(0), VT(0));
+    bv.dw[t] = mk4<VT>(VT(0), VT(0), VT(0), VT(0));
 }
 
 template <typename T>
@@ -342,8 +370,8 @@ __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos,
     }
     t = normalized(t);
     const V3<T> o = cross(n, t);
-    const T im1 = bv.im[b1], ii1 = bv.ii[b1];
-    const T im2 = b2 >= 0 ? bv.im[b2] : T(0), ii2 = b2 >= 0 ? bv.ii[b2] : T(0);
+    const T im1 = bv.vr[b1].w, ii1 = bv.wr[b1].w;
+    const T im2 = b2 >= 0 ? bv.vr[b2].w : T(0), ii2 = b2 >= 0 ? bv.wr[b2].w : T(0);
     // D = -(r1^x I1^-1 r1^x + r2^x I2^-1 r2^x) + (1/m1 + 1/m2) 1 with scalar sphere inertia:
     // -r^x r^x = |r|^2 1 - r r^T
     T D[9];
@@ -374,67 +402,59 @@ __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos,
     const T c00 = yy * zz - yz * yz, c01 = xz * yz - xy * zz, c02 = xy * yz - xz * yy;
     const T det = xx * c00 + xy * c01 + xz * c02;
     const T id = T(1) / det;
-    cc.dinv[k] = c00 * id;
-    cc.dinv[k + cap] = c01 * id;
-    cc.dinv[k + 2 * cap] = c02 * id;
-    cc.dinv[k + 3 * cap] = (xx * zz - xz * xz) * id;
-    cc.dinv[k + 4 * cap] = (xy * xz - xx * yz) * id;
-    cc.dinv[k + 5 * cap] = (xx * yy - xy * xy) * id;
-    cc.dn_inv[k] = T(1) / xx;
-    cc.dnn[k] = xx;
     const T d2 = yy * zz - yz * yz;
     const T id2 = T(1) / d2;
-    cc.dto_inv[k] = zz * id2;
-    cc.dto_inv[k + cap] = -yz * id2;
-    cc.dto_inv[k + 2 * cap] = yy * id2;
-    cc.b1[k] = b1;
-    cc.b2[k] = b2;
-    st3c(cc.r1, k, cap, r1);
-    st3c(cc.r2, k, cap, r2);
-    st3c(cc.n, k, cap, n);
-    st3c(cc.t, k, cap, t);
-    st3c(cc.o, k, cap, o);
-    cc.dist[k] = raw.dist[c];
-    cc.mu[k] = raw.mu[c];
-    st3c(cc.p, k, cap, v3(T(0), T(0), T(0)));
+    T4<T> *R = cc.rec + (int64_t)kRec * k;
+    R[0] = mk4<T>(n.x, n.y, n.z, raw.dist[c]);
+    R[1] = mk4<T>(r1.x, r1.y, r1.z, T(1) / xx);
+    R[2] = mk4<T>(r2.x, r2.y, r2.z, xx);
+    R[3] = mk4<T>(t.x, t.y, t.z, raw.mu[c]);
+    R[4] = mk4<T>(o.x, o.y, o.z, zz * id2);
+    R[5] = mk4<T>(c00 * id, c01 * id, c02 * id, (xx * zz - xz * xz) * id);
+    R[6] = mk4<T>((xy * xz - xx * yz) * id, (xx * yy - xy * xy) * id, -yz * id2, yy * id2);
+    cc.ids[k] = make_int2(b1, b2);
+    cc.p[k] = mk4<T>(T(0), T(0), T(0), T(0));
     (void)nb;
 }
 
 // ---- one colour of one sweep ----------------------------------------------------------------
-// loads that bypass L1: in the persistent sweep, other SMs update these between colours
-template <typename T>
-__device__ __forceinline__ V3<T> ld3cg(const T *a, int64_t i, int64_t s) {
-    return v3(__ldcg(a + i), __ldcg(a + i + s), __ldcg(a + i + 2 * s));
-}
-
 // one contact of one sweep; COHERENT: read the velocity corrections and the impulse from L2
 template <typename T, bool FRICTION, bool COHERENT>
-__device__ __forceinline__ void sweep_contact(int64_t k, int64_t cap, T dtinv, const Cache<T> &cc,
-                                              const BodyV<T> &bv, int64_t nb, int track_delta,
+__device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T> &cc,
+                                              const BodyV<T> &bv, int track_delta,
                                               unsigned long long *delta) {
-    const int32_t b1 = cc.b1[k], b2 = cc.b2[k];
-    const V3<T> r1 = ld3c(cc.r1, k, cap), r2 = ld3c(cc.r2, k, cap);
-    const V3<T> n = ld3c(cc.n, k, cap);
-    const V3<T> pc = COHERENT ? ld3cg(cc.p, k, cap) : ld3c(cc.p, k, cap);  // contact frame
-    const T im1 = bv.im[b1], ii1 = bv.ii[b1];
-    V3<T> dv1 = COHERENT ? ld3cg(bv.dv, b1, nb) : ld3c(bv.dv, b1, nb);
-    V3<T> dw1 = COHERENT ? ld3cg(bv.dw, b1, nb) : ld3c(bv.dw, b1, nb);
-    const V3<T> v1 = ld3c(bv.v, b1, nb), w1 = ld3c(bv.w, b1, nb);
+    const int2 ids = cc.ids[k];
+    const int32_t b1 = ids.x, b2 = ids.y;
+    const T4<T> *R = cc.rec + (int64_t)kRec * k;
+    const T4<T> q0 = R[0], q1 = R[1], q2 = R[2];
+    const V3<T> n = xyz<T>(q0), r1 = xyz<T>(q1), r2 = xyz<T>(q2);
+    const T dist = q0.w, dn_inv = q1.w;
+    const T4<T> pc4 = COHERENT ? ldcg4(cc.p + k) : cc.p[k];
+    const V3<T> pc = xyz<T>(pc4);  // contact frame
+    const T4<T> vr1 = bv.vr[b1], wr1 = bv.wr[b1];
+    const T im1 = vr1.w, ii1 = wr1.w;
+    V3<T> dv1 = xyz<T>(COHERENT ? ldcg4(bv.dv + b1) : bv.dv[b1]);
+    V3<T> dw1 = xyz<T>(COHERENT ? ldcg4(bv.dw + b1) : bv.dw[b1]);
+    const V3<T> v1 = xyz<T>(vr1), w1 = xyz<T>(wr1);
     V3<T> dv2 = v3(T(0), T(0), T(0)), dw2 = dv2, v2 = dv2, w2 = dv2;
     T im2 = T(0), ii2 = T(0);
     if (b2 >= 0) {
-        im2 = bv.im[b2];
-        ii2 = bv.ii[b2];
-        dv2 = COHERENT ? ld3cg(bv.dv, b2, nb) : ld3c(bv.dv, b2, nb);
-        dw2 = COHERENT ? ld3cg(bv.dw, b2, nb) : ld3c(bv.dw, b2, nb);
-        v2 = ld3c(bv.v, b2, nb);
-        w2 = ld3c(bv.w, b2, nb);
+        const T4<T> vr2 = bv.vr[b2], wr2 = bv.wr[b2];
+        im2 = vr2.w;
+        ii2 = wr2.w;
+        dv2 = xyz<T>(COHERENT ? ldcg4(bv.dv + b2) : bv.dv[b2]);
+        dw2 = xyz<T>(COHERENT ? ldcg4(bv.dw + b2) : bv.dw[b2]);
+        v2 = xyz<T>(vr2);
+        w2 = xyz<T>(wr2);
     }
     V3<T> t, o;
     V3<T> pold;
+    T4<T> q3, q4;
     if (FRICTION) {
-        t = ld3c(cc.t, k, cap);
-        o = ld3c(cc.o, k, cap);
+        q3 = R[3];
+        q4 = R[4];
+        t = xyz<T>(q3);
+        o = xyz<T>(q4);
         pold = n * pc.x + t * pc.y + o * pc.z;
     } else {
         pold = n * pc.x;
@@ -447,21 +467,20 @@ __device__ __forceinline__ void sweep_contact(int64_t k, int64_t cap, T dtinv, c
         dw2 = dw2 + ii2 * cross(r2, pold);
     }
     const V3<T> gdot = ((v1 + dv1) - (v2 + dv2) + cross(w1 + dw1, r1)) - cross(w2 + dw2, r2);
-    T gn = dot(n, gdot) + cc.dist[k] * dtinv;
+    T gn = dot(n, gdot) + dist * dtinv;
     V3<T> pnew = v3(T(0), T(0), T(0));
     V3<T> pcf = pnew;
     if (gn < T(0)) {
         if (!FRICTION) {
-            pcf.x = -cc.dn_inv[k] * gn;
+            pcf.x = -dn_inv * gn;
             pnew = n * pcf.x;
         } else {
             const T gt = dot(t, gdot), go = dot(o, gdot);
-            const T *di = cc.dinv;
-            const T dxx = di[k], dxy = di[k + cap], dxz = di[k + 2 * cap], dyy = di[k + 3 * cap],
-                    dyz = di[k + 4 * cap], dzz = di[k + 5 * cap];
+            const T4<T> q5 = R[5], q6 = R[6];
+            const T dxx = q5.x, dxy = q5.y, dxz = q5.z, dyy = q5.w, dyz = q6.x, dzz = q6.y;
             pcf = v3(-(dxx * gn + dxy * gt + dxz * go), -(dxy * gn + dyy * gt + dyz * go),
                      -(dxz * gn + dyz * gt + dzz * go));
-            const T mu = cc.mu[k];
+            const T mu = q3.w;
             T flimit = mu * pcf.x;
             T fsq = pcf.y * pcf.y + pcf.z * pcf.z;
             if (fsq > flimit * flimit || pcf.x < T(0)) {
@@ -470,16 +489,16 @@ __device__ __forceinline__ void sweep_contact(int64_t k, int64_t cap, T dtinv, c
                 const V3<T> e1 = cross(ii1 * cross(r1, ptmp), r1);
                 const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
                 const T gdot_n = gn + dot(n, e1 + e2);
-                pcf.x = -(cc.dn_inv[k] * gdot_n);
+                pcf.x = -(dn_inv * gdot_n);
                 pcf.x = pcf.x > T(0) ? pcf.x : T(0);
                 ptmp = n * pcf.x;
                 const V3<T> f1 = cross(ii1 * cross(r1, ptmp), r1);
                 const V3<T> f2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
                 const V3<T> gdot2 = (gdot + f1) + f2;
                 const T g2t = dot(t, gdot2), g2o = dot(o, gdot2);
-                const T *ti = cc.dto_inv;
-                pcf.y = -(ti[k] * g2t + ti[k + cap] * g2o);
-                pcf.z = -(ti[k + cap] * g2t + ti[k + 2 * cap] * g2o);
+                const T ttt = q4.w, tto = q6.z, too = q6.w;
+                pcf.y = -(ttt * g2t + tto * g2o);
+                pcf.z = -(tto * g2t + too * g2o);
                 flimit = mu * pcf.x;
                 fsq = pcf.y * pcf.y + pcf.z * pcf.z;
                 if (fsq > flimit * flimit) {
@@ -497,12 +516,12 @@ __device__ __forceinline__ void sweep_contact(int64_t k, int64_t cap, T dtinv, c
             dw2 = dw2 - ii2 * cross(r2, pnew);
         }
     }
-    st3c(cc.p, k, cap, pcf);
-    st3c(bv.dv, b1, nb, dv1);
-    st3c(bv.dw, b1, nb, dw1);
+    cc.p[k] = mk4<T>(pcf.x, pcf.y, pcf.z, T(0));
+    bv.dv[b1] = mk4<T>(dv1.x, dv1.y, dv1.z, T(0));
+    bv.dw[b1] = mk4<T>(dw1.x, dw1.y, dw1.z, T(0));
     if (b2 >= 0) {
-        st3c(bv.dv, b2, nb, dv2);
-        st3c(bv.dw, b2, nb, dw2);
+        bv.dv[b2] = mk4<T>(dv2.x, dv2.y, dv2.z, T(0));
+        bv.dw[b2] = mk4<T>(dw2.x, dw2.y, dw2.z, T(0));
     }
     if (track_delta) {
         const V3<T> dp = pold - pnew;
@@ -517,7 +536,7 @@ __global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int6
                                                 int track_delta, unsigned long long *delta) {
     const int64_t k = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= end) return;
-    sweep_contact<T, FRICTION, false>(k, cap, dtinv, cc, bv, nb, track_delta, delta);
+    sweep_contact<T, FRICTION, false>(k, dtinv, cc, bv, track_delta, delta);
 }
 
 // All sweeps of a step in one cooperative launch: colour after colour, separated by bounded
@@ -537,8 +556,37 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
         for (int col = 0; col < ncolors; ++col) {
             const int64_t e = color_start[col + 1];
             for (int64_t k = color_start[col] + g0; k < e; k += stride)
-                sweep_contact<T, FRICTION, true>(k, cap, dtinv, cc, bv, nb, track, delta);
+                sweep_contact<T, FRICTION, true>(k, dtinv, cc, bv, track, delta);
             if (!grid_sync(bar, err)) return;
+        }
+    }
+}
+
+// All sweeps of a step inside one thread-block cluster: the colours are separated by the
+// cluster's hardware barrier (release/acquire at cluster scope) instead of a barrier through
+// global atomics, which costs a few microseconds per colour.  Used while the largest colour
+// fits the cluster's threads a few times over; no thread waits on anything but the barrier.
+constexpr int kClusterBlk = 512;
+constexpr int kClusterPerThread = 4;
+
+template <typename T, bool FRICTION>
+__global__ void __launch_bounds__(kClusterBlk) k_sweeps_cluster(int iters, int ncolors,
+                                                                const int32_t *color_start,
+                                                                int64_t cap, T dtinv, Cache<T> cc,
+                                                                BodyV<T> bv, int64_t nb,
+                                                                int track_last,
+                                                                unsigned long long *delta) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;   // the grid is one cluster
+    const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t e = color_start[col + 1];
+            for (int64_t k = color_start[col] + g0; k < e; k += stride)
+                sweep_contact<T, FRICTION, true>(k, dtinv, cc, bv, track, delta);
+            cluster.sync();
         }
     }
 }
@@ -549,25 +597,26 @@ __global__ void k_residual(int64_t nc, int64_t cap, double dtinv, Cache<T> cc, B
                            int64_t nb, unsigned long long *res) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nc) return;
-    const int32_t b1 = cc.b1[k], b2 = cc.b2[k];
-    auto L = [&](const T *a, int32_t b) { return v3(double(a[b]), double(a[b + nb]), double(a[b + 2 * nb])); };
-    auto C3 = [&](const T *a) { return v3(double(a[k]), double(a[k + cap]), double(a[k + 2 * cap])); };
-    const V3<double> r1 = C3(cc.r1), r2 = C3(cc.r2), n = C3(cc.n), t = C3(cc.t), o = C3(cc.o);
-    V3<double> a = L(bv.v, b1) + L(bv.dv, b1), wa = L(bv.w, b1) + L(bv.dw, b1);
+    const int2 ids = cc.ids[k];
+    const int32_t b1 = ids.x, b2 = ids.y;
+    auto D3 = [](const T4<T> &q) { return v3(double(q.x), double(q.y), double(q.z)); };
+    const T4<T> *R = cc.rec + (int64_t)kRec * k;
+    const V3<double> n = D3(R[0]), r1 = D3(R[1]), r2 = D3(R[2]), t = D3(R[3]), o = D3(R[4]);
+    V3<double> a = D3(bv.vr[b1]) + D3(bv.dv[b1]), wa = D3(bv.wr[b1]) + D3(bv.dw[b1]);
     V3<double> b = v3(0.0, 0.0, 0.0), wb = b;
     if (b2 >= 0) {
-        b = L(bv.v, b2) + L(bv.dv, b2);
-        wb = L(bv.w, b2) + L(bv.dw, b2);
+        b = D3(bv.vr[b2]) + D3(bv.dv[b2]);
+        wb = D3(bv.wr[b2]) + D3(bv.dw[b2]);
     }
     const V3<double> gdot = ((a - b) + cross(wa, r1)) - cross(wb, r2);
-    const double gn = dot(n, gdot) + double(cc.dist[k]) * dtinv;
-    const V3<double> pc = C3(cc.p);
-    const double pn = pc.x, Dnn = double(cc.dnn[k]);
+    const double gn = dot(n, gdot) + double(R[0].w) * dtinv;
+    const V3<double> pc = D3(cc.p[k]);
+    const double pn = pc.x, Dnn = double(R[2].w);
     double r = fabs(fmin(pn * Dnn, gn));
     if (FRICTION) {
         const double pt = pc.y, po = pc.z, gt = dot(t, gdot), go = dot(o, gdot);
         const double pto = sqrt(pt * pt + po * po), gto = sqrt(gt * gt + go * go);
-        const double mu = double(cc.mu[k]);
+        const double mu = double(R[3].w);
         r = fmax(r, fmax(0.0, pto - mu * pn) * Dnn);
         if (pn > 0.0) {
             if (pto < mu * pn * (1.0 - 1e-9)) r = fmax(r, gto);
@@ -585,8 +634,8 @@ __global__ void k_integrate(int64_t n, double dt, double drag, int has_drag, Bod
                             int32_t *rank, int32_t *cell_count, int32_t *err) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    V3<VT> v = ld3c(bv.v, t, n) + ld3c(bv.dv, t, n);
-    V3<VT> w = ld3c(bv.w, t, n) + ld3c(bv.dw, t, n);
+    V3<VT> v = xyz<VT>(bv.vr[t]) + xyz<VT>(bv.dv[t]);
+    V3<VT> w = xyz<VT>(bv.wr[t]) + xyz<VT>(bv.dw[t]);
     const double4 p = pr[t];
     const double nx = p.x + double(v.x) * dt, ny = p.y + double(v.y) * dt, nz = p.z + double(v.z) * dt;
     if (TRACKQ) {
@@ -639,8 +688,8 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         b.color = nullptr;
         cudaFree(b.body_adj);
         b.body_adj = nullptr;
-        // raw: 2 int + 11 T; cache: 2 int + 27 T  (per contact)
-        const size_t bytes = (size_t)cap * (4 * sizeof(int32_t) + 42 * es) + 64 * 256;
+        // raw: 2 int + 11 T; cache: 2 int + (kRec + 1) x 4 T  (per contact)
+        const size_t bytes = (size_t)cap * (4 * sizeof(int32_t) + (11 + 4 * (kRec + 1)) * es) + 64 * 256;
         PEB_CUDA(c, cudaMalloc(&b.cache, bytes));
         PEB_CUDA(c, cudaMalloc(&b.order, (size_t)cap * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.color, (size_t)cap * sizeof(int32_t)));
@@ -651,7 +700,7 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         PEB_CUDA(c, cudaMalloc(&b.cnt, ((size_t)n + 2) * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.body_cnt, ((size_t)n + 2) * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.used, (size_t)n * sizeof(uint64_t)));
-        PEB_CUDA(c, cudaMalloc(&b.vel, (size_t)n * 14 * es));
+        PEB_CUDA(c, cudaMalloc(&b.vel, (size_t)n * 16 * es));
         PEB_CUDA(c, cudaMalloc(&b.flags, 256 * sizeof(int32_t)));
         PEB_CUDA(c, cudaMallocHost(&b.color_start, 260 * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.red, 4 * sizeof(double)));
@@ -679,28 +728,78 @@ void layout(Ctx *c, Raw<T> &raw, Cache<T> &cc, BodyV<T> &bv) {
     raw.n = (T *)take(3 * cap * sizeof(T));
     raw.dist = (T *)take(cap * sizeof(T));
     raw.mu = (T *)take(cap * sizeof(T));
-    cc.b1 = (int32_t *)take(cap * 4);
-    cc.b2 = (int32_t *)take(cap * 4);
-    cc.r1 = (T *)take(3 * cap * sizeof(T));
-    cc.r2 = (T *)take(3 * cap * sizeof(T));
-    cc.n = (T *)take(3 * cap * sizeof(T));
-    cc.t = (T *)take(3 * cap * sizeof(T));
-    cc.o = (T *)take(3 * cap * sizeof(T));
-    cc.dist = (T *)take(cap * sizeof(T));
-    cc.mu = (T *)take(cap * sizeof(T));
-    cc.dn_inv = (T *)take(cap * sizeof(T));
-    cc.dnn = (T *)take(cap * sizeof(T));
-    cc.dinv = (T *)take(6 * cap * sizeof(T));
-    cc.dto_inv = (T *)take(3 * cap * sizeof(T));
-    cc.p = (T *)take(3 * cap * sizeof(T));
+    cc.ids = (int2 *)take(cap * sizeof(int2));
+    cc.rec = (T4<T> *)take(kRec * cap * sizeof(T4<T>));
+    cc.p = (T4<T> *)take(cap * sizeof(T4<T>));
     const int64_t n = std::max<int64_t>(c->n, 1);
-    T *v = (T *)b.vel;
-    bv.v = v;
-    bv.w = v + 3 * n;
-    bv.dv = v + 6 * n;
-    bv.dw = v + 9 * n;
-    bv.im = v + 12 * n;
-    bv.ii = v + 13 * n;
+    T4<T> *v = (T4<T> *)b.vel;
+    bv.vr = v;
+    bv.wr = v + n;
+    bv.dv = v + 2 * n;
+    bv.dw = v + 3 * n;
+}
+
+// Runs all sweeps in one cluster when the largest colour is small enough; *done reports it.
+// The cluster size (16 CTAs if the GPU schedules such clusters, else 8) is probed once.
+template <typename VT>
+int sweeps_in_cluster(Ctx *c, bool fr, int iters, int ncolors, int maxcol, int64_t cap, VT dtinv,
+                      const Cache<VT> &cc, const BodyV<VT> &bv, int64_t n,
+                      unsigned long long *dl, bool *done) {
+    NbgsBuf &nb = c->nb;
+    auto kern = fr ? k_sweeps_cluster<VT, true> : k_sweeps_cluster<VT, false>;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    cfg.blockDim = dim3(kClusterBlk);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (nb.cluster < 0) {
+        nb.cluster = 0;
+        for (int size : {16, 8}) {
+            auto probe = k_sweeps_cluster<VT, true>;
+            if (size > 8 &&
+                cudaFuncSetAttribute((const void *)probe, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if (size > 8) {
+                cudaFuncSetAttribute((const void *)k_sweeps_cluster<VT, false>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                cudaGetLastError();
+            }
+            cfg.gridDim = dim3(size);
+            attr[0].val.clusterDim.x = size;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)probe, &cfg) == cudaSuccess &&
+                nclusters >= 1) {
+                nb.cluster = size;
+                break;
+            }
+            cudaGetLastError();
+        }
+    }
+    if (nb.cluster == 0 || maxcol > (int64_t)nb.cluster * kClusterBlk * kClusterPerThread)
+        return PE_B200_OK;
+    PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start, (ncolors + 1) * sizeof(int32_t),
+                                cudaMemcpyHostToDevice, c->stream));
+    cfg.gridDim = dim3(nb.cluster);
+    attr[0].val.clusterDim.x = nb.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, iters, ncolors, (const int32_t *)nb.cstart_dev,
+                                             cap, dtinv, cc, bv, n, c->want_residual ? 1 : 0, dl);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        nb.cluster = 0;
+        return PE_B200_OK;
+    }
+    c->launches++;
+    *done = true;
+    return PE_B200_OK;
 }
 
 template <typename VT>
@@ -822,12 +921,20 @@ int nbgs_step_t(Ctx *c, double dt) {
     if (nc > 0) {
         prof_begin(c, ST_SWEEP);
         bool done = iters == 0;
-        if (!done && !nb.coop_disabled) {
+        int maxcol = 1;
+        for (int col = 0; col < ncolors; ++col)
+            maxcol = std::max(maxcol, nb.color_start[col + 1] - nb.color_start[col]);
+        const int mode = c->tune.nbgs_sweeps;
+        // the one-cluster form has the cheaper barrier but only a few SMs' load bandwidth; on
+        // B200 the grid form is faster for every scene measured, so it is the automatic choice
+        if (!done && nb.cluster != 0 && mode == 1) {
+            int rc = sweeps_in_cluster<VT>(c, fr, iters, ncolors, maxcol, cap, VT(1.0 / dt), cc,
+                                           bv, n, dl, &done);
+            if (rc) return rc;
+        }
+        if (!done && !nb.coop_disabled && mode != 3) {
             // all sweeps in one cooperative launch (colours separated by grid barriers); as few
             // blocks as the largest colour needs, so the barriers stay short
-            int maxcol = 1;
-            for (int col = 0; col < ncolors; ++col)
-                maxcol = std::max(maxcol, nb.color_start[col + 1] - nb.color_start[col]);
             auto kern = fr ? k_sweeps_persistent<VT, true> : k_sweeps_persistent<VT, false>;
             int occ = 0;
             cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0);

@@ -218,10 +218,15 @@ class Engine:
     def tuning(self) -> dict:
         t = _abi.Tuning()
         self._check(self._L.pe_b200_get_tuning(self._h, C.byref(t)))
-        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_ if k != "reserved"}
+        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_}
 
-    def set_tuning(self, dem_variant: int, rebuild_per_sm: int, skin: float):
-        t = _abi.Tuning(dem_variant=dem_variant, rebuild_per_sm=rebuild_per_sm, skin=skin)
+    def set_tuning(self, dem_variant: int = 0, rebuild_per_sm: int = 0, skin: float = 0.0,
+                   nbgs_sweeps: int = 0):
+        """skin <= 0 keeps the current skin."""
+        if skin <= 0:
+            skin = self.tuning()["skin"]
+        t = _abi.Tuning(dem_variant=dem_variant, rebuild_per_sm=rebuild_per_sm, skin=skin,
+                        nbgs_sweeps=nbgs_sweeps)
         self._check(self._L.pe_b200_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, dt: float, trial_steps: int = 100) -> dict:
@@ -229,7 +234,7 @@ class Engine:
         (the state is restored)."""
         t = _abi.Tuning()
         self._check(self._L.pe_b200_autotune(self._h, float(dt), int(trial_steps), C.byref(t)))
-        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_ if k != "reserved"}
+        return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_}
 
     def neighbor_list_stats(self) -> dict:
         r, e, c = C.c_int64(), C.c_int64(), C.c_int64()
