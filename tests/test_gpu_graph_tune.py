@@ -123,3 +123,22 @@ def test_list_overflow_falls_back_to_the_grid(precision):
     tol = 1e-12 if precision == _abi.FP64 else 1e-6
     assert rel_err(x, xg) < tol
     assert rel_err(v, vg) < (1e-9 if precision == _abi.FP64 else 1e-3)
+
+
+@pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
+@pytest.mark.parametrize("model", [0, 1])
+def test_nbgs_sweep_forms_agree(precision, model):
+    """One cluster, one cooperative grid and one launch per colour run the same colour order,
+    and the contacts of a colour share no body: the results are identical."""
+    s = scenes.nbgs_box(0, n=4096, dims=(16.0, 16.0, 40.0), dense=True)
+    out = []
+    for mode in (1, 2, 3):
+        e = Engine(solver=_abi.HCSITS, precision=precision, relaxation_model=model,
+                   max_iterations=30).load_scene(s)
+        e.set_tuning(nbgs_sweeps=mode)
+        e.step(s.dt, 3)
+        out.append(e.download())
+        e.close()
+    for o in out[1:]:
+        for a, b in zip(o, out[0]):
+            assert np.array_equal(a, b)
