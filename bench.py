@@ -1,6 +1,6 @@
 """Benchmark of the B200 rigid-body step (sphere-steps/s).
 
-Default workload: the large DEM scene -- 1,048,576 spheres, log-normal radii (median 0.5,
+Default workload: the large DEM scene -- 1,048,576 spheres, 1000 steps, log-normal radii (median 0.5,
 sigma_log 0.2, clipped to [0.3, 0.9]) in a random packing at 30% solid fraction at the bottom of a
 200x200x400 box of planes, linear spring-dashpot k_n=1e5, c_n=50, mu=0.4, dt=5e-5 -- advanced by
 the mixed-precision path (FP64 positions, FP32 velocities/forces).  Beside it, on the same scene,
@@ -43,7 +43,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dem_large_1m",
@@ -202,7 +202,7 @@ class Clocks:
     def start(self):
         try:
             cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                   "-lms", "200"]
+                   "-lms", "20"]
             if self.uuid:
                 cmd += ["-i", self.uuid]
             self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
@@ -249,6 +249,46 @@ def make_engine(ss, kind, precision, iters=100, lists=True):
         e.load_scene(ss[0])
     else:
         e.load_scenes(ss)
+    return e
+
+
+def stage_inputs(ss, torch):
+    """The bodies of the scenes in pinned host arrays (materials re-indexed per scene), and the
+    small per-scene tables, ready for one upload."""
+    pin = lambda a, dtype: torch.from_numpy(np.ascontiguousarray(a, dtype)).pin_memory().numpy()
+    off, mats, mat, walls = 0, [], [], []
+    for s in ss:
+        mats.append(s.materials)
+        mat.append(s.mat + off)
+        walls.append((s.planes, s.plane_mat + off, s.boxes, s.box_mat + off))
+        off += s.materials.shape[0]
+    scene = None
+    if len(ss) > 1:
+        scene = pin(np.concatenate([np.full(s.n, k, np.int32) for k, s in enumerate(ss)]), np.int32)
+    return {"x": pin(np.concatenate([s.x for s in ss]), np.float64),
+            "v": pin(np.concatenate([s.v for s in ss]), np.float64),
+            "w": pin(np.concatenate([s.w for s in ss]), np.float64),
+            "r": pin(np.concatenate([s.r for s in ss]), np.float64),
+            "mat": pin(np.concatenate(mat), np.int32), "scene": scene,
+            "materials": np.concatenate(mats), "walls": walls, "gravity": ss[0].gravity,
+            "damping": ss[0].damping, "nscenes": len(ss)}
+
+
+def engine_from_staged(st, kind, precision, iters=100, lists=True):
+    from pe_b200 import _abi
+    from pe_b200.engine import Engine
+    solver = _abi.DEM if kind == "dem" else _abi.HCSITS
+    model = _abi.INELASTIC_FRICTIONLESS
+    if kind == "hcsits" and float(st["materials"][0, 2]) > 0:
+        model = _abi.APPROX_INELASTIC_COULOMB_DECOUPLING
+    e = Engine(solver=solver, precision=precision, relaxation_model=model, max_iterations=iters,
+               neighbor_lists=lists)
+    e.set_materials(st["materials"])
+    for k, (pl, pm, bx, bm) in enumerate(st["walls"]):
+        e.set_walls(k, pl, pm, bx, bm)
+    e.set_gravity(st["gravity"])
+    e.set_damping(st["damping"])
+    e.upload(st["x"], st["v"], st["w"], st["r"], st["mat"], st["scene"], st["nscenes"])
     return e
 
 
@@ -467,21 +507,28 @@ def our_arm(args):
     total_sph = float(tot.item())
     value = total_sph * args.steps / (ms_max / 1e3)
 
-    # end to end through the public API: host arrays in, K steps, host arrays out
+    # end to end through the public API: a new context, the bodies uploaded from pinned host
+    # arrays, K steps, the state downloaded into pinned host arrays; wall clock
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    host = [(np.ascontiguousarray(s.x), np.ascontiguousarray(s.v), np.ascontiguousarray(s.w))
-            for s in ss]
+    staged = stage_inputs(ss, torch)
+    outs = [torch.zeros((nsph, 3), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
     t0 = time.perf_counter()
-    e2 = make_engine(ss, kind, precision)
+    e2 = engine_from_staged(staged, kind, precision)
     if tuning is not None:
         e2.set_tuning(tuning["dem_variant"], tuning["rebuild_per_sm"], tuning["skin"])
+    t1 = time.perf_counter()
     e2.step(dt, args.steps)
-    out = e2.download()
+    t2 = time.perf_counter()
+    out = e2.download(out=outs)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    h2d = sum(s.x.nbytes + s.v.nbytes + s.w.nbytes + s.r.nbytes + s.mat.nbytes for s in ss)
+    t3 = time.perf_counter()
+    e2e_s = t3 - t0
+    e2e_parts = {"setup_upload_ms": 1e3 * (t1 - t0), "steps_issue_ms": 1e3 * (t2 - t1),
+                 "download_sync_ms": 1e3 * (t3 - t2)}
+    h2d = sum(staged[k].nbytes for k in ("x", "v", "w", "r", "mat")) + \
+        (staged["scene"].nbytes if staged["scene"] is not None else 0)
     d2h = sum(a.nbytes for a in out if a is not None)
     e2.close()
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
@@ -538,7 +585,9 @@ def our_arm(args):
             "clocks": clk, "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
-                    "note": "upload + steps + download through the C ABI, wall clock"},
+                    "note": "new context, upload from pinned host arrays, steps, download into "
+                            "pinned host arrays, through the C ABI; wall clock",
+                    "parts": e2e_parts},
             "roofline": roofline,
             "stages_ms_per_step": {k: v[0] / args.steps for k, v in prof.items() if v[1]},
             "neighbor_lists": nls}

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libpe_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fopenmp", "--expt-relaxed-constexpr",
               "-I" + INCLUDE]
 
 
@@ -71,7 +71,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=(), out: str =
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, sources()))
     tmp = lib + ".tmp"
-    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-Xcompiler", "-fopenmp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -111,6 +111,7 @@ void free_device(Ctx *c) {
     nbgs_free(c);
     dem_list_free(c);
     adjoint_free(c);
+    stage_free(c);
     c->uploaded = false;
     c->binned = false;
 }
@@ -252,16 +253,23 @@ void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int6
     c->plan_rmax.assign(c->nscenes, 0.0);
     c->plan_count.assign(c->nscenes, 0);
     for (int s = 0; s < c->nscenes; ++s) {
-        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        double rmax = 0.0;
-        for (int64_t k = begin[s]; k < begin[s] + count[s]; ++k) {
-            const int64_t i = order[k];
-            rmax = std::max(rmax, r[i]);
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = std::min(lo[a], x[3 * i + a] - r[i]);
-                hi[a] = std::max(hi[a], x[3 * i + a] + r[i]);
-            }
+        double lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY;
+        double hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY, rmax = 0.0;
+        const int64_t k0 = begin[s], k1 = begin[s] + count[s];
+#pragma omp parallel for schedule(static) \
+    reduction(min : lo0, lo1, lo2) reduction(max : hi0, hi1, hi2, rmax)
+        for (int64_t k = k0; k < k1; ++k) {
+            const int64_t i = order.empty() ? k : order[k];
+            const double ri = r[i];
+            rmax = std::max(rmax, ri);
+            lo0 = std::min(lo0, x[3 * i] - ri);
+            lo1 = std::min(lo1, x[3 * i + 1] - ri);
+            lo2 = std::min(lo2, x[3 * i + 2] - ri);
+            hi0 = std::max(hi0, x[3 * i] + ri);
+            hi1 = std::max(hi1, x[3 * i + 1] + ri);
+            hi2 = std::max(hi2, x[3 * i + 2] + ri);
         }
+        double lo[3] = {lo0, lo1, lo2}, hi[3] = {hi0, hi1, hi2};
         if (count[s] == 0) {
             for (int a = 0; a < 3; ++a) { lo[a] = 0; hi[a] = 1; }
             rmax = 0.5;
@@ -536,16 +544,26 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
     if (n > 0 && (!x || !v || !w || !r || !mat)) return PE_B200_ERR_ARG;
     if (c->mats.empty()) return set_err(c, PE_B200_ERR_STATE, "materials must be set before bodies");
     cudaSetDevice(c->device);
+    // the first invalid sphere (in upload order) decides the error, as pe's createSphere calls
+    // would have failed one at a time; the scan itself runs on all host threads
+    int64_t first_bad = n;
+    const int64_t nmat = (int64_t)c->mats.size();
+#pragma omp parallel for reduction(min : first_bad) schedule(static)
     for (int64_t i = 0; i < n; ++i) {
+        bool ok = r[i] > 0.0 && mat[i] >= 0 && mat[i] < nmat &&
+                  (!scene || (scene[i] >= 0 && scene[i] < nscenes));
+        for (int a = 0; a < 3; ++a)
+            ok = ok && isfinite(x[3 * i + a]) && isfinite(v[3 * i + a]) && isfinite(w[3 * i + a]);
+        if (!ok && i < first_bad) first_bad = i;
+    }
+    if (first_bad < n) {
+        const int64_t i = first_bad;
         // createSphere: the radius must be positive (Sphere.cpp:1193-1194)
         if (!(r[i] > 0.0)) return set_err(c, PE_B200_ERR_ARG, "Invalid sphere radius");
-        if (mat[i] < 0 || (size_t)mat[i] >= c->mats.size())
-            return set_err(c, PE_B200_ERR_ARG, "Invalid material ID");
+        if (mat[i] < 0 || mat[i] >= nmat) return set_err(c, PE_B200_ERR_ARG, "Invalid material ID");
         if (scene && (scene[i] < 0 || scene[i] >= nscenes))
             return set_err(c, PE_B200_ERR_ARG, "Invalid scene ID");
-        for (int a = 0; a < 3; ++a)
-            if (!isfinite(x[3 * i + a]) || !isfinite(v[3 * i + a]) || !isfinite(w[3 * i + a]))
-                return set_err(c, PE_B200_ERR_NAN, "non-finite body state");
+        return set_err(c, PE_B200_ERR_NAN, "non-finite body state");
     }
     free_device(c);
     c->epoch++;
@@ -557,16 +575,21 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
     c->scene_boxes.resize(c->scene_planes.size());
     c->scene_box_mat.resize(c->scene_planes.size());
     // group bodies by scene (stable) for the grid plan
-    std::vector<int64_t> count(nscenes, 0), begin(nscenes, 0), order(n);
-    for (int64_t i = 0; i < n; ++i) count[scene ? scene[i] : 0]++;
-    for (int s = 1; s < nscenes; ++s) begin[s] = begin[s - 1] + count[s - 1];
-    {
+    // (one scene: upload order itself, no permutation array)
+    std::vector<int64_t> count(nscenes, 0), begin(nscenes, 0), order;
+    if (!scene) {
+        count[0] = n;
+    } else {
+        order.resize(n);
+        for (int64_t i = 0; i < n; ++i) count[scene[i]]++;
+        for (int s = 1; s < nscenes; ++s) begin[s] = begin[s - 1] + count[s - 1];
         std::vector<int64_t> fill(begin);
-        for (int64_t i = 0; i < n; ++i) order[fill[scene ? scene[i] : 0]++] = i;
+        for (int64_t i = 0; i < n; ++i) order[fill[scene[i]]++] = i;
     }
     const bool lists = c->p.solver == PE_B200_DEM && c->p.neighbor_lists && n > 0;
     if (lists) {
         double rmin = INFINITY;
+#pragma omp parallel for schedule(static) reduction(min : rmin)
         for (int64_t i = 0; i < n; ++i) rmin = std::min(rmin, r[i]);
         c->nl.skin = c->p.skin > 0.0 ? c->p.skin : 0.1 * rmin;
     }
@@ -580,40 +603,9 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
     if (rc) return rc;
     rc = grid_alloc(c);
     if (rc) return rc;
-    // pack the host arrays into the device layout (upload order)
-    std::vector<double> pr(4 * (size_t)std::max<int64_t>(n, 1));
-    std::vector<uint32_t> tag(std::max<int64_t>(n, 1));
-    std::vector<int32_t> uid(std::max<int64_t>(n, 1));
-    std::vector<char> vw((size_t)std::max<int64_t>(n, 1) * c->vw_bytes);
-    const bool f64 = c->p.precision == PE_B200_FP64;
-    for (int64_t i = 0; i < n; ++i) {
-        pr[4 * i] = x[3 * i];
-        pr[4 * i + 1] = x[3 * i + 1];
-        pr[4 * i + 2] = x[3 * i + 2];
-        pr[4 * i + 3] = r[i];
-        tag[i] = (uint32_t)mat[i] | ((uint32_t)(scene ? scene[i] : 0) << 16);
-        uid[i] = (int32_t)i;
-        for (int a = 0; a < 3; ++a) {
-            if (f64) {
-                ((double *)vw.data())[a * n + i] = v[3 * i + a];
-                ((double *)vw.data())[(3 + a) * n + i] = w[3 * i + a];
-            } else {
-                ((float *)vw.data())[a * n + i] = (float)v[3 * i + a];
-                ((float *)vw.data())[(3 + a) * n + i] = (float)w[3 * i + a];
-            }
-        }
-    }
-    if (n > 0) {
-        PEB_CUDA(c, cudaMemcpy(c->cur.pr, pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(c->cur.vw, vw.data(), n * c->vw_bytes, cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(c->cur.tag, tag.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(c->cur.uid, uid.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
-        if (c->p.track_orientation) {
-            std::vector<double> q(4 * (size_t)n, 0.0);
-            for (int64_t i = 0; i < n; ++i) q[4 * i] = 1.0;
-            PEB_CUDA(c, cudaMemcpy(c->cur.q, q.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-        }
-    }
+    // the caller's arrays go to the device as they are; a kernel packs them
+    rc = pack_bodies(c, x, v, w, r, mat, scene);
+    if (rc) return rc;
     c->uploaded = true;
     c->binned = false;
     if (lists) {
@@ -630,30 +622,9 @@ int pe_b200_set_state(pe_b200_ctx *h, const double *x, const double *v, const do
     cudaSetDevice(c->device);
     const int64_t n = c->n;
     if (n == 0) return PE_B200_OK;
-    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
-    // current order -> upload order map
-    std::vector<int32_t> uid(n);
-    std::vector<double> pr(4 * (size_t)n);
-    std::vector<char> vw((size_t)n * c->vw_bytes);
-    PEB_CUDA(c, cudaMemcpy(uid.data(), c->cur.uid, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    PEB_CUDA(c, cudaMemcpy(pr.data(), c->cur.pr, n * sizeof(double4), cudaMemcpyDeviceToHost));
-    PEB_CUDA(c, cudaMemcpy(vw.data(), c->cur.vw, n * c->vw_bytes, cudaMemcpyDeviceToHost));
-    const bool f64 = c->p.precision == PE_B200_FP64;
-    for (int64_t k = 0; k < n; ++k) {
-        const int64_t i = uid[k];
-        for (int a = 0; a < 3; ++a) {
-            if (x) pr[4 * k + a] = x[3 * i + a];
-            if (f64) {
-                if (v) ((double *)vw.data())[a * n + k] = v[3 * i + a];
-                if (w) ((double *)vw.data())[(3 + a) * n + k] = w[3 * i + a];
-            } else {
-                if (v) ((float *)vw.data())[a * n + k] = (float)v[3 * i + a];
-                if (w) ((float *)vw.data())[(3 + a) * n + k] = (float)w[3 * i + a];
-            }
-        }
-    }
-    PEB_CUDA(c, cudaMemcpy(c->cur.pr, pr.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-    PEB_CUDA(c, cudaMemcpy(c->cur.vw, vw.data(), n * c->vw_bytes, cudaMemcpyHostToDevice));
+    // scattered by the body permutation on the device
+    const int src = scatter_state(c, x, v, w);
+    if (src) return src;
     c->binned = false;
     if (c->nl.enabled) {
         const int rc = dem_list_request_rebuild(c);
@@ -742,32 +713,9 @@ int pe_b200_download_bodies(pe_b200_ctx *h, double *x, double *v, double *w, dou
     cudaSetDevice(c->device);
     const int64_t n = c->n;
     if (n == 0) return PE_B200_OK;
-    std::vector<int32_t> uid(n);
-    std::vector<double> pr(4 * (size_t)n);
-    std::vector<char> vw((size_t)n * c->vw_bytes);
-    std::vector<double> qq(q ? 4 * (size_t)n : 0);
-    PEB_CUDA(c, cudaMemcpyAsync(uid.data(), c->cur.uid, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-    PEB_CUDA(c, cudaMemcpyAsync(pr.data(), c->cur.pr, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-    PEB_CUDA(c, cudaMemcpyAsync(vw.data(), c->cur.vw, n * c->vw_bytes, cudaMemcpyDeviceToHost, c->stream));
-    if (q) PEB_CUDA(c, cudaMemcpyAsync(qq.data(), c->cur.q, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-    int rc = check_device_errors(c);
-    const bool f64 = c->p.precision == PE_B200_FP64;
-    for (int64_t k = 0; k < n; ++k) {
-        const int64_t i = uid[k];
-        if (i < 0 || i >= n) return set_err(c, PE_B200_ERR_STATE, "corrupt body permutation");
-        for (int a = 0; a < 3; ++a) {
-            if (x) x[3 * i + a] = pr[4 * k + a];
-            if (f64) {
-                if (v) v[3 * i + a] = ((double *)vw.data())[a * n + k];
-                if (w) w[3 * i + a] = ((double *)vw.data())[(3 + a) * n + k];
-            } else {
-                if (v) v[3 * i + a] = ((float *)vw.data())[a * n + k];
-                if (w) w[3 * i + a] = ((float *)vw.data())[(3 + a) * n + k];
-            }
-        }
-        if (q)
-            for (int a = 0; a < 4; ++a) q[4 * i + a] = qq[4 * k + a];
-    }
+    const int rc = check_device_errors(c);
+    const int urc = unpack_bodies(c, x, v, w, q);
+    if (urc) return urc;
     return rc;
 }
 

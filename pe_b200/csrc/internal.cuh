@@ -190,6 +190,8 @@ struct Ctx {
     AdjState adj;
     Tuning tune;
     StepGraph sg;
+    void *stage = nullptr;          // host-layout staging for uploads and downloads (transfer.cu)
+    size_t stage_bytes = 0;
     int32_t graph_steps = 16;       // DEM list steps per graph replay; 0 = no graphs
     uint64_t epoch = 1;             // bumped by every change that captured kernels bake in
     // profiling
@@ -288,6 +290,12 @@ void plan_cells(Ctx *c, double skin);
 int upload_tables(Ctx *c);
 // pe_b200_step's loop, shared with the autotuner
 int run_steps(Ctx *c, int32_t nsteps, double dt);
+// transfer.cu: the caller's arrays (upload order, interleaved xyz) <-> the device layout
+int pack_bodies(Ctx *c, const double *x, const double *v, const double *w, const double *r,
+                const int32_t *mat, const int32_t *scene);
+int unpack_bodies(Ctx *c, double *x, double *v, double *w, double *q);
+int scatter_state(Ctx *c, const double *x, const double *v, const double *w);
+void stage_free(Ctx *c);
 // autotune.cu
 int set_list_skin(Ctx *c, double skin);
 int set_tuning(Ctx *c, const Tuning &t, double skin);

@@ -153,9 +153,17 @@ class Engine:
     def step(self, dt: float, nsteps: int = 1):
         self._check(self._L.pe_b200_step(self._h, int(nsteps), float(dt)))
 
-    def download(self):
+    def download(self, out=None):
+        """(x, v, w[, q]) in upload order.  out: arrays to fill instead of new ones (e.g. pinned
+        host buffers reused across calls); each must be C-contiguous float64 of shape (n, 3)."""
         n = self.n
-        x, v, w = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        if out is not None:
+            x, v, w = out[0], out[1], out[2]
+            for a in (x, v, w):
+                if a.dtype != np.float64 or a.shape != (n, 3) or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError("download buffers must be C-contiguous float64 (n, 3)")
+        else:
+            x, v, w = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
         q = np.empty((n, 4)) if self.track_orientation else None
         self._check(self._L.pe_b200_download_bodies(self._h, _p(x), _p(v), _p(w), _p(q)))
         return (x, v, w, q) if self.track_orientation else (x, v, w)
