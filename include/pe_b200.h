@@ -69,7 +69,10 @@ typedef struct {
     double skin;               /* DEM neighbour-list skin; <= 0: 0.1 x the smallest radius */
     int32_t neighbor_lists;    /* DEM: 1 = Verlet lists rebuilt on demand (default),
                                   0 = grid search every step */
-    int32_t reserved;
+    int32_t force_model;       /* DEM normal force law, pe's DEMConfig forceModel
+                                  (pe/config/DEMConfig.h, pe/core/response/ForceModel.h):
+                                  0 = linear spring-dashpot ('basic'), 1 = extended Hertz for
+                                  sphere-sphere contacts ('hertz'; walls stay linear) */
 } pe_b200_params;
 
 /* createMaterial argument list, src/core/Materials.cpp:175 */

@@ -284,6 +284,8 @@ class CollisionSystem {
     void setSolver(int solver);   /* PE_B200_DEM or PE_B200_HCSITS */
     void setPrecision(int prec);  /* PE_B200_FP64 or PE_B200_MIXED */
     void setDevice(int device);
+    /* pe's compile-time DEMConfig forceModel at run time: 0 linear ('basic'), 1 Hertz */
+    void setForceModel(int model);
     int getSolver() const { return p_.solver; }
     int getPrecision() const { return p_.precision; }
     /* number of contacts and NBGS colours of the last step */
@@ -624,6 +626,11 @@ inline void CollisionSystem::setSolver(int solver) {
 inline void CollisionSystem::setPrecision(int prec) {
     if (prec != PE_B200_FP64 && prec != PE_B200_MIXED) throw std::invalid_argument("Invalid precision");
     p_.precision = prec;
+    world_->markParamsDirty();
+}
+inline void CollisionSystem::setForceModel(int model) {
+    if (model != 0 && model != 1) throw std::invalid_argument("Invalid force model");
+    p_.force_model = model;
     world_->markParamsDirty();
 }
 inline void CollisionSystem::setDevice(int device) {

@@ -437,7 +437,18 @@ static int32_t body_mat(const pe_or_world *w, int64_t b) {
     return w->box_mat[b - w->n - w->nplanes];
 }
 
-/* response/DEMSolver.h:176-380 (single-process branch; linear law, forceModel == basic) */
+/* Materials.h:586-600: effective Young's modulus 1/E = (1-nu1^2)/E1 + (1-nu2^2)/E2, in pe's
+ * operation order */
+static double effective_young(const pe_or_material *a, const pe_or_material *b) {
+    const double tmp1 = b->young * (1.0 - a->poisson * a->poisson);
+    const double tmp2 = a->young * (1.0 - b->poisson * b->poisson);
+    return (a->young * b->young) / (tmp1 + tmp2);
+}
+
+/* response/DEMSolver.h:176-380 (single-process branch): the extended Hertz law for sphere-sphere
+ * contacts when forceModel == hertz (:343-357; contacttrait/DEMSolver.h:143-160 for the
+ * effective radius and modulus; other contacts have no effective radius), else the linear
+ * spring-dashpot law (:360-366) */
 static void dem_resolve(const pe_or_world *w, const pe_or_contact *c, double *F, double *T) {
     if (!(c->dist < -THR)) return; /* ContactBase.h:307-310 isPenetrating */
     const v3 gpos = ld3(c->gpos), n = ld3(c->n);
@@ -447,7 +458,16 @@ static void dem_resolve(const pe_or_world *w, const pe_or_contact *c, double *F,
     const double relVelN = -dot(n, rvel);
     const v3 relVel = neg(rvel);
     const v3 relVelT = sub(relVel, mul(n, relVelN));
-    double fNabs = cp.k * delta + cp.cn * relVelN;
+    double fNabs;
+    if (w->force_model == 1 && c->b2 < w->n) {
+        const double r1 = w->r[c->b1], r2 = w->r[c->b2];
+        const double Reff = (r1 * r2) / (r1 + r2);
+        const double Eeff = effective_young(&w->mats[w->mat[c->b1]], &w->mats[w->mat[c->b2]]);
+        const double k = (4.0 / 3.0) * Eeff * sqrt(Reff);
+        fNabs = k * pow(delta, 1.5) + cp.cn * relVelN * pow(delta, 0.5);
+    } else {
+        fNabs = cp.k * delta + cp.cn * relVelN;
+    }
     if (fNabs < 0.0) fNabs = 0.0;
     const v3 fN = smul(fNabs, n);
     const double ft1 = cp.ct * length(relVelT), ft2 = cp.mu * fNabs;

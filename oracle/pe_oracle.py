@@ -29,7 +29,7 @@ class World(C.Structure):
                 ("nplanes", C.c_int32), ("planes", C.c_void_p), ("plane_mat", C.c_void_p),
                 ("nboxes", C.c_int32), ("boxes", C.c_void_p), ("box_mat", C.c_void_p),
                 ("nmat", C.c_int32), ("mats", C.c_void_p), ("gravity", C.c_double * 3),
-                ("damping", C.c_double)]
+                ("damping", C.c_double), ("force_model", C.c_int32)]
 
 
 class Contact(C.Structure):
@@ -80,8 +80,10 @@ def _ptr(a):
 class OracleWorld:
     """FP64 CPU world holding a copy of a pe_b200.scenes.Scene."""
 
-    def __init__(self, scene, track_orientation: bool = False):
+    def __init__(self, scene, track_orientation: bool = False, force_model: int = 0):
+        """force_model: pe's DEMConfig forceModel, 0 basic (linear), 1 hertz."""
         s = scene
+        self.force_model = int(force_model)
         self.x = np.ascontiguousarray(s.x, np.float64).copy()
         self.v = np.ascontiguousarray(s.v, np.float64).copy()
         self.w = np.ascontiguousarray(s.w, np.float64).copy()
@@ -112,6 +114,7 @@ class OracleWorld:
         for a in range(3):
             w.gravity[a] = self.gravity[a]
         w.damping = self.damping
+        w.force_model = self.force_model
         return w
 
     def contacts(self) -> np.ndarray:

@@ -41,7 +41,7 @@ class Params(C.Structure):
                 ("max_iterations", C.c_int32), ("erp", C.c_double),
                 ("gravity", C.c_double * 3), ("damping", C.c_double), ("device", C.c_int32),
                 ("track_orientation", C.c_int32), ("max_contacts", C.c_int64),
-                ("skin", C.c_double), ("neighbor_lists", C.c_int32), ("reserved", C.c_int32)]
+                ("skin", C.c_double), ("neighbor_lists", C.c_int32), ("force_model", C.c_int32)]
 
 
 class Material(C.Structure):

@@ -152,6 +152,8 @@ int upload_tables(Ctx *c) {
         md[k].rct = 1.0 / m.dampingT;
         md[k].csf = m.csf;
         md[k].cdf = m.cdf;
+        md[k].young = m.young;
+        md[k].poisson = m.poisson;
     }
     cudaFree(c->d_mats);
     c->d_mats = nullptr;
@@ -372,6 +374,7 @@ void pe_b200_default_params(pe_b200_params *p) {
     p->max_contacts = 0;
     p->skin = 0.0;
     p->neighbor_lists = 1;
+    p->force_model = 0;
 }
 
 int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
@@ -383,6 +386,7 @@ int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
         p->relaxation_model != PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING)
         return PE_B200_ERR_UNSUPPORTED;
     if (p->max_iterations < 0 || p->damping < 0 || p->damping > 1) return PE_B200_ERR_ARG;
+    if (p->force_model != 0 && p->force_model != 1) return PE_B200_ERR_ARG;
     Ctx *c = new (std::nothrow) Ctx();
     if (!c) return PE_B200_ERR_NOMEM;
     c->p = *p;

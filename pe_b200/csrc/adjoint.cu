@@ -381,9 +381,10 @@ void adjoint_free(Ctx *c) {
 }
 
 int adjoint_forward(Ctx *c, int32_t nsteps, double dt, int32_t every) {
-    if (c->p.solver != PE_B200_DEM || c->p.precision != PE_B200_FP64 || c->p.track_orientation)
+    if (c->p.solver != PE_B200_DEM || c->p.precision != PE_B200_FP64 || c->p.track_orientation ||
+        c->p.force_model != 0)
         return set_err(c, PE_B200_ERR_UNSUPPORTED,
-                       "the adjoint needs the DEM solver in FP64 without orientation tracking");
+                       "the adjoint needs the linear DEM law in FP64 without orientation tracking");
     if (nsteps < 1 || every < 1 || !(dt > 0.0)) return PE_B200_ERR_ARG;
     adjoint_free(c);
     AdjState &A = c->adj;

@@ -57,10 +57,13 @@ __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
 // orientation (n from body 2 to body 1).  r1/r2: contact point relative to the two centres
 // (pe evaluates (gpos - gpos_) for velFromWF and addForceAtPos alike); w2 may be zero (walls).
 // Adds the force on body `self` (1 or 2) to acc.
+// reff > 0 selects the extended Hertz law (sphere-sphere contacts with forceModel == hertz,
+// response/DEMSolver.h:343-357); reff = r1 r2 / (r1 + r2) (contacttrait/DEMSolver.h:152-159)
 template <typename T>
 __device__ __forceinline__ void dem_contact(V3<T> n, T dist, V3<T> r1, V3<T> r2, V3<T> v1,
                                             V3<T> w1, V3<T> v2, V3<T> w2, const MatDev &m1,
-                                            const MatDev &m2, bool self_is_1, Acc<T> &acc) {
+                                            const MatDev &m2, bool self_is_1, Acc<T> &acc,
+                                            T reff = T(0)) {
     // velFromWF, RigidBody.h:1080-1085
     const V3<T> rvel = (v1 + cross(w1, r1)) - (v2 + cross(w2, r2));
     // Contact.cpp:86-105: composed coefficients and the static/dynamic friction pick
@@ -75,7 +78,17 @@ __device__ __forceinline__ void dem_contact(V3<T> n, T dist, V3<T> r1, V3<T> r2,
     const T relVelN = -nvel;
     const V3<T> relVel = -rvel;
     const V3<T> relVelT = relVel - n * relVelN;
-    T fNabs = k * delta + cn * relVelN;
+    T fNabs;
+    if (reff > T(0)) {
+        // Materials.h:586-600, pe's operation order
+        const T tmp1 = T(m2.young) * (T(1) - T(m1.poisson) * T(m1.poisson));
+        const T tmp2 = T(m1.young) * (T(1) - T(m2.poisson) * T(m2.poisson));
+        const T eeff = (T(m1.young) * T(m2.young)) / (tmp1 + tmp2);
+        const T kh = (T(4) / T(3)) * eeff * sqrt(reff);
+        fNabs = kh * pow(delta, T(1.5)) + cn * relVelN * pow(delta, T(0.5));
+    } else {
+        fNabs = k * delta + cn * relVelN;
+    }
     if (fNabs < T(0)) fNabs = T(0);
     const V3<T> fN = fNabs * n;
     const T fTabs = tmin(ct * length(relVelT), mu * fNabs);
@@ -130,11 +143,12 @@ struct DemArgs {
     float *disp;
     int32_t *nl_flags;
     float half_skin;
+    int hertz;        // extended Hertz law for sphere pairs (force_model 1)
 };
 
 // one sphere pair (this body and neighbour j), both in the buffers of `a`; self1: this body is
 // pe's body 1, i.e. has the smaller system id (MaxContacts.h:550-551)
-template <typename T, typename VT>
+template <typename T, typename VT, bool HERTZ>
 __device__ __forceinline__ void pair_force_o(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
                                              V3<T> wi, const MatDev &mi, int32_t j,
                                              const double4 &pj, bool self1, Acc<T> &acc) {
@@ -166,17 +180,18 @@ __device__ __forceinline__ void pair_force_o(const DemArgs<VT> &a, const double4
         r2 = n * k;
         r1 = r2 - d;
     }
+    const T reff = HERTZ ? (T(p1.w) * T(p2.w)) / (T(p1.w) + T(p2.w)) : T(0);
     if (self1)
-        dem_contact<T>(n, T(dist), r1, r2, vi, wi, vj, wj, mi, mj, true, acc);
+        dem_contact<T>(n, T(dist), r1, r2, vi, wi, vj, wj, mi, mj, true, acc, reff);
     else
-        dem_contact<T>(n, T(dist), r1, r2, vj, wj, vi, wi, mj, mi, false, acc);
+        dem_contact<T>(n, T(dist), r1, r2, vj, wj, vi, wi, mj, mi, false, acc, reff);
 }
 
-template <typename T, typename VT>
+template <typename T, typename VT, bool HERTZ>
 __device__ __forceinline__ void pair_force(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
                                            V3<T> wi, int32_t uidi, const MatDev &mi,
                                            int32_t j, const double4 &pj, Acc<T> &acc) {
-    pair_force_o<T, VT>(a, pi, vi, wi, mi, j, pj, uidi < a.uid[j], acc);
+    pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j, pj, uidi < a.uid[j], acc);
 }
 
 // walls of the sphere's scene: planes (MaxContacts.h:777-790), then boxes
@@ -332,7 +347,7 @@ __device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, in
 
 // all grid neighbours of body b (slot cells of the sphere's scene); the bound is conservative
 // for penetrating contacts
-template <typename T, typename VT>
+template <typename T, typename VT, bool HERTZ>
 __device__ __forceinline__ void grid_forces(const DemArgs<VT> &a, const SceneInfo &s, int32_t b,
                                             const double4 &pi, V3<T> vi, V3<T> wi, int32_t uidi,
                                             const MatDev &mi, Acc<T> &acc) {
@@ -355,13 +370,13 @@ __device__ __forceinline__ void grid_forces(const DemArgs<VT> &a, const SceneInf
                 const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
                 const double rs = pi.w + pj.w;
                 if (ddx * ddx + ddy * ddy + ddz * ddz >= rs * rs) continue;
-                pair_force<T, VT>(a, pi, vi, wi, uidi, mi, j, pj, acc);
+                pair_force<T, VT, HERTZ>(a, pi, vi, wi, uidi, mi, j, pj, acc);
             }
         }
     }
 }
 
-template <typename VT, bool TRACKQ>
+template <typename VT, bool TRACKQ, bool HERTZ>
 __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     using T = VT;  // arithmetic type of the contact law (double or float)
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -376,7 +391,7 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     Acc<T> acc;
     acc.F = v3(T(0), T(0), T(0));
     acc.T_ = acc.F;
-    grid_forces<T, VT>(a, s, b, pi, vi, wi, uidi, mi, acc);
+    grid_forces<T, VT, HERTZ>(a, s, b, pi, vi, wi, uidi, mi, acc);
     wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
     V3<T> v;
     const double4 o = integrate<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v);
@@ -404,7 +419,7 @@ constexpr DemShape kDemShapes[] = {{kDemBlock, PEB_LIST_MIN_BLOCKS_F32, 5},
 constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]));
 
 // list step: body t stays at index t (the order changes only at rebuilds)
-template <typename VT, bool TRACKQ, int BLOCK, int MINB>
+template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool HERTZ>
 __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -426,7 +441,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
         // a body without candidates at the last rebuild has no contact partner before the
         // next one, lists or not; the others read whether that rebuild's lists fit
         if (k < e && a.nl_flags[1] != 0) {
-            grid_forces<T, VT>(a, s, (int32_t)t, pi, vi, wi, a.uid[t], mi, acc);
+            grid_forces<T, VT, HERTZ>(a, s, (int32_t)t, pi, vi, wi, a.uid[t], mi, acc);
         } else if (k < e) {
             // entries: neighbour index, top bit set when this body is pe's body 1; two at a
             // time so their loads overlap
@@ -434,13 +449,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
                 const uint32_t e0 = (uint32_t)a.nl_idx[k], e1 = (uint32_t)a.nl_idx[k + 1];
                 const int32_t j0 = (int32_t)(e0 & 0x7fffffffu), j1 = (int32_t)(e1 & 0x7fffffffu);
                 const double4 p0 = a.pr[j0], p1 = a.pr[j1];
-                pair_force_o<T, VT>(a, pi, vi, wi, mi, j0, p0, (e0 >> 31) != 0u, acc);
-                pair_force_o<T, VT>(a, pi, vi, wi, mi, j1, p1, (e1 >> 31) != 0u, acc);
+                pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j0, p0, (e0 >> 31) != 0u, acc);
+                pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j1, p1, (e1 >> 31) != 0u, acc);
             }
             if (k < e) {
                 const uint32_t e0 = (uint32_t)a.nl_idx[k];
                 const int32_t j0 = (int32_t)(e0 & 0x7fffffffu);
-                pair_force_o<T, VT>(a, pi, vi, wi, mi, j0, a.pr[j0], (e0 >> 31) != 0u, acc);
+                pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j0, a.pr[j0], (e0 >> 31) != 0u, acc);
             }
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
@@ -495,6 +510,7 @@ DemArgs<VT> dem_args(Ctx *c, double dt) {
     a.disp = c->nl.disp;
     a.nl_flags = c->nl.flags;
     a.half_skin = float(0.5 * c->nl.skin * (1.0 - 1e-5));
+    a.hertz = c->p.force_model == 1 ? 1 : 0;
     return a;
 }
 
@@ -502,10 +518,14 @@ template <typename VT>
 int launch_dem(Ctx *c, double dt) {
     DemArgs<VT> a = dem_args<VT>(c, dt);
     prof_begin(c, ST_DEM);
-    if (c->p.track_orientation)
-        k_dem_step<VT, true><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
-    else
-        k_dem_step<VT, false><<<grid_for(c->n, kDemBlock), kDemBlock, 0, c->stream>>>(a);
+    const unsigned g = grid_for(c->n, kDemBlock);
+    if (a.hertz) {
+        if (c->p.track_orientation) k_dem_step<VT, true, true><<<g, kDemBlock, 0, c->stream>>>(a);
+        else k_dem_step<VT, false, true><<<g, kDemBlock, 0, c->stream>>>(a);
+    } else {
+        if (c->p.track_orientation) k_dem_step<VT, true, false><<<g, kDemBlock, 0, c->stream>>>(a);
+        else k_dem_step<VT, false, false><<<g, kDemBlock, 0, c->stream>>>(a);
+    }
     PEB_LAUNCHED(c);
     prof_end(c, ST_DEM);
     return PE_B200_OK;
@@ -677,12 +697,12 @@ int list_rebuild(Ctx *c) {
     return PE_B200_OK;
 }
 
-template <typename VT, bool TRACKQ, int V>
+template <typename VT, bool TRACKQ, int V, bool HERTZ>
 void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
-    k_dem_list<VT, TRACKQ, B, M><<<grid_for(c->n, B), B, 0, c->stream>>>(a);
+    k_dem_list<VT, TRACKQ, B, M, HERTZ><<<grid_for(c->n, B), B, 0, c->stream>>>(a);
 }
 
 template <typename VT>
@@ -708,16 +728,20 @@ int list_step(Ctx *c, double dt) {
     DemArgs<VT> a = dem_args<VT>(c, dt);
     a.sorted = nullptr;   // the grid fallback sees the state in cell order
     prof_begin(c, ST_DEM);
-    if (c->p.track_orientation)
-        launch_list_shape<VT, true, 0>(c, a);
+    // the Hertz law and orientation tracking run the default launch shape
+    if (a.hertz)
+        c->p.track_orientation ? launch_list_shape<VT, true, 0, true>(c, a)
+                               : launch_list_shape<VT, false, 0, true>(c, a);
+    else if (c->p.track_orientation)
+        launch_list_shape<VT, true, 0, false>(c, a);
     else
         switch (c->tune.dem_variant) {
-            case 1: launch_list_shape<VT, false, 1>(c, a); break;
-            case 2: launch_list_shape<VT, false, 2>(c, a); break;
-            case 3: launch_list_shape<VT, false, 3>(c, a); break;
-            case 4: launch_list_shape<VT, false, 4>(c, a); break;
-            case 5: launch_list_shape<VT, false, 5>(c, a); break;
-            default: launch_list_shape<VT, false, 0>(c, a); break;
+            case 1: launch_list_shape<VT, false, 1, false>(c, a); break;
+            case 2: launch_list_shape<VT, false, 2, false>(c, a); break;
+            case 3: launch_list_shape<VT, false, 3, false>(c, a); break;
+            case 4: launch_list_shape<VT, false, 4, false>(c, a); break;
+            case 5: launch_list_shape<VT, false, 5, false>(c, a); break;
+            default: launch_list_shape<VT, false, 0, false>(c, a); break;
         }
     PEB_LAUNCHED(c);
     prof_end(c, ST_DEM);
@@ -985,8 +1009,9 @@ cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream) {
     a.disp = nullptr;
     a.nl_flags = nullptr;
     a.half_skin = 0.f;
+    a.hertz = 0;
     if (r.n > 0)
-        k_dem_step<double, false><<<grid_for(r.n, kDemBlock), kDemBlock, 0, stream>>>(a);
+        k_dem_step<double, false, false><<<grid_for(r.n, kDemBlock), kDemBlock, 0, stream>>>(a);
     return cudaGetLastError();
 }
 

@@ -47,6 +47,7 @@ struct MatDev {
     double density;
     double rk, rcn, rct;   // 1/stiffness, 1/dampingN, 1/dampingT
     double csf, cdf;
+    double young, poisson; // the extended Hertz law's effective modulus (Materials.h:586-600)
 };
 
 struct BodyBuf {

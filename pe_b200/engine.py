@@ -23,7 +23,8 @@ class Engine:
                  relaxation_model: int = _abi.APPROX_INELASTIC_COULOMB_DECOUPLING,
                  max_iterations: int = 100, erp: float = 0.7, gravity=(0.0, 0.0, 0.0),
                  damping: float = 1.0, device: int = 0, track_orientation: bool = False,
-                 max_contacts: int = 0, neighbor_lists: bool = True, skin: float = 0.0):
+                 max_contacts: int = 0, neighbor_lists: bool = True, skin: float = 0.0,
+                 force_model: int = 0):
         self._L = _abi.load()
         p = _abi.default_params()
         p.solver, p.precision = solver, precision
@@ -35,6 +36,7 @@ class Engine:
         p.max_contacts = max_contacts
         p.neighbor_lists = 1 if neighbor_lists else 0
         p.skin = float(skin)
+        p.force_model = int(force_model)
         h = C.c_void_p()
         self._check(self._L.pe_b200_create(C.byref(p), C.byref(h)), ctx=None)
         self._h = h

@@ -40,14 +40,14 @@ def run_steps(exe, scene_path, n, steps, tmp, extra=()):
             a[9 * n:].reshape(n, 4))
 
 
-def golden(name, scene, dem_steps=(1, 10), hc=True, hc_converged=False):
+def golden(name, scene, dem_steps=(1, 10), hc=True, hc_converged=False, dem_exe="ref_dem"):
     with tempfile.TemporaryDirectory() as tmp:
         sp = os.path.join(tmp, "scene.bin")
         scene.save(sp)
         rec = {"scene": np.frombuffer(scene.to_bytes(), np.uint8)}
-        rec["pairs"] = run_pairs("ref_dem", sp, tmp)
+        rec["pairs"] = run_pairs(dem_exe, sp, tmp)
         for k in dem_steps:
-            x, v, w, q = run_steps("ref_dem", sp, scene.n, k, tmp)
+            x, v, w, q = run_steps(dem_exe, sp, scene.n, k, tmp)
             rec[f"dem{k}_x"], rec[f"dem{k}_v"], rec[f"dem{k}_w"], rec[f"dem{k}_q"] = x, v, w, q
         if hc:
             rec["hc_pairs"] = run_pairs("ref_hcsits", sp, tmp)
@@ -61,6 +61,16 @@ def golden(name, scene, dem_steps=(1, 10), hc=True, hc_converged=False):
     path = os.path.join(OUT, name + ".npz")
     np.savez_compressed(path, **rec)
     print(path, os.path.getsize(path), "bytes,", len(rec["pairs"]), "contacts")
+
+
+def hertz_scene(seed, n=64, with_boxes=False):
+    """small_random with two materials whose Young's moduli and Poisson ratios differ, for pe's
+    extended Hertz law (sphere-sphere contacts)."""
+    s = scenes.small_random(seed, n=n, with_boxes=with_boxes)
+    s.materials = np.stack([scenes.material(1.0, 1e5, 50.0, 40.0, 0.3, young=2e6, poisson=0.3),
+                            scenes.material(2.0, 2e5, 30.0, 20.0, 0.15, young=5e6, poisson=0.2)])
+    s.name = f"hertz_{seed}_{n}"
+    return s
 
 
 def adjoint_fd(name="adjoint_fd", seed=2, n=64, steps=40):
@@ -97,9 +107,18 @@ def adjoint_fd(name="adjoint_fd", seed=2, n=64, steps=40):
     print(path, os.path.getsize(path), "bytes, loss", rec["loss"])
 
 
+def hertz_goldens():
+    golden("hertz64_boxes", hertz_scene(1, with_boxes=True), dem_steps=(1, 10), hc=False,
+           dem_exe="ref_dem_hertz")
+    golden("hertz64_planes", hertz_scene(2), dem_steps=(1, 10), hc=False, dem_exe="ref_dem_hertz")
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["adjoint_fd"]:
         adjoint_fd()
+        sys.exit(0)
+    if sys.argv[1:] == ["hertz"]:
+        hertz_goldens()
         sys.exit(0)
     golden("small64_boxes", scenes.small_random(1, n=64, with_boxes=True))
     golden("small64_planes", scenes.small_random(2, n=64, with_boxes=False))
@@ -112,3 +131,4 @@ if __name__ == "__main__":
     golden("loose125_boxes", scenes.small_random(4, n=125, overlap=0.0, with_boxes=True),
            dem_steps=(1,), hc_converged=True)
     adjoint_fd()
+    hertz_goldens()

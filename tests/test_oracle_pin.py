@@ -113,3 +113,20 @@ def test_oracle_finite_differences_match_reference():
         pm[key] -= h
         f = (loss(set_params(s, **pp)) - loss(set_params(s, **pm))) / (2 * h)
         assert abs(f - float(g["fd_" + key])) < 1e-7 * abs(float(g["fd_" + key])) + 1e-12, key
+
+
+@pytest.mark.parametrize("name", ["hertz64_boxes", "hertz64_planes"])
+def test_hertz_dem_steps_match_reference(name):
+    """pe's extended Hertz law (forceModel = hertz, compiled into ref_dem_hertz) against the
+    oracle's restatement: sphere pairs use the Hertz law, walls the linear one."""
+    g = load_golden(name)
+    for k in (1, 10):
+        o = OracleWorld(g["scene"], force_model=1)
+        o.dem_step(g["scene"].dt, k)
+        assert rel_err(o.x, g[f"dem{k}_x"]) < 1e-13
+        assert rel_err(o.v, g[f"dem{k}_v"]) < 1e-12
+        assert rel_err_w(o.w, g[f"dem{k}_w"], g[f"dem{k}_v"], g["scene"].r) < 1e-12
+    # the linear law gives a different trajectory: the golden vectors do pin the Hertz branch
+    o = OracleWorld(g["scene"], force_model=0)
+    o.dem_step(g["scene"].dt, 10)
+    assert rel_err(o.v, g["dem10_v"]) > 1e-3
