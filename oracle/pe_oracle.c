@@ -584,15 +584,12 @@ static inline v3 wf_imp(const body_props *bp, int64_t b, v3 r, v3 p) {
 static inline void hc_apply(const body_props *bp, hc_bodies *B, const hc_contact *h, v3 p,
                             double sign) {
     /* dv1 += sign*im1*p; dw1 += sign*Iinv1*(r1 x p); body 2 with the opposite sign.  Walls
-     * carry zero inverse mass and inertia, so their corrections stay exactly zero. */
-    if (h->b1 < bp->n) {
-        B->dv[h->b1] = add(B->dv[h->b1], smul(sign, smul(bp->im[h->b1], p)));
-        B->dw[h->b1] = add(B->dw[h->b1], smul(sign, wf_imp(bp, h->b1, h->r1, p)));
-    }
-    if (h->b2 < bp->n) {
-        B->dv[h->b2] = sub(B->dv[h->b2], smul(sign, smul(bp->im[h->b2], p)));
-        B->dw[h->b2] = sub(B->dw[h->b2], smul(sign, wf_imp(bp, h->b2, h->r2, p)));
-    }
+     * carry zero inverse mass and inertia, so their corrections stay zero as in pe -- unless an
+     * impulse is not finite, which pe then spreads through the wall as well. */
+    B->dv[h->b1] = add(B->dv[h->b1], smul(sign, smul(bp->im[h->b1], p)));
+    B->dw[h->b1] = add(B->dw[h->b1], smul(sign, wf_imp(bp, h->b1, h->r1, p)));
+    B->dv[h->b2] = sub(B->dv[h->b2], smul(sign, smul(bp->im[h->b2], p)));
+    B->dw[h->b2] = sub(B->dw[h->b2], smul(sign, wf_imp(bp, h->b2, h->r2, p)));
 }
 
 static inline v3 hc_gdot(const hc_bodies *B, const hc_contact *h) {
@@ -678,6 +675,279 @@ static double relax_approx_coulomb(const body_props *bp, hc_bodies *B, hc_contac
     return delta_max;
 }
 
+/* HardContactSemiImplicitTimesteppingSolvers.h:2631-2723: one projected Jacobi-like update
+ * per contact with relaxation w = 1, then the projection onto the friction cone (approximate:
+ * the plain residual D p + gdot; exact: its normal part raised by mu |(D p + gdot)_to|) */
+static double relax_orthogonal(const body_props *bp, hc_bodies *B, hc_contact *C, int64_t nc,
+                               double dtinv, int approximate) {
+    double delta_max = 0.0;
+    for (int64_t i = 0; i < nc; ++i) {
+        hc_contact *h = &C[i];
+        hc_apply(bp, B, h, h->p, -1.0);
+        const v3 gdot = hc_gdot(B, h);
+        const m3 cf = m3_cols(h->n, h->t, h->o);
+        v3 g = m3_mulv(m3_trans(cf), gdot);
+        g.x += h->dist * dtinv;
+        const double w = 1.0;
+        v3 pcf = m3_mulv(m3_trans(cf), h->p);
+        if (approximate) {
+            pcf = sub(pcf, smul(w, add(m3_mulv(h->D, pcf), g)));
+        } else {
+            v3 tmp = add(m3_mulv(h->D, pcf), g);
+            tmp.x += sqrt(tmp.y * tmp.y + tmp.z * tmp.z) * h->mu;
+            pcf = sub(pcf, smul(w, tmp));
+        }
+        const double flimit = h->mu * pcf.x;
+        const double fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+        if (pcf.x > 0.0 && fsq < flimit * flimit) {
+            /* inside the cone */
+        } else if (pcf.x < 0.0 && fsq < pcf.x / (h->mu * h->mu)) {
+            pcf = mk(0.0, 0.0, 0.0);
+        } else {
+            const double f = sqrt(fsq);
+            pcf.x = (f * h->mu + pcf.x) / (h->mu * h->mu + 1.0);
+            const double factor = h->mu * pcf.x / f;
+            pcf.y *= factor;
+            pcf.z *= factor;
+        }
+        const v3 p_wf = m3_mulv(cf, pcf);
+        delta_max = fmax(delta_max, maxabs3(sub(h->p, p_wf)));
+        h->p = p_wf;
+        hc_apply(bp, B, h, h->p, 1.0);
+    }
+    return delta_max;
+}
+
+/* 2x2 helpers in pe's evaluation order: Matrix2 * Vector2 and trans(a) * b */
+static inline void m2_mulv(double a00, double a01, double a10, double a11, double x0, double x1,
+                           double *y0, double *y1) {
+    *y0 = a00 * x0 + a01 * x1;
+    *y1 = a10 * x0 + a11 * x1;
+}
+/* real(0.5) * trans(x) * (A * x) - trans(x) * b, left to right */
+static inline double quad2(double a00, double a01, double a10, double a11, double x0, double x1,
+                           double b0, double b1) {
+    double y0, y1;
+    m2_mulv(a00, a01, a10, a11, x0, x1, &y0, &y1);
+    return ((0.5 * x0) * y0 + (0.5 * x1) * y1) - (x0 * b0 + x1 * b1);
+}
+
+/* HardContactSemiImplicitTimesteppingSolvers.h:2330-2595: exact Coulomb friction by
+ * alternating normal and tangential one-contact solves (20 rounds); a tangential solution
+ * outside the cone is replaced by the minimiser of the tangential energy on the cone's circle,
+ * found by a golden-section search over the angle (maxSubIterations = 20, HCSITS.h:423) */
+static double relax_coulomb_decoupling(const body_props *bp, hc_bodies *B, hc_contact *C,
+                                       int64_t nc, double dtinv) {
+    double delta_max = 0.0;
+    for (int64_t i = 0; i < nc; ++i) {
+        hc_contact *h = &C[i];
+        hc_apply(bp, B, h, h->p, -1.0);
+        const v3 gdot = hc_gdot(B, h);
+        const m3 cf = m3_cols(h->n, h->t, h->o);
+        v3 g = m3_mulv(m3_trans(cf), gdot);
+        g.x += h->dist * dtinv;
+        if (g.x >= 0.0) {
+            delta_max = fmax(delta_max, maxabs3(h->p));
+            h->p = mk(0.0, 0.0, 0.0);
+            continue;
+        }
+        v3 pcf = neg(m3_mulv(h->Dinv, g));
+        double flimit = h->mu * pcf.x;
+        double fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+        if (fsq > flimit * flimit || pcf.x < 0.0) {
+            for (int j = 0; j < 20; ++j) {
+                pcf.x = 0.0;
+                const v3 pto = add(mul(h->t, pcf.y), mul(h->o, pcf.z));
+                v3 gc = add(add(gdot, cross(wf_imp(bp, h->b1, h->r1, pto), h->r1)),
+                            cross(wf_imp(bp, h->b2, h->r2, pto), h->r2));
+                const double gc_n = dot(h->n, gc) + h->dist * dtinv;
+                pcf.x = fmax(0.0, -(h->Dn_inv * gc_n));
+                pcf.y = pcf.z = 0.0;
+                const v3 pn = mul(h->n, pcf.x);
+                gc = add(add(gdot, cross(wf_imp(bp, h->b1, h->r1, pn), h->r1)),
+                         cross(wf_imp(bp, h->b2, h->r2, pn), h->r2));
+                const double gt = dot(h->t, gc), go = dot(h->o, gc);
+                double r0, r1;
+                m2_mulv(h->Dto_inv[0], h->Dto_inv[1], h->Dto_inv[2], h->Dto_inv[3], gt, go, &r0, &r1);
+                pcf.y = -r0;
+                pcf.z = -r1;
+                flimit = h->mu * pcf.x;
+                fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+                if (fsq > flimit * flimit) {
+                    const double a00 = h->D.m[4], a01 = h->D.m[5], a10 = h->D.m[7], a11 = h->D.m[8];
+                    const double f = flimit / sqrt(fsq);
+                    const double phi = 0.5 * (1.0 + sqrt(5.0));
+                    const double shift = atan2(-pcf.z, pcf.y);
+                    const double acos_f = acos(f);
+                    double alpha_left = -acos_f - shift;
+                    double alpha_right = acos_f - shift;
+                    double alpha_mid = (alpha_right + alpha_left * phi) / (1.0 + phi);
+                    double xm0 = flimit * cos(alpha_mid), xm1 = flimit * sin(alpha_mid);
+                    double f_mid = quad2(a00, a01, a10, a11, xm0, xm1, -gt, -go);
+                    int leftlarger = 0;
+                    for (int k = 0; k < 20; ++k) {
+                        const double alpha_next = alpha_left + (alpha_right - alpha_mid);
+                        const double xn0 = flimit * cos(alpha_next), xn1 = flimit * sin(alpha_next);
+                        const double f_next = quad2(a00, a01, a10, a11, xn0, xn1, -gt, -go);
+                        if (leftlarger) {
+                            if (f_next < f_mid) {
+                                alpha_right = alpha_mid; alpha_mid = alpha_next;
+                                xm0 = xn0; xm1 = xn1; f_mid = f_next; leftlarger = 1;
+                            } else {
+                                alpha_left = alpha_next; leftlarger = 0;
+                            }
+                        } else {
+                            if (f_next < f_mid) {
+                                alpha_left = alpha_mid; alpha_mid = alpha_next;
+                                xm0 = xn0; xm1 = xn1; f_mid = f_next; leftlarger = 0;
+                            } else {
+                                alpha_right = alpha_next; leftlarger = 1;
+                            }
+                        }
+                    }
+                    pcf.y = xm0;
+                    pcf.z = xm1;
+                }
+            }
+        }
+        const v3 p_wf = m3_mulv(cf, pcf);
+        delta_max = fmax(delta_max, maxabs3(sub(h->p, p_wf)));
+        h->p = p_wf;
+        hc_apply(bp, B, h, h->p, 1.0);
+    }
+    return delta_max;
+}
+
+/* r_ub of the generalized maximum dissipation search (HCSITS.h:2890-2895) */
+static inline double gmd_radius(const hc_contact *h, double gn, double a3, double alpha,
+                                double shiftI) {
+    double r = h->mu * (-gn) / (h->D.m[0] + h->mu * a3 * cos(alpha + shiftI));
+    if (r < 0.0) r = INFINITY;
+    return r;
+}
+
+/* HardContactSemiImplicitTimesteppingSolvers.h:2745-3055: friction by the generalized maximum
+ * dissipation principle: the tangential impulse minimising the kinetic energy on the
+ * intersection of the plane of maximum compression with the friction cone, by a golden-section
+ * search over the angle */
+static double relax_gmd(const body_props *bp, hc_bodies *B, hc_contact *C, int64_t nc,
+                        double dtinv) {
+    double delta_max = 0.0;
+    for (int64_t i = 0; i < nc; ++i) {
+        hc_contact *h = &C[i];
+        hc_apply(bp, B, h, h->p, -1.0);
+        const v3 gdot = hc_gdot(B, h);
+        const m3 cf = m3_cols(h->n, h->t, h->o);
+        v3 g = m3_mulv(m3_trans(cf), gdot);
+        g.x += h->dist * dtinv;
+        if (g.x >= 0.0) {
+            delta_max = fmax(delta_max, maxabs3(h->p));
+            h->p = mk(0.0, 0.0, 0.0);
+            continue;
+        }
+        v3 pcf = neg(m3_mulv(h->Dinv, g));
+        const double flimit = h->mu * pcf.x;
+        const double fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+        if (fsq > flimit * flimit || pcf.x < 0.0) {
+            const double *D = h->D.m;
+            const double invA_nn = 1.0 / D[0];
+            const double offdiag = D[5] - invA_nn * D[1] * D[2];
+            const double A00 = D[4] - invA_nn * (D[1] * D[1]), A01 = offdiag, A10 = offdiag;
+            const double A11 = D[8] - invA_nn * (D[2] * D[2]);
+            const double bb0 = -g.y + invA_nn * D[1] * g.x, bb1 = -g.z + invA_nn * D[2] * g.x;
+            const double shiftI = atan2(-D[2], D[1]);
+            const double shiftJ = atan2(-pcf.z, pcf.y);
+            const double a3 = sqrt(D[1] * D[1] + D[2] * D[2]);
+            const double fractionI = -D[0] / (h->mu * a3);
+            const double fractionJ =
+                fmin(invA_nn * h->mu * ((-g.x) / sqrt(fsq) - a3 * cos(shiftI - shiftJ)), 1.0);
+            double alpha_left, alpha_right;
+            if (fractionJ < -1.0) {
+                const double angleI = acos(fractionI);
+                alpha_left = -angleI - shiftI;
+                alpha_right = +angleI - shiftI;
+                if (alpha_left < 0.0) {
+                    alpha_left += 2 * M_PI;
+                    alpha_right += 2 * M_PI;
+                }
+            } else if (D[0] > h->mu * a3) {
+                const double angleJ = acos(fractionJ);
+                alpha_left = -angleJ - shiftJ;
+                alpha_right = +angleJ - shiftJ;
+                if (alpha_left < 0.0) {
+                    alpha_left += 2 * M_PI;
+                    alpha_right += 2 * M_PI;
+                }
+            } else {
+                const double angleJ = acos(fractionJ);
+                double a1l = -angleJ - shiftJ, a1r = +angleJ - shiftJ;
+                if (a1l < 0.0) { a1l += 2 * M_PI; a1r += 2 * M_PI; }
+                const double angleI = acos(fractionI);
+                double a2l = -angleI - shiftI, a2r = +angleI - shiftI;
+                if (a2l < 0.0) { a2l += 2 * M_PI; a2r += 2 * M_PI; }
+                if (a1l > a2l) {
+                    double t0 = a1l; a1l = a2l; a2l = t0;
+                    t0 = a1r; a1r = a2r; a2r = t0;
+                }
+                if (a2l > a1r) {
+                    a2r -= 2 * M_PI;
+                    if (!(a2r > a1r)) a1r = a2r;
+                } else {
+                    a1l = a2l;
+                    if (!(a2r > a1r)) a1r = a2r;
+                }
+                alpha_left = a1l;
+                alpha_right = a1r;
+            }
+            const double phi = 0.5 * (1.0 + sqrt(5.0));
+            double alpha_mid = (alpha_right + alpha_left * phi) / (1.0 + phi);
+            double r = gmd_radius(h, g.x, a3, alpha_mid, shiftI);
+            double xm0 = r * cos(alpha_mid), xm1 = r * sin(alpha_mid);
+            double f_mid = quad2(A00, A01, A10, A11, xm0, xm1, bb0, bb1);
+            int leftlarger = 0;
+            for (int k = 0; k < 20; ++k) {
+                const double alpha_next = alpha_left + (alpha_right - alpha_mid);
+                r = gmd_radius(h, g.x, a3, alpha_next, shiftI);
+                const double xn0 = r * cos(alpha_next), xn1 = r * sin(alpha_next);
+                const double f_next = quad2(A00, A01, A10, A11, xn0, xn1, bb0, bb1);
+                if (leftlarger) {
+                    if (f_next < f_mid) {
+                        alpha_right = alpha_mid; alpha_mid = alpha_next;
+                        xm0 = xn0; xm1 = xn1; f_mid = f_next; leftlarger = 1;
+                    } else {
+                        alpha_left = alpha_next; leftlarger = 0;
+                    }
+                } else {
+                    if (f_next < f_mid) {
+                        alpha_left = alpha_mid; alpha_mid = alpha_next;
+                        xm0 = xn0; xm1 = xn1; f_mid = f_next; leftlarger = 0;
+                    } else {
+                        alpha_right = alpha_next; leftlarger = 1;
+                    }
+                }
+            }
+            {
+                const double alpha_init = atan2(pcf.z, pcf.y);
+                r = gmd_radius(h, g.x, a3, alpha_init, shiftI);
+                const double xi0 = r * cos(alpha_init), xi1 = r * sin(alpha_init);
+                const double f_init = quad2(A00, A01, A10, A11, xi0, xi1, bb0, bb1);
+                if (f_init < f_mid) {
+                    xm0 = xi0;
+                    xm1 = xi1;
+                }
+            }
+            pcf.x = invA_nn * (-g.x - D[1] * xm0 - D[2] * xm1);
+            pcf.y = xm0;
+            pcf.z = xm1;
+        }
+        const v3 p_wf = m3_mulv(cf, pcf);
+        delta_max = fmax(delta_max, maxabs3(sub(h->p, p_wf)));
+        h->p = p_wf;
+        hc_apply(bp, B, h, h->p, 1.0);
+    }
+    return delta_max;
+}
+
 /* Complementarity residual of the final impulses, in velocity units (max over contacts):
  *   normal:   |min(p_n * D_nn, gdot_n)|                (0 <= p_n  _|_  gdot_n >= 0)
  *   cone:     max(0, |p_to| - mu p_n) * D_nn           (|p_to| <= mu p_n)
@@ -734,8 +1004,15 @@ static int64_t hcsits_run(pe_or_world *w, double dt, int model, int max_iter, do
     const double dtinv = 1.0 / dt;
     double delta = 0.0;
     for (int it = 0; it < max_iter; ++it) {
-        if (model == PE_OR_FRICTIONLESS) delta = relax_frictionless(&bp, &B, C, nc, dtinv);
-        else delta = relax_approx_coulomb(&bp, &B, C, nc, dtinv);
+        /* the switch of HardContactSemiImplicitTimesteppingSolvers.h:1900-1926 */
+        switch (model) {
+            case PE_OR_FRICTIONLESS: delta = relax_frictionless(&bp, &B, C, nc, dtinv); break;
+            case PE_OR_APPROX_COULOMB_DECOUPLING: delta = relax_approx_coulomb(&bp, &B, C, nc, dtinv); break;
+            case PE_OR_APPROX_COULOMB_ORTHOGONAL: delta = relax_orthogonal(&bp, &B, C, nc, dtinv, 1); break;
+            case PE_OR_COULOMB_DECOUPLING: delta = relax_coulomb_decoupling(&bp, &B, C, nc, dtinv); break;
+            case PE_OR_COULOMB_ORTHOGONAL: delta = relax_orthogonal(&bp, &B, C, nc, dtinv, 0); break;
+            default: delta = relax_gmd(&bp, &B, C, nc, dtinv); break;
+        }
     }
     if (delta_out) *delta_out = delta;
     if (resid_out) *resid_out = hc_residual(&B, C, nc, dtinv, model != PE_OR_FRICTIONLESS);
@@ -759,7 +1036,7 @@ static int64_t hcsits_run(pe_or_world *w, double dt, int model, int max_iter, do
 int64_t pe_or_hcsits_step_contacts(pe_or_world *w, double dt, int model, int max_iter,
                                    double erp, const pe_or_contact *contacts, int64_t nc,
                                    double *delta_out, double *resid_out) {
-    if (dt <= 0.0 || (model != PE_OR_FRICTIONLESS && model != PE_OR_APPROX_COULOMB_DECOUPLING))
+    if (dt <= 0.0 || model < PE_OR_FRICTIONLESS || model > PE_OR_GENERALIZED_MAX_DISSIPATION)
         return -2;
     return hcsits_run(w, dt, model, max_iter, erp, contacts, nc, delta_out, resid_out);
 }
@@ -767,7 +1044,7 @@ int64_t pe_or_hcsits_step_contacts(pe_or_world *w, double dt, int model, int max
 int64_t pe_or_hcsits_step(pe_or_world *w, double dt, int model, int max_iter, double erp,
                           const int64_t *order, int64_t norder, double *delta_out,
                           double *resid_out) {
-    if (dt <= 0.0 || (model != PE_OR_FRICTIONLESS && model != PE_OR_APPROX_COULOMB_DECOUPLING))
+    if (dt <= 0.0 || model < PE_OR_FRICTIONLESS || model > PE_OR_GENERALIZED_MAX_DISSIPATION)
         return -2;
     clist l;
     if (find_contacts_list(w, &l) != 0) return -1;

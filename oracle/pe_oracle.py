@@ -16,6 +16,10 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libpe_oracle.so")
 
 FRICTIONLESS = 0
 APPROX_COULOMB_DECOUPLING = 1
+APPROX_COULOMB_ORTHOGONAL = 2
+COULOMB_DECOUPLING = 3
+COULOMB_ORTHOGONAL = 4
+GENERALIZED_MAX_DISSIPATION = 5
 
 
 class Material(C.Structure):

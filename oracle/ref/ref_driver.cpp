@@ -121,8 +121,8 @@ void configure_solver(int argc, char** argv, int first) {
     int model = argc > first ? std::atoi(argv[first]) : 0;
     int maxit = argc > first + 1 ? std::atoi(argv[first + 1]) : 100;
     typedef CollisionSystem<Config> CS;
-    theCollisionSystem()->setRelaxationModel(model == 0 ? CS::InelasticFrictionlessContact
-                                             : CS::ApproximateInelasticCoulombContactByDecoupling);
+    // pe's RelaxationModel values 0-5 (HardContactSemiImplicitTimesteppingSolvers.h:172-179)
+    theCollisionSystem()->setRelaxationModel(static_cast<typename CS::RelaxationModel>(model));
     theCollisionSystem()->setMaxIterations(static_cast<size_t>(maxit));
 #else
     (void)argc; (void)argv; (void)first;

@@ -51,7 +51,7 @@ def golden(name, scene, dem_steps=(1, 10), hc=True, hc_converged=False, dem_exe=
             rec[f"dem{k}_x"], rec[f"dem{k}_v"], rec[f"dem{k}_w"], rec[f"dem{k}_q"] = x, v, w, q
         if hc:
             rec["hc_pairs"] = run_pairs("ref_hcsits", sp, tmp)
-            for model in (0, 1):
+            for model in (0, 1, 2, 3, 4, 5):
                 x, v, w, q = run_steps("ref_hcsits", sp, scene.n, 1, tmp, (model, 100))
                 rec[f"hc{model}_x"], rec[f"hc{model}_v"], rec[f"hc{model}_w"] = x, v, w
                 rec[f"hc{model}_q"] = q
