@@ -48,9 +48,13 @@ typedef enum {
 } pe_b200_precision;
 
 typedef enum {
-    /* HardContactSemiImplicitTimesteppingSolvers.h:172-179 (the first two models) */
+    /* pe's RelaxationModel, HardContactSemiImplicitTimesteppingSolvers.h:172-179 */
     PE_B200_INELASTIC_FRICTIONLESS = 0,
-    PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING = 1
+    PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING = 1,
+    PE_B200_APPROX_INELASTIC_COULOMB_ORTHOGONAL_PROJECTIONS = 2,
+    PE_B200_INELASTIC_COULOMB_DECOUPLING = 3,
+    PE_B200_INELASTIC_COULOMB_ORTHOGONAL_PROJECTIONS = 4,
+    PE_B200_INELASTIC_GENERALIZED_MAX_DISSIPATION = 5
 } pe_b200_relaxation_model;
 
 typedef struct {

@@ -270,12 +270,11 @@ class CollisionSystem {
         InelasticCoulombContactByOrthogonalProjections,
         InelasticGeneralizedMaximumDissipationContact
     };
-    /* HCSITS.h:793-850; models other than the first two raise std::runtime_error at the next
-     * step, where pe raises it (HCSITS.h:1926) */
+    /* HCSITS.h:793-850 */
     void setMaxIterations(std::size_t n);
     void setRelaxationModel(RelaxationModel m);
     void setErrorReductionParameter(real erp);
-    /* the relaxation parameter only enters the models this library does not implement */
+    /* pe stores it but none of its relaxation models reads it (they use w = 1) */
     void setRelaxationParameter(real omega) { omega_ = omega; }
     real getRelaxationParameter() const { return omega_; }
     std::size_t getMaxIterations() const { return (std::size_t)p_.max_iterations; }
@@ -457,9 +456,6 @@ class World {
             if (!b->isFixed())
                 throw std::runtime_error("Box " + std::to_string(b->getID()) +
                                          " is not fixed: only fixed boxes are supported");
-        if (cs_.p_.solver == PE_B200_HCSITS &&
-            cs_.model_ > CollisionSystem::ApproximateInelasticCoulombContactByDecoupling)
-            throw std::runtime_error("Unsupported relaxation model.");
         if (structure_dirty_) {
             std::vector<pe_b200_material> mats;
             for (const Material &m : detail::materials()) mats.push_back(m.record());
@@ -608,11 +604,9 @@ inline void CollisionSystem::setMaxIterations(std::size_t n) {
 }
 inline void CollisionSystem::setRelaxationModel(RelaxationModel m) {
     model_ = m;
-    if (m <= ApproximateInelasticCoulombContactByDecoupling) {
-        p_.relaxation_model = (int32_t)m;
-        if (world_->context())
-            world_->check(pe_b200_set_relaxation_model(world_->context(), p_.relaxation_model));
-    }
+    p_.relaxation_model = (int32_t)m;
+    if (world_->context())
+        world_->check(pe_b200_set_relaxation_model(world_->context(), p_.relaxation_model));
 }
 inline void CollisionSystem::setErrorReductionParameter(real erp) {
     p_.erp = erp;

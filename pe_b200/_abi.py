@@ -17,7 +17,10 @@ STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CAPACITY", 3: "ERR_NAN", 4: "ERR_
 
 DEM, HCSITS = 0, 1
 FP64, MIXED = 0, 1
+# pe's RelaxationModel (HardContactSemiImplicitTimesteppingSolvers.h:172-179)
 INELASTIC_FRICTIONLESS, APPROX_INELASTIC_COULOMB_DECOUPLING = 0, 1
+APPROX_INELASTIC_COULOMB_ORTHOGONAL_PROJECTIONS, INELASTIC_COULOMB_DECOUPLING = 2, 3
+INELASTIC_COULOMB_ORTHOGONAL_PROJECTIONS, INELASTIC_GENERALIZED_MAX_DISSIPATION = 4, 5
 
 # every symbol include/pe_b200.h declares
 EXPORTS = ["pe_b200_default_params", "pe_b200_create", "pe_b200_destroy", "pe_b200_last_error",

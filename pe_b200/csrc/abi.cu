@@ -382,8 +382,8 @@ int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
     *out = nullptr;
     if (p->solver != PE_B200_DEM && p->solver != PE_B200_HCSITS) return PE_B200_ERR_ARG;
     if (p->precision != PE_B200_FP64 && p->precision != PE_B200_MIXED) return PE_B200_ERR_ARG;
-    if (p->relaxation_model != PE_B200_INELASTIC_FRICTIONLESS &&
-        p->relaxation_model != PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING)
+    if (p->relaxation_model < PE_B200_INELASTIC_FRICTIONLESS ||
+        p->relaxation_model > PE_B200_INELASTIC_GENERALIZED_MAX_DISSIPATION)
         return PE_B200_ERR_UNSUPPORTED;
     if (p->max_iterations < 0 || p->damping < 0 || p->damping > 1) return PE_B200_ERR_ARG;
     if (p->force_model != 0 && p->force_model != 1) return PE_B200_ERR_ARG;
@@ -460,7 +460,8 @@ int pe_b200_set_max_iterations(pe_b200_ctx *h, int32_t n) {
 int pe_b200_set_relaxation_model(pe_b200_ctx *h, int32_t m) {
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c) return PE_B200_ERR_ARG;
-    if (m != PE_B200_INELASTIC_FRICTIONLESS && m != PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING)
+    // the models of HCSITS.h:172-179; others throw "Unsupported relaxation model." (:1926)
+    if (m < PE_B200_INELASTIC_FRICTIONLESS || m > PE_B200_INELASTIC_GENERALIZED_MAX_DISSIPATION)
         return set_err(c, PE_B200_ERR_UNSUPPORTED, "Unsupported relaxation model.");
     c->p.relaxation_model = m;
     return PE_B200_OK;

@@ -139,6 +139,8 @@ struct Cache {
     int2 *ids;    // body 1, body 2 (-1: wall)
     T4<T> *rec;   // kRec per contact
     T4<T> *p;     // impulse in the contact frame (n, t, o, -)
+    T4<T> *dc;    // 2 per contact: Delassus block in the contact frame [xy xz yy yz] [zz - - -]
+                  // (its xx is rec[2].w), read by relaxation models 2-5 only
 };
 
 // Per body, slot order: velocities after the predictor with 1/m, 1/I (read-only in the sweeps)
@@ -412,17 +414,197 @@ __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos,
     R[4] = mk4<T>(o.x, o.y, o.z, zz * id2);
     R[5] = mk4<T>(c00 * id, c01 * id, c02 * id, (xx * zz - xz * xz) * id);
     R[6] = mk4<T>((xy * xz - xx * yz) * id, (xx * yy - xy * xy) * id, -yz * id2, yy * id2);
+    cc.dc[2 * k] = mk4<T>(xy, xz, yy, yz);
+    cc.dc[2 * k + 1] = mk4<T>(zz, T(0), T(0), T(0));
     cc.ids[k] = make_int2(b1, b2);
     cc.p[k] = mk4<T>(T(0), T(0), T(0), T(0));
     (void)nb;
 }
 
 // ---- one colour of one sweep ----------------------------------------------------------------
-// one contact of one sweep; COHERENT: read the velocity corrections and the impulse from L2
-template <typename T, bool FRICTION, bool COHERENT>
+// ---- one-contact solvers of pe's relaxation models 2-5, in the contact frame --------------
+// g: relative velocity in the contact frame with the ERP-scaled penetration term on its normal
+// component; D: the Delassus block (symmetric); pc: the contact's impulse before this update.
+
+// projection onto the friction cone of the orthogonal-projection models (HCSITS.h:2680-2700)
+template <typename T>
+__device__ __forceinline__ V3<T> cone_projection(V3<T> p, T mu) {
+    const T flimit = mu * p.x;
+    const T fsq = p.y * p.y + p.z * p.z;
+    if (p.x > T(0) && fsq < flimit * flimit) return p;
+    if (p.x < T(0) && fsq < p.x / (mu * mu)) return v3(T(0), T(0), T(0));
+    const T f = sqrt(fsq);
+    p.x = (f * mu + p.x) / (mu * mu + T(1));
+    const T factor = mu * p.x / f;
+    p.y *= factor;
+    p.z *= factor;
+    return p;
+}
+
+// models 2 and 4 (HCSITS.h:2631-2723): one step of relaxation w = 1 on D p + g, the exact form
+// raising its normal part by mu |(D p + g)_to|, then the cone projection
+template <typename T, bool EXACT>
+__device__ __forceinline__ V3<T> solve_orthogonal(V3<T> pc, V3<T> g, const T D[6], T mu) {
+    V3<T> tmp = v3(D[0] * pc.x + D[1] * pc.y + D[2] * pc.z + g.x,
+                   D[1] * pc.x + D[3] * pc.y + D[4] * pc.z + g.y,
+                   D[2] * pc.x + D[4] * pc.y + D[5] * pc.z + g.z);
+    if (EXACT) tmp.x += sqrt(tmp.y * tmp.y + tmp.z * tmp.z) * mu;
+    return cone_projection<T>(pc - tmp, mu);
+}
+
+// 0.5 x^T A x - x^T b for the golden-section searches (A symmetric 2x2)
+template <typename T>
+__device__ __forceinline__ T quad2(T a00, T a01, T a11, T x0, T x1, T b0, T b1) {
+    const T y0 = a00 * x0 + a01 * x1, y1 = a01 * x0 + a11 * x1;
+    return ((T(0.5) * x0) * y0 + (T(0.5) * x1) * y1) - (x0 * b0 + x1 * b1);
+}
+
+// golden-section search over the angle of the friction circle (radius(alpha)), keeping the
+// smallest energy found (HCSITS.h:2440-2500, 2895-2945); 20 sub-iterations (HCSITS.h:423)
+template <typename T, typename R>
+__device__ __forceinline__ void golden_angle(T alpha_left, T alpha_right, R radius, T a00, T a01,
+                                             T a11, T b0, T b1, T &x0, T &x1, T &fmid) {
+    const T phi = T(0.5) * (T(1) + sqrt(T(5)));
+    T alpha_mid = (alpha_right + alpha_left * phi) / (T(1) + phi);
+    T r = radius(alpha_mid);
+    x0 = r * cos(alpha_mid);
+    x1 = r * sin(alpha_mid);
+    fmid = quad2<T>(a00, a01, a11, x0, x1, b0, b1);
+    bool leftlarger = false;
+    for (int k = 0; k < 20; ++k) {
+        const T alpha_next = alpha_left + (alpha_right - alpha_mid);
+        r = radius(alpha_next);
+        const T n0 = r * cos(alpha_next), n1 = r * sin(alpha_next);
+        const T fnext = quad2<T>(a00, a01, a11, n0, n1, b0, b1);
+        if (leftlarger) {
+            if (fnext < fmid) {
+                alpha_right = alpha_mid; alpha_mid = alpha_next;
+                x0 = n0; x1 = n1; fmid = fnext; leftlarger = true;
+            } else {
+                alpha_left = alpha_next; leftlarger = false;
+            }
+        } else {
+            if (fnext < fmid) {
+                alpha_left = alpha_mid; alpha_mid = alpha_next;
+                x0 = n0; x1 = n1; fmid = fnext; leftlarger = false;
+            } else {
+                alpha_right = alpha_next; leftlarger = true;
+            }
+        }
+    }
+}
+
+// model 3 (HCSITS.h:2330-2595): exact Coulomb friction by 20 rounds of a normal solve for the
+// current tangential impulse and a tangential solve for the new normal one; a tangential solve
+// outside the cone is replaced by the energy minimiser on the cone's circle.  corr(p) is the
+// change of the relative velocity an impulse p (world frame) causes through the bodies'
+// rotational inertia alone, as pe writes it.
+template <typename T, typename Corr>
+__device__ __forceinline__ V3<T> solve_coulomb_decoupling(V3<T> pcf, const V3<T> &gdot,
+                                                          const V3<T> &n, const V3<T> &t,
+                                                          const V3<T> &o, T dist_dtinv,
+                                                          T dn_inv, T tt, T to, T oo,
+                                                          const T D[6], T mu, Corr corr) {
+    for (int j = 0; j < 20; ++j) {
+        pcf.x = T(0);
+        V3<T> gc = gdot + corr(t * pcf.y + o * pcf.z);
+        const T gcn = dot(n, gc) + dist_dtinv;
+        pcf.x = -(dn_inv * gcn);
+        pcf.x = pcf.x > T(0) ? pcf.x : T(0);
+        gc = gdot + corr(n * pcf.x);
+        const T gt = dot(t, gc), go = dot(o, gc);
+        pcf.y = -(tt * gt + to * go);
+        pcf.z = -(to * gt + oo * go);
+        const T flimit = mu * pcf.x;
+        const T fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+        if (fsq > flimit * flimit) {
+            const T f = flimit / sqrt(fsq);
+            const T shift = atan2(-pcf.z, pcf.y);
+            const T acos_f = acos(f);
+            T x0, x1, fm;
+            golden_angle<T>(-acos_f - shift, acos_f - shift, [flimit](T) { return flimit; },
+                            D[3], D[4], D[5], -gt, -go, x0, x1, fm);
+            pcf.y = x0;
+            pcf.z = x1;
+        }
+    }
+    return pcf;
+}
+
+// model 5 (HCSITS.h:2745-3055): generalized maximum dissipation: the tangential impulse of
+// least kinetic energy on the intersection of the plane of maximum compression with the
+// friction cone, by a golden-section search over the angle; pcf enters as -D^-1 g.
+template <typename T>
+__device__ __forceinline__ V3<T> solve_gmd(V3<T> pcf, const V3<T> &g, const T D[6], T mu,
+                                           T fsq) {
+    const T twopi = T(6.283185307179586476925286766559);
+    const T invA_nn = T(1) / D[0];
+    const T offdiag = D[4] - invA_nn * D[1] * D[2];
+    const T a00 = D[3] - invA_nn * (D[1] * D[1]), a11 = D[5] - invA_nn * (D[2] * D[2]);
+    const T b0 = -g.y + invA_nn * D[1] * g.x, b1 = -g.z + invA_nn * D[2] * g.x;
+    const T shiftI = atan2(-D[2], D[1]);
+    const T shiftJ = atan2(-pcf.z, pcf.y);
+    const T a3 = sqrt(D[1] * D[1] + D[2] * D[2]);
+    const T fractionI = -D[0] / (mu * a3);
+    T fractionJ = invA_nn * mu * ((-g.x) / sqrt(fsq) - a3 * cos(shiftI - shiftJ));
+    fractionJ = fractionJ < T(1) ? fractionJ : T(1);
+    T alpha_left, alpha_right;
+    if (fractionJ < T(-1)) {
+        const T angleI = acos(fractionI);
+        alpha_left = -angleI - shiftI;
+        alpha_right = +angleI - shiftI;
+        if (alpha_left < T(0)) { alpha_left += twopi; alpha_right += twopi; }
+    } else if (D[0] > mu * a3) {
+        const T angleJ = acos(fractionJ);
+        alpha_left = -angleJ - shiftJ;
+        alpha_right = +angleJ - shiftJ;
+        if (alpha_left < T(0)) { alpha_left += twopi; alpha_right += twopi; }
+    } else {
+        const T angleJ = acos(fractionJ);
+        T a1l = -angleJ - shiftJ, a1r = +angleJ - shiftJ;
+        if (a1l < T(0)) { a1l += twopi; a1r += twopi; }
+        const T angleI = acos(fractionI);
+        T a2l = -angleI - shiftI, a2r = +angleI - shiftI;
+        if (a2l < T(0)) { a2l += twopi; a2r += twopi; }
+        if (a1l > a2l) {
+            T u = a1l; a1l = a2l; a2l = u;
+            u = a1r; a1r = a2r; a2r = u;
+        }
+        if (a2l > a1r) {
+            a2r -= twopi;
+            if (!(a2r > a1r)) a1r = a2r;
+        } else {
+            a1l = a2l;
+            if (!(a2r > a1r)) a1r = a2r;
+        }
+        alpha_left = a1l;
+        alpha_right = a1r;
+    }
+    auto radius = [&](T alpha) {
+        T r = mu * (-g.x) / (D[0] + mu * a3 * cos(alpha + shiftI));
+        return r < T(0) ? T(INFINITY) : r;
+    };
+    T x0, x1, fm;
+    golden_angle<T>(alpha_left, alpha_right, radius, a00, offdiag, a11, b0, b1, x0, x1, fm);
+    {
+        const T alpha_init = atan2(pcf.z, pcf.y);
+        const T r = radius(alpha_init);
+        const T i0 = r * cos(alpha_init), i1 = r * sin(alpha_init);
+        if (quad2<T>(a00, offdiag, a11, i0, i1, b0, b1) < fm) {
+            x0 = i0;
+            x1 = i1;
+        }
+    }
+    return v3(invA_nn * (-g.x - D[1] * x0 - D[2] * x1), x0, x1);
+}
+
+// one contact of one sweep of relaxation model MODEL (pe's RelaxationModel, HCSITS.h:172-179);
+// COHERENT: read the velocity corrections and the impulse from L2
+template <typename T, int MODEL, bool COHERENT>
 __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T> &cc,
                                               const BodyV<T> &bv, int track_delta,
                                               unsigned long long *delta) {
+    constexpr bool FRICTION = MODEL != 0;
     const int2 ids = cc.ids[k];
     const int32_t b1 = ids.x, b2 = ids.y;
     const T4<T> *R = cc.rec + (int64_t)kRec * k;
@@ -470,45 +652,81 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     T gn = dot(n, gdot) + dist * dtinv;
     V3<T> pnew = v3(T(0), T(0), T(0));
     V3<T> pcf = pnew;
-    if (gn < T(0)) {
-        if (!FRICTION) {
-            pcf.x = -dn_inv * gn;
-            pnew = n * pcf.x;
-        } else {
-            const T gt = dot(t, gdot), go = dot(o, gdot);
+    bool apply = false;
+    if (MODEL == 0 || MODEL == 1) {
+        if (gn < T(0)) {
+            apply = true;
+            if (!FRICTION) {
+                pcf.x = -dn_inv * gn;
+                pnew = n * pcf.x;
+            } else {
+                const T gt = dot(t, gdot), go = dot(o, gdot);
+                const T4<T> q5 = R[5], q6 = R[6];
+                const T dxx = q5.x, dxy = q5.y, dxz = q5.z, dyy = q5.w, dyz = q6.x, dzz = q6.y;
+                pcf = v3(-(dxx * gn + dxy * gt + dxz * go), -(dxy * gn + dyy * gt + dyz * go),
+                         -(dxz * gn + dyz * gt + dzz * go));
+                const T mu = q3.w;
+                T flimit = mu * pcf.x;
+                T fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+                if (fsq > flimit * flimit || pcf.x < T(0)) {
+                    // decoupled relaxation (HCSITS.h:2187-2228)
+                    V3<T> ptmp = t * pc.y + o * pc.z;
+                    const V3<T> e1 = cross(ii1 * cross(r1, ptmp), r1);
+                    const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
+                    const T gdot_n = gn + dot(n, e1 + e2);
+                    pcf.x = -(dn_inv * gdot_n);
+                    pcf.x = pcf.x > T(0) ? pcf.x : T(0);
+                    ptmp = n * pcf.x;
+                    const V3<T> f1 = cross(ii1 * cross(r1, ptmp), r1);
+                    const V3<T> f2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
+                    const V3<T> gdot2 = (gdot + f1) + f2;
+                    const T g2t = dot(t, gdot2), g2o = dot(o, gdot2);
+                    const T ttt = q4.w, tto = q6.z, too = q6.w;
+                    pcf.y = -(ttt * g2t + tto * g2o);
+                    pcf.z = -(tto * g2t + too * g2o);
+                    flimit = mu * pcf.x;
+                    fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+                    if (fsq > flimit * flimit) {
+                        const T f = flimit / sqrt(fsq);
+                        pcf.y *= f;
+                        pcf.z *= f;
+                    }
+                }
+                pnew = n * pcf.x + t * pcf.y + o * pcf.z;
+            }
+        }
+    } else {
+        const T mu = q3.w;
+        const V3<T> g = v3(gn, dot(t, gdot), dot(o, gdot));
+        const T4<T> d0 = cc.dc[2 * k], d1 = cc.dc[2 * k + 1];
+        const T D[6] = {q2.w, d0.x, d0.y, d0.z, d0.w, d1.x};   // xx xy xz yy yz zz
+        if (MODEL == 2 || MODEL == 4) {
+            pcf = solve_orthogonal<T, MODEL == 4>(pc, g, D, mu);
+            apply = true;
+        } else if (gn < T(0)) {
+            apply = true;
             const T4<T> q5 = R[5], q6 = R[6];
-            const T dxx = q5.x, dxy = q5.y, dxz = q5.z, dyy = q5.w, dyz = q6.x, dzz = q6.y;
-            pcf = v3(-(dxx * gn + dxy * gt + dxz * go), -(dxy * gn + dyy * gt + dyz * go),
-                     -(dxz * gn + dyz * gt + dzz * go));
-            const T mu = q3.w;
-            T flimit = mu * pcf.x;
-            T fsq = pcf.y * pcf.y + pcf.z * pcf.z;
+            pcf = v3(-(q5.x * g.x + q5.y * g.y + q5.z * g.z), -(q5.y * g.x + q5.w * g.y + q6.x * g.z),
+                     -(q5.z * g.x + q6.x * g.y + q6.y * g.z));
+            const T flimit = mu * pcf.x;
+            const T fsq = pcf.y * pcf.y + pcf.z * pcf.z;
             if (fsq > flimit * flimit || pcf.x < T(0)) {
-                // decoupled relaxation (HCSITS.h:2187-2228)
-                V3<T> ptmp = t * pc.y + o * pc.z;
-                const V3<T> e1 = cross(ii1 * cross(r1, ptmp), r1);
-                const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
-                const T gdot_n = gn + dot(n, e1 + e2);
-                pcf.x = -(dn_inv * gdot_n);
-                pcf.x = pcf.x > T(0) ? pcf.x : T(0);
-                ptmp = n * pcf.x;
-                const V3<T> f1 = cross(ii1 * cross(r1, ptmp), r1);
-                const V3<T> f2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
-                const V3<T> gdot2 = (gdot + f1) + f2;
-                const T g2t = dot(t, gdot2), g2o = dot(o, gdot2);
-                const T ttt = q4.w, tto = q6.z, too = q6.w;
-                pcf.y = -(ttt * g2t + tto * g2o);
-                pcf.z = -(tto * g2t + too * g2o);
-                flimit = mu * pcf.x;
-                fsq = pcf.y * pcf.y + pcf.z * pcf.z;
-                if (fsq > flimit * flimit) {
-                    const T f = flimit / sqrt(fsq);
-                    pcf.y *= f;
-                    pcf.z *= f;
+                if (MODEL == 3) {
+                    auto corr = [&](const V3<T> &pp) {
+                        const V3<T> e1 = cross(ii1 * cross(r1, pp), r1);
+                        const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, pp), r2) : v3(T(0), T(0), T(0));
+                        return e1 + e2;
+                    };
+                    pcf = solve_coulomb_decoupling<T>(pcf, gdot, n, t, o, dist * dtinv, dn_inv, q4.w,
+                                                      q6.z, q6.w, D, mu, corr);
+                } else {
+                    pcf = solve_gmd<T>(pcf, g, D, mu, fsq);
                 }
             }
-            pnew = n * pcf.x + t * pcf.y + o * pcf.z;
         }
+        if (apply) pnew = n * pcf.x + t * pcf.y + o * pcf.z;
+    }
+    if (apply) {
         dv1 = dv1 + im1 * pnew;
         dw1 = dw1 + ii1 * cross(r1, pnew);
         if (b2 >= 0) {
@@ -530,18 +748,18 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     }
 }
 
-template <typename T, bool FRICTION>
+template <typename T, int MODEL>
 __global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int64_t cap, T dtinv,
                                                 Cache<T> cc, BodyV<T> bv, int64_t nb,
                                                 int track_delta, unsigned long long *delta) {
     const int64_t k = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= end) return;
-    sweep_contact<T, FRICTION, false>(k, dtinv, cc, bv, track_delta, delta);
+    sweep_contact<T, MODEL, false>(k, dtinv, cc, bv, track_delta, delta);
 }
 
 // All sweeps of a step in one cooperative launch: colour after colour, separated by bounded
 // grid barriers (each colour is conflict-free, so its contacts run in parallel).
-template <typename T, bool FRICTION>
+template <typename T, int MODEL>
 __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolors,
                                                             const int32_t *color_start,
                                                             int64_t cap, T dtinv, Cache<T> cc,
@@ -556,7 +774,7 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
         for (int col = 0; col < ncolors; ++col) {
             const int64_t e = color_start[col + 1];
             for (int64_t k = color_start[col] + g0; k < e; k += stride)
-                sweep_contact<T, FRICTION, true>(k, dtinv, cc, bv, track, delta);
+                sweep_contact<T, MODEL, true>(k, dtinv, cc, bv, track, delta);
             if (!grid_sync(bar, err)) return;
         }
     }
@@ -569,7 +787,7 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
 constexpr int kClusterBlk = 512;
 constexpr int kClusterPerThread = 4;
 
-template <typename T, bool FRICTION>
+template <typename T, int MODEL>
 __global__ void __launch_bounds__(kClusterBlk) k_sweeps_cluster(int iters, int ncolors,
                                                                 const int32_t *color_start,
                                                                 int64_t cap, T dtinv, Cache<T> cc,
@@ -585,7 +803,7 @@ __global__ void __launch_bounds__(kClusterBlk) k_sweeps_cluster(int iters, int n
         for (int col = 0; col < ncolors; ++col) {
             const int64_t e = color_start[col + 1];
             for (int64_t k = color_start[col] + g0; k < e; k += stride)
-                sweep_contact<T, FRICTION, true>(k, dtinv, cc, bv, track, delta);
+                sweep_contact<T, MODEL, true>(k, dtinv, cc, bv, track, delta);
             cluster.sync();
         }
     }
@@ -688,8 +906,8 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         b.color = nullptr;
         cudaFree(b.body_adj);
         b.body_adj = nullptr;
-        // raw: 2 int + 11 T; cache: 2 int + (kRec + 1) x 4 T  (per contact)
-        const size_t bytes = (size_t)cap * (4 * sizeof(int32_t) + (11 + 4 * (kRec + 1)) * es) + 64 * 256;
+        // raw: 2 int + 11 T; cache: 2 int + (kRec + 3) x 4 T  (per contact)
+        const size_t bytes = (size_t)cap * (4 * sizeof(int32_t) + (11 + 4 * (kRec + 3)) * es) + 64 * 256;
         PEB_CUDA(c, cudaMalloc(&b.cache, bytes));
         PEB_CUDA(c, cudaMalloc(&b.order, (size_t)cap * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.color, (size_t)cap * sizeof(int32_t)));
@@ -731,6 +949,7 @@ void layout(Ctx *c, Raw<T> &raw, Cache<T> &cc, BodyV<T> &bv) {
     cc.ids = (int2 *)take(cap * sizeof(int2));
     cc.rec = (T4<T> *)take(kRec * cap * sizeof(T4<T>));
     cc.p = (T4<T> *)take(cap * sizeof(T4<T>));
+    cc.dc = (T4<T> *)take(2 * cap * sizeof(T4<T>));
     const int64_t n = std::max<int64_t>(c->n, 1);
     T4<T> *v = (T4<T> *)b.vel;
     bv.vr = v;
@@ -739,14 +958,49 @@ void layout(Ctx *c, Raw<T> &raw, Cache<T> &cc, BodyV<T> &bv) {
     bv.dw = v + 3 * n;
 }
 
+// the sweep kernels of relaxation model m (pe's RelaxationModel 0-5)
+template <typename VT>
+auto cluster_kernel(int m) -> decltype(&k_sweeps_cluster<VT, 0>) {
+    switch (m) {
+        case 1: return k_sweeps_cluster<VT, 1>;
+        case 2: return k_sweeps_cluster<VT, 2>;
+        case 3: return k_sweeps_cluster<VT, 3>;
+        case 4: return k_sweeps_cluster<VT, 4>;
+        case 5: return k_sweeps_cluster<VT, 5>;
+        default: return k_sweeps_cluster<VT, 0>;
+    }
+}
+template <typename VT>
+auto persistent_kernel(int m) -> decltype(&k_sweeps_persistent<VT, 0>) {
+    switch (m) {
+        case 1: return k_sweeps_persistent<VT, 1>;
+        case 2: return k_sweeps_persistent<VT, 2>;
+        case 3: return k_sweeps_persistent<VT, 3>;
+        case 4: return k_sweeps_persistent<VT, 4>;
+        case 5: return k_sweeps_persistent<VT, 5>;
+        default: return k_sweeps_persistent<VT, 0>;
+    }
+}
+template <typename VT>
+auto colour_kernel(int m) -> decltype(&k_sweep<VT, 0>) {
+    switch (m) {
+        case 1: return k_sweep<VT, 1>;
+        case 2: return k_sweep<VT, 2>;
+        case 3: return k_sweep<VT, 3>;
+        case 4: return k_sweep<VT, 4>;
+        case 5: return k_sweep<VT, 5>;
+        default: return k_sweep<VT, 0>;
+    }
+}
+
 // Runs all sweeps in one cluster when the largest colour is small enough; *done reports it.
 // The cluster size (16 CTAs if the GPU schedules such clusters, else 8) is probed once.
 template <typename VT>
-int sweeps_in_cluster(Ctx *c, bool fr, int iters, int ncolors, int maxcol, int64_t cap, VT dtinv,
+int sweeps_in_cluster(Ctx *c, int model, int iters, int ncolors, int maxcol, int64_t cap, VT dtinv,
                       const Cache<VT> &cc, const BodyV<VT> &bv, int64_t n,
                       unsigned long long *dl, bool *done) {
     NbgsBuf &nb = c->nb;
-    auto kern = fr ? k_sweeps_cluster<VT, true> : k_sweeps_cluster<VT, false>;
+    auto kern = cluster_kernel<VT>(model);
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -758,15 +1012,14 @@ int sweeps_in_cluster(Ctx *c, bool fr, int iters, int ncolors, int maxcol, int64
     if (nb.cluster < 0) {
         nb.cluster = 0;
         for (int size : {16, 8}) {
-            auto probe = k_sweeps_cluster<VT, true>;
+            auto probe = cluster_kernel<VT>(model);
             if (size > 8 &&
                 cudaFuncSetAttribute((const void *)probe, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
                 cudaGetLastError();
                 continue;
             }
             if (size > 8) {
-                cudaFuncSetAttribute((const void *)k_sweeps_cluster<VT, false>,
-                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
                 cudaGetLastError();
             }
             cfg.gridDim = dim3(size);
@@ -786,6 +1039,10 @@ int sweeps_in_cluster(Ctx *c, bool fr, int iters, int ncolors, int maxcol, int64
         return PE_B200_OK;
     PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start, (ncolors + 1) * sizeof(int32_t),
                                 cudaMemcpyHostToDevice, c->stream));
+    if (nb.cluster > 8) {
+        cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaGetLastError();
+    }
     cfg.gridDim = dim3(nb.cluster);
     attr[0].val.clusterDim.x = nb.cluster;
     attr[0].val.clusterDim.y = 1;
@@ -914,7 +1171,8 @@ int nbgs_step_t(Ctx *c, double dt) {
     }
     c->last_ncolors = ncolors;
     // 5. sweeps
-    const bool fr = c->p.relaxation_model == PE_B200_APPROX_INELASTIC_COULOMB_DECOUPLING;
+    const int model = c->p.relaxation_model;
+    const bool fr = model != PE_B200_INELASTIC_FRICTIONLESS;
     const int iters = c->p.max_iterations;
     unsigned long long *dl = (unsigned long long *)nb.red;
     if (c->want_residual) PEB_CUDA(c, cudaMemsetAsync(nb.red, 0, 2 * sizeof(double), c->stream));
@@ -928,14 +1186,14 @@ int nbgs_step_t(Ctx *c, double dt) {
         // the one-cluster form has the cheaper barrier but only a few SMs' load bandwidth; on
         // B200 the grid form is faster for every scene measured, so it is the automatic choice
         if (!done && nb.cluster != 0 && mode == 1) {
-            int rc = sweeps_in_cluster<VT>(c, fr, iters, ncolors, maxcol, cap, VT(1.0 / dt), cc,
+            int rc = sweeps_in_cluster<VT>(c, model, iters, ncolors, maxcol, cap, VT(1.0 / dt), cc,
                                            bv, n, dl, &done);
             if (rc) return rc;
         }
         if (!done && !nb.coop_disabled && mode != 3) {
             // all sweeps in one cooperative launch (colours separated by grid barriers); as few
             // blocks as the largest colour needs, so the barriers stay short
-            auto kern = fr ? k_sweeps_persistent<VT, true> : k_sweeps_persistent<VT, false>;
+            auto kern = persistent_kernel<VT>(model);
             int occ = 0;
             cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0);
             if (e == cudaSuccess && occ > 0) {
@@ -966,12 +1224,8 @@ int nbgs_step_t(Ctx *c, double dt) {
             for (int col = 0; col < ncolors; ++col) {
                 const int64_t b = nb.color_start[col], e = nb.color_start[col + 1];
                 if (e <= b) continue;
-                if (fr)
-                    k_sweep<VT, true><<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
-                        b, e, cap, VT(1.0 / dt), cc, bv, n, track, dl);
-                else
-                    k_sweep<VT, false><<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
-                        b, e, cap, VT(1.0 / dt), cc, bv, n, track, dl);
+                colour_kernel<VT>(model)<<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
+                    b, e, cap, VT(1.0 / dt), cc, bv, n, track, dl);
                 PEB_LAUNCHED(c);
             }
         }
