@@ -35,9 +35,12 @@
 #ifndef PE_B200_WORLD_HPP
 #define PE_B200_WORLD_HPP
 
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
+#include <fstream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -363,6 +366,15 @@ class World {
     CollisionSystem &collisionSystem() { return cs_; }
     pe_b200_ctx *context() { return ctx_; }
 
+    /* pe's binary checkpoint (BodyBinaryWriter::writeFile, src/core/BodyBinaryWriter.cpp:47-245)
+     * for one process: spheres and boxes in the local chunk, planes (which pe writes only when
+     * global) left out; big-endian as pe's network-order buffers.  Sphere orientations are not
+     * tracked here and are written as the identity. */
+    void writeCheckpoint(const char *filename) const;
+    /* BodyBinaryReader::readFile (src/core/BodyBinaryReader.cpp:57-300): every body of the world
+     * is replaced by the file's; material ids refer to the material table as it is now */
+    void readCheckpoint(const char *filename);
+
     // -- used by the free functions and the body classes ----------------------------------------
     SphereID addSphere(id_t uid, const Vec3 &x, real r, MaterialID m, bool visible) {
         pull();
@@ -503,6 +515,8 @@ class World {
         check(pe_b200_set_damping(ctx_, damping_));
     }
 
+    friend class BodyBinaryWriter;
+    friend class BodyBinaryReader;
     CollisionSystem cs_;
     pe_b200_ctx *ctx_ = nullptr;
     std::vector<std::unique_ptr<Sphere>> spheres_;
@@ -517,6 +531,186 @@ class World {
 };
 
 typedef World *WorldID;
+
+/* pe's checkpoint writer and reader (pe/core/BodyBinaryWriter.h:96, BodyBinaryReader.h:61) */
+class BodyBinaryWriter {
+  public:
+    void writeFile(const char *filename) { World::instance().writeCheckpoint(filename); }
+};
+class BodyBinaryReader {
+  public:
+    void readFile(const char *filename) { World::instance().readCheckpoint(filename); }
+};
+
+namespace detail {
+// big-endian encoding of pe's send buffers (pe/core/BodyBinaryWriter.h:68)
+inline void put_be(std::string &out, const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t k = 0; k < n; ++k) out.push_back((char)b[n - 1 - k]);
+}
+template <typename T>
+inline void put(std::string &out, T v) { put_be(out, &v, sizeof(T)); }
+inline void put_vec(std::string &out, const Vec3 &v) {
+    for (int a = 0; a < 3; ++a) put<double>(out, v[a]);
+}
+template <typename T>
+inline T get(const std::string &in, size_t &p) {
+    if (p + sizeof(T) > in.size()) throw std::runtime_error("Invalid body data chunk size.");
+    T v;
+    unsigned char *b = reinterpret_cast<unsigned char *>(&v);
+    for (size_t k = 0; k < sizeof(T); ++k) b[sizeof(T) - 1 - k] = (unsigned char)in[p + k];
+    p += sizeof(T);
+    return v;
+}
+inline Vec3 get_vec(const std::string &in, size_t &p) {
+    const double x = get<double>(in, p), y = get<double>(in, p), z = get<double>(in, p);
+    return Vec3(x, y, z);
+}
+// rotation matrix (row-major) <-> unit quaternion (w, x, y, z)
+inline void quat_of(const real R[9], real q[4]) {
+    const real tr = R[0] + R[4] + R[8];
+    if (tr > 0) {
+        const real s = std::sqrt(tr + 1.0) * 2;
+        q[0] = 0.25 * s; q[1] = (R[7] - R[5]) / s; q[2] = (R[2] - R[6]) / s; q[3] = (R[3] - R[1]) / s;
+    } else if (R[0] > R[4] && R[0] > R[8]) {
+        const real s = std::sqrt(1.0 + R[0] - R[4] - R[8]) * 2;
+        q[0] = (R[7] - R[5]) / s; q[1] = 0.25 * s; q[2] = (R[1] + R[3]) / s; q[3] = (R[2] + R[6]) / s;
+    } else if (R[4] > R[8]) {
+        const real s = std::sqrt(1.0 + R[4] - R[0] - R[8]) * 2;
+        q[0] = (R[2] - R[6]) / s; q[1] = (R[1] + R[3]) / s; q[2] = 0.25 * s; q[3] = (R[5] + R[7]) / s;
+    } else {
+        const real s = std::sqrt(1.0 + R[8] - R[0] - R[4]) * 2;
+        q[0] = (R[3] - R[1]) / s; q[1] = (R[2] + R[6]) / s; q[2] = (R[5] + R[7]) / s; q[3] = 0.25 * s;
+    }
+}
+inline void rot_of(const real q[4], real R[9]) {
+    const real w = q[0], x = q[1], y = q[2], z = q[3];
+    R[0] = 1 - 2 * (y * y + z * z); R[1] = 2 * (x * y - w * z);     R[2] = 2 * (x * z + w * y);
+    R[3] = 2 * (x * y + w * z);     R[4] = 1 - 2 * (x * x + z * z); R[5] = 2 * (y * z - w * x);
+    R[6] = 2 * (x * z - w * y);     R[7] = 2 * (y * z + w * x);     R[8] = 1 - 2 * (x * x + y * y);
+}
+}  // namespace detail
+
+inline void World::writeCheckpoint(const char *filename) const {
+    using namespace detail;
+    pull();
+    auto rigid = [](std::string &out, const RigidBody &b, bool fixed, const Vec3 &x, const real q[4],
+                    const Vec3 &v, const Vec3 &w) {
+        put<uint64_t>(out, b.sid_);
+        put<uint64_t>(out, b.uid_);
+        put<uint8_t>(out, b.visible_ ? 1 : 0);
+        put<uint8_t>(out, fixed ? 1 : 0);
+        put_vec(out, x);
+        for (int k = 0; k < 4; ++k) put<double>(out, q[k]);
+        put_vec(out, v);
+        put_vec(out, w);
+        put<uint64_t>(out, b.mat_);
+    };
+    std::string glob, loc;
+    put<uint64_t>(glob, 0);
+    for (uint8_t t = 1; t <= 7; ++t) {
+        put<uint8_t>(glob, t);
+        put<uint32_t>(glob, 0);
+    }
+    put<uint64_t>(loc, next_sid_);
+    const real ident[4] = {1, 0, 0, 0};
+    for (uint8_t t : {1, 2, 3, 4, 6, 7}) {
+        put<uint8_t>(loc, t);
+        if (t == 1) {
+            put<uint32_t>(loc, (uint32_t)spheres_.size());
+            for (const auto &s : spheres_) {
+                rigid(loc, *s, false, s->x_, ident, s->v_, s->w_);
+                put<double>(loc, s->r_);
+            }
+        } else if (t == 2) {
+            put<uint32_t>(loc, (uint32_t)boxes_.size());
+            for (const auto &b : boxes_) {
+                real q[4];
+                quat_of(b->R_, q);
+                rigid(loc, *b, b->fixed_, b->x_, q, Vec3(), Vec3());
+                put_vec(loc, b->l_);
+            }
+        } else {
+            put<uint32_t>(loc, 0);
+        }
+    }
+    std::string head = std::string("PE") + std::string("\x00\x01\x08\x04\x08\x08\x01", 7);
+    put<uint32_t>(head, 1);
+    const uint32_t header_size = (uint32_t)head.size() + 3 * 4;
+    const uint32_t offset = header_size + (uint32_t)glob.size();
+    put<uint32_t>(head, header_size);
+    put<uint32_t>(head, offset);
+    put<uint32_t>(head, offset + (uint32_t)loc.size());
+    std::ofstream f(filename, std::ios::binary);
+    if (!f) throw std::runtime_error("Cannot open file.");
+    f << head << glob << loc;
+    if (!f) throw std::runtime_error("Cannot write file.");
+}
+
+inline void World::readCheckpoint(const char *filename) {
+    using namespace detail;
+    std::ifstream f(filename, std::ios::binary);
+    if (!f) throw std::runtime_error("Cannot open file.");
+    const std::string in((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    // the header checks of BodyBinaryReader.cpp:100-162
+    if (in.size() < 25 || in[0] != 'P' || in[1] != 'E') throw std::runtime_error("Invalid file format.");
+    if (in[2] != 0 || in[3] != 1) throw std::runtime_error("Unsupported file format version.");
+    if (in[4] != 8) throw std::runtime_error("Invalid size of floating point data.");
+    if (in[5] != 4 || in[6] != 8 || in[7] != 8 || in[8] != 1)
+        throw std::runtime_error("Size of a data type does not match the data type used to produce the file.");
+    size_t p = 9;
+    if (get<uint32_t>(in, p) != 1)
+        throw std::runtime_error("Number of processes differ from the number of processes used to produce the file.");
+    const uint32_t goff = get<uint32_t>(in, p), loff = get<uint32_t>(in, p), lend = get<uint32_t>(in, p);
+    if (loff < goff || lend < loff || lend > in.size()) throw std::runtime_error("Invalid body data offset.");
+    clear();
+    id_t counter = 0;
+    auto chunk = [&](size_t q, size_t end) {
+        const id_t c = (id_t)get<uint64_t>(in, q);
+        while (q < end) {
+            const uint8_t t = get<uint8_t>(in, q);
+            const uint32_t cnt = get<uint32_t>(in, q);
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const id_t sid = (id_t)get<uint64_t>(in, q), uid = (id_t)get<uint64_t>(in, q);
+                const bool vis = get<uint8_t>(in, q) != 0, fixed = get<uint8_t>(in, q) != 0;
+                const Vec3 x = get_vec(in, q);
+                real qq[4];
+                for (int a = 0; a < 4; ++a) qq[a] = get<double>(in, q);
+                const Vec3 v = get_vec(in, q), w = get_vec(in, q);
+                const MaterialID m = (MaterialID)get<uint64_t>(in, q);
+                getMaterial(m);
+                if (t == 1) {
+                    const real r = get<double>(in, q);
+                    spheres_.emplace_back(new Sphere(this, sid, uid, x, r, m, vis));
+                    spheres_.back()->v_ = v;
+                    spheres_.back()->w_ = w;
+                } else if (t == 2) {
+                    const Vec3 l = get_vec(in, q);
+                    boxes_.emplace_back(new Box(this, sid, uid, x, l, m, vis));
+                    rot_of(qq, boxes_.back()->R_);
+                    boxes_.back()->fixed_ = fixed;
+                } else if (t == 5) {
+                    real R[9];
+                    rot_of(qq, R);
+                    const Vec3 nrm(R[2], R[5], R[8]);
+                    planes_.emplace_back(new Plane(this, sid, uid, nrm, nrm * x, m, vis));
+                } else {
+                    throw std::runtime_error("Unsupported geometry type in checkpoint.");
+                }
+            }
+        }
+        return c;
+    };
+    chunk(goff, loff);
+    counter = chunk(loff, lend);
+    // bodies in system-id order, as pe's storage holds them after creation
+    auto by_sid = [](const auto &a, const auto &b) { return a->sid_ < b->sid_; };
+    std::stable_sort(spheres_.begin(), spheres_.end(), by_sid);
+    std::stable_sort(boxes_.begin(), boxes_.end(), by_sid);
+    next_sid_ = counter;
+    structure_dirty_ = true;
+    host_stale_ = false;
+}
 
 /* theWorld() (pe/core/World.h:333) */
 inline WorldID theWorld() { return &World::instance(); }

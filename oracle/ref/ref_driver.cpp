@@ -179,6 +179,32 @@ int main(int argc, char** argv) {
             const int steps = std::atoi(argv[3]);
             for (int k = 0; k < steps; ++k) world->simulationStep(s.dt);
             write_state(argv[4], sp);
+        } else if (mode == "peb_write" && argc >= 5) {
+            // pe's own checkpoint writer (src/core/BodyBinaryWriter.cpp) after `steps` steps
+            const int steps = std::atoi(argv[3]);
+            for (int k = 0; k < steps; ++k) world->simulationStep(s.dt);
+            BodyBinaryWriter writer;
+            writer.writeFile(argv[4]);
+        } else if (mode == "peb_read" && argc >= 6) {
+            // pe's own checkpoint reader (src/core/BodyBinaryReader.cpp): it replaces every body
+            // of the world by the file's; the scene's planes (which pe does not write unless
+            // global) are created again, then `steps` steps run and the spheres' state is written
+            BodyBinaryReader reader;
+            reader.readFile(argv[3]);
+            std::vector<MaterialID> mids;
+            for (uint32_t m = 0; m < s.nmat; ++m) mids.push_back(static_cast<MaterialID>(5 + m));
+            for (uint32_t p = 0; p < s.nplanes; ++p) {
+                const double* a = &s.planes[4 * p];
+                createPlane(static_cast<pe::id_t>(s.n + p), Vec3(a[0], a[1], a[2]), a[3],
+                            mids[s.plane_mat[p]]);
+            }
+            std::vector<SphereID> read;
+            for (World::Bodies::CastIterator<Sphere> it = world->begin<Sphere>();
+                 it != world->end<Sphere>(); ++it)
+                read.push_back(*it);
+            const int steps = std::atoi(argv[4]);
+            for (int k = 0; k < steps; ++k) world->simulationStep(s.dt);
+            write_state(argv[5], read);
         } else if (mode == "pairs" && argc >= 4) {
             write_pairs(argv[3]);
         } else if (mode == "time" && argc >= 5) {

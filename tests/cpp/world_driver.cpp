@@ -176,7 +176,83 @@ static int run(const char *scene, const char *solver, const char *prec, int step
     return o ? 0 : 4;
 }
 
+// the compiled reference's body creation order: spheres (user id = index), planes, boxes
+static void build_like_reference(const SceneFile &sf) {
+    using namespace pe;
+    std::vector<MaterialID> mid;
+    for (size_t k = 0; k < sf.mats.size() / 9; ++k) {
+        const double *m = &sf.mats[9 * k];
+        mid.push_back(createMaterial("scene_material_" + std::to_string(k), m[0], m[1], m[2], m[3],
+                                     m[4], m[5], m[6], m[7], m[8]));
+    }
+    for (uint64_t i = 0; i < sf.n; ++i) {
+        SphereID s = createSphere(i, sf.x[3 * i], sf.x[3 * i + 1], sf.x[3 * i + 2], sf.r[i],
+                                  mid[sf.mat[i]]);
+        s->setLinearVel(sf.v[3 * i], sf.v[3 * i + 1], sf.v[3 * i + 2]);
+        s->setAngularVel(sf.w[3 * i], sf.w[3 * i + 1], sf.w[3 * i + 2]);
+    }
+    const size_t np = sf.plane_mat.size();
+    for (size_t k = 0; k < np; ++k) {
+        const double *p = &sf.planes[4 * k];
+        createPlane(sf.n + k, Vec3(p[0], p[1], p[2]), p[3], mid[sf.plane_mat[k]]);
+    }
+    for (size_t k = 0; k < sf.box_mat.size(); ++k) {
+        const double *b = &sf.boxes[15 * k];
+        createBox(sf.n + np + k, Vec3(b[0], b[1], b[2]), Vec3(b[3], b[4], b[5]), mid[sf.box_mat[k]])
+            ->setFixed(true);
+    }
+}
+
+// peb_write <scene> <out.peb>: the scene's bodies as pe's checkpoint writer would store them
+static int peb_write(const char *scene, const char *out) {
+    SceneFile sf;
+    if (!read_scene(scene, sf)) return 2;
+    build_like_reference(sf);
+    pe::BodyBinaryWriter().writeFile(out);
+    std::printf("ok\n");
+    return 0;
+}
+
+// peb_resume <scene> <in.peb> <steps> <out>: the scene's materials, the checkpoint's bodies, the
+// scene's planes again (pe writes only global planes), then `steps` FP64 DEM steps on the GPU
+static int peb_resume(const char *scene, const char *in, int steps, const char *out) {
+    using namespace pe;
+    SceneFile sf;
+    if (!read_scene(scene, sf)) return 2;
+    build_like_reference(sf);
+    BodyBinaryReader().readFile(in);
+    for (size_t k = 0; k < sf.plane_mat.size(); ++k) {
+        const double *p = &sf.planes[4 * k];
+        createPlane(sf.n + k, Vec3(p[0], p[1], p[2]), p[3], 5 + sf.plane_mat[k]);
+    }
+    WorldID world = theWorld();
+    world->setGravity(sf.g[0], sf.g[1], sf.g[2]);
+    world->setDamping(sf.damping);
+    theCollisionSystem()->setSolver(PE_B200_DEM);
+    theCollisionSystem()->setPrecision(PE_B200_FP64);
+    try {
+        world->run(steps, sf.dt);
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "step failed: %s\n", e.what());
+        return 3;
+    }
+    std::vector<double> res;
+    for (int f = 0; f < 3; ++f)
+        for (size_t i = 0; i < world->numSpheres(); ++i) {
+            SphereID s = world->sphere(i);
+            const Vec3 a = f == 0 ? s->getPosition() : f == 1 ? s->getLinearVel() : s->getAngularVel();
+            res.insert(res.end(), {a[0], a[1], a[2]});
+        }
+    std::ofstream o(out, std::ios::binary);
+    o.write((const char *)res.data(), res.size() * sizeof(double));
+    std::printf("ok\n");
+    return o ? 0 : 4;
+}
+
 int main(int argc, char **argv) {
+    if (argc == 4 && std::strcmp(argv[1], "peb_write") == 0) return peb_write(argv[2], argv[3]);
+    if (argc == 6 && std::strcmp(argv[1], "peb_resume") == 0)
+        return peb_resume(argv[2], argv[3], std::atoi(argv[4]), argv[5]);
     if (argc >= 2 && std::strcmp(argv[1], "errors") == 0) return errors();
     if (argc == 7 && std::strcmp(argv[1], "run") == 0)
         return run(argv[2], argv[3], argv[4], std::atoi(argv[5]), argv[6]);

@@ -107,6 +107,20 @@ def adjoint_fd(name="adjoint_fd", seed=2, n=64, steps=40):
     print(path, os.path.getsize(path), "bytes, loss", rec["loss"])
 
 
+def peb_fixture(steps=5):
+    """pe's own checkpoint of small64_boxes after `steps` DEM steps, and that state."""
+    s = scenes.small_random(1, n=64, with_boxes=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        sp = os.path.join(tmp, "scene.bin")
+        s.save(sp)
+        peb = os.path.join(OUT, "peb_small64_boxes.peb")
+        subprocess.run([os.path.join(REF, "ref_dem"), "peb_write", sp, str(steps), peb], check=True)
+        x, v, w, q = run_steps("ref_dem", sp, s.n, steps, tmp)
+    path = os.path.join(OUT, "peb_small64_boxes.npz")
+    np.savez_compressed(path, scene=np.frombuffer(s.to_bytes(), np.uint8), x=x, v=v, w=w, q=q)
+    print(peb, os.path.getsize(peb), "bytes")
+
+
 def hertz_goldens():
     golden("hertz64_boxes", hertz_scene(1, with_boxes=True), dem_steps=(1, 10), hc=False,
            dem_exe="ref_dem_hertz")
@@ -120,6 +134,9 @@ if __name__ == "__main__":
     if sys.argv[1:] == ["hertz"]:
         hertz_goldens()
         sys.exit(0)
+    if sys.argv[1:] == ["peb"]:
+        peb_fixture()
+        sys.exit(0)
     golden("small64_boxes", scenes.small_random(1, n=64, with_boxes=True))
     golden("small64_planes", scenes.small_random(2, n=64, with_boxes=False))
     golden("lattice512", scenes.dem_lattice(0, side=8), dem_steps=(1, 10, 100))
@@ -132,3 +149,4 @@ if __name__ == "__main__":
            dem_steps=(1,), hc_converged=True)
     adjoint_fd()
     hertz_goldens()
+    peb_fixture()

@@ -81,3 +81,36 @@ def test_world_api_mixed_precision_runs(driver, tmp_path):
     o = OracleWorld(s)
     o.dem_step(s.dt, 10)
     assert rel_err(x, o.x) < 1e-6
+
+
+def test_world_api_checkpoint_bytes_match_pe_format(driver, tmp_path):
+    """BodyBinaryWriter of the C++ API writes pe's checkpoint format byte for byte (the Python
+    writer is itself checked byte-identical against pe's writer in test_checkpoint.py)."""
+    from pe_b200 import checkpoint as ck
+    s = load_golden("small64_boxes")["scene"]
+    sp, out = str(tmp_path / "s.bin"), str(tmp_path / "cpp.peb")
+    s.save(sp)
+    r = subprocess.run([driver, "peb_write", sp, out], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    bodies, counter = ck.scene_bodies(s)
+    ref = str(tmp_path / "py.peb")
+    ck.write_peb(ref, bodies, counter)
+    assert open(out, "rb").read() == open(ref, "rb").read()
+
+
+@pytest.mark.gpu
+def test_world_api_resumes_pe_checkpoint(driver, tmp_path):
+    """pe's own checkpoint after 5 steps (tests/golden/peb_small64_boxes.peb), read by the C++
+    API's BodyBinaryReader and advanced 5 more steps on the GPU, lands on pe's uninterrupted
+    10-step state."""
+    from helpers import GOLDEN
+    g = load_golden("small64_boxes")
+    s = g["scene"]
+    sp, out = str(tmp_path / "s.bin"), str(tmp_path / "o.bin")
+    s.save(sp)
+    r = subprocess.run([driver, "peb_resume", sp, os.path.join(GOLDEN, "peb_small64_boxes.peb"),
+                        "5", out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    a = np.fromfile(out, "<f8").reshape(3, s.n, 3)
+    assert rel_err(a[0], g["dem10_x"]) < 1e-12
+    assert rel_err(a[1], g["dem10_v"]) < 1e-10
