@@ -477,4 +477,36 @@ __device__ __forceinline__ bool grid_sync(unsigned int *bar, int32_t *err) {
     return s_ok != 0;
 }
 
+// Grid-wide barrier on a counter that only grows within one launch (the caller zeroes it
+// before the launch): a block's arrival is one release-add, and a block leaves once an
+// acquire-load sees every block of this and all earlier episodes arrived.  Compared with
+// grid_sync there is no reset and no second word the last block has to publish, so a barrier
+// costs about one L2 round trip less.  *episode is the calling block's barrier count (thread 0
+// keeps it).  The wait is bounded like grid_sync's.
+__device__ __forceinline__ bool grid_sync_counted(unsigned int *count, unsigned int &episode,
+                                                  int32_t *err) {
+    __shared__ int s_ok2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int target = (++episode) * gridDim.x;
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(count), "r"(1u) : "memory");
+        unsigned int v = 0;
+        unsigned long long spins = 0;
+        int ok = 1;
+        for (;;) {
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if (v >= target) break;
+            if (++spins > 4096) __nanosleep(64);
+            if (spins > kSpinLimit) {
+                ok = 0;
+                atomicOr(err, DERR_TIMEOUT);
+                break;
+            }
+        }
+        s_ok2 = ok;
+    }
+    __syncthreads();
+    return s_ok2 != 0;
+}
+
 }  // namespace peb

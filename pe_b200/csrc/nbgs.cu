@@ -769,13 +769,14 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
                                                             unsigned int *bar, int32_t *err) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned int episode = 0;   // bar[0] was zeroed before the launch
     for (int it = 0; it < iters; ++it) {
         const int track = (track_last && it == iters - 1) ? 1 : 0;
         for (int col = 0; col < ncolors; ++col) {
             const int64_t e = color_start[col + 1];
             for (int64_t k = color_start[col] + g0; k < e; k += stride)
                 sweep_contact<T, MODEL, true>(k, dtinv, cc, bv, track, delta);
-            if (!grid_sync(bar, err)) return;
+            if (!grid_sync_counted(bar, episode, err)) return;
         }
     }
 }
@@ -1196,12 +1197,18 @@ int nbgs_step_t(Ctx *c, double dt) {
             auto kern = persistent_kernel<VT>(model);
             int occ = 0;
             cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0);
-            if (e == cudaSuccess && occ > 0) {
-                const unsigned grid = (unsigned)std::min<int64_t>(
-                    (int64_t)occ * c->sm_count, std::max<int64_t>(1, (maxcol + kBlk - 1) / kBlk));
+            const unsigned grid = (unsigned)std::min<int64_t>(
+                (int64_t)std::max(occ, 1) * c->sm_count, std::max<int64_t>(1, (maxcol + kBlk - 1) / kBlk));
+            // the barrier counter of one launch counts iters x colours x blocks arrivals; past
+            // 2^32 the colours are launched one by one instead
+            const bool fits = (double)iters * ncolors * grid < 4.0e9;
+            if (e == cudaSuccess && occ > 0 && fits) {
                 PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start,
                                             (ncolors + 1) * sizeof(int32_t),
                                             cudaMemcpyHostToDevice, c->stream));
+                // the barrier counter of this launch starts at zero (its episodes count up);
+                // iters x colours x blocks stays far below 2^32
+                PEB_CUDA(c, cudaMemsetAsync(nb.bar, 0, sizeof(unsigned int), c->stream));
                 int iters_a = iters, ncol_a = ncolors, track_a = c->want_residual ? 1 : 0;
                 int64_t cap_a = cap, n_a = n;
                 VT dtinv_a = VT(1.0 / dt);
@@ -1211,10 +1218,10 @@ int nbgs_step_t(Ctx *c, double dt) {
                 e = cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(kBlk), args, 0,
                                                 c->stream);
             }
-            if (e == cudaSuccess) {
+            if (e == cudaSuccess && occ > 0 && fits) {
                 done = true;
                 c->launches++;
-            } else {
+            } else if (e != cudaSuccess) {
                 cudaGetLastError();
                 nb.coop_disabled = true;
             }
