@@ -69,7 +69,7 @@ typedef struct {
     int32_t track_orientation; /* 1: integrate sphere quaternions (Default.h:190-193) */
     int64_t max_contacts;      /* HCSITS contact capacity; 0 = automatic (8 per sphere).
                                   DEM lists: initial capacity in entries (grown on demand);
-                                  0 = automatic (16 per sphere) */
+                                  0 = automatic (16 per sphere); at most INT32_MAX */
     double skin;               /* DEM neighbour-list skin; <= 0: 0.1 x the smallest radius */
     int32_t neighbor_lists;    /* DEM: 1 = Verlet lists rebuilt on demand (default),
                                   0 = grid search every step */
@@ -253,6 +253,20 @@ int pe_b200_dem_step_static(int64_t n, const double *x, const double *v, const d
                             double dt, const double domain_lo[3], const double domain_hi[3],
                             double max_radius, double *x_out, double *v_out, double *w_out,
                             void *stream);
+
+/* Consistency checks of the device state, run on the host (no pe counterpart beyond its debug
+ * assertions, pe_INTERNAL_ASSERT, compiled out in release builds):
+ *   - HCSITS: in the contact order of the last step no body appears twice in one colour (the
+ *     condition under which the parallel Gauss-Seidel sweep of a colour is race-free);
+ *   - DEM neighbour lists: entries in range, no self entries, every pair listed from both sides,
+ *     orientation bit = (user id of the sphere < user id of the neighbour).
+ * *problems receives the number of violations (0 = consistent).  Synchronises the stream. */
+int pe_b200_validate(pe_b200_ctx *ctx, int64_t *problems);
+/* Self-test of the bounded device waits: launches one kernel that waits on a flag nothing sets,
+ * which gives up after `polls` polls (1 <= polls <= 2^24) and records a timeout.  Returns
+ * PE_B200_ERR_TIMEOUT, as a real barrier or peer wait that ran out would, and leaves the context
+ * usable. */
+int pe_b200_selftest_timeout(pe_b200_ctx *ctx, int64_t polls);
 
 /* Number of kernels this context launched since creation (device-side work accounting). */
 int64_t pe_b200_kernel_launches(const pe_b200_ctx *ctx);

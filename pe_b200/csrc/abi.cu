@@ -1,4 +1,5 @@
 // abi.cu -- the extern "C" entry points of libpe_b200.so (declared in include/pe_b200.h).
+#include <nvtx3/nvToolsExt.h>
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -24,6 +25,11 @@ int set_err(Ctx *c, int code, const std::string &msg) {
 int cuda_err(Ctx *c, cudaError_t e, const char *where) {
     char buf[512];
     snprintf(buf, sizeof buf, "CUDA error %d (%s) at %s", (int)e, cudaGetErrorString(e), where);
+    // a failed allocation is not sticky: clear it, so the next launch check does not see it
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return set_err(c, PE_B200_ERR_NOMEM, buf);
+    }
     return set_err(c, PE_B200_ERR_CUDA, buf);
 }
 
@@ -42,6 +48,8 @@ static cudaEvent_t take_event(Ctx *c) {
 }
 
 void prof_begin(Ctx *c, int stage) {
+    // NVTX range per stage for timeline tools (host-side only; safe during graph capture)
+    nvtxRangePushA(kStageNames[stage]);
     if (!c->prof) return;
     cudaEvent_t e = take_event(c);
     if (!e) return;
@@ -50,6 +58,7 @@ void prof_begin(Ctx *c, int stage) {
 }
 
 void prof_end(Ctx *c, int stage) {
+    nvtxRangePop();
     if (!c->prof || !c->ev_pending[stage]) return;
     cudaEvent_t e = take_event(c);
     if (!e) return;
@@ -387,6 +396,7 @@ int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
         return PE_B200_ERR_UNSUPPORTED;
     if (p->max_iterations < 0 || p->damping < 0 || p->damping > 1) return PE_B200_ERR_ARG;
     if (p->force_model != 0 && p->force_model != 1) return PE_B200_ERR_ARG;
+    if (p->max_contacts < 0 || p->max_contacts > INT32_MAX) return PE_B200_ERR_ARG;   // int32 offsets
     Ctx *c = new (std::nothrow) Ctx();
     if (!c) return PE_B200_ERR_NOMEM;
     c->p = *p;
@@ -804,6 +814,28 @@ int pe_b200_profile(pe_b200_ctx *h, int32_t cap, const char **names, double *tot
     }
     *n_out = ST_COUNT;
     return PE_B200_OK;
+}
+
+int pe_b200_validate(pe_b200_ctx *h, int64_t *problems) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !problems) return PE_B200_ERR_ARG;
+    *problems = 0;
+    if (!c->uploaded) return PE_B200_OK;
+    cudaSetDevice(c->device);
+    int rc = validate_lists(c, problems);
+    if (!rc) rc = validate_coloring(c, problems);
+    return rc;
+}
+
+int pe_b200_selftest_timeout(pe_b200_ctx *h, int64_t polls) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || polls < 1 || polls > (int64_t(1) << 24)) return PE_B200_ERR_ARG;
+    cudaSetDevice(c->device);
+    int rc = check_device_errors(c);   // a pending device error belongs to an earlier call
+    if (rc) return rc;
+    rc = selftest_timeout(c, polls);
+    if (rc) return rc;
+    return check_device_errors(c);
 }
 
 int64_t pe_b200_kernel_launches(const pe_b200_ctx *h) {

@@ -852,9 +852,17 @@ int list_capacity_check(Ctx *c) {
 }
 
 // queues the read-back of the rebuild flags that list_capacity_check looks at
-int list_queue_check(Ctx *c) {
+// A read-back is a copy in the stream between two kernels, so it is queued once every
+// kCheckEvery steps: a list overflow (which only a rebuild can cause) is noticed that much later,
+// and the steps in between search the grid for the spheres that have candidates.
+constexpr int kCheckEvery = 8;
+
+int list_queue_check(Ctx *c, int steps = 1) {
     ListBuf &L = c->nl;
+    L.since_check += steps;
+    if (L.since_check < kCheckEvery) return PE_B200_OK;
     if (!L.check_pending) {
+        L.since_check = 0;
         PEB_CUDA(c, cudaMemcpyAsync(L.h_flags, L.flags, 4 * sizeof(int32_t),
                                     cudaMemcpyDeviceToHost, c->stream));
         PEB_CUDA(c, cudaEventRecord(L.ev, c->stream));
@@ -964,7 +972,7 @@ int dem_list_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *done) {
         PEB_CUDA(c, cudaGraphLaunch(G.exec, c->stream));
         c->launches += G.launches;
         *done += gs;
-        rc = list_queue_check(c);
+        rc = list_queue_check(c, gs);
         if (rc) return rc;
     }
     return PE_B200_OK;

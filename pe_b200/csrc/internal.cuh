@@ -102,6 +102,7 @@ struct ListBuf {
     int64_t rb_blk_cap = 0;
     bool coop_disabled = false;
     bool warm = false;          // a list step has run since the buffers were (re)allocated
+    int since_check = 1 << 20;  // steps since the last queued read-back of flags
 };
 
 // launch shapes of the DEM list step, picked by pe_b200_autotune (autotune.cu)
@@ -308,6 +309,12 @@ int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *g
 void adjoint_free(Ctx *c);
 int nbgs_step(Ctx *c, double dt);
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out);
+// body slots of the contacts of the last HCSITS step, in colour order (device memory)
+const int2 *nbgs_ids_ptr(Ctx *c);
+// validate.cu: host checks of the device state; each adds the problems it finds to *bad
+int validate_coloring(Ctx *c, int64_t *bad);
+int validate_lists(Ctx *c, int64_t *bad);
+int selftest_timeout(Ctx *c, int64_t polls);
 void nbgs_free(Ctx *c);
 
 // ------------------------------------------------------------------------------------------

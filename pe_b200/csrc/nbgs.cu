@@ -1298,6 +1298,21 @@ int nbgs_step(Ctx *c, double dt) {
     return (c->p.precision == PE_B200_FP64) ? nbgs_step_t<double>(c, dt) : nbgs_step_t<float>(c, dt);
 }
 
+const int2 *nbgs_ids_ptr(Ctx *c) {
+    if (c->p.precision == PE_B200_FP64) {
+        Raw<double> raw;
+        Cache<double> cc;
+        BodyV<double> bv;
+        layout(c, raw, cc, bv);
+        return cc.ids;
+    }
+    Raw<float> raw;
+    Cache<float> cc;
+    BodyV<float> bv;
+    layout(c, raw, cc, bv);
+    return cc.ids;
+}
+
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out) {
     const int64_t n = c->n;
     *n_out = 0;

@@ -253,6 +253,22 @@ class Engine:
                                                         C.byref(c), C.byref(sk)))
         return {"rebuilds": r.value, "entries": e.value, "capacity": c.value, "skin": sk.value}
 
+    def last_error(self) -> str:
+        m = self._L.pe_b200_last_error(self._h)
+        return m.decode() if m else ""
+
+    def validate(self) -> int:
+        """Number of inconsistencies in the device state: a body twice in one colour of the last
+        HCSITS step, or a malformed / asymmetric DEM neighbour list (0 = consistent)."""
+        p = C.c_int64()
+        self._check(self._L.pe_b200_validate(self._h, C.byref(p)))
+        return int(p.value)
+
+    def selftest_timeout(self, polls: int = 100000) -> int:
+        """Runs the bounded-wait self-test kernel; returns its status code (expected:
+        _abi.ERR_TIMEOUT) without raising."""
+        return int(self._L.pe_b200_selftest_timeout(self._h, int(polls)))
+
     def kernel_launches(self) -> int:
         return int(self._L.pe_b200_kernel_launches(self._h))
 

@@ -90,9 +90,13 @@ class Scene:
 def scene_from_bytes(buf: bytes, name: str = "") -> Scene:
     fmt = "<8sIIQII3dddI"
     hs = struct.calcsize(fmt)
+    if len(buf) < hs:
+        raise ValueError("truncated scene file")
     magic, ver, nm, n, npl, nbx, gx, gy, gz, dt, damping, steps = struct.unpack_from(fmt, buf, 0)
     if magic != SCENE_MAGIC or ver != SCENE_VERSION:
         raise ValueError("not a scene file")
+    if len(buf) != hs + 72 * nm + 36 * npl + 124 * nbx + 84 * n:
+        raise ValueError("scene file size does not match its header")
     off = hs
 
     def take(dtype, count, shape):
