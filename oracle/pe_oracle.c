@@ -161,6 +161,46 @@ void pe_or_sphere_mass(double r, double density, double *inv_mass, double *inv_i
     if (inertia) *inertia = I;
 }
 
+/* Quaternion.h:591-602 (toRotationMatrix) */
+static void quat_to_rot(const double *q, double *R) {
+    R[0] = 1.0 - 2.0 * q[2] * q[2] - 2.0 * q[3] * q[3];
+    R[1] = 2.0 * (q[1] * q[2] - q[0] * q[3]);
+    R[2] = 2.0 * (q[1] * q[3] + q[0] * q[2]);
+    R[3] = 2.0 * (q[1] * q[2] + q[0] * q[3]);
+    R[4] = 1.0 - 2.0 * q[1] * q[1] - 2.0 * q[3] * q[3];
+    R[5] = 2.0 * (q[2] * q[3] - q[0] * q[1]);
+    R[6] = 2.0 * (q[1] * q[3] - q[0] * q[2]);
+    R[7] = 2.0 * (q[2] * q[3] + q[0] * q[1]);
+    R[8] = 1.0 - 2.0 * q[1] * q[1] - 2.0 * q[2] * q[2];
+}
+
+/* BoxBase.h:186-189 (mass), BoxBase.cpp:152-158 (inertia, inverted by Matrix3x3::getInverse,
+ * Matrix3x3.h:1084-1105, reduced here to the diagonal): im, I[3], Iinv[3] in the body frame */
+static void box_mass(const double *len, double density, double *im, double *I, double *Iinv) {
+    const double mass = len[0] * len[1] * len[2] * density;
+    *im = 1.0 / mass;
+    I[0] = mass / 12.0 * (len[1] * len[1] + len[2] * len[2]);
+    I[1] = mass / 12.0 * (len[0] * len[0] + len[2] * len[2]);
+    I[2] = mass / 12.0 * (len[0] * len[0] + len[1] * len[1]);
+    double det = I[0] * ((I[1] * I[2]) - (0.0 * 0.0)) + 0.0 * ((0.0 * 0.0) - (I[2] * 0.0)) +
+                 0.0 * ((0.0 * 0.0) - (I[1] * 0.0));
+    det = 1.0 / det;
+    Iinv[0] = det * ((I[1] * I[2]) - (0.0 * 0.0));
+    Iinv[1] = det * ((I[2] * I[0]) - (0.0 * 0.0));
+    Iinv[2] = det * ((I[0] * I[1]) - (0.0 * 0.0));
+}
+
+/* R * diag(d) * R^T in pe's operation order ((R * D) * trans(R), RotationMatrix.h:1370-1429) */
+static m3 rot_diag_rt(const double *R, const double *d) {
+    m3 D;
+    memset(&D, 0, sizeof D);
+    D.m[0] = d[0]; D.m[4] = d[1]; D.m[8] = d[2];
+    m3 Rm, Rt;
+    memcpy(Rm.m, R, sizeof Rm.m);
+    Rt = m3_trans(Rm);
+    return m3_mul(m3_mul(Rm, D), Rt);
+}
+
 typedef struct {
     int64_t n, nb;   /* spheres, all bodies */
     double *im;      /* inverse mass per body (walls 0) */
@@ -168,18 +208,25 @@ typedef struct {
     double *I;       /* inertia (scalar) per body (walls 0) */
     int32_t *bmat;   /* material per body */
     double *bpos;    /* 3 per body: centre (planes: anchor point normal*d) */
+    int64_t mbase;   /* id of the first moving box */
+    m3 *Iinv_w;      /* moving boxes: inverse inertia in the world frame (RigidBody.h:866-869) */
+    m3 *I_w;         /* moving boxes: inertia in the world frame (RigidBody.h:842-845) */
 } body_props;
 
 static int body_props_init(const pe_or_world *w, body_props *bp) {
     const int64_t nw = (int64_t)w->nplanes + w->nboxes;
     bp->n = w->n;
-    bp->nb = w->n + nw;
+    bp->nb = w->n + nw + w->nmboxes;
+    bp->mbase = w->n + nw;
+    bp->Iinv_w = (m3 *)calloc((size_t)(w->nmboxes > 0 ? w->nmboxes : 1), sizeof(m3));
+    bp->I_w = (m3 *)calloc((size_t)(w->nmboxes > 0 ? w->nmboxes : 1), sizeof(m3));
     bp->im = (double *)calloc((size_t)bp->nb, sizeof(double));
     bp->ii = (double *)calloc((size_t)bp->nb, sizeof(double));
     bp->I = (double *)calloc((size_t)bp->nb, sizeof(double));
     bp->bmat = (int32_t *)calloc((size_t)bp->nb, sizeof(int32_t));
     bp->bpos = (double *)calloc((size_t)bp->nb * 3, sizeof(double));
-    if (!bp->im || !bp->ii || !bp->I || !bp->bmat || !bp->bpos) return -1;
+    if (!bp->im || !bp->ii || !bp->I || !bp->bmat || !bp->bpos || !bp->Iinv_w || !bp->I_w)
+        return -1;
     for (int64_t i = 0; i < w->n; ++i) {
         pe_or_sphere_mass(w->r[i], w->mats[w->mat[i]].density, &bp->im[i], &bp->ii[i], &bp->I[i]);
         bp->bmat[i] = w->mat[i];
@@ -196,11 +243,22 @@ static int body_props_init(const pe_or_world *w, body_props *bp) {
         bp->bmat[b] = w->box_mat[k];
         st3(bp->bpos + 3 * b, ld3(w->boxes + 15 * k));
     }
+    for (int32_t m = 0; m < w->nmboxes; ++m) {
+        const int64_t b = bp->mbase + m;
+        double I[3], Iinv[3], R[9];
+        box_mass(w->mb_len + 3 * m, w->mats[w->mb_mat[m]].density, &bp->im[b], I, Iinv);
+        quat_to_rot(w->mb_q + 4 * m, R);
+        bp->Iinv_w[m] = rot_diag_rt(R, Iinv);
+        bp->I_w[m] = rot_diag_rt(R, I);
+        bp->bmat[b] = w->mb_mat[m];
+        st3(bp->bpos + 3 * b, ld3(w->mb_x + 3 * m));
+    }
     return 0;
 }
 
 static void body_props_free(body_props *bp) {
     free(bp->im); free(bp->ii); free(bp->I); free(bp->bmat); free(bp->bpos);
+    free(bp->Iinv_w); free(bp->I_w);
 }
 
 /* Materials.h:633-639, 671-677, 709-715: harmonic composition inv(inv(a)+inv(b)) */
@@ -244,6 +302,7 @@ static void cpush(clist *l, int64_t b1, int64_t b2, v3 gpos, v3 n, double dist) 
     pe_or_contact *c = &l->c[l->n++];
     c->b1 = b1; c->b2 = b2;
     st3(c->gpos, gpos); st3(c->n, n); c->dist = dist;
+    c->kind = 0;
 }
 
 /* MaxContacts.h:547-569 (i < j: body 1 is the sphere with the smaller system id) */
@@ -272,13 +331,69 @@ static void collide_sphere_plane(const pe_or_world *w, int64_t i, int32_t p, cli
     }
 }
 
-/* MaxContacts.h:589-668 */
-static void collide_sphere_box(const pe_or_world *w, int64_t i, int32_t bi, clist *l) {
-    const double *B = w->boxes + 15 * bi;
-    const v3 L = mk(0.5 * B[3], 0.5 * B[4], 0.5 * B[5]);
-    const double *R = B + 6;
-    const v3 spos = ld3(w->x + 3 * i), bpos = ld3(B);
-    const int64_t bid = w->n + w->nplanes + bi;
+/* A box as the fine detection sees it: centre, rotation (row-major), side lengths, half
+ * lengths (real(0.5) * length, as MaxContacts.h and BoxBase.cpp compute them) and body id. */
+typedef struct {
+    v3 x;
+    double R[9];
+    double len[3], hl[3];
+    int64_t id;
+    int fixed;
+} obox;
+
+
+static int64_t mbox_base(const pe_or_world *w) { return w->n + w->nplanes + w->nboxes; }
+
+static obox fixed_box(const pe_or_world *w, int32_t k) {
+    const double *B = w->boxes + 15 * k;
+    obox b;
+    b.x = ld3(B);
+    memcpy(b.R, B + 6, sizeof b.R);
+    for (int a = 0; a < 3; ++a) { b.len[a] = B[3 + a]; b.hl[a] = 0.5 * B[3 + a]; }
+    b.id = w->n + w->nplanes + k;
+    b.fixed = 1;
+    return b;
+}
+
+static obox moving_box(const pe_or_world *w, int32_t m) {
+    obox b;
+    b.x = ld3(w->mb_x + 3 * m);
+    quat_to_rot(w->mb_q + 4 * m, b.R);
+    for (int a = 0; a < 3; ++a) { b.len[a] = w->mb_len[3 * m + a]; b.hl[a] = 0.5 * b.len[a]; }
+    b.id = mbox_base(w) + m;
+    b.fixed = 0;
+    return b;
+}
+
+/* BoxBase.cpp:100-115 (calcBoundingBox): lo[0..2], hi[3..5] */
+static void box_aabb(const obox *b, double *bb) {
+    const double *R = b->R, *L = b->len;
+    const double e[3] = {
+        0.5 * (fabs(R[0] * L[0]) + fabs(R[1] * L[1]) + fabs(R[2] * L[2])) + THR,
+        0.5 * (fabs(R[3] * L[0]) + fabs(R[4] * L[1]) + fabs(R[5] * L[2])) + THR,
+        0.5 * (fabs(R[6] * L[0]) + fabs(R[7] * L[1]) + fabs(R[8] * L[2])) + THR};
+    const double c[3] = {b->x.x, b->x.y, b->x.z};
+    for (int a = 0; a < 3; ++a) { bb[a] = c[a] - e[a]; bb[3 + a] = c[a] + e[a]; }
+}
+
+/* SphereBase.h:208-218 */
+static void sphere_aabb(const pe_or_world *w, int64_t i, double *bb) {
+    const double r = w->r[i] + THR;
+    for (int a = 0; a < 3; ++a) { bb[a] = w->x[3 * i + a] - r; bb[3 + a] = w->x[3 * i + a] + r; }
+}
+
+/* BoundingBox.h:487-497 */
+static int aabb_overlap(const double *a, const double *b) {
+    return !(b[0] > a[3] || b[1] > a[4] || b[2] > a[5] || b[3] < a[0] || b[4] < a[1] ||
+             b[5] < a[2]);
+}
+
+/* MaxContacts.h:589-668 (sphere i against a box, fixed or moving) */
+static void collide_sphere_obox(const pe_or_world *w, int64_t i, const obox *bx, clist *l) {
+    const v3 L = mk(bx->hl[0], bx->hl[1], bx->hl[2]);
+    const double *R = bx->R;
+    const v3 spos = ld3(w->x + 3 * i), bpos = bx->x;
+    const int64_t bid = bx->id;
     int outside = 0;
     const v3 d = sub(spos, bpos);
     double p[3] = {d.x * R[0] + d.y * R[3] + d.z * R[6], d.x * R[1] + d.y * R[4] + d.z * R[7],
@@ -311,10 +426,297 @@ static void collide_sphere_box(const pe_or_world *w, int64_t i, int32_t bi, clis
     if (dist < THR) cpush(l, i, bid, add(bpos, q), normalized(n), dist);
 }
 
-static int cmp_contact(const void *a, const void *b) {
-    const pe_or_contact *x = (const pe_or_contact *)a, *y = (const pe_or_contact *)b;
+/* MaxContacts.h:2380-2528: every corner of the box on the plane's side is tested */
+static void collide_box_plane(const pe_or_world *w, const obox *b, int32_t p, clist *l) {
+    const v3 pn = ld3(w->planes + 4 * p);
+    const double pd = w->planes[4 * p + 3];
+    const double *R = b->R;
+    const double range[3] = {0.5 * b->len[0], 0.5 * b->len[1], 0.5 * b->len[2]};
+    const double nrel[3] = {R[0] * pn.x + R[3] * pn.y + R[6] * pn.z,
+                            R[1] * pn.x + R[4] * pn.y + R[7] * pn.z,
+                            R[2] * pn.x + R[5] * pn.y + R[8] * pn.z};
+    double mn = range[0];
+    if (range[1] < mn) mn = range[1];
+    if (range[2] < mn) mn = range[2];
+    const double minlength = -0.99 * mn;
+    /* corner order of pe: lower-left-front, lower-right-front, lower-right-back,
+     * lower-left-back, then the same four on the upper face */
+    static const int sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                 {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+    for (int k = 0; k < 8; ++k) {
+        const double a = sg[k][0] > 0 ? range[0] * nrel[0] : -(range[0] * nrel[0]);
+        const double bb = sg[k][1] > 0 ? range[1] * nrel[1] : -(range[1] * nrel[1]);
+        const double c = sg[k][2] > 0 ? range[2] * nrel[2] : -(range[2] * nrel[2]);
+        if (!((a + bb) + c < minlength)) continue;
+        const double cl[3] = {sg[k][0] * range[0], sg[k][1] * range[1], sg[k][2] * range[2]};
+        const v3 pos = add(b->x, mk(R[0] * cl[0] + R[1] * cl[1] + R[2] * cl[2],
+                                    R[3] * cl[0] + R[4] * cl[1] + R[5] * cl[2],
+                                    R[6] * cl[0] + R[7] * cl[1] + R[8] * cl[2]));
+        const double kk = pos.x * pn.x + pos.y * pn.y + pos.z * pn.z;
+        const double dist = kk - pd;
+        if (dist < THR) cpush(l, b->id, w->n + p, pos, pn, dist);
+    }
+}
+
+/* R^T v and R v for row-major R (RotationMatrix.h:1318-1324 with trans()) */
+static v3 rt_mulv(const double *R, v3 v) {
+    return mk(R[0] * v.x + R[3] * v.y + R[6] * v.z, R[1] * v.x + R[4] * v.y + R[7] * v.z,
+              R[2] * v.x + R[5] * v.y + R[8] * v.z);
+}
+static v3 r_mulv(const double *R, v3 v) {
+    return mk(R[0] * v.x + R[1] * v.y + R[2] * v.z, R[3] * v.x + R[4] * v.y + R[5] * v.z,
+              R[6] * v.x + R[7] * v.y + R[8] * v.z);
+}
+static inline double v3_get(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+static inline void v3_set(v3 *a, int i, double s) {
+    if (i == 0) a->x = s; else if (i == 1) a->y = s; else a->z = s;
+}
+
+/* GeomTools.cpp:387-408 */
+static void intersect_lines(v3 o1, v3 d1, v3 o2, v3 d2, double *s, double *t) {
+    const v3 c = cross(d1, d2);
+    const double sqrlen = c.x * c.x + c.y * c.y + c.z * c.z;
+    if (sqrlen < 1e-8) { /* parallelThreshold, Thresholds.h:170 */
+        *s = 0.0;
+        *t = 0.0;
+        return;
+    }
+    const double isqrlen = 1.0 / sqrlen;
+    const v3 p = sub(o2, o1);
+    const double dd = dot(d1, d2);
+    const double a = dot(d1, p);
+    const double b = dot(neg(d2), p);
+    *s = (a * dot(d2, d2) + dd * b) * isqrlen;
+    *t = (b * dot(d1, d1) + dd * a) * isqrlen;
+}
+
+/* one contact point of the vertex/face case (MaxContacts.h:1419-2250): body 1 is B, body 2 A */
+static void bb_push(clist *l, const obox *A, const obox *B, v3 gpos, v3 n, double dist) {
+    cpush(l, B->id, A->id, gpos, n, dist);
+}
+
+/* MaxContacts.h:867-2250: separating-axis test over the 15 axes of the two boxes, then one
+ * contact at the closest points of the two edges (edge/edge case) or the contact points of
+ * the incident face clipped against the reference face (vertex/face case). */
+static void collide_box_box(const obox *p1, const obox *p2, clist *l) {
+    const obox *b1 = p1, *b2 = p2;
+    if (b2->id < b1->id) { const obox *t = b1; b1 = b2; b2 = t; }
+    double maxDepth = -1.79769313486231570815e308;
+    int invertNormal = 0;
+    int contactCase = 0;
+    v3 contactNormal = mk(0.0, 0.0, 0.0), normal_c = mk(0.0, 0.0, 0.0);
+    const double *R1 = b1->R, *R2 = b2->R;
+    double rR[9], rQ[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            rR[3 * i + j] = R1[i] * R2[j] + R1[3 + i] * R2[3 + j] + R1[6 + i] * R2[6 + j];
+    for (int k = 0; k < 9; ++k) rQ[k] = fabs(rR[k]);
+    const v3 rPv = rt_mulv(R1, sub(b2->x, b1->x));
+    const double rPos[3] = {rPv.x, rPv.y, rPv.z};
+    const double *hl1 = b1->hl, *hl2 = b2->hl;
+    /* the three face axes of box 1 */
+    for (int i = 0; i < 3; ++i) {
+        const double term1 =
+            fabs(rPos[i]) - (hl1[i] + hl2[0] * rQ[3 * i] + hl2[1] * rQ[3 * i + 1] + hl2[2] * rQ[3 * i + 2]);
+        if (term1 > THR) return;
+        if (i == 0 || term1 > maxDepth) {
+            maxDepth = term1;
+            contactNormal = mk(R1[i], R1[3 + i], R1[6 + i]);
+            contactCase = 1 + i;
+            invertNormal = rPos[i] < 0.0;
+        }
+    }
+    /* the three face axes of box 2 */
+    for (int j = 0; j < 3; ++j) {
+        const double term1 = rPos[0] * rR[j] + rPos[1] * rR[3 + j] + rPos[2] * rR[6 + j];
+        const double term2 =
+            fabs(term1) - (hl1[0] * rQ[j] + hl1[1] * rQ[3 + j] + hl1[2] * rQ[6 + j] + hl2[j]);
+        if (term2 > THR) return;
+        if (term2 > maxDepth) {
+            maxDepth = term2;
+            contactNormal = mk(R2[j], R2[3 + j], R2[6 + j]);
+            contactCase = 4 + j;
+            invertNormal = term1 < 0.0;
+        }
+    }
+    /* the nine edge-edge axes, in pe's order (au x bu, au x bv, ... aw x bw); per case: the
+     * indices of term1 = rPos[p0]*rR[p1] - rPos[p2]*rR[p3], term2 = hl1[h0]*rQ[q0] +
+     * hl1[h1]*rQ[q1], term3 = hl2[h2]*rQ[q2] + hl2[h3]*rQ[q3], length from rR[s0], rR[s1] and
+     * the axis in box 1's frame */
+    static const int E[9][16] = {
+        /* p0 p1 p2 p3  h0 q0 h1 q1  h2 q2 h3 q3  s0 s1 axis(zero component) */
+        {2, 3, 1, 6, 1, 6, 2, 3, 2, 1, 1, 2, 6, 3, 0, 0},
+        {2, 4, 1, 7, 1, 7, 2, 4, 0, 2, 2, 0, 7, 4, 0, 0},
+        {2, 5, 1, 8, 1, 8, 2, 5, 1, 0, 0, 1, 8, 5, 0, 0},
+        {0, 6, 2, 0, 2, 0, 0, 6, 2, 4, 1, 5, 6, 0, 1, 0},
+        {0, 7, 2, 1, 2, 1, 0, 7, 0, 5, 2, 3, 7, 1, 1, 0},
+        {0, 8, 2, 2, 2, 2, 0, 8, 1, 3, 0, 4, 8, 2, 1, 0},
+        {1, 0, 0, 3, 0, 3, 1, 0, 2, 7, 1, 8, 3, 0, 2, 0},
+        {1, 1, 0, 4, 0, 4, 1, 1, 0, 8, 2, 6, 4, 1, 2, 0},
+        {1, 2, 0, 5, 0, 5, 1, 2, 1, 6, 0, 7, 5, 2, 2, 0}};
+    for (int e = 0; e < 9; ++e) {
+        const int *c = E[e];
+        const double term1 = rPos[c[0]] * rR[c[1]] - rPos[c[2]] * rR[c[3]];
+        const double term2 = hl1[c[4]] * rQ[c[5]] + hl1[c[6]] * rQ[c[7]];
+        const double term3 = hl2[c[8]] * rQ[c[9]] + hl2[c[10]] * rQ[c[11]];
+        double sum = fabs(term1) - (term2 + term3);
+        if (fabs(term1) > term2 + term3 + THR) return;
+        const double a = rR[c[12]], b = rR[c[13]];
+        const double length = sqrt(a * a + b * b);
+        if (length > 2.2204460492503131e-16) { /* epsilon */
+            sum /= length;
+            if (sum > maxDepth && fabs(sum - maxDepth) > 1e-8) { /* accuracy */
+                maxDepth = sum;
+                /* au x b*: (0, -s0, s1); av x b*: (s0, 0, -s1); aw x b*: (-s0, s1, 0) */
+                if (c[14] == 0) normal_c = mk(0.0, -a / length, b / length);
+                else if (c[14] == 1) normal_c = mk(a / length, 0.0, -b / length);
+                else normal_c = mk(-a / length, b / length, 0.0);
+                contactCase = 7 + e;
+                invertNormal = term1 < 0.0;
+            }
+        }
+    }
+    if (contactCase == 0) return;
+    if (contactCase > 6) contactNormal = r_mulv(R1, normal_c);
+    if (invertNormal) contactNormal = neg(contactNormal);
+
+    if (contactCase > 6) { /* edge/edge, MaxContacts.h:1343-1417 */
+        v3 pB1 = b1->x;
+        v3 sg = rt_mulv(R1, contactNormal);
+        v3 sv;
+        for (int i = 0; i < 3; ++i) v3_set(&sv, i, v3_get(sg, i) > 0.0 ? hl1[i] : -hl1[i]);
+        pB1 = add(pB1, r_mulv(R1, sv));
+        v3 pB2 = b2->x;
+        sg = rt_mulv(R2, contactNormal);
+        for (int i = 0; i < 3; ++i) v3_set(&sv, i, v3_get(sg, i) > 0.0 ? -hl2[i] : hl2[i]);
+        pB2 = add(pB2, r_mulv(R2, sv));
+        v3 ua, ub;
+        for (int i = 0; i < 3; ++i) {
+            v3_set(&ua, i, R1[(contactCase - 7) / 3 + i * 3]);
+            v3_set(&ub, i, R2[(contactCase - 7) % 3 + i * 3]);
+        }
+        double s, t;
+        intersect_lines(pB1, ua, pB2, ub, &s, &t);
+        pB1 = add(pB1, smul(s, ua));
+        pB2 = add(pB2, smul(t, ub));
+        const v3 gpos = smul(0.5, add(pB1, pB2));
+        cpush(l, b2->id, b1->id, gpos, contactNormal, maxDepth);
+        if (!l->oom) l->c[l->n - 1].kind = 1;
+        return;
+    }
+
+    /* vertex/face: A owns the reference face */
+    const obox *A = b1, *B = b2;
+    const double *hla = hl1, *hlb = hl2;
+    if (contactCase > 3) {
+        A = b2; B = b1;
+        hla = hl2; hlb = hl1;
+        contactNormal = neg(contactNormal);
+    }
+    const double *Ra = A->R, *Rb = B->R;
+    const v3 na = rt_mulv(Ra, contactNormal), nb = rt_mulv(Rb, contactNormal);
+    const double normala[3] = {na.x, na.y, na.z}, normalb[3] = {nb.x, nb.y, nb.z};
+    int xb, yb, zb;
+    if (fabs(normalb[0]) > fabs(normalb[1])) {
+        if (fabs(normalb[0]) > fabs(normalb[2])) { xb = 0; yb = 1; zb = 2; }
+        else { xb = 2; yb = 0; zb = 1; }
+    } else if (fabs(normalb[1]) > fabs(normalb[2])) { xb = 1; yb = 2; zb = 0; }
+    else { xb = 2; yb = 0; zb = 1; }
+    const int xa = contactCase < 4 ? contactCase - 1 : contactCase - 4;
+    const int ya = xa == 0 ? 1 : (xa == 1 ? 2 : 0);
+    const int za = xa == 0 ? 2 : (xa == 1 ? 0 : 1);
+    /* the incident face of B in B's frame, then in A's frame */
+    double vb[4][3];
+    for (int k = 0; k < 4; ++k) {
+        vb[k][xb] = normalb[xb] > 0.0 ? -hlb[xb] : hlb[xb];
+        vb[k][yb] = (k & 1) ? hlb[yb] : -hlb[yb];
+        vb[k][zb] = (k & 2) ? hlb[zb] : -hlb[zb];
+    }
+    const v3 ab = sub(B->x, A->x);
+    double vba[4][3];
+    for (int k = 0; k < 4; ++k) {
+        const v3 t = rt_mulv(Ra, add(ab, r_mulv(Rb, mk(vb[k][0], vb[k][1], vb[k][2]))));
+        vba[k][0] = t.x; vba[k][1] = t.y; vba[k][2] = t.z;
+    }
+    const double offseta = normala[xa] > 0.0 ? hla[xa] : -hla[xa];
+    /* the incident face's edges (v0-v1, v0-v2, v3-v1, v3-v2) against the four side lines of
+     * the reference face (y = +h, y = -h, z = +h, z = -h in A's frame), MaxContacts.h:1546 */
+    static const int EDGE[4][2] = {{0, 1}, {0, 2}, {3, 1}, {3, 2}};
+    for (int e = 0; e < 4; ++e) {
+        const double *P = vba[EDGE[e][0]], *Q = vba[EDGE[e][1]];
+        for (int side = 0; side < 4; ++side) {
+            const int cc = side < 2 ? ya : za, o = side < 2 ? za : ya;
+            const double h = (side & 1) ? -hla[cc] : hla[cc];
+            if (!((P[cc] > h) ^ (Q[cc] > h))) continue;
+            const double s = (h - P[cc]) / (Q[cc] - P[cc]);
+            if (!(s > 0.0 && s < 1.0)) continue;
+            const double tmp = P[o] + s * (Q[o] - P[o]);
+            if (!(fabs(tmp) < hla[o])) continue;
+            const double dist = fabs(P[xa] + s * (Q[xa] - P[xa])) - hla[xa];
+            if (!(dist < THR)) continue;
+            double posa[3];
+            posa[xa] = offseta;
+            posa[cc] = h;
+            posa[o] = tmp;
+            const v3 gpos = add(A->x, r_mulv(Ra, mk(posa[0], posa[1], posa[2])));
+            bb_push(l, A, B, gpos, contactNormal, dist);
+        }
+    }
+    /* vertices of B inside the reference face */
+    for (int k = 0; k < 4; ++k) {
+        if (fabs(vba[k][ya]) <= hla[ya] && fabs(vba[k][za]) <= hla[za]) {
+            const double dist = fabs(vba[k][xa]) - hla[xa];
+            if (dist < THR) {
+                const v3 gpos = add(A->x, r_mulv(Ra, mk(vba[k][0], vba[k][1], vba[k][2])));
+                bb_push(l, A, B, gpos, contactNormal, dist);
+            }
+        }
+    }
+    /* vertices of A's reference face inside B's incident face (a vertex on B's vertex is
+     * counted once, MaxContacts.h:2179-2185) */
+    double va[4][3];
+    for (int k = 0; k < 4; ++k) {
+        va[k][xa] = normala[xa] > 0.0 ? hla[xa] : -hla[xa];
+        va[k][ya] = (k & 1) ? hla[ya] : -hla[ya];
+        va[k][za] = (k & 2) ? hla[za] : -hla[za];
+    }
+    const v3 ba = sub(A->x, B->x);
+    for (int k = 0; k < 4; ++k) {
+        const v3 t = rt_mulv(Rb, add(ba, r_mulv(Ra, mk(va[k][0], va[k][1], va[k][2]))));
+        const double vab[3] = {t.x, t.y, t.z};
+        const double ay = fabs(vab[yb]), az = fabs(vab[zb]);
+        if (((ay <= hlb[yb] && az < hlb[zb]) || (ay < hlb[yb] && az <= hlb[zb]))) {
+            const double dist = fabs(vab[xb]) - hlb[xb];
+            if (dist < THR) {
+                const v3 gpos = add(B->x, r_mulv(Rb, t));
+                bb_push(l, A, B, gpos, contactNormal, dist);
+            }
+        }
+    }
+}
+
+static int cmp_contact(const pe_or_contact *x, const pe_or_contact *y) {
     if (x->b1 != y->b1) return x->b1 < y->b1 ? -1 : 1;
     if (x->b2 != y->b2) return x->b2 < y->b2 ? -1 : 1;
+    return 0;
+}
+
+/* merge sort by (b1, b2), stable so that the contacts of one box pair keep their order */
+static int stable_sort_contacts(pe_or_contact *c, int64_t n) {
+    pe_or_contact *tmp = (pe_or_contact *)malloc((size_t)n * sizeof(pe_or_contact));
+    if (!tmp) return -1;
+    for (int64_t width = 1; width < n; width *= 2) {
+        for (int64_t lo = 0; lo < n; lo += 2 * width) {
+            const int64_t mid = lo + width < n ? lo + width : n;
+            const int64_t hi = lo + 2 * width < n ? lo + 2 * width : n;
+            int64_t a = lo, b = mid, k = lo;
+            while (a < mid && b < hi) tmp[k++] = (cmp_contact(&c[b], &c[a]) < 0) ? c[b++] : c[a++];
+            while (a < mid) tmp[k++] = c[a++];
+            while (b < hi) tmp[k++] = c[b++];
+        }
+        memcpy(c, tmp, (size_t)n * sizeof(pe_or_contact));
+    }
+    free(tmp);
     return 0;
 }
 
@@ -396,10 +798,45 @@ static int find_contacts_list(const pe_or_world *w, clist *l) {
      * finite bodies in the grids, tested here directly */
     for (int64_t i = 0; i < n; ++i) {
         for (int32_t p = 0; p < w->nplanes; ++p) collide_sphere_plane(w, i, p, l);
-        for (int32_t b = 0; b < w->nboxes; ++b) collide_sphere_box(w, i, b, l);
+        for (int32_t b = 0; b < w->nboxes; ++b) {
+            const obox fb = fixed_box(w, b);
+            collide_sphere_obox(w, i, &fb, l);
+        }
+    }
+    /* moving boxes: HashGrids::collide (HashGrids.h:1351-1358) tests the bounding boxes before
+     * the fine detection; planes are infinite bodies and always tested (HashGrids.h:1278-1285);
+     * fixed boxes are finite bodies in the grids */
+    const int32_t M = w->nmboxes;
+    if (M > 0) {
+        obox *mb = (obox *)malloc((size_t)M * sizeof(obox));
+        double *bb = (double *)malloc((size_t)M * 6 * sizeof(double));
+        if (!mb || !bb) { free(mb); free(bb); free(l->c); return -1; }
+        for (int32_t m = 0; m < M; ++m) {
+            mb[m] = moving_box(w, m);
+            box_aabb(&mb[m], bb + 6 * m);
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            double sb[6];
+            sphere_aabb(w, i, sb);
+            for (int32_t m = 0; m < M; ++m)
+                if (aabb_overlap(sb, bb + 6 * m)) collide_sphere_obox(w, i, &mb[m], l);
+        }
+        for (int32_t m = 0; m < M; ++m) {
+            for (int32_t p = 0; p < w->nplanes; ++p) collide_box_plane(w, &mb[m], p, l);
+            for (int32_t k = 0; k < w->nboxes; ++k) {
+                const obox fb = fixed_box(w, k);
+                double fbb[6];
+                box_aabb(&fb, fbb);
+                if (aabb_overlap(bb + 6 * m, fbb)) collide_box_box(&mb[m], &fb, l);
+            }
+            for (int32_t m2 = m + 1; m2 < M; ++m2)
+                if (aabb_overlap(bb + 6 * m, bb + 6 * m2)) collide_box_box(&mb[m], &mb[m2], l);
+        }
+        free(mb);
+        free(bb);
     }
     if (l->oom) { free(l->c); return -1; }
-    if (l->n > 1) qsort(l->c, (size_t)l->n, sizeof(pe_or_contact), cmp_contact);
+    if (l->n > 1 && stable_sort_contacts(l->c, l->n) != 0) { free(l->c); return -1; }
     return 0;
 }
 
@@ -418,24 +855,44 @@ int64_t pe_or_find_contacts(const pe_or_world *w, pe_or_contact *out, int64_t ca
 
 /* RigidBody.h:1080-1085 */
 static inline v3 vel_from_wf(const pe_or_world *w, int64_t b, v3 gpos) {
-    if (b >= w->n) return mk(0.0, 0.0, 0.0);
-    const v3 v = ld3(w->v + 3 * b), om = ld3(w->w + 3 * b), x = ld3(w->x + 3 * b);
+    const int64_t mb = mbox_base(w);
+    if (b >= w->n && b < mb) return mk(0.0, 0.0, 0.0);
+    const double *vv = b < w->n ? w->v + 3 * b : w->mb_v + 3 * (b - mb);
+    const double *ww = b < w->n ? w->w + 3 * b : w->mb_w + 3 * (b - mb);
+    const double *xx = b < w->n ? w->x + 3 * b : w->mb_x + 3 * (b - mb);
+    const v3 v = ld3(vv), om = ld3(ww), x = ld3(xx);
     return add(v, cross(om, sub(gpos, x)));
+}
+
+/* index of a dynamic body in the force accumulators (spheres, then moving boxes); -1: wall */
+static inline int64_t dyn_index(const pe_or_world *w, int64_t b) {
+    if (b < w->n) return b;
+    const int64_t mb = mbox_base(w);
+    return b >= mb ? w->n + (b - mb) : -1;
+}
+
+static inline const double *body_x(const pe_or_world *w, int64_t b) {
+    return b < w->n ? w->x + 3 * b : w->mb_x + 3 * (b - mbox_base(w));
 }
 
 /* RigidBody.h:1775-1803 */
 static inline void add_force_at_pos(const pe_or_world *w, double *F, double *T, int64_t b, v3 f,
                                     v3 gpos) {
-    if (b >= w->n) return; /* walls are fixed: their accumulated force is never used */
-    st3(F + 3 * b, add(ld3(F + 3 * b), f));
-    st3(T + 3 * b, add(ld3(T + 3 * b), cross(sub(gpos, ld3(w->x + 3 * b)), f)));
+    const int64_t d = dyn_index(w, b);
+    if (d < 0) return; /* walls are fixed: their accumulated force is never used */
+    st3(F + 3 * d, add(ld3(F + 3 * d), f));
+    st3(T + 3 * d, add(ld3(T + 3 * d), cross(sub(gpos, ld3(body_x(w, b))), f)));
 }
 
 static int32_t body_mat(const pe_or_world *w, int64_t b) {
     if (b < w->n) return w->mat[b];
     if (b < w->n + w->nplanes) return w->plane_mat[b - w->n];
-    return w->box_mat[b - w->n - w->nplanes];
+    if (b < mbox_base(w)) return w->box_mat[b - w->n - w->nplanes];
+    return w->mb_mat[b - mbox_base(w)];
 }
+
+
+
 
 /* Materials.h:586-600: effective Young's modulus 1/E = (1-nu1^2)/E1 + (1-nu2^2)/E2, in pe's
  * operation order */
@@ -453,7 +910,8 @@ static void dem_resolve(const pe_or_world *w, const pe_or_contact *c, double *F,
     if (!(c->dist < -THR)) return; /* ContactBase.h:307-310 isPenetrating */
     const v3 gpos = ld3(c->gpos), n = ld3(c->n);
     const v3 rvel = sub(vel_from_wf(w, c->b1, gpos), vel_from_wf(w, c->b2, gpos));
-    const contact_params cp = compose(w, body_mat(w, c->b1), body_mat(w, c->b2), n, rvel);
+    contact_params cp = compose(w, body_mat(w, c->b1), body_mat(w, c->b2), n, rvel);
+    if (c->kind == 1) cp.k = cp.cn = cp.ct = 0.0;
     const double delta = -c->dist;
     const double relVelN = -dot(n, rvel);
     const v3 relVel = neg(rvel);
@@ -479,13 +937,37 @@ static void dem_resolve(const pe_or_world *w, const pe_or_contact *c, double *F,
     add_force_at_pos(w, F, T, c->b2, neg(fT), gpos);
 }
 
+/* boxtrait/Default.h:149-220 (BoxTrait::move) for moving box m, force F and torque T */
+static void box_move(pe_or_world *w, int32_t m, v3 F, v3 T, double dt) {
+    const pe_or_material *mt = &w->mats[w->mb_mat[m]];
+    double im, I[3], Iinv[3], R[9];
+    box_mass(w->mb_len + 3 * m, mt->density, &im, I, Iinv);
+    quat_to_rot(w->mb_q + 4 * m, R);
+    const v3 g = mk(w->gravity[0], w->gravity[1], w->gravity[2]);
+    const v3 vdot = add(mul(F, im), g);
+    const v3 tmp1 = rt_mulv(R, T);
+    const v3 tmp2 = mk(Iinv[0] * tmp1.x, Iinv[1] * tmp1.y, Iinv[2] * tmp1.z);
+    const v3 wdot = r_mulv(R, tmp2);
+    v3 v = add(ld3(w->mb_v + 3 * m), mul(vdot, dt));
+    v3 om = add(ld3(w->mb_w + 3 * m), mul(wdot, dt));
+    st3(w->mb_x + 3 * m, add(ld3(w->mb_x + 3 * m), mul(v, dt)));
+    quat_update(w->mb_q + 4 * m, mul(om, dt));
+    if (w->damping < 1.0) {
+        const double drag = pow(w->damping, dt);
+        v = mul(v, drag);
+        om = mul(om, drag);
+    }
+    st3(w->mb_v + 3 * m, v);
+    st3(w->mb_w + 3 * m, om);
+}
+
 /* collisionsystem/DEMSolver.h:1155-1262 + spheretrait/Default.h:149-220 */
 int64_t pe_or_dem_step(pe_or_world *w, double dt) {
     clist l;
     if (find_contacts_list(w, &l) != 0) return -1;
-    const int64_t n = w->n;
-    double *F = (double *)calloc((size_t)(3 * n + 3), sizeof(double));
-    double *T = (double *)calloc((size_t)(3 * n + 3), sizeof(double));
+    const int64_t n = w->n, nd = w->n + w->nmboxes;
+    double *F = (double *)calloc((size_t)(3 * nd + 3), sizeof(double));
+    double *T = (double *)calloc((size_t)(3 * nd + 3), sizeof(double));
     if (!F || !T) { free(F); free(T); free(l.c); return -1; }
     for (int64_t k = 0; k < l.n; ++k) dem_resolve(w, &l.c[k], F, T);
     const v3 g = mk(w->gravity[0], w->gravity[1], w->gravity[2]);
@@ -506,6 +988,8 @@ int64_t pe_or_dem_step(pe_or_world *w, double dt) {
         st3(w->v + 3 * i, v);
         st3(w->w + 3 * i, om);
     }
+    for (int32_t m = 0; m < w->nmboxes; ++m)
+        box_move(w, m, ld3(F + 3 * (n + m)), ld3(T + 3 * (n + m)), dt);
     free(F); free(T);
     const int64_t nc = l.n;
     free(l.c);
@@ -552,7 +1036,10 @@ static void hc_cache(const pe_or_world *w, const body_props *bp, const pe_or_con
         const v3 rv = sub(vel_from_wf(w, c->b1, gpos), vel_from_wf(w, c->b2, gpos));
         h->mu = compose(w, body_mat(w, c->b1), body_mat(w, c->b2), n, rv).mu;
     }
-    const m3 I1 = m3_scaled_identity(bp->ii[c->b1]), I2 = m3_scaled_identity(bp->ii[c->b2]);
+    const m3 I1 = c->b1 >= bp->mbase ? bp->Iinv_w[c->b1 - bp->mbase]
+                                     : m3_scaled_identity(bp->ii[c->b1]);
+    const m3 I2 = c->b2 >= bp->mbase ? bp->Iinv_w[c->b2 - bp->mbase]
+                                     : m3_scaled_identity(bp->ii[c->b2]);
     const m3 a = m3_cross_v3(v3_cross_m3(h->r1, I1), h->r1);
     const m3 b = m3_cross_v3(v3_cross_m3(h->r2, I2), h->r2);
     m3 D;
@@ -578,6 +1065,7 @@ typedef struct {
 } hc_bodies;
 
 static inline v3 wf_imp(const body_props *bp, int64_t b, v3 r, v3 p) {
+    if (b >= bp->mbase) return m3_mulv(bp->Iinv_w[b - bp->mbase], cross(r, p));
     return smul(bp->ii[b], cross(r, p));
 }
 
@@ -1001,6 +1489,12 @@ static int64_t hcsits_run(pe_or_world *w, double dt, int model, int max_iter, do
         const v3 Iw = smul(bp.I[i], om);
         B.w[i] = add(om, smul(dt, smul(bp.ii[i], cross(Iw, om))));
     }
+    for (int32_t m = 0; m < w->nmboxes; ++m) {
+        const int64_t b = bp.mbase + m;
+        const v3 v = ld3(w->mb_v + 3 * m), om = ld3(w->mb_w + 3 * m);
+        B.v[b] = add(v, mul(g, dt));
+        B.w[b] = add(om, smul(dt, m3_mulv(bp.Iinv_w[m], cross(m3_mulv(bp.I_w[m], om), om))));
+    }
     const double dtinv = 1.0 / dt;
     double delta = 0.0;
     for (int it = 0; it < max_iter; ++it) {
@@ -1028,6 +1522,19 @@ static int64_t hcsits_run(pe_or_world *w, double dt, int model, int max_iter, do
         }
         st3(w->v + 3 * i, v);
         st3(w->w + 3 * i, om);
+    }
+    for (int32_t m = 0; m < w->nmboxes; ++m) {
+        const int64_t b = bp.mbase + m;
+        v3 v = add(B.v[b], B.dv[b]), om = add(B.w[b], B.dw[b]);
+        st3(w->mb_x + 3 * m, add(ld3(w->mb_x + 3 * m), mul(v, dt)));
+        quat_update(w->mb_q + 4 * m, mul(om, dt));
+        if (w->damping < 1.0) {
+            const double drag = pow(w->damping, dt);
+            v = mul(v, drag);
+            om = mul(om, drag);
+        }
+        st3(w->mb_v + 3 * m, v);
+        st3(w->mb_w + 3 * m, om);
     }
     free(C); free(B.v); free(B.w); free(B.dv); free(B.dw); body_props_free(&bp);
     return nc;

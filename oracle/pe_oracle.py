@@ -33,16 +33,30 @@ class World(C.Structure):
                 ("nplanes", C.c_int32), ("planes", C.c_void_p), ("plane_mat", C.c_void_p),
                 ("nboxes", C.c_int32), ("boxes", C.c_void_p), ("box_mat", C.c_void_p),
                 ("nmat", C.c_int32), ("mats", C.c_void_p), ("gravity", C.c_double * 3),
-                ("damping", C.c_double), ("force_model", C.c_int32)]
+                ("damping", C.c_double), ("force_model", C.c_int32),
+                ("nmboxes", C.c_int32), ("mb_x", C.c_void_p), ("mb_q", C.c_void_p),
+                ("mb_v", C.c_void_p), ("mb_w", C.c_void_p), ("mb_len", C.c_void_p),
+                ("mb_mat", C.c_void_p)]
 
 
 class Contact(C.Structure):
     _fields_ = [("b1", C.c_int64), ("b2", C.c_int64), ("gpos", C.c_double * 3),
-                ("n", C.c_double * 3), ("dist", C.c_double)]
+                ("n", C.c_double * 3), ("dist", C.c_double), ("kind", C.c_int64)]
 
 
+# kind: 0 vertex/face, 1 edge/edge (no DEM force: pe's edge/edge contacts have zero stiffness)
 CONTACT_DTYPE = np.dtype([("b1", "<i8"), ("b2", "<i8"), ("gpos", "<f8", 3), ("n", "<f8", 3),
-                          ("dist", "<f8")])
+                          ("dist", "<f8"), ("kind", "<i8")])
+
+
+def as_contacts(c) -> np.ndarray:
+    """A contact array in CONTACT_DTYPE (records without a kind are vertex/face contacts)."""
+    c = np.asarray(c)
+    out = np.zeros(c.shape[0], CONTACT_DTYPE)
+    for f in CONTACT_DTYPE.names:
+        if f in c.dtype.names:
+            out[f] = c[f]
+    return out
 
 _lib = None
 
@@ -106,6 +120,15 @@ class OracleWorld:
         self.damping = float(s.damping)
         self.n = s.n
         self.nwalls = self.planes.shape[0] + self.boxes.shape[0]
+        # moving boxes (bodies n + nwalls + m)
+        nmb = int(getattr(s, "nmbox", 0))
+        self.nmbox = nmb
+        self.mb_x = np.ascontiguousarray(s.mbox_x if nmb else np.zeros((0, 3)), np.float64).copy()
+        self.mb_q = np.ascontiguousarray(s.mbox_q if nmb else np.zeros((0, 4)), np.float64).copy()
+        self.mb_v = np.ascontiguousarray(s.mbox_v if nmb else np.zeros((0, 3)), np.float64).copy()
+        self.mb_w = np.ascontiguousarray(s.mbox_w if nmb else np.zeros((0, 3)), np.float64).copy()
+        self.mb_len = np.ascontiguousarray(s.mbox_len if nmb else np.zeros((0, 3)), np.float64)
+        self.mb_mat = np.ascontiguousarray(s.mbox_mat if nmb else np.zeros(0), np.int32)
 
     def _struct(self) -> World:
         w = World()
@@ -119,6 +142,10 @@ class OracleWorld:
             w.gravity[a] = self.gravity[a]
         w.damping = self.damping
         w.force_model = self.force_model
+        w.nmboxes = self.nmbox
+        w.mb_x, w.mb_q, w.mb_v, w.mb_w = (_ptr(self.mb_x), _ptr(self.mb_q), _ptr(self.mb_v),
+                                          _ptr(self.mb_w))
+        w.mb_len, w.mb_mat = _ptr(self.mb_len), _ptr(self.mb_mat)
         return w
 
     def contacts(self) -> np.ndarray:
@@ -149,7 +176,7 @@ class OracleWorld:
         s = self._struct()
         delta, resid = C.c_double(0.0), C.c_double(0.0)
         if contacts is not None:
-            contacts = np.ascontiguousarray(contacts, CONTACT_DTYPE)
+            contacts = as_contacts(contacts)
             nc = lib().pe_or_hcsits_step_contacts(C.byref(s), dt, model, max_iter, erp,
                                                   _ptr(contacts), contacts.shape[0],
                                                   C.byref(delta), C.byref(resid))

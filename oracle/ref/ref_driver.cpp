@@ -6,7 +6,8 @@
 //
 // Usage:
 //   ref_<solver> step  <scene> <steps> <out.bin> [model] [max_iter]
-//       runs <steps> World::simulationStep calls; writes x, v, w (3n doubles each), q (4n)
+//       runs <steps> World::simulationStep calls; writes x, v, w (3n doubles each), q (4n),
+//       then for the moving boxes x, v, w (3M each) and q (4M)
 //   ref_<solver> pairs <scene> <out.bin>
 //       runs pe's coarse+fine detection once and writes the contacts in pe's detection order:
 //       int64 count, then per contact b1, b2 (int64 user ids), gpos[3], normal[3], dist
@@ -14,7 +15,8 @@
 //       times <steps> steps after <warmup> untimed steps, prints one JSON line
 //
 // Body user ids: spheres 0..n-1 (created first, in order, so pe's system-id order is the index
-// order), planes n..n+P-1, boxes n+P..n+P+B-1.  Scene file layout: pe_b200/scenes.py.
+// order), planes n..n+P-1, fixed boxes n+P..n+P+B-1, moving boxes n+P+B..n+P+B+M-1.  Scene file
+// layout: pe_b200/scenes.py.
 #include <pe/core.h>
 
 #include <chrono>
@@ -39,6 +41,10 @@ struct SceneFile {
     uint32_t steps = 0;
     std::vector<double> mats, planes, boxes, x, v, w, r;
     std::vector<int32_t> plane_mat, box_mat, mat;
+    // scene version 2: moving boxes (created after the fixed boxes)
+    uint32_t nmb = 0;
+    std::vector<double> mb_x, mb_q, mb_v, mb_w, mb_len;
+    std::vector<int32_t> mb_mat;
 };
 
 template <typename T>
@@ -74,8 +80,19 @@ SceneFile load(const char* path) {
     s.w.resize(3 * s.n);                  rd(f, s.w.data(), s.w.size());
     s.r.resize(s.n);                      rd(f, s.r.data(), s.r.size());
     s.mat.resize(s.n);                    rd(f, s.mat.data(), s.mat.size());
+    if (ver >= 2) {
+        rd(f, &s.nmb, 1);
+        s.mb_x.resize(3 * s.nmb);         rd(f, s.mb_x.data(), s.mb_x.size());
+        s.mb_q.resize(4 * s.nmb);         rd(f, s.mb_q.data(), s.mb_q.size());
+        s.mb_v.resize(3 * s.nmb);         rd(f, s.mb_v.data(), s.mb_v.size());
+        s.mb_w.resize(3 * s.nmb);         rd(f, s.mb_w.data(), s.mb_w.size());
+        s.mb_len.resize(3 * s.nmb);       rd(f, s.mb_len.data(), s.mb_len.size());
+        s.mb_mat.resize(s.nmb);           rd(f, s.mb_mat.data(), s.mb_mat.size());
+    }
     return s;
 }
+
+std::vector<BoxID> g_mboxes;   // the moving boxes of the loaded scene, in scene order
 
 std::vector<SphereID> build_world(const SceneFile& s) {
     WorldID world = theWorld();
@@ -113,6 +130,16 @@ std::vector<SphereID> build_world(const SceneFile& s) {
                               Vec3(a[3], a[4], a[5]), mids[s.box_mat[b]]);
         box->setFixed(true);
     }
+    g_mboxes.clear();
+    for (uint32_t m = 0; m < s.nmb; ++m) {
+        const double *x = &s.mb_x[3 * m], *q = &s.mb_q[4 * m], *l = &s.mb_len[3 * m];
+        BoxID box = createBox(static_cast<pe::id_t>(s.n + s.nplanes + s.nboxes + m),
+                              Vec3(x[0], x[1], x[2]), Vec3(l[0], l[1], l[2]), mids[s.mb_mat[m]]);
+        box->setOrientation(Quat(q[0], q[1], q[2], q[3]));
+        box->setLinearVel(s.mb_v[3 * m], s.mb_v[3 * m + 1], s.mb_v[3 * m + 2]);
+        box->setAngularVel(s.mb_w[3 * m], s.mb_w[3 * m + 1], s.mb_w[3 * m + 2]);
+        g_mboxes.push_back(box);
+    }
     return spheres;
 }
 
@@ -137,6 +164,12 @@ void write_state(const char* path, const std::vector<SphereID>& sp) {
     for (size_t i = 0; i < sp.size(); ++i) { const Vec3& a = sp[i]->getLinearVel(); out.push_back(a[0]); out.push_back(a[1]); out.push_back(a[2]); }
     for (size_t i = 0; i < sp.size(); ++i) { const Vec3& a = sp[i]->getAngularVel(); out.push_back(a[0]); out.push_back(a[1]); out.push_back(a[2]); }
     for (size_t i = 0; i < sp.size(); ++i) { const Quat& q = sp[i]->getQuaternion(); for (int k = 0; k < 4; ++k) out.push_back(q[k]); }
+    // moving boxes: x, v, w (3 each per box), then q (4 per box)
+    const std::vector<BoxID>& mb = g_mboxes;
+    for (size_t i = 0; i < mb.size(); ++i) { const Vec3& a = mb[i]->getPosition(); out.push_back(a[0]); out.push_back(a[1]); out.push_back(a[2]); }
+    for (size_t i = 0; i < mb.size(); ++i) { const Vec3& a = mb[i]->getLinearVel(); out.push_back(a[0]); out.push_back(a[1]); out.push_back(a[2]); }
+    for (size_t i = 0; i < mb.size(); ++i) { const Vec3& a = mb[i]->getAngularVel(); out.push_back(a[0]); out.push_back(a[1]); out.push_back(a[2]); }
+    for (size_t i = 0; i < mb.size(); ++i) { const Quat& q = mb[i]->getQuaternion(); for (int k = 0; k < 4; ++k) out.push_back(q[k]); }
     f.write(reinterpret_cast<const char*>(out.data()),
             static_cast<std::streamsize>(out.size() * sizeof(double)));
 }

@@ -52,10 +52,21 @@ class Scene:
     steps: int
     name: str = ""
     damping: float = 1.0     # pe Settings::damping (1 = no drag)
+    # moving (non-fixed) boxes, created in pe after the fixed boxes
+    mbox_x: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 3)))
+    mbox_q: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 4)))  # w x y z
+    mbox_v: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 3)))
+    mbox_w: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 3)))
+    mbox_len: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 3)))
+    mbox_mat: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
 
     @property
     def n(self) -> int:
         return int(self.r.shape[0])
+
+    @property
+    def nmbox(self) -> int:
+        return int(self.mbox_len.shape[0])
 
     def copy(self) -> "Scene":
         return dataclasses.replace(self, **{f.name: (getattr(self, f.name).copy()
@@ -65,7 +76,10 @@ class Scene:
 
     # --- binary scene file (read by the compiled-reference driver and the C++ host layer) ---
     def to_bytes(self) -> bytes:
-        hdr = struct.pack("<8sIIQII3dddI", SCENE_MAGIC, SCENE_VERSION, self.materials.shape[0],
+        """Version 1 without moving boxes (the layout the compiled-reference driver reads);
+        version 2 appends uint32 M and the moving boxes' x, q, v, w, side lengths, materials."""
+        ver = SCENE_VERSION if self.nmbox == 0 else 2
+        hdr = struct.pack("<8sIIQII3dddI", SCENE_MAGIC, ver, self.materials.shape[0],
                           self.n, self.planes.shape[0], self.boxes.shape[0],
                           *[float(g) for g in self.gravity], float(self.dt),
                           float(self.damping), int(self.steps))
@@ -80,6 +94,14 @@ class Scene:
                  np.ascontiguousarray(self.w, "<f8").tobytes(),
                  np.ascontiguousarray(self.r, "<f8").tobytes(),
                  np.ascontiguousarray(self.mat, "<i4").tobytes()]
+        if ver == 2:
+            parts += [struct.pack("<I", self.nmbox),
+                      np.ascontiguousarray(self.mbox_x, "<f8").tobytes(),
+                      np.ascontiguousarray(self.mbox_q, "<f8").tobytes(),
+                      np.ascontiguousarray(self.mbox_v, "<f8").tobytes(),
+                      np.ascontiguousarray(self.mbox_w, "<f8").tobytes(),
+                      np.ascontiguousarray(self.mbox_len, "<f8").tobytes(),
+                      np.ascontiguousarray(self.mbox_mat, "<i4").tobytes()]
         return b"".join(parts)
 
     def save(self, path: str) -> None:
@@ -93,9 +115,15 @@ def scene_from_bytes(buf: bytes, name: str = "") -> Scene:
     if len(buf) < hs:
         raise ValueError("truncated scene file")
     magic, ver, nm, n, npl, nbx, gx, gy, gz, dt, damping, steps = struct.unpack_from(fmt, buf, 0)
-    if magic != SCENE_MAGIC or ver != SCENE_VERSION:
+    if magic != SCENE_MAGIC or ver not in (1, 2):
         raise ValueError("not a scene file")
-    if len(buf) != hs + 72 * nm + 36 * npl + 124 * nbx + 84 * n:
+    base = hs + 72 * nm + 36 * npl + 124 * nbx + 84 * n
+    nmb = 0
+    if ver == 2:
+        if len(buf) < base + 4:
+            raise ValueError("truncated scene file")
+        nmb, = struct.unpack_from("<I", buf, base)
+    if len(buf) != base + (4 + 132 * nmb if ver == 2 else 0):
         raise ValueError("scene file size does not match its header")
     off = hs
 
@@ -115,9 +143,18 @@ def scene_from_bytes(buf: bytes, name: str = "") -> Scene:
     w = take("<f8", n * 3, (n, 3))
     r = take("<f8", n, (n,))
     mat = take("<i4", n, (n,))
-    return Scene(x=x, v=v, w=w, r=r, mat=mat, planes=planes, plane_mat=plane_mat, boxes=boxes,
-                 box_mat=box_mat, materials=materials, gravity=np.array([gx, gy, gz]), dt=dt,
-                 steps=steps, name=name, damping=damping)
+    s = Scene(x=x, v=v, w=w, r=r, mat=mat, planes=planes, plane_mat=plane_mat, boxes=boxes,
+              box_mat=box_mat, materials=materials, gravity=np.array([gx, gy, gz]), dt=dt,
+              steps=steps, name=name, damping=damping)
+    if ver == 2:
+        off += 4
+        s.mbox_x = take("<f8", nmb * 3, (nmb, 3))
+        s.mbox_q = take("<f8", nmb * 4, (nmb, 4))
+        s.mbox_v = take("<f8", nmb * 3, (nmb, 3))
+        s.mbox_w = take("<f8", nmb * 3, (nmb, 3))
+        s.mbox_len = take("<f8", nmb * 3, (nmb, 3))
+        s.mbox_mat = take("<i4", nmb, (nmb,))
+    return s
 
 
 def load_scene(path: str) -> Scene:
@@ -365,6 +402,87 @@ def small_random(seed: int, n: int = 64, box: float = 4.0, overlap: float = 0.05
     s = _scene(x, v, r, mat, planes, np.arange(6) % 2, boxes, np.zeros(len(boxes)), mats, G,
                1e-4, 10, f"small_{seed}_{n}")
     s.w = rng.normal(0.0, spin, size=(n, 3))
+    return s
+
+
+def random_quaternions(rng, m: int) -> np.ndarray:
+    """m uniformly distributed unit quaternions (w, x, y, z)."""
+    q = rng.normal(size=(m, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    q[q[:, 0] < 0] *= -1.0
+    return q
+
+
+def small_rotations(rng, m: int, max_angle: float) -> np.ndarray:
+    """m unit quaternions (w, x, y, z) of rotations by U[0, max_angle] about random axes."""
+    ax = rng.normal(size=(m, 3))
+    ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+    ang = rng.uniform(0.0, max_angle, size=m)
+    return np.concatenate([np.cos(ang / 2)[:, None], np.sin(ang / 2)[:, None] * ax], axis=1)
+
+
+def tumbling_boxes(seed: int = 0, side: int = 3, max_angle: float = 0.3, mu: float = 0.3,
+                   spheres: bool = True) -> Scene:
+    """side^3 moving boxes (side lengths U[0.75, 0.95], tilted by up to max_angle about random
+    axes) on a unit lattice resting on a floor plane, a fixed box against one column, and one
+    sphere in every lattice corner between eight boxes; random velocities and spins, gravity.
+    Tilted neighbours overlap slightly, so the first steps have face/face, edge/edge,
+    box/plane, box/fixed-box and sphere/box contacts."""
+    rng = np.random.default_rng(seed)
+    nbox = side ** 3
+    idx = np.stack(np.meshgrid(np.arange(side), np.arange(side), np.arange(side),
+                               indexing="ij"), axis=-1).reshape(-1, 3)[:, ::-1].astype(float)
+    bx = idx + np.array([1.5, 1.5, 0.5]) + rng.uniform(-0.02, 0.02, size=(nbox, 3))
+    blen = rng.uniform(0.75, 0.95, size=(nbox, 3))
+    bq = small_rotations(rng, nbox, max_angle)
+    bv = rng.normal(0.0, 0.2, size=(nbox, 3))
+    bw = rng.normal(0.0, 0.5, size=(nbox, 3))
+    if spheres:
+        cidx = np.stack(np.meshgrid(np.arange(side - 1), np.arange(side - 1),
+                                    np.arange(side - 1), indexing="ij"),
+                        axis=-1).reshape(-1, 3)[:, ::-1].astype(float)
+        sx = cidx + np.array([2.0, 2.0, 1.0]) + rng.uniform(-0.02, 0.02, size=cidx.shape)
+    else:
+        sx = np.zeros((0, 3))
+    ns = sx.shape[0]
+    r = rng.uniform(0.3, 0.4, size=ns)
+    L = side + 3.0
+    planes = box_planes([0, 0, 0], [L, L, L + 4.0])
+    boxes = np.array([aabox([0.5, 1.5 + (side - 1) / 2.0, 1.0], [1.0 - 0.02, side, 2.0])])
+    mats = [material(1.0, 2e4, 20.0, 20.0, mu), material(0.5, 3e4, 10.0, 10.0, 0.5 * mu)]
+    s = _scene(sx, rng.normal(0.0, 0.2, size=(ns, 3)), r, rng.integers(0, 2, size=ns),
+               planes, np.arange(6) % 2, boxes, [1], mats, G, 1e-4, 20,
+               f"tumbling_boxes_{seed}_{nbox}")
+    s.w = rng.normal(0.0, 0.5, size=(ns, 3))
+    s.mbox_x, s.mbox_q, s.mbox_v, s.mbox_w = bx, bq, bv, bw
+    s.mbox_len = blen
+    s.mbox_mat = rng.integers(0, 2, size=nbox).astype(np.int32)
+    return s
+
+
+def box_stack(layers: int = 4, per_side: int = 3) -> Scene:
+    """pe's box-stack arrangement: layers of equal, axis-aligned cubes resting face to face on
+    a floor plane (the degenerate, fully aligned case of the box/box test), plus one sphere
+    flying into the stack."""
+    a = 1.0
+    pts = []
+    for z in range(layers):
+        for y in range(per_side):
+            for x in range(per_side):
+                pts.append([x * a, y * a, 0.5 * a + z * a - 1e-4 * (z + 1)])
+    bx = np.array(pts) + np.array([2.0, 2.0, 0.0])
+    nb = bx.shape[0]
+    planes = np.array([[0.0, 0.0, 1.0, 0.0]])
+    mats = [material(1.0, 1e5, 50.0, 50.0, 0.4)]
+    s = _scene(np.array([[2.0 + per_side * a / 2, -1.0, 1.5]]), np.array([[0.0, 3.0, 0.0]]),
+               np.array([0.4]), [0], planes, [0], np.zeros((0, 15)), [], mats, G, 1e-4, 20,
+               f"box_stack_{layers}x{per_side}")
+    s.mbox_x = bx
+    s.mbox_q = np.tile([1.0, 0.0, 0.0, 0.0], (nb, 1))
+    s.mbox_v = np.zeros((nb, 3))
+    s.mbox_w = np.zeros((nb, 3))
+    s.mbox_len = np.full((nb, 3), a)
+    s.mbox_mat = np.zeros(nb, np.int32)
     return s
 
 

@@ -121,6 +121,50 @@ def peb_fixture(steps=5):
     print(peb, os.path.getsize(peb), "bytes")
 
 
+def run_steps_boxes(exe, scene_path, n, nmb, steps, tmp, extra=()):
+    """Sphere and moving-box states after `steps` reference steps."""
+    out = os.path.join(tmp, "state.bin")
+    subprocess.run([os.path.join(REF, exe), "step", scene_path, str(steps), out,
+                    *[str(e) for e in extra]], check=True)
+    a = np.fromfile(out, "<f8")
+    sizes = [3 * n, 3 * n, 3 * n, 4 * n, 3 * nmb, 3 * nmb, 3 * nmb, 4 * nmb]
+    parts = np.split(a, np.cumsum(sizes)[:-1])
+    shapes = [(n, 3), (n, 3), (n, 3), (n, 4), (nmb, 3), (nmb, 3), (nmb, 3), (nmb, 4)]
+    return [p.reshape(sh) for p, sh in zip(parts, shapes)]
+
+
+def box_golden(name, scene, dem_steps=(1, 10), hc_converged_iters=20000):
+    """Moving-box scene: pe's contacts (detection order), DEM states, one HCSITS step per
+    relaxation model in pe's contact order, and a converged frictionless step."""
+    keys = ("x", "v", "w", "q", "bx", "bv", "bw", "bq")
+    with tempfile.TemporaryDirectory() as tmp:
+        sp = os.path.join(tmp, "scene.bin")
+        scene.save(sp)
+        rec = {"scene": np.frombuffer(scene.to_bytes(), np.uint8)}
+        rec["pairs"] = run_pairs("ref_dem", sp, tmp)
+        for k in dem_steps:
+            for key, a in zip(keys, run_steps_boxes("ref_dem", sp, scene.n, scene.nmbox, k, tmp)):
+                rec[f"dem{k}_{key}"] = a
+        rec["hc_pairs"] = run_pairs("ref_hcsits", sp, tmp)
+        for model in (0, 1, 2, 3, 4, 5):
+            st = run_steps_boxes("ref_hcsits", sp, scene.n, scene.nmbox, 1, tmp, (model, 100))
+            for key, a in zip(keys, st):
+                rec[f"hc{model}_{key}"] = a
+        st = run_steps_boxes("ref_hcsits", sp, scene.n, scene.nmbox, 1, tmp,
+                             (0, hc_converged_iters))
+        for key, a in zip(keys, st):
+            rec[f"hc0conv_{key}"] = a
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **rec)
+    print(path, os.path.getsize(path), "bytes,", len(rec["pairs"]), "contacts")
+
+
+def box_goldens():
+    box_golden("boxes27_tumbling", scenes.tumbling_boxes(0))
+    box_golden("boxes64_tilted", scenes.tumbling_boxes(2, side=4, spheres=False))
+    box_golden("boxes36_stack", scenes.box_stack())
+
+
 def hertz_goldens():
     golden("hertz64_boxes", hertz_scene(1, with_boxes=True), dem_steps=(1, 10), hc=False,
            dem_exe="ref_dem_hertz")
@@ -137,6 +181,9 @@ if __name__ == "__main__":
     if sys.argv[1:] == ["peb"]:
         peb_fixture()
         sys.exit(0)
+    if sys.argv[1:] == ["boxes"]:
+        box_goldens()
+        sys.exit(0)
     golden("small64_boxes", scenes.small_random(1, n=64, with_boxes=True))
     golden("small64_planes", scenes.small_random(2, n=64, with_boxes=False))
     golden("lattice512", scenes.dem_lattice(0, side=8), dem_steps=(1, 10, 100))
@@ -150,3 +197,4 @@ if __name__ == "__main__":
     adjoint_fd()
     hertz_goldens()
     peb_fixture()
+    box_goldens()

@@ -132,3 +132,63 @@ def test_hertz_dem_steps_match_reference(name):
     o = OracleWorld(g["scene"], force_model=0)
     o.dem_step(g["scene"].dt, 10)
     assert rel_err(o.v, g["dem10_v"]) > 1e-3
+
+
+# ---- moving boxes (box/box, box/plane, box/fixed-box and sphere/box contacts) ------------------
+BOX_GOLDENS = ["boxes27_tumbling", "boxes64_tilted", "boxes36_stack"]
+
+
+def contact_key(b1, b2, gpos, dist):
+    return sorted(zip(b1.tolist(), b2.tolist(), map(tuple, np.round(gpos, 12).tolist()),
+                      np.round(dist, 14).tolist()))
+
+
+@pytest.mark.parametrize("name", BOX_GOLDENS)
+def test_box_contacts_match_reference(name):
+    """Same contacts as pe's fine detection (MaxContacts.h:589-668, 867-2250, 2380-2528):
+    bodies in pe's orientation, contact points, normals and distances; several per box pair."""
+    g = load_golden(name)
+    c = OracleWorld(g["scene"]).contacts()
+    ref = g["pairs"]
+    assert len(c) == len(ref)
+    assert contact_key(c["b1"], c["b2"], c["gpos"], c["dist"]) == \
+        contact_key(ref["b1"], ref["b2"], ref["gpos"], ref["dist"])
+    # normals, matched through the (stable) canonical order of both lists
+    oi = np.lexsort((np.round(c["gpos"][:, 2], 12), np.round(c["gpos"][:, 1], 12),
+                     np.round(c["gpos"][:, 0], 12), c["b2"], c["b1"]))
+    ri = np.lexsort((np.round(ref["gpos"][:, 2], 12), np.round(ref["gpos"][:, 1], 12),
+                     np.round(ref["gpos"][:, 0], 12), ref["b2"], ref["b1"]))
+    assert rel_err(c["n"][oi], ref["n"][ri]) < 1e-15
+
+
+@pytest.mark.parametrize("name", BOX_GOLDENS)
+def test_box_dem_steps_match_reference(name):
+    """DEM with moving boxes (BoxTrait::move, boxtrait/Default.h:149-220), including pe's zero
+    stiffness at edge/edge contacts."""
+    g = load_golden(name)
+    s = g["scene"]
+    for k in (1, 10):
+        o = OracleWorld(s, track_orientation=True)
+        o.dem_step(s.dt, k)
+        assert rel_err(o.mb_x, g[f"dem{k}_bx"]) < 1e-14
+        assert rel_err(o.mb_v, g[f"dem{k}_bv"]) < 1e-13
+        assert rel_err(o.mb_w, g[f"dem{k}_bw"]) < 1e-13
+        assert rel_err(o.mb_q, g[f"dem{k}_bq"]) < 1e-14
+        if s.n:
+            assert rel_err(o.x, g[f"dem{k}_x"]) < 1e-14
+            assert rel_err(o.v, g[f"dem{k}_v"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", BOX_GOLDENS)
+@pytest.mark.parametrize("model", [0, 1, 2, 3, 4, 5])
+def test_box_hcsits_step_bit_exact_in_reference_order(name, model):
+    """Hard contacts with moving boxes (world-frame inverse inertia R I^-1 R^T in the Delassus
+    blocks and the impulse updates, gyroscopic term in the body cache) reproduce pe's step
+    exactly in pe's contact order."""
+    g = load_golden(name)
+    s = g["scene"]
+    o = OracleWorld(s, track_orientation=True)
+    o.hcsits_step(s.dt, model, 100, contacts=g["hc_pairs"])
+    for a, key in ((o.mb_x, "bx"), (o.mb_v, "bv"), (o.mb_w, "bw"), (o.mb_q, "bq"),
+                   (o.x, "x"), (o.v, "v"), (o.w, "w")):
+        assert np.array_equal(a, g[f"hc{model}_{key}"], equal_nan=True), key
