@@ -134,6 +134,26 @@ int pe_b200_upload_bodies(pe_b200_ctx *ctx, int64_t n, const double *x, const do
                           const double *w, const double *r, const int32_t *mat,
                           const int32_t *scene, int32_t nscenes);
 
+/* Moving (non-fixed) boxes, after pe_b200_upload_bodies (which removes them again): m boxes,
+ * centres x (3 each), orientations q (4 each, unit quaternion w x y z), linear and angular
+ * velocities v, w (3 each), side lengths (3 each, > 0), material ids, scene ids (NULL: scene 0;
+ * otherwise grouped by scene, non-decreasing).  FP64 contexts only (PE_B200_ERR_UNSUPPORTED
+ * otherwise).  In contact ids box k is n + (all planes) + (all fixed boxes) + k, as if created
+ * in pe after the fixed boxes.
+ * Replaces: createBox + setOrientation / setLinearVel / setAngularVel for a box that is not fixed
+ * (src/core/rigidbody/Box.cpp:1312-1330, 289-336).  The step then adds pe's box contacts
+ * (MaxContacts.h:589-668 sphere/box, 867-2250 box/box, 2380-2528 box/plane), BoxTrait::move
+ * (boxtrait/Default.h:149-220) for DEM and the box bodies of the hard-contact solver; the DEM
+ * step runs on the cell grid (no neighbour lists) while boxes are present. */
+int pe_b200_upload_boxes(pe_b200_ctx *ctx, int32_t m, const double *x, const double *q,
+                         const double *v, const double *w, const double *lengths,
+                         const int32_t *mat, const int32_t *scene);
+/* Current state of the moving boxes (any pointer may be NULL).  Replaces: Box::getPosition /
+ * getQuaternion / getLinearVel / getAngularVel. */
+int pe_b200_download_boxes(pe_b200_ctx *ctx, double *x, double *q, double *v, double *w);
+/* Number of moving boxes (-1 for a NULL context). */
+int32_t pe_b200_box_count(const pe_b200_ctx *ctx);
+
 /* Overwrites positions/velocities of the uploaded spheres (same order; any pointer may be NULL
  * to keep that field).  Replaces: RigidBody::setPosition / setLinearVel / setAngularVel. */
 int pe_b200_set_state(pe_b200_ctx *ctx, const double *x, const double *v, const double *w);

@@ -33,7 +33,8 @@ EXPORTS = ["pe_b200_default_params", "pe_b200_create", "pe_b200_destroy", "pe_b2
            "pe_b200_profile", "pe_b200_dem_step_static", "pe_b200_neighbor_list_stats",
            "pe_b200_adjoint_forward", "pe_b200_adjoint_backward", "pe_b200_set_graph_steps",
            "pe_b200_graph_active", "pe_b200_get_tuning", "pe_b200_set_tuning",
-           "pe_b200_autotune", "pe_b200_validate", "pe_b200_selftest_timeout"]
+           "pe_b200_autotune", "pe_b200_validate", "pe_b200_selftest_timeout",
+           "pe_b200_upload_boxes", "pe_b200_download_boxes", "pe_b200_box_count"]
 
 STATIC_MAX_SPHERES = 32768
 STATIC_MAX_CELLS = 131072
@@ -106,6 +107,9 @@ def load() -> C.CDLL:
         "pe_b200_set_tuning": (C.c_int, [vp, P(Tuning)]),
         "pe_b200_autotune": (C.c_int, [vp, dp, i32, P(Tuning)]),
         "pe_b200_validate": (C.c_int, [vp, P(i64)]),
+        "pe_b200_upload_boxes": (C.c_int, [vp, i32, vp, vp, vp, vp, vp, vp, vp]),
+        "pe_b200_download_boxes": (C.c_int, [vp, vp, vp, vp, vp]),
+        "pe_b200_box_count": (i32, [vp]),
         "pe_b200_selftest_timeout": (C.c_int, [vp, i64]),
         "pe_b200_profile": (C.c_int, [vp, i32, P(C.c_char_p), P(dp), P(i64), P(i32)]),
         "pe_b200_stream": (vp, [vp]),

@@ -19,6 +19,9 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fopenmp", "--expt-relaxed-constexpr",
               "-I" + INCLUDE]
+# per-file flags: the box fine detection rounds every product and sum separately, as pe's FP64
+# code does (its case selection compares depths that tie for aligned boxes)
+FILE_FLAGS = {"boxes.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -60,7 +63,8 @@ def build(force: bool = False, verbose: bool = False, extra_flags=(), out: str =
 
     def compile_one(src):
         obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [cc, *ARCH, *NVCC_FLAGS, *extra_flags, "-c", src, "-o", obj]
+        cmd = [cc, *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), *extra_flags,
+               "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr}")

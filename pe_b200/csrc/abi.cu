@@ -1,5 +1,7 @@
 // abi.cu -- the extern "C" entry points of libpe_b200.so (declared in include/pe_b200.h).
 #include <nvtx3/nvToolsExt.h>
+
+#include <cmath>
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -120,6 +122,7 @@ void free_device(Ctx *c) {
     nbgs_free(c);
     dem_list_free(c);
     adjoint_free(c);
+    mbox_free(c);
     stage_free(c);
     c->uploaded = false;
     c->binned = false;
@@ -351,6 +354,14 @@ namespace peb {
 
 int run_steps(Ctx *c, int32_t nsteps, double dt) {
     int32_t k = 0;
+    if (c->p.solver == PE_B200_DEM && c->mb.m > 0) {
+        // moving boxes: the grid step (the neighbour lists and graphs cover spheres only)
+        for (; k < nsteps; ++k) {
+            const int rc = dem_step(c, dt);
+            if (rc) return rc;
+        }
+        return PE_B200_OK;
+    }
     if (c->p.solver == PE_B200_DEM && c->nl.enabled && !c->prof) {
         int rc = dem_list_graph_run(c, nsteps, dt, &k);
         if (rc) return rc;
@@ -630,6 +641,53 @@ int pe_b200_upload_bodies(pe_b200_ctx *h, int64_t n, const double *x, const doub
     return PE_B200_OK;
 }
 
+static int check_device_errors(Ctx *c);
+
+int pe_b200_upload_boxes(pe_b200_ctx *h, int32_t m, const double *x, const double *q,
+                         const double *v, const double *w, const double *lengths,
+                         const int32_t *mat, const int32_t *scene) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || m < 0 || m > (1 << 24)) return PE_B200_ERR_ARG;
+    if (m > 0 && (!x || !q || !v || !w || !lengths || !mat)) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "spheres must be uploaded before boxes");
+    if (m > 0 && c->p.precision != PE_B200_FP64)
+        return set_err(c, PE_B200_ERR_UNSUPPORTED, "moving boxes need FP64 precision");
+    const int64_t nmat = (int64_t)c->mats.size();
+    for (int32_t k = 0; k < m; ++k) {
+        // createBox: side lengths must be positive (src/core/rigidbody/Box.cpp:1316-1319)
+        if (!(lengths[3 * k] > 0.0) || !(lengths[3 * k + 1] > 0.0) || !(lengths[3 * k + 2] > 0.0))
+            return set_err(c, PE_B200_ERR_ARG, "Invalid side length");
+        if (mat[k] < 0 || mat[k] >= nmat) return set_err(c, PE_B200_ERR_ARG, "Invalid material ID");
+        if (scene && (scene[k] < 0 || scene[k] >= c->nscenes || (k > 0 && scene[k] < scene[k - 1])))
+            return set_err(c, PE_B200_ERR_ARG, "Invalid scene ID (boxes must be grouped by scene)");
+        bool ok = true;
+        for (int a = 0; a < 3; ++a)
+            ok = ok && std::isfinite(x[3 * k + a]) && std::isfinite(v[3 * k + a]) &&
+                 std::isfinite(w[3 * k + a]);
+        const double *qq = q + 4 * k;
+        const double qn = qq[0] * qq[0] + qq[1] * qq[1] + qq[2] * qq[2] + qq[3] * qq[3];
+        // Quaternion(r, i, j, k) wants a unit quaternion (Quaternion.h:251-255)
+        if (!ok || !(std::fabs(qn - 1.0) < 1e-8)) return set_err(c, PE_B200_ERR_ARG, "Invalid box state");
+    }
+    cudaSetDevice(c->device);
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return mbox_upload(c, m, x, q, v, w, lengths, mat, scene);
+}
+
+int pe_b200_download_boxes(pe_b200_ctx *h, double *x, double *q, double *v, double *w) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c) return PE_B200_ERR_ARG;
+    cudaSetDevice(c->device);
+    const int rc = mbox_download(c, x, q, v, w);
+    if (rc) return rc;
+    return check_device_errors(c);
+}
+
+int32_t pe_b200_box_count(const pe_b200_ctx *h) {
+    const Ctx *c = reinterpret_cast<const Ctx *>(h);
+    return c ? c->mb.m : -1;
+}
+
 int pe_b200_set_state(pe_b200_ctx *h, const double *x, const double *v, const double *w) {
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c) return PE_B200_ERR_ARG;
@@ -701,6 +759,8 @@ int pe_b200_autotune(pe_b200_ctx *h, double dt, int32_t trial_steps, pe_b200_tun
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c) return PE_B200_ERR_ARG;
     if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    if (c->mb.m > 0)
+        return set_err(c, PE_B200_ERR_UNSUPPORTED, "the tuner covers sphere scenes only");
     cudaSetDevice(c->device);
     return autotune(c, dt, trial_steps, out);
 }
@@ -758,6 +818,8 @@ int pe_b200_adjoint_forward(pe_b200_ctx *h, int32_t nsteps, double dt, int32_t e
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c) return PE_B200_ERR_ARG;
     if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    if (c->mb.m > 0)
+        return set_err(c, PE_B200_ERR_UNSUPPORTED, "the adjoint step covers sphere scenes only");
     cudaSetDevice(c->device);
     return adjoint_forward(c, nsteps, dt, every);
 }

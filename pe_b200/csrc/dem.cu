@@ -144,6 +144,7 @@ struct DemArgs {
     int32_t *nl_flags;
     float half_skin;
     int hertz;        // extended Hertz law for sphere pairs (force_model 1)
+    const double *ext = nullptr;   // moving boxes: their force and torque on body b (6 per body)
 };
 
 // one sphere pair (this body and neighbour j), both in the buffers of `a`; self1: this body is
@@ -393,6 +394,11 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     acc.T_ = acc.F;
     grid_forces<T, VT, HERTZ>(a, s, b, pi, vi, wi, uidi, mi, acc);
     wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
+    if (a.ext) {
+        const double *e = a.ext + 6 * (int64_t)b;
+        acc.F = acc.F + v3(T(e[0]), T(e[1]), T(e[2]));
+        acc.T_ = acc.T_ + v3(T(e[3]), T(e[4]), T(e[5]));
+    }
     V3<T> v;
     const double4 o = integrate<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v);
     a.tag_out[t] = tagi;
@@ -511,6 +517,7 @@ DemArgs<VT> dem_args(Ctx *c, double dt) {
     a.nl_flags = c->nl.flags;
     a.half_skin = float(0.5 * c->nl.skin * (1.0 - 1e-5));
     a.hertz = c->p.force_model == 1 ? 1 : 0;
+    a.ext = c->mb.m > 0 ? c->mb.ext : nullptr;
     return a;
 }
 
@@ -757,17 +764,24 @@ __global__ void k_set_one(int32_t *p) { *p = 1; }
 }  // namespace
 
 int dem_step(Ctx *c, double dt) {
-    if (!c->binned) {
-        int rc = grid_bin_current(c);
+    int rc;
+    if (c->n > 0) {
+        if (!c->binned) {
+            rc = grid_bin_current(c);
+            if (rc) return rc;
+        }
+        rc = grid_sort(c);
         if (rc) return rc;
     }
-    int rc = grid_sort(c);
+    // moving boxes: their forces on the spheres and their own step, from the current state
+    rc = mbox_dem(c, dt);
     if (rc) return rc;
     if (c->n > 0) {
         rc = (c->p.precision == PE_B200_FP64) ? launch_dem<double>(c, dt) : launch_dem<float>(c, dt);
         if (rc) return rc;
         std::swap(c->cur, c->nxt);
     }
+    if (c->mb.m > 0) mbox_swap(c);
     return PE_B200_OK;
 }
 
@@ -1018,6 +1032,7 @@ cudaError_t dem_launch_fp64_raw(const DemRawArgs &r, cudaStream_t stream) {
     a.nl_flags = nullptr;
     a.half_skin = 0.f;
     a.hertz = 0;
+    a.ext = nullptr;
     if (r.n > 0)
         k_dem_step<double, false, false><<<grid_for(r.n, kDemBlock), kDemBlock, 0, stream>>>(a);
     return cudaGetLastError();

@@ -40,6 +40,7 @@ struct SceneInfo {
     // (axis-aligned planes only; a scene with another plane has an empty box)
     double wall_lo[3], wall_hi[3];
     double rmax;                   // largest sphere radius of the scene at upload
+    int32_t mbox_begin, nmbox;     // the scene's moving boxes (boxes.cu)
 };
 
 // per-material constants; reciprocals so a composed value is one division (Materials.h:633)
@@ -76,8 +77,25 @@ struct NbgsBuf {
     bool coop_disabled = false;
     int cluster = -1;               // CTAs of the one-cluster sweep kernel (0: not available)
     void *vel = nullptr;                      // v', w', dv, dw per body (VT[12])
+    int64_t nbod = 0;                         // bodies the per-body buffers hold
+    bool gen = false;                         // they hold world-frame inverse inertias too
     double *red = nullptr;                    // reduction scratch
     int64_t red_cap = 0;
+};
+
+// Moving (non-fixed) boxes, FP64 (boxes.cu).  State arrays per box: x (3), q (4: w x y z),
+// v (3), w (3), current and next step; props: 1/m, the body-frame inverse inertia diagonal (3),
+// the body-frame inertia diagonal (3), unused (BoxBase.cpp:152-158, BoxBase.h:186-189).
+struct MBoxBuf {
+    int32_t m = 0;
+    double *x = nullptr, *q = nullptr, *v = nullptr, *w = nullptr;
+    double *x2 = nullptr, *q2 = nullptr, *v2 = nullptr, *w2 = nullptr;
+    double *len = nullptr;     // side lengths, 3 per box
+    double *props = nullptr;   // 8 per box
+    int32_t *mat = nullptr, *scene = nullptr;
+    int32_t *cnt = nullptr;    // contacts per box / offsets (m + 2)
+    double *ext = nullptr;     // DEM: force and torque of the boxes on each sphere (6 per body)
+    int64_t ext_cap = 0;
 };
 
 // Verlet neighbour lists of the DEM step (dem_list.cu): every pair closer than r_i + r_j + skin
@@ -189,6 +207,7 @@ struct Ctx {
 
     NbgsBuf nb;
     ListBuf nl;
+    MBoxBuf mb;
     AdjState adj;
     Tuning tune;
     StepGraph sg;
@@ -309,6 +328,28 @@ int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *g
 void adjoint_free(Ctx *c);
 int nbgs_step(Ctx *c, double dt);
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out);
+// boxes.cu: moving boxes
+int mbox_upload(Ctx *c, int32_t m, const double *x, const double *q, const double *v,
+                const double *w, const double *len, const int32_t *mat, const int32_t *scene);
+int mbox_download(Ctx *c, double *x, double *q, double *v, double *w);
+void mbox_free(Ctx *c);
+// DEM: the boxes' forces on the spheres (mb.ext, by body index of the current buffers) and
+// the boxes' own step into the next box buffers; the caller swaps them after the sphere step
+int mbox_dem(Ctx *c, double dt);
+void mbox_swap(Ctx *c);
+// HCSITS (bodies n .. n+m-1 after the spheres): body cache, contacts (count, then write after
+// the sphere contacts), integration
+struct BodyCacheD {   // the FP64 body cache of the hard-contact step (slot order)
+    double4 *vr, *wr, *dv, *dw, *ia, *ib, *ic;
+};
+int mbox_hc_bodycache(Ctx *c, const BodyCacheD &bv, double dt);
+int mbox_hc_count(Ctx *c, int32_t *total);
+int mbox_hc_raw(Ctx *c, int64_t base, int64_t cap, int32_t *b1, int32_t *b2, double *r1,
+                double *r2, double *nrm, double *dist, double *mu);
+int mbox_hc_integrate(Ctx *c, const BodyCacheD &bv, double dt);
+// contacts involving moving boxes for pe_b200_find_contacts, in pe's orientation and ids
+int mbox_find_contacts(Ctx *c, std::vector<int64_t> &ids, std::vector<double> &geom);
+
 // body slots of the contacts of the last HCSITS step, in colour order (device memory)
 const int2 *nbgs_ids_ptr(Ctx *c);
 // validate.cu: host checks of the device state; each adds the problems it finds to *bad

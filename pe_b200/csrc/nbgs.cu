@@ -17,6 +17,7 @@
 // Colour order replaces pe's detection order; only converged frictionless velocities are
 // order-independent, which is what the parity tests compare.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -28,6 +29,7 @@ namespace peb {
 namespace {
 
 constexpr int kBlk = 256;
+constexpr int kMaxColors = 256;   // colours of one step (8 bits in the packed colour)
 
 struct CountF {
     int n = 0;
@@ -151,7 +153,44 @@ struct BodyV {
     T4<T> *wr;    // w, 1/I
     T4<T> *dv;    // dv, -
     T4<T> *dw;    // dw, -
+    // scenes with moving boxes: the rows of every body's world-frame inverse inertia
+    // R I^-1 R^T (RigidBody.h:866-869; a sphere's is 1/I on the diagonal), else null
+    T4<T> *ia = nullptr, *ib = nullptr, *ic = nullptr;
 };
+
+// a body's inverse inertia applied to a vector: the scalar of a sphere, or (GEN) the full
+// world-frame matrix of any body
+template <typename T, bool GEN>
+struct InvI;
+template <typename T>
+struct InvI<T, false> {
+    T s;
+    __device__ __forceinline__ V3<T> operator()(V3<T> a) const { return s * a; }
+};
+template <typename T>
+struct InvI<T, true> {
+    T4<T> a, b, c;
+    __device__ __forceinline__ V3<T> operator()(V3<T> v) const {
+        return v3(a.x * v.x + a.y * v.y + a.z * v.z, b.x * v.x + b.y * v.y + b.z * v.z,
+                  c.x * v.x + c.y * v.y + c.z * v.z);
+    }
+};
+template <typename T, bool GEN>
+__device__ __forceinline__ InvI<T, GEN> load_invi(const BodyV<T> &bv, int32_t b, T ii) {
+    if constexpr (GEN) {
+        InvI<T, true> r;
+        if (b >= 0) {
+            r.a = bv.ia[b];
+            r.b = bv.ib[b];
+            r.c = bv.ic[b];
+        } else {
+            r.a = r.b = r.c = mk4<T>(T(0), T(0), T(0), T(0));
+        }
+        return r;
+    } else {
+        return InvI<T, false>{ii};
+    }
+}
 
 template <typename T>
 __device__ __forceinline__ V3<T> ld3c(const T *a, int64_t i, int64_t s) {
@@ -189,6 +228,11 @@ __global__ void k_permute_cache(int64_t n, const int32_t *sorted, const double4 
     bv.wr[t] = mk4<VT>(wp.x, wp.y, wp.z, VT(ii));
     bv.dv[t] = mk4<VT>(VT(0), VT(0), VT(0), VT(0));
     bv.dw[t] = mk4<VT>(VT(0), VT(0), VT(0), VT(0));
+    if (bv.ia) {
+        bv.ia[t] = mk4<VT>(VT(ii), VT(0), VT(0), VT(0));
+        bv.ib[t] = mk4<VT>(VT(0), VT(ii), VT(0), VT(0));
+        bv.ic[t] = mk4<VT>(VT(0), VT(0), VT(ii), VT(0));
+    }
 }
 
 template <typename T>
@@ -304,7 +348,10 @@ __device__ __forceinline__ bool beats(uint32_t c, uint32_t e) {
 }
 
 // one Jones-Plassmann round: an uncoloured contact whose priority beats every uncoloured
-// neighbour (contacts sharing a dynamic body) takes the smallest colour free at both bodies
+// neighbour (contacts sharing a dynamic body) takes the smallest colour free at both bodies;
+// W 64-bit words of used colours per body (64 W colours: 64 for spheres, whose contacts are
+// few, 256 for scenes with boxes, where a box in a stack has dozens of contact points)
+template <int W>
 __global__ void k_color_round(int64_t nc, int round, const int32_t *b1, const int32_t *b2,
                               const int32_t *adj_start, const int32_t *adj, int32_t *color,
                               uint64_t *used, int32_t *remaining, int32_t *err) {
@@ -326,16 +373,22 @@ __global__ void k_color_round(int64_t nc, int round, const int32_t *b1, const in
             }
         }
     }
-    const uint64_t u = used[bodies[0]] | (bodies[1] >= 0 ? used[bodies[1]] : 0ull);
-    const int col = __ffsll((long long)~u) - 1;
+    int col = -1;
+#pragma unroll
+    for (int wd = 0; wd < W && col < 0; ++wd) {
+        const uint64_t u = used[(int64_t)bodies[0] * W + wd] |
+                           (bodies[1] >= 0 ? used[(int64_t)bodies[1] * W + wd] : 0ull);
+        const int f = __ffsll((long long)~u) - 1;
+        if (f >= 0) col = 64 * wd + f;
+    }
     if (col < 0) {
         atomicOr(err, DERR_COLORS);
         return;
     }
     // colour and round packed: low 8 bits colour, upper bits the round it was chosen in
     color[c] = (round << 8) | col;
-    used[bodies[0]] |= (1ull << col);
-    if (bodies[1] >= 0) used[bodies[1]] |= (1ull << col);
+    used[(int64_t)bodies[0] * W + (col >> 6)] |= (1ull << (col & 63));
+    if (bodies[1] >= 0) used[(int64_t)bodies[1] * W + (col >> 6)] |= (1ull << (col & 63));
 }
 
 __global__ void k_color_hist(int64_t nc, int32_t *color, int32_t *hist, int32_t *ncolors) {
@@ -354,7 +407,7 @@ __global__ void k_color_pos(int64_t nc, const int32_t *color, int32_t *fill, int
 }
 
 // ---- contact cache (HCSITS.h:1767-1815) --------------------------------------------------------
-template <typename T>
+template <typename T, bool GEN>
 __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos, BodyV<T> bv,
                         int64_t nb, Cache<T> cc) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -377,16 +430,40 @@ __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos,
     // D = -(r1^x I1^-1 r1^x + r2^x I2^-1 r2^x) + (1/m1 + 1/m2) 1 with scalar sphere inertia:
     // -r^x r^x = |r|^2 1 - r r^T
     T D[9];
-    const T a1 = dot(r1, r1), a2 = dot(r2, r2);
-    const T rr1[3] = {r1.x, r1.y, r1.z}, rr2[3] = {r2.x, r2.y, r2.z};
+    if constexpr (GEN) {
+        // -(r1^x I1 r1^x + r2^x I2 r2^x) + (1/m1 + 1/m2) 1 with the full world-frame inverse
+        // inertias, in pe's operation order (Matrix3x3.h:2355-2365, 2419-2432; HCSITS.h:1802)
+        T A[9], B[9];
+        const InvI<T, true> I1 = load_invi<T, true>(bv, b1, ii1), I2 = load_invi<T, true>(bv, b2, ii2);
+        auto rmr = [](const InvI<T, true> &I, V3<T> r, T *out) {
+            const T m[9] = {I.a.x, I.a.y, I.a.z, I.b.x, I.b.y, I.b.z, I.c.x, I.c.y, I.c.z};
+            T x[9];   // r^x * M
+            x[0] = r.y * m[6] - r.z * m[3]; x[1] = r.y * m[7] - r.z * m[4]; x[2] = r.y * m[8] - r.z * m[5];
+            x[3] = r.z * m[0] - r.x * m[6]; x[4] = r.z * m[1] - r.x * m[7]; x[5] = r.z * m[2] - r.x * m[8];
+            x[6] = r.x * m[3] - r.y * m[0]; x[7] = r.x * m[4] - r.y * m[1]; x[8] = r.x * m[5] - r.y * m[2];
+            // (r^x M) * r^x
+            out[0] = x[1] * r.z - x[2] * r.y; out[1] = x[2] * r.x - x[0] * r.z; out[2] = x[0] * r.y - x[1] * r.x;
+            out[3] = x[4] * r.z - x[5] * r.y; out[4] = x[5] * r.x - x[3] * r.z; out[5] = x[3] * r.y - x[4] * r.x;
+            out[6] = x[7] * r.z - x[8] * r.y; out[7] = x[8] * r.x - x[6] * r.z; out[8] = x[6] * r.y - x[7] * r.x;
+        };
+        rmr(I1, r1, A);
+        rmr(I2, r2, B);
+        const T ims = im1 + im2;
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 9; ++k) D[k] = -(A[k] + B[k]);
+        D[0] += ims; D[4] += ims; D[8] += ims;
+    } else {
+        const T a1 = dot(r1, r1), a2 = dot(r2, r2);
+        const T rr1[3] = {r1.x, r1.y, r1.z}, rr2[3] = {r2.x, r2.y, r2.z};
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const T d1 = (i == j ? a1 : T(0)) - rr1[i] * rr1[j];
-            const T d2 = (i == j ? a2 : T(0)) - rr2[i] * rr2[j];
-            D[3 * i + j] = ii1 * d1 + ii2 * d2 + (i == j ? im1 + im2 : T(0));
-        }
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const T d1 = (i == j ? a1 : T(0)) - rr1[i] * rr1[j];
+                const T d2 = (i == j ? a2 : T(0)) - rr2[i] * rr2[j];
+                D[3 * i + j] = ii1 * d1 + ii2 * d2 + (i == j ? im1 + im2 : T(0));
+            }
+    }
     // rotate into the contact frame: Dc = C^T D C with C = [n t o]
     const V3<T> C[3] = {n, t, o};
     T Dc[3][3];
@@ -600,7 +677,7 @@ __device__ __forceinline__ V3<T> solve_gmd(V3<T> pcf, const V3<T> &g, const T D[
 
 // one contact of one sweep of relaxation model MODEL (pe's RelaxationModel, HCSITS.h:172-179);
 // COHERENT: read the velocity corrections and the impulse from L2
-template <typename T, int MODEL, bool COHERENT>
+template <typename T, int MODEL, bool COHERENT, bool GEN = false>
 __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T> &cc,
                                               const BodyV<T> &bv, int track_delta,
                                               unsigned long long *delta) {
@@ -629,6 +706,7 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
         v2 = xyz<T>(vr2);
         w2 = xyz<T>(wr2);
     }
+    const InvI<T, GEN> I1 = load_invi<T, GEN>(bv, b1, ii1), I2 = load_invi<T, GEN>(bv, b2, ii2);
     V3<T> t, o;
     V3<T> pold;
     T4<T> q3, q4;
@@ -643,10 +721,10 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     }
     // remove this contact's impulse (HCSITS.h:2050-2053)
     dv1 = dv1 - im1 * pold;
-    dw1 = dw1 - ii1 * cross(r1, pold);
+    dw1 = dw1 - I1(cross(r1, pold));
     if (b2 >= 0) {
         dv2 = dv2 + im2 * pold;
-        dw2 = dw2 + ii2 * cross(r2, pold);
+        dw2 = dw2 + I2(cross(r2, pold));
     }
     const V3<T> gdot = ((v1 + dv1) - (v2 + dv2) + cross(w1 + dw1, r1)) - cross(w2 + dw2, r2);
     T gn = dot(n, gdot) + dist * dtinv;
@@ -671,14 +749,14 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
                 if (fsq > flimit * flimit || pcf.x < T(0)) {
                     // decoupled relaxation (HCSITS.h:2187-2228)
                     V3<T> ptmp = t * pc.y + o * pc.z;
-                    const V3<T> e1 = cross(ii1 * cross(r1, ptmp), r1);
-                    const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
+                    const V3<T> e1 = cross(I1(cross(r1, ptmp)), r1);
+                    const V3<T> e2 = (b2 >= 0) ? cross(I2(cross(r2, ptmp)), r2) : v3(T(0), T(0), T(0));
                     const T gdot_n = gn + dot(n, e1 + e2);
                     pcf.x = -(dn_inv * gdot_n);
                     pcf.x = pcf.x > T(0) ? pcf.x : T(0);
                     ptmp = n * pcf.x;
-                    const V3<T> f1 = cross(ii1 * cross(r1, ptmp), r1);
-                    const V3<T> f2 = (b2 >= 0) ? cross(ii2 * cross(r2, ptmp), r2) : v3(T(0), T(0), T(0));
+                    const V3<T> f1 = cross(I1(cross(r1, ptmp)), r1);
+                    const V3<T> f2 = (b2 >= 0) ? cross(I2(cross(r2, ptmp)), r2) : v3(T(0), T(0), T(0));
                     const V3<T> gdot2 = (gdot + f1) + f2;
                     const T g2t = dot(t, gdot2), g2o = dot(o, gdot2);
                     const T ttt = q4.w, tto = q6.z, too = q6.w;
@@ -713,8 +791,8 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
             if (fsq > flimit * flimit || pcf.x < T(0)) {
                 if (MODEL == 3) {
                     auto corr = [&](const V3<T> &pp) {
-                        const V3<T> e1 = cross(ii1 * cross(r1, pp), r1);
-                        const V3<T> e2 = (b2 >= 0) ? cross(ii2 * cross(r2, pp), r2) : v3(T(0), T(0), T(0));
+                        const V3<T> e1 = cross(I1(cross(r1, pp)), r1);
+                        const V3<T> e2 = (b2 >= 0) ? cross(I2(cross(r2, pp)), r2) : v3(T(0), T(0), T(0));
                         return e1 + e2;
                     };
                     pcf = solve_coulomb_decoupling<T>(pcf, gdot, n, t, o, dist * dtinv, dn_inv, q4.w,
@@ -728,10 +806,10 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     }
     if (apply) {
         dv1 = dv1 + im1 * pnew;
-        dw1 = dw1 + ii1 * cross(r1, pnew);
+        dw1 = dw1 + I1(cross(r1, pnew));
         if (b2 >= 0) {
             dv2 = dv2 - im2 * pnew;
-            dw2 = dw2 - ii2 * cross(r2, pnew);
+            dw2 = dw2 - I2(cross(r2, pnew));
         }
     }
     cc.p[k] = mk4<T>(pcf.x, pcf.y, pcf.z, T(0));
@@ -748,18 +826,18 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     }
 }
 
-template <typename T, int MODEL>
+template <typename T, int MODEL, bool GEN = false>
 __global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int64_t cap, T dtinv,
                                                 Cache<T> cc, BodyV<T> bv, int64_t nb,
                                                 int track_delta, unsigned long long *delta) {
     const int64_t k = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= end) return;
-    sweep_contact<T, MODEL, false>(k, dtinv, cc, bv, track_delta, delta);
+    sweep_contact<T, MODEL, false, GEN>(k, dtinv, cc, bv, track_delta, delta);
 }
 
 // All sweeps of a step in one cooperative launch: colour after colour, separated by bounded
 // grid barriers (each colour is conflict-free, so its contacts run in parallel).
-template <typename T, int MODEL>
+template <typename T, int MODEL, bool GEN = false>
 __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolors,
                                                             const int32_t *color_start,
                                                             int64_t cap, T dtinv, Cache<T> cc,
@@ -775,7 +853,7 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
         for (int col = 0; col < ncolors; ++col) {
             const int64_t e = color_start[col + 1];
             for (int64_t k = color_start[col] + g0; k < e; k += stride)
-                sweep_contact<T, MODEL, true>(k, dtinv, cc, bv, track, delta);
+                sweep_contact<T, MODEL, true, GEN>(k, dtinv, cc, bv, track, delta);
             if (!grid_sync_counted(bar, episode, err)) return;
         }
     }
@@ -915,15 +993,39 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         PEB_CUDA(c, cudaMalloc(&b.body_adj, (size_t)2 * cap * sizeof(int32_t)));
         b.cap = cap;
     }
+    // per-body buffers: spheres, then moving boxes (with inverse inertia rows, GEN)
+    const bool gen = c->mb.m > 0;
+    const int64_t nbod = n + c->mb.m;
+    if (b.cnt && (b.nbod != nbod || b.gen != gen)) {
+        cudaFree(b.cnt);
+        cudaFree(b.body_cnt);
+        cudaFree(b.used);
+        cudaFree(b.vel);
+        b.cnt = b.body_cnt = nullptr;
+        b.used = nullptr;
+        b.vel = nullptr;
+        cudaFree(b.flags);
+        cudaFree(b.red);
+        cudaFree(b.cstart_dev);
+        cudaFree(b.bar);
+        if (b.color_start) cudaFreeHost(b.color_start);
+        b.flags = nullptr;
+        b.red = nullptr;
+        b.cstart_dev = nullptr;
+        b.bar = nullptr;
+        b.color_start = nullptr;
+    }
     if (!b.cnt) {
-        PEB_CUDA(c, cudaMalloc(&b.cnt, ((size_t)n + 2) * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.body_cnt, ((size_t)n + 2) * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.used, (size_t)n * sizeof(uint64_t)));
-        PEB_CUDA(c, cudaMalloc(&b.vel, (size_t)n * 16 * es));
-        PEB_CUDA(c, cudaMalloc(&b.flags, 256 * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMallocHost(&b.color_start, 260 * sizeof(int32_t)));
+        b.nbod = nbod;
+        b.gen = gen;
+        PEB_CUDA(c, cudaMalloc(&b.cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.body_cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.used, (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t)));
+        PEB_CUDA(c, cudaMalloc(&b.vel, (size_t)nbod * (gen ? 28 : 16) * es));
+        PEB_CUDA(c, cudaMalloc(&b.flags, 2 * kMaxColors * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMallocHost(&b.color_start, (2 * kMaxColors + 8) * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.red, 4 * sizeof(double)));
-        PEB_CUDA(c, cudaMalloc(&b.cstart_dev, 130 * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMalloc(&b.cstart_dev, (kMaxColors + 2) * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.bar, 2 * sizeof(unsigned int)));
         PEB_CUDA(c, cudaMemset(b.bar, 0, 2 * sizeof(unsigned int)));
     }
@@ -951,12 +1053,19 @@ void layout(Ctx *c, Raw<T> &raw, Cache<T> &cc, BodyV<T> &bv) {
     cc.rec = (T4<T> *)take(kRec * cap * sizeof(T4<T>));
     cc.p = (T4<T> *)take(cap * sizeof(T4<T>));
     cc.dc = (T4<T> *)take(2 * cap * sizeof(T4<T>));
-    const int64_t n = std::max<int64_t>(c->n, 1);
+    const int64_t n = b.nbod;
     T4<T> *v = (T4<T> *)b.vel;
     bv.vr = v;
     bv.wr = v + n;
     bv.dv = v + 2 * n;
     bv.dw = v + 3 * n;
+    if (b.gen) {
+        bv.ia = v + 4 * n;
+        bv.ib = v + 5 * n;
+        bv.ic = v + 6 * n;
+    } else {
+        bv.ia = bv.ib = bv.ic = nullptr;
+    }
 }
 
 // the sweep kernels of relaxation model m (pe's RelaxationModel 0-5)
@@ -971,27 +1080,42 @@ auto cluster_kernel(int m) -> decltype(&k_sweeps_cluster<VT, 0>) {
         default: return k_sweeps_cluster<VT, 0>;
     }
 }
-template <typename VT>
-auto persistent_kernel(int m) -> decltype(&k_sweeps_persistent<VT, 0>) {
+template <typename VT, bool GEN>
+auto persistent_kernel_g(int m) -> decltype(&k_sweeps_persistent<VT, 0, GEN>) {
     switch (m) {
-        case 1: return k_sweeps_persistent<VT, 1>;
-        case 2: return k_sweeps_persistent<VT, 2>;
-        case 3: return k_sweeps_persistent<VT, 3>;
-        case 4: return k_sweeps_persistent<VT, 4>;
-        case 5: return k_sweeps_persistent<VT, 5>;
-        default: return k_sweeps_persistent<VT, 0>;
+        case 1: return k_sweeps_persistent<VT, 1, GEN>;
+        case 2: return k_sweeps_persistent<VT, 2, GEN>;
+        case 3: return k_sweeps_persistent<VT, 3, GEN>;
+        case 4: return k_sweeps_persistent<VT, 4, GEN>;
+        case 5: return k_sweeps_persistent<VT, 5, GEN>;
+        default: return k_sweeps_persistent<VT, 0, GEN>;
+    }
+}
+// gen: bodies with a full inverse inertia (moving boxes; FP64 only)
+template <typename VT>
+auto persistent_kernel(int m, bool gen) -> decltype(&k_sweeps_persistent<VT, 0, false>) {
+    if constexpr (std::is_same<VT, double>::value) {
+        if (gen) return persistent_kernel_g<VT, true>(m);
+    }
+    return persistent_kernel_g<VT, false>(m);
+}
+template <typename VT, bool GEN>
+auto colour_kernel_g(int m) -> decltype(&k_sweep<VT, 0, GEN>) {
+    switch (m) {
+        case 1: return k_sweep<VT, 1, GEN>;
+        case 2: return k_sweep<VT, 2, GEN>;
+        case 3: return k_sweep<VT, 3, GEN>;
+        case 4: return k_sweep<VT, 4, GEN>;
+        case 5: return k_sweep<VT, 5, GEN>;
+        default: return k_sweep<VT, 0, GEN>;
     }
 }
 template <typename VT>
-auto colour_kernel(int m) -> decltype(&k_sweep<VT, 0>) {
-    switch (m) {
-        case 1: return k_sweep<VT, 1>;
-        case 2: return k_sweep<VT, 2>;
-        case 3: return k_sweep<VT, 3>;
-        case 4: return k_sweep<VT, 4>;
-        case 5: return k_sweep<VT, 5>;
-        default: return k_sweep<VT, 0>;
+auto colour_kernel(int m, bool gen) -> decltype(&k_sweep<VT, 0, false>) {
+    if constexpr (std::is_same<VT, double>::value) {
+        if (gen) return colour_kernel_g<VT, true>(m);
     }
+    return colour_kernel_g<VT, false>(m);
 }
 
 // Runs all sweeps in one cluster when the largest colour is small enough; *done reports it.
@@ -1064,21 +1188,37 @@ template <typename VT>
 int nbgs_step_t(Ctx *c, double dt) {
     NbgsBuf &nb = c->nb;
     const int64_t n = c->n;
-    const int64_t auto_cap = c->p.max_contacts > 0 ? c->p.max_contacts : std::max<int64_t>(8 * n, 1024);
+    // moving boxes: bodies n .. n+m-1 with full inverse inertias (FP64 only, checked by the
+    // caller)
+    const bool gen = c->mb.m > 0;
+    const int64_t nbod = n + c->mb.m;
+    const int64_t auto_cap = c->p.max_contacts > 0 ? c->p.max_contacts : std::max<int64_t>(8 * nbod, 1024);
     int rc = nbgs_alloc(c, auto_cap);
     if (rc) return rc;
     // 1. sort, permute to slot order, body cache
-    if (!c->binned) {
-        rc = grid_bin_current(c);
+    if (n > 0) {
+        if (!c->binned) {
+            rc = grid_bin_current(c);
+            if (rc) return rc;
+        }
+        rc = grid_sort(c);
         if (rc) return rc;
     }
-    rc = grid_sort(c);
-    if (rc) return rc;
     Raw<VT> raw;
     Cache<VT> cc;
     BodyV<VT> bv;
     layout(c, raw, cc, bv);
-    {
+    auto body_cache_d = [&]() {
+        BodyCacheD d{};
+        if constexpr (std::is_same<VT, double>::value)
+            d = BodyCacheD{bv.vr, bv.wr, bv.dv, bv.dw, bv.ia, bv.ib, bv.ic};
+        return d;
+    };
+    if (gen) {
+        rc = mbox_hc_bodycache(c, body_cache_d(), dt);
+        if (rc) return rc;
+    }
+    if (n > 0) {
         prof_begin(c, ST_PERMUTE);
         const bool tq = c->p.track_orientation != 0;
         auto kern = tq ? k_permute_cache<VT, true> : k_permute_cache<VT, false>;
@@ -1090,16 +1230,26 @@ int nbgs_step_t(Ctx *c, double dt) {
         prof_end(c, ST_PERMUTE);
         std::swap(c->cur, c->nxt);
     }
-    // 2. detection: count, scan, write (state is in slot order now: sorted == identity)
+    // 2. detection: count, scan, write (state is in slot order now: sorted == identity);
+    // the contacts of the moving boxes follow the spheres' contacts
     VisitArgs va = visit_args(c, nullptr);
     prof_begin(c, ST_DETECT);
-    k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
-    PEB_LAUNCHED(c);
-    rc = scan_exclusive(c, nb.cnt, nb.cnt, n);
-    if (rc) return rc;
-    int32_t total = 0;
-    PEB_CUDA(c, cudaMemcpyAsync(&total, nb.cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    int32_t total = 0, total_s = 0, total_b = 0;
+    if (n > 0) {
+        k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
+        PEB_LAUNCHED(c);
+        rc = scan_exclusive(c, nb.cnt, nb.cnt, n);
+        if (rc) return rc;
+        PEB_CUDA(c, cudaMemcpyAsync(&total_s, nb.cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    if (gen) {
+        rc = mbox_hc_count(c, &total_b);
+        if (rc) return rc;
+    }
+    if ((int64_t)total_s + total_b > INT32_MAX)
+        return set_err(c, PE_B200_ERR_CAPACITY, "contact count exceeds int32");
+    total = total_s + total_b;
     if (total > nb.cap) {
         if (c->p.max_contacts > 0)
             return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
@@ -1110,33 +1260,42 @@ int nbgs_step_t(Ctx *c, double dt) {
     const int64_t nc = total;
     const int64_t cap = nb.cap;
     c->last_ncontacts = nc;
-    k_raw<VT><<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt, cap, (const VT *)c->cur.vw,
-                                                         c->d_mats, c->d_plane_mat, c->d_box_mat,
-                                                         c->p.erp, raw, c->d_err);
-    PEB_LAUNCHED(c);
+    if (n > 0) {
+        k_raw<VT><<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt, cap, (const VT *)c->cur.vw,
+                                                             c->d_mats, c->d_plane_mat, c->d_box_mat,
+                                                             c->p.erp, raw, c->d_err);
+        PEB_LAUNCHED(c);
+    }
+    if constexpr (std::is_same<VT, double>::value) {
+        if (gen) {
+            rc = mbox_hc_raw(c, total_s, cap, raw.b1, raw.b2, raw.r1, raw.r2, raw.n, raw.dist, raw.mu);
+            if (rc) return rc;
+        }
+    }
     prof_end(c, ST_DETECT);
     // 3. colouring
     int32_t ncolors = 0;
     if (nc > 0) {
         prof_begin(c, ST_COLOR);
-        PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)n + 1) * sizeof(int32_t), c->stream));
+        PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)nbod + 1) * sizeof(int32_t), c->stream));
         k_degree<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, raw.b1, raw.b2, nb.body_cnt);
         PEB_LAUNCHED(c);
-        rc = scan_exclusive(c, nb.body_cnt, nb.body_cnt, n);
+        rc = scan_exclusive(c, nb.body_cnt, nb.body_cnt, nbod);
         if (rc) return rc;
         int32_t *fill = nb.cnt;  // reuse: counts are consumed
-        PEB_CUDA(c, cudaMemcpyAsync(fill, nb.body_cnt, ((size_t)n + 1) * sizeof(int32_t),
+        PEB_CUDA(c, cudaMemcpyAsync(fill, nb.body_cnt, ((size_t)nbod + 1) * sizeof(int32_t),
                                     cudaMemcpyDeviceToDevice, c->stream));
         k_adj_fill<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, raw.b1, raw.b2, fill, nb.body_adj);
         PEB_LAUNCHED(c);
         PEB_CUDA(c, cudaMemsetAsync(nb.color, 0xff, (size_t)nc * sizeof(int32_t), c->stream));
-        PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)n * sizeof(uint64_t), c->stream));
+        const int words = gen ? 4 : 1;
+        PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)nbod * words * sizeof(uint64_t), c->stream));
         int round = 0;
         for (;;) {
             const int batch = 8;
             PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, batch * sizeof(int32_t), c->stream));
             for (int k = 0; k < batch; ++k, ++round) {
-                k_color_round<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(
+                (gen ? k_color_round<4> : k_color_round<1>)<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(
                     nc, round, raw.b1, raw.b2, nb.body_cnt, nb.body_adj, nb.color, nb.used,
                     nb.flags + k, c->d_err);
                 PEB_LAUNCHED(c);
@@ -1148,14 +1307,14 @@ int nbgs_step_t(Ctx *c, double dt) {
             if (round > 4096) return set_err(c, PE_B200_ERR_TIMEOUT, "colouring did not finish");
         }
         // counting sort by colour
-        PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, 256 * sizeof(int32_t), c->stream));
-        int32_t *hist = nb.flags, *nco = nb.flags + 128;
+        PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, 2 * kMaxColors * sizeof(int32_t), c->stream));
+        int32_t *hist = nb.flags, *nco = nb.flags + kMaxColors;
         k_color_hist<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, nb.color, hist, nco);
         PEB_LAUNCHED(c);
-        PEB_CUDA(c, cudaMemcpyAsync(nb.color_start, nb.flags, 130 * sizeof(int32_t),
+        PEB_CUDA(c, cudaMemcpyAsync(nb.color_start, nb.flags, (kMaxColors + 2) * sizeof(int32_t),
                                     cudaMemcpyDeviceToHost, c->stream));
         PEB_CUDA(c, cudaStreamSynchronize(c->stream));
-        ncolors = nb.color_start[128];
+        ncolors = nb.color_start[kMaxColors];
         std::vector<int32_t> start(ncolors + 1, 0);
         for (int k = 0; k < ncolors; ++k) start[k + 1] = start[k] + nb.color_start[k];
         for (int k = 0; k <= ncolors; ++k) nb.color_start[k] = start[k];
@@ -1166,7 +1325,12 @@ int nbgs_step_t(Ctx *c, double dt) {
         prof_end(c, ST_COLOR);
         prof_begin(c, ST_CACHE);
         // 4. contact cache in colour-sorted order
-        k_cache<VT><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+        if constexpr (std::is_same<VT, double>::value) {
+            if (gen) k_cache<VT, true><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+            else k_cache<VT, false><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+        } else {
+            k_cache<VT, false><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+        }
         PEB_LAUNCHED(c);
         prof_end(c, ST_CACHE);
     }
@@ -1186,7 +1350,7 @@ int nbgs_step_t(Ctx *c, double dt) {
         const int mode = c->tune.nbgs_sweeps;
         // the one-cluster form has the cheaper barrier but only a few SMs' load bandwidth; on
         // B200 the grid form is faster for every scene measured, so it is the automatic choice
-        if (!done && nb.cluster != 0 && mode == 1) {
+        if (!done && nb.cluster != 0 && mode == 1 && !gen) {
             int rc = sweeps_in_cluster<VT>(c, model, iters, ncolors, maxcol, cap, VT(1.0 / dt), cc,
                                            bv, n, dl, &done);
             if (rc) return rc;
@@ -1194,7 +1358,7 @@ int nbgs_step_t(Ctx *c, double dt) {
         if (!done && !nb.coop_disabled && mode != 3) {
             // all sweeps in one cooperative launch (colours separated by grid barriers); as few
             // blocks as the largest colour needs, so the barriers stay short
-            auto kern = persistent_kernel<VT>(model);
+            auto kern = persistent_kernel<VT>(model, gen);
             int occ = 0;
             cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0);
             const unsigned grid = (unsigned)std::min<int64_t>(
@@ -1231,7 +1395,7 @@ int nbgs_step_t(Ctx *c, double dt) {
             for (int col = 0; col < ncolors; ++col) {
                 const int64_t b = nb.color_start[col], e = nb.color_start[col + 1];
                 if (e <= b) continue;
-                colour_kernel<VT>(model)<<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
+                colour_kernel<VT>(model, gen)<<<grid_for(e - b, kBlk), kBlk, 0, c->stream>>>(
                     b, e, cap, VT(1.0 / dt), cc, bv, n, track, dl);
                 PEB_LAUNCHED(c);
             }
@@ -1252,13 +1416,19 @@ int nbgs_step_t(Ctx *c, double dt) {
         const int has_drag = c->p.damping < 1.0;
         const double drag = has_drag ? pow(c->p.damping, dt) : 1.0;
         auto kern = tq ? k_integrate<VT, true> : k_integrate<VT, false>;
-        kern<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(
-            n, dt, drag, has_drag, bv, c->d_scenes, c->cur.pr, c->cur.tag, c->cur.uid, c->cur.q,
-            c->nxt.pr, (VT *)c->nxt.vw, c->nxt.tag, c->nxt.uid, c->nxt.q, c->key, c->rank,
-            c->cell_count, c->d_err);
-        PEB_LAUNCHED(c);
+        if (n > 0) {
+            kern<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(
+                n, dt, drag, has_drag, bv, c->d_scenes, c->cur.pr, c->cur.tag, c->cur.uid, c->cur.q,
+                c->nxt.pr, (VT *)c->nxt.vw, c->nxt.tag, c->nxt.uid, c->nxt.q, c->key, c->rank,
+                c->cell_count, c->d_err);
+            PEB_LAUNCHED(c);
+        }
+        if (gen) {
+            rc = mbox_hc_integrate(c, body_cache_d(), dt);
+            if (rc) return rc;
+        }
         prof_end(c, ST_INTEGRATE);
-        std::swap(c->cur, c->nxt);
+        if (n > 0) std::swap(c->cur, c->nxt);
     }
     if (c->want_residual) {
         double r[2];
@@ -1294,7 +1464,7 @@ void nbgs_free(Ctx *c) {
 }
 
 int nbgs_step(Ctx *c, double dt) {
-    if (c->n == 0) return PE_B200_OK;
+    if (c->n == 0 && c->mb.m == 0) return PE_B200_OK;
     return (c->p.precision == PE_B200_FP64) ? nbgs_step_t<double>(c, dt) : nbgs_step_t<float>(c, dt);
 }
 
@@ -1316,7 +1486,27 @@ const int2 *nbgs_ids_ptr(Ctx *c) {
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out) {
     const int64_t n = c->n;
     *n_out = 0;
-    if (n == 0) return PE_B200_OK;
+    if (n == 0) {
+        // moving boxes only
+        std::vector<int64_t> bid;
+        std::vector<double> bg;
+        int rc = mbox_find_contacts(c, bid, bg);
+        if (rc) return rc;
+        const int64_t nb_ = (int64_t)bid.size() / 3;
+        std::vector<int64_t> idx(nb_);
+        for (int64_t k = 0; k < nb_; ++k) idx[k] = k;
+        std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+            if (bid[3 * a] != bid[3 * b]) return bid[3 * a] < bid[3 * b];
+            return bid[3 * a + 1] < bid[3 * b + 1];
+        });
+        for (int64_t k = 0; k < std::min<int64_t>(cap, nb_); ++k) {
+            ids[2 * k] = bid[3 * idx[k]];
+            ids[2 * k + 1] = bid[3 * idx[k] + 1];
+            for (int a = 0; a < 7; ++a) geom[7 * k + a] = bg[7 * idx[k] + a];
+        }
+        *n_out = nb_;
+        return PE_B200_OK;
+    }
     // make the sort describe the current state (keeps key/rank/counts valid for the next step)
     if (!c->binned) {
         int rc = grid_bin_current(c);
@@ -1355,10 +1545,26 @@ int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_ou
     cudaFree(d_ids);
     cudaFree(d_geom);
     if (e != cudaSuccess) return cuda_err(c, e, "find_contacts");
-    // canonical order (b1, b2)
+    // the contacts of the moving boxes (pe's orientation and ids) follow
+    {
+        std::vector<int64_t> bid;
+        std::vector<double> bg;
+        rc = mbox_find_contacts(c, bid, bg);
+        if (rc) return rc;
+        const int64_t nb_ = (int64_t)bid.size() / 3;
+        hid.resize(2 * (size_t)total);
+        hg.resize(7 * (size_t)total);
+        for (int64_t k = 0; k < nb_; ++k) {
+            hid.push_back(bid[3 * k]);
+            hid.push_back(bid[3 * k + 1]);
+            for (int a = 0; a < 7; ++a) hg.push_back(bg[7 * k + a]);
+        }
+        total += (int32_t)nb_;
+    }
+    // canonical order (b1, b2); the several contacts of a box pair keep their order
     std::vector<int64_t> idx(total);
     for (int64_t k = 0; k < total; ++k) idx[k] = k;
-    std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+    std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
         if (hid[2 * a] != hid[2 * b]) return hid[2 * a] < hid[2 * b];
         return hid[2 * a + 1] < hid[2 * b + 1];
     });

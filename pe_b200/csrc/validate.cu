@@ -42,7 +42,7 @@ int validate_coloring(Ctx *c, int64_t *bad) {
     std::vector<int32_t> ids(2 * nc);
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     PEB_CUDA(c, cudaMemcpy(ids.data(), nbgs_ids_ptr(c), nc * sizeof(int2), cudaMemcpyDeviceToHost));
-    *bad += coloring_problems(c->n, nc, ids.data(), ncol, nb.color_start);
+    *bad += coloring_problems(c->n + c->mb.m, nc, ids.data(), ncol, nb.color_start);
     return PE_B200_OK;
 }
 
@@ -50,7 +50,8 @@ int validate_coloring(Ctx *c, int64_t *bad) {
 int validate_lists(Ctx *c, int64_t *bad) {
     const ListBuf &L = c->nl;
     const int64_t n = c->n;
-    if (!L.enabled || n == 0 || !L.start || !L.flags) return PE_B200_OK;
+    // lists exist once a list step has run (scenes with moving boxes use the cell grid)
+    if (!L.enabled || !L.warm || c->mb.m > 0 || n == 0 || !L.start || !L.flags) return PE_B200_OK;
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     int32_t flags[4];
     PEB_CUDA(c, cudaMemcpy(flags, L.flags, sizeof flags, cudaMemcpyDeviceToHost));

@@ -105,7 +105,32 @@ class Engine:
         self.set_gravity(scene.gravity)
         self.set_damping(scene.damping)
         self.upload(scene.x, scene.v, scene.w, scene.r, scene.mat)
+        if getattr(scene, "nmbox", 0):
+            self.upload_boxes(scene.mbox_x, scene.mbox_q, scene.mbox_v, scene.mbox_w,
+                              scene.mbox_len, scene.mbox_mat)
         return self
+
+    def upload_boxes(self, x, q, v, w, lengths, mat, scene=None):
+        """Moving boxes (after the spheres): centres, unit quaternions (w x y z), velocities,
+        side lengths, material ids, optional scene ids grouped by scene."""
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(q, np.float64).reshape(-1, 4)
+        v = np.ascontiguousarray(v, np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(w, np.float64).reshape(-1, 3)
+        lengths = np.ascontiguousarray(lengths, np.float64).reshape(-1, 3)
+        mat = np.ascontiguousarray(mat, np.int32).reshape(-1)
+        sc = None if scene is None else np.ascontiguousarray(scene, np.int32).reshape(-1)
+        self._check(self._L.pe_b200_upload_boxes(self._h, x.shape[0], _p(x), _p(q), _p(v), _p(w),
+                                                 _p(lengths), _p(mat), _p(sc)))
+        self.nbox = x.shape[0]
+
+    def download_boxes(self):
+        """(x, q, v, w) of the moving boxes."""
+        m = int(self._L.pe_b200_box_count(self._h))
+        x, q = np.zeros((m, 3)), np.zeros((m, 4))
+        v, w = np.zeros((m, 3)), np.zeros((m, 3))
+        self._check(self._L.pe_b200_download_boxes(self._h, _p(x), _p(q), _p(v), _p(w)))
+        return x, q, v, w
 
     def load_scenes(self, scenes: Sequence) -> "Engine":
         """A batch of independent scenes (each keeps its own walls and grid); materials are
