@@ -24,8 +24,8 @@
  * unsupported configurations and device errors.
  *
  * Differences from pe, all checked at the call that hits them:
- *   - spheres move; planes and boxes are fixed walls (a box must be setFixed(true) before the
- *     next time step, as pe's fixed boxes are);
+ *   - spheres and boxes move, planes are fixed; fixed boxes are walls; moving boxes need FP64
+ *     precision (setPrecision(PE_B200_MIXED) with a moving box fails at the next step);
  *   - the solver is chosen at run time (theCollisionSystem()->setSolver) instead of by the
  *     compile-time pe_CONSTRAINT_SOLVER; the default is PE_B200_CONSTRAINT_SOLVER
  *     (PE_B200_DEM unless defined before including this header);
@@ -36,6 +36,7 @@
 #define PE_B200_WORLD_HPP
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -177,6 +178,9 @@ inline MaterialID createMaterial(real density, real cor, real csf, real cdf, rea
 
 // ---- bodies ------------------------------------------------------------------------------------
 class World;
+namespace detail {
+inline void rot_of(const real q[4], real R[9]);
+}
 
 class RigidBody {
   public:
@@ -235,22 +239,42 @@ class Plane : public RigidBody {
     friend class World;
 };
 
+/* A box: fixed boxes are walls, the others move (BoxTrait::move for DEM, box bodies in the
+ * hard-contact solver).  Contacts between a fixed and a moving box are computed with the fixed
+ * box as pe's lower system id, as when fixed boxes are created first. */
 class Box : public RigidBody {
   public:
-    const Vec3 &getPosition() const { return x_; }
+    Vec3 getPosition() const;
     const Vec3 &getLengths() const { return l_; }
     bool isFixed() const { return fixed_; }
     void setFixed(bool fixed);
-    /* rotation matrix, row-major */
-    const real *getRotation() const { return R_; }
-    /* RigidBody::rotate(axis, angle): rotation about the box centre (Rodrigues' formula) */
+    /* BoxBase::calcMass (pe/core/rigidbody/BoxBase.h:186-189) */
+    real getMass() const { return l_[0] * l_[1] * l_[2] * pe_b200::getMaterial(mat_).getDensity(); }
+    /* rotation matrix, row-major (Quaternion::toRotationMatrix of the orientation) */
+    const real *getRotation() const;
+    /* orientation (w, x, y, z) */
+    std::array<real, 4> getQuaternion() const;
+    Vec3 getLinearVel() const;
+    Vec3 getAngularVel() const;
+    void setPosition(real x, real y, real z);
+    void setPosition(const Vec3 &p) { setPosition(p[0], p[1], p[2]); }
+    void setLinearVel(real x, real y, real z);
+    void setLinearVel(const Vec3 &v) { setLinearVel(v[0], v[1], v[2]); }
+    void setAngularVel(real x, real y, real z);
+    void setAngularVel(const Vec3 &w) { setAngularVel(w[0], w[1], w[2]); }
+    /* Box::setOrientation (src/core/rigidbody/Box.cpp:289-300) */
+    void setOrientation(real r, real i, real j, real k);
+    /* Box::rotate (src/core/rigidbody/Box.cpp:489-500): q = Quat(axis, angle) * q */
     void rotate(const Vec3 &axis, real angle);
     void rotate(real x, real y, real z, real angle) { rotate(Vec3(x, y, z), angle); }
 
   private:
     Box(World *w, id_t sid, id_t uid, const Vec3 &x, const Vec3 &l, MaterialID m, bool visible)
-        : RigidBody(w, sid, uid, m, visible), x_(x), l_(l), R_{1, 0, 0, 0, 1, 0, 0, 0, 1} {}
-    Vec3 x_, l_;
+        : RigidBody(w, sid, uid, m, visible), x_(x), l_(l), q_{1, 0, 0, 0},
+          R_{1, 0, 0, 0, 1, 0, 0, 0, 1} {}
+    void changed();
+    Vec3 x_, l_, v_, w_;
+    real q_[4];
     real R_[9];
     bool fixed_ = false;
     friend class World;
@@ -405,16 +429,33 @@ class World {
         if (!host_stale_ || !ctx_) return;
         const std::size_t n = spheres_.size();
         std::vector<double> x(3 * n), v(3 * n), w(3 * n);
-        check(pe_b200_download_bodies(ctx_, x.data(), v.data(), w.data(), nullptr));
+        if (n) check(pe_b200_download_bodies(ctx_, x.data(), v.data(), w.data(), nullptr));
         for (std::size_t i = 0; i < n; ++i) {
             Sphere &s = *spheres_[i];
             s.x_ = Vec3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
             s.v_ = Vec3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
             s.w_ = Vec3(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
         }
+        std::vector<Box *> mv;
+        for (const auto &b : boxes_)
+            if (!b->fixed_) mv.push_back(b.get());
+        if (!mv.empty()) {
+            const std::size_t m = mv.size();
+            std::vector<double> bx(3 * m), bq(4 * m), bv(3 * m), bw(3 * m);
+            check(pe_b200_download_boxes(ctx_, bx.data(), bq.data(), bv.data(), bw.data()));
+            for (std::size_t k = 0; k < m; ++k) {
+                Box &b = *mv[k];
+                b.x_ = Vec3(bx[3 * k], bx[3 * k + 1], bx[3 * k + 2]);
+                for (int a = 0; a < 4; ++a) b.q_[a] = bq[4 * k + a];
+                detail::rot_of(b.q_, b.R_);
+                b.v_ = Vec3(bv[3 * k], bv[3 * k + 1], bv[3 * k + 2]);
+                b.w_ = Vec3(bw[3 * k], bw[3 * k + 1], bw[3 * k + 2]);
+            }
+        }
         host_stale_ = false;
     }
     void markStateDirty() { state_dirty_ = true; }
+    void markBoxesDirty() { boxes_dirty_ = true; }
     void markStructureDirty() { structure_dirty_ = true; }
     void markParamsDirty() { params_dirty_ = true; }
     void check(int rc) const {
@@ -464,10 +505,6 @@ class World {
             params_dirty_ = false;
             structure_dirty_ = true;
         }
-        for (const auto &b : boxes_)
-            if (!b->isFixed())
-                throw std::runtime_error("Box " + std::to_string(b->getID()) +
-                                         " is not fixed: only fixed boxes are supported");
         if (structure_dirty_) {
             std::vector<pe_b200_material> mats;
             for (const Material &m : detail::materials()) mats.push_back(m.record());
@@ -478,13 +515,16 @@ class World {
                 planes.insert(planes.end(), {p->n_[0], p->n_[1], p->n_[2], p->d_});
                 pm.push_back((int32_t)p->mat_);
             }
+            int32_t nfixed = 0;
             for (const auto &b : boxes_) {
+                if (!b->fixed_) continue;
                 boxes.insert(boxes.end(), {b->x_[0], b->x_[1], b->x_[2], b->l_[0], b->l_[1], b->l_[2]});
                 boxes.insert(boxes.end(), b->R_, b->R_ + 9);
                 bm.push_back((int32_t)b->mat_);
+                ++nfixed;
             }
             check(pe_b200_set_walls(ctx_, 0, (int32_t)planes_.size(), planes.data(), pm.data(),
-                                    (int32_t)boxes_.size(), boxes.data(), bm.data()));
+                                    nfixed, boxes.data(), bm.data()));
             const std::size_t n = spheres_.size();
             std::vector<double> x, v, w, r;
             std::vector<int32_t> mat;
@@ -495,11 +535,13 @@ class World {
                 r.push_back(s->r_);
                 mat.push_back((int32_t)s->mat_);
             }
-            if (n) check(pe_b200_upload_bodies(ctx_, (int64_t)n, x.data(), v.data(), w.data(),
-                                               r.data(), mat.data(), nullptr, 1));
+            check(pe_b200_upload_bodies(ctx_, (int64_t)n, x.data(), v.data(), w.data(), r.data(),
+                                        mat.data(), nullptr, 1));
+            upload_boxes();
             structure_dirty_ = false;
             state_dirty_ = false;
-        } else if (state_dirty_) {
+            boxes_dirty_ = false;
+        } else if (state_dirty_ || boxes_dirty_) {
             const std::size_t n = spheres_.size();
             std::vector<double> x(3 * n), v(3 * n), w(3 * n);
             for (std::size_t i = 0; i < n; ++i)
@@ -508,15 +550,35 @@ class World {
                     v[3 * i + a] = spheres_[i]->v_[a];
                     w[3 * i + a] = spheres_[i]->w_[a];
                 }
-            if (n) check(pe_b200_set_state(ctx_, x.data(), v.data(), w.data()));
+            if (n && state_dirty_) check(pe_b200_set_state(ctx_, x.data(), v.data(), w.data()));
+            if (boxes_dirty_) upload_boxes();
             state_dirty_ = false;
+            boxes_dirty_ = false;
         }
         check(pe_b200_set_gravity(ctx_, gravity_array()));
         check(pe_b200_set_damping(ctx_, damping_));
     }
 
+    // the moving boxes, in system-id order
+    void upload_boxes() {
+        std::vector<double> x, q, v, w, l;
+        std::vector<int32_t> mat;
+        for (const auto &b : boxes_) {
+            if (b->fixed_) continue;
+            x.insert(x.end(), {b->x_[0], b->x_[1], b->x_[2]});
+            q.insert(q.end(), b->q_, b->q_ + 4);
+            v.insert(v.end(), {b->v_[0], b->v_[1], b->v_[2]});
+            w.insert(w.end(), {b->w_[0], b->w_[1], b->w_[2]});
+            l.insert(l.end(), {b->l_[0], b->l_[1], b->l_[2]});
+            mat.push_back((int32_t)b->mat_);
+        }
+        check(pe_b200_upload_boxes(ctx_, (int32_t)mat.size(), x.data(), q.data(), v.data(),
+                                   w.data(), l.data(), mat.data(), nullptr));
+    }
+
     friend class BodyBinaryWriter;
     friend class BodyBinaryReader;
+    friend class Box;
     CollisionSystem cs_;
     pe_b200_ctx *ctx_ = nullptr;
     std::vector<std::unique_ptr<Sphere>> spheres_;
@@ -526,7 +588,7 @@ class World {
     double ga_[3] = {0.0, 0.0, 0.0};
     real damping_ = 1.0;
     id_t next_sid_ = 0;
-    bool structure_dirty_ = true, state_dirty_ = false, params_dirty_ = true;
+    bool structure_dirty_ = true, state_dirty_ = false, params_dirty_ = true, boxes_dirty_ = false;
     mutable bool host_stale_ = false;
 };
 
@@ -566,28 +628,17 @@ inline Vec3 get_vec(const std::string &in, size_t &p) {
     const double x = get<double>(in, p), y = get<double>(in, p), z = get<double>(in, p);
     return Vec3(x, y, z);
 }
-// rotation matrix (row-major) <-> unit quaternion (w, x, y, z)
-inline void quat_of(const real R[9], real q[4]) {
-    const real tr = R[0] + R[4] + R[8];
-    if (tr > 0) {
-        const real s = std::sqrt(tr + 1.0) * 2;
-        q[0] = 0.25 * s; q[1] = (R[7] - R[5]) / s; q[2] = (R[2] - R[6]) / s; q[3] = (R[3] - R[1]) / s;
-    } else if (R[0] > R[4] && R[0] > R[8]) {
-        const real s = std::sqrt(1.0 + R[0] - R[4] - R[8]) * 2;
-        q[0] = (R[7] - R[5]) / s; q[1] = 0.25 * s; q[2] = (R[1] + R[3]) / s; q[3] = (R[2] + R[6]) / s;
-    } else if (R[4] > R[8]) {
-        const real s = std::sqrt(1.0 + R[4] - R[0] - R[8]) * 2;
-        q[0] = (R[2] - R[6]) / s; q[1] = (R[1] + R[3]) / s; q[2] = 0.25 * s; q[3] = (R[5] + R[7]) / s;
-    } else {
-        const real s = std::sqrt(1.0 + R[8] - R[0] - R[4]) * 2;
-        q[0] = (R[3] - R[1]) / s; q[1] = (R[2] + R[6]) / s; q[2] = (R[5] + R[7]) / s; q[3] = 0.25 * s;
-    }
-}
+// Quaternion::toRotationMatrix, in pe's operation order (pe/math/Quaternion.h:591-602)
 inline void rot_of(const real q[4], real R[9]) {
-    const real w = q[0], x = q[1], y = q[2], z = q[3];
-    R[0] = 1 - 2 * (y * y + z * z); R[1] = 2 * (x * y - w * z);     R[2] = 2 * (x * z + w * y);
-    R[3] = 2 * (x * y + w * z);     R[4] = 1 - 2 * (x * x + z * z); R[5] = 2 * (y * z - w * x);
-    R[6] = 2 * (x * z - w * y);     R[7] = 2 * (y * z + w * x);     R[8] = 1 - 2 * (x * x + y * y);
+    R[0] = 1.0 - 2.0 * q[2] * q[2] - 2.0 * q[3] * q[3];
+    R[1] = 2.0 * (q[1] * q[2] - q[0] * q[3]);
+    R[2] = 2.0 * (q[1] * q[3] + q[0] * q[2]);
+    R[3] = 2.0 * (q[1] * q[2] + q[0] * q[3]);
+    R[4] = 1.0 - 2.0 * q[1] * q[1] - 2.0 * q[3] * q[3];
+    R[5] = 2.0 * (q[2] * q[3] - q[0] * q[1]);
+    R[6] = 2.0 * (q[1] * q[3] - q[0] * q[2]);
+    R[7] = 2.0 * (q[2] * q[3] + q[0] * q[1]);
+    R[8] = 1.0 - 2.0 * q[1] * q[1] - 2.0 * q[2] * q[2];
 }
 }  // namespace detail
 
@@ -625,9 +676,8 @@ inline void World::writeCheckpoint(const char *filename) const {
         } else if (t == 2) {
             put<uint32_t>(loc, (uint32_t)boxes_.size());
             for (const auto &b : boxes_) {
-                real q[4];
-                quat_of(b->R_, q);
-                rigid(loc, *b, b->fixed_, b->x_, q, Vec3(), Vec3());
+                rigid(loc, *b, b->fixed_, b->x_, b->q_, b->fixed_ ? Vec3() : b->v_,
+                      b->fixed_ ? Vec3() : b->w_);
                 put_vec(loc, b->l_);
             }
         } else {
@@ -687,8 +737,12 @@ inline void World::readCheckpoint(const char *filename) {
                 } else if (t == 2) {
                     const Vec3 l = get_vec(in, q);
                     boxes_.emplace_back(new Box(this, sid, uid, x, l, m, vis));
-                    rot_of(qq, boxes_.back()->R_);
-                    boxes_.back()->fixed_ = fixed;
+                    Box &bx = *boxes_.back();
+                    for (int a = 0; a < 4; ++a) bx.q_[a] = qq[a];
+                    rot_of(qq, bx.R_);
+                    bx.fixed_ = fixed;
+                    bx.v_ = v;
+                    bx.w_ = w;
                 } else if (t == 5) {
                     real R[9];
                     rot_of(qq, R);
@@ -773,22 +827,63 @@ inline void Sphere::setAngularVel(real x, real y, real z) {
     world_->markStateDirty();
 }
 inline void Box::setFixed(bool fixed) {
+    world_->pull();
     fixed_ = fixed;
+    if (fixed) v_ = w_ = Vec3();
     world_->markStructureDirty();
+}
+// a state change: a fixed box is part of the walls, a moving one of the box upload
+inline void Box::changed() {
+    if (fixed_) world_->markStructureDirty();
+    else world_->markBoxesDirty();
+}
+inline Vec3 Box::getPosition() const { world_->pull(); return x_; }
+inline const real *Box::getRotation() const { world_->pull(); return R_; }
+inline std::array<real, 4> Box::getQuaternion() const {
+    world_->pull();
+    return {q_[0], q_[1], q_[2], q_[3]};
+}
+inline Vec3 Box::getLinearVel() const { world_->pull(); return v_; }
+inline Vec3 Box::getAngularVel() const { world_->pull(); return w_; }
+inline void Box::setPosition(real x, real y, real z) {
+    world_->pull();
+    x_ = Vec3(x, y, z);
+    changed();
+}
+inline void Box::setLinearVel(real x, real y, real z) {
+    world_->pull();
+    if (!fixed_) v_ = Vec3(x, y, z);   // RigidBody::setLinearVel: no effect on fixed bodies
+    changed();
+}
+inline void Box::setAngularVel(real x, real y, real z) {
+    world_->pull();
+    if (!fixed_) w_ = Vec3(x, y, z);
+    changed();
+}
+inline void Box::setOrientation(real r, real i, real j, real k) {
+    world_->pull();
+    q_[0] = r; q_[1] = i; q_[2] = j; q_[3] = k;
+    detail::rot_of(q_, R_);
+    changed();
 }
 inline void Box::rotate(const Vec3 &axis, real angle) {
     if (axis.sqrLength() == 0.0) throw std::invalid_argument("Invalid rotation axis");
-    const Vec3 u = axis.getNormalized();
-    const real c = std::cos(angle), s = std::sin(angle), t = 1.0 - c;
-    const real Q[9] = {t * u[0] * u[0] + c,        t * u[0] * u[1] - s * u[2], t * u[0] * u[2] + s * u[1],
-                       t * u[0] * u[1] + s * u[2], t * u[1] * u[1] + c,        t * u[1] * u[2] - s * u[0],
-                       t * u[0] * u[2] - s * u[1], t * u[1] * u[2] + s * u[0], t * u[2] * u[2] + c};
-    real out[9];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            out[3 * i + j] = Q[3 * i] * R_[j] + Q[3 * i + 1] * R_[3 + j] + Q[3 * i + 2] * R_[6 + j];
-    for (int k = 0; k < 9; ++k) R_[k] = out[k];
-    world_->markStructureDirty();
+    world_->pull();
+    // Quaternion(axis, angle) (pe/math/Quaternion.h:274-294) times q (Quaternion.h:1146-1153)
+    real d[4] = {1.0, 0.0, 0.0, 0.0};
+    if (!(std::fabs(angle) < 1e-15)) {
+        const real sina = std::sin(angle * 0.5), cosa = std::cos(angle * 0.5);
+        const Vec3 u = axis.getNormalized();
+        d[0] = cosa; d[1] = sina * u[0]; d[2] = sina * u[1]; d[3] = sina * u[2];
+    }
+    const real *q = q_;
+    const real r0 = d[0] * q[0] - d[1] * q[1] - d[2] * q[2] - d[3] * q[3];
+    const real r1 = d[0] * q[1] + d[1] * q[0] + d[2] * q[3] - d[3] * q[2];
+    const real r2 = d[0] * q[2] + d[2] * q[0] + d[3] * q[1] - d[1] * q[3];
+    const real r3 = d[0] * q[3] + d[3] * q[0] + d[1] * q[2] - d[2] * q[1];
+    q_[0] = r0; q_[1] = r1; q_[2] = r2; q_[3] = r3;
+    detail::rot_of(q_, R_);
+    changed();
 }
 
 inline void CollisionSystem::setMaxIterations(std::size_t n) {

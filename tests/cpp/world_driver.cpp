@@ -76,6 +76,10 @@ struct SceneFile {
     std::vector<int32_t> plane_mat, box_mat, mat;
     double g[3], dt, damping;
     uint64_t n;
+    // scene version 2: moving boxes
+    uint32_t nmb = 0;
+    std::vector<double> mb_x, mb_q, mb_v, mb_w, mb_len;
+    std::vector<int32_t> mb_mat;
 };
 
 static bool read_scene(const char *path, SceneFile &s) {
@@ -107,6 +111,15 @@ static bool read_scene(const char *path, SceneFile &s) {
     rd(s.w, 3 * s.n);
     rd(s.r, s.n);
     rd(s.mat, s.n);
+    if (ver >= 2) {
+        f.read((char *)&s.nmb, 4);
+        rd(s.mb_x, 3 * (size_t)s.nmb);
+        rd(s.mb_q, 4 * (size_t)s.nmb);
+        rd(s.mb_v, 3 * (size_t)s.nmb);
+        rd(s.mb_w, 3 * (size_t)s.nmb);
+        rd(s.mb_len, 3 * (size_t)s.nmb);
+        rd(s.mb_mat, s.nmb);
+    }
     return (bool)f;
 }
 
@@ -145,6 +158,15 @@ static int run(const char *scene, const char *solver, const char *prec, int step
             }
         box->setFixed(true);
     }
+    std::vector<BoxID> moving;
+    for (uint32_t k = 0; k < sf.nmb; ++k) {
+        const double *x = &sf.mb_x[3 * k], *q = &sf.mb_q[4 * k], *l = &sf.mb_len[3 * k];
+        BoxID box = createBox(uid++, x[0], x[1], x[2], l[0], l[1], l[2], mid[sf.mb_mat[k]]);
+        box->setOrientation(q[0], q[1], q[2], q[3]);
+        box->setLinearVel(sf.mb_v[3 * k], sf.mb_v[3 * k + 1], sf.mb_v[3 * k + 2]);
+        box->setAngularVel(sf.mb_w[3 * k], sf.mb_w[3 * k + 1], sf.mb_w[3 * k + 2]);
+        moving.push_back(box);
+    }
     std::vector<SphereID> spheres;
     for (uint64_t i = 0; i < sf.n; ++i) {
         SphereID s = createSphere(uid++, sf.x[3 * i], sf.x[3 * i + 1], sf.x[3 * i + 2], sf.r[i],
@@ -158,7 +180,9 @@ static int run(const char *scene, const char *solver, const char *prec, int step
         world->run(first, sf.dt);
         double zsum = 0.0;
         for (SphereID s : spheres) zsum += s->getPosition()[2];
-        std::printf("mean z after %d steps: %.17g\n", first, zsum / (double)sf.n);
+        for (BoxID b : moving) zsum += b->getPosition()[2];
+        std::printf("mean z after %d steps: %.17g\n", first,
+                    zsum / (double)std::max<size_t>(1, sf.n + sf.nmb));
         for (int k = first; k < steps; ++k) world->simulationStep(sf.dt);
     } catch (const std::exception &e) {
         std::fprintf(stderr, "step failed: %s\n", e.what());
@@ -170,6 +194,16 @@ static int run(const char *scene, const char *solver, const char *prec, int step
             const Vec3 a = f == 0 ? s->getPosition() : f == 1 ? s->getLinearVel() : s->getAngularVel();
             res.insert(res.end(), {a[0], a[1], a[2]});
         }
+    // moving boxes: x, v, w (3 per box each), q (4 per box)
+    for (int f = 0; f < 3; ++f)
+        for (BoxID b : moving) {
+            const Vec3 a = f == 0 ? b->getPosition() : f == 1 ? b->getLinearVel() : b->getAngularVel();
+            res.insert(res.end(), {a[0], a[1], a[2]});
+        }
+    for (BoxID b : moving) {
+        const std::array<double, 4> q = b->getQuaternion();
+        res.insert(res.end(), q.begin(), q.end());
+    }
     std::ofstream o(out, std::ios::binary);
     o.write((const char *)res.data(), res.size() * sizeof(double));
     std::printf("ok\n");

@@ -114,3 +114,45 @@ def test_world_api_resumes_pe_checkpoint(driver, tmp_path):
     a = np.fromfile(out, "<f8").reshape(3, s.n, 3)
     assert rel_err(a[0], g["dem10_x"]) < 1e-12
     assert rel_err(a[1], g["dem10_v"]) < 1e-10
+
+
+def run_driver_boxes(driver, tmp_path, s, solver, prec, steps):
+    sp, out = str(tmp_path / "scene.bin"), str(tmp_path / "out.bin")
+    s.save(sp)
+    r = subprocess.run([driver, "run", sp, solver, prec, str(steps), out], capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    a = np.fromfile(out, "<f8")
+    n, m = s.n, s.nmbox
+    sph = a[:9 * n].reshape(3, n, 3)
+    b = a[9 * n:]
+    return sph, b[:9 * m].reshape(3, m, 3), b[9 * m:].reshape(m, 4)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["boxes27_tumbling", "boxes36_stack"])
+def test_world_api_moving_boxes_dem(driver, tmp_path, name):
+    """createBox without setFixed: the box moves (BoxTrait::move) and lands on pe's state."""
+    g = load_golden(name)
+    s = g["scene"]
+    sph, box, q = run_driver_boxes(driver, tmp_path, s, "dem", "fp64", 10)
+    e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(s)
+    e.step(s.dt, 10)
+    bx, bq, bv, bw = e.download_boxes()
+    e.close()
+    assert np.array_equal(box[0], bx) and np.array_equal(box[1], bv) and np.array_equal(q, bq)
+    assert rel_err(box[0], g["dem10_bx"]) < 1e-13
+    assert rel_err(q, g["dem10_bq"]) < 1e-13
+
+
+@pytest.mark.gpu
+def test_world_api_moving_boxes_hcsits(driver, tmp_path):
+    g = load_golden("boxes36_stack")
+    s = g["scene"]
+    sph, box, q = run_driver_boxes(driver, tmp_path, s, "hcsits", "fp64", 4)
+    e = Engine(solver=_abi.HCSITS, precision=_abi.FP64, relaxation_model=1,
+               max_iterations=100).load_scene(s)
+    e.step(s.dt, 4)
+    bx, bq, bv, bw = e.download_boxes()
+    e.close()
+    assert np.array_equal(box[0], bx) and np.array_equal(box[1], bv) and np.array_equal(q, bq)
