@@ -235,6 +235,10 @@ int main(int argc, char** argv) {
             for (World::Bodies::CastIterator<Sphere> it = world->begin<Sphere>();
                  it != world->end<Sphere>(); ++it)
                 read.push_back(*it);
+            g_mboxes.clear();
+            for (World::Bodies::CastIterator<Box> it = world->begin<Box>();
+                 it != world->end<Box>(); ++it)
+                if (!(*it)->isFixed()) g_mboxes.push_back(*it);
             const int steps = std::atoi(argv[4]);
             for (int k = 0; k < steps; ++k) world->simulationStep(s.dt);
             write_state(argv[5], read);

@@ -139,10 +139,11 @@ def read_peb(path: str) -> dict:
 
 
 def scene_bodies(scene, x=None, v=None, w=None, q=None,
-                 material_offset: int = PREDEFINED_MATERIALS) -> tuple:
+                 material_offset: int = PREDEFINED_MATERIALS, box_state=None) -> tuple:
     """The bodies of a pe_b200.scenes.Scene in the order pe creates them in the compiled
     reference's driver: spheres (system id = user id = index), then planes, then fixed
-    axis-aligned boxes; returns (bodies, next system id).  x, v, w, q override the state."""
+    axis-aligned boxes, then moving boxes; returns (bodies, next system id).  x, v, w, q
+    override the spheres' state, box_state = (x, q, v, w) the moving boxes'."""
     n = scene.n
     x = scene.x if x is None else x
     v = scene.v if v is None else v
@@ -159,22 +160,38 @@ def scene_bodies(scene, x=None, v=None, w=None, q=None,
         nrm, d = scene.planes[p, :3], scene.planes[p, 3]
         out.append(Body(PLANE, n + p, n + p, True, True, nrm * d, ident, np.zeros(3), np.zeros(3),
                         int(scene.plane_mat[p]) + material_offset))
-    for k in range(scene.boxes.shape[0]):
+    nb = scene.boxes.shape[0]
+    for k in range(nb):
         bx = scene.boxes[k]
         if not np.array_equal(bx[6:], np.eye(3).ravel()):
             raise ValueError("axis-aligned boxes only")
         out.append(Body(BOX, n + npl + k, n + npl + k, True, True, bx[:3].copy(), ident,
                         np.zeros(3), np.zeros(3), int(scene.box_mat[k]) + material_offset,
                         lengths=bx[3:6].copy()))
-    return out, n + npl + scene.boxes.shape[0]
+    # moving boxes, created after the fixed ones; state overrides as for the spheres
+    m = getattr(scene, "nmbox", 0)
+    bx_, bq_, bv_, bw_ = (scene.mbox_x, scene.mbox_q, scene.mbox_v, scene.mbox_w) if m else (
+        None, None, None, None)
+    if box_state is not None:
+        bx_, bq_, bv_, bw_ = box_state
+    for k in range(m):
+        sid = n + npl + nb + k
+        out.append(Body(BOX, sid, sid, True, False, np.asarray(bx_[k], float),
+                        np.asarray(bq_[k], float), np.asarray(bv_[k], float),
+                        np.asarray(bw_[k], float), int(scene.mbox_mat[k]) + material_offset,
+                        lengths=np.asarray(scene.mbox_len[k], float)))
+    return out, n + npl + nb + m
 
 
 def restore_scene(path: str, scene, material_offset: int = PREDEFINED_MATERIALS):
     """A copy of scene whose spheres are the checkpoint's (in system-id order), keeping the
-    scene's materials, planes and gravity; the checkpoint's boxes replace the scene's."""
+    scene's materials, planes and gravity; the checkpoint's fixed boxes replace the scene's
+    walls and its moving boxes the scene's moving boxes."""
     data = read_peb(path)
     sph = sorted([b for b in data["bodies"] if b.kind == SPHERE], key=lambda b: b.sid)
-    box = sorted([b for b in data["bodies"] if b.kind == BOX], key=lambda b: b.sid)
+    box = sorted([b for b in data["bodies"] if b.kind == BOX and b.fixed], key=lambda b: b.sid)
+    mov = sorted([b for b in data["bodies"] if b.kind == BOX and not b.fixed],
+                 key=lambda b: b.sid)
     s = scene.copy()
     s.x = np.array([b.x for b in sph]).reshape(-1, 3)
     s.v = np.array([b.v for b in sph]).reshape(-1, 3)
@@ -187,4 +204,10 @@ def restore_scene(path: str, scene, material_offset: int = PREDEFINED_MATERIALS)
     else:
         s.boxes = np.zeros((0, 15))
         s.box_mat = np.zeros(0, dtype=s.box_mat.dtype)
+    s.mbox_x = np.array([b.x for b in mov]).reshape(-1, 3)
+    s.mbox_q = np.array([b.q for b in mov]).reshape(-1, 4)
+    s.mbox_v = np.array([b.v for b in mov]).reshape(-1, 3)
+    s.mbox_w = np.array([b.w for b in mov]).reshape(-1, 3)
+    s.mbox_len = np.array([b.lengths for b in mov]).reshape(-1, 3)
+    s.mbox_mat = np.array([b.material - material_offset for b in mov], dtype=np.int32)
     return s

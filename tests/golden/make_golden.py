@@ -165,6 +165,24 @@ def box_goldens():
     box_golden("boxes36_stack", scenes.box_stack())
 
 
+def peb_box_fixture(steps=5):
+    """pe's own checkpoint of the tumbling-box scene (boxes27_tumbling) after `steps` DEM steps,
+    and that state (spheres and moving boxes)."""
+    s = scenes.tumbling_boxes(0)
+    keys = ("x", "v", "w", "q", "bx", "bv", "bw", "bq")
+    with tempfile.TemporaryDirectory() as tmp:
+        sp = os.path.join(tmp, "scene.bin")
+        s.save(sp)
+        peb = os.path.join(OUT, "peb_boxes27.peb")
+        subprocess.run([os.path.join(REF, "ref_dem"), "peb_write", sp, str(steps), peb], check=True)
+        st = run_steps_boxes("ref_dem", sp, s.n, s.nmbox, steps, tmp)
+    rec = {"scene": np.frombuffer(s.to_bytes(), np.uint8)}
+    rec.update(dict(zip(keys, st)))
+    path = os.path.join(OUT, "peb_boxes27.npz")
+    np.savez_compressed(path, **rec)
+    print(peb, os.path.getsize(peb), "bytes")
+
+
 def hertz_goldens():
     golden("hertz64_boxes", hertz_scene(1, with_boxes=True), dem_steps=(1, 10), hc=False,
            dem_exe="ref_dem_hertz")
@@ -183,6 +201,7 @@ if __name__ == "__main__":
         sys.exit(0)
     if sys.argv[1:] == ["boxes"]:
         box_goldens()
+        peb_box_fixture()
         sys.exit(0)
     golden("small64_boxes", scenes.small_random(1, n=64, with_boxes=True))
     golden("small64_planes", scenes.small_random(2, n=64, with_boxes=False))
@@ -198,3 +217,4 @@ if __name__ == "__main__":
     hertz_goldens()
     peb_fixture()
     box_goldens()
+    peb_box_fixture()
