@@ -13,12 +13,15 @@
 // the contact case by comparing depths that tie for aligned boxes (stacks), and pe's choice is
 // reproduced only when every product and sum rounds as in pe's FP64 code.
 //
-// Work layout.  Moving boxes are few next to the spheres; each box is one thread block that
-// walks the candidates of its scene (spheres, planes, fixed boxes, other moving boxes) with its
-// threads, so a box never needs the sphere grid and the result does not depend on scheduling:
-// every thread visits a fixed subset in a fixed order and the block reduces in a fixed tree.
-// Cost per step O(spheres x boxes) -- fine for pe's box scenes (stacks, dominoes, mixed
-// granular scenes with tens to thousands of boxes).
+// Work layout.  Each step first computes every box's rotation and bounding box and sorts the
+// boxes into a small uniform grid (one block; cells wide enough that bodies whose bounding
+// boxes overlap a box's sit in a neighbouring cell of the box's centre cell).  Each box is one
+// thread block that walks its candidates with its threads: the spheres in the cells of the
+// spheres' own grid that its bounding box covers, the scene's planes and fixed boxes, and the
+// moving boxes of the neighbouring box-grid cells.  The DEM force of the boxes on a sphere is
+// gathered by one warp per sphere over the neighbouring box-grid cells, for the spheres whose
+// cell has a box nearby.  Every thread or lane visits a fixed subset in a fixed order and sums
+// reduce in fixed trees, so results do not depend on scheduling.
 //
 // Contact ids inside this file: spheres 0..n-1 (index in the current buffers), moving box m
 // n + m, walls -(1 + global wall index) (planes first, then fixed boxes).
@@ -33,6 +36,9 @@ namespace peb {
 namespace {
 
 constexpr int kBoxBlk = 128;
+constexpr int kRowBatch = 256;       // rows of sphere-grid cells a box block stages at a time
+constexpr int kGridBlk = 1024;
+constexpr int kMaxBoxCells = 1 << 16;
 using V = V3<double>;
 
 struct BoxArgs {
@@ -51,6 +57,16 @@ struct BoxArgs {
     const int32_t *box_mat;
     const double *bx, *bq, *bv, *bw, *blen, *bprops;
     const int32_t *bmat, *bscene;
+    // the spheres' cell grid of the current step (slot -> body through sorted, or identity)
+    const int32_t *cell_start;
+    const int32_t *sorted;
+    // per-box rotation (9) and bounding box (6) of this step, and the box grid (k_box_grid)
+    const double *bR, *bbb;
+    const double *gparm;     // lo xyz, 1/h, then the three dims as doubles
+    const int32_t *gstart;   // cell -> first entry in gids
+    const int32_t *gids;     // boxes by cell, ascending index within a cell
+    const int32_t *gcell;    // box -> its cell
+    const uint32_t *gnear;   // bit per cell: a box in this cell or a neighbouring one
 };
 
 // an oriented box as the fine detection sees it
@@ -91,7 +107,7 @@ __device__ __forceinline__ double comp(V a, int i) { return i == 0 ? a.x : (i ==
 __device__ OBox moving_box(const BoxArgs &a, int32_t m) {
     OBox b;
     b.x = ld3(a.bx + 3 * m);
-    quat_to_rot(a.bq + 4 * m, b.R);
+    for (int k = 0; k < 9; ++k) b.R[k] = a.bR[9 * m + k];
     for (int k = 0; k < 3; ++k) {
         b.len[k] = a.blen[3 * m + k];
         b.hl[k] = 0.5 * b.len[k];
@@ -392,22 +408,62 @@ __device__ void collide_box_box(const OBox &p1, const OBox &p2, F &f) {
     }
 }
 
-// Every contact of moving box m, visited by thread tid of nthr: spheres of the box's scene,
-// the scene's planes, its fixed boxes and (all_pairs: every other / else: the later) moving
-// boxes of the scene.
+// the box grid cell of a point, clamped
+__device__ __forceinline__ void box_cell(const double *gp, double x, double y, double z, int &cx,
+                                         int &cy, int &cz) {
+    cx = clampi((int)floor((x - gp[0]) * gp[3]), 0, (int)gp[4] - 1);
+    cy = clampi((int)floor((y - gp[1]) * gp[3]), 0, (int)gp[5] - 1);
+    cz = clampi((int)floor((z - gp[2]) * gp[3]), 0, (int)gp[6] - 1);
+}
+
+// Every contact of moving box m, visited by thread tid of the nthr threads of a block (all of
+// them call it): the spheres in the cells of the spheres' grid that the box's bounding box,
+// grown by the largest radius, covers; the scene's planes and fixed boxes; and (all_pairs:
+// every other / else: the later) moving boxes of the scene in the neighbouring box-grid cells.
 template <typename F>
 __device__ void visit_box(const BoxArgs &a, int32_t m, int tid, int nthr, bool all_pairs, F &f) {
     const OBox B = moving_box(a, m);
-    double bb[6];
-    box_aabb(B, bb);
+    const double *bb = a.bbb + 6 * m;
     const int32_t sc = a.bscene[m];
     const SceneInfo &s = a.scenes[sc];
-    for (int64_t i = tid; i < a.n; i += nthr) {
-        if ((int32_t)(a.tag[i] >> 16) != sc) continue;
-        const double4 p = a.pr[i];
-        const double r = p.w + kContactThreshold;   // SphereBase.h:208-218
-        const double sb[6] = {p.x - r, p.y - r, p.z - r, p.x + r, p.y + r, p.z + r};
-        if (aabb_overlap(sb, bb)) collide_sphere_box((int32_t)i, p, B, f);
+    if (a.n > 0 && a.cell_start) {
+        // the covered cells come as rows along x (contiguous slots); the rows of a batch are
+        // laid end to end so that the threads share the spheres evenly
+        __shared__ int32_t rbeg[kRowBatch], rcnt[kRowBatch];
+        const double reach = s.rmax + kContactThreshold;
+        int x0, y0, z0, x1, y1, z1;
+        cell_coords(s, bb[0] - reach, bb[1] - reach, bb[2] - reach, x0, y0, z0);
+        cell_coords(s, bb[3] + reach, bb[4] + reach, bb[5] + reach, x1, y1, z1);
+        const int ny = y1 - y0 + 1, nrows = ny * (z1 - z0 + 1);
+        for (int r0 = 0; r0 < nrows; r0 += kRowBatch) {
+            const int nr = min(kRowBatch, nrows - r0);
+            __syncthreads();
+            for (int r = tid; r < nr; r += nthr) {
+                const int y = y0 + (r0 + r) % ny, z = z0 + (r0 + r) / ny;
+                const int64_t c0 = cell_key(s, x0, y, z), c1 = cell_key(s, x1, y, z) + 1;
+                rbeg[r] = a.cell_start[c0];
+                rcnt[r] = a.cell_start[c1] - rbeg[r];
+            }
+            __syncthreads();
+            if (tid == 0)
+                for (int r = 1; r < nr; ++r) rcnt[r] += rcnt[r - 1];   // inclusive prefix
+            __syncthreads();
+            const int total = rcnt[nr - 1];
+            for (int k = tid; k < total; k += nthr) {
+                int lo = 0, hi = nr - 1;   // the first row whose prefix exceeds k
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (rcnt[mid] > k) hi = mid;
+                    else lo = mid + 1;
+                }
+                const int slot = rbeg[lo] + k - (lo > 0 ? rcnt[lo - 1] : 0);
+                const int32_t i = a.sorted ? a.sorted[slot] : slot;
+                const double4 p = a.pr[i];
+                const double r = p.w + kContactThreshold;   // SphereBase.h:208-218
+                const double sb[6] = {p.x - r, p.y - r, p.z - r, p.x + r, p.y + r, p.z + r};
+                if (aabb_overlap(sb, bb)) collide_sphere_box(i, p, B, f);
+            }
+        }
     }
     for (int p = tid; p < s.nplanes; p += nthr)
         collide_box_plane(B, a.planes[s.plane_begin + p], -(1 + s.plane_begin + p), f);
@@ -417,12 +473,37 @@ __device__ void visit_box(const BoxArgs &a, int32_t m, int tid, int nthr, bool a
         box_aabb(W, wb);
         if (aabb_overlap(bb, wb)) collide_box_box(B, W, f);
     }
-    for (int j = s.mbox_begin + tid; j < s.mbox_begin + s.nmbox; j += nthr) {
-        if (j == m || (!all_pairs && j < m)) continue;
-        const OBox C = moving_box(a, j);
-        double cb[6];
-        box_aabb(C, cb);
-        if (aabb_overlap(bb, cb)) collide_box_box(B, C, f);
+    // the 27 neighbouring box-grid cells (z, then y, then x) staged at once; candidate g of
+    // their concatenation goes to thread g mod nthr
+    __shared__ int32_t nb_beg[27], nb_pre[27];
+    __syncthreads();
+    if (tid < 27) {
+        const double *gp = a.gparm;
+        const int gx = (int)gp[4], gy = (int)gp[5], gz = (int)gp[6];
+        const int32_t cm = a.gcell[m];
+        const int x = cm % gx + tid % 3 - 1, y = (cm / gx) % gy + (tid / 3) % 3 - 1,
+                  z = cm / (gx * gy) + tid / 9 - 1;
+        int32_t b0 = 0, cnt = 0;
+        if (x >= 0 && y >= 0 && z >= 0 && x < gx && y < gy && z < gz) {
+            const int32_t c = (z * gy + y) * gx + x;
+            b0 = a.gstart[c];
+            cnt = a.gstart[c + 1] - b0;
+        }
+        nb_beg[tid] = b0;
+        nb_pre[tid] = cnt;
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int i = 1; i < 27; ++i) nb_pre[i] += nb_pre[i - 1];   // inclusive prefix
+    __syncthreads();
+    const int total = nb_pre[26];
+    for (int g = tid; g < total; g += nthr) {
+        int i = 0;
+        while (nb_pre[i] <= g) ++i;
+        const int32_t j = a.gids[nb_beg[i] + g - (i > 0 ? nb_pre[i - 1] : 0)];
+        if (j == m || (!all_pairs && j < m) || a.bscene[j] != sc) continue;
+        if (!aabb_overlap(bb, a.bbb + 6 * j)) continue;
+        collide_box_box(B, moving_box(a, j), f);
     }
 }
 
@@ -479,34 +560,98 @@ __device__ bool dem_force(const BoxArgs &a, int32_t b1, int32_t b2, V gpos, V n,
 }
 
 // ---- DEM ---------------------------------------------------------------------------------------
-// the boxes' forces on sphere b (the sphere is body 1 of a sphere/box contact)
-__global__ void k_sphere_box_forces(BoxArgs a, double *ext) {
+// spheres in a box-grid cell with a box nearby go to the list; the others get zero force
+__global__ void k_sphere_box_near(BoxArgs a, double *ext, int32_t *list, int32_t *count) {
     const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= a.n) return;
     const double4 p = a.pr[b];
     const SceneInfo &s = a.scenes[a.tag[b] >> 16];
-    V F = v3(0.0, 0.0, 0.0), T = F;
-    const V x = v3(p.x, p.y, p.z);
-    const double r = p.w + kContactThreshold;
-    const double sb[6] = {p.x - r, p.y - r, p.z - r, p.x + r, p.y + r, p.z + r};
-    auto f = [&](int32_t b1, int32_t b2, V gpos, V n, double dist, int kind) {
-        V fN, fT;
-        if (!dem_force(a, b1, b2, gpos, n, dist, kind, fN, fT)) return;
-        const V r1 = gpos - x;
-        F = F + fN;
-        T = T + cross(r1, fN);
-        F = F + fT;
-        T = T + cross(r1, fT);
-    };
-    for (int32_t m = s.mbox_begin; m < s.mbox_begin + s.nmbox; ++m) {
-        const OBox B = moving_box(a, m);
-        double bb[6];
-        box_aabb(B, bb);
-        if (aabb_overlap(sb, bb)) collide_sphere_box((int32_t)b, p, B, f);
+    const double *gp = a.gparm;
+    // a sphere more than one cell outside the box grid touches no box (boxes' centres lie in
+    // the grid and the cells are wider than any box plus a sphere)
+    const double ux = floor((p.x - gp[0]) * gp[3]), uy = floor((p.y - gp[1]) * gp[3]),
+                 uz = floor((p.z - gp[2]) * gp[3]);
+    const bool inside = ux >= -1.0 && ux <= gp[4] && uy >= -1.0 && uy <= gp[5] && uz >= -1.0 &&
+                        uz <= gp[6];
+    int cx, cy, cz;
+    box_cell(gp, p.x, p.y, p.z, cx, cy, cz);
+    const int32_t own = (cz * (int)gp[5] + cy) * (int)gp[4] + cx;
+    if (s.nmbox > 0 && inside && ((a.gnear[own >> 5] >> (own & 31)) & 1u)) {
+        list[atomicAdd(count, 1)] = (int32_t)b;
+    } else {
+        double *e = ext + 6 * b;
+        for (int k = 0; k < 6; ++k) e[k] = 0.0;
     }
-    double *e = ext + 6 * b;
-    e[0] = F.x; e[1] = F.y; e[2] = F.z;
-    e[3] = T.x; e[4] = T.y; e[5] = T.z;
+}
+
+// The boxes' forces on the listed spheres (each sphere is body 1 of its sphere/box contacts),
+// one warp per sphere: lane l takes the candidates l, l + 32, ... of the neighbouring box-grid
+// cells (cell by cell, ascending box index within a cell) and a fixed butterfly sums the lanes,
+// so the result depends neither on scheduling nor on the list's order.
+__global__ void k_sphere_box_forces(BoxArgs a, double *ext, const int32_t *list,
+                                    const int32_t *count) {
+    __shared__ int32_t nb_beg[8][32], nb_pre[8][32];   // per warp of the 256-thread block
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int32_t nl = *count;
+    for (int64_t li = warp0; li < nl; li += nwarps) {
+        __syncwarp();
+        const int32_t b = list[li];
+        const double4 p = a.pr[b];
+        V F = v3(0.0, 0.0, 0.0), T = F;
+        const V x = v3(p.x, p.y, p.z);
+        const double r = p.w + kContactThreshold;
+        const double sb[6] = {p.x - r, p.y - r, p.z - r, p.x + r, p.y + r, p.z + r};
+        auto f = [&](int32_t b1, int32_t b2, V gpos, V n, double dist, int kind) {
+            V fN, fT;
+            if (!dem_force(a, b1, b2, gpos, n, dist, kind, fN, fT)) return;
+            const V r1 = gpos - x;
+            F = F + fN;
+            T = T + cross(r1, fN);
+            F = F + fT;
+            T = T + cross(r1, fT);
+        };
+        const int32_t sc = (int32_t)(a.tag[b] >> 16);
+        const double *gp = a.gparm;
+        const int gx = (int)gp[4], gy = (int)gp[5], gz = (int)gp[6];
+        int cx, cy, cz;
+        box_cell(gp, p.x, p.y, p.z, cx, cy, cz);
+        // lanes 0..26 load the 27 neighbouring cells (z, then y, then x); candidate g of their
+        // concatenation goes to lane g mod 32
+        int32_t b0 = 0, cnt = 0;
+        if (lane < 27) {
+            const int xx = cx + lane % 3 - 1, y = cy + (lane / 3) % 3 - 1, z = cz + lane / 9 - 1;
+            if (xx >= 0 && y >= 0 && z >= 0 && xx < gx && y < gy && z < gz) {
+                const int32_t c = (z * gy + y) * gx + xx;
+                b0 = a.gstart[c];
+                cnt = a.gstart[c + 1] - b0;
+            }
+        }
+        int32_t pre = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t u = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += u;
+        }
+        nb_beg[wib][lane] = b0;
+        nb_pre[wib][lane] = pre;
+        __syncwarp();
+        const int32_t total = nb_pre[wib][26];
+        for (int g = lane; g < total; g += 32) {
+            int i = 0;
+            while (nb_pre[wib][i] <= g) ++i;
+            const int32_t m = a.gids[nb_beg[wib][i] + g - (i > 0 ? nb_pre[wib][i - 1] : 0)];
+            if (a.bscene[m] != sc || !aabb_overlap(sb, a.bbb + 6 * m)) continue;
+            collide_sphere_box(b, p, moving_box(a, m), f);
+        }
+        double v[6] = {F.x, F.y, F.z, T.x, T.y, T.z};
+        for (int o = 16; o > 0; o >>= 1)
+            for (int q = 0; q < 6; ++q) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        if (lane == 0) {
+            double *e = ext + 6 * (int64_t)b;
+            for (int q = 0; q < 6; ++q) e[q] = v[q];
+        }
+    }
 }
 
 __device__ void block_sum6(double *v, double (*sh)[6]) {
@@ -761,6 +906,153 @@ __global__ void __launch_bounds__(kBoxBlk) k_box_list(BoxArgs a, const int32_t *
     visit_box(a, m, threadIdx.x, blockDim.x, false, write);
 }
 
+// per-box rotation and bounding box of this step
+__global__ void k_box_geom(int32_t m, const double *x, const double *q, const double *len,
+                           double *R, double *bbb) {
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    OBox b;
+    b.x = ld3(x + 3 * k);
+    quat_to_rot(q + 4 * k, b.R);
+    for (int a = 0; a < 3; ++a) b.len[a] = len[3 * k + a];
+    for (int a = 0; a < 9; ++a) R[9 * k + a] = b.R[a];
+    box_aabb(b, bbb + 6 * k);
+}
+
+// The box grid, built by one block: cells at least two box half-extents and one half-extent
+// plus the largest sphere radius wide, so a sphere or a box whose bounding box overlaps a box's
+// lies in a neighbouring cell of that box's centre cell; at most a few cells per box.  Boxes are
+// counted, scanned and filled into their cells, each cell is put in ascending box order, and a
+// bit per cell marks the cells with a box in or next to them.
+__global__ void __launch_bounds__(kGridBlk) k_box_grid(int32_t m, const double *bbb, double rmax,
+                                                       double *gp, int32_t *gcell,
+                                                       int32_t *gstart, int32_t *gfill,
+                                                       int32_t *gids, uint32_t *gnear) {
+    __shared__ double rlo[3][kGridBlk / 32], rhi[3][kGridBlk / 32], rext[kGridBlk / 32];
+    __shared__ int32_t part[kGridBlk];
+    __shared__ int32_t s_ncell;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int64_t want = 8 * (int64_t)m > 512 ? 8 * (int64_t)m : 512;
+    const int64_t max_cells = want < kMaxBoxCells ? want : kMaxBoxCells;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double ext = 0.0;
+    for (int32_t k = t; k < m; k += kGridBlk) {
+        const double *b = bbb + 6 * k;
+        for (int a = 0; a < 3; ++a) {
+            const double c = 0.5 * (b[a] + b[3 + a]);
+            lo[a] = fmin(lo[a], c);
+            hi[a] = fmax(hi[a], c);
+            ext = fmax(ext, 0.5 * (b[3 + a] - b[a]));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = fmin(lo[a], __shfl_down_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmax(hi[a], __shfl_down_sync(0xffffffffu, hi[a], o));
+        }
+        ext = fmax(ext, __shfl_down_sync(0xffffffffu, ext, o));
+    }
+    if (lane == 0) {
+        for (int a = 0; a < 3; ++a) {
+            rlo[a][wid] = lo[a];
+            rhi[a][wid] = hi[a];
+        }
+        rext[wid] = ext;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int w = 1; w < kGridBlk / 32; ++w) {
+            for (int a = 0; a < 3; ++a) {
+                rlo[a][0] = fmin(rlo[a][0], rlo[a][w]);
+                rhi[a][0] = fmax(rhi[a][0], rhi[a][w]);
+            }
+            rext[0] = fmax(rext[0], rext[w]);
+        }
+        double h = fmax(2.0 * rext[0], rext[0] + rmax) + 4.0 * kContactThreshold;
+        if (!(h > 0.0 && h < 1e300)) h = 1.0;
+        double span[3];
+        for (int a = 0; a < 3; ++a) {
+            const double sp = rhi[a][0] - rlo[a][0];
+            span[a] = (sp >= 0.0 && sp < 1e300) ? sp : 0.0;   // non-finite states: one cell
+        }
+        int dim[3] = {1, 1, 1};
+        int64_t ncell = 1;
+        for (int it = 0; it < 256; ++it) {
+            ncell = 1;
+            for (int a = 0; a < 3; ++a) {
+                dim[a] = (int)fmin(fmax(floor(span[a] / h) + 1.0, 1.0), 4096.0);
+                ncell *= dim[a];
+            }
+            if (ncell <= max_cells) break;
+            h *= 1.26;
+        }
+        if (ncell > max_cells) {   // spans beyond any grid: every box in one cell
+            dim[0] = dim[1] = dim[2] = 1;
+            ncell = 1;
+        }
+        for (int a = 0; a < 3; ++a) gp[a] = rlo[a][0];
+        gp[3] = 1.0 / h;
+        for (int a = 0; a < 3; ++a) gp[4 + a] = dim[a];
+        s_ncell = (int32_t)ncell;
+    }
+    __syncthreads();
+    const int32_t ncell = s_ncell;
+    for (int32_t c = t; c <= ncell; c += kGridBlk) gstart[c] = 0;
+    for (int32_t w = t; w <= (ncell >> 5); w += kGridBlk) gnear[w] = 0u;
+    __syncthreads();
+    const int gx = (int)gp[4], gy = (int)gp[5], gz = (int)gp[6];
+    for (int32_t k = t; k < m; k += kGridBlk) {
+        const double *b = bbb + 6 * k;
+        int cx, cy, cz;
+        box_cell(gp, 0.5 * (b[0] + b[3]), 0.5 * (b[1] + b[4]), 0.5 * (b[2] + b[5]), cx, cy, cz);
+        const int32_t c = (cz * gy + cy) * gx + cx;
+        gcell[k] = c;
+        atomicAdd(&gstart[c + 1], 1);
+        for (int z = max(cz - 1, 0); z <= min(cz + 1, gz - 1); ++z)
+            for (int y = max(cy - 1, 0); y <= min(cy + 1, gy - 1); ++y)
+                for (int x = max(cx - 1, 0); x <= min(cx + 1, gx - 1); ++x) {
+                    const int32_t nc = (z * gy + y) * gx + x;
+                    atomicOr(&gnear[nc >> 5], 1u << (nc & 31));
+                }
+    }
+    __syncthreads();
+    // exclusive scan of the counts: each thread a contiguous chunk, then the chunk totals
+    const int32_t chunk = (ncell + kGridBlk) / kGridBlk;
+    const int32_t b0 = t * chunk + 1, b1 = min(b0 + chunk, ncell + 1);
+    int32_t sum = 0;
+    for (int32_t c = b0; c < b1; ++c) sum += gstart[c];
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < kGridBlk; o <<= 1) {
+        const int32_t u = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += u;
+        __syncthreads();
+    }
+    int32_t run = t > 0 ? part[t - 1] : 0;
+    for (int32_t c = b0; c < b1; ++c) {
+        run += gstart[c];
+        gstart[c] = run;
+    }
+    __syncthreads();
+    for (int32_t c = t; c < ncell; c += kGridBlk) gfill[c] = gstart[c];
+    __syncthreads();
+    for (int32_t k = t; k < m; k += kGridBlk) gids[atomicAdd(&gfill[gcell[k]], 1)] = k;
+    __syncthreads();
+    for (int32_t c = t; c < ncell; c += kGridBlk) {   // ascending box order in each cell
+        const int32_t e0 = gstart[c], e1 = gstart[c + 1];
+        for (int32_t i = e0 + 1; i < e1; ++i) {
+            const int32_t v = gids[i];
+            int32_t j = i - 1;
+            while (j >= e0 && gids[j] > v) {
+                gids[j + 1] = gids[j];
+                --j;
+            }
+            gids[j + 1] = v;
+        }
+    }
+}
+
 BoxArgs box_args(Ctx *c) {
     BoxArgs a;
     a.n = c->n;
@@ -784,7 +1076,29 @@ BoxArgs box_args(Ctx *c) {
     a.bprops = c->mb.props;
     a.bmat = c->mb.mat;
     a.bscene = c->mb.scene;
+    a.cell_start = c->cell_start;
+    a.sorted = nullptr;
+    a.bR = c->mb.R;
+    a.bbb = c->mb.aabb;
+    a.gparm = c->mb.gparm;
+    a.gstart = c->mb.gstart;
+    a.gids = c->mb.gids;
+    a.gcell = c->mb.gcell;
+    a.gnear = c->mb.gnear;
     return a;
+}
+
+// this step's box rotations, bounding boxes and box grid
+int box_geometry(Ctx *c) {
+    MBoxBuf &b = c->mb;
+    k_box_geom<<<grid_for(b.m, 128), 128, 0, c->stream>>>(b.m, b.x, b.q, b.len, b.R, b.aabb);
+    PEB_LAUNCHED(c);
+    double rmax = 0.0;
+    for (const SceneInfo &s : c->scenes) rmax = std::max(rmax, s.rmax);
+    k_box_grid<<<1, kGridBlk, 0, c->stream>>>(b.m, b.aabb, c->n > 0 ? rmax : 0.0, b.gparm, b.gcell,
+                                              b.gstart, b.gfill, b.gids, b.gnear);
+    PEB_LAUNCHED(c);
+    return PE_B200_OK;
 }
 
 // exclusive scan of cnt[0..m) into cnt[0..m], small m, on the host (the counts come back for
@@ -841,6 +1155,8 @@ void mbox_free(Ctx *c) {
     cudaFree(b.mat);
     cudaFree(b.cnt);
     cudaFree(b.ext);
+    cudaFree(b.R);
+    cudaFree(b.gstart);
     b = MBoxBuf();
 }
 
@@ -857,6 +1173,16 @@ int mbox_upload(Ctx *c, int32_t m, const double *x, const double *q, const doubl
         PEB_CUDA(c, cudaMalloc(&b.len, 11 * nm * sizeof(double)));
         PEB_CUDA(c, cudaMalloc(&b.mat, 2 * nm * sizeof(int32_t)));
         PEB_CUDA(c, cudaMalloc(&b.cnt, (nm + 2) * sizeof(int32_t)));
+        // rotations, bounding boxes, grid parameters; grid cells, box lists, neighbour bits
+        PEB_CUDA(c, cudaMalloc(&b.R, (15 * nm + 8) * sizeof(double)));
+        b.aabb = b.R + 9 * nm;
+        b.gparm = b.aabb + 6 * nm;
+        const size_t cells = (size_t)kMaxBoxCells + 2;
+        PEB_CUDA(c, cudaMalloc(&b.gstart, (2 * cells + 2 * nm + cells / 32 + 2) * sizeof(int32_t)));
+        b.gfill = b.gstart + cells;
+        b.gids = b.gfill + cells;
+        b.gcell = b.gids + nm;
+        b.gnear = (uint32_t *)(b.gcell + nm);
         b.q = b.x + 3 * nm;
         b.v = b.q + 4 * nm;
         b.w = b.v + 3 * nm;
@@ -916,15 +1242,26 @@ int mbox_dem(Ctx *c, double dt) {
     MBoxBuf &b = c->mb;
     if (b.m == 0) return PE_B200_OK;
     const int64_t n = c->n;
-    if (b.ext_cap < n) {
+    const size_t nn = (size_t)std::max<int64_t>(n, 1);
+    if (b.ext_cap < n || !b.ext) {
         cudaFree(b.ext);
         b.ext = nullptr;
-        PEB_CUDA(c, cudaMalloc(&b.ext, (size_t)std::max<int64_t>(n, 1) * 6 * sizeof(double)));
+        PEB_CUDA(c, cudaMalloc(&b.ext, nn * 6 * sizeof(double) + (nn + 2) * sizeof(int32_t)));
         b.ext_cap = n;
     }
-    const BoxArgs a = box_args(c);
+    int32_t *near_list = (int32_t *)(b.ext + 6 * nn);
+    int32_t *near_count = near_list + nn;
+    int rc = box_geometry(c);
+    if (rc) return rc;
+    BoxArgs a = box_args(c);
+    a.sorted = c->sorted;   // the grid step leaves the state in body order
     if (n > 0) {
-        k_sphere_box_forces<<<grid_for(n, 256), 256, 0, c->stream>>>(a, b.ext);
+        PEB_CUDA(c, cudaMemsetAsync(near_count, 0, sizeof(int32_t), c->stream));
+        k_sphere_box_near<<<grid_for(n, 256), 256, 0, c->stream>>>(a, b.ext, near_list, near_count);
+        PEB_LAUNCHED(c);
+        const int64_t warps = std::min<int64_t>(n, (int64_t)c->sm_count * 64);
+        k_sphere_box_forces<<<(unsigned)((warps + 7) / 8), 256, 0, c->stream>>>(a, b.ext, near_list,
+                                                                              near_count);
         PEB_LAUNCHED(c);
     }
     const int has_drag = c->p.damping < 1.0;
@@ -949,6 +1286,8 @@ int mbox_hc_count(Ctx *c, int32_t *total) {
     *total = 0;
     const MBoxBuf &b = c->mb;
     if (b.m == 0) return PE_B200_OK;
+    int rc = box_geometry(c);   // the state is in slot order here: sorted is the identity
+    if (rc) return rc;
     k_box_count<<<b.m, kBoxBlk, 0, c->stream>>>(box_args(c), b.cnt);
     PEB_LAUNCHED(c);
     return scan_counts(c, b.m, total);
@@ -981,10 +1320,14 @@ int mbox_find_contacts(Ctx *c, std::vector<int64_t> &ids, std::vector<double> &g
     ids.clear();
     geom.clear();
     if (b.m == 0) return PE_B200_OK;
-    k_box_count<<<b.m, kBoxBlk, 0, c->stream>>>(box_args(c), b.cnt);
+    int rc = box_geometry(c);
+    if (rc) return rc;
+    BoxArgs a = box_args(c);
+    a.sorted = c->sorted;   // the current state, binned by the grid just sorted
+    k_box_count<<<b.m, kBoxBlk, 0, c->stream>>>(a, b.cnt);
     PEB_LAUNCHED(c);
     int32_t total = 0;
-    int rc = scan_counts(c, b.m, &total);
+    rc = scan_counts(c, b.m, &total);
     if (rc) return rc;
     if (total == 0) return PE_B200_OK;
     int64_t *d_ids = nullptr;
@@ -993,8 +1336,8 @@ int mbox_find_contacts(Ctx *c, std::vector<int64_t> &ids, std::vector<double> &g
     if (e == cudaSuccess) e = cudaMalloc(&d_geom, (size_t)total * 7 * sizeof(double));
     const int64_t total_walls = (int64_t)(c->planes.size() / 4 + c->boxes.size() / 15);
     if (e == cudaSuccess) {
-        k_box_list<<<b.m, kBoxBlk, 0, c->stream>>>(box_args(c), b.cnt, total, c->n, total_walls,
-                                                   d_ids, d_geom);
+        k_box_list<<<b.m, kBoxBlk, 0, c->stream>>>(a, b.cnt, total, c->n, total_walls, d_ids,
+                                                   d_geom);
         c->launches++;
         e = cudaGetLastError();
     }

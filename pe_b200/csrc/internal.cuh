@@ -94,8 +94,14 @@ struct MBoxBuf {
     double *props = nullptr;   // 8 per box
     int32_t *mat = nullptr, *scene = nullptr;
     int32_t *cnt = nullptr;    // contacts per box / offsets (m + 2)
-    double *ext = nullptr;     // DEM: force and torque of the boxes on each sphere (6 per body)
+    double *ext = nullptr;     // DEM: force and torque of the boxes on each sphere (6 per body),
+                               // then the list of spheres near a box (n + 2 ints)
     int64_t ext_cap = 0;
+    // per step: rotations (9 per box), bounding boxes (6 per box) and the box grid
+    double *R = nullptr, *aabb = nullptr;
+    double *gparm = nullptr;   // lo xyz, 1/h, dims
+    int32_t *gstart = nullptr, *gfill = nullptr, *gids = nullptr, *gcell = nullptr;
+    uint32_t *gnear = nullptr; // bit per cell: a box in it or in a neighbouring cell
 };
 
 // Verlet neighbour lists of the DEM step (dem_list.cu): every pair closer than r_i + r_j + skin
