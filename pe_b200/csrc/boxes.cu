@@ -229,35 +229,41 @@ __device__ void intersect_lines(V o1, V d1, V o2, V d2, double &s, double &t) {
     t = (b * dot(d1, d1) + dd * a) * isqrlen;
 }
 
-// the nine edge/edge axes in pe's order (au x bu, au x bv, ..., aw x bw): term1 =
-// rPos[p0]*rR[p1] - rPos[p2]*rR[p3], term2 = hl1[h0]*rQ[q0] + hl1[h1]*rQ[q1], term3 =
-// hl2[h2]*rQ[q2] + hl2[h3]*rQ[q3], axis length from rR[s0], rR[s1], zero axis component
-__constant__ int8_t kEdgeAxes[9][15] = {
-    {2, 3, 1, 6, 1, 6, 2, 3, 2, 1, 1, 2, 6, 3, 0}, {2, 4, 1, 7, 1, 7, 2, 4, 0, 2, 2, 0, 7, 4, 0},
-    {2, 5, 1, 8, 1, 8, 2, 5, 1, 0, 0, 1, 8, 5, 0}, {0, 6, 2, 0, 2, 0, 0, 6, 2, 4, 1, 5, 6, 0, 1},
-    {0, 7, 2, 1, 2, 1, 0, 7, 0, 5, 2, 3, 7, 1, 1}, {0, 8, 2, 2, 2, 2, 0, 8, 1, 3, 0, 4, 8, 2, 1},
-    {1, 0, 0, 3, 0, 3, 1, 0, 2, 7, 1, 8, 3, 0, 2}, {1, 1, 0, 4, 0, 4, 1, 1, 0, 8, 2, 6, 4, 1, 2},
-    {1, 2, 0, 5, 0, 5, 1, 2, 1, 6, 0, 7, 5, 2, 2}};
+// component i of (a, b, c) and the vector with component ix = vx, iy = vy and the remaining
+// one vz, both by selects: runtime axis indices then need no indexed local arrays
+__device__ __forceinline__ double sel3(int i, double a, double b, double c) {
+    return i == 0 ? a : (i == 1 ? b : c);
+}
+__device__ __forceinline__ double sel3(int i, V v) { return sel3(i, v.x, v.y, v.z); }
+__device__ __forceinline__ V perm3(int ix, double vx, int iy, double vy, double vz) {
+    return v3(ix == 0 ? vx : (iy == 0 ? vy : vz), ix == 1 ? vx : (iy == 1 ? vy : vz),
+              ix == 2 ? vx : (iy == 2 ? vy : vz));
+}
 
 // MaxContacts.h:867-2250
 template <typename F>
 __device__ void collide_box_box(const OBox &p1, const OBox &p2, F &f) {
-    const OBox &b1 = (p2.key < p1.key) ? p2 : p1;
-    const OBox &b2 = (p2.key < p1.key) ? p1 : p2;
+    const bool swp = p2.key < p1.key;
+    const OBox b1 = swp ? p2 : p1;
+    const OBox b2 = swp ? p1 : p2;
     double maxDepth = -1.79769313486231570815e308;
     bool invertNormal = false;
     int contactCase = 0;
     V contactNormal = v3(0.0, 0.0, 0.0), normal_c = contactNormal;
     const double *R1 = b1.R, *R2 = b2.R;
     double rR[9], rQ[9];
+#pragma unroll
     for (int i = 0; i < 3; ++i)
+#pragma unroll
         for (int j = 0; j < 3; ++j)
             rR[3 * i + j] = R1[i] * R2[j] + R1[3 + i] * R2[3 + j] + R1[6 + i] * R2[6 + j];
+#pragma unroll
     for (int k = 0; k < 9; ++k) rQ[k] = fabs(rR[k]);
     const V rp = rt_mulv(R1, b2.x - b1.x);
     const double rPos[3] = {rp.x, rp.y, rp.z};
     const double *hl1 = b1.hl, *hl2 = b2.hl;
     // the face axes of box 1 (MaxContacts.h:905-970)
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         const double term1 = fabs(rPos[i]) - (hl1[i] + hl2[0] * rQ[3 * i] + hl2[1] * rQ[3 * i + 1] +
                                                hl2[2] * rQ[3 * i + 2]);
@@ -270,6 +276,7 @@ __device__ void collide_box_box(const OBox &p1, const OBox &p2, F &f) {
         }
     }
     // the face axes of box 2
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
         const double term1 = rPos[0] * rR[j] + rPos[1] * rR[3 + j] + rPos[2] * rR[6 + j];
         const double term2 =
@@ -282,9 +289,18 @@ __device__ void collide_box_box(const OBox &p1, const OBox &p2, F &f) {
             invertNormal = term1 < 0.0;
         }
     }
-    // the edge/edge axes
+    // the nine edge/edge axes in pe's order (au x bu, au x bv, ..., aw x bw): term1 =
+    // rPos[p0]*rR[p1] - rPos[p2]*rR[p3], term2 = hl1[h0]*rQ[q0] + hl1[h1]*rQ[q1], term3 =
+    // hl2[h2]*rQ[q2] + hl2[h3]*rQ[q3], axis length from rR[s0], rR[s1], zero axis component
+    constexpr int8_t E[9][15] = {
+        {2, 3, 1, 6, 1, 6, 2, 3, 2, 1, 1, 2, 6, 3, 0}, {2, 4, 1, 7, 1, 7, 2, 4, 0, 2, 2, 0, 7, 4, 0},
+        {2, 5, 1, 8, 1, 8, 2, 5, 1, 0, 0, 1, 8, 5, 0}, {0, 6, 2, 0, 2, 0, 0, 6, 2, 4, 1, 5, 6, 0, 1},
+        {0, 7, 2, 1, 2, 1, 0, 7, 0, 5, 2, 3, 7, 1, 1}, {0, 8, 2, 2, 2, 2, 0, 8, 1, 3, 0, 4, 8, 2, 1},
+        {1, 0, 0, 3, 0, 3, 1, 0, 2, 7, 1, 8, 3, 0, 2}, {1, 1, 0, 4, 0, 4, 1, 1, 0, 8, 2, 6, 4, 1, 2},
+        {1, 2, 0, 5, 0, 5, 1, 2, 1, 6, 0, 7, 5, 2, 2}};
+#pragma unroll
     for (int e = 0; e < 9; ++e) {
-        const int8_t *c = kEdgeAxes[e];
+        const int8_t *c = E[e];
         const double term1 = rPos[c[0]] * rR[c[1]] - rPos[c[2]] * rR[c[3]];
         const double term2 = hl1[c[4]] * rQ[c[5]] + hl1[c[6]] * rQ[c[7]];
         const double term3 = hl2[c[8]] * rQ[c[9]] + hl2[c[10]] * rQ[c[11]];
@@ -310,16 +326,18 @@ __device__ void collide_box_box(const OBox &p1, const OBox &p2, F &f) {
 
     if (contactCase > 6) {   // edge/edge, MaxContacts.h:1343-1417
         V sg = rt_mulv(R1, contactNormal);
-        V sv = v3(comp(sg, 0) > 0.0 ? hl1[0] : -hl1[0], comp(sg, 1) > 0.0 ? hl1[1] : -hl1[1],
-                  comp(sg, 2) > 0.0 ? hl1[2] : -hl1[2]);
+        V sv = v3(sg.x > 0.0 ? hl1[0] : -hl1[0], sg.y > 0.0 ? hl1[1] : -hl1[1],
+                  sg.z > 0.0 ? hl1[2] : -hl1[2]);
         V pB1 = b1.x + r_mulv(R1, sv);
         sg = rt_mulv(R2, contactNormal);
-        sv = v3(comp(sg, 0) > 0.0 ? -hl2[0] : hl2[0], comp(sg, 1) > 0.0 ? -hl2[1] : hl2[1],
-                comp(sg, 2) > 0.0 ? -hl2[2] : hl2[2]);
+        sv = v3(sg.x > 0.0 ? -hl2[0] : hl2[0], sg.y > 0.0 ? -hl2[1] : hl2[1],
+                sg.z > 0.0 ? -hl2[2] : hl2[2]);
         V pB2 = b2.x + r_mulv(R2, sv);
         const int ia = (contactCase - 7) / 3, ib = (contactCase - 7) % 3;
-        const V ua = v3(R1[ia], R1[ia + 3], R1[ia + 6]);
-        const V ub = v3(R2[ib], R2[ib + 3], R2[ib + 6]);
+        const V ua = v3(sel3(ia, R1[0], R1[1], R1[2]), sel3(ia, R1[3], R1[4], R1[5]),
+                        sel3(ia, R1[6], R1[7], R1[8]));
+        const V ub = v3(sel3(ib, R2[0], R2[1], R2[2]), sel3(ib, R2[3], R2[4], R2[5]),
+                        sel3(ib, R2[6], R2[7], R2[8]));
         double s, t;
         intersect_lines(pB1, ua, pB2, ub, s, t);
         pB1 = pB1 + s * ua;
@@ -329,80 +347,83 @@ __device__ void collide_box_box(const OBox &p1, const OBox &p2, F &f) {
         return;
     }
 
-    // vertex/face, MaxContacts.h:1419-2250: A owns the reference face
+    // vertex/face, MaxContacts.h:1419-2250: A owns the reference face.  Points of A's frame are
+    // kept with their components in the order (xa, ya, za): the reference face's normal axis
+    // first, so the clipping below reads fixed components.
     const bool sw = contactCase > 3;
-    const OBox &A = sw ? b2 : b1;
-    const OBox &B = sw ? b1 : b2;
-    const double *hla = A.hl, *hlb = B.hl;
+    const OBox A = sw ? b2 : b1;
+    const OBox B = sw ? b1 : b2;
     if (sw) contactNormal = -contactNormal;
     const double *Ra = A.R, *Rb = B.R;
     const V na = rt_mulv(Ra, contactNormal), nb = rt_mulv(Rb, contactNormal);
-    const double normala[3] = {na.x, na.y, na.z}, normalb[3] = {nb.x, nb.y, nb.z};
     int xb, yb, zb;
-    if (fabs(normalb[0]) > fabs(normalb[1])) {
-        if (fabs(normalb[0]) > fabs(normalb[2])) { xb = 0; yb = 1; zb = 2; }
+    if (fabs(nb.x) > fabs(nb.y)) {
+        if (fabs(nb.x) > fabs(nb.z)) { xb = 0; yb = 1; zb = 2; }
         else { xb = 2; yb = 0; zb = 1; }
-    } else if (fabs(normalb[1]) > fabs(normalb[2])) { xb = 1; yb = 2; zb = 0; }
+    } else if (fabs(nb.y) > fabs(nb.z)) { xb = 1; yb = 2; zb = 0; }
     else { xb = 2; yb = 0; zb = 1; }
     const int xa = contactCase < 4 ? contactCase - 1 : contactCase - 4;
     const int ya = xa == 0 ? 1 : (xa == 1 ? 2 : 0);
     const int za = xa == 0 ? 2 : (xa == 1 ? 0 : 1);
-    // the incident face of B in A's frame
-    double vba[4][3];
+    const double hxa = sel3(xa, A.hl[0], A.hl[1], A.hl[2]), hya = sel3(ya, A.hl[0], A.hl[1], A.hl[2]),
+                 hza = sel3(za, A.hl[0], A.hl[1], A.hl[2]);
+    const double hxb = sel3(xb, B.hl[0], B.hl[1], B.hl[2]), hyb = sel3(yb, B.hl[0], B.hl[1], B.hl[2]),
+                 hzb = sel3(zb, B.hl[0], B.hl[1], B.hl[2]);
+    const double nax = sel3(xa, na), nbx = sel3(xb, nb);
+    // the incident face of B in A's frame: T in A's axes, P the same with (xa, ya, za) order
+    V T[4], P[4];
     const V ab = B.x - A.x;
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-        double vb[3];
-        vb[xb] = normalb[xb] > 0.0 ? -hlb[xb] : hlb[xb];
-        vb[yb] = (k & 1) ? hlb[yb] : -hlb[yb];
-        vb[zb] = (k & 2) ? hlb[zb] : -hlb[zb];
-        const V t = rt_mulv(Ra, ab + r_mulv(Rb, v3(vb[0], vb[1], vb[2])));
-        vba[k][0] = t.x; vba[k][1] = t.y; vba[k][2] = t.z;
+        const V vb = perm3(xb, nbx > 0.0 ? -hxb : hxb, yb, (k & 1) ? hyb : -hyb,
+                           (k & 2) ? hzb : -hzb);
+        T[k] = rt_mulv(Ra, ab + r_mulv(Rb, vb));
+        P[k] = v3(sel3(xa, T[k]), sel3(ya, T[k]), sel3(za, T[k]));
     }
-    const double offseta = normala[xa] > 0.0 ? hla[xa] : -hla[xa];
+    const double offseta = nax > 0.0 ? hxa : -hxa;
     // the incident face's edges v0-v1, v0-v2, v3-v1, v3-v2 against the reference face's side
     // lines y = +h, y = -h, z = +h, z = -h (MaxContacts.h:1546-2065)
-    const int EP[4] = {0, 0, 3, 3}, EQ[4] = {1, 2, 1, 2};
+    constexpr int EP[4] = {0, 0, 3, 3}, EQ[4] = {1, 2, 1, 2};
+#pragma unroll
     for (int e = 0; e < 4; ++e) {
-        const double *P = vba[EP[e]], *Q = vba[EQ[e]];
+        const V Pe = P[EP[e]], Qe = P[EQ[e]];
+#pragma unroll
         for (int side = 0; side < 4; ++side) {
-            const int cc = side < 2 ? ya : za, o = side < 2 ? za : ya;
-            const double h = (side & 1) ? -hla[cc] : hla[cc];
-            if (!((P[cc] > h) ^ (Q[cc] > h))) continue;
-            const double s = (h - P[cc]) / (Q[cc] - P[cc]);
+            const bool ys = side < 2;   // the side lines y = +-h, else z = +-h
+            const double hc = ys ? hya : hza, ho = ys ? hza : hya;
+            const double h = (side & 1) ? -hc : hc;
+            const double pc = ys ? Pe.y : Pe.z, qc = ys ? Qe.y : Qe.z;
+            if (!((pc > h) ^ (qc > h))) continue;
+            const double s = (h - pc) / (qc - pc);
             if (!(s > 0.0 && s < 1.0)) continue;
-            const double tmp = P[o] + s * (Q[o] - P[o]);
-            if (!(fabs(tmp) < hla[o])) continue;
-            const double dist = fabs(P[xa] + s * (Q[xa] - P[xa])) - hla[xa];
+            const double po = ys ? Pe.z : Pe.y, qo = ys ? Qe.z : Qe.y;
+            const double tmp = po + s * (qo - po);
+            if (!(fabs(tmp) < ho)) continue;
+            const double dist = fabs(Pe.x + s * (Qe.x - Pe.x)) - hxa;
             if (!(dist < kContactThreshold)) continue;
-            double posa[3];
-            posa[xa] = offseta;
-            posa[cc] = h;
-            posa[o] = tmp;
-            f(B.ref, A.ref, A.x + r_mulv(Ra, v3(posa[0], posa[1], posa[2])), contactNormal, dist, 0);
+            const V posa = perm3(xa, offseta, ya, ys ? h : tmp, ys ? tmp : h);
+            f(B.ref, A.ref, A.x + r_mulv(Ra, posa), contactNormal, dist, 0);
         }
     }
     // vertices of B inside the reference face (MaxContacts.h:2067-2118)
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-        if (fabs(vba[k][ya]) <= hla[ya] && fabs(vba[k][za]) <= hla[za]) {
-            const double dist = fabs(vba[k][xa]) - hla[xa];
+        if (fabs(P[k].y) <= hya && fabs(P[k].z) <= hza) {
+            const double dist = fabs(P[k].x) - hxa;
             if (dist < kContactThreshold)
-                f(B.ref, A.ref, A.x + r_mulv(Ra, v3(vba[k][0], vba[k][1], vba[k][2])),
-                  contactNormal, dist, 0);
+                f(B.ref, A.ref, A.x + r_mulv(Ra, T[k]), contactNormal, dist, 0);
         }
     }
     // vertices of A's reference face inside B's incident face, a vertex on B's vertex counted
     // once (MaxContacts.h:2179-2250)
     const V ba = A.x - B.x;
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-        double va[3];
-        va[xa] = normala[xa] > 0.0 ? hla[xa] : -hla[xa];
-        va[ya] = (k & 1) ? hla[ya] : -hla[ya];
-        va[za] = (k & 2) ? hla[za] : -hla[za];
-        const V t = rt_mulv(Rb, ba + r_mulv(Ra, v3(va[0], va[1], va[2])));
-        const double vab[3] = {t.x, t.y, t.z};
-        const double ay = fabs(vab[yb]), az = fabs(vab[zb]);
-        if ((ay <= hlb[yb] && az < hlb[zb]) || (ay < hlb[yb] && az <= hlb[zb])) {
-            const double dist = fabs(vab[xb]) - hlb[xb];
+        const V va = perm3(xa, offseta, ya, (k & 1) ? hya : -hya, (k & 2) ? hza : -hza);
+        const V t = rt_mulv(Rb, ba + r_mulv(Ra, va));
+        const double ay = fabs(sel3(yb, t)), az = fabs(sel3(zb, t));
+        if ((ay <= hyb && az < hzb) || (ay < hyb && az <= hzb)) {
+            const double dist = fabs(sel3(xb, t)) - hxb;
             if (dist < kContactThreshold) f(B.ref, A.ref, B.x + r_mulv(Rb, t), contactNormal, dist, 0);
         }
     }
