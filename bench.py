@@ -597,6 +597,42 @@ def our_arm(args):
     return line
 
 
+def boxes_extra(torch, flush, dev):
+    """Scenes with moving boxes (FP64, the only precision for boxes): a 6x6x6 stack of cubes
+    resting face to face (every face contact held by gravity) under the hard-contact solver,
+    and 110,592 spheres with 1,000 tilted boxes falling on them under DEM; body-steps/s on the
+    GPU and in pe on one host core."""
+    from pe_b200 import _abi
+    out = {}
+    for label, sc, kind in (("stack_216_hcsits", scenes.box_stack(6, 6, overlap=0.0), "hcsits"),
+                            ("spheres110k_boxes1000_dem", scenes.spheres_and_boxes(0), "dem")):
+        e = make_engine([sc], kind, _abi.FP64)
+        st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+        k = 20
+        ms, _, prof = timed_steps(e, sc.dt, k, 3, torch, flush, st)
+        stt = e.stats()
+        e.close()
+        nb = sc.n + sc.nmbox
+        rec = {"bodies": nb, "spheres": sc.n, "boxes": sc.nmbox, "ms_per_step": ms / k,
+               "body_steps_per_s": nb * k / (ms / 1e3), "precision": "fp64"}
+        if kind == "hcsits":
+            rec.update({"contacts": stt["contacts"], "colors": stt["colors"], "sweeps": 100})
+        exe = os.path.join(REF_DIR, "ref_dem" if kind == "dem" else "ref_hcsits")
+        if os.path.exists(exe):
+            with tempfile.TemporaryDirectory() as tmp:
+                sp = os.path.join(tmp, "s.bin")
+                sc.save(sp)
+                extra = ["1", "100"] if kind == "hcsits" else []
+                r = subprocess.run([exe, "time", sp, "1", "5", *extra], capture_output=True,
+                                   text=True, timeout=600)
+                if r.returncode == 0:
+                    sec = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
+                    rec["pe_one_core"] = {"ms_per_step": sec / 5 * 1e3,
+                                          "body_steps_per_s": nb * 5 / sec}
+        out[label] = rec
+    return out
+
+
 def extras(args, torch, flush, dev, ss, kind, mixed_value):
     """Beside the headline: the plain FP64 GPU path (grid search every step, the first CUDA
     form), the FP64 path with neighbour lists, the mixed-vs-FP64 position error after 1000 steps,
@@ -678,6 +714,8 @@ def extras(args, torch, flush, dev, ss, kind, mixed_value):
                     "contacts": stt["contacts"], "colors": stt["colors"], "sweeps": 100,
                     "stages_ms_per_step": {a: b[0] / ksteps for a, b in prof.items() if b[1]}}
                 e.close()
+    if args.workload == "dem_large_1m":
+        out["moving_boxes"] = boxes_extra(torch, flush, dev)
     ref, why = run_reference(args.workload, steps=10, budget_s=20.0)
     if ref:
         out["cpu_baseline"] = {"value": ref["sphere_steps_per_s"], "unit": UNIT,

@@ -230,9 +230,11 @@ typedef struct {
     double skin;             /* neighbour-list skin (cells are re-planned to 2 r_max + skin) */
     double ms_per_step;      /* pe_b200_autotune: measured time of the winner; else -1 */
     int32_t variants;        /* output: number of launch shapes */
-    int32_t nbgs_sweeps;     /* HCSITS sweeps: 0 automatic (= 2), 1 one thread-block cluster
-                                with hardware barriers, 2 one cooperative grid with barriers
-                                through global memory, 3 one launch per colour */
+    int32_t nbgs_sweeps;     /* HCSITS sweeps: 0 automatic (4 when every colour fits one
+                                block, else 2), 1 one thread-block cluster with hardware
+                                barriers, 2 one cooperative grid with barriers through global
+                                memory, 3 one launch per colour, 4 one thread block with
+                                __syncthreads between colours (when every colour fits it) */
 } pe_b200_tuning;
 int pe_b200_get_tuning(pe_b200_ctx *ctx, pe_b200_tuning *out);
 int pe_b200_set_tuning(pe_b200_ctx *ctx, const pe_b200_tuning *t);

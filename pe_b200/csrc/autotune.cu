@@ -65,7 +65,7 @@ int set_list_skin(Ctx *c, double skin) {
 
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
     if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < 0 ||
-        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 3)
+        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 4)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
     c->tune.nbgs_sweeps = t.nbgs_sweeps;
     if (t.dem_variant != c->tune.dem_variant || t.rebuild_per_sm != c->tune.rebuild_per_sm) {

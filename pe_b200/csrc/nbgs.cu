@@ -30,6 +30,7 @@ namespace {
 
 constexpr int kBlk = 256;
 constexpr int kMaxColors = 256;   // colours of one step (8 bits in the packed colour)
+constexpr size_t kBlockSmemMax = 200 * 1024;   // shared memory of the single-block sweep form
 
 struct CountF {
     int n = 0;
@@ -859,6 +860,79 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
     }
 }
 
+// All sweeps of a step in one thread block, when every colour fits the block: the colours are
+// separated by __syncthreads, and the body and impulse updates of a colour, made on this SM,
+// are read back through its L1 by the next.  Scenes whose contacts crowd on few bodies (box
+// stacks: dozens of contact points per box, so many colours of a few dozen contacts) spend most
+// of a sweep on the barriers; this form makes a barrier cost a few dozen cycles.
+template <typename T, int MODEL, bool GEN = false>
+__global__ void __launch_bounds__(kBlk) k_sweeps_block(int iters, int ncolors,
+                                                       const int32_t *color_start, int64_t cap,
+                                                       T dtinv, Cache<T> cc, BodyV<T> bv,
+                                                       int64_t nb, int track_last,
+                                                       unsigned long long *delta) {
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t e = color_start[col + 1];
+            for (int64_t k = color_start[col] + threadIdx.x; k < e; k += blockDim.x)
+                sweep_contact<T, MODEL, false, GEN>(k, dtinv, cc, bv, track, delta);
+            __syncthreads();
+        }
+    }
+}
+
+// The single-block form with the bodies' velocity records in shared memory (when they fit):
+// the updates of one colour reach the next colour's reads at shared-memory latency.  A
+// contact's impulse is read and written by one thread only, so it stays in global memory.
+template <typename T, int MODEL, bool GEN = false>
+__global__ void __launch_bounds__(kBlk) k_sweeps_block_smem(int iters, int ncolors,
+                                                            const int32_t *color_start,
+                                                            int64_t cap, T dtinv, Cache<T> cc,
+                                                            BodyV<T> bv, int64_t nbod,
+                                                            int track_last,
+                                                            unsigned long long *delta) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T4<T> *sh = (T4<T> *)smem;
+    const int nrow = GEN ? 7 : 4;   // vr wr dv dw (ia ib ic)
+    BodyV<T> sb;
+    sb.vr = sh;
+    sb.wr = sh + nbod;
+    sb.dv = sh + 2 * nbod;
+    sb.dw = sh + 3 * nbod;
+    if (GEN) {
+        sb.ia = sh + 4 * nbod;
+        sb.ib = sh + 5 * nbod;
+        sb.ic = sh + 6 * nbod;
+    }
+    (void)nrow;
+    for (int64_t i = threadIdx.x; i < nbod; i += blockDim.x) {
+        sb.vr[i] = bv.vr[i];
+        sb.wr[i] = bv.wr[i];
+        sb.dv[i] = bv.dv[i];
+        sb.dw[i] = bv.dw[i];
+        if (GEN) {
+            sb.ia[i] = bv.ia[i];
+            sb.ib[i] = bv.ib[i];
+            sb.ic[i] = bv.ic[i];
+        }
+    }
+    __syncthreads();
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t e = color_start[col + 1];
+            for (int64_t k = color_start[col] + threadIdx.x; k < e; k += blockDim.x)
+                sweep_contact<T, MODEL, false, GEN>(k, dtinv, cc, sb, track, delta);
+            __syncthreads();
+        }
+    }
+    for (int64_t i = threadIdx.x; i < nbod; i += blockDim.x) {
+        bv.dv[i] = sb.dv[i];
+        bv.dw[i] = sb.dw[i];
+    }
+}
+
 // All sweeps of a step inside one thread-block cluster: the colours are separated by the
 // cluster's hardware barrier (release/acquire at cluster scope) instead of a barrier through
 // global atomics, which costs a few microseconds per colour.  Used while the largest colour
@@ -1098,6 +1172,42 @@ auto persistent_kernel(int m, bool gen) -> decltype(&k_sweeps_persistent<VT, 0, 
         if (gen) return persistent_kernel_g<VT, true>(m);
     }
     return persistent_kernel_g<VT, false>(m);
+}
+template <typename VT, bool GEN>
+auto block_kernel_g(int m) -> decltype(&k_sweeps_block<VT, 0, GEN>) {
+    switch (m) {
+        case 1: return k_sweeps_block<VT, 1, GEN>;
+        case 2: return k_sweeps_block<VT, 2, GEN>;
+        case 3: return k_sweeps_block<VT, 3, GEN>;
+        case 4: return k_sweeps_block<VT, 4, GEN>;
+        case 5: return k_sweeps_block<VT, 5, GEN>;
+        default: return k_sweeps_block<VT, 0, GEN>;
+    }
+}
+template <typename VT>
+auto block_kernel(int m, bool gen) -> decltype(&k_sweeps_block<VT, 0, false>) {
+    if constexpr (std::is_same<VT, double>::value) {
+        if (gen) return block_kernel_g<VT, true>(m);
+    }
+    return block_kernel_g<VT, false>(m);
+}
+template <typename VT, bool GEN>
+auto block_smem_kernel_g(int m) -> decltype(&k_sweeps_block_smem<VT, 0, GEN>) {
+    switch (m) {
+        case 1: return k_sweeps_block_smem<VT, 1, GEN>;
+        case 2: return k_sweeps_block_smem<VT, 2, GEN>;
+        case 3: return k_sweeps_block_smem<VT, 3, GEN>;
+        case 4: return k_sweeps_block_smem<VT, 4, GEN>;
+        case 5: return k_sweeps_block_smem<VT, 5, GEN>;
+        default: return k_sweeps_block_smem<VT, 0, GEN>;
+    }
+}
+template <typename VT>
+auto block_smem_kernel(int m, bool gen) -> decltype(&k_sweeps_block_smem<VT, 0, false>) {
+    if constexpr (std::is_same<VT, double>::value) {
+        if (gen) return block_smem_kernel_g<VT, true>(m);
+    }
+    return block_smem_kernel_g<VT, false>(m);
 }
 template <typename VT, bool GEN>
 auto colour_kernel_g(int m) -> decltype(&k_sweep<VT, 0, GEN>) {
@@ -1354,6 +1464,37 @@ int nbgs_step_t(Ctx *c, double dt) {
             int rc = sweeps_in_cluster<VT>(c, model, iters, ncolors, maxcol, cap, VT(1.0 / dt), cc,
                                            bv, n, dl, &done);
             if (rc) return rc;
+        }
+        if (!done && (mode == 0 || mode == 4) && maxcol <= kBlk) {
+            // every colour fits one block: all sweeps in one block, colours separated by
+            // __syncthreads (automatic, or asked for with 4)
+            PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start,
+                                        (ncolors + 1) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                        c->stream));
+            const size_t smem = (size_t)(gen ? 7 : 4) * nb.nbod * sizeof(T4<VT>);
+            bool smem_ok = smem <= kBlockSmemMax;
+            if (smem_ok) {
+                auto kern = block_smem_kernel<VT>(model, gen);
+                // opt in to the large shared-memory carve-out (per kernel; cheap to repeat)
+                smem_ok = cudaFuncSetAttribute((const void *)kern,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kBlockSmemMax) == cudaSuccess;
+                if (smem_ok) {
+                    kern<<<1, kBlk, smem, c->stream>>>(iters, ncolors, nb.cstart_dev, cap,
+                                                       VT(1.0 / dt), cc, bv, nb.nbod,
+                                                       c->want_residual ? 1 : 0, dl);
+                    PEB_LAUNCHED(c);
+                } else {
+                    cudaGetLastError();
+                }
+            }
+            if (!smem_ok) {
+                block_kernel<VT>(model, gen)<<<1, kBlk, 0, c->stream>>>(
+                    iters, ncolors, nb.cstart_dev, cap, VT(1.0 / dt), cc, bv, n,
+                    c->want_residual ? 1 : 0, dl);
+                PEB_LAUNCHED(c);
+            }
+            done = true;
         }
         if (!done && !nb.coop_disabled && mode != 3) {
             // all sweeps in one cooperative launch (colours separated by grid barriers); as few

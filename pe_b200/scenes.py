@@ -460,7 +460,7 @@ def tumbling_boxes(seed: int = 0, side: int = 3, max_angle: float = 0.3, mu: flo
     return s
 
 
-def box_stack(layers: int = 4, per_side: int = 3) -> Scene:
+def box_stack(layers: int = 4, per_side: int = 3, overlap: float = 1e-4) -> Scene:
     """pe's box-stack arrangement: layers of equal, axis-aligned cubes resting face to face on
     a floor plane (the degenerate, fully aligned case of the box/box test), plus one sphere
     flying into the stack."""
@@ -469,7 +469,7 @@ def box_stack(layers: int = 4, per_side: int = 3) -> Scene:
     for z in range(layers):
         for y in range(per_side):
             for x in range(per_side):
-                pts.append([x * a, y * a, 0.5 * a + z * a - 1e-4 * (z + 1)])
+                pts.append([x * a, y * a, 0.5 * a + z * a - overlap * (z + 1)])
     bx = np.array(pts) + np.array([2.0, 2.0, 0.0])
     nb = bx.shape[0]
     planes = np.array([[0.0, 0.0, 1.0, 0.0]])
@@ -483,6 +483,30 @@ def box_stack(layers: int = 4, per_side: int = 3) -> Scene:
     s.mbox_w = np.zeros((nb, 3))
     s.mbox_len = np.full((nb, 3), a)
     s.mbox_mat = np.zeros(nb, np.int32)
+    return s
+
+
+def spheres_and_boxes(seed: int = 0, sphere_side: int = 48, box_side: int = 10) -> Scene:
+    """A mixed DEM scene: the lattice of dem_lattice(seed, sphere_side) with box_side^3 moving
+    boxes (side lengths U[0.5, 0.9] of their lattice spacing, tilted up to 0.5 rad) on a coarser
+    lattice above the spheres, falling onto them; the box of planes is raised to hold them."""
+    rng = np.random.default_rng(seed)
+    s = dem_lattice(seed, side=sphere_side)
+    nb = box_side ** 3
+    idx = np.stack(np.meshgrid(*[np.arange(box_side)] * 3, indexing="ij"),
+                   axis=-1).reshape(-1, 3).astype(float)
+    top = s.x[:, 2].max() + 2.0
+    lo = s.x[:, 0].min()
+    sp = (s.x[:, 0].max() - lo) / box_side
+    s.mbox_x = np.c_[idx[:, 0] * sp + sp / 2 + lo, idx[:, 1] * sp + sp / 2 + lo,
+                     top + idx[:, 2] * sp]
+    s.mbox_q = small_rotations(rng, nb, 0.5)
+    s.mbox_v = rng.normal(0.0, 0.1, size=(nb, 3))
+    s.mbox_w = rng.normal(0.0, 0.1, size=(nb, 3))
+    s.mbox_len = rng.uniform(0.5, 0.9, size=(nb, 3)) * sp
+    s.mbox_mat = np.zeros(nb, np.int32)
+    s.planes[s.planes[:, 2] < -0.5, 3] = -(top + box_side * sp + 5.0)
+    s.name = f"spheres_and_boxes_{s.n}_{nb}"
     return s
 
 

@@ -142,3 +142,22 @@ def test_nbgs_sweep_forms_agree(precision, model):
     for o in out[1:]:
         for a, b in zip(o, out[0]):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["dense512", "boxes36_stack"])
+def test_nbgs_single_block_form_agrees(name):
+    """When every colour fits one block, all sweeps can run in that block with __syncthreads
+    between colours; it gives the grid form's and the per-colour form's results bit for bit."""
+    from helpers import load_golden
+    s = load_golden(name)["scene"]
+    out = []
+    for mode in (2, 3, 4, 0):
+        e = Engine(solver=_abi.HCSITS, precision=_abi.FP64, relaxation_model=1,
+                   max_iterations=50).load_scene(s)
+        e.set_tuning(nbgs_sweeps=mode)
+        e.step(s.dt, 2)
+        out.append(e.download_boxes() if s.nmbox else e.download())
+        e.close()
+    for o in out[1:]:
+        for a, b in zip(o, out[0]):
+            assert np.array_equal(a, b)
