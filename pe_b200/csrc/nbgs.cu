@@ -355,9 +355,9 @@ __device__ __forceinline__ bool beats(uint32_t c, uint32_t e) {
 // proposed the same colour with a higher priority (a fixed hash of the contact index).  The
 // highest-priority proposal of every clash stands, so each round colours a large share of the
 // remaining contacts -- a few rounds even where a box carries dozens of contact points, against
-// a round per priority level when only local priority maxima take colours.  The result depends only on the
-// contact order, not on scheduling.  W 64-bit words of settled colours per body (64 W colours:
-// 64 for spheres, whose contacts are few, 256 for scenes with boxes).
+// a round per priority level when only local priority maxima take colours.  The result depends
+// only on the contact order, not on scheduling.  W 64-bit words of settled colours per body
+// (64 W colours: 64 for spheres, whose contacts are few, 256 for scenes with boxes).
 template <int W>
 __global__ void k_color_propose(int64_t nc, const int32_t *b1, const int32_t *b2,
                                 const int32_t *color, const uint64_t *used, int32_t *tent,
