@@ -32,6 +32,7 @@ namespace {
 constexpr int kBlk = 256;
 constexpr int kMaxColors = 256;   // colours of one step (8 bits in the packed colour)
 constexpr size_t kBlockSmemMax = 200 * 1024;   // shared memory of the single-block sweep form
+constexpr int64_t kSerialColourMax = 8192;      // contacts coloured by one thread in one launch
 
 struct CountF {
     int n = 0;
@@ -405,6 +406,57 @@ __global__ void k_color_settle(int64_t nc, int round, const int32_t *b1, const i
     atomicOr((unsigned long long *)&used[(int64_t)bodies[0] * W + (t >> 6)], 1ull << (t & 63));
     if (bodies[1] >= 0)
         atomicOr((unsigned long long *)&used[(int64_t)bodies[1] * W + (t >> 6)], 1ull << (t & 63));
+}
+
+// Few contacts: one thread colours them greedily in contact order (the smallest colour free at
+// both bodies), in one launch.  Where a body carries dozens of contacts (box stacks) this needs
+// about as many colours as the busiest body has contacts, the least possible, where the parallel
+// rounds need a launch pair per round and end with more colours.
+// The used-colour masks live in shared memory when they fit (used_global == null), else in
+// the zeroed global array.
+template <int W>
+__global__ void k_color_serial(int64_t nc, const int32_t *__restrict__ b1,
+                               const int32_t *__restrict__ b2, int32_t *__restrict__ color,
+                               int64_t nbod, uint64_t *used_global, int32_t *err) {
+    extern __shared__ uint64_t used_shared[];
+    uint64_t *used = used_global ? used_global : used_shared;
+    if (!used_global)
+        for (int64_t i = threadIdx.x; i < nbod * W; i += blockDim.x) used_shared[i] = 0ull;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    // the bodies of the next contacts are loaded ahead, off the chain of mask updates
+    constexpr int kAhead = 8;
+    int32_t qa[kAhead], qb[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) {
+        qa[k] = k < nc ? __ldg(b1 + k) : 0;
+        qb[k] = k < nc ? __ldg(b2 + k) : -1;
+    }
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t a = qa[0], b = qb[0];
+#pragma unroll
+        for (int k = 0; k + 1 < kAhead; ++k) {
+            qa[k] = qa[k + 1];
+            qb[k] = qb[k + 1];
+        }
+        qa[kAhead - 1] = c + kAhead < nc ? __ldg(b1 + c + kAhead) : 0;
+        qb[kAhead - 1] = c + kAhead < nc ? __ldg(b2 + c + kAhead) : -1;
+        int col = -1;
+#pragma unroll
+        for (int wd = 0; wd < W && col < 0; ++wd) {
+            const uint64_t u = used[(int64_t)a * W + wd] | (b >= 0 ? used[(int64_t)b * W + wd] : 0ull);
+            const int f = __ffsll((long long)~u) - 1;
+            if (f >= 0) col = 64 * wd + f;
+        }
+        if (col < 0) {
+            atomicOr(err, DERR_COLORS);
+            color[c] = 0;
+            continue;
+        }
+        color[c] = col;
+        used[(int64_t)a * W + (col >> 6)] |= 1ull << (col & 63);
+        if (b >= 0) used[(int64_t)b * W + (col >> 6)] |= 1ull << (col & 63);
+    }
 }
 
 __global__ void k_color_hist(int64_t nc, int32_t *color, int32_t *hist, int32_t *ncolors) {
@@ -1416,7 +1468,14 @@ int nbgs_step_t(Ctx *c, double dt) {
         const int words = gen ? 4 : 1;
         PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)nbod * words * sizeof(uint64_t), c->stream));
         int round = 0;
-        for (;;) {
+        if (nc <= kSerialColourMax) {
+            const size_t masks = (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t);
+            const bool in_smem = masks <= 48 * 1024;
+            (gen ? k_color_serial<4> : k_color_serial<1>)<<<1, 256, in_smem ? masks : 0, c->stream>>>(
+                nc, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used, c->d_err);
+            PEB_LAUNCHED(c);
+        }
+        for (; nc > kSerialColourMax;) {
             const int batch = 8;
             PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, batch * sizeof(int32_t), c->stream));
             int32_t *tent = nb.order;   // free until the colour sort below
