@@ -274,7 +274,7 @@ def stage_inputs(ss, torch):
             "damping": ss[0].damping, "nscenes": len(ss)}
 
 
-def engine_from_staged(st, kind, precision, iters=100, lists=True):
+def engine_from_staged(st, kind, precision, iters=100, lists=True, skin=0.0):
     from pe_b200 import _abi
     from pe_b200.engine import Engine
     solver = _abi.DEM if kind == "dem" else _abi.HCSITS
@@ -282,7 +282,7 @@ def engine_from_staged(st, kind, precision, iters=100, lists=True):
     if kind == "hcsits" and float(st["materials"][0, 2]) > 0:
         model = _abi.APPROX_INELASTIC_COULOMB_DECOUPLING
     e = Engine(solver=solver, precision=precision, relaxation_model=model, max_iterations=iters,
-               neighbor_lists=lists)
+               neighbor_lists=lists, skin=skin)
     e.set_materials(st["materials"])
     for k, (pl, pm, bx, bm) in enumerate(st["walls"]):
         e.set_walls(k, pl, pm, bx, bm)
@@ -453,6 +453,53 @@ def adjoint_extra(torch):
     return out
 
 
+def nsph_total(ss, dist, torch, dev):
+    tot = torch.tensor([float(sum(s.n for s in ss))], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return float(tot.item())
+
+
+def end_to_end(ss, kind, precision, tuning, dt, steps, torch, dev, dist):
+    """The public API end to end: a new context, the bodies uploaded from pinned host arrays,
+    `steps` steps, the state downloaded into pinned host arrays; wall clock. One untimed pass
+    first (host thread pools, first allocations), then the median of three passes, each taken
+    as the max over ranks."""
+    staged = stage_inputs(ss, torch)
+    nsph = sum(s.n for s in ss)
+    outs = [torch.zeros((nsph, 3), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+    runs = []
+    for rep in range(4):
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        # the tuned skin sizes the cells at upload; the launch shapes follow
+        e2 = engine_from_staged(staged, kind, precision,
+                                skin=tuning["skin"] if tuning is not None else 0.0)
+        if tuning is not None:
+            e2.set_tuning(tuning["dem_variant"], tuning["rebuild_per_sm"], tuning["skin"])
+        t1 = time.perf_counter()
+        e2.step(dt, steps)
+        t2 = time.perf_counter()
+        out = e2.download(out=outs)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        e2.close()
+        te = torch.tensor([t3 - t0, t1 - t0, t2 - t1, t3 - t2], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        runs.append([float(a) for a in te.tolist()])
+    h2d = sum(staged[k].nbytes for k in ("x", "v", "w", "r", "mat")) + \
+        (staged["scene"].nbytes if staged["scene"] is not None else 0)
+    d2h = sum(a.nbytes for a in out if a is not None)
+    timed = sorted(runs[1:], key=lambda r: r[0])
+    med = timed[len(timed) // 2]
+    parts = {"setup_upload_ms": 1e3 * med[1], "steps_issue_ms": 1e3 * med[2],
+             "download_sync_ms": 1e3 * med[3]}
+    return med[0], parts, [1e3 * r[0] for r in runs], h2d, d2h
+
+
 def our_arm(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -494,6 +541,11 @@ def our_arm(args):
         uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
     except Exception:
         uuid = None
+    # end to end first: nvidia-smi polling (the clock record of the device-timed region) slows
+    # the driver calls that allocate and free, here and for a while after it stops
+    e2e_s, e2e_parts, e2e_runs, h2d, d2h = end_to_end(ss, kind, precision, tuning, dt, args.steps,
+                                                      torch, dev, dist)
+    e2e_value = nsph_total(ss, dist, torch, dev) * args.steps / e2e_s
     clocks = Clocks(uuid)
     clocks.start()
     ms, launches, prof = timed_steps(e, dt, args.steps, args.warmup, torch, flush, stream, dist)
@@ -507,35 +559,6 @@ def our_arm(args):
     total_sph = float(tot.item())
     value = total_sph * args.steps / (ms_max / 1e3)
 
-    # end to end through the public API: a new context, the bodies uploaded from pinned host
-    # arrays, K steps, the state downloaded into pinned host arrays; wall clock
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    staged = stage_inputs(ss, torch)
-    outs = [torch.zeros((nsph, 3), dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
-    t0 = time.perf_counter()
-    e2 = engine_from_staged(staged, kind, precision)
-    if tuning is not None:
-        e2.set_tuning(tuning["dem_variant"], tuning["rebuild_per_sm"], tuning["skin"])
-    t1 = time.perf_counter()
-    e2.step(dt, args.steps)
-    t2 = time.perf_counter()
-    out = e2.download(out=outs)
-    torch.cuda.synchronize()
-    t3 = time.perf_counter()
-    e2e_s = t3 - t0
-    e2e_parts = {"setup_upload_ms": 1e3 * (t1 - t0), "steps_issue_ms": 1e3 * (t2 - t1),
-                 "download_sync_ms": 1e3 * (t3 - t2)}
-    h2d = sum(staged[k].nbytes for k in ("x", "v", "w", "r", "mat")) + \
-        (staged["scene"].nbytes if staged["scene"] is not None else 0)
-    d2h = sum(a.nbytes for a in out if a is not None)
-    e2.close()
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    e2e_value = total_sph * args.steps / float(te.item())
 
     if dist is not None:
         dist.destroy_process_group()
@@ -586,8 +609,9 @@ def our_arm(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
                     "note": "new context, upload from pinned host arrays, steps, download into "
-                            "pinned host arrays, through the C ABI; wall clock",
-                    "parts": e2e_parts},
+                            "pinned host arrays, through the C ABI; wall clock; median of 3 "
+                            "passes after 1 untimed pass, max over ranks",
+                    "parts": e2e_parts, "passes_ms": e2e_runs},
             "roofline": roofline,
             "stages_ms_per_step": {k: v[0] / args.steps for k, v in prof.items() if v[1]},
             "neighbor_lists": nls}

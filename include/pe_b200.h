@@ -226,7 +226,8 @@ int pe_b200_graph_active(const pe_b200_ctx *ctx);
 /* Launch shapes of the DEM neighbour-list step (no pe counterpart). */
 typedef struct {
     int32_t dem_variant;     /* launch shape of the force/integration kernel, 0..variants-1 */
-    int32_t rebuild_per_sm;  /* CTAs per SM of the persistent list rebuild; 0 = as many as fit */
+    int32_t rebuild_per_sm;  /* CTAs per SM of the persistent list rebuild; 0 = as many as fit;
+                                -1 = one launch per rebuild stage (the same lists) */
     double skin;             /* neighbour-list skin (cells are re-planned to 2 r_max + skin) */
     double ms_per_step;      /* pe_b200_autotune: measured time of the winner; else -1 */
     int32_t variants;        /* output: number of launch shapes */

@@ -5,7 +5,8 @@
 // or in which order, except for the skin, which changes when the state is re-sorted and so the
 // last bits of the forces:
 //   dem_variant     threads per block / resident blocks per SM of k_dem_list (dem.cu)
-//   rebuild_per_sm  CTAs per SM of the persistent rebuild kernel (rebuild.cu)
+//   rebuild_per_sm  CTAs per SM of the persistent rebuild kernel (rebuild.cu); -1 rebuilds with
+//                   one launch per stage instead (the same lists, entry for entry)
 //   skin            neighbour-list skin (cells are re-planned to 2 r_max + skin)
 // Each trial restores the state saved at entry, forces a list rebuild, runs a few untimed steps
 // (graph capture included), then times `trial` steps with CUDA events after forcing one more
@@ -64,7 +65,7 @@ int set_list_skin(Ctx *c, double skin) {
 }
 
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
-    if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < 0 ||
+    if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < -1 ||
         t.nbgs_sweeps < 0 || t.nbgs_sweeps > 4)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
     c->tune.nbgs_sweeps = t.nbgs_sweeps;

@@ -717,7 +717,7 @@ int list_step(Ctx *c, double dt) {
     ListBuf &L = c->nl;
     prof_begin(c, ST_REBUILD);
     int rc = PE_B200_OK;
-    if (!L.coop_disabled) {
+    if (!L.coop_disabled && c->tune.rebuild_per_sm >= 0) {
         rc = dem_list_rebuild_persistent(c);
         if (rc != PE_B200_OK) {
             // no cooperative launch here: the rebuild kernels run one by one and return at
@@ -805,6 +805,7 @@ int dem_list_alloc(Ctx *c) {
     PEB_CUDA(c, cudaMalloc(&L.tmp.vw, n * (size_t)c->vw_bytes));
     PEB_CUDA(c, cudaMalloc(&L.tmp.tag, n * sizeof(uint32_t)));
     PEB_CUDA(c, cudaMalloc(&L.tmp.uid, n * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.stash, (size_t)kListStash * n * sizeof(int32_t)));
     if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&L.tmp.q, n * sizeof(double4)));
     L.enabled = true;
     L.check_pending = false;
@@ -828,6 +829,7 @@ void dem_list_free(Ctx *c) {
     cudaFree(L.tmp.tag);
     cudaFree(L.tmp.uid);
     cudaFree(L.tmp.q);
+    cudaFree(L.stash);
     if (L.h_flags) cudaFreeHost(L.h_flags);
     if (L.ev) cudaEventDestroy(L.ev);
     const double skin = L.skin;

@@ -27,6 +27,7 @@ constexpr float kContactThresholdF = 5e-7f;  // pe/core/Thresholds.h:103 (float)
 constexpr double kFrictionThreshold = 1e-8;  // pe/core/Thresholds.h:161
 constexpr int kMaxScenes = 65535;
 constexpr int kMaxMaterials = 65535;
+constexpr int kListStash = 8;   // neighbours per sphere the rebuild's counting pass keeps
 
 struct SceneInfo {
     double lo[3];
@@ -120,6 +121,8 @@ struct ListBuf {
     cudaEvent_t ev = nullptr;
     bool check_pending = false;
     BodyBuf tmp;                // permutation target of a rebuild
+    int32_t *stash = nullptr;   // kListStash x n, column-major: the first neighbours found by
+                                // the counting pass of the persistent rebuild
     // persistent rebuild kernel (rebuild.cu): grid barrier words and per-block partial sums
     unsigned int *rb_bar = nullptr;
     int32_t *rb_blk = nullptr;

@@ -6,7 +6,8 @@
 // separated by grid-wide barriers:
 //   clear cell counts | bin (cell key + slot, atomic histogram) | scan counts -> cell offsets |
 //   scatter | order each cell by body index | gather bodies into cell order | copy back |
-//   count neighbours closer than r_i + r_j + skin | scan counts -> list offsets | write lists
+//   count neighbours closer than r_i + r_j + skin (keeping the first few) | scan counts ->
+//   list offsets | write lists
 // Every barrier wait is bounded: a block that waits too long sets an error flag and returns.
 #include <algorithm>
 
@@ -25,7 +26,7 @@ struct RebuildArgs {
     BodyBuf cur, tmp;
     double4 *other_pr;
     int32_t *key, *rank, *sorted, *cell_count, *cell_start;
-    int32_t *cnt, *start, *idx;
+    int32_t *cnt, *start, *idx, *stash;
     int64_t cap;
     double skin;
     float *disp;
@@ -111,38 +112,119 @@ __device__ bool grid_scan(const RebuildArgs<VT> &a, const int32_t *in, int32_t *
     return true;
 }
 
-// neighbours of body t (state in cell order): count, or write with the orientation bit
+// The cells within reach of body t (state in cell order): at most 3 x 3 rows of at most 3
+// cells, since a partner is at most r_max + skin further and cells are wider than that.
+struct Reach {
+    double4 p;
+    int32_t uid;
+    int x0, x1, y0, y1, z0, z1;
+    const SceneInfo *s;
+};
+
+template <typename VT>
+__device__ __forceinline__ Reach reach_of(const RebuildArgs<VT> &a, int64_t t) {
+    Reach q;
+    q.p = a.cur.pr[t];
+    q.uid = a.cur.uid[t];
+    q.s = &a.scenes[a.cur.tag[t] >> 16];
+    const SceneInfo &s = *q.s;
+    int cx, cy, cz;
+    cell_coords(s, q.p.x, q.p.y, q.p.z, cx, cy, cz);
+    const double reach = (q.p.w + s.rmax + a.skin) * (1.0 + 1e-12) + 1e-12;
+    search_range(s, 0, q.p.x, reach, cx, q.x0, q.x1);
+    search_range(s, 1, q.p.y, reach, cy, q.y0, q.y1);
+    search_range(s, 2, q.p.z, reach, cz, q.z0, q.z1);
+    return q;
+}
+
+__device__ __forceinline__ bool within(const double4 &pi, const double4 &pj, double skin) {
+    const double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const double rc = pi.w + pj.w + skin;
+    return dx * dx + dy * dy + dz * dz < rc * rc;
+}
+
+// list entry: the partner's slot, top bit set when body t has the smaller uid
+template <typename VT>
+__device__ __forceinline__ int32_t entry(const RebuildArgs<VT> &a, int32_t uidt, int j) {
+    return (int32_t)((uint32_t)j | (uidt < a.cur.uid[j] ? 0x80000000u : 0u));
+}
+
+// Emits neighbour k of body t: MODE 0 keeps the first kListStash in the stash, MODE 1 writes
+// the list at pos.
+template <int MODE, typename VT>
+__device__ __forceinline__ void emit(const RebuildArgs<VT> &a, int64_t t, int pos, int k,
+                                     int32_t v) {
+    if (MODE == 1) a.idx[pos + k] = v;
+    else if (k < kListStash) a.stash[(int64_t)k * a.n + t] = v;
+}
+
+// Neighbours of body t, row by row, one candidate at a time: MODE 0 counts (and stashes), 1
+// writes.  The form for rows longer than 32 candidates.
+template <int MODE, typename VT>
+__device__ int neighbours_serial(const RebuildArgs<VT> &a, int64_t t, int pos, const Reach &q) {
+    const SceneInfo &s = *q.s;
+    int count = 0;
+    for (int z = q.z0; z <= q.z1; ++z) {
+        for (int y = q.y0; y <= q.y1; ++y) {
+            const int64_t c0 = cell_key(s, q.x0, y, z);
+            const int e = a.cell_start[c0 + (q.x1 - q.x0) + 1];
+            for (int j = a.cell_start[c0]; j < e; ++j) {
+                if (j == t || !within(q.p, a.cur.pr[j], a.skin)) continue;
+                emit<MODE>(a, t, pos, count, entry(a, q.uid, j));
+                ++count;
+            }
+        }
+    }
+    return count;
+}
+
+// Neighbours of body t with the bounds of all rows loaded together and the rows' candidates
+// visited in lockstep (candidate i of every row, then i + 1), so that up to nine position
+// loads are in flight at once.  Hits are bits of per-row masks and are emitted in (z, y, slot)
+// order: the same list, entry for entry, as the row-by-row scan.
 template <int MODE, typename VT>
 __device__ int list_neighbours(const RebuildArgs<VT> &a, int64_t t, int pos) {
-    const double4 pi = a.cur.pr[t];
-    const SceneInfo &s = a.scenes[a.cur.tag[t] >> 16];
-    const int32_t uidt = a.cur.uid[t];
-    int cx, cy, cz;
-    cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
-    // only the cells within reach of the sphere (a partner is at most r_max + skin further)
-    const double reach = (pi.w + s.rmax + a.skin) * (1.0 + 1e-12) + 1e-12;
-    int x0, x1, y0, y1, z0, z1;
-    search_range(s, 0, pi.x, reach, cx, x0, x1);
-    search_range(s, 1, pi.y, reach, cy, y0, y1);
-    search_range(s, 2, pi.z, reach, cz, z0, z1);
-    int count = 0;
-    for (int z = z0; z <= z1; ++z) {
-        for (int y = y0; y <= y1; ++y) {
-            const int64_t c0 = cell_key(s, x0, y, z);
-            const int64_t c1 = c0 + (x1 - x0) + 1;
-            const int e = a.cell_start[c1];
-            for (int j = a.cell_start[c0]; j < e; ++j) {
-                if (j == t) continue;
-                const double4 pj = a.cur.pr[j];
-                const double dx = pi.x - pj.x, dy2 = pi.y - pj.y, dz2 = pi.z - pj.z;
-                const double rc = pi.w + pj.w + a.skin;
-                if (dx * dx + dy2 * dy2 + dz2 * dz2 < rc * rc) {
-                    if (MODE == 1)
-                        a.idx[pos++] = (int32_t)((uint32_t)j |
-                                                 (uidt < a.cur.uid[j] ? 0x80000000u : 0u));
-                    ++count;
-                }
+    const Reach q = reach_of(a, t);
+    const SceneInfo &s = *q.s;
+    const int nx = q.x1 - q.x0 + 1;
+    int b[9], len[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        const int y = q.y0 + r % 3, z = q.z0 + r / 3;
+        b[r] = 0;
+        len[r] = 0;
+        if (y <= q.y1 && z <= q.z1) {
+            const int64_t c0 = cell_key(s, q.x0, y, z);
+            b[r] = a.cell_start[c0];
+            len[r] = a.cell_start[c0 + nx] - b[r];
+        }
+    }
+    int longest = 0;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) longest = max(longest, len[r]);
+    if (longest > 32) return neighbours_serial<MODE>(a, t, pos, q);
+    uint32_t hit[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) hit[r] = 0u;
+    for (int i = 0; i < longest; ++i) {
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            if (i < len[r]) {
+                const int j = b[r] + i;
+                if (j != t && within(q.p, a.cur.pr[j], a.skin)) hit[r] |= 1u << i;
             }
+        }
+    }
+    int count = 0;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        for (uint32_t m = hit[r]; m; m &= m - 1) {
+            if (MODE == 0 && count >= kListStash) {
+                count += __popc(m);
+                break;
+            }
+            emit<MODE>(a, t, pos, count, entry(a, q.uid, b[r] + __ffs(m) - 1));
+            ++count;
         }
     }
     return count;
@@ -210,7 +292,7 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
         if (a.cur.q) a.cur.q[t] = a.tmp.q[t];
     }
     if (!grid_sync(a.bar, a.err)) return;
-    // 8. neighbour counts
+    // 8. neighbour counts; the first kListStash neighbours of each body are kept
     for (int64_t t = g0; t < n; t += stride) a.cnt[t] = list_neighbours<0, VT>(a, t, 0);
     if (!grid_sync(a.bar, a.err)) return;
     // 9. list offsets
@@ -223,9 +305,19 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
         a.flags[3] += 1;
         a.flags[0] = 0;
     }
-    // 10. write the lists (if they fit; otherwise the force kernel searches the fresh grid)
+    // 10. write the lists (if they fit; otherwise the force kernel searches the fresh grid):
+    // copied from the stash, or searched again for bodies with more neighbours than it holds
     if (need <= a.cap)
-        for (int64_t t = g0; t < n; t += stride) list_neighbours<1, VT>(a, t, a.start[t]);
+        for (int64_t t = g0; t < n; t += stride) {
+            const int k = a.cnt[t];
+            if (k == 0) continue;
+            const int pos = a.start[t];
+            if (k > kListStash) {
+                list_neighbours<1, VT>(a, t, pos);
+                continue;
+            }
+            for (int i = 0; i < k; ++i) a.idx[pos + i] = a.stash[(int64_t)i * n + t];
+        }
 }
 
 template <typename VT>
@@ -261,6 +353,7 @@ int launch_rebuild(Ctx *c) {
     a.cnt = L.cnt;
     a.start = L.start;
     a.idx = L.idx;
+    a.stash = L.stash;
     a.cap = L.cap;
     a.skin = L.skin;
     a.disp = L.disp;
