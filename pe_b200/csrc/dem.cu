@@ -429,6 +429,11 @@ template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool HERTZ>
 __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // launched early behind the rebuild kernel: nothing of the state or the lists is read
+    // before it has finished; the next step's rebuild may be scheduled from here on (it waits
+    // for this kernel in turn)
+    pdl_wait();
+    pdl_trigger();
     bool moved = false;
     if (t < a.n) {
         // every load of this body's own records first: they are independent, and none may
@@ -709,7 +714,18 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
-    k_dem_list<VT, TRACKQ, B, M, HERTZ><<<grid_for(c->n, B), B, 0, c->stream>>>(a);
+    // scheduled while the rebuild kernel before it finishes (a rebuild that has nothing to do
+    // lets it start at once)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid_for(c->n, B));
+    cfg.blockDim = dim3(B);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_dem_list<VT, TRACKQ, B, M, HERTZ>, a);
 }
 
 template <typename VT>

@@ -128,6 +128,7 @@ struct ListBuf {
     int32_t *rb_blk = nullptr;
     int64_t rb_blk_cap = 0;
     bool coop_disabled = false;
+    bool rebuild_pdl_off = false;  // the rebuild's cooperative launch without the early start
     bool warm = false;          // a list step has run since the buffers were (re)allocated
     int since_check = 1 << 20;  // steps since the last queued read-back of flags
 };
@@ -496,6 +497,13 @@ __device__ __forceinline__ void search_range(const SceneInfo &s, int a, double p
 __device__ __forceinline__ int64_t cell_key(const SceneInfo &s, int cx, int cy, int cz) {
     return s.cell_base + ((int64_t)cz * s.dim[1] + cy) * s.dim[0] + cx;
 }
+
+// Programmatic dependent launch: a kernel launched with the programmatic-serialization
+// attribute may be scheduled while the kernel before it in the stream still runs; pdl_wait()
+// returns once that kernel has completed and its writes are visible (at once when the launch
+// had no such attribute), and pdl_trigger() lets the kernel after this one be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
 
 // Grid-wide barrier for cooperative launches, with a bounded wait: a block that waits longer
 // than ~2 s records DERR_TIMEOUT and every thread of it sees false.  bar[0] counts arrivals,

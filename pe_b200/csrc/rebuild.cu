@@ -2,7 +2,8 @@
 //
 // One cooperative launch per step.  Unless the previous force kernel requested a rebuild (a
 // sphere has moved skin/2 since the last one) every block returns after reading one flag, so a
-// step without a rebuild pays a single short launch.  A rebuild runs its stages back to back,
+// step without a rebuild pays a single short launch; both kernels are launched to be scheduled
+// while the one before them finishes (programmatic dependent launch).  A rebuild runs its stages back to back,
 // separated by grid-wide barriers:
 //   clear cell counts | bin (cell key + slot, atomic histogram) | scan counts -> cell offsets |
 //   scatter | order each cell by body index | gather bodies into cell order | copy back |
@@ -232,7 +233,12 @@ __device__ int list_neighbours(const RebuildArgs<VT> &a, int64_t t, int pos) {
 
 template <typename VT>
 __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
-    if (!a.flags[0]) return;  // uniform: no rebuild requested
+    // scheduled while the previous force kernel finishes; its flag is read after it has
+    pdl_wait();
+    if (!a.flags[0]) {  // uniform: no rebuild requested; the force kernel may start
+        pdl_trigger();
+        return;
+    }
     const int64_t n = a.n;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -361,6 +367,27 @@ int launch_rebuild(Ctx *c) {
     a.bar = L.rb_bar;
     a.blk = L.rb_blk;
     a.err = c->d_err;
+    // cooperative, and scheduled while the force kernel before it finishes; without the early
+    // start if the driver refuses the pair of attributes
+    if (!L.rebuild_pdl_off) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(kRbBlock);
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 2;
+        if (cudaLaunchKernelEx(&cfg, k_rebuild<VT>, a) == cudaSuccess) {
+            c->launches++;
+            return PE_B200_OK;
+        }
+        cudaGetLastError();
+        L.rebuild_pdl_off = true;
+    }
     void *args[] = {&a};
     PEB_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_rebuild<VT>, dim3(grid),
                                             dim3(kRbBlock), args, 0, c->stream));
