@@ -173,6 +173,7 @@ int upload_tables(Ctx *c) {
     if (!md.empty())
         PEB_CUDA(c, cudaMemcpy(c->d_mats, md.data(), md.size() * sizeof(MatDev),
                                cudaMemcpyHostToDevice));
+    c->mats_dev = md;
     // walls, concatenated per scene
     c->planes.clear();
     c->plane_mat.clear();

@@ -145,6 +145,10 @@ struct DemArgs {
     float half_skin;
     int hertz;        // extended Hertz law for sphere pairs (force_model 1)
     const double *ext = nullptr;   // moving boxes: their force and torque on body b (6 per body)
+    // one scene and one material: their records as launch parameters (read from the constant
+    // bank instead of through the body's tag)
+    SceneInfo s0;
+    MatDev m0;
 };
 
 // one sphere pair (this body and neighbour j), both in the buffers of `a`; self1: this body is
@@ -425,7 +429,7 @@ constexpr DemShape kDemShapes[] = {{kDemBlock, PEB_LIST_MIN_BLOCKS_F32, 5},
 constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]));
 
 // list step: body t stays at index t (the order changes only at rebuilds)
-template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool HERTZ>
+template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool HERTZ, bool ONE = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -444,8 +448,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
         int k = a.nl_start[t];
         const int e = a.nl_start[t + 1];
         const float disp0 = a.disp[t];
-        const SceneInfo &s = a.scenes[tagi >> 16];
-        const MatDev &mi = a.mats[tagi & 0xffffu];
+        const SceneInfo &s = ONE ? a.s0 : a.scenes[tagi >> 16];
+        const MatDev &mi = ONE ? a.m0 : a.mats[tagi & 0xffffu];
         Acc<T> acc;
         acc.F = v3(T(0), T(0), T(0));
         acc.T_ = acc.F;
@@ -714,6 +718,7 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
+    const bool one = c->nscenes == 1 && c->mats_dev.size() == 1 && !TRACKQ && !HERTZ;
     // scheduled while the rebuild kernel before it finishes (a rebuild that has nothing to do
     // lets it start at once)
     cudaLaunchConfig_t cfg = {};
@@ -725,7 +730,14 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_dem_list<VT, TRACKQ, B, M, HERTZ>, a);
+    if (one) {
+        DemArgs<VT> b = a;
+        b.s0 = c->scenes[0];
+        b.m0 = c->mats_dev[0];
+        cudaLaunchKernelEx(&cfg, k_dem_list<VT, TRACKQ, B, M, HERTZ, true>, b);
+    } else {
+        cudaLaunchKernelEx(&cfg, k_dem_list<VT, TRACKQ, B, M, HERTZ, false>, a);
+    }
 }
 
 template <typename VT>

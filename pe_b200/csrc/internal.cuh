@@ -182,6 +182,7 @@ struct Ctx {
 
     // host copies
     std::vector<pe_b200_material> mats;
+    std::vector<MatDev> mats_dev;   // host copy of d_mats
     std::vector<double> planes;     // 4 per plane, concatenated over scenes
     std::vector<int32_t> plane_mat;
     std::vector<double> boxes;      // 15 per box
