@@ -257,15 +257,19 @@ int pe_b200_autotune(pe_b200_ctx *ctx, double dt, int32_t trial_steps, pe_b200_t
  *   x, v, w (3n doubles each, interleaved xyz), r (n), mat (n): device inputs;
  *   x_out, v_out, w_out: device outputs (may alias nothing of the inputs);
  *   mats/planes/boxes: host tables (as pe_b200_set_materials / pe_b200_set_walls);
- *   domain_lo/hi: box the grid covers (bodies outside are clamped into border cells, still
- *   exact); max_radius: no sphere may be larger (checked, PE_B200_ERR_ARG otherwise);
- *   stream: cudaStream_t to run on (NULL: the legacy default stream).  Returns after the step
- *   has finished on the device.
+ *   domain_lo/hi: finite box the grid covers (bodies outside are clamped into border cells,
+ *   still exact); max_radius: finite, and no sphere may be larger (checked on the device: the
+ *   call then returns PE_B200_ERR_ARG and leaves x_out, v_out and w_out unwritten, as it does
+ *   for a material index outside [0, nmat)); stream: cudaStream_t to run on (NULL: the legacy
+ *   default stream).
+ * The call is synchronous: it returns after the step has finished on the device, copies its
+ * tables from host memory and reads its status back, so it cannot be recorded into a CUDA graph.
  * Limits: n <= PE_B200_STATIC_MAX_SPHERES, <= 64 materials, <= 64 planes, <= 64 boxes (larger
  * requests return PE_B200_ERR_ARG before any work); the grid is coarsened to at most
- * PE_B200_STATIC_MAX_CELLS cells.  All calls on a device share the array: calls whose work
- * overlaps on the GPU race and corrupt each other.  The first call on each device looks up the
- * array's address; make it before any stream capture. */
+ * PE_B200_STATIC_MAX_CELLS cells, whatever the domain's width.  All calls on a device share the
+ * array: calls whose work overlaps on the GPU race and corrupt each other.  The first call on
+ * each device (and the first after a cudaDeviceReset) looks up the array's device address,
+ * which allocates nothing. */
 #define PE_B200_STATIC_MAX_SPHERES 32768
 #define PE_B200_STATIC_MAX_CELLS 131072
 int pe_b200_dem_step_static(int64_t n, const double *x, const double *v, const double *w,

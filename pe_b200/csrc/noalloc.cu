@@ -19,13 +19,19 @@
 //   - every call on a device shares it and finds the previous call's contents; each call clears
 //     what must start at zero.  Two calls whose work overlaps on the GPU (different streams or
 //     host threads without ordering) race on the array and corrupt each other's results;
-//   - the first call on a device looks up the array's device address (cudaGetSymbolAddress,
-//     with that device current) and caches it; make that first call before any stream capture.
+//   - in host code the array's name is only a host-side stand-in: its device address is looked
+//     up with cudaGetSymbolAddress, with the device current, by the first call on each device
+//     (again after cudaDeviceReset, which unloads the module: the cache is keyed on the CUDA
+//     context's unique id, not on the device ordinal);
+//   - a call is synchronous: it copies its small tables from host memory and waits for its
+//     stream before returning, so it cannot be recorded into a CUDA graph.
+#include <cuda.h>
 #include <math.h>
 
 #include <mutex>
 
 #include "internal.cuh"
+#include "static_grid.h"
 
 namespace peb {
 
@@ -70,19 +76,58 @@ static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
 namespace {
 
 std::mutex g_addr_mu;
-unsigned char *g_addr[128] = {};
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;   // unique id of the context the address belongs to
+    unsigned char *addr = nullptr;
+};
+ScratchAddr g_addr[128];
 
-// device address of g_static_scratch on `dev` (which must be current), looked up once
+// The driver's context queries, fetched through the runtime (no link against libcuda).
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+
+// Unique id of the current context (0 if none is current or the driver cannot say).
+unsigned long long current_context_id() {
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PfnCtxGetId>(f);
+        looked_up = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Set-up, once per device and context: the device address of g_static_scratch on `dev`, which
+// must be current.  The lookup allocates nothing.
 cudaError_t scratch_address(int dev, unsigned char **out) {
     std::lock_guard<std::mutex> lk(g_addr_mu);
     if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
-    if (!g_addr[dev]) {
+    ScratchAddr &s = g_addr[dev];
+    unsigned long long id = current_context_id();
+    if (!s.addr || id == 0 || id != s.ctx_id) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) return e;
-        g_addr[dev] = static_cast<unsigned char *>(p);
+        s.addr = static_cast<unsigned char *>(p);
+        // the lookup made the device's primary context current if none was
+        if (id == 0) id = current_context_id();
+        s.ctx_id = id;
     }
-    *out = g_addr[dev];
+    *out = s.addr;
     return cudaSuccess;
 }
 
@@ -172,10 +217,11 @@ __global__ void k_fixup_s(int64_t ncell, const int32_t *start, int32_t *sorted) 
     }
 }
 
+// the caller's outputs are written only when every radius and material index was valid
 __global__ void k_unpack(int64_t n, const double4 *pr, const double *vw, const int32_t *uid,
-                         double *x, double *v, double *w) {
+                         const int32_t *err, double *x, double *v, double *w) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+    if (t >= n || (*err & (SERR_RADIUS | SERR_MATERIAL)) != 0) return;
     const int64_t i = uid[t];
     const double4 p = pr[t];
     x[3 * i] = p.x;
@@ -211,6 +257,7 @@ extern "C" int pe_b200_dem_step_static(int64_t n, const double *x, const double 
     if ((nplanes > 0 && (!planes || !plane_mat)) || (nboxes > 0 && (!boxes || !box_mat)))
         return PE_B200_ERR_ARG;
     if (!gravity || !domain_lo || !domain_hi || !(dt > 0.0) || !(max_radius > 0.0) ||
+        !isfinite(max_radius) ||
         !(damping >= 0.0 && damping <= 1.0))
         return PE_B200_ERR_ARG;
     if (n > 0 && (!x || !v || !w || !r || !mat || !x_out || !v_out || !w_out))
@@ -247,17 +294,13 @@ extern "C" int pe_b200_dem_step_static(int64_t n, const double *x, const double 
     }
     // grid: cells at least the largest AABB extent, coarsened to fit the fixed cell budget
     SceneInfo si = SceneInfo();
-    double h = 2.0 * (max_radius + kContactThreshold) * (1.0 + 1e-9);
-    int64_t dim[3], nc;
-    for (;;) {
-        nc = 1;
-        for (int a = 0; a < 3; ++a) {
-            dim[a] = (int64_t)floor((domain_hi[a] - domain_lo[a]) / h) + 1;
-            nc *= dim[a];
-        }
-        if (nc <= kMaxCells) break;
-        h *= 1.26;
-    }
+    StaticGrid grid;
+    if (!static_grid_plan(domain_lo, domain_hi, 2.0 * (max_radius + kContactThreshold) * (1.0 + 1e-9),
+                          kMaxCells, &grid))
+        return PE_B200_ERR_ARG;
+    const double h = grid.h;
+    const int64_t nc = grid.ncell;
+    const int64_t *dim = grid.dim;
     for (int a = 0; a < 3; ++a) {
         si.lo[a] = domain_lo[a];
         si.dim[a] = (int32_t)dim[a];
@@ -352,7 +395,8 @@ extern "C" int pe_b200_dem_step_static(int64_t n, const double *x, const double 
         a.cell_count = count;
         a.err = d_err;
         PEB_S(dem_launch_fp64_raw(a, st));
-        k_unpack<<<grid_for(n, 256), 256, 0, st>>>(n, pr_b, vw_b, uid_b, x_out, v_out, w_out);
+        k_unpack<<<grid_for(n, 256), 256, 0, st>>>(n, pr_b, vw_b, uid_b, d_err, x_out, v_out,
+                                                   w_out);
         PEB_S(cudaGetLastError());
     }
     int32_t herr = 0;

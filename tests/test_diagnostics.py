@@ -27,6 +27,21 @@ def test_host_checks_count_planted_inconsistencies(tmp_path):
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
 
 
+def test_static_step_grid_plan_coarsens_instead_of_overflowing(tmp_path):
+    """The allocation-free step's grid planner (pe_b200/csrc/static_grid.h) on wide domains and
+    tiny radii (e.g. +-1e6 with r = 1e-3, whose finest grid would overflow int64) and on
+    domains it must refuse."""
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    exe = str(tmp_path / "static_grid_test")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "pe_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "static_grid_test.cpp"), "-o", exe],
+                   check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
 def test_contact_capacity_beyond_int32_is_rejected():
     with pytest.raises(PeB200Error) as ei:
         Engine(max_contacts=2 ** 31)
