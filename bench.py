@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--workload", default="dem_large_1m",
                     choices=["dem_large_1m", "dem_lattice_4096", "nbgs_box_32768", "ensemble_512"])
     ap.add_argument("--no-extras", action="store_true", help="headline measurement only")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the pe-on-one-core leg (minutes of set-up at 1M spheres)")
     ap.add_argument("--tuning", default=None,
                     help="dem_variant,rebuild_per_sm,skin instead of running the autotuner")
     return ap.parse_args()
@@ -86,15 +88,11 @@ def shard_scenes(ss, rank, world):
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
-def ref_sample_scene(workload):
-    """Bounded sample of the workload for the single-threaded reference: the same packing,
-    radii, materials and time step, on a smaller footprint (pe's body setup grows faster than
-    linearly with the body count)."""
+def ref_scene(workload):
+    """The workload's scene for the single-threaded reference, and its executable.  The single
+    scenes are the full configured scenes; for the ensemble, one median-size scene."""
     if workload == "dem_large_1m":
-        n = 262144
-        side = 200.0 * (n / 1048576) ** 0.5
-        return scenes.dem_large(0, n=n, dims=(side, side, 400.0)), "ref_dem", \
-            f"{n} spheres of the 1M DEM scene's packing on a {side:.0f}x{side:.0f} footprint"
+        return scenes.dem_large(0), "ref_dem", "the full 1,048,576-sphere scene"
     if workload == "dem_lattice_4096":
         return scenes.dem_lattice(0), "ref_dem", "the full 4096-sphere lattice scene"
     if workload == "nbgs_box_32768":
@@ -106,84 +104,68 @@ def ref_sample_scene(workload):
     raise ValueError(workload)
 
 
-def run_reference(workload, steps, warmup=1, budget_s=60.0):
-    exe_scene, exe, sample = ref_sample_scene(workload)
-    path = os.path.join(REF_DIR, exe)
-    if not os.path.exists(path):
-        return None, f"compiled reference missing ({path}); build with make -C oracle/ref"
-    with tempfile.TemporaryDirectory() as tmp:
-        sp = os.path.join(tmp, "scene.bin")
-        exe_scene.save(sp)
-        extra = ["0", "100"] if exe == "ref_hcsits" else []
-        # probe one step to size the timed sample within the budget
-        t0 = time.perf_counter()
-        r = subprocess.run([path, "time", sp, "0", "1", *extra], capture_output=True, text=True)
-        if r.returncode != 0:
-            return None, "reference run failed: " + r.stderr.strip()[-200:]
-        one = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
-        k = max(1, min(steps, int(budget_s / max(one, 1e-6))))
-        r = subprocess.run([path, "time", sp, str(warmup), str(k), *extra], capture_output=True,
-                           text=True)
-        if r.returncode != 0:
-            return None, "reference run failed: " + r.stderr.strip()[-200:]
-        res = json.loads(r.stdout.strip().splitlines()[-1])
-        res["wall_s"] = time.perf_counter() - t0
-        res["sample"] = f"{sample}; {k} timed steps after {warmup} warm-up"
-        res["cores"] = 1
-        return res, None
+# timed steps per reference process: pe needs ~3 minutes to set up the 1M-sphere scene (body
+# creation and the first hash-grid insertion) and then ~3 s per step on one core
+REF_STEPS = {"dem_large_1m": 6, "dem_lattice_4096": 200, "nbgs_box_32768": 10, "ensemble_512": 50}
 
 
-def run_reference_parallel(workload, steps, budget_s=60.0):
-    """pe is single-threaded, so the host's throughput is that of independent processes, one
-    per core: each runs its own sample of the workload (as many as the cores and half the free
-    memory allow) and the sphere-steps/s add up."""
-    if workload == "dem_large_1m":
-        n = 65536
-        side = 200.0 * (n / 1048576) ** 0.5
-        samples = [scenes.dem_large(0, n=n, dims=(side, side, 400.0))]
-        exe, what = "ref_dem", f"{n} spheres of the 1M DEM scene's packing ({side:.0f}x{side:.0f} footprint)"
-    else:
-        sc, exe, what = ref_sample_scene(workload)
-        samples = [sc]
-    path = os.path.join(REF_DIR, exe)
-    if not os.path.exists(path):
-        return None, f"compiled reference missing ({path}); build with make -C oracle/ref"
-    cores = os.cpu_count() or 1
-    try:
-        avail = int([l for l in open("/proc/meminfo") if l.startswith("MemAvailable")][0].split()[1]) * 1024
-    except (OSError, IndexError, ValueError):
-        avail = 8 << 30
-    with tempfile.TemporaryDirectory() as tmp:
+class RefRun:
+    """pe (oracle/_ref, compiled from pe's own sources) timing `steps` World::simulationStep
+    calls on a workload's scene, after `warmup` untimed ones, in `procs` concurrent
+    single-threaded processes that each advance their own copy of the scene (pe's step is
+    single-threaded; the host's throughput is the sum).  Started at once, collected by result()."""
+
+    def __init__(self, workload, steps, warmup=1, procs=1):
+        self.err = None
+        self.jobs = []
+        self.t0 = time.perf_counter()
+        sc, exe, what = ref_scene(workload)
+        self.n, self.steps, self.warmup, self.what = sc.n, steps, warmup, what
+        path = os.path.join(REF_DIR, exe)
+        if not os.path.exists(path):
+            self.err = f"compiled reference missing ({path}); build with make -C oracle/ref"
+            return
+        self.tmp = tempfile.TemporaryDirectory()
+        sp = os.path.join(self.tmp.name, "scene.bin")
+        sc.save(sp)
         extra = ["0", "100"] if exe == "ref_hcsits" else []
-        files = []
-        for k, sc in enumerate(samples[:cores]):
-            sp = os.path.join(tmp, f"scene{k}.bin")
-            sc.save(sp)
-            files.append((sp, sc.n))
-        # probe: one step of the first sample, and its memory
-        import resource
-        t0 = time.perf_counter()
-        r = subprocess.run([path, "time", files[0][0], "0", "1", *extra], capture_output=True, text=True)
-        if r.returncode != 0:
-            return None, "reference run failed: " + r.stderr.strip()[-200:]
-        one = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
-        rss = resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss * 1024
-        procs = max(1, min(cores, int(0.5 * avail / max(rss, 1 << 20))))
-        k = max(1, min(steps, int(budget_s / max(one, 1e-6))))
-        jobs = [subprocess.Popen([path, "time", files[q % len(files)][0], "1", str(k), *extra],
-                                 stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
-                for q in range(procs)]
+        self.procs = procs
+        self.jobs = [subprocess.Popen([path, "time", sp, str(warmup), str(steps), *extra],
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+                     for _ in range(procs)]
+
+    def result(self):
+        if self.err:
+            return None, self.err
         res = []
-        for j in jobs:
+        for j in self.jobs:
             out, err = j.communicate()
             if j.returncode != 0:
                 return None, "reference run failed: " + err.strip()[-200:]
             res.append(json.loads(out.strip().splitlines()[-1]))
+        wall = time.perf_counter() - self.t0
+        self.tmp.cleanup()
         total = sum(x["sphere_steps_per_s"] for x in res)
-        return {"sphere_steps_per_s": total, "steps": k, "seconds": max(x["seconds"] for x in res),
-                "cores": procs, "wall_s": time.perf_counter() - t0,
-                "sample": f"{procs} concurrent single-threaded processes, each {what}; {k} timed "
-                          f"steps after 1 warm-up; host has {cores} cores"}, None
+        cores = os.cpu_count() or 1
+        return {"sphere_steps_per_s": total, "steps": self.steps, "spheres": self.n,
+                "seconds": max(x["seconds"] for x in res), "cores": self.procs, "wall_s": wall,
+                "sample": f"{self.procs} concurrent single-threaded pe process(es), each on "
+                          f"{self.what}; {self.steps} timed steps after {self.warmup} untimed, "
+                          f"set-up excluded (whole run {wall:.1f} s); host has {cores} "
+                          f"cores"}, None
+
+
+def ref_procs(workload):
+    """Processes for the reference arm: one per host core, as far as half the free memory
+    allows (pe holds about 1.4 KB per sphere)."""
+    cores = os.cpu_count() or 1
+    try:
+        avail = int([l for l in open("/proc/meminfo")
+                     if l.startswith("MemAvailable")][0].split()[1]) * 1024
+    except (OSError, IndexError, ValueError):
+        avail = 8 << 30
+    n = ref_scene(workload)[0].n
+    return max(1, min(cores, int(0.5 * avail / max(1400 * n, 1 << 20))))
 
 
 # ------------------------------------------------------------------------------------------
@@ -354,8 +336,11 @@ def timed_chunks(e, dt, chunks, chunk, warmup, torch, flush_buf, stream):
 def adjoint_extra(torch):
     """The differentiable-DEM workload: 16384 spheres in the hopper, 2000 FP64 steps with a
     checkpoint every 100, gradient of final centre-of-mass height plus mass fraction below the
-    opening w.r.t. all initial velocities and k_n, c_n, mu; and the adjoint of the last 100-step
-    segment against central differences (h = 1e-6) of the GPU step and of the compiled pe."""
+    opening w.r.t. all initial velocities and k_n, c_n, mu.  Checked over the full horizon against
+    central differences of the GPU forward (parameters, and the four initial-velocity components
+    with the largest adjoint) and against pe's own FP64 central differences of the parameters
+    (tests/golden/hopper_fd.npz, made by the compiled reference); and over the last 100-step
+    segment, where every sphere near the floor is in contact, against GPU central differences."""
     from pe_b200 import _abi
     from pe_b200.adjoint import LossSpec, make_single_material, set_params
     from pe_b200.engine import Engine
@@ -379,6 +364,57 @@ def adjoint_extra(torch):
            "grad_params": {"k_n": gp[0], "c_n": gp[1], "c_t": gp[2], "mu": gp[3]},
            "grad_v0_linf": float(np.abs(gv0).max())}
     e.close()
+
+    def gpu_x(t, steps):
+        g = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(t)
+        g.step(t.dt, steps)
+        x = g.download()[0]
+        g.close()
+        return x
+
+    rel = lambda a, b: float(np.abs(np.asarray(a) - np.asarray(b)).max() /
+                             max(np.abs(np.asarray(b)).max(), 1e-300))
+    hp = {"k_n": 1e-1, "c_n": 1e-4, "mu": 1e-6}
+    pk = {"k_n": 0, "c_n": 1, "mu": 3}
+
+    def check(start, steps, gv, gpar):
+        flat = np.argsort(-np.abs(gv).ravel())[:4]
+        idx = [(int(f // 3), int(f % 3)) for f in flat]
+        h = 1e-6
+        fd = []
+        for (i, a) in idx:
+            sp_, sm_ = start.copy(), start.copy()
+            sp_.v[i, a] += h
+            sm_.v[i, a] -= h
+            fd.append(spec.diff(gpu_x(sp_, steps), gpu_x(sm_, steps)) / (2 * h))
+        pfd = {}
+        for key, hk in hp.items():
+            pp, pm = dict(p), dict(p)
+            pp[key] += hk
+            pm[key] -= hk
+            pfd[key] = spec.diff(gpu_x(set_params(start, **pp), steps),
+                                 gpu_x(set_params(start, **pm), steps)) / (2 * hk)
+        ad = [float(gv[i, a]) for i, a in idx]
+        return {"steps": steps, "h": h, "v_components": idx, "adjoint": ad, "fd_gpu": fd,
+                "rel_err_vs_fd_gpu": rel(ad, fd),
+                "params_adjoint": {k: float(gpar[j]) for k, j in pk.items()},
+                "params_fd_gpu": pfd,
+                "params_rel_err_vs_fd_gpu": {k: abs(gpar[j] - pfd[k]) / max(abs(pfd[k]), 1e-300)
+                                             for k, j in pk.items()}}
+
+    full = check(s, K, gv0, gp)
+    gold = os.path.join(ROOT, "tests", "golden", "hopper_fd.npz")
+    if os.path.exists(gold):
+        g = np.load(gold)
+        if int(g["steps"]) == K and int(g["spheres"]) == s.n:
+            ref = {k: float(g["fd_" + k]) for k in hp}
+            full["params_fd_reference"] = ref
+            full["params_rel_err_vs_fd_reference"] = {
+                k: abs(gp[j] - ref[k]) / max(abs(ref[k]), 1e-300) for k, j in pk.items()}
+            full["reference_fd_source"] = ("pe compiled from its sources, FP64 central "
+                                           "differences over the full horizon "
+                                           "(tests/golden/make_golden.py hopper_fd)")
+    out["full_horizon_check"] = full
     # the last segment: state after K - 100 steps, adjoint of 100 steps vs central differences
     e = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(s)
     e.step(s.dt, K - EVERY)
@@ -386,69 +422,13 @@ def adjoint_extra(torch):
     e.close()
     seg = s.copy()
     seg.x, seg.v, seg.w = xs, vs, ws
-
-    def gpu_x(t):
-        g = Engine(solver=_abi.DEM, precision=_abi.FP64, neighbor_lists=False).load_scene(t)
-        g.step(t.dt, EVERY)
-        x = g.download()[0]
-        g.close()
-        return x
-
     e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(seg)
     e.adjoint_forward(EVERY, s.dt, 10)
     xe = e.download()[0]
     _, gvs, _, gps = e.adjoint_backward(spec.grad(xe), z, z)
     e.close()
-    # velocity components of spheres with the largest adjoint (the ones in contact)
-    flat = np.argsort(-np.abs(gvs).ravel())[:4]
-    idx = [(int(f // 3), int(f % 3)) for f in flat]
-    h = 1e-6
-    fd, fdr = [], []
-    ref = os.path.join(REF_DIR, "ref_dem")
-    have_ref = os.path.exists(ref)
-
-    def ref_x(t, tmp):
-        sp = os.path.join(tmp, "seg.bin")
-        t.save(sp)
-        o = os.path.join(tmp, "o.bin")
-        subprocess.run([ref, "step", sp, str(EVERY), o], check=True)
-        a = np.fromfile(o, "<f8")
-        return a[:3 * t.n].reshape(t.n, 3)
-
-    with tempfile.TemporaryDirectory() as tmp:
-        for (i, a) in idx:
-            sp_, sm_ = seg.copy(), seg.copy()
-            sp_.v[i, a] += h
-            sm_.v[i, a] -= h
-            fd.append(spec.diff(gpu_x(sp_), gpu_x(sm_)) / (2 * h))
-            if have_ref:
-                fdr.append(spec.diff(ref_x(sp_, tmp), ref_x(sm_, tmp)) / (2 * h))
-        pfd, pfdr = {}, {}
-        for key, k, hp in (("k_n", 0, 1e-1), ("c_n", 1, 1e-4), ("mu", 3, 1e-6)):
-            pp, pm = dict(p), dict(p)
-            pp[key] += hp
-            pm[key] -= hp
-            pfd[key] = spec.diff(gpu_x(set_params(seg, **pp)), gpu_x(set_params(seg, **pm))) / (2 * hp)
-            if have_ref:
-                pfdr[key] = spec.diff(ref_x(set_params(seg, **pp), tmp),
-                                      ref_x(set_params(seg, **pm), tmp)) / (2 * hp)
-    ad = np.array([gvs[i, a] for i, a in idx])
-    fd = np.array(fd)
-    rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
-    segment = {"steps": EVERY, "from_step": K - EVERY, "h": h,
-               "v_components": idx, "adjoint": ad.tolist(), "fd_gpu": fd.tolist(),
-               "rel_err_vs_fd_gpu": rel(ad, fd),
-               "params_adjoint": {"k_n": gps[0], "c_n": gps[1], "mu": gps[3]},
-               "params_fd_gpu": pfd,
-               "params_rel_err_vs_fd_gpu": {k: abs(gps[j] - pfd[k]) / max(abs(pfd[k]), 1e-300)
-                                            for k, j in (("k_n", 0), ("c_n", 1), ("mu", 3))}}
-    if have_ref:
-        fdr = np.array(fdr)
-        segment.update({"fd_reference": fdr.tolist(), "rel_err_vs_fd_reference": rel(ad, fdr),
-                        "params_fd_reference": pfdr,
-                        "params_rel_err_vs_fd_reference": {
-                            k: abs(gps[j] - pfdr[k]) / max(abs(pfdr[k]), 1e-300)
-                            for k, j in (("k_n", 0), ("c_n", 1), ("mu", 3))}})
+    segment = check(seg, EVERY, gvs, gps)
+    segment["from_step"] = K - EVERY
     out["segment_check"] = segment
     return out
 
@@ -516,6 +496,11 @@ def our_arm(args):
     from pe_b200 import _abi
     from pe_b200.engine import Engine
 
+    # the cpu_baseline leg: pe on one host core over the same scene, started now (its set-up
+    # takes minutes at 1M spheres) and collected after the GPU measurements
+    ref_run = None
+    if world == 1 and not args.no_cpu_baseline:
+        ref_run = RefRun(args.workload, REF_STEPS[args.workload], warmup=1, procs=1)
     ss, kind = build_workload(args.workload, rank=rank, world=world)
     nsph = sum(s.n for s in ss)
     dt = ss[0].dt
@@ -618,6 +603,15 @@ def our_arm(args):
     e.close()
     if not args.no_extras:
         line.update(extras(args, torch, flush, dev, ss, kind, value))
+    if ref_run is not None:
+        ref, why = ref_run.result()
+        if ref:
+            line["cpu_baseline"] = {"value": ref["sphere_steps_per_s"], "unit": UNIT,
+                                    "cores": ref["cores"], "kind": "reference",
+                                    "sample": ref["sample"]}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0,
+                                    "kind": "reference", "sample": why}
     return line
 
 
@@ -654,6 +648,63 @@ def boxes_extra(torch, flush, dev):
                     rec["pe_one_core"] = {"ms_per_step": sec / 5 * 1e3,
                                           "body_steps_per_s": nb * 5 / sec}
         out[label] = rec
+    return out
+
+
+def nbgs_extra(torch, flush, dev):
+    """The 32,768-sphere hard-contact workload as specified (free fall in the 40x40x120 box, few
+    contacts) and a pre-settled dense variant (a lattice at the bottom of a 32x32x120 box, about
+    20,000 contacts), each frictionless (pe's InelasticFrictionlessContact) and with mu = 0.5
+    (pe's default ApproximateInelasticCoulombContactByDecoupling), 100 sweeps per step, mixed
+    precision and FP64.  Frictional runs report the FP64 complementarity residual of the last
+    step's impulses (one extra step with the residual enabled, after the timed ones); on the
+    4096-sphere dense packing the GPU's residual is reported beside the oracle's for the same
+    sweep counts (committed with the golden vectors)."""
+    from pe_b200 import _abi
+    out = {}
+    variants = (("nbgs_32k", lambda mu: scenes.nbgs_box(0, mu=mu)),
+                ("nbgs_32k_dense", lambda mu: scenes.nbgs_box(0, n=32768, mu=mu,
+                                                              dims=(32.0, 32.0, 120.0),
+                                                              dense=True)))
+    for label, make in variants:
+        for mu in (0.0, 0.5):
+            sc = make(mu)
+            key = label if mu == 0.0 else label + "_mu0.5"
+            for prec, name in ((_abi.MIXED, "mixed"), (_abi.FP64, "fp64")):
+                e = make_engine([sc], "hcsits", prec)
+                st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+                ksteps = 10
+                ms, _, prof = timed_steps(e, sc.dt, ksteps, 2, torch, flush, st)
+                stt = e.stats()
+                rec = {"value": sc.n * ksteps / (ms / 1e3), "ms_per_step": ms / ksteps,
+                       "contacts": stt["contacts"], "colors": stt["colors"], "sweeps": 100,
+                       "model": "approx_coulomb_decoupling" if mu > 0 else "frictionless",
+                       "stages_ms_per_step": {a: b[0] / ksteps for a, b in prof.items() if b[1]}}
+                if mu > 0:
+                    e.set_residual(True)
+                    e.step(sc.dt)
+                    rec["residual_fp64"] = e.stats()["residual"]
+                    rec["residual_note"] = ("max over contacts of the complementarity residual, "
+                                            "velocity units, after 100 sweeps of one step")
+                out.setdefault(key, {})[name] = rec
+                e.close()
+    gold = os.path.join(ROOT, "tests", "golden", "dense4096_conv.npz")
+    if os.path.exists(gold):
+        g = np.load(gold)
+        sc = scenes.nbgs_box(0, n=4096, mu=0.5, dims=(16.0, 16.0, 60.0), dense=True)
+        rows = []
+        for k, r_or in zip(g["mu05_sweeps"], g["mu05_residual_oracle"]):
+            e = make_engine([sc], "hcsits", _abi.FP64, iters=int(k))
+            e.set_residual(True)
+            e.step(sc.dt)
+            stt = e.stats()
+            e.close()
+            rows.append({"sweeps": int(k), "residual_gpu_fp64": stt["residual"],
+                         "residual_oracle": float(r_or)})
+        out["nbgs_4096_dense_mu0.5_residual_vs_oracle"] = {
+            "spheres": sc.n, "contacts": int(g["contacts"]), "rows": rows,
+            "note": "same packing and model; the oracle sweeps in pe's detection order, the GPU "
+                    "colour by colour"}
     return out
 
 
@@ -724,30 +775,9 @@ def extras(args, torch, flush, dev, ss, kind, mixed_value):
                                "stages_ms_per_step": {a: b[0] / k for a, b in prof.items() if b[1]}}
         e.close()
         out["adjoint_hopper_16384"] = adjoint_extra(torch)
-        for label, sc in (("nbgs_32k", scenes.nbgs_box(0)),
-                          ("nbgs_32k_dense", scenes.nbgs_box(0, n=32768, dims=(32.0, 32.0, 120.0),
-                                                            dense=True))):
-            for prec, name in ((_abi.MIXED, "mixed"), (_abi.FP64, "fp64")):
-                e = make_engine([sc], "hcsits", prec)
-                st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
-                ksteps = 10
-                ms, _, prof = timed_steps(e, sc.dt, ksteps, 2, torch, flush, st)
-                stt = e.stats()
-                out.setdefault(label, {})[name] = {
-                    "value": sc.n * ksteps / (ms / 1e3), "ms_per_step": ms / ksteps,
-                    "contacts": stt["contacts"], "colors": stt["colors"], "sweeps": 100,
-                    "stages_ms_per_step": {a: b[0] / ksteps for a, b in prof.items() if b[1]}}
-                e.close()
+        out.update(nbgs_extra(torch, flush, dev))
     if args.workload == "dem_large_1m":
         out["moving_boxes"] = boxes_extra(torch, flush, dev)
-    ref, why = run_reference(args.workload, steps=10, budget_s=20.0)
-    if ref:
-        out["cpu_baseline"] = {"value": ref["sphere_steps_per_s"], "unit": UNIT,
-                               "cores": ref["cores"], "kind": "reference",
-                               "sample": ref["sample"]}
-    else:
-        out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                               "sample": why}
     return out
 
 
@@ -769,16 +799,22 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    ref, why = run_reference_parallel(args.workload, steps=max(1, args.steps), budget_s=60.0)
+    procs = ref_procs(args.workload)
+    run = RefRun(args.workload, REF_STEPS[args.workload], warmup=1, procs=procs)
+    ref, why = run.result()
     if not ref:
         return {"impl": "reference", "unavailable": why}
     v = ref["sphere_steps_per_s"]
+    sc = ref_scene(args.workload)[0]
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": ref["steps"],
-            "warmup": args.warmup, "ms_per_step": 1e3 * ref["seconds"] / ref["steps"],
+            "warmup": 1, "ms_per_step": 1e3 * ref["seconds"] / ref["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "precision": "fp64 (pe compiled -O3 -DNDEBUG)"},
+            "config": {"workload": args.workload, "spheres": sc.n, "spheres_per_rank": sc.n,
+                       "scenes": 1, "dt": sc.dt,
+                       "precision": "fp64 (pe's real; compiled -O3 -DNDEBUG from its sources)",
+                       "parallelism": f"{procs} host processes, each the whole scene"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": ref["cores"], "kind": "reference",
                              "sample": ref["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -189,9 +189,92 @@ def hertz_goldens():
     golden("hertz64_planes", hertz_scene(2), dem_steps=(1, 10), hc=False, dem_exe="ref_dem_hertz")
 
 
+def dense_converged(name="dense4096_conv", iters=20000):
+    """A dense packing with thousands of contacts: 4096 spheres on a 16x16x16 lattice of spacing
+    1.0 (radii U[0.45, 0.55], so about half of the neighbours touch or overlap) resting on the
+    floor of a box of planes, 6,593 contacts.  pe's frictionless HCSITS step with `iters` sweeps
+    (its velocities change by < 1e-13 relative between 16,000 and 64,000 sweeps, so they are the
+    unique converged ones) and the scene."""
+    s = scenes.nbgs_box(0, n=4096, dims=(16.0, 16.0, 60.0), dense=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        sp = os.path.join(tmp, "scene.bin")
+        s.save(sp)
+        x, v, w, _ = run_steps("ref_hcsits", sp, s.n, 1, tmp, (0, iters))
+        ncont = len(run_pairs("ref_hcsits", sp, tmp))
+    rec = {"scene": np.frombuffer(s.to_bytes(), np.uint8), "hc0conv_x": x, "hc0conv_v": v,
+           "hc0conv_w": w, "iters": iters, "contacts": ncont}
+    # the same packing with mu = 0.5 under pe's default model (approximate Coulomb friction by
+    # decoupling): pe reports no residual, so the oracle's complementarity residual (its
+    # restatement of that model, pinned bit for bit to pe in pe's contact order) after a given
+    # number of sweeps is the reference for the frictional runs
+    from oracle.pe_oracle import APPROX_COULOMB_DECOUPLING, OracleWorld
+    sf = scenes.nbgs_box(0, n=4096, mu=0.5, dims=(16.0, 16.0, 60.0), dense=True)
+    assert np.array_equal(sf.x, s.x) and np.array_equal(sf.r, s.r)
+    sweeps = np.array([100, 1000, 4000])
+    res = []
+    for k in sweeps:
+        o = OracleWorld(sf)
+        res.append(o.hcsits_step(sf.dt, APPROX_COULOMB_DECOUPLING, int(k))[2])
+    rec["mu05_sweeps"], rec["mu05_residual_oracle"] = sweeps, np.array(res)
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **rec)
+    print(path, os.path.getsize(path), "bytes,", ncont, "contacts")
+
+
+def hopper_fd(name="hopper_fd"):
+    """pe's own FP64 central differences of the hopper workload's loss over its full horizon
+    (16,384 spheres, 2000 steps) with respect to k_n, c_n and mu: the scene of
+    pe_b200.scenes.hopper(0) with one material whose composed coefficients equal the hopper's
+    (so that a derivative with respect to the composed value is one with respect to the
+    material's), the loss of pe_b200.adjoint.LossSpec with the opening at z = 10, the steps of
+    the adjoint checks (k_n 1e-1, c_n 1e-4, mu 1e-6).  The six runs go to six processes."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from pe_b200.adjoint import LossSpec, make_single_material, set_params
+
+    s0 = scenes.hopper(0)
+    m = s0.materials[0]
+    p = {"k_n": m[6] / 2, "c_n": m[7] / 2, "c_t": m[8] / 2, "mu": 2 * m[2]}
+    s = make_single_material(s0, **p)
+    spec = LossSpec.for_scene(s, z_open=10.0)
+    steps = s.steps
+    with tempfile.TemporaryDirectory() as tmp:
+        def final_x(args):
+            tag, t = args
+            d = os.path.join(tmp, tag)
+            os.makedirs(d)
+            sp = os.path.join(d, "scene.bin")
+            t.save(sp)
+            return run_steps("ref_dem", sp, t.n, steps, d)[0]
+
+        jobs = []
+        hs = {"k_n": 1e-1, "c_n": 1e-4, "mu": 1e-6}
+        for key, h in hs.items():
+            pp, pm = dict(p), dict(p)
+            pp[key] += h
+            pm[key] -= h
+            jobs.append((key + "_p", set_params(s, **pp)))
+            jobs.append((key + "_m", set_params(s, **pm)))
+        with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+            xs = dict(zip([j[0] for j in jobs], ex.map(final_x, jobs)))
+    rec = {"steps": steps, "spheres": s.n}
+    for key, h in hs.items():
+        rec["h_" + key] = h
+        rec["fd_" + key] = spec.diff(xs[key + "_p"], xs[key + "_m"]) / (2 * h)
+    path = os.path.join(OUT, name + ".npz")
+    np.savez_compressed(path, **rec)
+    print(path, {k: float(v) for k, v in rec.items()})
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["adjoint_fd"]:
         adjoint_fd()
+        sys.exit(0)
+    if sys.argv[1:] == ["hopper_fd"]:
+        hopper_fd()
+        sys.exit(0)
+    if sys.argv[1:] == ["dense"]:
+        dense_converged()
         sys.exit(0)
     if sys.argv[1:] == ["hertz"]:
         hertz_goldens()
@@ -213,6 +296,8 @@ if __name__ == "__main__":
            dem_steps=(1,), hc_converged=True)
     golden("loose125_boxes", scenes.small_random(4, n=125, overlap=0.0, with_boxes=True),
            dem_steps=(1,), hc_converged=True)
+    dense_converged()
+    hopper_fd()
     adjoint_fd()
     hertz_goldens()
     peb_fixture()

@@ -14,6 +14,11 @@ def load_golden(name):
     return d
 
 
+def load_golden_arrays(name):
+    """A golden file without a scene record (numbers only)."""
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
 def rel_err(a, b):
     """Norm-wise relative error max|a-b| / max|b| (0 when both vanish)."""
     a = np.asarray(a, np.float64)

@@ -40,6 +40,45 @@ def test_frictionless_mixed_precision_close_to_reference(name):
     assert rel_err(x - s.x, g["hc0conv_x"] - s.x) < 1e-4
 
 
+@pytest.mark.parametrize("precision,tol", [(_abi.FP64, 1e-6), (_abi.MIXED, 1e-4)])
+def test_dense_packing_converged_velocities_match_reference(precision, tol):
+    """4096 spheres on a 16x16x16 lattice of spacing 1.0 resting on the floor, 6,593 contacts
+    (about half of the neighbours overlap): the GPU's colour-ordered frictionless sweeps converge
+    to pe's converged velocities (pe: 20,000 sweeps in its detection order)."""
+    g = load_golden("dense4096_conv")
+    s = g["scene"]
+    e = hc_engine(s, _abi.INELASTIC_FRICTIONLESS, 20000, precision=precision)
+    e.step(s.dt)
+    x, v, w = e.download()
+    st = e.stats()
+    assert st["contacts"] == int(g["contacts"])
+    assert rel_err(v, g["hc0conv_v"]) < tol
+    assert rel_err(x - s.x, g["hc0conv_x"] - s.x) < tol
+    if precision == _abi.FP64:
+        assert rel_err(x, g["hc0conv_x"]) < 1e-9
+
+
+def test_dense_packing_friction_residual_like_oracle():
+    """The same 4096-sphere packing with mu = 0.5 under pe's default model (approximate Coulomb
+    friction by decoupling): after 1000 and 4000 sweeps the GPU's FP64 complementarity residual is
+    of the oracle's size for the same sweep count (the fixed-point problem is the same; the sweep
+    orders differ), and both shrink with the sweeps."""
+    g = load_golden("dense4096_conv")
+    s = scenes.nbgs_box(0, n=4096, mu=0.5, dims=(16.0, 16.0, 60.0), dense=True)
+    assert np.array_equal(s.x, g["scene"].x)
+    got = []
+    for k, r_or in zip(g["mu05_sweeps"], g["mu05_residual_oracle"]):
+        e = hc_engine(s, _abi.APPROX_INELASTIC_COULOMB_DECOUPLING, int(k))
+        e.set_residual(True)
+        e.step(s.dt)
+        st = e.stats()
+        e.close()
+        got.append(st["residual"])
+        if k >= 1000:
+            assert st["residual"] < 10.0 * float(r_or) + 1e-9, (k, st["residual"], r_or)
+    assert got[2] < got[1] < got[0]
+
+
 def test_contact_count_matches_oracle():
     s = scenes.nbgs_box(0, n=2000, dims=(12.0, 12.0, 30.0), dense=True)
     e = hc_engine(s, _abi.APPROX_INELASTIC_COULOMB_DECOUPLING, 10)

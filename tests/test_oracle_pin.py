@@ -66,6 +66,18 @@ def test_hcsits_converged_frictionless_any_order(name):
     assert rel_err(o.x, g["hc0conv_x"]) < 1e-9
 
 
+def test_dense_converged_frictionless_matches_reference():
+    """The dense 4096-sphere packing (6,593 contacts): the oracle's converged frictionless
+    velocities after 16,000 sweeps in its own order equal pe's after 20,000 to 1e-6."""
+    g = load_golden("dense4096_conv")
+    s = g["scene"]
+    assert int(g["contacts"]) == len(OracleWorld(s).contacts())
+    o = OracleWorld(s)
+    o.hcsits_step(s.dt, FRICTIONLESS, 16000)
+    assert rel_err(o.v, g["hc0conv_v"]) < 1e-6
+    assert rel_err(o.x, g["hc0conv_x"]) < 1e-9
+
+
 REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
 
 
