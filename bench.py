@@ -333,6 +333,13 @@ def timed_chunks(e, dt, chunks, chunk, warmup, torch, flush_buf, stream):
     return sum(a.elapsed_time(b) for a, b in evs), e.kernel_launches() - l0, e.graph_active()
 
 
+# steps of the adjoint checks' finite differences, largest first (the first is the step the
+# gradient checks use elsewhere): the composed k_n, c_n, mu, and initial velocities
+HOPPER_PARAM_STEPS = {"k_n": (1e-1, 1e-2, 1e-3), "c_n": (1e-4, 1e-5, 1e-6),
+                      "mu": (1e-5, 1e-6, 1e-7)}
+HOPPER_V_STEPS = (1e-6, 1e-7, 1e-8)
+
+
 def adjoint_extra(torch):
     """The differentiable-DEM workload: 16384 spheres in the hopper, 2000 FP64 steps with a
     checkpoint every 100, gradient of final centre-of-mass height plus mass fraction below the
@@ -372,46 +379,62 @@ def adjoint_extra(torch):
         g.close()
         return x
 
-    rel = lambda a, b: float(np.abs(np.asarray(a) - np.asarray(b)).max() /
-                             max(np.abs(np.asarray(b)).max(), 1e-300))
-    hp = {"k_n": 1e-1, "c_n": 1e-4, "mu": 1e-6}
+    from pe_b200.adjoint import difference_ladder
     pk = {"k_n": 0, "c_n": 1, "mu": 3}
+    relerr = lambda a, b: abs(a - b) / max(abs(b), 1e-300)
 
     def check(start, steps, gv, gpar):
+        """Adjoint against finite differences of the GPU forward from `start`: the parameters
+        and the four initial-velocity components with the largest adjoint, each at a ladder
+        of steps (the first is the step of the other checks; see difference_ladder)."""
+        cache = {}
+
+        def xs(key, off, make):
+            if off == 0.0:
+                key = "base"
+            if (key, off) not in cache:
+                cache[(key, off)] = gpu_x(make(off), steps)
+            return cache[(key, off)]
+
+        res = {}
         flat = np.argsort(-np.abs(gv).ravel())[:4]
-        idx = [(int(f // 3), int(f % 3)) for f in flat]
-        h = 1e-6
-        fd = []
-        for (i, a) in idx:
-            sp_, sm_ = start.copy(), start.copy()
-            sp_.v[i, a] += h
-            sm_.v[i, a] -= h
-            fd.append(spec.diff(gpu_x(sp_, steps), gpu_x(sm_, steps)) / (2 * h))
-        pfd = {}
-        for key, hk in hp.items():
-            pp, pm = dict(p), dict(p)
-            pp[key] += hk
-            pm[key] -= hk
-            pfd[key] = spec.diff(gpu_x(set_params(start, **pp), steps),
-                                 gpu_x(set_params(start, **pm), steps)) / (2 * hk)
-        ad = [float(gv[i, a]) for i, a in idx]
-        return {"steps": steps, "h": h, "v_components": idx, "adjoint": ad, "fd_gpu": fd,
-                "rel_err_vs_fd_gpu": rel(ad, fd),
-                "params_adjoint": {k: float(gpar[j]) for k, j in pk.items()},
-                "params_fd_gpu": pfd,
-                "params_rel_err_vs_fd_gpu": {k: abs(gpar[j] - pfd[k]) / max(abs(pfd[k]), 1e-300)
-                                             for k, j in pk.items()}}
+        quantities = [(k, float(gpar[j]), HOPPER_PARAM_STEPS[k],
+                       lambda off, k=k: set_params(start, **dict(p, **{k: p[k] + off})))
+                      for k, j in pk.items()]
+        for f in flat:
+            i, a = int(f // 3), int(f % 3)
+
+            def mv(off, i=i, a=a):
+                t = start.copy()
+                t.v[i, a] += off
+                return t
+            quantities.append((f"v[{i}][{a}]", float(gv[i, a]), HOPPER_V_STEPS, mv))
+        for name, ad, hs, make in quantities:
+            rows, ch = difference_ladder(
+                lambda u, w, name=name, make=make: spec.diff(xs(name, u, make), xs(name, w, make)),
+                hs)
+            res[name] = {"adjoint": ad, "ladder": rows, "chosen_h": ch["h"],
+                         "rel_err": relerr(ad, ch["central"]),
+                         "rel_err_at_first_h": relerr(ad, rows[0]["central"])}
+        return {"steps": steps, "quantities": res,
+                "max_rel_err": max(q["rel_err"] for q in res.values())}
 
     full = check(s, K, gv0, gp)
     gold = os.path.join(ROOT, "tests", "golden", "hopper_fd.npz")
     if os.path.exists(gold):
         g = np.load(gold)
         if int(g["steps"]) == K and int(g["spheres"]) == s.n:
-            ref = {k: float(g["fd_" + k]) for k in hp}
-            full["params_fd_reference"] = ref
-            full["params_rel_err_vs_fd_reference"] = {
-                k: abs(gp[j] - ref[k]) / max(abs(ref[k]), 1e-300) for k, j in pk.items()}
-            full["reference_fd_source"] = ("pe compiled from its sources, FP64 central "
+            ref = {}
+            for k, j in pk.items():
+                rows = [{"h": float(h), "forward": float(fw), "backward": float(bw),
+                         "central": 0.5 * float(fw + bw),
+                         "smooth": bool(abs(fw - bw) <= 1e-4 * abs(0.5 * (fw + bw)))}
+                        for h, fw, bw in zip(g["h_" + k], g["fwd_" + k], g["bwd_" + k])]
+                ch = next((r for r in rows if r["smooth"]), rows[-1])
+                ref[k] = {"ladder": rows, "chosen_h": ch["h"],
+                          "rel_err": relerr(float(gp[j]), ch["central"])}
+            full["reference_params"] = ref
+            full["reference_fd_source"] = ("pe compiled from its sources, FP64 one-sided "
                                            "differences over the full horizon "
                                            "(tests/golden/make_golden.py hopper_fd)")
     out["full_horizon_check"] = full

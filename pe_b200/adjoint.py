@@ -78,6 +78,29 @@ class LossSpec:
         return g
 
 
+def difference_ladder(diff, hs, smooth_tol=1e-4):
+    """Finite differences of a loss at each step h of the ladder `hs` (largest first).
+
+    diff(a, b) returns loss(input + a) - loss(input + b), summed term by term (LossSpec.diff of
+    two runs).  For each h: the forward difference (L(p+h) - L(p)) / h, the backward difference
+    (L(p) - L(p-h)) / h and the central difference (their mean).  A DEM loss is only piecewise
+    smooth: pe's dashpot force jumps from 0 to c_n v_n when a contact starts, so when a
+    perturbation moves some contact's first step across a step boundary inside [p - h, p + h],
+    the difference quotient picks up that jump.  The forward and backward differences then
+    disagree; `smooth` marks the steps where they agree to smooth_tol (relative).  `chosen` is
+    the largest smooth step (the smallest step when none is), the one a derivative is checked
+    against."""
+    rows = []
+    for h in hs:
+        fwd = diff(h, 0.0) / h
+        bwd = diff(0.0, -h) / h
+        cen = 0.5 * (fwd + bwd)
+        rows.append({"h": h, "forward": fwd, "backward": bwd, "central": cen,
+                     "smooth": bool(abs(fwd - bwd) <= smooth_tol * max(abs(cen), 1e-300))})
+    chosen = next((r for r in rows if r["smooth"]), rows[-1])
+    return rows, chosen
+
+
 def _coeffs(s):
     m = s.materials[0]
     return {"k_n": m[6] / 2.0, "c_n": m[7] / 2.0, "c_t": m[8] / 2.0, "mu": m[2] + m[2]}

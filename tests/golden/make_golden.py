@@ -221,13 +221,21 @@ def dense_converged(name="dense4096_conv", iters=20000):
     print(path, os.path.getsize(path), "bytes,", ncont, "contacts")
 
 
+# steps of the hopper's finite differences, largest first: k_n, c_n and mu (the composed
+# coefficients; the hopper has k_n = 5e4, c_n = 25, mu = 0.4)
+HOPPER_PARAM_STEPS = {"k_n": (1e-1, 1e-2, 1e-3), "c_n": (1e-4, 1e-5, 1e-6),
+                      "mu": (1e-5, 1e-6, 1e-7)}
+
+
 def hopper_fd(name="hopper_fd"):
-    """pe's own FP64 central differences of the hopper workload's loss over its full horizon
+    """pe's own FP64 finite differences of the hopper workload's loss over its full horizon
     (16,384 spheres, 2000 steps) with respect to k_n, c_n and mu: the scene of
     pe_b200.scenes.hopper(0) with one material whose composed coefficients equal the hopper's
     (so that a derivative with respect to the composed value is one with respect to the
-    material's), the loss of pe_b200.adjoint.LossSpec with the opening at z = 10, the steps of
-    the adjoint checks (k_n 1e-1, c_n 1e-4, mu 1e-6).  The six runs go to six processes."""
+    material's), the loss of pe_b200.adjoint.LossSpec with the opening at z = 10.  For every step
+    of HOPPER_PARAM_STEPS the forward and backward one-sided differences are stored (their
+    disagreement shows a contact onset crossed inside the step).  The runs go to parallel
+    processes."""
     from concurrent.futures import ThreadPoolExecutor
 
     from pe_b200.adjoint import LossSpec, make_single_material, set_params
@@ -247,23 +255,26 @@ def hopper_fd(name="hopper_fd"):
             t.save(sp)
             return run_steps("ref_dem", sp, t.n, steps, d)[0]
 
-        jobs = []
-        hs = {"k_n": 1e-1, "c_n": 1e-4, "mu": 1e-6}
-        for key, h in hs.items():
-            pp, pm = dict(p), dict(p)
-            pp[key] += h
-            pm[key] -= h
-            jobs.append((key + "_p", set_params(s, **pp)))
-            jobs.append((key + "_m", set_params(s, **pm)))
-        with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        jobs = [("base", s)]
+        for key, hs in HOPPER_PARAM_STEPS.items():
+            for k, h in enumerate(hs):
+                pp, pm = dict(p), dict(p)
+                pp[key] += h
+                pm[key] -= h
+                jobs.append((f"{key}_{k}_p", set_params(s, **pp)))
+                jobs.append((f"{key}_{k}_m", set_params(s, **pm)))
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
             xs = dict(zip([j[0] for j in jobs], ex.map(final_x, jobs)))
     rec = {"steps": steps, "spheres": s.n}
-    for key, h in hs.items():
-        rec["h_" + key] = h
-        rec["fd_" + key] = spec.diff(xs[key + "_p"], xs[key + "_m"]) / (2 * h)
+    for key, hs in HOPPER_PARAM_STEPS.items():
+        rec["h_" + key] = np.array(hs)
+        rec["fwd_" + key] = np.array([spec.diff(xs[f"{key}_{k}_p"], xs["base"]) / h
+                                      for k, h in enumerate(hs)])
+        rec["bwd_" + key] = np.array([spec.diff(xs["base"], xs[f"{key}_{k}_m"]) / h
+                                      for k, h in enumerate(hs)])
     path = os.path.join(OUT, name + ".npz")
     np.savez_compressed(path, **rec)
-    print(path, {k: float(v) for k, v in rec.items()})
+    print(path, {k: v.tolist() if hasattr(v, "tolist") else v for k, v in rec.items()})
 
 
 if __name__ == "__main__":
