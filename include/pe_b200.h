@@ -158,6 +158,12 @@ int32_t pe_b200_box_count(const pe_b200_ctx *ctx);
  * to keep that field).  Replaces: RigidBody::setPosition / setLinearVel / setAngularVel. */
 int pe_b200_set_state(pe_b200_ctx *ctx, const double *x, const double *v, const double *w);
 
+/* Overwrites the orientations of the uploaded spheres (4 doubles each, unit quaternion w x y z,
+ * upload order; they start as the identity).  Contexts created with track_orientation = 1 only
+ * (PE_B200_ERR_STATE otherwise).  Replaces: RigidBody::setOrientation
+ * (src/core/rigidbody/Sphere.cpp:319-332). */
+int pe_b200_set_orientations(pe_b200_ctx *ctx, const double *q);
+
 /* Advances every scene by nsteps steps of size dt.
  * Replaces: World::simulationStep (src/core/World.cpp:330-357) ->
  * CollisionSystem::simulationStep (DEMSolver.h:1155-1262, HCSITS.h:1472-1520).

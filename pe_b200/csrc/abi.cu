@@ -707,6 +707,16 @@ int pe_b200_set_state(pe_b200_ctx *h, const double *x, const double *v, const do
     return PE_B200_OK;
 }
 
+int pe_b200_set_orientations(pe_b200_ctx *h, const double *q) {
+    Ctx *c = reinterpret_cast<Ctx *>(h);
+    if (!c || !q) return PE_B200_ERR_ARG;
+    if (!c->uploaded) return set_err(c, PE_B200_ERR_STATE, "no bodies uploaded");
+    if (!c->p.track_orientation)
+        return set_err(c, PE_B200_ERR_STATE, "orientations are not tracked by this context");
+    cudaSetDevice(c->device);
+    return scatter_orientations(c, q);
+}
+
 int pe_b200_step(pe_b200_ctx *h, int32_t nsteps, double dt) {
     Ctx *c = reinterpret_cast<Ctx *>(h);
     if (!c) return PE_B200_ERR_ARG;

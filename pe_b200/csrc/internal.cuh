@@ -327,6 +327,7 @@ int pack_bodies(Ctx *c, const double *x, const double *v, const double *w, const
                 const int32_t *mat, const int32_t *scene);
 int unpack_bodies(Ctx *c, double *x, double *v, double *w, double *q);
 int scatter_state(Ctx *c, const double *x, const double *v, const double *w);
+int scatter_orientations(Ctx *c, const double *q);
 void stage_free(Ctx *c);
 // autotune.cu
 int set_list_skin(Ctx *c, double skin);

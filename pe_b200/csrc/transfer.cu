@@ -70,6 +70,14 @@ __global__ void k_scatter_state(int64_t n, const int32_t *uid, const double *x, 
     }
 }
 
+// overwrite the orientations (w x y z per body, upload order) of the bodies
+__global__ void k_scatter_q(int64_t n, const int32_t *uid, const double *q, double4 *qd) {
+    GRID_STRIDE(t, n) {
+        const int64_t i = uid[t];
+        qd[t] = make_double4(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+    }
+}
+
 int stage_reserve(Ctx *c, size_t bytes) {
     if (c->stage_bytes >= bytes) return PE_B200_OK;
     cudaFree(c->stage);
@@ -169,6 +177,19 @@ int scatter_state(Ctx *c, const double *x, const double *v, const double *w) {
     else
         k_scatter_state<float><<<g, 256, 0, c->stream>>>(n, c->cur.uid, x ? s.x : nullptr, v ? s.v : nullptr,
                                                          w ? s.w : nullptr, c->cur.pr, (float *)c->cur.vw);
+    PEB_LAUNCHED(c);
+    return PE_B200_OK;
+}
+
+int scatter_orientations(Ctx *c, const double *q) {
+    const int64_t n = c->n;
+    if (n == 0) return PE_B200_OK;
+    int rc = stage_reserve(c, stage_size(n));
+    if (rc) return rc;
+    const StageView s = stage_layout(c);
+    PEB_CUDA(c, cudaMemcpyAsync(s.r, q, 4 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+    k_scatter_q<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->cur.uid, s.r, c->cur.q);
     PEB_LAUNCHED(c);
     return PE_B200_OK;
 }
