@@ -105,6 +105,9 @@ void free_device(Ctx *c) {
     cudaFree(c->cell_count);
     cudaFree(c->cell_start);
     cudaFree(c->scan_tmp);
+    cudaFree(c->tile_list);
+    c->tile_list = nullptr;
+    c->tile_cap = 0;
     cudaFree(c->d_scenes);
     cudaFree(c->d_mats);
     cudaFree(c->d_planes);
@@ -319,7 +322,7 @@ void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int6
 // plus the neighbour-list skin, so that the 27 cells around a body hold every body closer than
 // r_i + r_j + skin; grown if the grid would be much larger than the body count.
 void plan_cells(Ctx *c, double skin) {
-    int64_t base = 0;
+    int64_t base = 0, tiles = 0;
     for (int s = 0; s < c->nscenes; ++s) {
         SceneInfo &si = c->scenes[s];
         const double *lo = &c->plan_bounds[6 * s], *hi = &c->plan_bounds[6 * s + 3];
@@ -344,8 +347,13 @@ void plan_cells(Ctx *c, double skin) {
         si.rmax = c->plan_rmax[s];
         si.cell_base = base;
         base += nc;
+        si.tile_w = (int32_t)std::min<int64_t>(kTileCells, dim[0]);
+        si.nseg = (int32_t)((dim[0] + si.tile_w - 1) / si.tile_w);
+        si.tile_base = tiles;
+        tiles += (int64_t)si.nseg * dim[1] * dim[2];
     }
     c->ncell = base;
+    c->ntiles = tiles;
 }
 
 
@@ -751,6 +759,7 @@ int pe_b200_get_tuning(pe_b200_ctx *h, pe_b200_tuning *out) {
     out->ms_per_step = -1.0;
     out->variants = dem_variant_count();
     out->nbgs_sweeps = c->tune.nbgs_sweeps;
+    out->dem_grid = c->tune.dem_grid;
     return PE_B200_OK;
 }
 
@@ -763,6 +772,7 @@ int pe_b200_set_tuning(pe_b200_ctx *h, const pe_b200_tuning *t) {
     tu.dem_variant = t->dem_variant;
     tu.rebuild_per_sm = t->rebuild_per_sm;
     tu.nbgs_sweeps = t->nbgs_sweeps;
+    tu.dem_grid = t->dem_grid;
     return set_tuning(c, tu, c->nl.enabled ? t->skin : c->nl.skin);
 }
 

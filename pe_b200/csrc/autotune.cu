@@ -66,9 +66,10 @@ int set_list_skin(Ctx *c, double skin) {
 
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
     if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < -1 ||
-        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 4)
+        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 4 || t.dem_grid < 0 || t.dem_grid > 1)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
     c->tune.nbgs_sweeps = t.nbgs_sweeps;
+    c->tune.dem_grid = t.dem_grid;
     if (t.dem_variant != c->tune.dem_variant || t.rebuild_per_sm != c->tune.rebuild_per_sm) {
         c->tune = t;
         c->epoch++;
@@ -167,6 +168,7 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
         out->ms_per_step = best_ms;
         out->variants = dem_variant_count();
         out->nbgs_sweeps = best.nbgs_sweeps;
+        out->dem_grid = c->tune.dem_grid;
     }
     return PE_B200_OK;
 }

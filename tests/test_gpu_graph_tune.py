@@ -210,3 +210,76 @@ def test_list_rebuild_forms_agree(name):
     xg, vg, _ = g.download()
     g.close()
     assert rel_err(out[0][0], xg) < 1e-9 and rel_err(out[0][1], vg) < 1e-6
+
+
+def _crowded(seed=0, side=22, big=2.5):
+    """Small spheres on a lattice around one large sphere: the large radius sets the cell edge
+    (2 r_max), so a tile's neighbourhood holds far more candidates than the grid step stages in
+    shared memory and those tiles search global memory instead."""
+    s = scenes.small_random(seed, n=side ** 3, overlap=0.02, with_boxes=False)
+    s.x = s.x * 0.22
+    s.r = s.r * 0.22
+    c = s.x.mean(0)
+    keep = np.linalg.norm(s.x - c, axis=1) > big + 0.2
+    t = s.copy()
+    t.x = np.vstack([s.x[keep], c[None, :]])
+    t.v = np.vstack([s.v[keep], np.zeros((1, 3))])
+    t.w = np.vstack([s.w[keep], np.zeros((1, 3))])
+    t.r = np.concatenate([s.r[keep], [big]])
+    t.mat = np.concatenate([s.mat[keep], s.mat[:1]]).astype(np.int32)
+    return t
+
+
+def _grid_run(s, precision, form, steps=6, scenes_list=None, **kw):
+    e = Engine(solver=_abi.DEM, precision=precision, neighbor_lists=False, **kw)
+    if scenes_list:
+        e.load_scenes(scenes_list)
+    else:
+        e.load_scene(s)
+    e.set_tuning(dem_grid=form)
+    e.step(s.dt, steps)
+    out = e.download()
+    boxes = e.download_boxes() if s.nmbox else None
+    e.close()
+    return out, boxes
+
+
+@pytest.mark.parametrize("case", ["lattice", "dense", "boxes_walls", "moving_boxes", "hertz",
+                                  "orientation", "mixed", "batched", "crowded"])
+def test_grid_step_forms_agree_bitwise(case):
+    """The tiled grid step (candidates staged in shared memory) and the one-thread-per-sphere
+    grid step sum the same contact forces in the same order: identical trajectories."""
+    kw, prec, ss = {}, _abi.FP64, None
+    if case == "lattice":
+        s = scenes.dem_lattice(2, side=14)
+    elif case == "dense":
+        s = scenes.nbgs_box(1, n=4096, dims=(16.0, 16.0, 60.0), dense=True)
+        s.dt = 1e-4
+    elif case == "boxes_walls":
+        s = scenes.small_random(31, n=1000, overlap=0.03, with_boxes=True)
+    elif case == "moving_boxes":
+        s = scenes.tumbling_boxes(1)
+    elif case == "hertz":
+        s = scenes.small_random(32, n=512, overlap=0.03)
+        kw["force_model"] = 1
+    elif case == "orientation":
+        s = scenes.small_random(33, n=512, overlap=0.03)
+        kw["track_orientation"] = True
+    elif case == "mixed":
+        s = scenes.dem_lattice(3, side=12)
+        prec = _abi.MIXED
+    elif case == "batched":
+        ss = [scenes.small_random(40 + k, n=100 + 50 * k, with_boxes=bool(k % 2)) for k in range(5)]
+        for t in ss:
+            t.dt = ss[0].dt
+        s = ss[0]
+    else:
+        s = _crowded()
+    a, ab = _grid_run(s, prec, 0, scenes_list=ss, **kw)
+    b, bb = _grid_run(s, prec, 1, scenes_list=ss, **kw)
+    assert np.isfinite(a[0]).all()
+    for u, w in zip(a, b):
+        assert np.array_equal(u, w), case
+    if ab is not None:
+        for u, w in zip(ab, bb):
+            assert np.array_equal(u, w), case
