@@ -242,9 +242,10 @@ typedef struct {
                                 barriers, 2 one cooperative grid with barriers through global
                                 memory, 3 one launch per colour, 4 one thread block with
                                 __syncthreads between colours (when every colour fits it) */
-    int32_t dem_grid;        /* DEM grid step (cell search every step): 0 tiles of cell rows with
-                                the candidates staged in shared memory, 1 one thread per sphere
-                                searching global memory (the same results) */
+    int32_t dem_grid;        /* DEM grid step (cell search every step): 0 candidates read from an
+                                FP32 position copy in cell order, with an exact FP64 test for the
+                                close ones; 1 every candidate through its FP64 record (the same
+                                results) */
 } pe_b200_tuning;
 int pe_b200_get_tuning(pe_b200_ctx *ctx, pe_b200_tuning *out);
 int pe_b200_set_tuning(pe_b200_ctx *ctx, const pe_b200_tuning *t);

@@ -105,9 +105,8 @@ void free_device(Ctx *c) {
     cudaFree(c->cell_count);
     cudaFree(c->cell_start);
     cudaFree(c->scan_tmp);
-    cudaFree(c->tile_list);
-    c->tile_list = nullptr;
-    c->tile_cap = 0;
+    cudaFree(c->posf);
+    c->posf = nullptr;
     cudaFree(c->d_scenes);
     cudaFree(c->d_mats);
     cudaFree(c->d_planes);
@@ -322,7 +321,7 @@ void plan_grids(Ctx *c, const double *x, const double *r, const std::vector<int6
 // plus the neighbour-list skin, so that the 27 cells around a body hold every body closer than
 // r_i + r_j + skin; grown if the grid would be much larger than the body count.
 void plan_cells(Ctx *c, double skin) {
-    int64_t base = 0, tiles = 0;
+    int64_t base = 0;
     for (int s = 0; s < c->nscenes; ++s) {
         SceneInfo &si = c->scenes[s];
         const double *lo = &c->plan_bounds[6 * s], *hi = &c->plan_bounds[6 * s + 3];
@@ -347,13 +346,8 @@ void plan_cells(Ctx *c, double skin) {
         si.rmax = c->plan_rmax[s];
         si.cell_base = base;
         base += nc;
-        si.tile_w = (int32_t)std::min<int64_t>(kTileCells, dim[0]);
-        si.nseg = (int32_t)((dim[0] + si.tile_w - 1) / si.tile_w);
-        si.tile_base = tiles;
-        tiles += (int64_t)si.nseg * dim[1] * dim[2];
     }
     c->ncell = base;
-    c->ntiles = tiles;
 }
 
 

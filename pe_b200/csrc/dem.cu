@@ -415,68 +415,27 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
     a.rank[t] = atomicAdd(&a.cell_count[kk], 1);
 }
 
-// ---- tiled grid step ---------------------------------------------------------------------------
-// The same step as k_dem_step with the 27-cell search served from shared memory.  A tile is a
-// segment of up to kTileCells cells of one cell row (scene, y, z); its spheres' candidates lie in
-// the 3 x 3 neighbouring rows, cells x0 - 1 .. x1 + 1, which are nine contiguous slot ranges of
-// the sorted order.  The block stages those candidates once (position relative to the tile in
-// FP32, radius, body index), and each sphere of the tile walks its 3 x 3 x 3 cells in
-// k_dem_step's order (z, y, slot), rejecting far candidates with an FP32 test whose margin
-// covers its rounding; the survivors take k_dem_step's exact FP64 test and pair force.  The
-// forces are therefore summed in the same order from the same terms: results are bitwise those of
-// k_dem_step.  Tiles whose neighbourhood exceeds the staging capacity search global memory.
-constexpr int kTileBlock = 128;
-constexpr int kTileCap = 1536;   // staged candidates (20 B each)
-
-// Non-empty tiles of this step, compacted with a warp ballot: list[0] counts, list[1..] holds
-// tile numbers (in no particular order; every tile is independent).
-__global__ void k_tiles(int64_t ntiles, int32_t nscenes, const SceneInfo *__restrict__ scenes,
-                        const int32_t *__restrict__ cell_start, int32_t *__restrict__ list) {
-    const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    bool busy = false;
-    if (tile < ntiles) {
-        int lo = 0, hi = nscenes - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (scenes[mid].tile_base <= tile) lo = mid;
-            else hi = mid - 1;
-        }
-        const SceneInfo &s = scenes[lo];
-        int64_t l = tile - s.tile_base;
-        const int seg = (int)(l % s.nseg);
-        l /= s.nseg;
-        const int y = (int)(l % s.dim[1]), z = (int)(l / s.dim[1]);
-        const int x0 = seg * s.tile_w, x1 = min(x0 + s.tile_w, s.dim[0]) - 1;
-        const int64_t k0 = cell_key(s, x0, y, z);
-        busy = cell_start[k0] != cell_start[k0 + (x1 - x0) + 1];
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, busy);
-    if (m == 0u) return;
-    const int lane = threadIdx.x & 31;
-    int base = 0;
-    if (lane == 0) base = atomicAdd(&list[0], __popc(m));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (busy) list[1 + base + __popc(m & ((1u << lane) - 1u))] = (int32_t)tile;
-}
-
-// The candidates of one tile's neighbourhood in shared memory.
-struct TileStage {
-    float4 pos[kTileCap];       // position relative to the tile origin, radius
-    int32_t idx[kTileCap];      // body index in the current buffers
-    int32_t row_slot[9];        // first sorted slot of each neighbour row (dz, dy)
-    int32_t row_off[10];        // offset of each row in pos/idx; row_off[9] = total
-};
-
+// ---- grid step with a sorted FP32 copy of the positions ---------------------------------------
+// The same step as k_dem_step with the 27-cell search reading, per candidate, one 16-byte record
+// of the sort's FP32 position copy (posf, slot order: consecutive candidates are consecutive
+// records, and no load waits on another) instead of the slot's body index and then its FP64
+// record.  Far candidates are rejected by an FP32 test whose margin covers its rounding; the
+// survivors take k_dem_step's exact FP64 test and pair force in k_dem_step's order, so the
+// results are bitwise those of k_dem_step.
 template <typename T, typename VT, bool HERTZ>
-__device__ __forceinline__ void tile_forces(const DemArgs<VT> &a, const SceneInfo &s,
-                                            const TileStage &st, double rx, double ry, double rz,
-                                            float tol, int32_t b, const double4 &pi, V3<T> vi,
-                                            V3<T> wi, int32_t uidi, const MatDev &mi,
-                                            Acc<T> &acc) {
+__device__ __forceinline__ void grid_forces_sorted(const DemArgs<VT> &a, const SceneInfo &s,
+                                                   const float4 *__restrict__ posf, int32_t b,
+                                                   const double4 &pi, V3<T> vi, V3<T> wi,
+                                                   int32_t uidi, const MatDev &mi, Acc<T> &acc) {
     int cx, cy, cz;
     cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
-    const int xa = max(cx - 1, 0), xb = min(cx + 1, s.dim[0] - 1);
-    const float pxf = float(pi.x - rx), pyf = float(pi.y - ry), pzf = float(pi.z - rz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    // coordinates relative to the grid origin, as the sort wrote them
+    const float pxf = float(pi.x - s.lo[0]), pyf = float(pi.y - s.lo[1]),
+                pzf = float(pi.z - s.lo[2]);
+    // |d_fp32 - d| stays below ~1e-7 (|x| + |y| + |z| + 2 r + d) for any partner closer than
+    // r_i + r_j; the margin is 100 times that
+    const float tol = 1e-5f * (1.0f + fabsf(pxf) + fabsf(pyf) + fabsf(pzf) + 4.0f * float(pi.w));
     const float prf = float(pi.w) + tol;
     for (int dz = -1; dz <= 1; ++dz) {
         const int z = cz + dz;
@@ -484,16 +443,15 @@ __device__ __forceinline__ void tile_forces(const DemArgs<VT> &a, const SceneInf
         for (int dy = -1; dy <= 1; ++dy) {
             const int y = cy + dy;
             if (y < 0 || y >= s.dim[1]) continue;
-            const int r = (dz + 1) * 3 + (dy + 1);
-            const int64_t c0 = cell_key(s, xa, y, z);
-            const int sb = a.cell_start[c0], se = a.cell_start[c0 + (xb - xa) + 1];
-            const int shift = st.row_off[r] - st.row_slot[r];
-            for (int slot = sb; slot < se; ++slot) {
-                const float4 q = st.pos[slot + shift];
+            const int64_t c0 = cell_key(s, x0, y, z);
+            const int64_t c1 = c0 + (x1 - x0) + 1;
+            const int e = a.cell_start[c1];
+            for (int slot = a.cell_start[c0]; slot < e; ++slot) {
+                const float4 q = posf[slot];
                 const float dx = pxf - q.x, dy2 = pyf - q.y, dz2 = pzf - q.z;
                 const float rs = prf + q.w;
                 if (dx * dx + dy2 * dy2 + dz2 * dz2 >= rs * rs) continue;
-                const int32_t j = st.idx[slot + shift];
+                const int32_t j = a.sorted[slot];
                 if (j == b) continue;
                 const double4 pj = a.pr[j];
                 const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
@@ -506,96 +464,37 @@ __device__ __forceinline__ void tile_forces(const DemArgs<VT> &a, const SceneInf
 }
 
 template <typename VT, bool TRACKQ, bool HERTZ>
-__global__ void __launch_bounds__(kTileBlock, 4)
-    k_dem_tile(DemArgs<VT> a, int32_t nscenes, const int32_t *__restrict__ list) {
+__global__ void __launch_bounds__(kDemBlock) k_dem_sorted(DemArgs<VT> a,
+                                                          const float4 *__restrict__ posf) {
     using T = VT;
-    __shared__ TileStage st;
-    const int32_t ntile = list[0];
-    for (int32_t it = blockIdx.x; it < ntile; it += gridDim.x) {
-        const int64_t tile = list[1 + it];
-        int lo = 0, hi = nscenes - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (a.scenes[mid].tile_base <= tile) lo = mid;
-            else hi = mid - 1;
-        }
-        const SceneInfo &s = a.scenes[lo];
-        int64_t l = tile - s.tile_base;
-        const int seg = (int)(l % s.nseg);
-        l /= s.nseg;
-        const int y = (int)(l % s.dim[1]), z = (int)(l / s.dim[1]);
-        const int x0 = seg * s.tile_w, x1 = min(x0 + s.tile_w, s.dim[0]) - 1;
-        const int64_t k0 = cell_key(s, x0, y, z);
-        const int own_b = a.cell_start[k0], own_e = a.cell_start[k0 + (x1 - x0) + 1];
-        __syncthreads();   // the previous tile's readers are done with the stage
-        if (threadIdx.x < 9) {
-            const int zz = z + (int)threadIdx.x / 3 - 1, yy = y + (int)threadIdx.x % 3 - 1;
-            int rb = 0, re = 0;
-            if (zz >= 0 && zz < s.dim[2] && yy >= 0 && yy < s.dim[1]) {
-                const int xa = max(x0 - 1, 0), xb = min(x1 + 1, s.dim[0] - 1);
-                const int64_t c0 = cell_key(s, xa, yy, zz);
-                rb = a.cell_start[c0];
-                re = a.cell_start[c0 + (xb - xa) + 1];
-            }
-            st.row_slot[threadIdx.x] = rb;
-            st.row_off[threadIdx.x + 1] = re - rb;   // counts; prefix below
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            st.row_off[0] = 0;
-            for (int r = 0; r < 9; ++r) st.row_off[r + 1] += st.row_off[r];
-        }
-        __syncthreads();
-        const int total = st.row_off[9];
-        const bool staged = total <= kTileCap;
-        // origin of the tile's first cell: relative coordinates stay below ~(tile_w + 3) h
-        const double rx = s.lo[0] + x0 * s.h, ry = s.lo[1] + y * s.h, rz = s.lo[2] + z * s.h;
-        // FP32 margin: |d_fp32 - d| <= ~4.2e-7 span + 2.4e-7 d for coordinates within the span;
-        // 2e-5 (1 + span) covers it 50 times over
-        const float tol = 2e-5f * (1.0f + float(s.h) * float(s.tile_w + 3));
-        if (staged) {
-            for (int i = threadIdx.x; i < total; i += blockDim.x) {
-                int r = 0;
-                while (r < 8 && i >= st.row_off[r + 1]) ++r;
-                const int32_t j = a.sorted[st.row_slot[r] + (i - st.row_off[r])];
-                const double4 p = a.pr[j];
-                st.pos[i] = make_float4(float(p.x - rx), float(p.y - ry), float(p.z - rz),
-                                        float(p.w));
-                st.idx[i] = j;
-            }
-        }
-        __syncthreads();
-        for (int t = own_b + (int)threadIdx.x; t < own_e; t += blockDim.x) {
-            const int32_t b = a.sorted[t];
-            const double4 pi = a.pr[b];
-            const uint32_t tagi = a.tag[b];
-            const int32_t uidi = a.uid[b];
-            const MatDev &mi = a.mats[tagi & 0xffffu];
-            const V3<T> vi = ld_vw(a.vw, a.n, b, 0), wi = ld_vw(a.vw, a.n, b, 1);
-            Acc<T> acc;
-            acc.F = v3(T(0), T(0), T(0));
-            acc.T_ = acc.F;
-            if (staged)
-                tile_forces<T, VT, HERTZ>(a, s, st, rx, ry, rz, tol, b, pi, vi, wi, uidi, mi, acc);
-            else
-                grid_forces<T, VT, HERTZ>(a, s, b, pi, vi, wi, uidi, mi, acc);
-            wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
-            if (a.ext) {
-                const double *e = a.ext + 6 * (int64_t)b;
-                acc.F = acc.F + v3(T(e[0]), T(e[1]), T(e[2]));
-                acc.T_ = acc.T_ + v3(T(e[3]), T(e[4]), T(e[5]));
-            }
-            V3<T> v;
-            const double4 o = integrate<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v);
-            a.tag_out[t] = tagi;
-            a.uid_out[t] = uidi;
-            int ncx, ncy, ncz;
-            cell_coords(s, o.x, o.y, o.z, ncx, ncy, ncz);
-            const int32_t kk = (int32_t)cell_key(s, ncx, ncy, ncz);
-            a.key[t] = kk;
-            a.rank[t] = atomicAdd(&a.cell_count[kk], 1);
-        }
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const int32_t b = a.sorted[t];
+    const double4 pi = a.pr[b];
+    const uint32_t tagi = a.tag[b];
+    const int32_t uidi = a.uid[b];
+    const SceneInfo &s = a.scenes[tagi >> 16];
+    const MatDev &mi = a.mats[tagi & 0xffffu];
+    const V3<T> vi = ld_vw(a.vw, a.n, b, 0), wi = ld_vw(a.vw, a.n, b, 1);
+    Acc<T> acc;
+    acc.F = v3(T(0), T(0), T(0));
+    acc.T_ = acc.F;
+    grid_forces_sorted<T, VT, HERTZ>(a, s, posf, b, pi, vi, wi, uidi, mi, acc);
+    wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
+    if (a.ext) {
+        const double *e = a.ext + 6 * (int64_t)b;
+        acc.F = acc.F + v3(T(e[0]), T(e[1]), T(e[2]));
+        acc.T_ = acc.T_ + v3(T(e[3]), T(e[4]), T(e[5]));
     }
+    V3<T> v;
+    const double4 o = integrate<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v);
+    a.tag_out[t] = tagi;
+    a.uid_out[t] = uidi;
+    int ncx, ncy, ncz;
+    cell_coords(s, o.x, o.y, o.z, ncx, ncy, ncz);
+    const int32_t kk = (int32_t)cell_key(s, ncx, ncy, ncz);
+    a.key[t] = kk;
+    a.rank[t] = atomicAdd(&a.cell_count[kk], 1);
 }
 
 // launch shapes of the list step kernel: threads per block and the resident blocks per SM the
@@ -713,40 +612,13 @@ DemArgs<VT> dem_args(Ctx *c, double dt) {
     return a;
 }
 
-template <typename VT, bool TRACKQ, bool HERTZ>
-void launch_tile(Ctx *c, const DemArgs<VT> &a) {
-    // resident tiles: as many blocks as fit on every SM (each loops over the tile list)
-    static int per_sm[2][2][2] = {};
-    int &k = per_sm[sizeof(VT) == 8][TRACKQ][HERTZ];
-    if (k == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                      &k, k_dem_tile<VT, TRACKQ, HERTZ>, kTileBlock, 0) != cudaSuccess)
-        k = 4;
-    const int64_t g = std::min<int64_t>(c->ntiles, (int64_t)std::max(k, 1) * c->sm_count);
-    k_dem_tile<VT, TRACKQ, HERTZ><<<(unsigned)std::max<int64_t>(g, 1), kTileBlock, 0, c->stream>>>(
-        a, c->nscenes, c->tile_list);
-}
-
 template <typename VT>
 int launch_dem(Ctx *c, double dt) {
     DemArgs<VT> a = dem_args<VT>(c, dt);
     prof_begin(c, ST_DEM);
-    if (c->tune.dem_grid != 1) {
-        if (c->tile_cap < c->ntiles + 1) {
-            cudaFree(c->tile_list);
-            c->tile_list = nullptr;
-            c->tile_cap = 0;
-            PEB_CUDA(c, cudaMalloc(&c->tile_list, (size_t)(c->ntiles + 1) * sizeof(int32_t)));
-            c->tile_cap = c->ntiles + 1;
-        }
-        PEB_CUDA(c, cudaMemsetAsync(c->tile_list, 0, sizeof(int32_t), c->stream));
-        k_tiles<<<grid_for(c->ntiles, 256), 256, 0, c->stream>>>(c->ntiles, c->nscenes,
-                                                                 c->d_scenes, c->cell_start,
-                                                                 c->tile_list);
-        PEB_LAUNCHED(c);
-    }
+    const unsigned g = grid_for(c->n, kDemBlock);
     if (c->tune.dem_grid == 1) {
-        // one thread per sphere, candidates from global memory
-        const unsigned g = grid_for(c->n, kDemBlock);
+        // one thread per sphere, candidates through the sorted order and their FP64 records
         if (a.hertz) {
             if (c->p.track_orientation) k_dem_step<VT, true, true><<<g, kDemBlock, 0, c->stream>>>(a);
             else k_dem_step<VT, false, true><<<g, kDemBlock, 0, c->stream>>>(a);
@@ -754,12 +626,15 @@ int launch_dem(Ctx *c, double dt) {
             if (c->p.track_orientation) k_dem_step<VT, true, false><<<g, kDemBlock, 0, c->stream>>>(a);
             else k_dem_step<VT, false, false><<<g, kDemBlock, 0, c->stream>>>(a);
         }
-    } else if (a.hertz) {
-        if (c->p.track_orientation) launch_tile<VT, true, true>(c, a);
-        else launch_tile<VT, false, true>(c, a);
     } else {
-        if (c->p.track_orientation) launch_tile<VT, true, false>(c, a);
-        else launch_tile<VT, false, false>(c, a);
+        const float4 *pf = c->posf;
+        if (a.hertz) {
+            if (c->p.track_orientation) k_dem_sorted<VT, true, true><<<g, kDemBlock, 0, c->stream>>>(a, pf);
+            else k_dem_sorted<VT, false, true><<<g, kDemBlock, 0, c->stream>>>(a, pf);
+        } else {
+            if (c->p.track_orientation) k_dem_sorted<VT, true, false><<<g, kDemBlock, 0, c->stream>>>(a, pf);
+            else k_dem_sorted<VT, false, false><<<g, kDemBlock, 0, c->stream>>>(a, pf);
+        }
     }
     PEB_LAUNCHED(c);
     prof_end(c, ST_DEM);
@@ -1017,7 +892,10 @@ int dem_step(Ctx *c, double dt) {
             rc = grid_bin_current(c);
             if (rc) return rc;
         }
-        rc = grid_sort(c);
+        // the sorted FP32 position copy of the default grid form
+        const bool with_pos = c->tune.dem_grid != 1;
+        if (with_pos && !c->posf) PEB_CUDA(c, cudaMalloc(&c->posf, (size_t)c->n * sizeof(float4)));
+        rc = grid_sort(c, with_pos);
         if (rc) return rc;
     }
     // moving boxes: their forces on the spheres and their own step, from the current state

@@ -100,13 +100,17 @@ __global__ void k_scatter(int64_t n, const int32_t *__restrict__ key,
     sorted[start[key[i]] + rank[i]] = (int32_t)i;
 }
 
-// insertion sort of each cell's slots by body index (cells hold a handful of bodies)
+// insertion sort of each cell's slots by body index (cells hold a handful of bodies); with
+// posf, the cell's bodies' positions relative to their scene's grid origin and radii in FP32,
+// in slot order (the candidate records of the grid DEM step)
 __global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
-                        int32_t *__restrict__ sorted) {
+                        int32_t *__restrict__ sorted, const double4 *__restrict__ pr,
+                        const uint32_t *__restrict__ tag, const SceneInfo *__restrict__ scenes,
+                        float4 *__restrict__ posf) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     const int b = start[c], e = start[c + 1];
-    if (e - b < 2) return;
+    if (e == b) return;
     for (int i = b + 1; i < e; ++i) {
         const int32_t v = sorted[i];
         int j = i - 1;
@@ -115,6 +119,14 @@ __global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
             --j;
         }
         sorted[j + 1] = v;
+    }
+    if (!posf) return;
+    for (int i = b; i < e; ++i) {
+        const int32_t j = sorted[i];
+        const double4 p = pr[j];
+        const SceneInfo &s = scenes[tag[j] >> 16];
+        posf[i] = make_float4(float(p.x - s.lo[0]), float(p.y - s.lo[1]), float(p.z - s.lo[2]),
+                              float(p.w));
     }
 }
 
@@ -223,7 +235,7 @@ int grid_bin_current(Ctx *c) {
 
 // cell_count/key/rank describe the current body order -> cell_start + sorted;
 // cell_count is cleared for the producing kernel of this step.
-int grid_sort(Ctx *c) {
+int grid_sort(Ctx *c, bool with_pos) {
     prof_begin(c, ST_SORT);
     int rc = scan_exclusive(c, c->cell_count, c->cell_start, c->ncell);
     if (rc) return rc;
@@ -231,8 +243,9 @@ int grid_sort(Ctx *c) {
         k_scatter<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->n, c->key, c->rank,
                                                               c->cell_start, c->sorted);
         PEB_LAUNCHED(c);
-        k_fixup<<<grid_for(c->ncell, 256), 256, 0, c->stream>>>(c->ncell, c->cell_start,
-                                                                c->sorted);
+        k_fixup<<<grid_for(c->ncell, 256), 256, 0, c->stream>>>(
+            c->ncell, c->cell_start, c->sorted, c->cur.pr, c->cur.tag, c->d_scenes,
+            with_pos ? c->posf : nullptr);
         PEB_LAUNCHED(c);
     }
     PEB_CUDA(c, cudaMemsetAsync(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t),

@@ -28,7 +28,6 @@ constexpr double kFrictionThreshold = 1e-8;  // pe/core/Thresholds.h:161
 constexpr int kMaxScenes = 65535;
 constexpr int kMaxMaterials = 65535;
 constexpr int kListStash = 8;   // neighbours per sphere the rebuild's counting pass keeps
-constexpr int kTileCells = 32;  // cells of one row per tile of the grid step (dem.cu)
 
 struct SceneInfo {
     double lo[3];
@@ -43,10 +42,6 @@ struct SceneInfo {
     double wall_lo[3], wall_hi[3];
     double rmax;                   // largest sphere radius of the scene at upload
     int32_t mbox_begin, nmbox;     // the scene's moving boxes (boxes.cu)
-    // tiles of the grid step (dem.cu k_dem_tile): segments of tile_w cells of one cell row,
-    // nseg per row, numbered from tile_base over all scenes
-    int64_t tile_base;
-    int32_t tile_w, nseg;
 };
 
 // per-material constants; reciprocals so a composed value is one division (Materials.h:633)
@@ -143,7 +138,7 @@ struct Tuning {
     int32_t dem_variant = 0;    // index into the k_dem_list launch shapes (dem.cu)
     int32_t rebuild_per_sm = 0; // persistent rebuild CTAs per SM; 0 = as many as fit
     int32_t nbgs_sweeps = 0;    // 0 automatic, 1 one cluster, 2 cooperative grid, 3 per colour
-    int32_t dem_grid = 0;       // grid step: 0 tiled (shared-memory candidates), 1 per sphere
+    int32_t dem_grid = 0;       // grid step: 0 sorted FP32 candidate copy, 1 FP64 records only
 };
 
 // a captured CUDA graph of `steps` DEM list steps (dem.cu); valid while the buffers it was
@@ -209,9 +204,8 @@ struct Ctx {
     int32_t *cell_count = nullptr, *cell_start = nullptr;
     int32_t *scan_tmp = nullptr;
     int64_t scan_tmp_cap = 0;
-    int64_t ntiles = 0;             // tiles of the grid step over all scenes
-    int32_t *tile_list = nullptr;   // the non-empty ones of this step (tile_cap entries + count)
-    int64_t tile_cap = 0;
+    float4 *posf = nullptr;         // grid step: FP32 positions relative to the grid origin and
+                                    // radii, in the sort's slot order (grid_sort)
     SceneInfo *d_scenes = nullptr;
     MatDev *d_mats = nullptr;
     double4 *d_planes = nullptr;    // (n, d)
@@ -286,7 +280,8 @@ unsigned capped_grid(const Ctx *c, int64_t n, int block);
 // grid build: (re)bins bodies and sorts them by cell (grid.cu)
 int grid_alloc(Ctx *c);
 int grid_bin_current(Ctx *c);
-int grid_sort(Ctx *c);
+// with_pos: also write posf (the FP32 positions in slot order) for the grid DEM step
+int grid_sort(Ctx *c, bool with_pos = false);
 int scan_exclusive(Ctx *c, const int32_t *in, int32_t *out, int64_t n);  // out[n] = total
 int scan_exclusive_cond(Ctx *c, const int32_t *in, int32_t *out, int64_t n, const int32_t *cond);
 int scan_reserve(Ctx *c, int64_t n);
