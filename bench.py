@@ -53,6 +53,9 @@ def parse():
                     help="skip the pe-on-one-core leg (minutes of set-up at 1M spheres)")
     ap.add_argument("--tuning", default=None,
                     help="dem_variant,rebuild_per_sm,skin instead of running the autotuner")
+    ap.add_argument("--profile-case", default=None, choices=sorted(PROFILE_CASES),
+                    help="run one small case of one stage for a profiler (prints a short JSON "
+                         "line, not a bench line); see profile_case()")
     return ap.parse_args()
 
 
@@ -843,8 +846,80 @@ def reference_arm(args):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# Small cases of the library's kernels, each a few launches on inputs larger than L2, for the
+# committed ncu summaries (profiles/): python bench.py --profile-case NAME --steps K
+PROFILE_CASES = {
+    # the plain FP64 grid step (sort + k_dem_sorted) on the 1M scene
+    "dem_grid_fp64": ("dem", 1048576, "fp64", False),
+    "dem_grid_mixed": ("dem", 1048576, "mixed", False),
+    # the headline list step (k_dem_list, k_rebuild) on the full 1M scene
+    "dem_list_mixed": ("dem", 1048576, "mixed", True),
+    "dem_list_fp64": ("dem", 1048576, "fp64", True),
+    # hard-contact step on the dense 32k packing (detection, colouring, cache, sweeps)
+    "nbgs_dense_mixed": ("hcsits", 32768, "mixed", None),
+    # the 512-scene ensemble (list step)
+    "ensemble_mixed": ("ensemble", 0, "mixed", True),
+    # the adjoint of 100 steps of the hopper
+    "adjoint_hopper": ("adjoint", 16384, "fp64", None),
+}
+
+
+def profile_case(args):
+    """Runs --steps steps of one PROFILE_CASES entry after --warmup steps; prints the stage
+    times (library events) as one JSON line."""
+    import torch
+    from pe_b200 import _abi
+    from pe_b200.engine import Engine
+    kind, n, prec, lists = PROFILE_CASES[args.profile_case]
+    precision = _abi.FP64 if prec == "fp64" else _abi.MIXED
+    if kind == "dem":
+        side = 200.0 * (n / 1048576) ** 0.5
+        sc = scenes.dem_large(0, n=n, dims=(side, side, 400.0)) if n != 1048576 else \
+            scenes.dem_large(0)
+        e = make_engine([sc], "dem", precision, lists=lists)
+        dt = sc.dt
+    elif kind == "hcsits":
+        sc = scenes.nbgs_box(0, n=n, dims=(32.0, 32.0, 120.0), dense=True)
+        e = make_engine([sc], "hcsits", precision)
+        dt = sc.dt
+    elif kind == "ensemble":
+        ens = scenes.batched_ensemble(0)
+        e = make_engine(ens, "dem", precision)
+        dt = ens[0].dt
+    else:
+        from pe_b200.adjoint import make_single_material
+        s0 = scenes.hopper(0)
+        m = s0.materials[0]
+        sc = make_single_material(s0, k_n=m[6] / 2, c_n=m[7] / 2, c_t=m[8] / 2, mu=2 * m[2])
+        e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(sc)
+        e.step(sc.dt, 1900)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.adjoint_forward(args.steps, sc.dt, 10)
+        x = e.download()[0]
+        z = np.zeros_like(x)
+        e.adjoint_backward(x * 0 + 1.0, z, z)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": args.profile_case, "steps": args.steps,
+                          "wall_ms": 1e3 * (time.perf_counter() - t0)}))
+        e.close()
+        return
+    e.step(dt, args.warmup)
+    torch.cuda.synchronize()
+    e.set_profiling(True)
+    e.step(dt, args.steps)
+    prof = e.profile()
+    print(json.dumps({"case": args.profile_case, "steps": args.steps,
+                      "stages_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()
+                                             if v[1]}}))
+    e.close()
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args)
+        return
     line = reference_arm(args) if args.impl == "reference" else our_arm(args)
     if line is not None:
         print(json.dumps(line), flush=True)

@@ -422,9 +422,21 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_step(DemArgs<VT> a) {
 // record.  Far candidates are rejected by an FP32 test whose margin covers its rounding; the
 // survivors take k_dem_step's exact FP64 test and pair force in k_dem_step's order, so the
 // results are bitwise those of k_dem_step.
+// slots [b, e) of the row of cells (z, y), x0 .. x1 (empty outside the grid)
+__device__ __forceinline__ void row_slots(const int32_t *__restrict__ cell_start,
+                                          const SceneInfo &s, int x0, int x1, int y, int z,
+                                          int &b, int &e) {
+    b = e = 0;
+    if (z < 0 || z >= s.dim[2] || y < 0 || y >= s.dim[1]) return;
+    const int64_t c0 = cell_key(s, x0, y, z);
+    b = cell_start[c0];
+    e = cell_start[c0 + (x1 - x0) + 1];
+}
+
 template <typename T, typename VT, bool HERTZ>
 __device__ __forceinline__ void grid_forces_sorted(const DemArgs<VT> &a, const SceneInfo &s,
-                                                   const float4 *__restrict__ posf, int32_t b,
+                                                   const float4 *__restrict__ posf, int64_t self,
+                                                   int32_t b,
                                                    const double4 &pi, V3<T> vi, V3<T> wi,
                                                    int32_t uidi, const MatDev &mi, Acc<T> &acc) {
     int cx, cy, cz;
@@ -437,29 +449,55 @@ __device__ __forceinline__ void grid_forces_sorted(const DemArgs<VT> &a, const S
     // r_i + r_j; the margin is 100 times that
     const float tol = 1e-5f * (1.0f + fabsf(pxf) + fabsf(pyf) + fabsf(pzf) + 4.0f * float(pi.w));
     const float prf = float(pi.w) + tol;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= s.dim[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = cy + dy;
-            if (y < 0 || y >= s.dim[1]) continue;
-            const int64_t c0 = cell_key(s, x0, y, z);
-            const int64_t c1 = c0 + (x1 - x0) + 1;
-            const int e = a.cell_start[c1];
-            for (int slot = a.cell_start[c0]; slot < e; ++slot) {
-                const float4 q = posf[slot];
-                const float dx = pxf - q.x, dy2 = pyf - q.y, dz2 = pzf - q.z;
-                const float rs = prf + q.w;
-                if (dx * dx + dy2 * dy2 + dz2 * dz2 >= rs * rs) continue;
-                const int32_t j = a.sorted[slot];
-                if (j == b) continue;
-                const double4 pj = a.pr[j];
-                const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
-                const double rsd = pi.w + pj.w;
-                if (ddx * ddx + ddy * ddy + ddz * ddz >= rsd * rsd) continue;
-                pair_force<T, VT, HERTZ>(a, pi, vi, wi, uidi, mi, j, pj, acc);
+    // one candidate that passed the FP32 test: k_dem_step's exact test and pair force (the body's
+    // own slot is the one candidate k_dem_step skips as j == b)
+    auto exact = [&](int slot) {
+        if (slot == self) return;
+        const int32_t j = a.sorted[slot];
+        const double4 pj = a.pr[j];
+        const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+        const double rsd = pi.w + pj.w;
+        if (ddx * ddx + ddy * ddy + ddz * ddz >= rsd * rsd) return;
+        pair_force<T, VT, HERTZ>(a, pi, vi, wi, uidi, mi, j, pj, acc);
+    };
+    auto near = [&](const float4 &q) {
+        const float dx = pxf - q.x, dy = pyf - q.y, dz = pzf - q.z;
+        const float rs = prf + q.w;
+        return dx * dx + dy * dy + dz * dz < rs * rs;
+    };
+    // rows (z, y) in k_dem_step's order; the next row's bounds load while this one runs
+    int nb, ne;
+    row_slots(a.cell_start, s, x0, x1, cy - 1, cz - 1, nb, ne);
+#pragma unroll 1
+    for (int r = 0; r < 9; ++r) {
+        int slot = nb;
+        const int e = ne;
+        if (r < 8) row_slots(a.cell_start, s, x0, x1, cy + (r + 1) % 3 - 1, cz + (r + 1) / 3 - 1,
+                             nb, ne);
+        // eight candidate records in flight at a time; the hits keep their slot order
+        for (; slot + 8 <= e; slot += 8) {
+            unsigned hit = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) hit |= near(posf[slot + k]) ? (1u << k) : 0u;
+            while (hit) {
+                const int k = __ffs(hit) - 1;
+                hit &= hit - 1u;
+                exact(slot + k);
             }
         }
+        if (slot + 4 <= e) {
+            unsigned hit = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) hit |= near(posf[slot + k]) ? (1u << k) : 0u;
+            while (hit) {
+                const int k = __ffs(hit) - 1;
+                hit &= hit - 1u;
+                exact(slot + k);
+            }
+            slot += 4;
+        }
+        for (; slot < e; ++slot)
+            if (near(posf[slot])) exact(slot);
     }
 }
 
@@ -479,7 +517,7 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_sorted(DemArgs<VT> a,
     Acc<T> acc;
     acc.F = v3(T(0), T(0), T(0));
     acc.T_ = acc.F;
-    grid_forces_sorted<T, VT, HERTZ>(a, s, posf, b, pi, vi, wi, uidi, mi, acc);
+    grid_forces_sorted<T, VT, HERTZ>(a, s, posf, t, b, pi, vi, wi, uidi, mi, acc);
     wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
     if (a.ext) {
         const double *e = a.ext + 6 * (int64_t)b;
