@@ -107,6 +107,8 @@ void free_device(Ctx *c) {
     cudaFree(c->scan_tmp);
     cudaFree(c->posf);
     c->posf = nullptr;
+    cudaFree(c->near);
+    c->near = nullptr;
     cudaFree(c->d_scenes);
     cudaFree(c->d_mats);
     cudaFree(c->d_planes);

@@ -501,9 +501,73 @@ __device__ __forceinline__ void grid_forces_sorted(const DemArgs<VT> &a, const S
     }
 }
 
+// The grid step in two kernels.  k_grid_near (few registers, so many warps hide the candidate
+// loads) runs the FP32 test of every candidate of a sphere's 27 cells and records the slots
+// that pass, in k_dem_step's order, up to kNear of them; k_dem_near takes each recorded slot
+// through k_dem_step's exact test and pair force (or, for a sphere with more than kNear, searches
+// its cells again), then the walls and the integration.  Same terms in the same order: bitwise
+// the results of k_dem_step.
+constexpr int kNear = 16;
+constexpr int kNearBlock = 256;
+
+__global__ void __launch_bounds__(kNearBlock, 6) k_grid_near(
+    int64_t n, const int32_t *__restrict__ sorted, const double4 *__restrict__ pr,
+    const uint32_t *__restrict__ tag, const SceneInfo *__restrict__ scenes,
+    const int32_t *__restrict__ cell_start, const float4 *__restrict__ posf,
+    int32_t *__restrict__ near_cnt, int32_t *__restrict__ near_idx) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t b = sorted[t];
+    const double4 pi = pr[b];
+    const SceneInfo &s = scenes[tag[b] >> 16];
+    int cx, cy, cz;
+    cell_coords(s, pi.x, pi.y, pi.z, cx, cy, cz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.dim[0] - 1);
+    // the values and margin of grid_forces_sorted
+    const float pxf = float(pi.x - s.lo[0]), pyf = float(pi.y - s.lo[1]),
+                pzf = float(pi.z - s.lo[2]);
+    const float tol = 1e-5f * (1.0f + fabsf(pxf) + fabsf(pyf) + fabsf(pzf) + 4.0f * float(pi.w));
+    const float prf = float(pi.w) + tol;
+    auto near = [&](const float4 &q) {
+        const float dx = pxf - q.x, dy = pyf - q.y, dz = pzf - q.z;
+        const float rs = prf + q.w;
+        return dx * dx + dy * dy + dz * dz < rs * rs;
+    };
+    int cnt = 0;
+    auto keep = [&](int slot) {
+        if (slot == t) return;
+        if (cnt < kNear) near_idx[(int64_t)cnt * n + t] = slot;
+        ++cnt;
+    };
+    int nb, ne;
+    row_slots(cell_start, s, x0, x1, cy - 1, cz - 1, nb, ne);
+#pragma unroll 1
+    for (int r = 0; r < 9; ++r) {
+        int slot = nb;
+        const int e = ne;
+        if (r < 8) row_slots(cell_start, s, x0, x1, cy + (r + 1) % 3 - 1, cz + (r + 1) / 3 - 1,
+                             nb, ne);
+        for (; slot + 8 <= e; slot += 8) {
+            unsigned hit = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) hit |= near(posf[slot + k]) ? (1u << k) : 0u;
+            while (hit) {
+                const int k = __ffs(hit) - 1;
+                hit &= hit - 1u;
+                keep(slot + k);
+            }
+        }
+        for (; slot < e; ++slot)
+            if (near(posf[slot])) keep(slot);
+    }
+    near_cnt[t] = cnt;
+}
+
 template <typename VT, bool TRACKQ, bool HERTZ>
-__global__ void __launch_bounds__(kDemBlock) k_dem_sorted(DemArgs<VT> a,
-                                                          const float4 *__restrict__ posf) {
+__global__ void __launch_bounds__(kDemBlock) k_dem_near(DemArgs<VT> a,
+                                                        const float4 *__restrict__ posf,
+                                                        const int32_t *__restrict__ near_cnt,
+                                                        const int32_t *__restrict__ near_idx) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
@@ -511,13 +575,25 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_sorted(DemArgs<VT> a,
     const double4 pi = a.pr[b];
     const uint32_t tagi = a.tag[b];
     const int32_t uidi = a.uid[b];
+    const int cnt = near_cnt[t];
     const SceneInfo &s = a.scenes[tagi >> 16];
     const MatDev &mi = a.mats[tagi & 0xffffu];
     const V3<T> vi = ld_vw(a.vw, a.n, b, 0), wi = ld_vw(a.vw, a.n, b, 1);
     Acc<T> acc;
     acc.F = v3(T(0), T(0), T(0));
     acc.T_ = acc.F;
-    grid_forces_sorted<T, VT, HERTZ>(a, s, posf, t, b, pi, vi, wi, uidi, mi, acc);
+    if (cnt > kNear) {
+        grid_forces_sorted<T, VT, HERTZ>(a, s, posf, t, b, pi, vi, wi, uidi, mi, acc);
+    } else {
+        for (int k = 0; k < cnt; ++k) {
+            const int32_t j = a.sorted[near_idx[(int64_t)k * a.n + t]];
+            const double4 pj = a.pr[j];
+            const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+            const double rsd = pi.w + pj.w;
+            if (ddx * ddx + ddy * ddy + ddz * ddz >= rsd * rsd) continue;
+            pair_force<T, VT, HERTZ>(a, pi, vi, wi, uidi, mi, j, pj, acc);
+        }
+    }
     wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
     if (a.ext) {
         const double *e = a.ext + 6 * (int64_t)b;
@@ -666,12 +742,17 @@ int launch_dem(Ctx *c, double dt) {
         }
     } else {
         const float4 *pf = c->posf;
+        const int32_t *nc = c->near, *ni = c->near + c->n;
+        k_grid_near<<<grid_for(c->n, kNearBlock), kNearBlock, 0, c->stream>>>(
+            c->n, c->sorted, c->cur.pr, c->cur.tag, c->d_scenes, c->cell_start, pf, c->near,
+            c->near + c->n);
+        PEB_LAUNCHED(c);
         if (a.hertz) {
-            if (c->p.track_orientation) k_dem_sorted<VT, true, true><<<g, kDemBlock, 0, c->stream>>>(a, pf);
-            else k_dem_sorted<VT, false, true><<<g, kDemBlock, 0, c->stream>>>(a, pf);
+            if (c->p.track_orientation) k_dem_near<VT, true, true><<<g, kDemBlock, 0, c->stream>>>(a, pf, nc, ni);
+            else k_dem_near<VT, false, true><<<g, kDemBlock, 0, c->stream>>>(a, pf, nc, ni);
         } else {
-            if (c->p.track_orientation) k_dem_sorted<VT, true, false><<<g, kDemBlock, 0, c->stream>>>(a, pf);
-            else k_dem_sorted<VT, false, false><<<g, kDemBlock, 0, c->stream>>>(a, pf);
+            if (c->p.track_orientation) k_dem_near<VT, true, false><<<g, kDemBlock, 0, c->stream>>>(a, pf, nc, ni);
+            else k_dem_near<VT, false, false><<<g, kDemBlock, 0, c->stream>>>(a, pf, nc, ni);
         }
     }
     PEB_LAUNCHED(c);
@@ -932,7 +1013,10 @@ int dem_step(Ctx *c, double dt) {
         }
         // the sorted FP32 position copy of the default grid form
         const bool with_pos = c->tune.dem_grid != 1;
-        if (with_pos && !c->posf) PEB_CUDA(c, cudaMalloc(&c->posf, (size_t)c->n * sizeof(float4)));
+        if (with_pos && !c->posf) {
+            PEB_CUDA(c, cudaMalloc(&c->posf, (size_t)c->n * sizeof(float4)));
+            PEB_CUDA(c, cudaMalloc(&c->near, (size_t)c->n * (1 + kNear) * sizeof(int32_t)));
+        }
         rc = grid_sort(c, with_pos);
         if (rc) return rc;
     }

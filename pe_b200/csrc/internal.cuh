@@ -206,6 +206,8 @@ struct Ctx {
     int64_t scan_tmp_cap = 0;
     float4 *posf = nullptr;         // grid step: FP32 positions relative to the grid origin and
                                     // radii, in the sort's slot order (grid_sort)
+    int32_t *near = nullptr;        // grid step: per slot the count of candidates that passed
+                                    // the FP32 test, then up to 16 of their slots (component-major)
     SceneInfo *d_scenes = nullptr;
     MatDev *d_mats = nullptr;
     double4 *d_planes = nullptr;    // (n, d)
