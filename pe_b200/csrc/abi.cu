@@ -417,7 +417,8 @@ int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
     if (!c) return PE_B200_ERR_NOMEM;
     c->p = *p;
     c->device = p->device;
-    c->vw_bytes = 6 * (p->precision == PE_B200_FP64 ? 8 : 4);
+    // six FP64 components, or six FP32 components and the extension plane (internal.cuh)
+    c->vw_bytes = p->precision == PE_B200_FP64 ? 6 * 8 : 7 * 4;
     cudaError_t e = cudaSetDevice(p->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int32_t));

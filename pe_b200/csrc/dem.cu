@@ -284,12 +284,14 @@ __device__ __forceinline__ void wall_forces(const DemArgs<VT> &a, const SceneInf
     }
 }
 
-// SphereTrait::move, Default.h:166-216: new position (radius kept), v and w; writes q
+// SphereTrait::move, Default.h:166-216: new position (radius kept), v and w; writes q.
+// Mixed precision: ext carries the linear velocity's extension bytes in and out (internal.cuh);
+// the velocity is updated and the position advanced in FP64, then split again.
 template <typename VT, bool TRACKQ>
 __device__ __forceinline__ double4 integrate_core(const DemArgs<VT> &a, int64_t b, int64_t t,
                                                   const double4 &pi, V3<VT> vi, V3<VT> wi,
                                                   const MatDev &mi, const Acc<VT> &acc,
-                                                  V3<VT> &v, V3<VT> &w) {
+                                                  V3<VT> &v, V3<VT> &w, uint32_t &ext) {
     using T = VT;
     T im, ii;
     if (sizeof(T) == 8) {
@@ -307,11 +309,22 @@ __device__ __forceinline__ double4 integrate_core(const DemArgs<VT> &a, int64_t 
     const V3<T> gg = v3(T(a.g[0]), T(a.g[1]), T(a.g[2]));
     const V3<T> vdot = acc.F * T(im) + gg;
     const V3<T> wdot = T(ii) * acc.T_;
-    v = vi + vdot * T(a.dt);
     w = wi + wdot * T(a.dt);
-    const double nxp = pi.x + double(v.x) * a.dt;
-    const double nyp = pi.y + double(v.y) * a.dt;
-    const double nzp = pi.z + double(v.z) * a.dt;
+    double nxp, nyp, nzp;
+    double vx = 0.0, vy = 0.0, vz = 0.0;   // mixed: the FP64 linear velocity
+    if constexpr (sizeof(T) == 8) {
+        v = vi + vdot * T(a.dt);
+        nxp = pi.x + double(v.x) * a.dt;
+        nyp = pi.y + double(v.y) * a.dt;
+        nzp = pi.z + double(v.z) * a.dt;
+    } else {
+        vx = vext_value(vi.x, ext, 0) + double(vdot.x) * a.dt;
+        vy = vext_value(vi.y, ext, 1) + double(vdot.y) * a.dt;
+        vz = vext_value(vi.z, ext, 2) + double(vdot.z) * a.dt;
+        nxp = pi.x + vx * a.dt;
+        nyp = pi.y + vy * a.dt;
+        nzp = pi.z + vz * a.dt;
+    }
     if (TRACKQ) {
         // q = Quat(phi, |phi|) * q (Quaternion.h:274-294, 1146-1153)
         const double phx = double(w.x) * a.dt, phy = double(w.y) * a.dt, phz = double(w.z) * a.dt;
@@ -331,12 +344,32 @@ __device__ __forceinline__ double4 integrate_core(const DemArgs<VT> &a, int64_t 
         r.w = d0 * q.w + d3 * q.x + d1 * q.z - d2 * q.y;
         a.q_out[t] = r;
     }
-    if (a.has_drag) {
-        v = v * T(a.drag);
-        w = w * T(a.drag);
+    if constexpr (sizeof(T) == 8) {
+        if (a.has_drag) {
+            v = v * T(a.drag);
+            w = w * T(a.drag);
+        }
+    } else {
+        if (a.has_drag) {
+            vx *= a.drag;
+            vy *= a.drag;
+            vz *= a.drag;
+            w = w * T(a.drag);
+        }
+        ext = 0u;
+        v.x = vext_split(vx, ext, 0);
+        v.y = vext_split(vy, ext, 1);
+        v.z = vext_split(vz, ext, 2);
     }
     if (!isfinite(nxp) || !isfinite(nyp) || !isfinite(nzp)) atomicOr(a.err, DERR_NAN);
     return make_double4(nxp, nyp, nzp, pi.w);
+}
+
+// the extension bytes of body i's velocity (zero in FP64)
+template <typename VT>
+__device__ __forceinline__ uint32_t ld_ext(const VT *vw, int64_t n, int64_t i) {
+    if constexpr (sizeof(VT) == 4) return ld_vext(vw, n, i);
+    else return 0u;
 }
 
 template <typename VT, bool TRACKQ>
@@ -344,9 +377,10 @@ __device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, in
                                              const double4 &pi, V3<VT> vi, V3<VT> wi,
                                              const MatDev &mi, const Acc<VT> &acc, V3<VT> &v) {
     V3<VT> w;
-    const double4 out = integrate_core<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v, w);
+    uint32_t ext = ld_ext(a.vw, a.n, b);
+    const double4 out = integrate_core<VT, TRACKQ>(a, b, t, pi, vi, wi, mi, acc, v, w, ext);
     a.pr_out[t] = out;
-    st_vw(a.vw_out, a.n, t, v, w);
+    st_vw(a.vw_out, a.n, t, v, w, ext);
     return out;
 }
 
@@ -641,6 +675,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
         const double4 pi = a.pr[t];
         const uint32_t tagi = a.tag[t];
         const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
+        uint32_t ext = ld_ext(a.vw, a.n, t);
         int k = a.nl_start[t];
         const int e = a.nl_start[t + 1];
         const float disp0 = a.disp[t];
@@ -671,10 +706,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
         V3<T> v, w;
-        const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w);
+        const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w, ext);
         // whole 32-byte records: a partial sector write would make L2 fetch the sector first
         a.pr_out[t] = o;
-        st_vw(a.vw_out, a.n, t, v, w);
+        st_vw(a.vw_out, a.n, t, v, w, ext);
         const float vx = float(v.x), vy = float(v.y), vz = float(v.z);
         const float d = disp0 + sqrtf(vx * vx + vy * vy + vz * vz) * float(a.dt) * 1.0001f;
         a.disp[t] = d;

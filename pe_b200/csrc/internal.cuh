@@ -446,25 +446,60 @@ __device__ __forceinline__ double dot_rn(double ax, double ay, double az, double
     return __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
 }
 
-// velocities are component-major: component c (vx vy vz wx wy wz) of body i at vw[c * n + i]
+// velocities are component-major: component c (vx vy vz wx wy wz) of body i at vw[c * n + i].
+// In mixed precision a seventh plane holds, per body, one extension byte for each linear
+// component (bits 0-7 vx, 8-15 vy, 16-23 vz): the velocity is hi + e 2^-8 ulp(hi), hi the FP32
+// component and e the signed byte.  A velocity that gains the same small increment every step
+// (free flight: v += g dt) would round the same way step after step in 24 bits; with 32 bits
+// the drift stays ~2^-33 per step.  Kernels that do not track the extension store it as zero.
+constexpr int vw_planes(int bytes) { return bytes == 8 ? 6 : 7; }
+
 template <typename T>
 __device__ __forceinline__ V3<T> ld_vw(const T *vw, int64_t n, int64_t i, int which) {
     const T *p = vw + 3 * which * n + i;
     return v3(p[0], p[n], p[2 * n]);
 }
+__device__ __forceinline__ uint32_t ld_vext(const float *vw, int64_t n, int64_t i) {
+    return reinterpret_cast<const uint32_t *>(vw + 6 * n)[i];
+}
 template <typename T>
-__device__ __forceinline__ void st_vw(T *vw, int64_t n, int64_t i, V3<T> v, V3<T> w) {
+__device__ __forceinline__ void st_vw(T *vw, int64_t n, int64_t i, V3<T> v, V3<T> w,
+                                      uint32_t ext = 0u) {
     vw[i] = v.x;
     vw[n + i] = v.y;
     vw[2 * n + i] = v.z;
     vw[3 * n + i] = w.x;
     vw[4 * n + i] = w.y;
     vw[5 * n + i] = w.z;
+    if constexpr (sizeof(T) == 4) reinterpret_cast<uint32_t *>(vw + 6 * n)[i] = ext;
 }
 template <typename T>
 __device__ __forceinline__ void cp_vw(T *dst, int64_t i, const T *src, int64_t j, int64_t n) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) dst[c * n + i] = src[c * n + j];
+    if constexpr (sizeof(T) == 4)
+        reinterpret_cast<uint32_t *>(dst + 6 * n)[i] =
+            reinterpret_cast<const uint32_t *>(src + 6 * n)[j];
+}
+// 2^-8 ulp(hi) as a double (zero and subnormal hi use the smallest normal exponent)
+__device__ __forceinline__ double vext_unit(float hi) {
+    const int ex = max((int)((__float_as_uint(hi) >> 23) & 0xffu), 1);
+    return __longlong_as_double((long long)(ex - 158 + 1023) << 52);
+}
+// the FP64 value of component c of an extended velocity
+__device__ __forceinline__ double vext_value(float hi, uint32_t ext, int c) {
+    const int e = (int)(int8_t)(uint8_t)((ext >> (8 * c)) & 0xffu);
+    return double(hi) + double(e) * vext_unit(hi);
+}
+// FP64 velocity component -> FP32 component (round to nearest), its extension byte or-ed into
+// ext at position c.  v - hi is exact, and so is the division by a power of two.
+__device__ __forceinline__ float vext_split(double v, uint32_t &ext, int c) {
+    const float hi = __double2float_rn(v);
+    const double r = (v - double(hi)) / vext_unit(hi);
+    int e = isfinite(r) ? (int)rint(r) : 0;
+    e = max(-127, min(127, e));
+    ext |= ((uint32_t)(uint8_t)(int8_t)e) << (8 * c);
+    return hi;
 }
 
 __device__ __forceinline__ void sphere_mass(double r, double density, double &im, double &ii,

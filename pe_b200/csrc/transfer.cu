@@ -13,14 +13,30 @@ namespace peb {
 
 namespace {
 
+// a body's velocities from a caller's FP64 linear velocity (3 doubles) and angular velocity;
+// in mixed precision the linear one keeps its extension bytes
+template <typename VT>
+__device__ __forceinline__ void st_vw_in(VT *vw, int64_t n, int64_t i, const double *v,
+                                         V3<VT> w) {
+    if constexpr (sizeof(VT) == 4) {
+        uint32_t ext = 0u;
+        V3<float> a;
+        a.x = vext_split(v[0], ext, 0);
+        a.y = vext_split(v[1], ext, 1);
+        a.z = vext_split(v[2], ext, 2);
+        st_vw(vw, n, i, a, w, ext);
+    } else {
+        st_vw(vw, n, i, v3(v[0], v[1], v[2]), w);
+    }
+}
+
 template <typename VT>
 __global__ void k_pack(int64_t n, const double *x, const double *v, const double *w,
                        const double *r, const int32_t *mat, const int32_t *scene, double4 *pr,
                        VT *vw, uint32_t *tag, int32_t *uid, double4 *q) {
     GRID_STRIDE(i, n) {
         pr[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], r[i]);
-        st_vw(vw, n, i, v3(VT(v[3 * i]), VT(v[3 * i + 1]), VT(v[3 * i + 2])),
-              v3(VT(w[3 * i]), VT(w[3 * i + 1]), VT(w[3 * i + 2])));
+        st_vw_in(vw, n, i, v + 3 * i, v3(VT(w[3 * i]), VT(w[3 * i + 1]), VT(w[3 * i + 2])));
         tag[i] = (uint32_t)mat[i] | ((uint32_t)(scene ? scene[i] : 0) << 16);
         uid[i] = (int32_t)i;
         if (q) q[i] = make_double4(1.0, 0.0, 0.0, 0.0);
@@ -37,9 +53,16 @@ __global__ void k_unpack(int64_t n, const double4 *pr, const VT *vw, const int32
         x[3 * i + 1] = p.y;
         x[3 * i + 2] = p.z;
         const V3<VT> a = ld_vw(vw, n, t, 0), b = ld_vw(vw, n, t, 1);
-        v[3 * i] = a.x;
-        v[3 * i + 1] = a.y;
-        v[3 * i + 2] = a.z;
+        if constexpr (sizeof(VT) == 4) {
+            const uint32_t ext = ld_vext(vw, n, t);
+            v[3 * i] = vext_value(a.x, ext, 0);
+            v[3 * i + 1] = vext_value(a.y, ext, 1);
+            v[3 * i + 2] = vext_value(a.z, ext, 2);
+        } else {
+            v[3 * i] = a.x;
+            v[3 * i + 1] = a.y;
+            v[3 * i + 2] = a.z;
+        }
         w[3 * i] = b.x;
         w[3 * i + 1] = b.y;
         w[3 * i + 2] = b.z;
@@ -63,10 +86,14 @@ __global__ void k_scatter_state(int64_t n, const int32_t *uid, const double *x, 
             const double4 p = pr[t];
             pr[t] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], p.w);
         }
-        V3<VT> a = ld_vw(vw, n, t, 0), b = ld_vw(vw, n, t, 1);
-        if (v) a = v3(VT(v[3 * i]), VT(v[3 * i + 1]), VT(v[3 * i + 2]));
-        if (w) b = v3(VT(w[3 * i]), VT(w[3 * i + 1]), VT(w[3 * i + 2]));
-        st_vw(vw, n, t, a, b);
+        const V3<VT> b = w ? v3(VT(w[3 * i]), VT(w[3 * i + 1]), VT(w[3 * i + 2])) : ld_vw(vw, n, t, 1);
+        if (v) {
+            st_vw_in(vw, n, t, v + 3 * i, b);
+        } else {
+            const V3<VT> a = ld_vw(vw, n, t, 0);
+            if constexpr (sizeof(VT) == 4) st_vw(vw, n, t, a, b, ld_vext(vw, n, t));
+            else st_vw(vw, n, t, a, b);
+        }
     }
 }
 

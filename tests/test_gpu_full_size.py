@@ -34,9 +34,15 @@ def test_1m_runs_are_bit_identical(large):
 
 
 def test_1m_mixed_within_stated_error_of_fp64(large):
-    xm, _, _ = run(large, 300, precision=_abi.MIXED)
-    xd, _, _ = run(large, 300, precision=_abi.FP64)
-    assert rel_err(xm, xd) < 1e-6
+    """The stated error of the mixed-precision form: after 1000 steps of the 1M scene, every
+    sphere's position is within 1e-6 of the FP64 run's, relative to the largest displacement
+    (max |x_mixed - x_fp64| / max |x_fp64 - x_0|), and so is the RMS over spheres."""
+    xm, _, _ = run(large, 1000, precision=_abi.MIXED)
+    xd, _, _ = run(large, 1000, precision=_abi.FP64)
+    d, disp = np.abs(xm - xd), np.abs(xd - large.x)
+    assert d.max() / disp.max() < 1e-6
+    assert np.sqrt((d ** 2).sum() / (disp ** 2).sum()) < 1e-6
+    assert rel_err(xm, xd) < 1e-9
 
 
 def test_1m_lists_follow_the_grid_step(large):
