@@ -491,11 +491,16 @@ __device__ __forceinline__ double vext_value(float hi, uint32_t ext, int c) {
     const int e = (int)(int8_t)(uint8_t)((ext >> (8 * c)) & 0xffu);
     return double(hi) + double(e) * vext_unit(hi);
 }
+// 2^8 / ulp(hi), the reciprocal of vext_unit (a power of two, so multiplying by it is exact)
+__device__ __forceinline__ double vext_inv_unit(float hi) {
+    const int ex = max((int)((__float_as_uint(hi) >> 23) & 0xffu), 1);
+    return __longlong_as_double((long long)(158 - ex + 1023) << 52);
+}
 // FP64 velocity component -> FP32 component (round to nearest), its extension byte or-ed into
-// ext at position c.  v - hi is exact, and so is the division by a power of two.
+// ext at position c.  v - hi is exact, and so is the scaling by a power of two.
 __device__ __forceinline__ float vext_split(double v, uint32_t &ext, int c) {
     const float hi = __double2float_rn(v);
-    const double r = (v - double(hi)) / vext_unit(hi);
+    const double r = (v - double(hi)) * vext_inv_unit(hi);
     int e = isfinite(r) ? (int)rint(r) : 0;
     e = max(-127, min(127, e));
     ext |= ((uint32_t)(uint8_t)(int8_t)e) << (8 * c);
