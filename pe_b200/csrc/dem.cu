@@ -149,6 +149,10 @@ struct DemArgs {
     // bank instead of through the body's tag)
     SceneInfo s0;
     MatDev m0;
+    // list step: the spheres marked at the last rebuild and their forces
+    const int32_t *act = nullptr;     // exclusive offsets of the marks (n + 1)
+    const int32_t *alist = nullptr;   // the marked spheres
+    VT *facc = nullptr;               // their force and torque, component-major (6 x n)
 };
 
 // one sphere pair (this body and neighbour j), both in the buffers of `a`; self1: this body is
@@ -658,27 +662,31 @@ constexpr DemShape kDemShapes[] = {{kDemBlock, PEB_LIST_MIN_BLOCKS_F32, 5},
                                    {256, 4, 3}};
 constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]));
 
-// list step: body t stays at index t (the order changes only at rebuilds)
-template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool HERTZ, bool ONE = false>
-__global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
+// List step, in two kernels; body t stays at index t (the order changes only at rebuilds).
+// The rebuild marks the spheres that can feel a force before the next rebuild -- those with list
+// entries, and those within reach of a wall (not inside the box of the scene's planes by
+// skin/2, or near a fixed box) -- and lists them in ascending order (act: exclusive offsets of
+// the marks, act[n] the count; alist: the marked spheres).  k_dem_contacts sums the pair and
+// wall forces of the marked spheres only, in the order of the single-kernel form, into facc;
+// k_dem_move then integrates every sphere, reading facc for the marked ones, so the common
+// sphere of a sparse scene runs a short kernel without the contact code's registers.
+
+// forces on the marked spheres (a grid-stride loop over the marked list)
+template <typename VT, bool HERTZ, bool ONE = false>
+__global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a) {
     using T = VT;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // launched early behind the rebuild kernel: nothing of the state or the lists is read
-    // before it has finished; the next step's rebuild may be scheduled from here on (it waits
-    // for this kernel in turn)
+    // launched early behind the rebuild kernel: nothing is read before it has finished
     pdl_wait();
     pdl_trigger();
-    bool moved = false;
-    if (t < a.n) {
-        // every load of this body's own records first: they are independent, and none may
-        // wait behind this thread's stores
+    const int32_t na = a.act[a.n];
+    for (int32_t m = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x); m < na;
+         m += (int32_t)(gridDim.x * blockDim.x)) {
+        const int64_t t = a.alist[m];
         const double4 pi = a.pr[t];
         const uint32_t tagi = a.tag[t];
         const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
-        uint32_t ext = ld_ext(a.vw, a.n, t);
         int k = a.nl_start[t];
         const int e = a.nl_start[t + 1];
-        const float disp0 = a.disp[t];
         const SceneInfo &s = ONE ? a.s0 : a.scenes[tagi >> 16];
         const MatDev &mi = ONE ? a.m0 : a.mats[tagi & 0xffffu];
         Acc<T> acc;
@@ -705,6 +713,45 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_list(DemArgs<VT> a) {
             }
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
+        const int64_t cap = a.n;
+        a.facc[m] = acc.F.x;
+        a.facc[cap + m] = acc.F.y;
+        a.facc[2 * cap + m] = acc.F.z;
+        a.facc[3 * cap + m] = acc.T_.x;
+        a.facc[4 * cap + m] = acc.T_.y;
+        a.facc[5 * cap + m] = acc.T_.z;
+    }
+}
+
+// integration of every sphere with the forces of k_dem_contacts
+template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool ONE = false>
+__global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a) {
+    using T = VT;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // launched early behind the contact kernel; the next step's rebuild may be scheduled from
+    // here on (it waits for this kernel in turn)
+    pdl_wait();
+    pdl_trigger();
+    bool moved = false;
+    if (t < a.n) {
+        // every load of this body's own records first: they are independent, and none may
+        // wait behind this thread's stores
+        const double4 pi = a.pr[t];
+        const uint32_t tagi = ONE ? 0u : a.tag[t];
+        const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
+        uint32_t ext = ld_ext(a.vw, a.n, t);
+        const int32_t m = a.act[t];
+        const bool marked = a.act[t + 1] > m;
+        const float disp0 = a.disp[t];
+        const MatDev &mi = ONE ? a.m0 : a.mats[tagi & 0xffffu];
+        Acc<T> acc;
+        acc.F = v3(T(0), T(0), T(0));
+        acc.T_ = acc.F;
+        if (marked) {
+            const int64_t cap = a.n;
+            acc.F = v3(a.facc[m], a.facc[cap + m], a.facc[2 * cap + m]);
+            acc.T_ = v3(a.facc[3 * cap + m], a.facc[4 * cap + m], a.facc[5 * cap + m]);
+        }
         V3<T> v, w;
         const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w, ext);
         // whole 32-byte records: a partial sector write would make L2 fetch the sector first
@@ -758,6 +805,9 @@ DemArgs<VT> dem_args(Ctx *c, double dt) {
     a.half_skin = float(0.5 * c->nl.skin * (1.0 - 1e-5));
     a.hertz = c->p.force_model == 1 ? 1 : 0;
     a.ext = c->mb.m > 0 ? c->mb.ext : nullptr;
+    a.act = c->nl.act;
+    a.alist = c->nl.alist;
+    a.facc = (VT *)c->nl.facc;
     return a;
 }
 
@@ -913,6 +963,19 @@ __global__ void k_list(int64_t n, const double4 *pr, const uint32_t *tag, const 
     }
 }
 
+// the list step's marks (internal.cuh list_marked) from the neighbour counts
+__global__ void k_mark_c(int64_t n, const double4 *pr, const uint32_t *tag, const SceneInfo *scenes,
+                         const double *boxes, double margin, const int32_t *cnt, int32_t *act,
+                         const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(t, n) act[t] = list_marked(scenes[tag[t] >> 16], pr[t], boxes, margin, cnt[t]) ? 1 : 0;
+}
+
+__global__ void k_alist_c(int64_t n, const int32_t *act, int32_t *alist, const int32_t *cond) {
+    if (!*cond) return;
+    GRID_STRIDE(t, n) if (act[t + 1] > act[t]) alist[act[t]] = (int32_t)t;
+}
+
 __global__ void k_rebuild_done(int64_t n, const int32_t *start, int64_t cap, int32_t *flags) {
     if (!flags[0]) return;
     flags[0] = 0;
@@ -949,8 +1012,16 @@ int list_rebuild(Ctx *c) {
                                                        c->cell_start, L.skin, L.cnt, nullptr, 0,
                                                        nullptr, cond);
     PEB_LAUNCHED(c);
+    k_mark_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+                                                          c->d_boxes, 0.5 * L.skin * (1.0 + 1e-9),
+                                                          L.cnt, L.act, cond);
+    PEB_LAUNCHED(c);
     rc = scan_exclusive_cond(c, L.cnt, L.start, n, cond);
     if (rc) return rc;
+    rc = scan_exclusive_cond(c, L.act, L.act, n, cond);
+    if (rc) return rc;
+    k_alist_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.act, L.alist, cond);
+    PEB_LAUNCHED(c);
     k_list<1><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->cur.uid, c->d_scenes,
                                                        c->cell_start, L.skin, nullptr, L.start,
                                                        L.cap, L.idx, cond);
@@ -967,24 +1038,31 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
     const bool one = c->nscenes == 1 && c->mats_dev.size() == 1 && !TRACKQ && !HERTZ;
-    // scheduled while the rebuild kernel before it finishes (a rebuild that has nothing to do
-    // lets it start at once)
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid_for(c->n, B));
-    cfg.blockDim = dim3(B);
-    cfg.stream = c->stream;
+    // each kernel is scheduled while the one before it finishes (a rebuild that has nothing to
+    // do lets the contact kernel start at once)
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cudaLaunchConfig_t cc = {};
+    cc.gridDim = dim3((unsigned)std::min<int64_t>(grid_for(c->n, 128), 4 * (int64_t)c->sm_count));
+    cc.blockDim = dim3(128);
+    cc.stream = c->stream;
+    cc.attrs = at;
+    cc.numAttrs = 1;
+    cudaLaunchConfig_t cm = cc;
+    cm.gridDim = dim3((unsigned)grid_for(c->n, B));
+    cm.blockDim = dim3(B);
     if (one) {
         DemArgs<VT> b = a;
         b.s0 = c->scenes[0];
         b.m0 = c->mats_dev[0];
-        cudaLaunchKernelEx(&cfg, k_dem_list<VT, TRACKQ, B, M, HERTZ, true>, b);
+        cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, true>, b);
+        c->launches++;
+        cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, true>, b);
     } else {
-        cudaLaunchKernelEx(&cfg, k_dem_list<VT, TRACKQ, B, M, HERTZ, false>, a);
+        cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, false>, a);
+        c->launches++;
+        cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, false>, a);
     }
 }
 
@@ -1088,6 +1166,10 @@ int dem_list_alloc(Ctx *c) {
     PEB_CUDA(c, cudaMalloc(&L.tmp.tag, n * sizeof(uint32_t)));
     PEB_CUDA(c, cudaMalloc(&L.tmp.uid, n * sizeof(int32_t)));
     PEB_CUDA(c, cudaMalloc(&L.stash, (size_t)kListStash * n * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.act, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemset(L.act, 0, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.alist, n * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMalloc(&L.facc, 6 * n * (c->p.precision == PE_B200_FP64 ? 8 : 4)));
     if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&L.tmp.q, n * sizeof(double4)));
     L.enabled = true;
     L.check_pending = false;
@@ -1112,6 +1194,9 @@ void dem_list_free(Ctx *c) {
     cudaFree(L.tmp.uid);
     cudaFree(L.tmp.q);
     cudaFree(L.stash);
+    cudaFree(L.act);
+    cudaFree(L.alist);
+    cudaFree(L.facc);
     if (L.h_flags) cudaFreeHost(L.h_flags);
     if (L.ev) cudaEventDestroy(L.ev);
     const double skin = L.skin;

@@ -123,6 +123,12 @@ struct ListBuf {
     BodyBuf tmp;                // permutation target of a rebuild
     int32_t *stash = nullptr;   // kListStash x n, column-major: the first neighbours found by
                                 // the counting pass of the persistent rebuild
+    // spheres that can feel a force before the next rebuild (list entries, or near a wall):
+    // exclusive offsets of the marks (n + 1; act[n] = count), the marked spheres in ascending
+    // order, and their force and torque of the current step (6 x n of the precision's type)
+    int32_t *act = nullptr;
+    int32_t *alist = nullptr;
+    void *facc = nullptr;
     // persistent rebuild kernel (rebuild.cu): grid barrier words and per-block partial sums
     unsigned int *rb_bar = nullptr;
     int32_t *rb_blk = nullptr;
@@ -544,6 +550,29 @@ __device__ __forceinline__ void search_range(const SceneInfo &s, int a, double p
 
 __device__ __forceinline__ int64_t cell_key(const SceneInfo &s, int cx, int cy, int cz) {
     return s.cell_base + ((int64_t)cz * s.dim[1] + cy) * s.dim[0] + cx;
+}
+
+// Whether a sphere can feel a force before the next neighbour-list rebuild (the list step's
+// marked spheres, dem.cu): it has list entries, or a wall may come within reach while it moves
+// less than `margin` (half the skin) -- it is not inside the box of its scene's axis-aligned
+// planes by r + margin (wall_forces then tests the planes), or it is within r + margin of the
+// bounding sphere of one of the scene's fixed boxes (wall_forces tests every box).
+__device__ __forceinline__ bool list_marked(const SceneInfo &s, const double4 &p,
+                                            const double *boxes, double margin, int cnt) {
+    if (cnt > 0) return true;
+    const double r = p.w + margin;
+    const bool clear = p.x - r > s.wall_lo[0] && p.x + r < s.wall_hi[0] &&
+                       p.y - r > s.wall_lo[1] && p.y + r < s.wall_hi[1] &&
+                       p.z - r > s.wall_lo[2] && p.z + r < s.wall_hi[2];
+    if (!clear) return true;
+    for (int k = 0; k < s.nboxes; ++k) {
+        const double *B = boxes + 15 * (int64_t)(s.box_begin + k);
+        const double hx = 0.5 * B[3], hy = 0.5 * B[4], hz = 0.5 * B[5];
+        const double reach = (sqrt(hx * hx + hy * hy + hz * hz) + r) * (1.0 + 1e-9);
+        const double dx = p.x - B[0], dy = p.y - B[1], dz = p.z - B[2];
+        if (dx * dx + dy * dy + dz * dz < reach * reach) return true;
+    }
+    return false;
 }
 
 // Programmatic dependent launch: a kernel launched with the programmatic-serialization

@@ -7,8 +7,9 @@
 // separated by grid-wide barriers:
 //   clear cell counts | bin (cell key + slot, atomic histogram) | scan counts -> cell offsets |
 //   scatter | order each cell by body index | gather bodies into cell order | copy back |
-//   count neighbours closer than r_i + r_j + skin (keeping the first few) | scan counts ->
-//   list offsets | write lists
+//   count neighbours closer than r_i + r_j + skin (keeping the first few), mark the spheres that
+//   can feel a force before the next rebuild | scan counts -> list offsets | scan marks -> the
+//   marked spheres | write lists
 // Every barrier wait is bounded: a block that waits too long sets an error flag and returns.
 #include <algorithm>
 
@@ -30,6 +31,8 @@ struct RebuildArgs {
     int32_t *cnt, *start, *idx, *stash;
     int64_t cap;
     double skin;
+    const double *boxes;   // fixed boxes (15 doubles each), for the marks of the list step
+    int32_t *act, *alist;  // marks -> exclusive offsets (n + 1), the marked spheres
     float *disp;
     int32_t *flags;
     unsigned int *bar;   // [0] arrivals, [1] generation
@@ -298,12 +301,23 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
         if (a.cur.q) a.cur.q[t] = a.tmp.q[t];
     }
     if (!grid_sync(a.bar, a.err)) return;
-    // 8. neighbour counts; the first kListStash neighbours of each body are kept
-    for (int64_t t = g0; t < n; t += stride) a.cnt[t] = list_neighbours<0, VT>(a, t, 0);
+    // 8. neighbour counts; the first kListStash neighbours of each body are kept; the mark of
+    // every sphere that can feel a force before the next rebuild
+    const double margin = 0.5 * a.skin * (1.0 + 1e-9);
+    for (int64_t t = g0; t < n; t += stride) {
+        const int k = list_neighbours<0, VT>(a, t, 0);
+        a.cnt[t] = k;
+        const double4 p = a.cur.pr[t];
+        a.act[t] = list_marked(a.scenes[a.cur.tag[t] >> 16], p, a.boxes, margin, k) ? 1 : 0;
+    }
     if (!grid_sync(a.bar, a.err)) return;
-    // 9. list offsets
+    // 9. list offsets, and the marked spheres in ascending order
     if (!grid_scan(a, a.cnt, a.start, n)) return;
     if (!grid_sync(a.bar, a.err)) return;
+    if (!grid_scan(a, a.act, a.act, n)) return;
+    if (!grid_sync(a.bar, a.err)) return;
+    for (int64_t t = g0; t < n; t += stride)
+        if (a.act[t + 1] > a.act[t]) a.alist[a.act[t]] = (int32_t)t;
     const int64_t need = a.start[n];
     if (g0 == 0) {
         a.flags[1] = need > a.cap ? 1 : 0;
@@ -362,6 +376,9 @@ int launch_rebuild(Ctx *c) {
     a.stash = L.stash;
     a.cap = L.cap;
     a.skin = L.skin;
+    a.boxes = c->d_boxes;
+    a.act = L.act;
+    a.alist = L.alist;
     a.disp = L.disp;
     a.flags = L.flags;
     a.bar = L.rb_bar;
