@@ -91,7 +91,7 @@ def test_dem_mixed_precision_error_bound():
     e.step(s.dt, 200)
     x, v, w = e.download()
     assert rel_err(x - s.x, o.x - s.x) < 1e-6
-    assert rel_err(x, o.x) < 1e-9
+    assert rel_err(x, o.x) < 1e-7
     assert rel_err(v, o.v) < 1e-5
 
 
