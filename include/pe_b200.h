@@ -2,7 +2,9 @@
  * pe_b200.h -- C ABI of the B200 rigid-body time step (libpe_b200.so).
  *
  * The library owns device memory and one CUDA stream per context.  Host arrays passed in are
- * copied; the caller keeps ownership.  Every entry point returns a pe_b200_status; no C++
+ * copied; the caller keeps ownership.  Device memory comes from a stream-ordered pool per device
+ * that keeps what destroyed contexts free, so a new context reuses it instead of mapping fresh
+ * pages; pe_b200_release_memory hands the kept memory back to the device.  Every entry point returns a pe_b200_status; no C++
  * exception crosses this boundary.  A context is used by one host thread at a time.
  *
  * Each entry point replaces a piece of pe's compile-time plugin boundary (the
@@ -99,6 +101,11 @@ int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out);
 /* Releases the context and all its device memory.
  * Replaces: CollisionSystem<Config>::~CollisionSystem (DEMSolver.h:441). */
 int pe_b200_destroy(pe_b200_ctx *ctx);
+
+/* Returns the device memory the library keeps for reuse on `device` (the buffers of destroyed
+ * contexts) to the device; live contexts keep theirs.  No pe counterpart (pe allocates on the
+ * host with new/delete). */
+int pe_b200_release_memory(int32_t device);
 
 /* Human-readable text of the last error on this context ("" if none). */
 const char *pe_b200_last_error(const pe_b200_ctx *ctx);

@@ -27,7 +27,7 @@ EXPORTS = ["pe_b200_default_params", "pe_b200_create", "pe_b200_destroy", "pe_b2
            "pe_b200_set_gravity", "pe_b200_set_damping", "pe_b200_set_max_iterations",
            "pe_b200_set_relaxation_model", "pe_b200_set_error_reduction",
            "pe_b200_set_materials", "pe_b200_set_walls", "pe_b200_upload_bodies",
-           "pe_b200_set_state", "pe_b200_set_orientations", "pe_b200_step", "pe_b200_download_bodies",
+           "pe_b200_set_state", "pe_b200_set_orientations", "pe_b200_release_memory", "pe_b200_step", "pe_b200_download_bodies",
            "pe_b200_find_contacts", "pe_b200_last_step_stats", "pe_b200_set_residual",
            "pe_b200_kernel_launches", "pe_b200_stream", "pe_b200_set_profiling",
            "pe_b200_profile", "pe_b200_dem_step_static", "pe_b200_neighbor_list_stats",
@@ -93,6 +93,7 @@ def load() -> C.CDLL:
         "pe_b200_upload_bodies": (C.c_int, [vp, i64, vp, vp, vp, vp, vp, vp, i32]),
         "pe_b200_set_state": (C.c_int, [vp, vp, vp, vp]),
         "pe_b200_set_orientations": (C.c_int, [vp, vp]),
+        "pe_b200_release_memory": (C.c_int, [i32]),
         "pe_b200_step": (C.c_int, [vp, i32, dp]),
         "pe_b200_download_bodies": (C.c_int, [vp, vp, vp, vp, vp]),
         "pe_b200_find_contacts": (C.c_int, [vp, i64, vp, vp, P(i64)]),

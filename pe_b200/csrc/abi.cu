@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <new>
 
 #include "internal.cuh"
@@ -17,6 +18,48 @@ unsigned capped_grid(const Ctx *c, int64_t n, int block) {
     const int64_t g = (n + block - 1) / block;
     const int64_t cap = 8 * (int64_t)c->sm_count;
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64] = {};
+}  // namespace
+
+// The library's pool on `dev`: device memory that contexts free stays reserved (release
+// threshold: never) and serves the next allocations, on any of the library's streams.
+static cudaError_t lib_pool(int dev, cudaMemPool_t *out) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        g_pool[dev] = p;
+    }
+    *out = g_pool[dev];
+    return cudaSuccess;
+}
+
+cudaError_t dmalloc_bytes(Ctx *c, void **p, size_t bytes) {
+    *p = nullptr;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = lib_pool(c->device, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), pool, c->stream);
+}
+
+void dfree(Ctx *c, void *p) {
+    if (p) cudaFreeAsync(p, c ? c->stream : nullptr);
 }
 
 int set_err(Ctx *c, int code, const std::string &msg) {
@@ -87,34 +130,34 @@ static void prof_collect(Ctx *c) {
 
 namespace {
 
-void free_bodies(BodyBuf &b) {
-    cudaFree(b.pr);
-    cudaFree(b.vw);
-    cudaFree(b.tag);
-    cudaFree(b.uid);
-    cudaFree(b.q);
+void free_bodies(Ctx *c, BodyBuf &b) {
+    dfree(c, b.pr);
+    dfree(c, b.vw);
+    dfree(c, b.tag);
+    dfree(c, b.uid);
+    dfree(c, b.q);
     b = BodyBuf();
 }
 
 void free_device(Ctx *c) {
-    free_bodies(c->cur);
-    free_bodies(c->nxt);
-    cudaFree(c->key);
-    cudaFree(c->rank);
-    cudaFree(c->sorted);
-    cudaFree(c->cell_count);
-    cudaFree(c->cell_start);
-    cudaFree(c->scan_tmp);
-    cudaFree(c->posf);
+    free_bodies(c, c->cur);
+    free_bodies(c, c->nxt);
+    dfree(c, c->key);
+    dfree(c, c->rank);
+    dfree(c, c->sorted);
+    dfree(c, c->cell_count);
+    dfree(c, c->cell_start);
+    dfree(c, c->scan_tmp);
+    dfree(c, c->posf);
     c->posf = nullptr;
-    cudaFree(c->near);
+    dfree(c, c->near);
     c->near = nullptr;
-    cudaFree(c->d_scenes);
-    cudaFree(c->d_mats);
-    cudaFree(c->d_planes);
-    cudaFree(c->d_plane_mat);
-    cudaFree(c->d_boxes);
-    cudaFree(c->d_box_mat);
+    dfree(c, c->d_scenes);
+    dfree(c, c->d_mats);
+    dfree(c, c->d_planes);
+    dfree(c, c->d_plane_mat);
+    dfree(c, c->d_boxes);
+    dfree(c, c->d_box_mat);
     c->key = c->rank = c->sorted = c->cell_count = c->cell_start = c->scan_tmp = nullptr;
     c->scan_tmp_cap = 0;
     c->d_scenes = nullptr;
@@ -134,11 +177,11 @@ void free_device(Ctx *c) {
 
 int alloc_bodies(Ctx *c, BodyBuf &b) {
     const size_t n = (size_t)std::max<int64_t>(c->n, 1);
-    PEB_CUDA(c, cudaMalloc(&b.pr, n * sizeof(double4)));
-    PEB_CUDA(c, cudaMalloc(&b.vw, n * (size_t)c->vw_bytes));
-    PEB_CUDA(c, cudaMalloc(&b.tag, n * sizeof(uint32_t)));
-    PEB_CUDA(c, cudaMalloc(&b.uid, n * sizeof(int32_t)));
-    if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&b.q, n * sizeof(double4)));
+    PEB_CUDA(c, dmalloc(c, &b.pr, n * sizeof(double4)));
+    PEB_CUDA(c, dmalloc(c, &b.vw, n * (size_t)c->vw_bytes));
+    PEB_CUDA(c, dmalloc(c, &b.tag, n * sizeof(uint32_t)));
+    PEB_CUDA(c, dmalloc(c, &b.uid, n * sizeof(int32_t)));
+    if (c->p.track_orientation) PEB_CUDA(c, dmalloc(c, &b.q, n * sizeof(double4)));
     return PE_B200_OK;
 }
 
@@ -171,12 +214,12 @@ int upload_tables(Ctx *c) {
         md[k].young = m.young;
         md[k].poisson = m.poisson;
     }
-    cudaFree(c->d_mats);
+    dfree(c, c->d_mats);
     c->d_mats = nullptr;
-    PEB_CUDA(c, cudaMalloc(&c->d_mats, std::max<size_t>(md.size(), 1) * sizeof(MatDev)));
+    PEB_CUDA(c, dmalloc(c, &c->d_mats, std::max<size_t>(md.size(), 1) * sizeof(MatDev)));
     if (!md.empty())
-        PEB_CUDA(c, cudaMemcpy(c->d_mats, md.data(), md.size() * sizeof(MatDev),
-                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_mats, md.data(), md.size() * sizeof(MatDev),
+                               cudaMemcpyHostToDevice, c->stream));
     c->mats_dev = md;
     // walls, concatenated per scene
     c->planes.clear();
@@ -218,10 +261,10 @@ int upload_tables(Ctx *c) {
         c->box_mat.insert(c->box_mat.end(), c->scene_box_mat[s].begin(),
                           c->scene_box_mat[s].end());
     }
-    cudaFree(c->d_planes);
-    cudaFree(c->d_plane_mat);
-    cudaFree(c->d_boxes);
-    cudaFree(c->d_box_mat);
+    dfree(c, c->d_planes);
+    dfree(c, c->d_plane_mat);
+    dfree(c, c->d_boxes);
+    dfree(c, c->d_box_mat);
     c->d_planes = nullptr;
     c->d_planes_f = nullptr;
     c->d_plane_mat = nullptr;
@@ -229,33 +272,33 @@ int upload_tables(Ctx *c) {
     c->d_box_mat = nullptr;
     const size_t np = c->planes.size() / 4, nb = c->boxes.size() / 15;
     // FP64 planes followed by an FP32 copy for the kernels' quick rejection test
-    PEB_CUDA(c, cudaMalloc(&c->d_planes, std::max<size_t>(np, 1) * (sizeof(double4) + sizeof(float4))));
+    PEB_CUDA(c, dmalloc(c, &c->d_planes, std::max<size_t>(np, 1) * (sizeof(double4) + sizeof(float4))));
     c->d_planes_f = reinterpret_cast<float4 *>(c->d_planes + std::max<size_t>(np, 1));
-    PEB_CUDA(c, cudaMalloc(&c->d_plane_mat, std::max<size_t>(np, 1) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&c->d_boxes, std::max<size_t>(nb, 1) * 15 * sizeof(double)));
-    PEB_CUDA(c, cudaMalloc(&c->d_box_mat, std::max<size_t>(nb, 1) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &c->d_plane_mat, std::max<size_t>(np, 1) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &c->d_boxes, std::max<size_t>(nb, 1) * 15 * sizeof(double)));
+    PEB_CUDA(c, dmalloc(c, &c->d_box_mat, std::max<size_t>(nb, 1) * sizeof(int32_t)));
     if (np) {
-        PEB_CUDA(c, cudaMemcpy(c->d_planes, c->planes.data(), np * sizeof(double4),
-                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_planes, c->planes.data(), np * sizeof(double4),
+                               cudaMemcpyHostToDevice, c->stream));
         std::vector<float> pf(4 * np);
         for (size_t k = 0; k < 4 * np; ++k) pf[k] = (float)c->planes[k];
-        PEB_CUDA(c, cudaMemcpy(c->d_planes_f, pf.data(), np * sizeof(float4),
-                               cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(c->d_plane_mat, c->plane_mat.data(), np * sizeof(int32_t),
-                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_planes_f, pf.data(), np * sizeof(float4),
+                               cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_plane_mat, c->plane_mat.data(), np * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, c->stream));
     }
     if (nb) {
-        PEB_CUDA(c, cudaMemcpy(c->d_boxes, c->boxes.data(), nb * 15 * sizeof(double),
-                               cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(c->d_box_mat, c->box_mat.data(), nb * sizeof(int32_t),
-                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_boxes, c->boxes.data(), nb * 15 * sizeof(double),
+                               cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_box_mat, c->box_mat.data(), nb * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, c->stream));
     }
-    cudaFree(c->d_scenes);
+    dfree(c, c->d_scenes);
     c->d_scenes = nullptr;
-    PEB_CUDA(c, cudaMalloc(&c->d_scenes, std::max<size_t>(c->scenes.size(), 1) * sizeof(SceneInfo)));
+    PEB_CUDA(c, dmalloc(c, &c->d_scenes, std::max<size_t>(c->scenes.size(), 1) * sizeof(SceneInfo)));
     if (!c->scenes.empty())
-        PEB_CUDA(c, cudaMemcpy(c->d_scenes, c->scenes.data(), c->scenes.size() * sizeof(SceneInfo),
-                               cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpyAsync(c->d_scenes, c->scenes.data(), c->scenes.size() * sizeof(SceneInfo),
+                               cudaMemcpyHostToDevice, c->stream));
     return PE_B200_OK;
 }
 
@@ -421,21 +464,37 @@ int pe_b200_create(const pe_b200_params *p, pe_b200_ctx **out) {
     c->vw_bytes = p->precision == PE_B200_FP64 ? 6 * 8 : 7 * 4;
     cudaError_t e = cudaSetDevice(p->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int32_t));
+    if (e == cudaSuccess) e = dmalloc(c, &c->d_err, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_err, 0, sizeof(int32_t), c->stream);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_err, sizeof(int32_t));
     if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, p->device);
     if (e != cudaSuccess) {
         int rc = cuda_err(c, e, "pe_b200_create");
         if (c->stream) cudaStreamDestroy(c->stream);
-        cudaFree(c->d_err);
+        dfree(c, c->d_err);
         if (c->h_err) cudaFreeHost(c->h_err);
         delete c;
         return rc;
     }
     *out = reinterpret_cast<pe_b200_ctx *>(c);
     return PE_B200_OK;
+}
+
+int pe_b200_release_memory(int32_t device) {
+    if (device < 0 || device >= 64) return PE_B200_ERR_ARG;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        pool = g_pool[device];
+    }
+    if (!pool) return PE_B200_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return PE_B200_ERR_CUDA;
+    const cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+    cudaSetDevice(prev);
+    return e == cudaSuccess ? PE_B200_OK : PE_B200_ERR_CUDA;
 }
 
 int pe_b200_destroy(pe_b200_ctx *h) {
@@ -447,7 +506,7 @@ int pe_b200_destroy(pe_b200_ctx *h) {
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     c->ev_pool.clear();
     free_device(c);
-    cudaFree(c->d_err);
+    dfree(c, c->d_err);
     if (c->h_err) cudaFreeHost(c->h_err);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

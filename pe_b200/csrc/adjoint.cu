@@ -338,20 +338,20 @@ __global__ void __launch_bounds__(128) k_adjoint(AdjArgs a) {
     }
 }
 
-void free_ckpt(BodyBuf &b) {
-    cudaFree(b.pr);
-    cudaFree(b.vw);
-    cudaFree(b.tag);
-    cudaFree(b.uid);
+void free_ckpt(Ctx *c, BodyBuf &b) {
+    dfree(c, b.pr);
+    dfree(c, b.vw);
+    dfree(c, b.tag);
+    dfree(c, b.uid);
     b = BodyBuf();
 }
 
 int alloc_ckpt(Ctx *c, BodyBuf &b) {
     const size_t n = (size_t)std::max<int64_t>(c->n, 1);
-    PEB_CUDA(c, cudaMalloc(&b.pr, n * sizeof(double4)));
-    PEB_CUDA(c, cudaMalloc(&b.vw, n * (size_t)c->vw_bytes));
-    PEB_CUDA(c, cudaMalloc(&b.tag, n * sizeof(uint32_t)));
-    PEB_CUDA(c, cudaMalloc(&b.uid, n * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &b.pr, n * sizeof(double4)));
+    PEB_CUDA(c, dmalloc(c, &b.vw, n * (size_t)c->vw_bytes));
+    PEB_CUDA(c, dmalloc(c, &b.tag, n * sizeof(uint32_t)));
+    PEB_CUDA(c, dmalloc(c, &b.uid, n * sizeof(int32_t)));
     return PE_B200_OK;
 }
 
@@ -373,8 +373,8 @@ int plain_step(Ctx *c, double dt) {
 }  // namespace
 
 void adjoint_free(Ctx *c) {
-    for (auto &b : c->adj.ckpt) free_ckpt(b);
-    for (auto &b : c->adj.seg) free_ckpt(b);
+    for (auto &b : c->adj.ckpt) free_ckpt(c, b);
+    for (auto &b : c->adj.seg) free_ckpt(c, b);
     c->adj.ckpt.clear();
     c->adj.seg.clear();
     c->adj.nsteps = 0;
@@ -420,11 +420,11 @@ int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *g
     double *d_gpar = nullptr;
     const unsigned blocks = grid_for(n, 128);
     cudaError_t e = cudaSuccess;
-    for (int k = 0; k < 6 && e == cudaSuccess; ++k) e = cudaMalloc(&l[k], vb);
-    if (e == cudaSuccess) e = cudaMalloc(&d_gpar, 4 * sizeof(double) * blocks);
+    for (int k = 0; k < 6 && e == cudaSuccess; ++k) e = dmalloc(c, &l[k], vb);
+    if (e == cudaSuccess) e = dmalloc(c, &d_gpar, 4 * sizeof(double) * blocks);
     auto cleanup = [&]() {
-        for (int k = 0; k < 6; ++k) cudaFree(l[k]);
-        cudaFree(d_gpar);
+        for (int k = 0; k < 6; ++k) dfree(c, l[k]);
+        dfree(c, d_gpar);
     };
     if (e != cudaSuccess) {
         cleanup();
@@ -509,7 +509,7 @@ int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *g
     c->binned = false;
     if (!rc && c->nl.enabled) rc = dem_list_request_rebuild(c);
     cudaStreamSynchronize(c->stream);
-    free_ckpt(final_state);
+    free_ckpt(c, final_state);
     cleanup();
     return rc;
 }

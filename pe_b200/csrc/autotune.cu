@@ -21,12 +21,12 @@ namespace peb {
 
 namespace {
 
-void free_snap(BodyBuf &b) {
-    cudaFree(b.pr);
-    cudaFree(b.vw);
-    cudaFree(b.tag);
-    cudaFree(b.uid);
-    cudaFree(b.q);
+void free_snap(Ctx *c, BodyBuf &b) {
+    dfree(c, b.pr);
+    dfree(c, b.vw);
+    dfree(c, b.tag);
+    dfree(c, b.uid);
+    dfree(c, b.q);
     b = BodyBuf();
 }
 
@@ -51,12 +51,12 @@ int set_list_skin(Ctx *c, double skin) {
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     c->nl.skin = skin;
     plan_cells(c, skin);
-    cudaFree(c->cell_count);
-    cudaFree(c->cell_start);
+    dfree(c, c->cell_count);
+    dfree(c, c->cell_start);
     c->cell_count = c->cell_start = nullptr;
-    PEB_CUDA(c, cudaMalloc(&c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMemset(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemsetAsync(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t), c->stream));
     int rc = upload_tables(c);
     if (rc) return rc;
     c->binned = false;
@@ -86,13 +86,13 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
     if (!(dt > 0.0) || trial < 2) return PE_B200_ERR_ARG;
     BodyBuf snap;
     const size_t n = (size_t)c->n;
-    cudaError_t e = cudaMalloc(&snap.pr, n * sizeof(double4));
-    if (e == cudaSuccess) e = cudaMalloc(&snap.vw, n * (size_t)c->vw_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&snap.tag, n * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&snap.uid, n * sizeof(int32_t));
-    if (e == cudaSuccess && c->cur.q) e = cudaMalloc(&snap.q, n * sizeof(double4));
+    cudaError_t e = dmalloc(c, &snap.pr, n * sizeof(double4));
+    if (e == cudaSuccess) e = dmalloc(c, &snap.vw, n * (size_t)c->vw_bytes);
+    if (e == cudaSuccess) e = dmalloc(c, &snap.tag, n * sizeof(uint32_t));
+    if (e == cudaSuccess) e = dmalloc(c, &snap.uid, n * sizeof(int32_t));
+    if (e == cudaSuccess && c->cur.q) e = dmalloc(c, &snap.q, n * sizeof(double4));
     if (e != cudaSuccess) {
-        free_snap(snap);
+        free_snap(c, snap);
         return cuda_err(c, e, "autotune snapshot");
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -159,7 +159,7 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
     c->prof = prof0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    free_snap(snap);
+    free_snap(c, snap);
     if (rc) return rc;
     if (out) {
         out->dem_variant = best.dem_variant;

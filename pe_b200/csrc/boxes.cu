@@ -1170,14 +1170,14 @@ static void box_props(const double *len, double density, double *out) {
 
 void mbox_free(Ctx *c) {
     MBoxBuf &b = c->mb;
-    cudaFree(b.x);
-    cudaFree(b.x2);
-    cudaFree(b.len);
-    cudaFree(b.mat);
-    cudaFree(b.cnt);
-    cudaFree(b.ext);
-    cudaFree(b.R);
-    cudaFree(b.gstart);
+    dfree(c, b.x);
+    dfree(c, b.x2);
+    dfree(c, b.len);
+    dfree(c, b.mat);
+    dfree(c, b.cnt);
+    dfree(c, b.ext);
+    dfree(c, b.R);
+    dfree(c, b.gstart);
     b = MBoxBuf();
 }
 
@@ -1189,17 +1189,17 @@ int mbox_upload(Ctx *c, int32_t m, const double *x, const double *q, const doubl
         MBoxBuf &b = c->mb;
         const size_t nm = (size_t)m;
         // one allocation per buffer set: x q v w (13 per box), twice; len + props (11); ints
-        PEB_CUDA(c, cudaMalloc(&b.x, 13 * nm * sizeof(double)));
-        PEB_CUDA(c, cudaMalloc(&b.x2, 13 * nm * sizeof(double)));
-        PEB_CUDA(c, cudaMalloc(&b.len, 11 * nm * sizeof(double)));
-        PEB_CUDA(c, cudaMalloc(&b.mat, 2 * nm * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.cnt, (nm + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.x, 13 * nm * sizeof(double)));
+        PEB_CUDA(c, dmalloc(c, &b.x2, 13 * nm * sizeof(double)));
+        PEB_CUDA(c, dmalloc(c, &b.len, 11 * nm * sizeof(double)));
+        PEB_CUDA(c, dmalloc(c, &b.mat, 2 * nm * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.cnt, (nm + 2) * sizeof(int32_t)));
         // rotations, bounding boxes, grid parameters; grid cells, box lists, neighbour bits
-        PEB_CUDA(c, cudaMalloc(&b.R, (15 * nm + 8) * sizeof(double)));
+        PEB_CUDA(c, dmalloc(c, &b.R, (15 * nm + 8) * sizeof(double)));
         b.aabb = b.R + 9 * nm;
         b.gparm = b.aabb + 6 * nm;
         const size_t cells = (size_t)kMaxBoxCells + 2;
-        PEB_CUDA(c, cudaMalloc(&b.gstart, (2 * cells + 2 * nm + cells / 32 + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.gstart, (2 * cells + 2 * nm + cells / 32 + 2) * sizeof(int32_t)));
         b.gfill = b.gstart + cells;
         b.gids = b.gfill + cells;
         b.gcell = b.gids + nm;
@@ -1220,21 +1220,21 @@ int mbox_upload(Ctx *c, int32_t m, const double *x, const double *q, const doubl
             ints[k] = mat[k];
             ints[nm + k] = scene ? scene[k] : 0;
         }
-        PEB_CUDA(c, cudaMemcpy(b.x, x, 3 * nm * sizeof(double), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(b.q, q, 4 * nm * sizeof(double), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(b.v, v, 3 * nm * sizeof(double), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(b.w, w, 3 * nm * sizeof(double), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(b.len, len, 3 * nm * sizeof(double), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(b.props, props.data(), 8 * nm * sizeof(double), cudaMemcpyHostToDevice));
-        PEB_CUDA(c, cudaMemcpy(b.mat, ints.data(), 2 * nm * sizeof(int32_t), cudaMemcpyHostToDevice));
+        PEB_CUDA(c, cudaMemcpyAsync(b.x, x, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(b.q, q, 4 * nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(b.v, v, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(b.w, w, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(b.len, len, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(b.props, props.data(), 8 * nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PEB_CUDA(c, cudaMemcpyAsync(b.mat, ints.data(), 2 * nm * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
         for (int32_t k = 0; k < m; ++k) {
             SceneInfo &s = c->scenes[ints[nm + k]];
             if (s.nmbox == 0) s.mbox_begin = k;
             s.nmbox++;
         }
     }
-    PEB_CUDA(c, cudaMemcpy(c->d_scenes, c->scenes.data(), c->scenes.size() * sizeof(SceneInfo),
-                           cudaMemcpyHostToDevice));
+    PEB_CUDA(c, cudaMemcpyAsync(c->d_scenes, c->scenes.data(), c->scenes.size() * sizeof(SceneInfo),
+                           cudaMemcpyHostToDevice, c->stream));
     c->epoch++;
     return PE_B200_OK;
 }
@@ -1244,10 +1244,11 @@ int mbox_download(Ctx *c, double *x, double *q, double *v, double *w) {
     const size_t nm = (size_t)b.m;
     if (nm == 0) return PE_B200_OK;
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (x) PEB_CUDA(c, cudaMemcpy(x, b.x, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost));
-    if (q) PEB_CUDA(c, cudaMemcpy(q, b.q, 4 * nm * sizeof(double), cudaMemcpyDeviceToHost));
-    if (v) PEB_CUDA(c, cudaMemcpy(v, b.v, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost));
-    if (w) PEB_CUDA(c, cudaMemcpy(w, b.w, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost));
+    if (x) PEB_CUDA(c, cudaMemcpyAsync(x, b.x, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (q) PEB_CUDA(c, cudaMemcpyAsync(q, b.q, 4 * nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (v) PEB_CUDA(c, cudaMemcpyAsync(v, b.v, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (w) PEB_CUDA(c, cudaMemcpyAsync(w, b.w, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     return PE_B200_OK;
 }
 
@@ -1265,9 +1266,9 @@ int mbox_dem(Ctx *c, double dt) {
     const int64_t n = c->n;
     const size_t nn = (size_t)std::max<int64_t>(n, 1);
     if (b.ext_cap < n || !b.ext) {
-        cudaFree(b.ext);
+        dfree(c, b.ext);
         b.ext = nullptr;
-        PEB_CUDA(c, cudaMalloc(&b.ext, nn * 6 * sizeof(double) + (nn + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.ext, nn * 6 * sizeof(double) + (nn + 2) * sizeof(int32_t)));
         b.ext_cap = n;
     }
     int32_t *near_list = (int32_t *)(b.ext + 6 * nn);
@@ -1353,8 +1354,8 @@ int mbox_find_contacts(Ctx *c, std::vector<int64_t> &ids, std::vector<double> &g
     if (total == 0) return PE_B200_OK;
     int64_t *d_ids = nullptr;
     double *d_geom = nullptr;
-    cudaError_t e = cudaMalloc(&d_ids, (size_t)total * 3 * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&d_geom, (size_t)total * 7 * sizeof(double));
+    cudaError_t e = dmalloc(c, &d_ids, (size_t)total * 3 * sizeof(int64_t));
+    if (e == cudaSuccess) e = dmalloc(c, &d_geom, (size_t)total * 7 * sizeof(double));
     const int64_t total_walls = (int64_t)(c->planes.size() / 4 + c->boxes.size() / 15);
     if (e == cudaSuccess) {
         k_box_list<<<b.m, kBoxBlk, 0, c->stream>>>(a, b.cnt, total, c->n, total_walls, d_ids,
@@ -1371,8 +1372,8 @@ int mbox_find_contacts(Ctx *c, std::vector<int64_t> &ids, std::vector<double> &g
         e = cudaMemcpyAsync(geom.data(), d_geom, geom.size() * sizeof(double),
                             cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(d_ids);
-    cudaFree(d_geom);
+    dfree(c, d_ids);
+    dfree(c, d_geom);
     if (e != cudaSuccess) return cuda_err(c, e, "box contacts");
     return PE_B200_OK;
 }

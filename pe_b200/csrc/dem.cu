@@ -1127,8 +1127,8 @@ int dem_step(Ctx *c, double dt) {
         // the sorted FP32 position copy of the default grid form
         const bool with_pos = c->tune.dem_grid != 1;
         if (with_pos && !c->posf) {
-            PEB_CUDA(c, cudaMalloc(&c->posf, (size_t)c->n * sizeof(float4)));
-            PEB_CUDA(c, cudaMalloc(&c->near, (size_t)c->n * (1 + kNear) * sizeof(int32_t)));
+            PEB_CUDA(c, dmalloc(c, &c->posf, (size_t)c->n * sizeof(float4)));
+            PEB_CUDA(c, dmalloc(c, &c->near, (size_t)c->n * (1 + kNear) * sizeof(int32_t)));
         }
         rc = grid_sort(c, with_pos);
         if (rc) return rc;
@@ -1150,27 +1150,27 @@ int dem_list_alloc(Ctx *c) {
     ListBuf &L = c->nl;
     const size_t n = (size_t)std::max<int64_t>(c->n, 1);
     L.cap = c->p.max_contacts > 0 ? c->p.max_contacts : std::max<int64_t>(16 * c->n, 1024);
-    PEB_CUDA(c, cudaMalloc(&L.start, (n + 2) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.cnt, (n + 2) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.idx, (size_t)L.cap * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.disp, n * sizeof(float)));
-    PEB_CUDA(c, cudaMalloc(&L.flags, 8 * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMemset(L.flags, 0, 8 * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMemset(L.disp, 0, n * sizeof(float)));
+    PEB_CUDA(c, dmalloc(c, &L.start, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.cnt, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.idx, (size_t)L.cap * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.disp, n * sizeof(float)));
+    PEB_CUDA(c, dmalloc(c, &L.flags, 8 * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemsetAsync(L.flags, 0, 8 * sizeof(int32_t), c->stream));
+    PEB_CUDA(c, cudaMemsetAsync(L.disp, 0, n * sizeof(float), c->stream));
     if (!L.h_flags) PEB_CUDA(c, cudaMallocHost(&L.h_flags, 8 * sizeof(int32_t)));
     if (!L.ev) PEB_CUDA(c, cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming));
-    PEB_CUDA(c, cudaMalloc(&L.rb_bar, 2 * sizeof(unsigned int)));
-    PEB_CUDA(c, cudaMemset(L.rb_bar, 0, 2 * sizeof(unsigned int)));
-    PEB_CUDA(c, cudaMalloc(&L.tmp.pr, n * sizeof(double4)));
-    PEB_CUDA(c, cudaMalloc(&L.tmp.vw, n * (size_t)c->vw_bytes));
-    PEB_CUDA(c, cudaMalloc(&L.tmp.tag, n * sizeof(uint32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.tmp.uid, n * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.stash, (size_t)kListStash * n * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.act, (n + 2) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMemset(L.act, 0, (n + 2) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.alist, n * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&L.facc, 6 * n * (c->p.precision == PE_B200_FP64 ? 8 : 4)));
-    if (c->p.track_orientation) PEB_CUDA(c, cudaMalloc(&L.tmp.q, n * sizeof(double4)));
+    PEB_CUDA(c, dmalloc(c, &L.rb_bar, 2 * sizeof(unsigned int)));
+    PEB_CUDA(c, cudaMemsetAsync(L.rb_bar, 0, 2 * sizeof(unsigned int), c->stream));
+    PEB_CUDA(c, dmalloc(c, &L.tmp.pr, n * sizeof(double4)));
+    PEB_CUDA(c, dmalloc(c, &L.tmp.vw, n * (size_t)c->vw_bytes));
+    PEB_CUDA(c, dmalloc(c, &L.tmp.tag, n * sizeof(uint32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.tmp.uid, n * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.stash, (size_t)kListStash * n * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.act, (n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, cudaMemsetAsync(L.act, 0, (n + 2) * sizeof(int32_t), c->stream));
+    PEB_CUDA(c, dmalloc(c, &L.alist, n * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &L.facc, 6 * n * (c->p.precision == PE_B200_FP64 ? 8 : 4)));
+    if (c->p.track_orientation) PEB_CUDA(c, dmalloc(c, &L.tmp.q, n * sizeof(double4)));
     L.enabled = true;
     L.check_pending = false;
     L.warm = false;
@@ -1181,22 +1181,22 @@ void dem_list_free(Ctx *c) {
     ListBuf &L = c->nl;
     dem_graph_free(c);
     if (L.check_pending && L.ev) cudaEventSynchronize(L.ev);
-    cudaFree(L.rb_bar);
-    cudaFree(L.rb_blk);
-    cudaFree(L.start);
-    cudaFree(L.cnt);
-    cudaFree(L.idx);
-    cudaFree(L.disp);
-    cudaFree(L.flags);
-    cudaFree(L.tmp.pr);
-    cudaFree(L.tmp.vw);
-    cudaFree(L.tmp.tag);
-    cudaFree(L.tmp.uid);
-    cudaFree(L.tmp.q);
-    cudaFree(L.stash);
-    cudaFree(L.act);
-    cudaFree(L.alist);
-    cudaFree(L.facc);
+    dfree(c, L.rb_bar);
+    dfree(c, L.rb_blk);
+    dfree(c, L.start);
+    dfree(c, L.cnt);
+    dfree(c, L.idx);
+    dfree(c, L.disp);
+    dfree(c, L.flags);
+    dfree(c, L.tmp.pr);
+    dfree(c, L.tmp.vw);
+    dfree(c, L.tmp.tag);
+    dfree(c, L.tmp.uid);
+    dfree(c, L.tmp.q);
+    dfree(c, L.stash);
+    dfree(c, L.act);
+    dfree(c, L.alist);
+    dfree(c, L.facc);
     if (L.h_flags) cudaFreeHost(L.h_flags);
     if (L.ev) cudaEventDestroy(L.ev);
     const double skin = L.skin;
@@ -1222,9 +1222,9 @@ int list_capacity_check(Ctx *c) {
             PEB_CUDA(c, cudaStreamSynchronize(c->stream));
             const int64_t need = std::max<int64_t>(L.h_flags[2], 0);
             const int64_t cap = std::max<int64_t>(2 * L.cap, need + need / 4 + 1024);
-            cudaFree(L.idx);
+            dfree(c, L.idx);
             L.idx = nullptr;
-            PEB_CUDA(c, cudaMalloc(&L.idx, (size_t)cap * sizeof(int32_t)));
+            PEB_CUDA(c, dmalloc(c, &L.idx, (size_t)cap * sizeof(int32_t)));
             L.cap = cap;
             c->epoch++;
             int rc = dem_list_request_rebuild(c);

@@ -142,9 +142,9 @@ int scan_reserve(Ctx *c, int64_t n) {
         m = tiles;
     }
     if (need + 1 > c->scan_tmp_cap) {
-        if (c->scan_tmp) cudaFree(c->scan_tmp);
+        if (c->scan_tmp) dfree(c, c->scan_tmp);
         c->scan_tmp = nullptr;
-        PEB_CUDA(c, cudaMalloc(&c->scan_tmp, (size_t)(need + 1) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &c->scan_tmp, (size_t)(need + 1) * sizeof(int32_t)));
         c->scan_tmp_cap = need + 1;
     }
     return PE_B200_OK;
@@ -168,9 +168,9 @@ int scan_exclusive_cond(Ctx *c, const int32_t *in, int32_t *out, int64_t n, cons
         m = tiles;
     }
     if (need + 1 > c->scan_tmp_cap) {
-        if (c->scan_tmp) cudaFree(c->scan_tmp);
+        if (c->scan_tmp) dfree(c, c->scan_tmp);
         c->scan_tmp = nullptr;
-        PEB_CUDA(c, cudaMalloc(&c->scan_tmp, (size_t)(need + 1) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &c->scan_tmp, (size_t)(need + 1) * sizeof(int32_t)));
         c->scan_tmp_cap = need + 1;
     }
     // the last input element, kept for the total (the scan may run in place)
@@ -212,11 +212,11 @@ int scan_exclusive_cond(Ctx *c, const int32_t *in, int32_t *out, int64_t n, cons
 
 int grid_alloc(Ctx *c) {
     const size_t n = (size_t)c->n;
-    PEB_CUDA(c, cudaMalloc(&c->key, n * sizeof(int32_t) + 16));
-    PEB_CUDA(c, cudaMalloc(&c->rank, n * sizeof(int32_t) + 16));
-    PEB_CUDA(c, cudaMalloc(&c->sorted, n * sizeof(int32_t) + 16));
-    PEB_CUDA(c, cudaMalloc(&c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
-    PEB_CUDA(c, cudaMalloc(&c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &c->key, n * sizeof(int32_t) + 16));
+    PEB_CUDA(c, dmalloc(c, &c->rank, n * sizeof(int32_t) + 16));
+    PEB_CUDA(c, dmalloc(c, &c->sorted, n * sizeof(int32_t) + 16));
+    PEB_CUDA(c, dmalloc(c, &c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
     return PE_B200_OK;
 }
 

@@ -259,6 +259,17 @@ enum : int32_t {
     DERR_COLORS = 16,
 };
 
+// Device memory of a context comes from a stream-ordered pool per device that keeps what
+// contexts free (abi.cu): a new context reuses the memory of the ones before it instead of
+// mapping fresh pages.  dmalloc allocates on the context's stream, dfree frees there (nullptr
+// allowed).
+cudaError_t dmalloc_bytes(Ctx *c, void **p, size_t bytes);
+void dfree(Ctx *c, void *p);
+template <typename T>
+inline cudaError_t dmalloc(Ctx *c, T **p, size_t bytes) {
+    return dmalloc_bytes(c, reinterpret_cast<void **>(p), bytes);
+}
+
 int set_err(Ctx *c, int code, const std::string &msg);
 int cuda_err(Ctx *c, cudaError_t e, const char *where);
 

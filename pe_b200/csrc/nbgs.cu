@@ -1118,37 +1118,37 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
     const size_t es = (c->p.precision == PE_B200_FP64) ? 8 : 4;
     const int64_t n = std::max<int64_t>(c->n, 1);
     if (b.cap < cap) {
-        cudaFree(b.cache);
+        dfree(c, b.cache);
         b.cache = nullptr;
-        cudaFree(b.order);
+        dfree(c, b.order);
         b.order = nullptr;
-        cudaFree(b.color);
+        dfree(c, b.color);
         b.color = nullptr;
-        cudaFree(b.body_adj);
+        dfree(c, b.body_adj);
         b.body_adj = nullptr;
         // raw: 2 int + 11 T; cache: 2 int + (kRec + 3) x 4 T  (per contact)
         const size_t bytes = (size_t)cap * (4 * sizeof(int32_t) + (11 + 4 * (kRec + 3)) * es) + 64 * 256;
-        PEB_CUDA(c, cudaMalloc(&b.cache, bytes));
-        PEB_CUDA(c, cudaMalloc(&b.order, (size_t)cap * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.color, (size_t)cap * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.body_adj, (size_t)2 * cap * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.cache, bytes));
+        PEB_CUDA(c, dmalloc(c, &b.order, (size_t)cap * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.color, (size_t)cap * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.body_adj, (size_t)2 * cap * sizeof(int32_t)));
         b.cap = cap;
     }
     // per-body buffers: spheres, then moving boxes (with inverse inertia rows, GEN)
     const bool gen = c->mb.m > 0;
     const int64_t nbod = n + c->mb.m;
     if (b.cnt && (b.nbod != nbod || b.gen != gen)) {
-        cudaFree(b.cnt);
-        cudaFree(b.body_cnt);
-        cudaFree(b.used);
-        cudaFree(b.vel);
+        dfree(c, b.cnt);
+        dfree(c, b.body_cnt);
+        dfree(c, b.used);
+        dfree(c, b.vel);
         b.cnt = b.body_cnt = nullptr;
         b.used = nullptr;
         b.vel = nullptr;
-        cudaFree(b.flags);
-        cudaFree(b.red);
-        cudaFree(b.cstart_dev);
-        cudaFree(b.bar);
+        dfree(c, b.flags);
+        dfree(c, b.red);
+        dfree(c, b.cstart_dev);
+        dfree(c, b.bar);
         if (b.color_start) cudaFreeHost(b.color_start);
         b.flags = nullptr;
         b.red = nullptr;
@@ -1159,16 +1159,16 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
     if (!b.cnt) {
         b.nbod = nbod;
         b.gen = gen;
-        PEB_CUDA(c, cudaMalloc(&b.cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.body_cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.used, (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t)));
-        PEB_CUDA(c, cudaMalloc(&b.vel, (size_t)nbod * (gen ? 28 : 16) * es));
-        PEB_CUDA(c, cudaMalloc(&b.flags, 2 * kMaxColors * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.body_cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.used, (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t)));
+        PEB_CUDA(c, dmalloc(c, &b.vel, (size_t)nbod * (gen ? 28 : 16) * es));
+        PEB_CUDA(c, dmalloc(c, &b.flags, 2 * kMaxColors * sizeof(int32_t)));
         PEB_CUDA(c, cudaMallocHost(&b.color_start, (2 * kMaxColors + 8) * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.red, 4 * sizeof(double)));
-        PEB_CUDA(c, cudaMalloc(&b.cstart_dev, (kMaxColors + 2) * sizeof(int32_t)));
-        PEB_CUDA(c, cudaMalloc(&b.bar, 2 * sizeof(unsigned int)));
-        PEB_CUDA(c, cudaMemset(b.bar, 0, 2 * sizeof(unsigned int)));
+        PEB_CUDA(c, dmalloc(c, &b.red, 4 * sizeof(double)));
+        PEB_CUDA(c, dmalloc(c, &b.cstart_dev, (kMaxColors + 2) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.bar, 2 * sizeof(unsigned int)));
+        PEB_CUDA(c, cudaMemsetAsync(b.bar, 0, 2 * sizeof(unsigned int), c->stream));
     }
     return PE_B200_OK;
 }
@@ -1666,18 +1666,18 @@ int nbgs_step_t(Ctx *c, double dt) {
 
 void nbgs_free(Ctx *c) {
     NbgsBuf &b = c->nb;
-    cudaFree(b.cache);
-    cudaFree(b.order);
-    cudaFree(b.color);
-    cudaFree(b.body_adj);
-    cudaFree(b.cnt);
-    cudaFree(b.body_cnt);
-    cudaFree(b.used);
-    cudaFree(b.vel);
-    cudaFree(b.flags);
-    cudaFree(b.red);
-    cudaFree(b.cstart_dev);
-    cudaFree(b.bar);
+    dfree(c, b.cache);
+    dfree(c, b.order);
+    dfree(c, b.color);
+    dfree(c, b.body_adj);
+    dfree(c, b.cnt);
+    dfree(c, b.body_cnt);
+    dfree(c, b.used);
+    dfree(c, b.vel);
+    dfree(c, b.flags);
+    dfree(c, b.red);
+    dfree(c, b.cstart_dev);
+    dfree(c, b.bar);
     if (b.color_start) cudaFreeHost(b.color_start);
     b = NbgsBuf();
 }
@@ -1735,12 +1735,12 @@ int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_ou
     int rc = grid_sort(c);
     if (rc) return rc;
     int32_t *cnt = nullptr;
-    PEB_CUDA(c, cudaMalloc(&cnt, ((size_t)n + 2) * sizeof(int32_t)));
+    PEB_CUDA(c, dmalloc(c, &cnt, ((size_t)n + 2) * sizeof(int32_t)));
     VisitArgs va = visit_args(c, c->sorted);
     k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, cnt);
     PEB_LAUNCHED(c);
     rc = scan_exclusive(c, cnt, cnt, n);
-    if (rc) { cudaFree(cnt); return rc; }
+    if (rc) { dfree(c, cnt); return rc; }
     int32_t total = 0;
     PEB_CUDA(c, cudaMemcpyAsync(&total, cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1748,10 +1748,10 @@ int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_ou
     std::vector<double> hg(7 * (size_t)std::max(total, 1));
     int64_t *d_ids = nullptr;
     double *d_geom = nullptr;
-    cudaError_t e = cudaMalloc(&d_ids, hid.size() * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&d_geom, hg.size() * sizeof(double));
+    cudaError_t e = dmalloc(c, &d_ids, hid.size() * sizeof(int64_t));
+    if (e == cudaSuccess) e = dmalloc(c, &d_geom, hg.size() * sizeof(double));
     if (e != cudaSuccess) {
-        cudaFree(cnt); cudaFree(d_ids); cudaFree(d_geom);
+        dfree(c, cnt); dfree(c, d_ids); dfree(c, d_geom);
         return cuda_err(c, e, "find_contacts alloc");
     }
     k_list<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, cnt, total, d_ids, d_geom);
@@ -1760,9 +1760,9 @@ int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_ou
     if (e == cudaSuccess) e = cudaMemcpyAsync(hid.data(), d_ids, hid.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hg.data(), d_geom, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(cnt);
-    cudaFree(d_ids);
-    cudaFree(d_geom);
+    dfree(c, cnt);
+    dfree(c, d_ids);
+    dfree(c, d_geom);
     if (e != cudaSuccess) return cuda_err(c, e, "find_contacts");
     // the contacts of the moving boxes (pe's orientation and ids) follow
     {

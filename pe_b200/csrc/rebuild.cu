@@ -353,9 +353,9 @@ int launch_rebuild(Ctx *c) {
     const int per_sm = c->tune.rebuild_per_sm > 0 ? std::min(occ, c->tune.rebuild_per_sm) : occ;
     const unsigned grid = (unsigned)std::min<int64_t>(want, (int64_t)per_sm * c->sm_count);
     if (L.rb_blk_cap < (int64_t)grid + 1) {
-        cudaFree(L.rb_blk);
+        dfree(c, L.rb_blk);
         L.rb_blk = nullptr;
-        PEB_CUDA(c, cudaMalloc(&L.rb_blk, ((size_t)grid + 1) * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &L.rb_blk, ((size_t)grid + 1) * sizeof(int32_t)));
         L.rb_blk_cap = grid + 1;
     }
     RebuildArgs<VT> a;

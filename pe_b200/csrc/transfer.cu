@@ -107,10 +107,10 @@ __global__ void k_scatter_q(int64_t n, const int32_t *uid, const double *q, doub
 
 int stage_reserve(Ctx *c, size_t bytes) {
     if (c->stage_bytes >= bytes) return PE_B200_OK;
-    cudaFree(c->stage);
+    dfree(c, c->stage);
     c->stage = nullptr;
     c->stage_bytes = 0;
-    PEB_CUDA(c, cudaMalloc(&c->stage, bytes));
+    PEB_CUDA(c, dmalloc(c, &c->stage, bytes));
     c->stage_bytes = bytes;
     return PE_B200_OK;
 }
@@ -222,7 +222,7 @@ int scatter_orientations(Ctx *c, const double *q) {
 }
 
 void stage_free(Ctx *c) {
-    cudaFree(c->stage);
+    dfree(c, c->stage);
     c->stage = nullptr;
     c->stage_bytes = 0;
 }

@@ -41,7 +41,8 @@ int validate_coloring(Ctx *c, int64_t *bad) {
     if (nc <= 0 || ncol <= 0 || !nb.cache || !nb.color_start) return PE_B200_OK;
     std::vector<int32_t> ids(2 * nc);
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
-    PEB_CUDA(c, cudaMemcpy(ids.data(), nbgs_ids_ptr(c), nc * sizeof(int2), cudaMemcpyDeviceToHost));
+    PEB_CUDA(c, cudaMemcpyAsync(ids.data(), nbgs_ids_ptr(c), nc * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     *bad += coloring_problems(c->n + c->mb.m, nc, ids.data(), ncol, nb.color_start);
     return PE_B200_OK;
 }
@@ -54,21 +55,24 @@ int validate_lists(Ctx *c, int64_t *bad) {
     if (!L.enabled || !L.warm || c->mb.m > 0 || n == 0 || !L.start || !L.flags) return PE_B200_OK;
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     int32_t flags[4];
-    PEB_CUDA(c, cudaMemcpy(flags, L.flags, sizeof flags, cudaMemcpyDeviceToHost));
+    PEB_CUDA(c, cudaMemcpyAsync(flags, L.flags, sizeof flags, cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     if (flags[1] != 0) return PE_B200_OK;
     std::vector<int32_t> start(n + 1), uid(n);
-    PEB_CUDA(c, cudaMemcpy(start.data(), L.start, (n + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    PEB_CUDA(c, cudaMemcpy(uid.data(), c->cur.uid, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    PEB_CUDA(c, cudaMemcpyAsync(start.data(), L.start, (n + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaMemcpyAsync(uid.data(), c->cur.uid, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     const int64_t m = std::min<int64_t>(std::max<int64_t>(start[n], 0), L.cap);
     std::vector<int32_t> idx(std::max<int64_t>(m, 1));
-    if (m) PEB_CUDA(c, cudaMemcpy(idx.data(), L.idx, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (m) PEB_CUDA(c, cudaMemcpyAsync(idx.data(), L.idx, m * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     *bad += list_problems(n, L.cap, start.data(), idx.data(), uid.data());
     return PE_B200_OK;
 }
 
 int selftest_timeout(Ctx *c, int64_t polls) {
     unsigned int *flag = nullptr;
-    PEB_CUDA(c, cudaMalloc(&flag, sizeof(unsigned int)));
+    PEB_CUDA(c, dmalloc(c, &flag, sizeof(unsigned int)));
     cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(unsigned int), c->stream);
     if (e == cudaSuccess) {
         k_wait_never<<<1, 32, 0, c->stream>>>(flag, (unsigned long long)polls, c->d_err);
@@ -76,7 +80,7 @@ int selftest_timeout(Ctx *c, int64_t polls) {
         c->launches++;
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(flag);
+    dfree(c, flag);
     if (e != cudaSuccess) return cuda_err(c, e, "timeout self-test");
     return PE_B200_OK;
 }
