@@ -193,7 +193,8 @@ int pe_b200_find_contacts(pe_b200_ctx *ctx, int64_t cap, int64_t *ids, double *g
 /* Statistics of the last step: number of contacts, number of colours (HCSITS), the L-inf
  * impulse change of the last sweep (pe's delta_max, HCSITS.h:1893-1946) and the complementarity
  * residual of the final impulses in velocity units (computed in FP64 when requested by
- * pe_b200_set_residual(ctx, 1); otherwise -1). */
+ * pe_b200_set_residual(ctx, 1); otherwise -1; a tangential impulse within 1e-9 of the friction
+ * cone, 1e-5 for FP32 impulses, counts as on the cone). */
 int pe_b200_last_step_stats(pe_b200_ctx *ctx, int64_t *ncontacts, int32_t *ncolors,
                             double *delta_max, double *residual);
 int pe_b200_set_residual(pe_b200_ctx *ctx, int32_t enabled);

@@ -1056,8 +1056,11 @@ __global__ void k_residual(int64_t nc, int64_t cap, double dtinv, Cache<T> cc, B
         const double pto = sqrt(pt * pt + po * po), gto = sqrt(gt * gt + go * go);
         const double mu = double(R[3].w);
         r = fmax(r, fmax(0.0, pto - mu * pn) * Dnn);
+        // an impulse projected onto the cone lands on it up to the rounding of the impulse's
+        // own type: FP32 impulses within 1e-5 of mu p_n count as on the cone (sliding)
+        const double on_cone = sizeof(T) == 4 ? 1e-5 : 1e-9;
         if (pn > 0.0) {
-            if (pto < mu * pn * (1.0 - 1e-9)) r = fmax(r, gto);
+            if (pto < mu * pn * (1.0 - on_cone)) r = fmax(r, gto);
             else if (pto > 0.0) r = fmax(r, gto + (pt * gt + po * go) / pto);
         }
     }
