@@ -414,9 +414,9 @@ int run_steps(Ctx *c, int32_t nsteps, double dt) {
         int rc = dem_list_graph_run(c, nsteps, dt, &k);
         if (rc) return rc;
     }
+    if (c->p.solver != PE_B200_DEM) return nbgs_run(c, nsteps - k, dt);
     for (; k < nsteps; ++k) {
-        const int rc = (c->p.solver != PE_B200_DEM) ? nbgs_step(c, dt)
-                       : (c->nl.enabled ? dem_list_step(c, dt) : dem_step(c, dt));
+        const int rc = c->nl.enabled ? dem_list_step(c, dt) : dem_step(c, dt);
         if (rc) return rc;
     }
     return PE_B200_OK;

@@ -74,6 +74,13 @@ struct NbgsBuf {
     uint64_t *used = nullptr;                 // colours used per body (bitmask)
     int32_t *flags = nullptr;                 // device counters (uncoloured, overflow, ...)
     int32_t *cstart_dev = nullptr;            // colour offsets on the device
+    // device counters of a step the host does not wait on (nbgs.cu kDd*): capacity exceeded,
+    // contacts needed, colours, largest colour, steps completed, ...
+    int32_t *dd = nullptr;
+    int32_t *h_dd = nullptr;                  // pinned mirror
+    int32_t *rem = nullptr;                   // uncoloured contacts left after each colouring round
+    unsigned int *bar2 = nullptr;             // grid barrier of the colouring rounds
+    bool on_device = false;                   // the last step's counts are only on the device
     unsigned int *bar = nullptr;              // grid barrier of the persistent sweep
     bool coop_disabled = false;
     int cluster = -1;               // CTAs of the one-cluster sweep kernel (0: not available)
@@ -362,6 +369,7 @@ int adjoint_backward(Ctx *c, const double *gx, const double *gv, const double *g
                      double *ov, double *ow, double *gpar);
 void adjoint_free(Ctx *c);
 int nbgs_step(Ctx *c, double dt);
+int nbgs_run(Ctx *c, int32_t nsteps, double dt);   // nsteps steps (retries aborted queued ones)
 int find_contacts(Ctx *c, int64_t cap, int64_t *ids, double *geom, int64_t *n_out);
 // boxes.cu: moving boxes
 int mbox_upload(Ctx *c, int32_t m, const double *x, const double *q, const double *v,

@@ -33,6 +33,18 @@ constexpr int kBlk = 256;
 constexpr int kMaxColors = 256;   // colours of one step (8 bits in the packed colour)
 constexpr size_t kBlockSmemMax = 200 * 1024;   // shared memory of the single-block sweep form
 constexpr int64_t kSerialColourMax = 8192;      // contacts coloured by one thread in one launch
+constexpr int kMaxRounds = 4096;                // rounds of the parallel colouring
+// device counters of a step (NbgsBuf.dd)
+enum : int {
+    kDdAbort = 0,    // the contacts exceeded the capacity: the rest of the call does nothing
+    kDdNeed = 1,     // the largest contact count seen
+    kDdNcolors = 2,  // colours of the step
+    kDdMaxcol = 3,   // contacts of the largest colour
+    kDdSteps = 4,    // steps completed (not aborted) since the host reset it
+    kDdNc = 5,       // contact count written by the host (scenes with moving boxes)
+    kDdSink = 6,     // error bits nobody reads (a capacity overflow that aborts instead)
+    kDdCount = 8
+};
 
 struct CountF {
     int n = 0;
@@ -320,19 +332,35 @@ __global__ void k_raw(int64_t n, VisitArgs a, const int32_t *off, int64_t cap, c
 }
 
 // ---- colouring --------------------------------------------------------------------------------
-__global__ void k_degree(int64_t nc, const int32_t *b1, const int32_t *b2, int32_t *deg) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    atomicAdd(&deg[b1[c]], 1);
-    if (b2[c] >= 0) atomicAdd(&deg[b2[c]], 1);
+// Kernels over the contacts read their count from device memory (ncp) and loop with a grid
+// stride, so a step can be queued without the host knowing the count; none runs when the
+// step was aborted for capacity (dd[kDdAbort]).
+__global__ void k_degree(const int32_t *ncp, const int32_t *dd, const int32_t *b1,
+                         const int32_t *b2, int32_t *deg) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc) {
+        atomicAdd(&deg[b1[c]], 1);
+        if (b2[c] >= 0) atomicAdd(&deg[b2[c]], 1);
+    }
 }
 
-__global__ void k_adj_fill(int64_t nc, const int32_t *b1, const int32_t *b2, int32_t *fill,
-                           int32_t *adj) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    adj[atomicAdd(&fill[b1[c]], 1)] = (int32_t)c;
-    if (b2[c] >= 0) adj[atomicAdd(&fill[b2[c]], 1)] = (int32_t)c;
+__global__ void k_adj_fill(const int32_t *ncp, const int32_t *dd, const int32_t *b1,
+                           const int32_t *b2, int32_t *fill, int32_t *adj) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc) {
+        adj[atomicAdd(&fill[b1[c]], 1)] = (int32_t)c;
+        if (b2[c] >= 0) adj[atomicAdd(&fill[b2[c]], 1)] = (int32_t)c;
+    }
+}
+
+// the capacity guard of a step queued without the host: more contacts than the buffers hold
+// abort the rest of the call (its steps leave the state as it is) and record the count
+__global__ void k_guard(const int32_t *total, int64_t cap, int32_t *dd) {
+    const int32_t t = *total;
+    if (t > cap) dd[kDdAbort] = 1;
+    if (t > dd[kDdNeed]) dd[kDdNeed] = t;
 }
 
 __device__ __forceinline__ uint32_t prio(uint32_t c) {
@@ -360,11 +388,9 @@ __device__ __forceinline__ bool beats(uint32_t c, uint32_t e) {
 // only on the contact order, not on scheduling.  W 64-bit words of settled colours per body
 // (64 W colours: 64 for spheres, whose contacts are few, 256 for scenes with boxes).
 template <int W>
-__global__ void k_color_propose(int64_t nc, const int32_t *b1, const int32_t *b2,
-                                const int32_t *color, const uint64_t *used, int32_t *tent,
-                                int32_t *err) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
+__device__ __forceinline__ void color_propose(int64_t c, const int32_t *b1, const int32_t *b2,
+                                              const int32_t *color, const uint64_t *used,
+                                              int32_t *tent, int32_t *err) {
     if (color[c] >= 0) {
         tent[c] = -1;
         return;
@@ -382,11 +408,10 @@ __global__ void k_color_propose(int64_t nc, const int32_t *b1, const int32_t *b2
 }
 
 template <int W>
-__global__ void k_color_settle(int64_t nc, int round, const int32_t *b1, const int32_t *b2,
-                               const int32_t *adj_start, const int32_t *adj, const int32_t *tent,
-                               int32_t *color, uint64_t *used, int32_t *remaining) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
+__device__ __forceinline__ void color_settle(int64_t c, int round, const int32_t *b1,
+                                             const int32_t *b2, const int32_t *adj_start,
+                                             const int32_t *adj, const int32_t *tent,
+                                             int32_t *color, uint64_t *used, int32_t *remaining) {
     const int32_t t = tent[c];
     if (t < 0) return;
     const int32_t bodies[2] = {b1[c], b2[c]};
@@ -408,6 +433,47 @@ __global__ void k_color_settle(int64_t nc, int round, const int32_t *b1, const i
         atomicOr((unsigned long long *)&used[(int64_t)bodies[1] * W + (t >> 6)], 1ull << (t & 63));
 }
 
+template <int W>
+__global__ void k_color_propose(const int32_t *ncp, const int32_t *b1, const int32_t *b2,
+                                const int32_t *color, const uint64_t *used, int32_t *tent,
+                                int32_t *err) {
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc) color_propose<W>(c, b1, b2, color, used, tent, err);
+}
+
+template <int W>
+__global__ void k_color_settle(const int32_t *ncp, int round, const int32_t *b1,
+                               const int32_t *b2, const int32_t *adj_start, const int32_t *adj,
+                               const int32_t *tent, int32_t *color, uint64_t *used,
+                               int32_t *remaining) {
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc)
+        color_settle<W>(c, round, b1, b2, adj_start, adj, tent, color, used, remaining);
+}
+
+// All rounds of the parallel colouring in one cooperative launch, for steps queued without
+// the host: rounds separated by bounded grid barriers until a round leaves no contact
+// uncoloured (rem: one counter per round, zeroed before the launch).  Does nothing when the
+// one-thread colouring handles the step (at most kSerialColourMax contacts).
+template <int W>
+__global__ void k_color_rounds(const int32_t *ncp, const int32_t *dd, const int32_t *b1,
+                               const int32_t *b2, const int32_t *adj_start, const int32_t *adj,
+                               int32_t *tent, int32_t *color, uint64_t *used, int32_t *rem,
+                               unsigned int *bar, int32_t *err) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    if (nc <= kSerialColourMax) return;
+    for (int round = 0; round < kMaxRounds; ++round) {
+        GRID_STRIDE(c, nc) color_propose<W>(c, b1, b2, color, used, tent, err);
+        if (!grid_sync(bar, err)) return;
+        GRID_STRIDE(c, nc)
+            color_settle<W>(c, round, b1, b2, adj_start, adj, tent, color, used, rem + round);
+        if (!grid_sync(bar, err)) return;
+        if (*(volatile int32_t *)(rem + round) == 0) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, DERR_COLORS);
+}
+
 // Few contacts: one thread colours them greedily in contact order (the smallest colour free at
 // both bodies), in one launch.  Where a body carries dozens of contacts (box stacks) this needs
 // about as many colours as the busiest body has contacts, the least possible, where the parallel
@@ -415,9 +481,13 @@ __global__ void k_color_settle(int64_t nc, int round, const int32_t *b1, const i
 // The used-colour masks live in shared memory when they fit (used_global == null), else in
 // the zeroed global array.
 template <int W>
-__global__ void k_color_serial(int64_t nc, const int32_t *__restrict__ b1,
-                               const int32_t *__restrict__ b2, int32_t *__restrict__ color,
-                               int64_t nbod, uint64_t *used_global, int32_t *err) {
+__global__ void k_color_serial(const int32_t *ncp, const int32_t *dd,
+                               const int32_t *__restrict__ b1, const int32_t *__restrict__ b2,
+                               int32_t *__restrict__ color, int64_t nbod, uint64_t *used_global,
+                               int32_t *err) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    if (nc > kSerialColourMax) return;   // the parallel rounds colour this step
     extern __shared__ uint64_t used_shared[];
     uint64_t *used = used_global ? used_global : used_shared;
     if (!used_global)
@@ -459,27 +529,70 @@ __global__ void k_color_serial(int64_t nc, const int32_t *__restrict__ b1,
     }
 }
 
-__global__ void k_color_hist(int64_t nc, int32_t *color, int32_t *hist, int32_t *ncolors) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    const int col = color[c] & 0xff;
-    color[c] = col;
-    atomicAdd(&hist[col], 1);
-    atomicMax(ncolors, col + 1);
+__global__ void k_color_hist(const int32_t *ncp, const int32_t *dd, int32_t *color,
+                             int32_t *hist, int32_t *ncolors) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc) {
+        const int col = color[c] & 0xff;
+        color[c] = col;
+        atomicAdd(&hist[col], 1);
+        atomicMax(ncolors, col + 1);
+    }
 }
 
-__global__ void k_color_pos(int64_t nc, const int32_t *color, int32_t *fill, int32_t *pos) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
-    pos[c] = atomicAdd(&fill[color[c]], 1);
+// colour offsets from the histogram (one block of kMaxColors threads): cstart[0..ncolors] and
+// a copy as the fill counters of k_color_pos; the colour count and the largest colour in dd
+__global__ void __launch_bounds__(kMaxColors) k_color_scan(const int32_t *hist,
+                                                           const int32_t *nco, int32_t *cstart,
+                                                           int32_t *fill, int32_t *dd) {
+    __shared__ int32_t s[kMaxColors];
+    const int ncol = *nco;
+    const int i = threadIdx.x;
+    const int32_t h = i < ncol ? hist[i] : 0;
+    s[i] = h;
+    __syncthreads();
+    // Hillis-Steele inclusive scan (256 entries)
+    for (int o = 1; o < kMaxColors; o <<= 1) {
+        const int32_t v = i >= o ? s[i - o] : 0;
+        __syncthreads();
+        s[i] += v;
+        __syncthreads();
+    }
+    const int32_t excl = s[i] - h;
+    if (i <= ncol) {
+        const int32_t start = (i == ncol) ? (ncol > 0 ? s[ncol - 1] : 0) : excl;
+        cstart[i] = start;
+        fill[i] = start;
+    }
+    __syncthreads();
+    // largest colour
+    s[i] = h;
+    __syncthreads();
+    for (int o = kMaxColors / 2; o > 0; o >>= 1) {
+        if (i < o) s[i] = max(s[i], s[i + o]);
+        __syncthreads();
+    }
+    if (i == 0) {
+        dd[kDdNcolors] = ncol;
+        dd[kDdMaxcol] = s[0];
+    }
+}
+
+__global__ void k_color_pos(const int32_t *ncp, const int32_t *dd, const int32_t *color,
+                            int32_t *fill, int32_t *pos) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc) pos[c] = atomicAdd(&fill[color[c]], 1);
 }
 
 // ---- contact cache (HCSITS.h:1767-1815) --------------------------------------------------------
 template <typename T, bool GEN>
-__global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos, BodyV<T> bv,
-                        int64_t nb, Cache<T> cc) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nc) return;
+__global__ void k_cache(const int32_t *ncp, const int32_t *dd, int64_t cap, Raw<T> raw,
+                        const int32_t *pos, BodyV<T> bv, int64_t nb, Cache<T> cc) {
+    if (dd[kDdAbort]) return;
+    const int64_t nc = *ncp;
+    GRID_STRIDE(c, nc) {
     const int64_t k = pos[c];
     const int32_t b1 = raw.b1[c], b2 = raw.b2[c];
     const V3<T> r1 = ld3c(raw.r1, c, cap), r2 = ld3c(raw.r2, c, cap), n = ld3c(raw.n, c, cap);
@@ -563,6 +676,7 @@ __global__ void k_cache(int64_t nc, int64_t cap, Raw<T> raw, const int32_t *pos,
     cc.dc[2 * k + 1] = mk4<T>(zz, T(0), T(0), T(0));
     cc.ids[k] = make_int2(b1, b2);
     cc.p[k] = mk4<T>(T(0), T(0), T(0), T(0));
+    }
     (void)nb;
 }
 
@@ -894,6 +1008,17 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     }
 }
 
+// Whether a sweep form runs for this step (decided on the device, so that a step can be queued
+// without the host knowing its colours): not after a capacity abort; gate 1 (one block) only
+// when every colour fits one block, gate 2 (the grid) only when one does not, gate 0 always.
+__device__ __forceinline__ bool sweeps_gate(const int32_t *dd, int gate) {
+    if (dd[kDdAbort]) return false;
+    const int maxcol = dd[kDdMaxcol];
+    if (gate == 1 && maxcol > kBlk) return false;
+    if (gate == 2 && maxcol <= kBlk) return false;
+    return true;
+}
+
 template <typename T, int MODEL, bool GEN = false>
 __global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int64_t cap, T dtinv,
                                                 Cache<T> cc, BodyV<T> bv, int64_t nb,
@@ -906,13 +1031,16 @@ __global__ void __launch_bounds__(kBlk) k_sweep(int64_t begin, int64_t end, int6
 // All sweeps of a step in one cooperative launch: colour after colour, separated by bounded
 // grid barriers (each colour is conflict-free, so its contacts run in parallel).
 template <typename T, int MODEL, bool GEN = false>
-__global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolors,
+__global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, const int32_t *dd,
+                                                            int gate,
                                                             const int32_t *color_start,
                                                             int64_t cap, T dtinv, Cache<T> cc,
                                                             BodyV<T> bv, int64_t nb,
                                                             int track_last,
                                                             unsigned long long *delta,
                                                             unsigned int *bar, int32_t *err) {
+    if (!sweeps_gate(dd, gate)) return;
+    const int ncolors = dd[kDdNcolors];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned int episode = 0;   // bar[0] was zeroed before the launch
@@ -933,11 +1061,13 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, int ncolo
 // stacks: dozens of contact points per box, so many colours of a few dozen contacts) spend most
 // of a sweep on the barriers; this form makes a barrier cost a few dozen cycles.
 template <typename T, int MODEL, bool GEN = false>
-__global__ void __launch_bounds__(kBlk) k_sweeps_block(int iters, int ncolors,
+__global__ void __launch_bounds__(kBlk) k_sweeps_block(int iters, const int32_t *dd, int gate,
                                                        const int32_t *color_start, int64_t cap,
                                                        T dtinv, Cache<T> cc, BodyV<T> bv,
                                                        int64_t nb, int track_last,
                                                        unsigned long long *delta) {
+    if (!sweeps_gate(dd, gate)) return;
+    const int ncolors = dd[kDdNcolors];
     for (int it = 0; it < iters; ++it) {
         const int track = (track_last && it == iters - 1) ? 1 : 0;
         for (int col = 0; col < ncolors; ++col) {
@@ -953,12 +1083,15 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_block(int iters, int ncolors,
 // the updates of one colour reach the next colour's reads at shared-memory latency.  A
 // contact's impulse is read and written by one thread only, so it stays in global memory.
 template <typename T, int MODEL, bool GEN = false>
-__global__ void __launch_bounds__(kBlk) k_sweeps_block_smem(int iters, int ncolors,
+__global__ void __launch_bounds__(kBlk) k_sweeps_block_smem(int iters, const int32_t *dd,
+                                                            int gate,
                                                             const int32_t *color_start,
                                                             int64_t cap, T dtinv, Cache<T> cc,
                                                             BodyV<T> bv, int64_t nbod,
                                                             int track_last,
                                                             unsigned long long *delta) {
+    if (!sweeps_gate(dd, gate)) return;
+    const int ncolors = dd[kDdNcolors];
     extern __shared__ __align__(16) unsigned char smem[];
     T4<T> *sh = (T4<T> *)smem;
     const int nrow = GEN ? 7 : 4;   // vr wr dv dw (ia ib ic)
@@ -1031,10 +1164,10 @@ __global__ void __launch_bounds__(kClusterBlk) k_sweeps_cluster(int iters, int n
 
 // complementarity residual of the final impulses (same definition as the oracle), in FP64
 template <typename T, bool FRICTION>
-__global__ void k_residual(int64_t nc, int64_t cap, double dtinv, Cache<T> cc, BodyV<T> bv,
-                           int64_t nb, unsigned long long *res) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nc) return;
+__global__ void k_residual(const int32_t *ncp, int64_t cap, double dtinv, Cache<T> cc,
+                           BodyV<T> bv, int64_t nb, unsigned long long *res) {
+    const int64_t nc = *ncp;
+    GRID_STRIDE(k, nc) {
     const int2 ids = cc.ids[k];
     const int32_t b1 = ids.x, b2 = ids.y;
     auto D3 = [](const T4<T> &q) { return v3(double(q.x), double(q.y), double(q.z)); };
@@ -1065,16 +1198,37 @@ __global__ void k_residual(int64_t nc, int64_t cap, double dtinv, Cache<T> cc, B
         }
     }
     atomicMax(res, (unsigned long long)__double_as_longlong(r));
+    }
 }
 
+// After a capacity abort (dd[kDdAbort]) the state is copied unchanged instead (the step does
+// nothing and is run again); otherwise thread 0 counts the step in dd[kDdSteps].
 template <typename VT, bool TRACKQ>
 __global__ void k_integrate(int64_t n, double dt, double drag, int has_drag, BodyV<VT> bv,
-                            const SceneInfo *scenes, const double4 *pr, const uint32_t *tag,
-                            const int32_t *uid, const double4 *q, double4 *pr_o, VT *vw_o,
-                            uint32_t *tag_o, int32_t *uid_o, double4 *q_o, int32_t *key,
-                            int32_t *rank, int32_t *cell_count, int32_t *err) {
+                            const SceneInfo *scenes, const double4 *pr, const VT *vw,
+                            const uint32_t *tag, const int32_t *uid, const double4 *q,
+                            double4 *pr_o, VT *vw_o, uint32_t *tag_o, int32_t *uid_o,
+                            double4 *q_o, int32_t *key, int32_t *rank, int32_t *cell_count,
+                            int32_t *dd, int32_t *err) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
+    if (dd[kDdAbort]) {
+        const double4 p = pr[t];
+        pr_o[t] = p;
+        cp_vw(vw_o, t, vw, t, n);
+        const uint32_t tg = tag[t];
+        tag_o[t] = tg;
+        uid_o[t] = uid[t];
+        if (TRACKQ) q_o[t] = q[t];
+        const SceneInfo &s = scenes[tg >> 16];
+        int cx, cy, cz;
+        cell_coords(s, p.x, p.y, p.z, cx, cy, cz);
+        const int32_t kk = (int32_t)cell_key(s, cx, cy, cz);
+        key[t] = kk;
+        rank[t] = atomicAdd(&cell_count[kk], 1);
+        return;
+    }
+    if (t == 0) dd[kDdSteps] += 1;
     V3<VT> v = xyz<VT>(bv.vr[t]) + xyz<VT>(bv.dv[t]);
     V3<VT> w = xyz<VT>(bv.wr[t]) + xyz<VT>(bv.dw[t]);
     const double4 p = pr[t];
@@ -1152,12 +1306,19 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         dfree(c, b.red);
         dfree(c, b.cstart_dev);
         dfree(c, b.bar);
+        dfree(c, b.dd);
+        dfree(c, b.rem);
+        dfree(c, b.bar2);
         if (b.color_start) cudaFreeHost(b.color_start);
+        if (b.h_dd) cudaFreeHost(b.h_dd);
         b.flags = nullptr;
         b.red = nullptr;
         b.cstart_dev = nullptr;
         b.bar = nullptr;
+        b.dd = b.rem = nullptr;
+        b.bar2 = nullptr;
         b.color_start = nullptr;
+        b.h_dd = nullptr;
     }
     if (!b.cnt) {
         b.nbod = nbod;
@@ -1166,12 +1327,19 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         PEB_CUDA(c, dmalloc(c, &b.body_cnt, ((size_t)nbod + 2) * sizeof(int32_t)));
         PEB_CUDA(c, dmalloc(c, &b.used, (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t)));
         PEB_CUDA(c, dmalloc(c, &b.vel, (size_t)nbod * (gen ? 28 : 16) * es));
-        PEB_CUDA(c, dmalloc(c, &b.flags, 2 * kMaxColors * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.flags, (3 * kMaxColors + 8) * sizeof(int32_t)));
         PEB_CUDA(c, cudaMallocHost(&b.color_start, (2 * kMaxColors + 8) * sizeof(int32_t)));
         PEB_CUDA(c, dmalloc(c, &b.red, 4 * sizeof(double)));
         PEB_CUDA(c, dmalloc(c, &b.cstart_dev, (kMaxColors + 2) * sizeof(int32_t)));
         PEB_CUDA(c, dmalloc(c, &b.bar, 2 * sizeof(unsigned int)));
         PEB_CUDA(c, cudaMemsetAsync(b.bar, 0, 2 * sizeof(unsigned int), c->stream));
+        PEB_CUDA(c, dmalloc(c, &b.dd, kDdCount * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMemsetAsync(b.dd, 0, kDdCount * sizeof(int32_t), c->stream));
+        PEB_CUDA(c, cudaMallocHost(&b.h_dd, kDdCount * sizeof(int32_t)));
+        memset(b.h_dd, 0, kDdCount * sizeof(int32_t));
+        PEB_CUDA(c, dmalloc(c, &b.rem, kMaxRounds * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.bar2, 2 * sizeof(unsigned int)));
+        PEB_CUDA(c, cudaMemsetAsync(b.bar2, 0, 2 * sizeof(unsigned int), c->stream));
     }
     return PE_B200_OK;
 }
@@ -1364,8 +1532,96 @@ int sweeps_in_cluster(Ctx *c, int model, int iters, int ncolors, int maxcol, int
     return PE_B200_OK;
 }
 
+// The colouring rounds of a queued step in one cooperative launch (k_color_rounds); a grid of
+// as many blocks as fit, at most one thread per contact of the capacity.
 template <typename VT>
-int nbgs_step_t(Ctx *c, double dt) {
+int launch_color_rounds(Ctx *c, const int32_t *ncp, int32_t *dd, const Raw<VT> &raw,
+                        int64_t cap) {
+    NbgsBuf &nb = c->nb;
+    static int occ = 0;
+    if (occ == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_color_rounds<1>, kBlk,
+                                                                  0) != cudaSuccess)
+        occ = 1;
+    const unsigned grid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((int64_t)std::max(occ, 1) * c->sm_count, (cap + kBlk - 1) / kBlk));
+    int32_t *tent = nb.order;   // free until the colour sort
+    const int32_t *b1 = raw.b1, *b2 = raw.b2, *adj_start = nb.body_cnt, *adj = nb.body_adj;
+    int32_t *color = nb.color, *rem = nb.rem, *err = c->d_err;
+    uint64_t *used = nb.used;
+    unsigned int *bar = nb.bar2;
+    void *args[] = {&ncp, &dd, &b1, &b2, &adj_start, &adj, &tent, &color, &used, &rem, &bar, &err};
+    PEB_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_color_rounds<1>, dim3(grid),
+                                            dim3(kBlk), args, 0, c->stream));
+    c->launches++;
+    return PE_B200_OK;
+}
+
+// The sweeps of a queued step: the single-block form and the grid form are both launched and
+// each runs only for the case it serves (sweeps_gate: every colour fits one block, or not).
+// The grid form's size follows the largest colour of an earlier step (any size is correct:
+// its blocks stride over a colour's contacts).
+template <typename VT>
+int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT dtinv,
+                         const Cache<VT> &cc, const BodyV<VT> &bv, int64_t n,
+                         unsigned long long *dl) {
+    NbgsBuf &nb = c->nb;
+    int32_t *dd = nb.dd;
+    const size_t smem = (size_t)(gen ? 7 : 4) * nb.nbod * sizeof(T4<VT>);
+    bool smem_ok = smem <= kBlockSmemMax;
+    if (smem_ok) {
+        auto kern = block_smem_kernel<VT>(model, gen);
+        smem_ok = cudaFuncSetAttribute((const void *)kern,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBlockSmemMax) == cudaSuccess;
+        if (smem_ok) {
+            kern<<<1, kBlk, smem, c->stream>>>(iters, dd, 1, nb.cstart_dev, cap, dtinv, cc, bv,
+                                               nb.nbod, 0, dl);
+            PEB_LAUNCHED(c);
+        } else {
+            cudaGetLastError();
+        }
+    }
+    if (!smem_ok) {
+        block_kernel<VT>(model, gen)<<<1, kBlk, 0, c->stream>>>(iters, dd, 1, nb.cstart_dev, cap,
+                                                                dtinv, cc, bv, n, 0, dl);
+        PEB_LAUNCHED(c);
+    }
+    auto kern = persistent_kernel<VT>(model, gen);
+    int occ = 0;
+    PEB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0));
+    // the largest colour of the last step whose counts reached the host, else one block per
+    // 4096 contacts of the capacity
+    const int64_t maxcol = nb.h_dd[kDdMaxcol] > 0 ? nb.h_dd[kDdMaxcol] : cap / 16;
+    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)std::max(occ, 1) * c->sm_count,
+                                                      std::max<int64_t>(1, (maxcol + kBlk - 1) / kBlk));
+    // the barrier counter counts iters x colours x blocks arrivals: past 2^32 (kMaxColors
+    // colours at most) the grid shrinks
+    const unsigned g = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(grid, (int64_t)(4.0e9 / ((double)std::max(iters, 1) * kMaxColors))));
+    PEB_CUDA(c, cudaMemsetAsync(nb.bar, 0, sizeof(unsigned int), c->stream));
+    int iters_a = iters, gate_a = 2, track_a = 0;
+    int64_t cap_a = cap, n_a = n;
+    VT dtinv_a = dtinv;
+    int32_t *cs = nb.cstart_dev;
+    Cache<VT> cc_a = cc;
+    BodyV<VT> bv_a = bv;
+    void *args[] = {&iters_a, &dd, &gate_a, &cs, &cap_a, &dtinv_a, &cc_a, &bv_a, &n_a, &track_a,
+                    &dl, &nb.bar, &c->d_err};
+    PEB_CUDA(c, cudaLaunchCooperativeKernel((const void *)kern, dim3(g), dim3(kBlk), args, 0,
+                                            c->stream));
+    c->launches++;
+    return PE_B200_OK;
+}
+
+// One hard-contact step: sort, permute, detect, colour, cache, sweep, integrate.
+// queued: the step is queued without the host waiting on the device (sphere scenes without a
+// residual request, automatic/grid/single-block sweep forms): the contact count stays on the
+// device (a count beyond the capacity aborts the rest of the call, which nbgs_run repeats after
+// growing the buffers), the colouring runs its rounds in one cooperative launch, and the sweep
+// form is chosen on the device from the largest colour.  Otherwise the host reads the counts
+// (moving boxes need them for their own kernels; per-colour launches need the colour offsets).
+template <typename VT>
+int nbgs_step_t(Ctx *c, double dt, bool queued) {
     NbgsBuf &nb = c->nb;
     const int64_t n = c->n;
     // moving boxes: bodies n .. n+m-1 with full inverse inertias (FP64 only, checked by the
@@ -1375,6 +1631,7 @@ int nbgs_step_t(Ctx *c, double dt) {
     const int64_t auto_cap = c->p.max_contacts > 0 ? c->p.max_contacts : std::max<int64_t>(8 * nbod, 1024);
     int rc = nbgs_alloc(c, auto_cap);
     if (rc) return rc;
+    nb.on_device = queued;
     // 1. sort, permute to slot order, body cache
     if (n > 0) {
         if (!c->binned) {
@@ -1414,113 +1671,154 @@ int nbgs_step_t(Ctx *c, double dt) {
     // the contacts of the moving boxes follow the spheres' contacts
     VisitArgs va = visit_args(c, nullptr);
     prof_begin(c, ST_DETECT);
-    int32_t total = 0, total_s = 0, total_b = 0;
-    if (n > 0) {
-        k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
+    int64_t nc = 0;                 // the count (host-known steps only)
+    int32_t total_s = 0;            // sphere contacts (host-known steps only)
+    int32_t *dd = nb.dd;
+    const int32_t *ncp = dd + kDdNc;   // the count on the device
+    if (queued) {
+        if (n > 0) {
+            k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
+            PEB_LAUNCHED(c);
+            rc = scan_exclusive(c, nb.cnt, nb.cnt, n);
+            if (rc) return rc;
+            PEB_CUDA(c, cudaMemcpyAsync(dd + kDdNc, nb.cnt + n, sizeof(int32_t),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+        } else {
+            PEB_CUDA(c, cudaMemsetAsync(dd + kDdNc, 0, sizeof(int32_t), c->stream));
+        }
+        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.cap, dd);
         PEB_LAUNCHED(c);
-        rc = scan_exclusive(c, nb.cnt, nb.cnt, n);
-        if (rc) return rc;
-        PEB_CUDA(c, cudaMemcpyAsync(&total_s, nb.cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    } else {
+        int32_t total_b = 0;
+        if (n > 0) {
+            k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
+            PEB_LAUNCHED(c);
+            rc = scan_exclusive(c, nb.cnt, nb.cnt, n);
+            if (rc) return rc;
+            PEB_CUDA(c, cudaMemcpyAsync(&total_s, nb.cnt + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+            PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+        }
+        if (gen) {
+            rc = mbox_hc_count(c, &total_b);
+            if (rc) return rc;
+        }
+        if ((int64_t)total_s + total_b > INT32_MAX)
+            return set_err(c, PE_B200_ERR_CAPACITY, "contact count exceeds int32");
+        const int32_t total = total_s + total_b;
+        if (total > nb.cap) {
+            if (c->p.max_contacts > 0)
+                return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
+            rc = nbgs_alloc(c, (int64_t)total * 5 / 4 + 1024);
+            if (rc) return rc;
+            layout(c, raw, cc, bv);
+            dd = nb.dd;
+        }
+        nc = total;
+        // the kernels read the count from the device
+        nb.h_dd[kDdNc] = total;
+        PEB_CUDA(c, cudaMemcpyAsync(dd + kDdNc, nb.h_dd + kDdNc, sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, c->stream));
+        c->last_ncontacts = nc;
     }
-    if (gen) {
-        rc = mbox_hc_count(c, &total_b);
-        if (rc) return rc;
-    }
-    if ((int64_t)total_s + total_b > INT32_MAX)
-        return set_err(c, PE_B200_ERR_CAPACITY, "contact count exceeds int32");
-    total = total_s + total_b;
-    if (total > nb.cap) {
-        if (c->p.max_contacts > 0)
-            return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
-        rc = nbgs_alloc(c, (int64_t)total * 5 / 4 + 1024);
-        if (rc) return rc;
-        layout(c, raw, cc, bv);
-    }
-    const int64_t nc = total;
     const int64_t cap = nb.cap;
-    c->last_ncontacts = nc;
     if (n > 0) {
+        // a queued step's overflow aborts it instead of reporting an error
         k_raw<VT><<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt, cap, (const VT *)c->cur.vw,
                                                              c->d_mats, c->d_plane_mat, c->d_box_mat,
-                                                             c->p.erp, raw, c->d_err);
+                                                             c->p.erp, raw, queued ? dd + kDdSink : c->d_err);
         PEB_LAUNCHED(c);
     }
     if constexpr (std::is_same<VT, double>::value) {
         if (gen) {
-            rc = mbox_hc_raw(c, total_s, cap, raw.b1, raw.b2, raw.r1, raw.r2, raw.n, raw.dist, raw.mu);
+            rc = mbox_hc_raw(c, total_s, cap, raw.b1, raw.b2, raw.r1, raw.r2, raw.n, raw.dist,
+                             raw.mu);
             if (rc) return rc;
         }
     }
     prof_end(c, ST_DETECT);
+    const unsigned cgrid = capped_grid(c, cap, kBlk);   // kernels over the contacts
     // 3. colouring
     int32_t ncolors = 0;
-    if (nc > 0) {
+    const bool any = queued || nc > 0;
+    if (any) {
         prof_begin(c, ST_COLOR);
         PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)nbod + 1) * sizeof(int32_t), c->stream));
-        k_degree<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, raw.b1, raw.b2, nb.body_cnt);
+        k_degree<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, raw.b1, raw.b2, nb.body_cnt);
         PEB_LAUNCHED(c);
         rc = scan_exclusive(c, nb.body_cnt, nb.body_cnt, nbod);
         if (rc) return rc;
         int32_t *fill = nb.cnt;  // reuse: counts are consumed
         PEB_CUDA(c, cudaMemcpyAsync(fill, nb.body_cnt, ((size_t)nbod + 1) * sizeof(int32_t),
                                     cudaMemcpyDeviceToDevice, c->stream));
-        k_adj_fill<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, raw.b1, raw.b2, fill, nb.body_adj);
+        k_adj_fill<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, raw.b1, raw.b2, fill, nb.body_adj);
         PEB_LAUNCHED(c);
-        PEB_CUDA(c, cudaMemsetAsync(nb.color, 0xff, (size_t)nc * sizeof(int32_t), c->stream));
+        PEB_CUDA(c, cudaMemsetAsync(nb.color, 0xff, (size_t)(queued ? cap : nc) * sizeof(int32_t), c->stream));
         const int words = gen ? 4 : 1;
         PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)nbod * words * sizeof(uint64_t), c->stream));
-        int round = 0;
-        if (nc <= kSerialColourMax) {
-            const size_t masks = (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t);
-            const bool in_smem = masks <= 48 * 1024;
-            (gen ? k_color_serial<4> : k_color_serial<1>)<<<1, 256, in_smem ? masks : 0, c->stream>>>(
-                nc, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used, c->d_err);
+        const size_t masks = (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t);
+        const bool in_smem = masks <= 48 * 1024;
+        if (queued) {
+            // one thread for a few contacts; otherwise every round in one cooperative launch
+            k_color_serial<1><<<1, 256, in_smem ? masks : 0, c->stream>>>(
+                ncp, dd, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used, c->d_err);
             PEB_LAUNCHED(c);
-        }
-        for (; nc > kSerialColourMax;) {
-            const int batch = 8;
-            PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, batch * sizeof(int32_t), c->stream));
-            int32_t *tent = nb.order;   // free until the colour sort below
-            for (int k = 0; k < batch; ++k, ++round) {
-                (gen ? k_color_propose<4> : k_color_propose<1>)<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(
-                    nc, raw.b1, raw.b2, nb.color, nb.used, tent, c->d_err);
-                PEB_LAUNCHED(c);
-                (gen ? k_color_settle<4> : k_color_settle<1>)<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(
-                    nc, round, raw.b1, raw.b2, nb.body_cnt, nb.body_adj, tent, nb.color, nb.used,
-                    nb.flags + k);
+            PEB_CUDA(c, cudaMemsetAsync(nb.rem, 0, kMaxRounds * sizeof(int32_t), c->stream));
+            rc = launch_color_rounds(c, ncp, dd, raw, cap);
+            if (rc) return rc;
+        } else {
+            int round = 0;
+            if (nc <= kSerialColourMax) {
+                (gen ? k_color_serial<4> : k_color_serial<1>)<<<1, 256, in_smem ? masks : 0, c->stream>>>(
+                    ncp, dd, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used, c->d_err);
                 PEB_LAUNCHED(c);
             }
-            int32_t rem[8];
-            PEB_CUDA(c, cudaMemcpyAsync(rem, nb.flags, sizeof rem, cudaMemcpyDeviceToHost, c->stream));
-            PEB_CUDA(c, cudaStreamSynchronize(c->stream));
-            if (rem[batch - 1] == 0) break;
-            if (round > 4096) return set_err(c, PE_B200_ERR_TIMEOUT, "colouring did not finish");
+            for (; nc > kSerialColourMax;) {
+                const int batch = 8;
+                PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, batch * sizeof(int32_t), c->stream));
+                int32_t *tent = nb.order;   // free until the colour sort below
+                for (int k = 0; k < batch; ++k, ++round) {
+                    (gen ? k_color_propose<4> : k_color_propose<1>)<<<cgrid, kBlk, 0, c->stream>>>(
+                        ncp, raw.b1, raw.b2, nb.color, nb.used, tent, c->d_err);
+                    PEB_LAUNCHED(c);
+                    (gen ? k_color_settle<4> : k_color_settle<1>)<<<cgrid, kBlk, 0, c->stream>>>(
+                        ncp, round, raw.b1, raw.b2, nb.body_cnt, nb.body_adj, tent, nb.color, nb.used,
+                        nb.flags + k);
+                    PEB_LAUNCHED(c);
+                }
+                int32_t rem[8];
+                PEB_CUDA(c, cudaMemcpyAsync(rem, nb.flags, sizeof rem, cudaMemcpyDeviceToHost, c->stream));
+                PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+                if (rem[batch - 1] == 0) break;
+                if (round > kMaxRounds) return set_err(c, PE_B200_ERR_TIMEOUT, "colouring did not finish");
+            }
         }
-        // counting sort by colour
+        // counting sort by colour: histogram, offsets on the device
         PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, 2 * kMaxColors * sizeof(int32_t), c->stream));
         int32_t *hist = nb.flags, *nco = nb.flags + kMaxColors;
-        k_color_hist<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, nb.color, hist, nco);
+        k_color_hist<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, nb.color, hist, nco);
         PEB_LAUNCHED(c);
-        PEB_CUDA(c, cudaMemcpyAsync(nb.color_start, nb.flags, (kMaxColors + 2) * sizeof(int32_t),
-                                    cudaMemcpyDeviceToHost, c->stream));
-        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
-        ncolors = nb.color_start[kMaxColors];
-        std::vector<int32_t> start(ncolors + 1, 0);
-        for (int k = 0; k < ncolors; ++k) start[k + 1] = start[k] + nb.color_start[k];
-        for (int k = 0; k <= ncolors; ++k) nb.color_start[k] = start[k];
-        PEB_CUDA(c, cudaMemcpyAsync(nb.flags, start.data(), (ncolors + 1) * sizeof(int32_t),
-                                    cudaMemcpyHostToDevice, c->stream));
-        k_color_pos<<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, nb.color, nb.flags, nb.order);
+        int32_t *cfill = nb.flags + 2 * kMaxColors;   // the colour offsets as fill counters
+        k_color_scan<<<1, kMaxColors, 0, c->stream>>>(hist, nco, nb.cstart_dev, cfill, dd);
+        PEB_LAUNCHED(c);
+        if (!queued) {
+            // the host-driven forms need the offsets on the host
+            PEB_CUDA(c, cudaMemcpyAsync(nb.color_start, nb.cstart_dev, (kMaxColors + 1) * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            PEB_CUDA(c, cudaMemcpyAsync(nb.h_dd, dd, kDdCount * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+            ncolors = nb.h_dd[kDdNcolors];
+        }
+        k_color_pos<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, nb.color, cfill, nb.order);
         PEB_LAUNCHED(c);
         prof_end(c, ST_COLOR);
         prof_begin(c, ST_CACHE);
         // 4. contact cache in colour-sorted order
         if constexpr (std::is_same<VT, double>::value) {
-            if (gen) k_cache<VT, true><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
-            else k_cache<VT, false><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+            if (gen) k_cache<VT, true><<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, cap, raw, nb.order, bv, n, cc);
+            else k_cache<VT, false><<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, cap, raw, nb.order, bv, n, cc);
         } else {
-            k_cache<VT, false><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, raw, nb.order, bv, n, cc);
+            k_cache<VT, false><<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, cap, raw, nb.order, bv, n, cc);
         }
         PEB_LAUNCHED(c);
         prof_end(c, ST_CACHE);
@@ -1532,7 +1830,12 @@ int nbgs_step_t(Ctx *c, double dt) {
     const int iters = c->p.max_iterations;
     unsigned long long *dl = (unsigned long long *)nb.red;
     if (c->want_residual) PEB_CUDA(c, cudaMemsetAsync(nb.red, 0, 2 * sizeof(double), c->stream));
-    if (nc > 0) {
+    if (queued && iters > 0) {
+        prof_begin(c, ST_SWEEP);
+        rc = launch_sweeps_queued<VT>(c, model, gen, iters, cap, VT(1.0 / dt), cc, bv, n, dl);
+        if (rc) return rc;
+        prof_end(c, ST_SWEEP);
+    } else if (!queued && nc > 0) {
         prof_begin(c, ST_SWEEP);
         bool done = iters == 0;
         int maxcol = 1;
@@ -1549,9 +1852,6 @@ int nbgs_step_t(Ctx *c, double dt) {
         if (!done && (mode == 0 || mode == 4) && maxcol <= kBlk) {
             // every colour fits one block: all sweeps in one block, colours separated by
             // __syncthreads (automatic, or asked for with 4)
-            PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start,
-                                        (ncolors + 1) * sizeof(int32_t), cudaMemcpyHostToDevice,
-                                        c->stream));
             const size_t smem = (size_t)(gen ? 7 : 4) * nb.nbod * sizeof(T4<VT>);
             bool smem_ok = smem <= kBlockSmemMax;
             if (smem_ok) {
@@ -1561,7 +1861,7 @@ int nbgs_step_t(Ctx *c, double dt) {
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)kBlockSmemMax) == cudaSuccess;
                 if (smem_ok) {
-                    kern<<<1, kBlk, smem, c->stream>>>(iters, ncolors, nb.cstart_dev, cap,
+                    kern<<<1, kBlk, smem, c->stream>>>(iters, dd, 0, nb.cstart_dev, cap,
                                                        VT(1.0 / dt), cc, bv, nb.nbod,
                                                        c->want_residual ? 1 : 0, dl);
                     PEB_LAUNCHED(c);
@@ -1571,7 +1871,7 @@ int nbgs_step_t(Ctx *c, double dt) {
             }
             if (!smem_ok) {
                 block_kernel<VT>(model, gen)<<<1, kBlk, 0, c->stream>>>(
-                    iters, ncolors, nb.cstart_dev, cap, VT(1.0 / dt), cc, bv, n,
+                    iters, dd, 0, nb.cstart_dev, cap, VT(1.0 / dt), cc, bv, n,
                     c->want_residual ? 1 : 0, dl);
                 PEB_LAUNCHED(c);
             }
@@ -1589,17 +1889,14 @@ int nbgs_step_t(Ctx *c, double dt) {
             // 2^32 the colours are launched one by one instead
             const bool fits = (double)iters * ncolors * grid < 4.0e9;
             if (e == cudaSuccess && occ > 0 && fits) {
-                PEB_CUDA(c, cudaMemcpyAsync(nb.cstart_dev, nb.color_start,
-                                            (ncolors + 1) * sizeof(int32_t),
-                                            cudaMemcpyHostToDevice, c->stream));
-                // the barrier counter of this launch starts at zero (its episodes count up);
-                // iters x colours x blocks stays far below 2^32
+                // the barrier counter of this launch starts at zero (its episodes count up)
                 PEB_CUDA(c, cudaMemsetAsync(nb.bar, 0, sizeof(unsigned int), c->stream));
-                int iters_a = iters, ncol_a = ncolors, track_a = c->want_residual ? 1 : 0;
+                int iters_a = iters, gate_a = 0, track_a = c->want_residual ? 1 : 0;
                 int64_t cap_a = cap, n_a = n;
                 VT dtinv_a = VT(1.0 / dt);
                 int32_t *cs = nb.cstart_dev;
-                void *args[] = {&iters_a, &ncol_a, &cs, &cap_a, &dtinv_a, &cc, &bv, &n_a,
+                int32_t *dd_a = dd;
+                void *args[] = {&iters_a, &dd_a, &gate_a, &cs, &cap_a, &dtinv_a, &cc, &bv, &n_a,
                                 &track_a, &dl, &nb.bar, &c->d_err};
                 e = cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(kBlk), args, 0,
                                                 c->stream);
@@ -1623,13 +1920,13 @@ int nbgs_step_t(Ctx *c, double dt) {
             }
         }
         prof_end(c, ST_SWEEP);
-        if (c->want_residual) {
-            if (fr)
-                k_residual<VT, true><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, 1.0 / dt, cc, bv, n, dl + 1);
-            else
-                k_residual<VT, false><<<grid_for(nc, kBlk), kBlk, 0, c->stream>>>(nc, cap, 1.0 / dt, cc, bv, n, dl + 1);
-            PEB_LAUNCHED(c);
-        }
+    }
+    if (c->want_residual && any) {
+        if (fr)
+            k_residual<VT, true><<<cgrid, kBlk, 0, c->stream>>>(ncp, cap, 1.0 / dt, cc, bv, n, dl + 1);
+        else
+            k_residual<VT, false><<<cgrid, kBlk, 0, c->stream>>>(ncp, cap, 1.0 / dt, cc, bv, n, dl + 1);
+        PEB_LAUNCHED(c);
     }
     // 6. integrate into the other buffer and bin for the next step
     {
@@ -1640,9 +1937,9 @@ int nbgs_step_t(Ctx *c, double dt) {
         auto kern = tq ? k_integrate<VT, true> : k_integrate<VT, false>;
         if (n > 0) {
             kern<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(
-                n, dt, drag, has_drag, bv, c->d_scenes, c->cur.pr, c->cur.tag, c->cur.uid, c->cur.q,
-                c->nxt.pr, (VT *)c->nxt.vw, c->nxt.tag, c->nxt.uid, c->nxt.q, c->key, c->rank,
-                c->cell_count, c->d_err);
+                n, dt, drag, has_drag, bv, c->d_scenes, c->cur.pr, (const VT *)c->cur.vw,
+                c->cur.tag, c->cur.uid, c->cur.q, c->nxt.pr, (VT *)c->nxt.vw, c->nxt.tag,
+                c->nxt.uid, c->nxt.q, c->key, c->rank, c->cell_count, dd, c->d_err);
             PEB_LAUNCHED(c);
         }
         if (gen) {
@@ -1681,13 +1978,69 @@ void nbgs_free(Ctx *c) {
     dfree(c, b.red);
     dfree(c, b.cstart_dev);
     dfree(c, b.bar);
+    dfree(c, b.dd);
+    dfree(c, b.rem);
+    dfree(c, b.bar2);
     if (b.color_start) cudaFreeHost(b.color_start);
+    if (b.h_dd) cudaFreeHost(b.h_dd);
     b = NbgsBuf();
 }
 
+namespace {
+
+// whether the hard-contact steps of this context are queued without host waits
+bool nbgs_queued(const Ctx *c) {
+    const int mode = c->tune.nbgs_sweeps;
+    return c->mb.m == 0 && !c->want_residual && (mode == 0 || mode == 2 || mode == 4);
+}
+
+}  // namespace
+
 int nbgs_step(Ctx *c, double dt) {
     if (c->n == 0 && c->mb.m == 0) return PE_B200_OK;
-    return (c->p.precision == PE_B200_FP64) ? nbgs_step_t<double>(c, dt) : nbgs_step_t<float>(c, dt);
+    const bool q = nbgs_queued(c);
+    return (c->p.precision == PE_B200_FP64) ? nbgs_step_t<double>(c, dt, q)
+                                            : nbgs_step_t<float>(c, dt, q);
+}
+
+// nsteps hard-contact steps.  Queued steps are checked once at the end: if some step found
+// more contacts than the buffers hold, it and every later step of the call left the state as
+// it was; the buffers grow to the count seen and those steps run again.
+int nbgs_run(Ctx *c, int32_t nsteps, double dt) {
+    if (c->n == 0 && c->mb.m == 0) return PE_B200_OK;
+    if (!nbgs_queued(c)) {
+        for (int32_t k = 0; k < nsteps; ++k) {
+            const int rc = nbgs_step(c, dt);
+            if (rc) return rc;
+        }
+        return PE_B200_OK;
+    }
+    int32_t left = nsteps;
+    for (int attempt = 0; left > 0; ++attempt) {
+        if (c->nb.dd) PEB_CUDA(c, cudaMemsetAsync(c->nb.dd + kDdSteps, 0, sizeof(int32_t), c->stream));
+        for (int32_t k = 0; k < left; ++k) {
+            const int rc = nbgs_step(c, dt);
+            if (rc) return rc;
+        }
+        NbgsBuf &nb = c->nb;
+        PEB_CUDA(c, cudaMemcpyAsync(nb.h_dd, nb.dd, kDdCount * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->last_ncontacts = nb.h_dd[kDdNc];
+        c->last_ncolors = nb.h_dd[kDdNcolors];
+        if (!nb.h_dd[kDdAbort]) break;
+        const int32_t done = nb.h_dd[kDdSteps];
+        if (c->p.max_contacts > 0)
+            return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
+        if (attempt >= 8) return set_err(c, PE_B200_ERR_CAPACITY, "contact buffers kept overflowing");
+        const int64_t need = nb.h_dd[kDdNeed];
+        int rc = nbgs_alloc(c, need + need / 4 + 1024);
+        if (rc) return rc;
+        PEB_CUDA(c, cudaMemsetAsync(nb.dd + kDdAbort, 0, sizeof(int32_t), c->stream));
+        nb.h_dd[kDdAbort] = 0;
+        left -= done;
+    }
+    return PE_B200_OK;
 }
 
 const int2 *nbgs_ids_ptr(Ctx *c) {

@@ -41,6 +41,12 @@ int validate_coloring(Ctx *c, int64_t *bad) {
     if (nc <= 0 || ncol <= 0 || !nb.cache || !nb.color_start) return PE_B200_OK;
     std::vector<int32_t> ids(2 * nc);
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    // a queued step left its colour offsets on the device only
+    if (nb.on_device && nb.cstart_dev) {
+        PEB_CUDA(c, cudaMemcpyAsync(nb.color_start, nb.cstart_dev, (ncol + 1) * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        PEB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
     PEB_CUDA(c, cudaMemcpyAsync(ids.data(), nbgs_ids_ptr(c), nc * sizeof(int2), cudaMemcpyDeviceToHost, c->stream));
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     *bad += coloring_problems(c->n + c->mb.m, nc, ids.data(), ncol, nb.color_start);
