@@ -803,7 +803,7 @@ int pe_b200_set_graph_steps(pe_b200_ctx *h, int32_t steps) {
 
 int pe_b200_graph_active(const pe_b200_ctx *h) {
     const Ctx *c = reinterpret_cast<const Ctx *>(h);
-    return (c && c->sg.exec && !c->sg.failed) ? 1 : 0;
+    return (c && ((c->sg.exec && !c->sg.failed) || (c->nb.gexec && !c->nb.gfailed))) ? 1 : 0;
 }
 
 int pe_b200_get_tuning(pe_b200_ctx *h, pe_b200_tuning *out) {

@@ -81,6 +81,15 @@ struct NbgsBuf {
     int32_t *rem = nullptr;                   // uncoloured contacts left after each colouring round
     unsigned int *bar2 = nullptr;             // grid barrier of the colouring rounds
     bool on_device = false;                   // the last step's counts are only on the device
+    bool plan_none = false;                   // queued steps planned without contacts
+    bool warm = false;                        // a queued step has run on these buffers
+    // a captured CUDA graph of `gsteps` queued steps, valid for the buffers, settings and
+    // sweep grid in gkey (nbgs.cu nbgs_run)
+    cudaGraphExec_t gexec = nullptr;
+    int32_t gsteps = 0;
+    int64_t glaunches = 0;
+    bool gfailed = false;
+    uint64_t gkey[12] = {};
     unsigned int *bar = nullptr;              // grid barrier of the persistent sweep
     bool coop_disabled = false;
     int cluster = -1;               // CTAs of the one-cluster sweep kernel (0: not available)

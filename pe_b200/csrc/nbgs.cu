@@ -355,11 +355,12 @@ __global__ void k_adj_fill(const int32_t *ncp, const int32_t *dd, const int32_t 
     }
 }
 
-// the capacity guard of a step queued without the host: more contacts than the buffers hold
-// abort the rest of the call (its steps leave the state as it is) and record the count
-__global__ void k_guard(const int32_t *total, int64_t cap, int32_t *dd) {
+// the guard of a step queued without the host: more contacts than the step was planned for
+// (the buffers' capacity, or none for a step planned without contacts) abort the rest of the
+// call (its steps leave the state as it is); the largest count is recorded
+__global__ void k_guard(const int32_t *total, int64_t limit, int32_t *dd) {
     const int32_t t = *total;
-    if (t > cap) dd[kDdAbort] = 1;
+    if (t > limit) dd[kDdAbort] = 1;
     if (t > dd[kDdNeed]) dd[kDdNeed] = t;
 }
 
@@ -1556,6 +1557,18 @@ int launch_color_rounds(Ctx *c, const int32_t *ncp, int32_t *dd, const Raw<VT> &
     return PE_B200_OK;
 }
 
+// Blocks of the grid sweep form of queued steps: enough for the largest colour of the last step
+// whose counts reached the host (one block per 4096 contacts of the capacity before any did),
+// rounded up to a power of two so that a captured graph of steps stays valid while that colour
+// changes little.
+inline int64_t queued_sweep_blocks(const Ctx *c) {
+    const NbgsBuf &nb = c->nb;
+    const int64_t maxcol = nb.h_dd && nb.h_dd[kDdMaxcol] > 0 ? nb.h_dd[kDdMaxcol] : nb.cap / 16;
+    int64_t b = 1;
+    while (b * kBlk < maxcol) b <<= 1;
+    return b;
+}
+
 // The sweeps of a queued step: the single-block form and the grid form are both launched and
 // each runs only for the case it serves (sweeps_gate: every colour fits one block, or not).
 // The grid form's size follows the largest colour of an earlier step (any size is correct:
@@ -1591,9 +1604,8 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
     PEB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, 0));
     // the largest colour of the last step whose counts reached the host, else one block per
     // 4096 contacts of the capacity
-    const int64_t maxcol = nb.h_dd[kDdMaxcol] > 0 ? nb.h_dd[kDdMaxcol] : cap / 16;
     const unsigned grid = (unsigned)std::min<int64_t>((int64_t)std::max(occ, 1) * c->sm_count,
-                                                      std::max<int64_t>(1, (maxcol + kBlk - 1) / kBlk));
+                                                      queued_sweep_blocks(c));
     // the barrier counter counts iters x colours x blocks arrivals: past 2^32 (kMaxColors
     // colours at most) the grid shrinks
     const unsigned g = (unsigned)std::max<int64_t>(
@@ -1686,7 +1698,8 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
         } else {
             PEB_CUDA(c, cudaMemsetAsync(dd + kDdNc, 0, sizeof(int32_t), c->stream));
         }
-        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.cap, dd);
+        // a step planned without contacts (none were found last time) aborts if it finds any
+        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.plan_none ? 0 : nb.cap, dd);
         PEB_LAUNCHED(c);
     } else {
         int32_t total_b = 0;
@@ -1739,7 +1752,7 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
     const unsigned cgrid = capped_grid(c, cap, kBlk);   // kernels over the contacts
     // 3. colouring
     int32_t ncolors = 0;
-    const bool any = queued || nc > 0;
+    const bool any = queued ? !nb.plan_none : nc > 0;
     if (any) {
         prof_begin(c, ST_COLOR);
         PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)nbod + 1) * sizeof(int32_t), c->stream));
@@ -1830,7 +1843,7 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
     const int iters = c->p.max_iterations;
     unsigned long long *dl = (unsigned long long *)nb.red;
     if (c->want_residual) PEB_CUDA(c, cudaMemsetAsync(nb.red, 0, 2 * sizeof(double), c->stream));
-    if (queued && iters > 0) {
+    if (queued && any && iters > 0) {
         prof_begin(c, ST_SWEEP);
         rc = launch_sweeps_queued<VT>(c, model, gen, iters, cap, VT(1.0 / dt), cc, bv, n, dl);
         if (rc) return rc;
@@ -1983,6 +1996,7 @@ void nbgs_free(Ctx *c) {
     dfree(c, b.bar2);
     if (b.color_start) cudaFreeHost(b.color_start);
     if (b.h_dd) cudaFreeHost(b.h_dd);
+    if (b.gexec) cudaGraphExecDestroy(b.gexec);
     b = NbgsBuf();
 }
 
@@ -2003,6 +2017,71 @@ int nbgs_step(Ctx *c, double dt) {
                                             : nbgs_step_t<float>(c, dt, q);
 }
 
+// Replays of a captured graph of c->graph_steps queued steps (even, so that the buffer swaps
+// cancel) while they fit in nsteps; *ran receives the steps run (0: graphs are off, not
+// possible, or the buffers are fresh).  The graph is captured again when a buffer, a setting it
+// bakes in or the sweep grid changes.  Nothing runs on the device during a capture, so a failed
+// capture only switches graphs off.
+int nbgs_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *ran) {
+    NbgsBuf &nb = c->nb;
+    *ran = 0;
+    const int32_t gs = c->graph_steps & ~1;
+    if (gs < 2 || nsteps < gs || nb.gfailed || c->prof || !nb.warm) return PE_B200_OK;
+    union {
+        double d;
+        uint64_t u;
+    } dtu;
+    dtu.d = dt;
+    union {
+        double d;
+        uint64_t u;
+    } erpu;
+    erpu.d = c->p.erp;
+    const uint64_t key[12] = {(uint64_t)(uintptr_t)c->cur.pr, (uint64_t)(uintptr_t)c->nxt.pr,
+                              (uint64_t)(uintptr_t)nb.cache, (uint64_t)nb.cap, c->epoch,
+                              (uint64_t)c->p.max_iterations, (uint64_t)c->p.relaxation_model,
+                              erpu.u, dtu.u, (uint64_t)nb.plan_none,
+                              (uint64_t)queued_sweep_blocks(c), (uint64_t)gs};
+    bool match = nb.gexec != nullptr;
+    for (int i = 0; i < 12 && match; ++i) match = nb.gkey[i] == key[i];
+    if (!match) {
+        if (nb.gexec) cudaGraphExecDestroy(nb.gexec);
+        nb.gexec = nullptr;
+        const BodyBuf cur0 = c->cur, nxt0 = c->nxt;
+        const int64_t l0 = c->launches;
+        cudaGraph_t g = nullptr;
+        int rc = PE_B200_OK;
+        cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (int32_t k = 0; k < gs && rc == PE_B200_OK; ++k) rc = nbgs_step(c, dt);
+            const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            if (e == cudaSuccess) e = e2;
+        }
+        const int64_t per = c->launches - l0;
+        c->launches = l0;
+        bool ok = e == cudaSuccess && rc == PE_B200_OK && g != nullptr && c->cur.pr == cur0.pr;
+        if (ok) ok = cudaGraphInstantiate(&nb.gexec, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        if (!ok) {
+            if (nb.gexec) cudaGraphExecDestroy(nb.gexec);
+            nb.gexec = nullptr;
+            nb.gfailed = true;
+            c->cur = cur0;
+            c->nxt = nxt0;
+            cudaGetLastError();
+            c->err.clear();
+            return PE_B200_OK;
+        }
+        for (int i = 0; i < 12; ++i) nb.gkey[i] = key[i];
+        nb.gsteps = gs;
+        nb.glaunches = per;
+    }
+    PEB_CUDA(c, cudaGraphLaunch(nb.gexec, c->stream));
+    c->launches += nb.glaunches;
+    *ran = gs;
+    return PE_B200_OK;
+}
+
 // nsteps hard-contact steps.  Queued steps are checked once at the end: if some step found
 // more contacts than the buffers hold, it and every later step of the call left the state as
 // it was; the buffers grow to the count seen and those steps run again.
@@ -2018,24 +2097,40 @@ int nbgs_run(Ctx *c, int32_t nsteps, double dt) {
     int32_t left = nsteps;
     for (int attempt = 0; left > 0; ++attempt) {
         if (c->nb.dd) PEB_CUDA(c, cudaMemsetAsync(c->nb.dd + kDdSteps, 0, sizeof(int32_t), c->stream));
-        for (int32_t k = 0; k < left; ++k) {
-            const int rc = nbgs_step(c, dt);
+        int32_t k = 0;
+        while (k < left) {
+            int32_t ran = 0;
+            int rc = nbgs_graph_run(c, left - k, dt, &ran);
             if (rc) return rc;
+            if (ran == 0) {
+                rc = nbgs_step(c, dt);
+                if (rc) return rc;
+                c->nb.warm = true;
+                ran = 1;
+            }
+            k += ran;
         }
         NbgsBuf &nb = c->nb;
         PEB_CUDA(c, cudaMemcpyAsync(nb.h_dd, nb.dd, kDdCount * sizeof(int32_t),
                                     cudaMemcpyDeviceToHost, c->stream));
         PEB_CUDA(c, cudaStreamSynchronize(c->stream));
         c->last_ncontacts = nb.h_dd[kDdNc];
-        c->last_ncolors = nb.h_dd[kDdNcolors];
-        if (!nb.h_dd[kDdAbort]) break;
+        c->last_ncolors = nb.h_dd[kDdNc] > 0 ? nb.h_dd[kDdNcolors] : 0;
+        if (!nb.h_dd[kDdAbort]) {
+            // the next call's steps skip the contact stages while the scene has no contacts
+            nb.plan_none = nb.h_dd[kDdNc] == 0;
+            break;
+        }
         const int32_t done = nb.h_dd[kDdSteps];
-        if (c->p.max_contacts > 0)
-            return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
-        if (attempt >= 8) return set_err(c, PE_B200_ERR_CAPACITY, "contact buffers kept overflowing");
         const int64_t need = nb.h_dd[kDdNeed];
-        int rc = nbgs_alloc(c, need + need / 4 + 1024);
-        if (rc) return rc;
+        if (attempt >= 8) return set_err(c, PE_B200_ERR_CAPACITY, "contact buffers kept overflowing");
+        if (need > nb.cap) {
+            if (c->p.max_contacts > 0)
+                return set_err(c, PE_B200_ERR_CAPACITY, "contact capacity exceeded");
+            int rc = nbgs_alloc(c, need + need / 4 + 1024);
+            if (rc) return rc;
+        }
+        nb.plan_none = false;
         PEB_CUDA(c, cudaMemsetAsync(nb.dd + kDdAbort, 0, sizeof(int32_t), c->stream));
         nb.h_dd[kDdAbort] = 0;
         left -= done;
