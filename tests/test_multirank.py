@@ -1,6 +1,6 @@
-"""The N>1 path of bench.py without GPUs: two gloo ranks on the CPU partition a batched ensemble
-by scene (each scene on exactly one rank, loads balanced) and combine their timings the way the
-benchmark does (max of the device times, sum of the spheres)."""
+"""The N>1 path without GPUs: two gloo ranks on the CPU partition a batched ensemble by scene
+through pe_b200.shard (each scene on exactly one rank, loads balanced) and combine their timings
+the way the benchmark does (max of the device times, sum of the spheres)."""
 import os
 import socket
 
@@ -23,14 +23,15 @@ def _free_port():
 def _rank_main(rank, world, port, out):
     import sys
     sys.path.insert(0, ROOT)
-    import bench
     from pe_b200 import scenes
+    from pe_b200.shard import local_scenes, shard_scenes
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         ens = scenes.batched_ensemble(0, scenes=40, nmin=64, nmax=1024)
-        mine = bench.shard_scenes(ens, rank, world)
+        mine = local_scenes(ens)
+        assert [s.name for s in mine] == [s.name for s in shard_scenes(ens, rank, world)]
         names = [None] * world
         dist.all_gather_object(names, [s.name for s in mine])
         # the benchmark's reductions: max of the per-rank times, sum of the per-rank spheres
@@ -68,8 +69,19 @@ def test_ensemble_partition_two_gloo_ranks():
 def test_shard_scenes_single_rank_keeps_everything():
     import sys
     sys.path.insert(0, ROOT)
-    import bench
     from pe_b200 import scenes
+    from pe_b200.shard import local_scenes, shard_scenes
     ens = scenes.batched_ensemble(1, scenes=10, nmin=64, nmax=256)
-    assert [s.name for s in bench.shard_scenes(ens, 0, 1)] == \
-        [s.name for s in sorted(ens, key=lambda s: -s.n)]
+    want = [s.name for s in sorted(ens, key=lambda s: -s.n)]
+    assert [s.name for s in shard_scenes(ens, 0, 1)] == want
+    assert [s.name for s in local_scenes(ens)] == want   # no process group: everything
+    with pytest.raises(ValueError):
+        shard_scenes(ens, 2, 2)
+
+
+def test_bench_uses_the_library_partition():
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    from pe_b200 import shard
+    assert bench.shard_scenes is shard.shard_scenes
