@@ -31,6 +31,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from pe_b200 import scenes  # noqa: E402
+from pe_b200.shard import shard_scenes  # noqa: E402
 
 METRIC = "sphere-steps/s (1M DEM, 32k NBGS) mixed+batched vs plain FP64 GPU at stated err"
 UNIT = "sphere-steps/s"
@@ -73,17 +74,6 @@ def build_workload(name, seed=0, rank=0, world=1):
     if name == "ensemble_512":
         return shard_scenes(scenes.batched_ensemble(seed), rank, world), "dem"
     raise ValueError(name)
-
-
-def shard_scenes(ss, rank, world):
-    load = [0] * world
-    mine = []
-    for k in sorted(range(len(ss)), key=lambda k: (-ss[k].n, k)):
-        r = min(range(world), key=lambda q: (load[q], q))
-        load[r] += ss[k].n
-        if r == rank:
-            mine.append(ss[k])
-    return mine
 
 
 # ------------------------------------------------------------------------------------------
@@ -578,19 +568,14 @@ def our_arm(args):
         e.close()
         return None
 
-    # dominant kernel roofline (the fused DEM step kernel or the NBGS sweeps)
-    peaks = {}
-    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(pp):
-        peaks = json.load(open(pp))
-    peak = peaks.get("hbm_gbs")
-    peak_src = "measured" if peak else "fallback"
-    peak = peak or 6650.0
+    # dominant stage roofline (the DEM list step's two force kernels, or the NBGS sweeps)
+    peak, peak_src = _peak_gbs()
     if kind == "dem":
         kms, kcnt = prof.get("dem_step", (0.0, 0))
         per = ALGO_BYTES["mixed"]
         algo = per * nsph
-        kname = "k_dem_list<float> (neighbour-list force + integration)"
+        kname = ("k_dem_contacts<float> (forces on the marked spheres) + k_dem_move<float> "
+                 "(integration of all spheres): the list step's force stage")
     else:
         kms, kcnt = prof.get("sweeps", (0.0, 0))
         st = e.stats()
@@ -612,7 +597,10 @@ def our_arm(args):
             "config": {"workload": args.workload, "spheres": int(total_sph),
                        "spheres_per_rank": nsph, "scenes": len(ss),
                        "precision": "mixed", "dt": dt, "tuning": tuning,
-                       "l2": "flushed between timed steps (256 MiB write + 256 MiB read, untimed)",
+                       "l2": "flushed between timed steps (256 MiB write + 256 MiB read, "
+                             "untimed); the flush also writes back the lines each step left "
+                             "dirty in L2, outside the timed region (graph_replay_16 runs 16 "
+                             "steps back to back and pays for them)",
                        "parallelism": ("1 GPU" if world == 1 else
                                        f"scenes partitioned over {world} ranks"
                                        if args.workload == "ensemble_512" else
@@ -676,6 +664,50 @@ def boxes_extra(torch, flush, dev):
                                           "body_steps_per_s": nb * 5 / sec}
         out[label] = rec
     return out
+
+
+def _peak_gbs():
+    """The HBM roofline peak: MEASURED_PEAKS.json's copy bandwidth, else the pool's fallback."""
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(pp)).get("hbm_gbs") if os.path.exists(pp) else None
+    return (peak, "measured") if peak else (6650.0, "fallback")
+
+
+def dense_extra(torch, flush, dev, steps):
+    """The contact-dense DEM workload (every sphere in contact every step, lists rebuilt often):
+    1,048,576 spheres, mixed precision, tuned launch shapes, stepped one call per step with the
+    L2 flushed between steps, and through CUDA-graph replays of 16 steps."""
+    from pe_b200 import _abi
+    s = scenes.dem_dense(0)
+    e = make_engine([s], "dem", _abi.MIXED)
+    tu = e.autotune(s.dt, 50)
+    st = torch.cuda.ExternalStream(e.stream_ptr(), device=dev)
+    k = max(20, min(steps, 200))
+    r0 = e.neighbor_list_stats()
+    ms, launches, prof = timed_steps(e, s.dt, k, 3, torch, flush, st)
+    r1 = e.neighbor_list_stats()
+    msg, _, active = timed_chunks(e, s.dt, max(2, k // 16), 16, 1, torch, flush, st)
+    kg = max(2, k // 16) * 16
+    e.close()
+    # the force stage's algorithmic bytes: the headline's per-sphere state traffic, plus the
+    # list entries read and each sphere's stored force, written then read (every sphere of this
+    # scene is marked)
+    per = ALGO_BYTES["mixed"] + 4.0 * r1["entries"] / s.n + 2 * 24.0
+    kms, kcnt = prof.get("dem_step", (0.0, 0))
+    kavg = kms / max(kcnt, 1)
+    peak = _peak_gbs()
+    achieved = per * s.n / (kavg / 1e3) / 1e9 if kavg > 0 else None
+    return {"value": s.n * k / (ms / 1e3), "unit": "sphere-steps/s", "ms_per_step": ms / k,
+            "roofline": {"bound": "hbm", "kernel": "k_dem_contacts + k_dem_move (force stage)",
+                         "achieved": achieved, "peak": peak[0], "unit": "GB/s",
+                         "frac": achieved / peak[0] if achieved else None,
+                         "peak_source": peak[1], "algorithmic_bytes_per_sphere": per,
+                         "avg_launch_ms": kavg},
+            "graph_replay_16_value": s.n * kg / (msg / 1e3), "graph_active": active,
+            "spheres": s.n, "precision": "mixed", "tuning": tu,
+            "rebuilds_per_step": (r1["rebuilds"] - r0["rebuilds"]) / (k + min(k, 200) + 3),
+            "list_entries_per_sphere": r1["entries"] / s.n,
+            "stages_ms_per_step": {a: b[0] / k for a, b in prof.items() if b[1]}}
 
 
 def nbgs_extra(torch, flush, dev):
@@ -810,6 +842,7 @@ def extras(args, torch, flush, dev, ss, kind, mixed_value):
                                "tuning": tu,
                                "stages_ms_per_step": {a: b[0] / k for a, b in prof.items() if b[1]}}
         e.close()
+        out["dem_dense_1m"] = dense_extra(torch, flush, dev, args.steps)
         out["adjoint_hopper_16384"] = adjoint_extra(torch)
         out.update(nbgs_extra(torch, flush, dev))
     if args.workload == "dem_large_1m":
@@ -865,8 +898,13 @@ PROFILE_CASES = {
     # the headline list step (k_dem_list, k_rebuild) on the full 1M scene
     "dem_list_mixed": ("dem", 1048576, "mixed", True),
     "dem_list_fp64": ("dem", 1048576, "fp64", True),
+    # the contact-dense 1M scene (every sphere in contact, frequent rebuilds)
+    "dem_dense_mixed": ("dense", 1048576, "mixed", True),
     # hard-contact step on the dense 32k packing (detection, colouring, cache, sweeps)
     "nbgs_dense_mixed": ("hcsits", 32768, "mixed", None),
+    "nbgs_dense_fp64": ("hcsits", 32768, "fp64", None),
+    # hard-contact step on the loose 32k scene (no contacts for most of its steps)
+    "nbgs_free_mixed": ("hcsits_free", 32768, "mixed", None),
     # the 512-scene ensemble (list step)
     "ensemble_mixed": ("ensemble", 0, "mixed", True),
     # the adjoint of 100 steps of the hopper
@@ -888,8 +926,13 @@ def profile_case(args):
             scenes.dem_large(0)
         e = make_engine([sc], "dem", precision, lists=lists)
         dt = sc.dt
-    elif kind == "hcsits":
-        sc = scenes.nbgs_box(0, n=n, dims=(32.0, 32.0, 120.0), dense=True)
+    elif kind == "dense":
+        sc = scenes.dem_dense(0)
+        e = make_engine([sc], "dem", precision, lists=lists)
+        dt = sc.dt
+    elif kind in ("hcsits", "hcsits_free"):
+        sc = scenes.nbgs_box(0, n=n, dims=(32.0, 32.0, 120.0), dense=True) \
+            if kind == "hcsits" else scenes.nbgs_box(0, n=n)
         e = make_engine([sc], "hcsits", precision)
         dt = sc.dt
     elif kind == "ensemble":

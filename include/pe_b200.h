@@ -228,14 +228,17 @@ int pe_b200_set_profiling(pe_b200_ctx *ctx, int32_t enabled);
 int pe_b200_profile(pe_b200_ctx *ctx, int32_t cap, const char **names, double *total_ms,
                     int64_t *count, int32_t *n_out);
 
-/* CUDA graphs of the DEM neighbour-list step (no pe counterpart; pe's step is a serial loop).
- * pe_b200_step(ctx, nsteps, dt) with nsteps >= steps captures `steps` consecutive steps once and
- * then replays the graph, so a replay costs one launch instead of two per step; the remainder
- * runs step by step.  Default 16; 0 (or 1) launches every step; odd values are rounded down.
- * Graphs are not used while profiling is on.  The results are the same as without graphs. */
+/* CUDA graphs of the DEM neighbour-list step and of the hard-contact step of sphere scenes (no
+ * pe counterpart; pe's step is a serial loop).  pe_b200_step(ctx, nsteps, dt) with
+ * nsteps >= steps captures `steps` consecutive steps once and then replays the graph, so a
+ * replay costs one launch; the remainder runs step by step.  Default 16; 0 (or 1) launches every
+ * step; odd values are rounded down.  Graphs are not used while profiling is on.  The results
+ * are the same as without graphs. */
 int pe_b200_set_graph_steps(pe_b200_ctx *ctx, int32_t steps);
-/* 1 when the last pe_b200_step ran through a captured graph. */
+/* 1 when the context holds a captured graph it can replay. */
 int pe_b200_graph_active(const pe_b200_ctx *ctx);
+/* Graphs captured and graph launches since the context was created. */
+int pe_b200_graph_stats(const pe_b200_ctx *ctx, int64_t *captures, int64_t *replays);
 
 /* Launch shapes of the DEM neighbour-list step (no pe counterpart). */
 typedef struct {
@@ -246,10 +249,12 @@ typedef struct {
     double ms_per_step;      /* pe_b200_autotune: measured time of the winner; else -1 */
     int32_t variants;        /* output: number of launch shapes */
     int32_t nbgs_sweeps;     /* HCSITS sweeps: 0 automatic (4 when every colour fits one
-                                block, else 2), 1 one thread-block cluster with hardware
-                                barriers, 2 one cooperative grid with barriers through global
-                                memory, 3 one launch per colour, 4 one thread block with
-                                __syncthreads between colours (when every colour fits it) */
+                                block, else 5 when the bodies fit, else 2), 1 one thread-block
+                                cluster with hardware barriers, 2 one cooperative grid with
+                                barriers through global memory, 3 one launch per colour, 4 one
+                                thread block with __syncthreads between colours (when every
+                                colour fits it), 5 one cluster with the bodies' records in its
+                                distributed shared memory (sphere scenes whose bodies fit) */
     int32_t dem_grid;        /* DEM grid step (cell search every step): 0 candidates read from an
                                 FP32 position copy in cell order, with an exact FP64 test for the
                                 close ones; 1 every candidate through its FP64 record (the same

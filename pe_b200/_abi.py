@@ -32,7 +32,7 @@ EXPORTS = ["pe_b200_default_params", "pe_b200_create", "pe_b200_destroy", "pe_b2
            "pe_b200_kernel_launches", "pe_b200_stream", "pe_b200_set_profiling",
            "pe_b200_profile", "pe_b200_dem_step_static", "pe_b200_neighbor_list_stats",
            "pe_b200_adjoint_forward", "pe_b200_adjoint_backward", "pe_b200_set_graph_steps",
-           "pe_b200_graph_active", "pe_b200_get_tuning", "pe_b200_set_tuning",
+           "pe_b200_graph_active", "pe_b200_graph_stats", "pe_b200_get_tuning", "pe_b200_set_tuning",
            "pe_b200_autotune", "pe_b200_validate", "pe_b200_selftest_timeout",
            "pe_b200_upload_boxes", "pe_b200_download_boxes", "pe_b200_box_count"]
 
@@ -106,6 +106,7 @@ def load() -> C.CDLL:
         "pe_b200_adjoint_backward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "pe_b200_set_graph_steps": (C.c_int, [vp, i32]),
         "pe_b200_graph_active": (C.c_int, [vp]),
+        "pe_b200_graph_stats": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "pe_b200_get_tuning": (C.c_int, [vp, P(Tuning)]),
         "pe_b200_set_tuning": (C.c_int, [vp, P(Tuning)]),
         "pe_b200_autotune": (C.c_int, [vp, dp, i32, P(Tuning)]),

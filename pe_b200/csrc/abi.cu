@@ -797,13 +797,28 @@ int pe_b200_set_graph_steps(pe_b200_ctx *h, int32_t steps) {
     if (!c || steps < 0) return PE_B200_ERR_ARG;
     c->graph_steps = steps & ~1;
     c->sg.failed = false;
+    c->nb.gfailed = false;
     dem_graph_free(c);
+    nbgs_graph_free(c);
     return PE_B200_OK;
 }
 
 int pe_b200_graph_active(const pe_b200_ctx *h) {
     const Ctx *c = reinterpret_cast<const Ctx *>(h);
-    return (c && ((c->sg.exec && !c->sg.failed) || (c->nb.gexec && !c->nb.gfailed))) ? 1 : 0;
+    if (!c) return 0;
+    if (c->sg.exec && !c->sg.failed) return 1;
+    if (c->nb.gfailed) return 0;
+    for (const NbgsBuf::GraphSlot &s : c->nb.gslot)
+        if (s.exec) return 1;
+    return 0;
+}
+
+int pe_b200_graph_stats(const pe_b200_ctx *h, int64_t *captures, int64_t *replays) {
+    const Ctx *c = reinterpret_cast<const Ctx *>(h);
+    if (!c || !captures || !replays) return PE_B200_ERR_ARG;
+    *captures = c->graph_captures;
+    *replays = c->graph_replays;
+    return PE_B200_OK;
 }
 
 int pe_b200_get_tuning(pe_b200_ctx *h, pe_b200_tuning *out) {

@@ -66,8 +66,10 @@ int set_list_skin(Ctx *c, double skin) {
 
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
     if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < -1 ||
-        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 4 || t.dem_grid < 0 || t.dem_grid > 1)
+        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 5 || t.dem_grid < 0 || t.dem_grid > 1)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
+    // captured hard-contact graphs bake the sweep form in
+    if (t.nbgs_sweeps != c->tune.nbgs_sweeps) c->epoch++;
     c->tune.nbgs_sweeps = t.nbgs_sweeps;
     c->tune.dem_grid = t.dem_grid;
     if (t.dem_variant != c->tune.dem_variant || t.rebuild_per_sm != c->tune.rebuild_per_sm) {

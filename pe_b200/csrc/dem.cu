@@ -153,11 +153,36 @@ struct DemArgs {
     const int32_t *act = nullptr;     // exclusive offsets of the marks (n + 1)
     const int32_t *alist = nullptr;   // the marked spheres
     VT *facc = nullptr;               // their force and torque, component-major (6 x n)
+    // list step: the rebuild's copy of the state in cell order, read instead of pr/vw/tag/uid/q
+    // by the force kernels of a step that rebuilt (nl_flags[4]); tag_out/uid_out then receive
+    // the reordered tags and ids in place
+    const double4 *alt_pr = nullptr;
+    const VT *alt_vw = nullptr;
+    const uint32_t *alt_tag = nullptr;
+    const int32_t *alt_uid = nullptr;
+    const double4 *alt_q = nullptr;
 };
 
+// The state a list step's force kernels read: the current buffers, or the copy in cell order
+// when the step rebuilt the lists (the copy is not moved back: the integration writes the next
+// state from it).  Read after the rebuild kernel has finished.
+template <typename VT>
+__device__ __forceinline__ DemArgs<VT> list_view(const DemArgs<VT> &a0) {
+    DemArgs<VT> a = a0;
+    if (a0.nl_flags[4]) {
+        a.pr = a0.alt_pr;
+        a.vw = a0.alt_vw;
+        a.tag = a0.alt_tag;
+        a.uid = a0.alt_uid;
+        a.q = a0.alt_q;
+    }
+    return a;
+}
+
 // one sphere pair (this body and neighbour j), both in the buffers of `a`; self1: this body is
-// pe's body 1, i.e. has the smaller system id (MaxContacts.h:550-551)
-template <typename T, typename VT, bool HERTZ>
+// pe's body 1, i.e. has the smaller system id (MaxContacts.h:550-551).  ONE: a single material
+// (a.m0), so the neighbour's tag is not read.
+template <typename T, typename VT, bool HERTZ, bool ONE = false>
 __device__ __forceinline__ void pair_force_o(const DemArgs<VT> &a, const double4 &pi, V3<T> vi,
                                              V3<T> wi, const MatDev &mi, int32_t j,
                                              const double4 &pj, bool self1, Acc<T> &acc) {
@@ -168,7 +193,7 @@ __device__ __forceinline__ void pair_force_o(const DemArgs<VT> &a, const double4
     const double dist = __dsub_rn(__dsub_rn(len, p1.w), p2.w);
     // only penetrating contacts produce a force (ContactBase.h:307-310)
     if (!(dist < -kContactThreshold)) return;
-    const MatDev &mj = a.mats[a.tag[j] & 0xffffu];
+    const MatDev &mj = ONE ? a.m0 : a.mats[a.tag[j] & 0xffffu];
     const V3<T> vj = ld_vw(a.vw, a.n, j, 0), wj = ld_vw(a.vw, a.n, j, 1);
     V3<T> n, r1, r2;
     if (sizeof(T) == 8) {
@@ -673,11 +698,12 @@ constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]))
 
 // forces on the marked spheres (a grid-stride loop over the marked list)
 template <typename VT, bool HERTZ, bool ONE = false>
-__global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a) {
+__global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
     using T = VT;
     // launched early behind the rebuild kernel: nothing is read before it has finished
     pdl_wait();
     pdl_trigger();
+    const DemArgs<VT> a = list_view(a0);
     const int32_t na = a.act[a.n];
     for (int32_t m = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x); m < na;
          m += (int32_t)(gridDim.x * blockDim.x)) {
@@ -703,13 +729,13 @@ __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a) {
                 const uint32_t e0 = (uint32_t)a.nl_idx[k], e1 = (uint32_t)a.nl_idx[k + 1];
                 const int32_t j0 = (int32_t)(e0 & 0x7fffffffu), j1 = (int32_t)(e1 & 0x7fffffffu);
                 const double4 p0 = a.pr[j0], p1 = a.pr[j1];
-                pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j0, p0, (e0 >> 31) != 0u, acc);
-                pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j1, p1, (e1 >> 31) != 0u, acc);
+                pair_force_o<T, VT, HERTZ, ONE>(a, pi, vi, wi, mi, j0, p0, (e0 >> 31) != 0u, acc);
+                pair_force_o<T, VT, HERTZ, ONE>(a, pi, vi, wi, mi, j1, p1, (e1 >> 31) != 0u, acc);
             }
             if (k < e) {
                 const uint32_t e0 = (uint32_t)a.nl_idx[k];
                 const int32_t j0 = (int32_t)(e0 & 0x7fffffffu);
-                pair_force_o<T, VT, HERTZ>(a, pi, vi, wi, mi, j0, a.pr[j0], (e0 >> 31) != 0u, acc);
+                pair_force_o<T, VT, HERTZ, ONE>(a, pi, vi, wi, mi, j0, a.pr[j0], (e0 >> 31) != 0u, acc);
             }
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
@@ -725,13 +751,15 @@ __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a) {
 
 // integration of every sphere with the forces of k_dem_contacts
 template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool ONE = false>
-__global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a) {
+__global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     // launched early behind the contact kernel; the next step's rebuild may be scheduled from
     // here on (it waits for this kernel in turn)
     pdl_wait();
     pdl_trigger();
+    const bool rebuilt = a0.nl_flags[4] != 0;
+    const DemArgs<VT> a = list_view(a0);
     bool moved = false;
     if (t < a.n) {
         // every load of this body's own records first: they are independent, and none may
@@ -751,6 +779,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a) {
             const int64_t cap = a.n;
             acc.F = v3(a.facc[m], a.facc[cap + m], a.facc[2 * cap + m]);
             acc.T_ = v3(a.facc[3 * cap + m], a.facc[4 * cap + m], a.facc[5 * cap + m]);
+        }
+        if (rebuilt) {   // the reordered tags and ids replace the current ones
+            a.tag_out[t] = ONE ? a.tag[t] : tagi;
+            a.uid_out[t] = a.uid[t];
         }
         V3<T> v, w;
         const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w, ext);
@@ -905,20 +937,6 @@ __global__ void k_permute_c(int64_t n, const int32_t *sorted, BodyBuf src, BodyB
     }
 }
 
-template <typename VT>
-__global__ void k_copy_c(int64_t n, BodyBuf src, BodyBuf dst, double4 *other_pr,
-                         const int32_t *cond) {
-    if (!*cond) return;
-    GRID_STRIDE(t, n) {
-        dst.pr[t] = src.pr[t];
-        other_pr[t] = src.pr[t];   // the other position buffer keeps the radius too
-        cp_vw((VT *)dst.vw, t, (const VT *)src.vw, t, n);
-        dst.tag[t] = src.tag[t];
-        dst.uid[t] = src.uid[t];
-        if (src.q) dst.q[t] = src.q[t];
-    }
-}
-
 // neighbours of body t (state in cell order, so slot == index): pairs closer than
 // r_i + r_j + skin.  mode 0 counts, mode 1 writes.
 template <int MODE>
@@ -977,6 +995,7 @@ __global__ void k_alist_c(int64_t n, const int32_t *act, int32_t *alist, const i
 }
 
 __global__ void k_rebuild_done(int64_t n, const int32_t *start, int64_t cap, int32_t *flags) {
+    flags[4] = flags[0] ? 1 : 0;   // the force kernels read the copy in cell order
     if (!flags[0]) return;
     flags[0] = 0;
     flags[1] = start[n] > cap ? 1 : 0;
@@ -1006,13 +1025,11 @@ int list_rebuild(Ctx *c) {
     k_permute_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->sorted, c->cur, L.tmp, L.disp,
                                                              cond);
     PEB_LAUNCHED(c);
-    k_copy_c<VT><<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.tmp, c->cur, c->nxt.pr, cond);
-    PEB_LAUNCHED(c);
-    k_list<0><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->cur.uid, c->d_scenes,
+    k_list<0><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, L.tmp.pr, L.tmp.tag, L.tmp.uid, c->d_scenes,
                                                        c->cell_start, L.skin, L.cnt, nullptr, 0,
                                                        nullptr, cond);
     PEB_LAUNCHED(c);
-    k_mark_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->d_scenes,
+    k_mark_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.tmp.pr, L.tmp.tag, c->d_scenes,
                                                           c->d_boxes, 0.5 * L.skin * (1.0 + 1e-9),
                                                           L.cnt, L.act, cond);
     PEB_LAUNCHED(c);
@@ -1022,7 +1039,7 @@ int list_rebuild(Ctx *c) {
     if (rc) return rc;
     k_alist_c<<<capped_grid(c, n, 256), 256, 0, c->stream>>>(n, L.act, L.alist, cond);
     PEB_LAUNCHED(c);
-    k_list<1><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, c->cur.pr, c->cur.tag, c->cur.uid, c->d_scenes,
+    k_list<1><<<capped_grid(c, n, 128), 128, 0, c->stream>>>(n, L.tmp.pr, L.tmp.tag, L.tmp.uid, c->d_scenes,
                                                        c->cell_start, L.skin, nullptr, L.start,
                                                        L.cap, L.idx, cond);
     PEB_LAUNCHED(c);
@@ -1088,6 +1105,13 @@ int list_step(Ctx *c, double dt) {
     if (rc) return rc;
     DemArgs<VT> a = dem_args<VT>(c, dt);
     a.sorted = nullptr;   // the grid fallback sees the state in cell order
+    a.alt_pr = L.tmp.pr;
+    a.alt_vw = (const VT *)L.tmp.vw;
+    a.alt_tag = L.tmp.tag;
+    a.alt_uid = L.tmp.uid;
+    a.alt_q = L.tmp.q;
+    a.tag_out = c->cur.tag;   // tags and ids stay in place (reordered there after a rebuild)
+    a.uid_out = c->cur.uid;
     prof_begin(c, ST_DEM);
     // the Hertz law and orientation tracking run the default launch shape
     if (a.hertz)
@@ -1305,6 +1329,7 @@ int capture_steps(Ctx *c, int32_t steps, double dt) {
     G.epoch = c->epoch;
     for (int i = 0; i < 12; ++i) G.key[i] = key[i];
     G.launches = per_replay;
+    c->graph_captures++;
     return PE_B200_OK;
 }
 
@@ -1354,6 +1379,7 @@ int dem_list_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *done) {
         }
         PEB_CUDA(c, cudaGraphLaunch(G.exec, c->stream));
         c->launches += G.launches;
+        c->graph_replays++;
         *done += gs;
         rc = list_queue_check(c, gs);
         if (rc) return rc;

@@ -83,16 +83,27 @@ struct NbgsBuf {
     bool on_device = false;                   // the last step's counts are only on the device
     bool plan_none = false;                   // queued steps planned without contacts
     bool warm = false;                        // a queued step has run on these buffers
-    // a captured CUDA graph of `gsteps` queued steps, valid for the buffers, settings and
-    // sweep grid in gkey (nbgs.cu nbgs_run)
-    cudaGraphExec_t gexec = nullptr;
-    int32_t gsteps = 0;
-    int64_t glaunches = 0;
+    // captured CUDA graphs of queued steps, each valid for the buffers, settings, plan and
+    // sweep grid in its key (nbgs.cu nbgs_graph_run); a miss replaces the least recently used
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;   // kernels per replay
+        uint64_t used = 0;      // last use (gclock)
+        uint64_t key[12] = {};
+    };
+    static constexpr int kGraphSlots = 4;
+    GraphSlot gslot[kGraphSlots];
+    uint64_t gclock = 0;
     bool gfailed = false;
-    uint64_t gkey[12] = {};
     unsigned int *bar = nullptr;              // grid barrier of the persistent sweep
     bool coop_disabled = false;
     int cluster = -1;               // CTAs of the one-cluster sweep kernel (0: not available)
+    // the sweep form with the bodies in one cluster's shared memory (nbgs.cu
+    // launch_sweeps_dsmem): CTAs per cluster for the body count and kernel probed last (0: the
+    // bodies do not fit)
+    int64_t ds_nbod = -1;
+    int ds_key = -1;
+    int ds_size = 0;
     void *vel = nullptr;                      // v', w', dv, dw per body (VT[12])
     int64_t nbod = 0;                         // bodies the per-body buffers hold
     bool gen = false;                         // they hold world-frame inverse inertias too
@@ -159,7 +170,8 @@ struct ListBuf {
 struct Tuning {
     int32_t dem_variant = 0;    // index into the k_dem_list launch shapes (dem.cu)
     int32_t rebuild_per_sm = 0; // persistent rebuild CTAs per SM; 0 = as many as fit
-    int32_t nbgs_sweeps = 0;    // 0 automatic, 1 one cluster, 2 cooperative grid, 3 per colour
+    int32_t nbgs_sweeps = 0;    // 0 automatic, 1 one cluster, 2 cooperative grid, 3 per colour,
+                                // 4 one block, 5 bodies in one cluster's shared memory
     int32_t dem_grid = 0;       // grid step: 0 sorted FP32 candidate copy, 1 FP64 records only
 };
 
@@ -251,7 +263,9 @@ struct Ctx {
     StepGraph sg;
     void *stage = nullptr;          // host-layout staging for uploads and downloads (transfer.cu)
     size_t stage_bytes = 0;
-    int32_t graph_steps = 16;       // DEM list steps per graph replay; 0 = no graphs
+    int32_t graph_steps = 16;       // steps per graph replay; 0 = no graphs
+    int64_t graph_captures = 0;     // graphs captured (DEM list and hard-contact steps)
+    int64_t graph_replays = 0;      // graph launches
     uint64_t epoch = 1;             // bumped by every change that captured kernels bake in
     // profiling
     bool prof = false;
@@ -409,6 +423,7 @@ int validate_coloring(Ctx *c, int64_t *bad);
 int validate_lists(Ctx *c, int64_t *bad);
 int selftest_timeout(Ctx *c, int64_t polls);
 void nbgs_free(Ctx *c);
+void nbgs_graph_free(Ctx *c);   // the captured hard-contact graphs
 
 // ------------------------------------------------------------------------------------------
 // device helpers

@@ -43,6 +43,7 @@ enum : int {
     kDdSteps = 4,    // steps completed (not aborted) since the host reset it
     kDdNc = 5,       // contact count written by the host (scenes with moving boxes)
     kDdSink = 6,     // error bits nobody reads (a capacity overflow that aborts instead)
+    kDdSeen = 7,     // the largest contact count of the call's steps (reset per call)
     kDdCount = 8
 };
 
@@ -171,6 +172,37 @@ struct BodyV {
     // scenes with moving boxes: the rows of every body's world-frame inverse inertia
     // R I^-1 R^T (RigidBody.h:866-869; a sphere's is 1/I on the diagonal), else null
     T4<T> *ia = nullptr, *ib = nullptr, *ic = nullptr;
+    // the sweeps' accessors (COH: bypass L1, for records other SMs update between colours)
+    __device__ __forceinline__ T4<T> get_vr(int32_t b) const { return vr[b]; }
+    __device__ __forceinline__ T4<T> get_wr(int32_t b) const { return wr[b]; }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_dv(int32_t b) const { return COH ? ldcg4(dv + b) : dv[b]; }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_dw(int32_t b) const { return COH ? ldcg4(dw + b) : dw[b]; }
+    __device__ __forceinline__ void put_dv(int32_t b, const T4<T> &v) const { dv[b] = v; }
+    __device__ __forceinline__ void put_dw(int32_t b, const T4<T> &v) const { dw[b] = v; }
+};
+
+// The body records of a sweep kept in the shared memory of one thread-block cluster: body b
+// lives in CTA b mod C (C = 2^shift, the cluster size) at row slot b / C, and is reached
+// through distributed shared memory from every CTA of the cluster.  Rows: vr, wr, dv, dw, each
+// `per` records long.
+template <typename T>
+struct ClusterBodies {
+    T4<T> *sh;
+    int per, shift;
+    __device__ __forceinline__ T4<T> *at(int row, int32_t b) const {
+        T4<T> *p = sh + (int64_t)row * per + (b >> shift);
+        return cooperative_groups::this_cluster().map_shared_rank(p, (unsigned)(b & ((1 << shift) - 1)));
+    }
+    __device__ __forceinline__ T4<T> get_vr(int32_t b) const { return *at(0, b); }
+    __device__ __forceinline__ T4<T> get_wr(int32_t b) const { return *at(1, b); }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_dv(int32_t b) const { return *at(2, b); }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_dw(int32_t b) const { return *at(3, b); }
+    __device__ __forceinline__ void put_dv(int32_t b, const T4<T> &v) const { *at(2, b) = v; }
+    __device__ __forceinline__ void put_dw(int32_t b, const T4<T> &v) const { *at(3, b) = v; }
 };
 
 // a body's inverse inertia applied to a vector: the scalar of a sphere, or (GEN) the full
@@ -190,8 +222,8 @@ struct InvI<T, true> {
                   c.x * v.x + c.y * v.y + c.z * v.z);
     }
 };
-template <typename T, bool GEN>
-__device__ __forceinline__ InvI<T, GEN> load_invi(const BodyV<T> &bv, int32_t b, T ii) {
+template <typename T, bool GEN, typename BV>
+__device__ __forceinline__ InvI<T, GEN> load_invi(const BV &bv, int32_t b, T ii) {
     if constexpr (GEN) {
         InvI<T, true> r;
         if (b >= 0) {
@@ -358,10 +390,26 @@ __global__ void k_adj_fill(const int32_t *ncp, const int32_t *dd, const int32_t 
 // the guard of a step queued without the host: more contacts than the step was planned for
 // (the buffers' capacity, or none for a step planned without contacts) abort the rest of the
 // call (its steps leave the state as it is); the largest count is recorded
+// the same for a step planned without contacts, in one launch instead of count, scan and
+// guard: a sphere with any contact aborts the call's remaining steps (they are repeated with
+// the contact stages, which record the counts).  dd[kDdNc] stays 0 from the last step that
+// counted (it found none, or this plan would not have been chosen).
+__global__ void k_any_contact(int64_t n, VisitArgs a, int32_t *dd) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || dd[kDdAbort]) return;
+    CountF f;
+    visit_contacts(a, a.sorted ? a.sorted[t] : (int32_t)t, f);
+    if (f.n > 0) {
+        dd[kDdAbort] = 1;
+        atomicMax(&dd[kDdSeen], f.n);
+    }
+}
+
 __global__ void k_guard(const int32_t *total, int64_t limit, int32_t *dd) {
     const int32_t t = *total;
     if (t > limit) dd[kDdAbort] = 1;
     if (t > dd[kDdNeed]) dd[kDdNeed] = t;
+    if (t > dd[kDdSeen]) dd[kDdSeen] = t;
 }
 
 __device__ __forceinline__ uint32_t prio(uint32_t c) {
@@ -860,9 +908,9 @@ __device__ __forceinline__ V3<T> solve_gmd(V3<T> pcf, const V3<T> &g, const T D[
 
 // one contact of one sweep of relaxation model MODEL (pe's RelaxationModel, HCSITS.h:172-179);
 // COHERENT: read the velocity corrections and the impulse from L2
-template <typename T, int MODEL, bool COHERENT, bool GEN = false>
+template <typename T, int MODEL, bool COHERENT, bool GEN = false, typename BV = BodyV<T>>
 __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T> &cc,
-                                              const BodyV<T> &bv, int track_delta,
+                                              const BV &bv, int track_delta,
                                               unsigned long long *delta) {
     constexpr bool FRICTION = MODEL != 0;
     const int2 ids = cc.ids[k];
@@ -873,23 +921,24 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     const T dist = q0.w, dn_inv = q1.w;
     const T4<T> pc4 = COHERENT ? ldcg4(cc.p + k) : cc.p[k];
     const V3<T> pc = xyz<T>(pc4);  // contact frame
-    const T4<T> vr1 = bv.vr[b1], wr1 = bv.wr[b1];
+    const T4<T> vr1 = bv.get_vr(b1), wr1 = bv.get_wr(b1);
     const T im1 = vr1.w, ii1 = wr1.w;
-    V3<T> dv1 = xyz<T>(COHERENT ? ldcg4(bv.dv + b1) : bv.dv[b1]);
-    V3<T> dw1 = xyz<T>(COHERENT ? ldcg4(bv.dw + b1) : bv.dw[b1]);
+    V3<T> dv1 = xyz<T>(bv.template get_dv<COHERENT>(b1));
+    V3<T> dw1 = xyz<T>(bv.template get_dw<COHERENT>(b1));
     const V3<T> v1 = xyz<T>(vr1), w1 = xyz<T>(wr1);
     V3<T> dv2 = v3(T(0), T(0), T(0)), dw2 = dv2, v2 = dv2, w2 = dv2;
     T im2 = T(0), ii2 = T(0);
     if (b2 >= 0) {
-        const T4<T> vr2 = bv.vr[b2], wr2 = bv.wr[b2];
+        const T4<T> vr2 = bv.get_vr(b2), wr2 = bv.get_wr(b2);
         im2 = vr2.w;
         ii2 = wr2.w;
-        dv2 = xyz<T>(COHERENT ? ldcg4(bv.dv + b2) : bv.dv[b2]);
-        dw2 = xyz<T>(COHERENT ? ldcg4(bv.dw + b2) : bv.dw[b2]);
+        dv2 = xyz<T>(bv.template get_dv<COHERENT>(b2));
+        dw2 = xyz<T>(bv.template get_dw<COHERENT>(b2));
         v2 = xyz<T>(vr2);
         w2 = xyz<T>(wr2);
     }
     const InvI<T, GEN> I1 = load_invi<T, GEN>(bv, b1, ii1), I2 = load_invi<T, GEN>(bv, b2, ii2);
+    static_assert(!GEN || std::is_same<BV, BodyV<T>>::value, "full inverse inertias: BodyV only");
     V3<T> t, o;
     V3<T> pold;
     T4<T> q3, q4;
@@ -996,11 +1045,11 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
         }
     }
     cc.p[k] = mk4<T>(pcf.x, pcf.y, pcf.z, T(0));
-    bv.dv[b1] = mk4<T>(dv1.x, dv1.y, dv1.z, T(0));
-    bv.dw[b1] = mk4<T>(dw1.x, dw1.y, dw1.z, T(0));
+    bv.put_dv(b1, mk4<T>(dv1.x, dv1.y, dv1.z, T(0)));
+    bv.put_dw(b1, mk4<T>(dw1.x, dw1.y, dw1.z, T(0)));
     if (b2 >= 0) {
-        bv.dv[b2] = mk4<T>(dv2.x, dv2.y, dv2.z, T(0));
-        bv.dw[b2] = mk4<T>(dw2.x, dw2.y, dw2.z, T(0));
+        bv.put_dv(b2, mk4<T>(dv2.x, dv2.y, dv2.z, T(0)));
+        bv.put_dw(b2, mk4<T>(dw2.x, dw2.y, dw2.z, T(0)));
     }
     if (track_delta) {
         const V3<T> dp = pold - pnew;
@@ -1163,6 +1212,64 @@ __global__ void __launch_bounds__(kClusterBlk) k_sweeps_cluster(int iters, int n
     }
 }
 
+// All sweeps of a step inside one thread-block cluster with the bodies' records in the
+// cluster's distributed shared memory (ClusterBodies: body b in CTA b mod C), so that a
+// colour's body loads and stores take a shared-memory round trip across the cluster instead of
+// an L2 round trip, and the colours are separated by the cluster's hardware barrier.  The
+// contacts' records stay in global memory; a thread handles the same contacts in every sweep,
+// so their read-only records are served by its SM's L1 from the second sweep on.  Every CTA
+// reaches the same barriers (the colour loop is uniform across the cluster), and the gate is
+// read from device memory that no kernel of this launch writes, so all CTAs agree on it.
+constexpr int kDsBlk = 512;
+
+template <typename T, int MODEL>
+__global__ void __launch_bounds__(kDsBlk) k_sweeps_dsmem(int iters, const int32_t *dd, int gate,
+                                                         const int32_t *color_start, int64_t cap,
+                                                         T dtinv, Cache<T> cc, BodyV<T> bv,
+                                                         int64_t nbod, int per, int shift,
+                                                         int track_last,
+                                                         unsigned long long *delta) {
+    namespace cg = cooperative_groups;
+    if (!sweeps_gate(dd, gate)) return;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int32_t cs[kMaxColors + 1];
+    T4<T> *sh = (T4<T> *)smem;
+    const int ncolors = dd[kDdNcolors];
+    const int rank = (int)cluster.block_rank();
+    for (int i = threadIdx.x; i <= ncolors; i += blockDim.x) cs[i] = color_start[i];
+    for (int j = threadIdx.x; j < per; j += blockDim.x) {
+        const int64_t b = ((int64_t)j << shift) + rank;
+        if (b < nbod) {
+            sh[j] = bv.vr[b];
+            sh[per + j] = bv.wr[b];
+            sh[2 * per + j] = bv.dv[b];
+            sh[3 * per + j] = bv.dw[b];
+        }
+    }
+    cluster.sync();
+    ClusterBodies<T> cb{sh, per, shift};
+    const int64_t stride = ((int64_t)blockDim.x) << shift;
+    const int64_t g0 = (int64_t)rank * blockDim.x + threadIdx.x;
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t e = cs[col + 1];
+            for (int64_t k = cs[col] + g0; k < e; k += stride)
+                sweep_contact<T, MODEL, false, false, ClusterBodies<T>>(k, dtinv, cc, cb, track,
+                                                                       delta);
+            cluster.sync();
+        }
+    }
+    for (int j = threadIdx.x; j < per; j += blockDim.x) {
+        const int64_t b = ((int64_t)j << shift) + rank;
+        if (b < nbod) {
+            bv.dv[b] = sh[2 * per + j];
+            bv.dw[b] = sh[3 * per + j];
+        }
+    }
+}
+
 // complementarity residual of the final impulses (same definition as the oracle), in FP64
 template <typename T, bool FRICTION>
 __global__ void k_residual(const int32_t *ncp, int64_t cap, double dtinv, Cache<T> cc,
@@ -1275,6 +1382,10 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
     NbgsBuf &b = c->nb;
     const size_t es = (c->p.precision == PE_B200_FP64) ? 8 : 4;
     const int64_t n = std::max<int64_t>(c->n, 1);
+    const bool gen = c->mb.m > 0;
+    const int64_t nbod = n + c->mb.m;
+    // graphs captured on the buffers replaced below are never launched again
+    if (b.cap < cap || (b.cnt && (b.nbod != nbod || b.gen != gen))) nbgs_graph_free(c);
     if (b.cap < cap) {
         dfree(c, b.cache);
         b.cache = nullptr;
@@ -1293,8 +1404,6 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         b.cap = cap;
     }
     // per-body buffers: spheres, then moving boxes (with inverse inertia rows, GEN)
-    const bool gen = c->mb.m > 0;
-    const int64_t nbod = n + c->mb.m;
     if (b.cnt && (b.nbod != nbod || b.gen != gen)) {
         dfree(c, b.cnt);
         dfree(c, b.body_cnt);
@@ -1533,6 +1642,98 @@ int sweeps_in_cluster(Ctx *c, int model, int iters, int ncolors, int maxcol, int
     return PE_B200_OK;
 }
 
+template <typename VT>
+auto dsmem_kernel(int m) -> decltype(&k_sweeps_dsmem<VT, 0>) {
+    switch (m) {
+        case 1: return k_sweeps_dsmem<VT, 1>;
+        case 2: return k_sweeps_dsmem<VT, 2>;
+        case 3: return k_sweeps_dsmem<VT, 3>;
+        case 4: return k_sweeps_dsmem<VT, 4>;
+        case 5: return k_sweeps_dsmem<VT, 5>;
+        default: return k_sweeps_dsmem<VT, 0>;
+    }
+}
+
+// Launches k_sweeps_dsmem when the bodies' records fit the shared memory of one cluster (16
+// CTAs where the GPU schedules such clusters, else 8); *done reports it.  The feasibility of a
+// (model, precision, body count) is probed once and kept.
+template <typename VT>
+int launch_sweeps_dsmem(Ctx *c, int model, int iters, int gate, int64_t cap, VT dtinv,
+                        const Cache<VT> &cc, const BodyV<VT> &bv, int track,
+                        unsigned long long *dl, bool *done) {
+    NbgsBuf &nb = c->nb;
+    *done = false;
+    if (nb.gen) return PE_B200_OK;
+    auto kern = dsmem_kernel<VT>(model);
+    const int key = model * 2 + (sizeof(VT) == 8 ? 1 : 0);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kDsBlk);
+    cfg.stream = c->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (nb.ds_nbod != nb.nbod || nb.ds_key != key) {
+        nb.ds_nbod = nb.nbod;
+        nb.ds_key = key;
+        nb.ds_size = 0;
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+        for (int size : {16, 8}) {
+            const int64_t per = (nb.nbod + size - 1) / size;
+            const int64_t bytes = 4 * per * (int64_t)sizeof(T4<VT>);
+            if (bytes + (int64_t)(kMaxColors + 1) * 4 + 1024 > optin) continue;
+            if (size > 8 && cudaFuncSetAttribute((const void *)kern,
+                                                 cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                                 1) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if (cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)bytes) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            cfg.gridDim = dim3(size);
+            cfg.dynamicSmemBytes = (size_t)bytes;
+            attr[0].val.clusterDim.x = size;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)kern, &cfg) == cudaSuccess &&
+                nclusters >= 1) {
+                nb.ds_size = size;
+                break;
+            }
+            cudaGetLastError();
+        }
+    }
+    if (nb.ds_size == 0) return PE_B200_OK;
+    const int size = nb.ds_size;
+    const int shift = size == 16 ? 4 : 3;
+    const int64_t per = (nb.nbod + size - 1) / size;
+    const size_t bytes = (size_t)(4 * per) * sizeof(T4<VT>);
+    // the attributes are per kernel: set again, since another body count may have set them
+    if (size > 8)
+        cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaGetLastError();
+    cfg.gridDim = dim3(size);
+    cfg.dynamicSmemBytes = bytes;
+    attr[0].val.clusterDim.x = size;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, iters, (const int32_t *)nb.dd, gate,
+                                             (const int32_t *)nb.cstart_dev, cap, dtinv, cc, bv,
+                                             nb.nbod, (int)per, shift, track, dl);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        nb.ds_size = 0;
+        return PE_B200_OK;
+    }
+    c->launches++;
+    *done = true;
+    return PE_B200_OK;
+}
+
 // The colouring rounds of a queued step in one cooperative launch (k_color_rounds); a grid of
 // as many blocks as fit, at most one thread per contact of the capacity.
 template <typename VT>
@@ -1598,6 +1799,15 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
         block_kernel<VT>(model, gen)<<<1, kBlk, 0, c->stream>>>(iters, dd, 1, nb.cstart_dev, cap,
                                                                 dtinv, cc, bv, n, 0, dl);
         PEB_LAUNCHED(c);
+    }
+    const int mode = c->tune.nbgs_sweeps;
+    if (mode == 0 || mode == 5) {
+        // the colours that do not fit one block: in one cluster's shared memory, if the bodies
+        // fit there
+        bool done = false;
+        int rc = launch_sweeps_dsmem<VT>(c, model, iters, 2, cap, dtinv, cc, bv, 0, dl, &done);
+        if (rc) return rc;
+        if (done) return PE_B200_OK;
     }
     auto kern = persistent_kernel<VT>(model, gen);
     int occ = 0;
@@ -1687,7 +1897,12 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
     int32_t total_s = 0;            // sphere contacts (host-known steps only)
     int32_t *dd = nb.dd;
     const int32_t *ncp = dd + kDdNc;   // the count on the device
-    if (queued) {
+    if (queued && nb.plan_none) {
+        if (n > 0) {
+            k_any_contact<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, dd);
+            PEB_LAUNCHED(c);
+        }
+    } else if (queued) {
         if (n > 0) {
             k_count<<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt);
             PEB_LAUNCHED(c);
@@ -1698,8 +1913,7 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
         } else {
             PEB_CUDA(c, cudaMemsetAsync(dd + kDdNc, 0, sizeof(int32_t), c->stream));
         }
-        // a step planned without contacts (none were found last time) aborts if it finds any
-        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.plan_none ? 0 : nb.cap, dd);
+        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.cap, dd);
         PEB_LAUNCHED(c);
     } else {
         int32_t total_b = 0;
@@ -1734,7 +1948,8 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
         c->last_ncontacts = nc;
     }
     const int64_t cap = nb.cap;
-    if (n > 0) {
+    // a step planned without contacts aborts if it finds any: it writes no records
+    if (n > 0 && !(queued && nb.plan_none)) {
         // a queued step's overflow aborts it instead of reporting an error
         k_raw<VT><<<grid_for(n, kBlk), kBlk, 0, c->stream>>>(n, va, nb.cnt, cap, (const VT *)c->cur.vw,
                                                              c->d_mats, c->d_plane_mat, c->d_box_mat,
@@ -1860,6 +2075,11 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
         if (!done && nb.cluster != 0 && mode == 1 && !gen) {
             int rc = sweeps_in_cluster<VT>(c, model, iters, ncolors, maxcol, cap, VT(1.0 / dt), cc,
                                            bv, n, dl, &done);
+            if (rc) return rc;
+        }
+        if (!done && mode == 5) {
+            int rc = launch_sweeps_dsmem<VT>(c, model, iters, 0, cap, VT(1.0 / dt), cc, bv,
+                                            c->want_residual ? 1 : 0, dl, &done);
             if (rc) return rc;
         }
         if (!done && (mode == 0 || mode == 4) && maxcol <= kBlk) {
@@ -1996,8 +2216,15 @@ void nbgs_free(Ctx *c) {
     dfree(c, b.bar2);
     if (b.color_start) cudaFreeHost(b.color_start);
     if (b.h_dd) cudaFreeHost(b.h_dd);
-    if (b.gexec) cudaGraphExecDestroy(b.gexec);
+    nbgs_graph_free(c);
     b = NbgsBuf();
+}
+
+void nbgs_graph_free(Ctx *c) {
+    for (NbgsBuf::GraphSlot &s : c->nb.gslot) {
+        if (s.exec) cudaGraphExecDestroy(s.exec);
+        s = NbgsBuf::GraphSlot();
+    }
 }
 
 namespace {
@@ -2005,7 +2232,7 @@ namespace {
 // whether the hard-contact steps of this context are queued without host waits
 bool nbgs_queued(const Ctx *c) {
     const int mode = c->tune.nbgs_sweeps;
-    return c->mb.m == 0 && !c->want_residual && (mode == 0 || mode == 2 || mode == 4);
+    return c->mb.m == 0 && !c->want_residual && (mode == 0 || mode == 2 || mode == 4 || mode == 5);
 }
 
 }  // namespace
@@ -2019,9 +2246,10 @@ int nbgs_step(Ctx *c, double dt) {
 
 // Replays of a captured graph of c->graph_steps queued steps (even, so that the buffer swaps
 // cancel) while they fit in nsteps; *ran receives the steps run (0: graphs are off, not
-// possible, or the buffers are fresh).  The graph is captured again when a buffer, a setting it
-// bakes in or the sweep grid changes.  Nothing runs on the device during a capture, so a failed
-// capture only switches graphs off.
+// possible, or the buffers are fresh).  A graph is kept per key (buffers, the settings it bakes
+// in, the plan with or without contacts, the sweep grid), so a scene whose plan or largest
+// colour alternates replays graphs captured before.  Nothing runs on the device during a
+// capture, so a failed capture only switches graphs off.
 int nbgs_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *ran) {
     NbgsBuf &nb = c->nb;
     *ran = 0;
@@ -2042,11 +2270,17 @@ int nbgs_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *ran) {
                               (uint64_t)c->p.max_iterations, (uint64_t)c->p.relaxation_model,
                               erpu.u, dtu.u, (uint64_t)nb.plan_none,
                               (uint64_t)queued_sweep_blocks(c), (uint64_t)gs};
-    bool match = nb.gexec != nullptr;
-    for (int i = 0; i < 12 && match; ++i) match = nb.gkey[i] == key[i];
-    if (!match) {
-        if (nb.gexec) cudaGraphExecDestroy(nb.gexec);
-        nb.gexec = nullptr;
+    NbgsBuf::GraphSlot *hit = nullptr, *lru = &nb.gslot[0];
+    for (NbgsBuf::GraphSlot &s : nb.gslot) {
+        bool match = s.exec != nullptr;
+        for (int i = 0; i < 12 && match; ++i) match = s.key[i] == key[i];
+        if (match) hit = &s;
+        if (!s.exec || (lru->exec && s.used < lru->used)) lru = &s;
+    }
+    if (!hit) {
+        hit = lru;
+        if (hit->exec) cudaGraphExecDestroy(hit->exec);
+        hit->exec = nullptr;
         const BodyBuf cur0 = c->cur, nxt0 = c->nxt;
         const int64_t l0 = c->launches;
         cudaGraph_t g = nullptr;
@@ -2060,11 +2294,10 @@ int nbgs_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *ran) {
         const int64_t per = c->launches - l0;
         c->launches = l0;
         bool ok = e == cudaSuccess && rc == PE_B200_OK && g != nullptr && c->cur.pr == cur0.pr;
-        if (ok) ok = cudaGraphInstantiate(&nb.gexec, g, 0) == cudaSuccess;
+        if (ok) ok = cudaGraphInstantiate(&hit->exec, g, 0) == cudaSuccess;
         if (g) cudaGraphDestroy(g);
         if (!ok) {
-            if (nb.gexec) cudaGraphExecDestroy(nb.gexec);
-            nb.gexec = nullptr;
+            nbgs_graph_free(c);
             nb.gfailed = true;
             c->cur = cur0;
             c->nxt = nxt0;
@@ -2072,12 +2305,14 @@ int nbgs_graph_run(Ctx *c, int32_t nsteps, double dt, int32_t *ran) {
             c->err.clear();
             return PE_B200_OK;
         }
-        for (int i = 0; i < 12; ++i) nb.gkey[i] = key[i];
-        nb.gsteps = gs;
-        nb.glaunches = per;
+        for (int i = 0; i < 12; ++i) hit->key[i] = key[i];
+        hit->launches = per;
+        c->graph_captures++;
     }
-    PEB_CUDA(c, cudaGraphLaunch(nb.gexec, c->stream));
-    c->launches += nb.glaunches;
+    hit->used = ++nb.gclock;
+    PEB_CUDA(c, cudaGraphLaunch(hit->exec, c->stream));
+    c->launches += hit->launches;
+    c->graph_replays++;
     *ran = gs;
     return PE_B200_OK;
 }
@@ -2096,7 +2331,10 @@ int nbgs_run(Ctx *c, int32_t nsteps, double dt) {
     }
     int32_t left = nsteps;
     for (int attempt = 0; left > 0; ++attempt) {
-        if (c->nb.dd) PEB_CUDA(c, cudaMemsetAsync(c->nb.dd + kDdSteps, 0, sizeof(int32_t), c->stream));
+        if (c->nb.dd) {
+            PEB_CUDA(c, cudaMemsetAsync(c->nb.dd + kDdSteps, 0, sizeof(int32_t), c->stream));
+            PEB_CUDA(c, cudaMemsetAsync(c->nb.dd + kDdSeen, 0, sizeof(int32_t), c->stream));
+        }
         int32_t k = 0;
         while (k < left) {
             int32_t ran = 0;
@@ -2117,8 +2355,9 @@ int nbgs_run(Ctx *c, int32_t nsteps, double dt) {
         c->last_ncontacts = nb.h_dd[kDdNc];
         c->last_ncolors = nb.h_dd[kDdNc] > 0 ? nb.h_dd[kDdNcolors] : 0;
         if (!nb.h_dd[kDdAbort]) {
-            // the next call's steps skip the contact stages while the scene has no contacts
-            nb.plan_none = nb.h_dd[kDdNc] == 0;
+            // the next call's steps skip the contact stages while the scene has no contacts:
+            // none in any step of this call
+            nb.plan_none = nb.h_dd[kDdSeen] == 0;
             break;
         }
         const int32_t done = nb.h_dd[kDdSteps];

@@ -6,7 +6,8 @@
 // while the one before them finishes (programmatic dependent launch).  A rebuild runs its stages back to back,
 // separated by grid-wide barriers:
 //   clear cell counts | bin (cell key + slot, atomic histogram) | scan counts -> cell offsets |
-//   scatter | order each cell by body index | gather bodies into cell order | copy back |
+//   scatter | order each cell by body index | gather bodies into cell order (the list buffers'
+//   copy of the state, which the force kernels of the step read instead of the current one) |
 //   count neighbours closer than r_i + r_j + skin (keeping the first few), mark the spheres that
 //   can feel a force before the next rebuild | scan counts -> list offsets | scan marks -> the
 //   marked spheres | write lists
@@ -25,8 +26,7 @@ template <typename VT>
 struct RebuildArgs {
     int64_t n, ncell;
     const SceneInfo *scenes;
-    BodyBuf cur, tmp;
-    double4 *other_pr;
+    BodyBuf cur, tmp;   // the state, and its copy in cell order (the lists index the copy)
     int32_t *key, *rank, *sorted, *cell_count, *cell_start;
     int32_t *cnt, *start, *idx, *stash;
     int64_t cap;
@@ -128,9 +128,9 @@ struct Reach {
 template <typename VT>
 __device__ __forceinline__ Reach reach_of(const RebuildArgs<VT> &a, int64_t t) {
     Reach q;
-    q.p = a.cur.pr[t];
-    q.uid = a.cur.uid[t];
-    q.s = &a.scenes[a.cur.tag[t] >> 16];
+    q.p = a.tmp.pr[t];
+    q.uid = a.tmp.uid[t];
+    q.s = &a.scenes[a.tmp.tag[t] >> 16];
     const SceneInfo &s = *q.s;
     int cx, cy, cz;
     cell_coords(s, q.p.x, q.p.y, q.p.z, cx, cy, cz);
@@ -150,7 +150,7 @@ __device__ __forceinline__ bool within(const double4 &pi, const double4 &pj, dou
 // list entry: the partner's slot, top bit set when body t has the smaller uid
 template <typename VT>
 __device__ __forceinline__ int32_t entry(const RebuildArgs<VT> &a, int32_t uidt, int j) {
-    return (int32_t)((uint32_t)j | (uidt < a.cur.uid[j] ? 0x80000000u : 0u));
+    return (int32_t)((uint32_t)j | (uidt < a.tmp.uid[j] ? 0x80000000u : 0u));
 }
 
 // Emits neighbour k of body t: MODE 0 keeps the first kListStash in the stash, MODE 1 writes
@@ -173,7 +173,7 @@ __device__ int neighbours_serial(const RebuildArgs<VT> &a, int64_t t, int pos, c
             const int64_t c0 = cell_key(s, q.x0, y, z);
             const int e = a.cell_start[c0 + (q.x1 - q.x0) + 1];
             for (int j = a.cell_start[c0]; j < e; ++j) {
-                if (j == t || !within(q.p, a.cur.pr[j], a.skin)) continue;
+                if (j == t || !within(q.p, a.tmp.pr[j], a.skin)) continue;
                 emit<MODE>(a, t, pos, count, entry(a, q.uid, j));
                 ++count;
             }
@@ -215,7 +215,7 @@ __device__ int list_neighbours(const RebuildArgs<VT> &a, int64_t t, int pos) {
         for (int r = 0; r < 9; ++r) {
             if (i < len[r]) {
                 const int j = b[r] + i;
-                if (j != t && within(q.p, a.cur.pr[j], a.skin)) hit[r] |= 1u << i;
+                if (j != t && within(q.p, a.tmp.pr[j], a.skin)) hit[r] |= 1u << i;
             }
         }
     }
@@ -239,6 +239,8 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
     // scheduled while the previous force kernel finishes; its flag is read after it has
     pdl_wait();
     if (!a.flags[0]) {  // uniform: no rebuild requested; the force kernel may start
+        // the force kernels read the current state (flags[4]: the step rebuilt, read the copy)
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.flags[4] = 0;
         pdl_trigger();
         return;
     }
@@ -290,28 +292,17 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
         a.disp[t] = 0.f;
     }
     if (!grid_sync(a.bar, a.err)) return;
-    // 7. copy back (the other position buffer keeps the radius too)
-    for (int64_t t = g0; t < n; t += stride) {
-        const double4 p = a.tmp.pr[t];
-        a.cur.pr[t] = p;
-        a.other_pr[t] = p;
-        cp_vw((VT *)a.cur.vw, t, (const VT *)a.tmp.vw, t, n);
-        a.cur.tag[t] = a.tmp.tag[t];
-        a.cur.uid[t] = a.tmp.uid[t];
-        if (a.cur.q) a.cur.q[t] = a.tmp.q[t];
-    }
-    if (!grid_sync(a.bar, a.err)) return;
-    // 8. neighbour counts; the first kListStash neighbours of each body are kept; the mark of
+    // 7. neighbour counts; the first kListStash neighbours of each body are kept; the mark of
     // every sphere that can feel a force before the next rebuild
     const double margin = 0.5 * a.skin * (1.0 + 1e-9);
     for (int64_t t = g0; t < n; t += stride) {
         const int k = list_neighbours<0, VT>(a, t, 0);
         a.cnt[t] = k;
-        const double4 p = a.cur.pr[t];
-        a.act[t] = list_marked(a.scenes[a.cur.tag[t] >> 16], p, a.boxes, margin, k) ? 1 : 0;
+        const double4 p = a.tmp.pr[t];
+        a.act[t] = list_marked(a.scenes[a.tmp.tag[t] >> 16], p, a.boxes, margin, k) ? 1 : 0;
     }
     if (!grid_sync(a.bar, a.err)) return;
-    // 9. list offsets, and the marked spheres in ascending order
+    // 8. list offsets, and the marked spheres in ascending order
     if (!grid_scan(a, a.cnt, a.start, n)) return;
     if (!grid_sync(a.bar, a.err)) return;
     if (!grid_scan(a, a.act, a.act, n)) return;
@@ -323,9 +314,10 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild(RebuildArgs<VT> a) {
         a.flags[1] = need > a.cap ? 1 : 0;
         a.flags[2] = (int32_t)need;
         a.flags[3] += 1;
+        a.flags[4] = 1;
         a.flags[0] = 0;
     }
-    // 10. write the lists (if they fit; otherwise the force kernel searches the fresh grid):
+    // 9. write the lists (if they fit; otherwise the force kernel searches the fresh grid):
     // copied from the stash, or searched again for bodies with more neighbours than it holds
     if (need <= a.cap)
         for (int64_t t = g0; t < n; t += stride) {
@@ -364,7 +356,6 @@ int launch_rebuild(Ctx *c) {
     a.scenes = c->d_scenes;
     a.cur = c->cur;
     a.tmp = L.tmp;
-    a.other_pr = c->nxt.pr;
     a.key = c->key;
     a.rank = c->rank;
     a.sorted = c->sorted;

@@ -250,6 +250,12 @@ class Engine:
     def graph_active(self) -> bool:
         return bool(self._L.pe_b200_graph_active(self._h))
 
+    def graph_stats(self) -> dict:
+        """Graphs captured and graph launches since the context was created."""
+        cap, rep = C.c_int64(), C.c_int64()
+        self._check(self._L.pe_b200_graph_stats(self._h, C.byref(cap), C.byref(rep)))
+        return {"captures": cap.value, "replays": rep.value}
+
     def tuning(self) -> dict:
         t = _abi.Tuning()
         self._check(self._L.pe_b200_get_tuning(self._h, C.byref(t)))

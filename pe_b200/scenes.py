@@ -322,6 +322,26 @@ def dem_large(seed: int = 0, n: int = 1048576, dims=(200.0, 200.0, 400.0)) -> Sc
                   5e-5, 1000, f"dem_large_{n}")
 
 
+def dem_dense(seed: int = 0, nx: int = 128, ny: int = 128, nz: int = 64) -> Scene:
+    """Contact-dense DEM: nx*ny*nz spheres (1,048,576 by default) on a simple cubic lattice of
+    spacing 1.0 with radii U[0.495, 0.505], so most lattice neighbours start in contact, filling
+    the lower half of a box of planes whose side walls touch the outer spheres; velocities
+    N(0, 0.5^2); k_n=1e5, c_n=50, mu=0.4, dt=5e-5.  Every sphere feels contact forces every step
+    and the released overlaps keep the packing agitated, so the lists are rebuilt often."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    idx = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"),
+                   axis=-1).reshape(-1, 3).astype(float)
+    x = idx + 0.5
+    r = rng.uniform(0.495, 0.505, size=n)
+    v = rng.normal(0.0, 0.5, size=(n, 3))
+    dims = np.array([float(nx), float(ny), 2.0 * nz])
+    planes = box_planes([0, 0, 0], dims)
+    mats = [material(1.0, 1e5, 50.0, 50.0, 0.4)]
+    return _scene(x, v, r, np.zeros(n), planes, np.zeros(6), np.zeros((0, 15)), [], mats, G,
+                  5e-5, 1000, f"dem_dense_{n}")
+
+
 def batched_ensemble(seed: int = 0, scenes: int = 512, nmin: int = 1024,
                      nmax: int = 65536) -> List[Scene]:
     """Batched ensemble: independent DEM scenes with body counts log-uniform in [nmin, nmax],

@@ -128,11 +128,12 @@ def test_list_overflow_falls_back_to_the_grid(precision):
 @pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
 @pytest.mark.parametrize("model", [0, 1])
 def test_nbgs_sweep_forms_agree(precision, model):
-    """One cluster, one cooperative grid and one launch per colour run the same colour order,
-    and the contacts of a colour share no body: the results are identical."""
+    """One cluster, one cooperative grid, one launch per colour and one cluster with the bodies
+    in its shared memory run the same colour order, and the contacts of a colour share no body:
+    the results are identical."""
     s = scenes.nbgs_box(0, n=4096, dims=(16.0, 16.0, 40.0), dense=True)
     out = []
-    for mode in (1, 2, 3):
+    for mode in (1, 2, 3, 5):
         e = Engine(solver=_abi.HCSITS, precision=precision, relaxation_model=model,
                    max_iterations=30).load_scene(s)
         e.set_tuning(nbgs_sweeps=mode)
@@ -304,3 +305,22 @@ def test_hard_contact_graph_replay_matches_step_by_step(precision):
             e.close()
         for a, b in zip(out[0], out[1]):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_hard_contact_graphs_are_kept_across_calls():
+    """Calls of 32 hard-contact steps replay the graphs captured by earlier calls: the plan
+    (with or without contacts) and the sweep grid each key a graph of their own."""
+    sc = scenes.nbgs_box(2, n=2000, dims=(12.0, 12.0, 30.0), dense=True)
+    e = Engine(solver=_abi.HCSITS, precision=_abi.MIXED, relaxation_model=1,
+               max_iterations=30).load_scene(sc)
+    e.step(sc.dt, 2)
+    e.step(sc.dt, 32)
+    g0 = e.graph_stats()
+    assert g0["captures"] >= 1
+    for _ in range(6):
+        e.step(sc.dt, 32)
+    g1 = e.graph_stats()
+    assert g1["replays"] - g0["replays"] >= 12
+    assert g1["captures"] - g0["captures"] <= 3
+    e.close()
