@@ -895,7 +895,7 @@ PROFILE_CASES = {
     # the plain FP64 grid step (sort + k_dem_sorted) on the 1M scene
     "dem_grid_fp64": ("dem", 1048576, "fp64", False),
     "dem_grid_mixed": ("dem", 1048576, "mixed", False),
-    # the headline list step (k_dem_list, k_rebuild) on the full 1M scene
+    # the headline list step (k_rebuild, k_dem_contacts, k_dem_move) on the full 1M scene
     "dem_list_mixed": ("dem", 1048576, "mixed", True),
     "dem_list_fp64": ("dem", 1048576, "fp64", True),
     # the contact-dense 1M scene (every sphere in contact, frequent rebuilds)

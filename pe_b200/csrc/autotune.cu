@@ -4,7 +4,7 @@
 // The tunables change only how the work is laid out on the GPU, never which pairs a body sums
 // or in which order, except for the skin, which changes when the state is re-sorted and so the
 // last bits of the forces:
-//   dem_variant     threads per block / resident blocks per SM of k_dem_list (dem.cu)
+//   dem_variant     threads per block / resident blocks per SM of k_dem_move (dem.cu)
 //   rebuild_per_sm  CTAs per SM of the persistent rebuild kernel (rebuild.cu); -1 rebuilds with
 //                   one launch per stage instead (the same lists, entry for entry)
 //   skin            neighbour-list skin (cells are re-planned to 2 r_max + skin)

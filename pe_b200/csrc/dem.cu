@@ -18,15 +18,16 @@
 //   grid   (k_dem_step) every step: the counting-sorted uniform grid, 27 cells per sphere; the
 //          thread owning sorted slot t writes its body to slot t of the other buffer, so the
 //          state is re-sorted by cell as a side effect, and it bins the result for the next sort.
-//   lists  (k_dem_list) Verlet lists: all pairs closer than r_i + r_j + skin when the list was
-//          built.  A sphere's accumulated path length is tracked; once any sphere has moved
-//          skin/2 the device requests a rebuild, which the next step performs (sort, permute to
-//          cell order, count/scan/write the lists) before its force kernel.  Every pair that can
-//          come within the contact threshold is therefore in the list, and the pair set is the
-//          grid's, exactly.  The rebuild kernels run every step and return at once unless
-//          requested, so the host never waits on the device to decide.  If a rebuild overflows
-//          the list capacity, that step's force kernel searches the fresh grid instead (exact)
-//          and the host grows the capacity at its next check.
+//   lists  (k_dem_contacts + k_dem_move) Verlet lists: all pairs closer than r_i + r_j + skin
+//          when the list was built.  A sphere's accumulated path length is tracked; once any
+//          sphere has moved skin/2 the device requests a rebuild, which the next step performs
+//          (sort, gather into cell order, count/scan/write the lists, mark the spheres that can
+//          feel a force) before its force kernels.  Every pair that can come within the contact
+//          threshold is therefore in the list, and the pair set is the grid's, exactly.  The
+//          rebuild kernel runs every step and returns at once unless requested, so the host
+//          never waits on the device to decide.  If a rebuild overflows the list capacity, that
+//          step's contact kernel searches the fresh grid instead (exact) and the host grows the
+//          capacity at its next check.
 #include <math_constants.h>
 
 #include <algorithm>
@@ -758,20 +759,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
     // here on (it waits for this kernel in turn)
     pdl_wait();
     pdl_trigger();
+    // whether this step rebuilt the lists (its state is then the copy in cell order); loaded
+    // beside the current state, which is read at once and read again from the copy only after
+    // a rebuild, so that the common step's loads do not wait for the flag
     const bool rebuilt = a0.nl_flags[4] != 0;
-    const DemArgs<VT> a = list_view(a0);
+    DemArgs<VT> a = a0;
     bool moved = false;
     if (t < a.n) {
         // every load of this body's own records first: they are independent, and none may
         // wait behind this thread's stores
-        const double4 pi = a.pr[t];
-        const uint32_t tagi = ONE ? 0u : a.tag[t];
-        const V3<T> vi = ld_vw(a.vw, a.n, t, 0), wi = ld_vw(a.vw, a.n, t, 1);
-        uint32_t ext = ld_ext(a.vw, a.n, t);
+        double4 pi = a0.pr[t];
+        uint32_t tagi = ONE ? 0u : a0.tag[t];
+        V3<T> vi = ld_vw(a0.vw, a.n, t, 0), wi = ld_vw(a0.vw, a.n, t, 1);
+        uint32_t ext = ld_ext(a0.vw, a.n, t);
         const int32_t m = a.act[t];
         const bool marked = a.act[t + 1] > m;
         const float disp0 = a.disp[t];
-        const MatDev &mi = ONE ? a.m0 : a.mats[tagi & 0xffffu];
         Acc<T> acc;
         acc.F = v3(T(0), T(0), T(0));
         acc.T_ = acc.F;
@@ -780,10 +783,18 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
             acc.F = v3(a.facc[m], a.facc[cap + m], a.facc[2 * cap + m]);
             acc.T_ = v3(a.facc[3 * cap + m], a.facc[4 * cap + m], a.facc[5 * cap + m]);
         }
-        if (rebuilt) {   // the reordered tags and ids replace the current ones
-            a.tag_out[t] = ONE ? a.tag[t] : tagi;
-            a.uid_out[t] = a.uid[t];
+        if (rebuilt) {
+            pi = a0.alt_pr[t];
+            tagi = a0.alt_tag[t];
+            vi = ld_vw(a0.alt_vw, a.n, t, 0);
+            wi = ld_vw(a0.alt_vw, a.n, t, 1);
+            ext = ld_ext(a0.alt_vw, a.n, t);
+            a.q = a0.alt_q;
+            // the reordered tags and ids replace the current ones
+            a.tag_out[t] = tagi;
+            a.uid_out[t] = a0.alt_uid[t];
         }
+        const MatDev &mi = ONE ? a.m0 : a.mats[tagi & 0xffffu];
         V3<T> v, w;
         const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w, ext);
         // whole 32-byte records: a partial sector write would make L2 fetch the sector first

@@ -168,7 +168,7 @@ struct ListBuf {
 
 // launch shapes of the DEM list step, picked by pe_b200_autotune (autotune.cu)
 struct Tuning {
-    int32_t dem_variant = 0;    // index into the k_dem_list launch shapes (dem.cu)
+    int32_t dem_variant = 0;    // index into the k_dem_move launch shapes (dem.cu)
     int32_t rebuild_per_sm = 0; // persistent rebuild CTAs per SM; 0 = as many as fit
     int32_t nbgs_sweeps = 0;    // 0 automatic, 1 one cluster, 2 cooperative grid, 3 per colour,
                                 // 4 one block, 5 bodies in one cluster's shared memory

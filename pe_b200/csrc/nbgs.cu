@@ -32,7 +32,12 @@ namespace {
 constexpr int kBlk = 256;
 constexpr int kMaxColors = 256;   // colours of one step (8 bits in the packed colour)
 constexpr size_t kBlockSmemMax = 200 * 1024;   // shared memory of the single-block sweep form
-constexpr int64_t kSerialColourMax = 8192;      // contacts coloured by one thread in one launch
+// contacts coloured by one thread in one launch: scenes with moving boxes (where it saves many
+// colours), and sphere scenes with the bodies' colour masks in shared memory or in global memory
+// (every contact's mask update is then an L2 round trip)
+constexpr int64_t kSerialColourMax = 8192;
+constexpr int64_t kSerialColourMaxSpheres = 512;
+constexpr int64_t kSerialColourMaxGlobal = 128;
 constexpr int kMaxRounds = 4096;                // rounds of the parallel colouring
 // device counters of a step (NbgsBuf.dd)
 enum : int {
@@ -503,15 +508,15 @@ __global__ void k_color_settle(const int32_t *ncp, int round, const int32_t *b1,
 // All rounds of the parallel colouring in one cooperative launch, for steps queued without
 // the host: rounds separated by bounded grid barriers until a round leaves no contact
 // uncoloured (rem: one counter per round, zeroed before the launch).  Does nothing when the
-// one-thread colouring handles the step (at most kSerialColourMax contacts).
+// one-thread colouring handles the step (at most serial_max contacts).
 template <int W>
-__global__ void k_color_rounds(const int32_t *ncp, const int32_t *dd, const int32_t *b1,
-                               const int32_t *b2, const int32_t *adj_start, const int32_t *adj,
-                               int32_t *tent, int32_t *color, uint64_t *used, int32_t *rem,
-                               unsigned int *bar, int32_t *err) {
+__global__ void k_color_rounds(const int32_t *ncp, const int32_t *dd, int64_t serial_max,
+                               const int32_t *b1, const int32_t *b2, const int32_t *adj_start,
+                               const int32_t *adj, int32_t *tent, int32_t *color, uint64_t *used,
+                               int32_t *rem, unsigned int *bar, int32_t *err) {
     if (dd[kDdAbort]) return;
     const int64_t nc = *ncp;
-    if (nc <= kSerialColourMax) return;
+    if (nc <= serial_max) return;
     for (int round = 0; round < kMaxRounds; ++round) {
         GRID_STRIDE(c, nc) color_propose<W>(c, b1, b2, color, used, tent, err);
         if (!grid_sync(bar, err)) return;
@@ -530,13 +535,13 @@ __global__ void k_color_rounds(const int32_t *ncp, const int32_t *dd, const int3
 // The used-colour masks live in shared memory when they fit (used_global == null), else in
 // the zeroed global array.
 template <int W>
-__global__ void k_color_serial(const int32_t *ncp, const int32_t *dd,
+__global__ void k_color_serial(const int32_t *ncp, const int32_t *dd, int64_t serial_max,
                                const int32_t *__restrict__ b1, const int32_t *__restrict__ b2,
                                int32_t *__restrict__ color, int64_t nbod, uint64_t *used_global,
                                int32_t *err) {
     if (dd[kDdAbort]) return;
     const int64_t nc = *ncp;
-    if (nc > kSerialColourMax) return;   // the parallel rounds colour this step
+    if (nc > serial_max) return;   // the parallel rounds colour this step
     extern __shared__ uint64_t used_shared[];
     uint64_t *used = used_global ? used_global : used_shared;
     if (!used_global)
@@ -1738,7 +1743,7 @@ int launch_sweeps_dsmem(Ctx *c, int model, int iters, int gate, int64_t cap, VT 
 // as many blocks as fit, at most one thread per contact of the capacity.
 template <typename VT>
 int launch_color_rounds(Ctx *c, const int32_t *ncp, int32_t *dd, const Raw<VT> &raw,
-                        int64_t cap) {
+                        int64_t cap, int64_t serial_max) {
     NbgsBuf &nb = c->nb;
     static int occ = 0;
     if (occ == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_color_rounds<1>, kBlk,
@@ -1751,7 +1756,8 @@ int launch_color_rounds(Ctx *c, const int32_t *ncp, int32_t *dd, const Raw<VT> &
     int32_t *color = nb.color, *rem = nb.rem, *err = c->d_err;
     uint64_t *used = nb.used;
     unsigned int *bar = nb.bar2;
-    void *args[] = {&ncp, &dd, &b1, &b2, &adj_start, &adj, &tent, &color, &used, &rem, &bar, &err};
+    void *args[] = {&ncp, &dd, &serial_max, &b1, &b2, &adj_start, &adj, &tent, &color, &used,
+                    &rem, &bar, &err};
     PEB_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_color_rounds<1>, dim3(grid),
                                             dim3(kBlk), args, 0, c->stream));
     c->launches++;
@@ -1985,22 +1991,26 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
         PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)nbod * words * sizeof(uint64_t), c->stream));
         const size_t masks = (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t);
         const bool in_smem = masks <= 48 * 1024;
+        const int64_t serial_max = gen ? kSerialColourMax
+                                       : (in_smem ? kSerialColourMaxSpheres : kSerialColourMaxGlobal);
         if (queued) {
             // one thread for a few contacts; otherwise every round in one cooperative launch
             k_color_serial<1><<<1, 256, in_smem ? masks : 0, c->stream>>>(
-                ncp, dd, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used, c->d_err);
+                ncp, dd, serial_max, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used,
+                c->d_err);
             PEB_LAUNCHED(c);
             PEB_CUDA(c, cudaMemsetAsync(nb.rem, 0, kMaxRounds * sizeof(int32_t), c->stream));
-            rc = launch_color_rounds(c, ncp, dd, raw, cap);
+            rc = launch_color_rounds(c, ncp, dd, raw, cap, serial_max);
             if (rc) return rc;
         } else {
             int round = 0;
-            if (nc <= kSerialColourMax) {
+            if (nc <= serial_max) {
                 (gen ? k_color_serial<4> : k_color_serial<1>)<<<1, 256, in_smem ? masks : 0, c->stream>>>(
-                    ncp, dd, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used, c->d_err);
+                    ncp, dd, serial_max, raw.b1, raw.b2, nb.color, nbod, in_smem ? nullptr : nb.used,
+                    c->d_err);
                 PEB_LAUNCHED(c);
             }
-            for (; nc > kSerialColourMax;) {
+            for (; nc > serial_max;) {
                 const int batch = 8;
                 PEB_CUDA(c, cudaMemsetAsync(nb.flags, 0, batch * sizeof(int32_t), c->stream));
                 int32_t *tent = nb.order;   // free until the colour sort below
