@@ -20,8 +20,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fopenmp", "--expt-relaxed-constexpr",
               "-I" + INCLUDE]
 # per-file flags: the box fine detection rounds every product and sum separately, as pe's FP64
-# code does (its case selection compares depths that tie for aligned boxes)
-FILE_FLAGS = {"boxes.cu": ["-fmad=false"]}
+# code does (its case selection compares depths that tie for aligned boxes); so do the
+# hard-contact kernels, whose sweep forms must give the same bits in every kernel they are
+# compiled into (contracted multiply-adds are chosen per kernel by the compiler)
+FILE_FLAGS = {"boxes.cu": ["-fmad=false"], "nbgs.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

@@ -1071,8 +1071,20 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
+    // the contact kernel strides over the marked spheres, whose count only the device knows:
+    // as many blocks as stay resident (all spheres may be marked in a contact-dense scene)
+    static int occ[2] = {0, 0};
+    int &oc = occ[one ? 1 : 0];
+    if (oc == 0) {
+        const void *kc = one ? (const void *)k_dem_contacts<VT, HERTZ, true>
+                             : (const void *)k_dem_contacts<VT, HERTZ, false>;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oc, kc, 128, 0) != cudaSuccess || oc < 1) {
+            cudaGetLastError();
+            oc = 4;
+        }
+    }
     cudaLaunchConfig_t cc = {};
-    cc.gridDim = dim3((unsigned)std::min<int64_t>(grid_for(c->n, 128), 4 * (int64_t)c->sm_count));
+    cc.gridDim = dim3((unsigned)std::min<int64_t>(grid_for(c->n, 128), (int64_t)oc * c->sm_count));
     cc.blockDim = dim3(128);
     cc.stream = c->stream;
     cc.attrs = at;

@@ -104,6 +104,7 @@ struct NbgsBuf {
     int64_t ds_nbod = -1;
     int ds_key = -1;
     int ds_size = 0;
+    int ds_optin = 0;               // shared memory a block may opt in to
     void *vel = nullptr;                      // v', w', dv, dw per body (VT[12])
     int64_t nbod = 0;                         // bodies the per-body buffers hold
     bool gen = false;                         // they hold world-frame inverse inertias too

@@ -164,6 +164,29 @@ struct Cache {
     T4<T> *p;     // impulse in the contact frame (n, t, o, -)
     T4<T> *dc;    // 2 per contact: Delassus block in the contact frame [xy xz yy yz] [zz - - -]
                   // (its xx is rec[2].w), read by relaxation models 2-5 only
+    // the sweeps' accessors
+    __device__ __forceinline__ int2 get_ids(int64_t k) const { return ids[k]; }
+    __device__ __forceinline__ const T4<T> *rec_of(int64_t k) const { return rec + (int64_t)kRec * k; }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_p(int64_t k) const { return COH ? ldcg4(p + k) : p[k]; }
+    __device__ __forceinline__ void put_p(int64_t k, const T4<T> &v) const { p[k] = v; }
+    __device__ __forceinline__ const T4<T> *dc_of(int64_t k) const { return dc + 2 * k; }
+};
+
+// A block's own copy of the records of the contacts it sweeps, in shared memory, indexed by the
+// block's local slot: the first NREC records of each contact (3 for the frictionless sweep, 7
+// with friction; relaxation models 0 and 1 only).
+template <typename T, int NREC>
+struct SmemContacts {
+    int2 *ids;
+    T4<T> *rec;
+    T4<T> *p;
+    __device__ __forceinline__ int2 get_ids(int64_t k) const { return ids[k]; }
+    __device__ __forceinline__ const T4<T> *rec_of(int64_t k) const { return rec + (int64_t)NREC * k; }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_p(int64_t k) const { return p[k]; }
+    __device__ __forceinline__ void put_p(int64_t k, const T4<T> &v) const { p[k] = v; }
+    __device__ __forceinline__ const T4<T> *dc_of(int64_t) const { return nullptr; }
 };
 
 // Per body, slot order: velocities after the predictor with 1/m, 1/I (read-only in the sweeps)
@@ -192,22 +215,46 @@ struct BodyV {
 // lives in CTA b mod C (C = 2^shift, the cluster size) at row slot b / C, and is reached
 // through distributed shared memory from every CTA of the cluster.  Rows: vr, wr, dv, dw, each
 // `per` records long.
+// loads and stores of a 4-vector at a shared::cluster address (mapa of a shared::cta address)
+__device__ __forceinline__ float4 ld_dsm(uint32_t a, float) {
+    float4 v;
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ double4 ld_dsm(uint32_t a, double) {
+    double4 v;
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a) : "memory");
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.z), "=d"(v.w) : "r"(a + 16) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_dsm(uint32_t a, const float4 &v) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};"
+                 :: "r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+}
+__device__ __forceinline__ void st_dsm(uint32_t a, const double4 &v) {
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" :: "r"(a), "d"(v.x), "d"(v.y) : "memory");
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" :: "r"(a + 16), "d"(v.z), "d"(v.w) : "memory");
+}
+
 template <typename T>
 struct ClusterBodies {
-    T4<T> *sh;
+    uint32_t base;   // shared::cta address of this CTA's rows (the same offset in every CTA)
     int per, shift;
-    __device__ __forceinline__ T4<T> *at(int row, int32_t b) const {
-        T4<T> *p = sh + (int64_t)row * per + (b >> shift);
-        return cooperative_groups::this_cluster().map_shared_rank(p, (unsigned)(b & ((1 << shift) - 1)));
+    __device__ __forceinline__ uint32_t at(int row, int32_t b) const {
+        const uint32_t a = base + (uint32_t)(((int64_t)row * per + (b >> shift)) * sizeof(T4<T>));
+        uint32_t r;
+        asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"((uint32_t)(b & ((1 << shift) - 1))));
+        return r;
     }
-    __device__ __forceinline__ T4<T> get_vr(int32_t b) const { return *at(0, b); }
-    __device__ __forceinline__ T4<T> get_wr(int32_t b) const { return *at(1, b); }
+    __device__ __forceinline__ T4<T> get_vr(int32_t b) const { return ld_dsm(at(0, b), T(0)); }
+    __device__ __forceinline__ T4<T> get_wr(int32_t b) const { return ld_dsm(at(1, b), T(0)); }
     template <bool COH>
-    __device__ __forceinline__ T4<T> get_dv(int32_t b) const { return *at(2, b); }
+    __device__ __forceinline__ T4<T> get_dv(int32_t b) const { return ld_dsm(at(2, b), T(0)); }
     template <bool COH>
-    __device__ __forceinline__ T4<T> get_dw(int32_t b) const { return *at(3, b); }
-    __device__ __forceinline__ void put_dv(int32_t b, const T4<T> &v) const { *at(2, b) = v; }
-    __device__ __forceinline__ void put_dw(int32_t b, const T4<T> &v) const { *at(3, b) = v; }
+    __device__ __forceinline__ T4<T> get_dw(int32_t b) const { return ld_dsm(at(3, b), T(0)); }
+    __device__ __forceinline__ void put_dv(int32_t b, const T4<T> &v) const { st_dsm(at(2, b), v); }
+    __device__ __forceinline__ void put_dw(int32_t b, const T4<T> &v) const { st_dsm(at(3, b), v); }
 };
 
 // a body's inverse inertia applied to a vector: the scalar of a sphere, or (GEN) the full
@@ -913,18 +960,19 @@ __device__ __forceinline__ V3<T> solve_gmd(V3<T> pcf, const V3<T> &g, const T D[
 
 // one contact of one sweep of relaxation model MODEL (pe's RelaxationModel, HCSITS.h:172-179);
 // COHERENT: read the velocity corrections and the impulse from L2
-template <typename T, int MODEL, bool COHERENT, bool GEN = false, typename BV = BodyV<T>>
-__device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T> &cc,
+template <typename T, int MODEL, bool COHERENT, bool GEN = false, typename BV = BodyV<T>,
+          typename CC = Cache<T>>
+__device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const CC &cc,
                                               const BV &bv, int track_delta,
                                               unsigned long long *delta) {
     constexpr bool FRICTION = MODEL != 0;
-    const int2 ids = cc.ids[k];
+    const int2 ids = cc.get_ids(k);
     const int32_t b1 = ids.x, b2 = ids.y;
-    const T4<T> *R = cc.rec + (int64_t)kRec * k;
+    const T4<T> *R = cc.rec_of(k);
     const T4<T> q0 = R[0], q1 = R[1], q2 = R[2];
     const V3<T> n = xyz<T>(q0), r1 = xyz<T>(q1), r2 = xyz<T>(q2);
     const T dist = q0.w, dn_inv = q1.w;
-    const T4<T> pc4 = COHERENT ? ldcg4(cc.p + k) : cc.p[k];
+    const T4<T> pc4 = cc.template get_p<COHERENT>(k);
     const V3<T> pc = xyz<T>(pc4);  // contact frame
     const T4<T> vr1 = bv.get_vr(b1), wr1 = bv.get_wr(b1);
     const T im1 = vr1.w, ii1 = wr1.w;
@@ -1013,7 +1061,8 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
     } else {
         const T mu = q3.w;
         const V3<T> g = v3(gn, dot(t, gdot), dot(o, gdot));
-        const T4<T> d0 = cc.dc[2 * k], d1 = cc.dc[2 * k + 1];
+        const T4<T> *dck = cc.dc_of(k);
+        const T4<T> d0 = dck[0], d1 = dck[1];
         const T D[6] = {q2.w, d0.x, d0.y, d0.z, d0.w, d1.x};   // xx xy xz yy yz zz
         if (MODEL == 2 || MODEL == 4) {
             pcf = solve_orthogonal<T, MODEL == 4>(pc, g, D, mu);
@@ -1049,7 +1098,7 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const Cache<T>
             dw2 = dw2 - I2(cross(r2, pnew));
         }
     }
-    cc.p[k] = mk4<T>(pcf.x, pcf.y, pcf.z, T(0));
+    cc.put_p(k, mk4<T>(pcf.x, pcf.y, pcf.z, T(0)));
     bv.put_dv(b1, mk4<T>(dv1.x, dv1.y, dv1.z, T(0)));
     bv.put_dw(b1, mk4<T>(dw1.x, dw1.y, dw1.z, T(0)));
     if (b2 >= 0) {
@@ -1220,29 +1269,44 @@ __global__ void __launch_bounds__(kClusterBlk) k_sweeps_cluster(int iters, int n
 // All sweeps of a step inside one thread-block cluster with the bodies' records in the
 // cluster's distributed shared memory (ClusterBodies: body b in CTA b mod C), so that a
 // colour's body loads and stores take a shared-memory round trip across the cluster instead of
-// an L2 round trip, and the colours are separated by the cluster's hardware barrier.  The
-// contacts' records stay in global memory; a thread handles the same contacts in every sweep,
-// so their read-only records are served by its SM's L1 from the second sweep on.  Every CTA
-// reaches the same barriers (the colour loop is uniform across the cluster), and the gate is
-// read from device memory that no kernel of this launch writes, so all CTAs agree on it.
+// an L2 round trip, and the colours are separated by the cluster's hardware barrier.  CTA r
+// sweeps the r-th of C equal chunks of every colour.  STAGE (relaxation models 0 and 1): the
+// records of the CTA's contacts are copied into its shared memory before the sweeps (as many as
+// fit, scap; the rest are read from global memory) and their impulses written back after, so a
+// colour touches no global memory.  Every CTA reaches the same barriers (the colour loop is
+// uniform across the cluster), and the gate is read from device memory that no kernel of this
+// launch writes, so all CTAs agree on it.
 constexpr int kDsBlk = 512;
 
-template <typename T, int MODEL>
+template <typename T, int MODEL, bool STAGE>
 __global__ void __launch_bounds__(kDsBlk) k_sweeps_dsmem(int iters, const int32_t *dd, int gate,
                                                          const int32_t *color_start, int64_t cap,
                                                          T dtinv, Cache<T> cc, BodyV<T> bv,
                                                          int64_t nbod, int per, int shift,
-                                                         int track_last,
+                                                         int scap, int track_last,
                                                          unsigned long long *delta) {
     namespace cg = cooperative_groups;
+    static_assert(!STAGE || MODEL <= 1, "staged records: relaxation models 0 and 1");
+    constexpr int NREC = MODEL == 0 ? 3 : 7;
     if (!sweeps_gate(dd, gate)) return;
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int32_t cs[kMaxColors + 1];
+    __shared__ int32_t lo_s[kMaxColors], n_s[kMaxColors], off_s[kMaxColors];
     T4<T> *sh = (T4<T> *)smem;
     const int ncolors = dd[kDdNcolors];
     const int rank = (int)cluster.block_rank();
-    for (int i = threadIdx.x; i <= ncolors; i += blockDim.x) cs[i] = color_start[i];
+    const int C = 1 << shift;
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t b0 = color_start[col], len = color_start[col + 1] - b0;
+            const int lo = (int)(b0 + len * rank / C), hi = (int)(b0 + len * (rank + 1) / C);
+            lo_s[col] = lo;
+            n_s[col] = hi - lo;
+            off_s[col] = off;
+            off += hi - lo;
+        }
+    }
     for (int j = threadIdx.x; j < per; j += blockDim.x) {
         const int64_t b = ((int64_t)j << shift) + rank;
         if (b < nbod) {
@@ -1252,17 +1316,36 @@ __global__ void __launch_bounds__(kDsBlk) k_sweeps_dsmem(int iters, const int32_
             sh[3 * per + j] = bv.dw[b];
         }
     }
+    SmemContacts<T, NREC> sc;
+    sc.rec = sh + 4 * (int64_t)per;
+    sc.p = sc.rec + (int64_t)NREC * scap;
+    sc.ids = (int2 *)(sc.p + scap);
+    __syncthreads();
+    if (STAGE) {
+        for (int col = 0; col < ncolors; ++col)
+            for (int i = threadIdx.x; i < n_s[col]; i += blockDim.x) {
+                const int local = off_s[col] + i;
+                if (local >= scap) break;
+                const int64_t k = lo_s[col] + i;
+                sc.ids[local] = cc.ids[k];
+                for (int q = 0; q < NREC; ++q) sc.rec[(int64_t)NREC * local + q] = cc.rec[(int64_t)kRec * k + q];
+                sc.p[local] = cc.p[k];
+            }
+    }
     cluster.sync();
-    ClusterBodies<T> cb{sh, per, shift};
-    const int64_t stride = ((int64_t)blockDim.x) << shift;
-    const int64_t g0 = (int64_t)rank * blockDim.x + threadIdx.x;
+    ClusterBodies<T> cb{(uint32_t)__cvta_generic_to_shared(sh), per, shift};
     for (int it = 0; it < iters; ++it) {
         const int track = (track_last && it == iters - 1) ? 1 : 0;
         for (int col = 0; col < ncolors; ++col) {
-            const int64_t e = cs[col + 1];
-            for (int64_t k = cs[col] + g0; k < e; k += stride)
-                sweep_contact<T, MODEL, false, false, ClusterBodies<T>>(k, dtinv, cc, cb, track,
-                                                                       delta);
+            const int n = n_s[col], lo = lo_s[col], off = off_s[col];
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                if (STAGE && off + i < scap)
+                    sweep_contact<T, MODEL, false, false, ClusterBodies<T>, SmemContacts<T, NREC>>(
+                        off + i, dtinv, sc, cb, track, delta);
+                else
+                    sweep_contact<T, MODEL, false, false, ClusterBodies<T>>(lo + i, dtinv, cc, cb,
+                                                                           track, delta);
+            }
             cluster.sync();
         }
     }
@@ -1272,6 +1355,14 @@ __global__ void __launch_bounds__(kDsBlk) k_sweeps_dsmem(int iters, const int32_
             bv.dv[b] = sh[2 * per + j];
             bv.dw[b] = sh[3 * per + j];
         }
+    }
+    if (STAGE) {
+        for (int col = 0; col < ncolors; ++col)
+            for (int i = threadIdx.x; i < n_s[col]; i += blockDim.x) {
+                const int local = off_s[col] + i;
+                if (local >= scap) break;
+                cc.p[lo_s[col] + i] = sc.p[local];
+            }
     }
 }
 
@@ -1648,20 +1739,23 @@ int sweeps_in_cluster(Ctx *c, int model, int iters, int ncolors, int maxcol, int
 }
 
 template <typename VT>
-auto dsmem_kernel(int m) -> decltype(&k_sweeps_dsmem<VT, 0>) {
+auto dsmem_kernel(int m, bool stage) -> decltype(&k_sweeps_dsmem<VT, 0, false>) {
+    if (stage && m == 0) return k_sweeps_dsmem<VT, 0, true>;
+    if (stage && m == 1) return k_sweeps_dsmem<VT, 1, true>;
     switch (m) {
-        case 1: return k_sweeps_dsmem<VT, 1>;
-        case 2: return k_sweeps_dsmem<VT, 2>;
-        case 3: return k_sweeps_dsmem<VT, 3>;
-        case 4: return k_sweeps_dsmem<VT, 4>;
-        case 5: return k_sweeps_dsmem<VT, 5>;
-        default: return k_sweeps_dsmem<VT, 0>;
+        case 1: return k_sweeps_dsmem<VT, 1, false>;
+        case 2: return k_sweeps_dsmem<VT, 2, false>;
+        case 3: return k_sweeps_dsmem<VT, 3, false>;
+        case 4: return k_sweeps_dsmem<VT, 4, false>;
+        case 5: return k_sweeps_dsmem<VT, 5, false>;
+        default: return k_sweeps_dsmem<VT, 0, false>;
     }
 }
 
 // Launches k_sweeps_dsmem when the bodies' records fit the shared memory of one cluster (16
-// CTAs where the GPU schedules such clusters, else 8); *done reports it.  The feasibility of a
-// (model, precision, body count) is probed once and kept.
+// CTAs where the GPU schedules such clusters, else 8), with as many of its contacts' records
+// staged beside them as fit; *done reports it.  The plan for a (model, precision, body count)
+// is probed once and kept.
 template <typename VT>
 int launch_sweeps_dsmem(Ctx *c, int model, int iters, int gate, int64_t cap, VT dtinv,
                         const Cache<VT> &cc, const BodyV<VT> &bv, int track,
@@ -1669,8 +1763,11 @@ int launch_sweeps_dsmem(Ctx *c, int model, int iters, int gate, int64_t cap, VT 
     NbgsBuf &nb = c->nb;
     *done = false;
     if (nb.gen) return PE_B200_OK;
-    auto kern = dsmem_kernel<VT>(model);
     const int key = model * 2 + (sizeof(VT) == 8 ? 1 : 0);
+    const bool can_stage = model <= 1;
+    const int64_t rec_bytes = (model == 0 ? 3 : 7) * (int64_t)sizeof(T4<VT>) + (int64_t)sizeof(T4<VT>) +
+                              (int64_t)sizeof(int2);
+    constexpr int64_t kStatic = 3 * kMaxColors * 4 + 1024;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1680,16 +1777,26 @@ int launch_sweeps_dsmem(Ctx *c, int model, int iters, int gate, int64_t cap, VT 
     cfg.stream = c->stream;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    auto plan = [&](int size, int64_t &per, int64_t &scap, int64_t &bytes, int optin) {
+        per = (nb.nbod + size - 1) / size;
+        const int64_t body_bytes = 4 * per * (int64_t)sizeof(T4<VT>);
+        const int64_t room = (int64_t)optin - kStatic - body_bytes;
+        scap = can_stage && room > 0 ? room / rec_bytes : 0;
+        if (scap < 64) scap = 0;
+        bytes = body_bytes + scap * rec_bytes;
+        return room >= 0;
+    };
     if (nb.ds_nbod != nb.nbod || nb.ds_key != key) {
         nb.ds_nbod = nb.nbod;
         nb.ds_key = key;
         nb.ds_size = 0;
         int optin = 0;
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+        nb.ds_optin = optin;
         for (int size : {16, 8}) {
-            const int64_t per = (nb.nbod + size - 1) / size;
-            const int64_t bytes = 4 * per * (int64_t)sizeof(T4<VT>);
-            if (bytes + (int64_t)(kMaxColors + 1) * 4 + 1024 > optin) continue;
+            int64_t per, scap, bytes;
+            if (!plan(size, per, scap, bytes, optin)) continue;
+            auto kern = dsmem_kernel<VT>(model, scap > 0);
             if (size > 8 && cudaFuncSetAttribute((const void *)kern,
                                                  cudaFuncAttributeNonPortableClusterSizeAllowed,
                                                  1) != cudaSuccess) {
@@ -1716,19 +1823,20 @@ int launch_sweeps_dsmem(Ctx *c, int model, int iters, int gate, int64_t cap, VT 
     if (nb.ds_size == 0) return PE_B200_OK;
     const int size = nb.ds_size;
     const int shift = size == 16 ? 4 : 3;
-    const int64_t per = (nb.nbod + size - 1) / size;
-    const size_t bytes = (size_t)(4 * per) * sizeof(T4<VT>);
+    int64_t per, scap, bytes;
+    plan(size, per, scap, bytes, nb.ds_optin);
+    auto kern = dsmem_kernel<VT>(model, scap > 0);
     // the attributes are per kernel: set again, since another body count may have set them
     if (size > 8)
         cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     cudaGetLastError();
     cfg.gridDim = dim3(size);
-    cfg.dynamicSmemBytes = bytes;
+    cfg.dynamicSmemBytes = (size_t)bytes;
     attr[0].val.clusterDim.x = size;
     const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, iters, (const int32_t *)nb.dd, gate,
                                              (const int32_t *)nb.cstart_dev, cap, dtinv, cc, bv,
-                                             nb.nbod, (int)per, shift, track, dl);
+                                             nb.nbod, (int)per, shift, (int)scap, track, dl);
     if (e != cudaSuccess) {
         cudaGetLastError();
         nb.ds_size = 0;
