@@ -31,6 +31,7 @@
 #include <math_constants.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "internal.cuh"
 
@@ -566,15 +567,19 @@ __device__ __forceinline__ void grid_forces_sorted(const DemArgs<VT> &a, const S
 }
 
 // The grid step in two kernels.  k_grid_near (few registers, so many warps hide the candidate
-// loads) runs the FP32 test of every candidate of a sphere's 27 cells and records the slots
-// that pass, in k_dem_step's order, up to kNear of them; k_dem_near takes each recorded slot
-// through k_dem_step's exact test and pair force (or, for a sphere with more than kNear, searches
-// its cells again), then the walls and the integration.  Same terms in the same order: bitwise
-// the results of k_dem_step.
+// loads) runs the FP32 test over half of each sphere's 27-cell neighbourhood: the candidates
+// in a later slot (in cell order, the rows of the neighbourhood come in increasing cell key, so
+// these are the own row's later slots and the whole of the later rows).  Every pair within
+// reach is so tested once, by its lower slot, and a pair that passes is recorded for both
+// spheres (atomic counters, up to kNear slots each; the counters start at zero).  k_dem_near
+// sorts a sphere's recorded slots, which puts them in the order in which k_dem_step's 27-cell
+// scan visits them (ascending slot), takes each through k_dem_step's exact test and pair force
+// (or, for a sphere with more than kNear, searches its cells again), then the walls and the
+// integration.  Same terms in the same order: bitwise the results of k_dem_step.
 constexpr int kNear = 16;
 constexpr int kNearBlock = 256;
 
-__global__ void __launch_bounds__(kNearBlock, 6) k_grid_near(
+__global__ void __launch_bounds__(kNearBlock, 5) k_grid_near(
     int64_t n, const int32_t *__restrict__ sorted, const double4 *__restrict__ pr,
     const uint32_t *__restrict__ tag, const SceneInfo *__restrict__ scenes,
     const int32_t *__restrict__ cell_start, const float4 *__restrict__ posf,
@@ -592,29 +597,35 @@ __global__ void __launch_bounds__(kNearBlock, 6) k_grid_near(
                 pzf = float(pi.z - s.lo[2]);
     const float tol = 1e-5f * (1.0f + fabsf(pxf) + fabsf(pyf) + fabsf(pzf) + 4.0f * float(pi.w));
     const float prf = float(pi.w) + tol;
-    auto near = [&](const float4 &q) {
+    auto near = [&](const float4 &q, float rq) {
         const float dx = pxf - q.x, dy = pyf - q.y, dz = pzf - q.z;
-        const float rs = prf + q.w;
+        const float rs = prf + rq;
         return dx * dx + dy * dy + dz * dz < rs * rs;
     };
-    int cnt = 0;
+    // a pair passes for one sphere's margin or the other's (each sphere's test in k_dem_near's
+    // fallback uses its own); the larger margin covers both
     auto keep = [&](int slot) {
-        if (slot == t) return;
-        if (cnt < kNear) near_idx[(int64_t)cnt * n + t] = slot;
-        ++cnt;
+        const int32_t p = atomicAdd(&near_cnt[t], 1);
+        if (p < kNear) near_idx[(int64_t)p * n + t] = slot;
+        const int32_t q = atomicAdd(&near_cnt[slot], 1);
+        if (q < kNear) near_idx[(int64_t)q * n + slot] = (int32_t)t;
     };
-    int nb, ne;
-    row_slots(cell_start, s, x0, x1, cy - 1, cz - 1, nb, ne);
+    auto test = [&](int slot) {
+        const float4 q = posf[slot];
+        // the partner's margin, as its own thread computes it
+        const float tq = 1e-5f * (1.0f + fabsf(q.x) + fabsf(q.y) + fabsf(q.z) + 4.0f * q.w);
+        return near(q, q.w + fmaxf(tq - tol, 0.0f));
+    };
+    // the own row's later slots, then the later rows (z, y) of the neighbourhood
 #pragma unroll 1
-    for (int r = 0; r < 9; ++r) {
-        int slot = nb;
-        const int e = ne;
-        if (r < 8) row_slots(cell_start, s, x0, x1, cy + (r + 1) % 3 - 1, cz + (r + 1) / 3 - 1,
-                             nb, ne);
+    for (int r = 4; r < 9; ++r) {
+        int slot, e;
+        row_slots(cell_start, s, x0, x1, cy + r % 3 - 1, cz + r / 3 - 1, slot, e);
+        if (r == 4) slot = (int)t + 1;
         for (; slot + 8 <= e; slot += 8) {
             unsigned hit = 0;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) hit |= near(posf[slot + k]) ? (1u << k) : 0u;
+            for (int k = 0; k < 8; ++k) hit |= test(slot + k) ? (1u << k) : 0u;
             while (hit) {
                 const int k = __ffs(hit) - 1;
                 hit &= hit - 1u;
@@ -622,9 +633,8 @@ __global__ void __launch_bounds__(kNearBlock, 6) k_grid_near(
             }
         }
         for (; slot < e; ++slot)
-            if (near(posf[slot])) keep(slot);
+            if (test(slot)) keep(slot);
     }
-    near_cnt[t] = cnt;
 }
 
 template <typename VT, bool TRACKQ, bool HERTZ>
@@ -648,9 +658,34 @@ __global__ void __launch_bounds__(kDemBlock) k_dem_near(DemArgs<VT> a,
     acc.T_ = acc.F;
     if (cnt > kNear) {
         grid_forces_sorted<T, VT, HERTZ>(a, s, posf, t, b, pi, vi, wi, uidi, mi, acc);
-    } else {
-        for (int k = 0; k < cnt; ++k) {
-            const int32_t j = a.sorted[near_idx[(int64_t)k * a.n + t]];
+    } else if (cnt > 0) {
+        // the recorded slots in ascending order (a sorting network over registers; empty
+        // places hold INT_MAX and sort last)
+        int32_t sl[kNear];
+#pragma unroll
+        for (int k = 0; k < kNear; ++k) sl[k] = k < cnt ? near_idx[(int64_t)k * a.n + t] : INT_MAX;
+        if (cnt > 1) {
+#pragma unroll
+            for (int kk = 2; kk <= kNear; kk <<= 1)
+#pragma unroll
+                for (int j = kk >> 1; j > 0; j >>= 1)
+#pragma unroll
+                    for (int i = 0; i < kNear; ++i) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const int32_t x = sl[i], y = sl[l];
+                            const bool up = (i & kk) == 0;
+                            if ((x > y) == up) {
+                                sl[i] = y;
+                                sl[l] = x;
+                            }
+                        }
+                    }
+        }
+#pragma unroll
+        for (int k = 0; k < kNear; ++k) {
+            if (k >= cnt) break;
+            const int32_t j = a.sorted[sl[k]];
             const double4 pj = a.pr[j];
             const double ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
             const double rsd = pi.w + pj.w;
@@ -871,6 +906,7 @@ int launch_dem(Ctx *c, double dt) {
     } else {
         const float4 *pf = c->posf;
         const int32_t *nc = c->near, *ni = c->near + c->n;
+        PEB_CUDA(c, cudaMemsetAsync(c->near, 0, (size_t)c->n * sizeof(int32_t), c->stream));
         k_grid_near<<<grid_for(c->n, kNearBlock), kNearBlock, 0, c->stream>>>(
             c->n, c->sorted, c->cur.pr, c->cur.tag, c->d_scenes, c->cell_start, pf, c->near,
             c->near + c->n);

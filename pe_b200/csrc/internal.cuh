@@ -80,6 +80,8 @@ struct NbgsBuf {
     int32_t *h_dd = nullptr;                  // pinned mirror
     int32_t *rem = nullptr;                   // uncoloured contacts left after each colouring round
     unsigned int *bar2 = nullptr;             // grid barrier of the colouring rounds
+    int32_t *slot_of = nullptr;               // per body: -1, or its claim in the compact sweep
+    bool compact_off = false;                 // the compact sweep form cannot be launched
     bool on_device = false;                   // the last step's counts are only on the device
     bool plan_none = false;                   // queued steps planned without contacts
     bool warm = false;                        // a queued step has run on these buffers

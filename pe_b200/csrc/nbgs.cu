@@ -189,6 +189,22 @@ struct SmemContacts {
     __device__ __forceinline__ const T4<T> *dc_of(int64_t) const { return nullptr; }
 };
 
+// The contacts of the compact single-block sweep: each contact's two bodies as slots of the
+// block's shared body records (sids, -1 for a wall); the solver records stay in global memory.
+template <typename T>
+struct CompactContacts {
+    const int2 *sids;
+    const T4<T> *rec;
+    T4<T> *p;
+    const T4<T> *dc;
+    __device__ __forceinline__ int2 get_ids(int64_t k) const { return sids[k]; }
+    __device__ __forceinline__ const T4<T> *rec_of(int64_t k) const { return rec + (int64_t)kRec * k; }
+    template <bool COH>
+    __device__ __forceinline__ T4<T> get_p(int64_t k) const { return p[k]; }
+    __device__ __forceinline__ void put_p(int64_t k, const T4<T> &v) const { p[k] = v; }
+    __device__ __forceinline__ const T4<T> *dc_of(int64_t k) const { return dc + 2 * k; }
+};
+
 // Per body, slot order: velocities after the predictor with 1/m, 1/I (read-only in the sweeps)
 // and the velocity corrections (read and written by the sweeps).
 template <typename T>
@@ -1115,11 +1131,22 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const CC &cc,
 // Whether a sweep form runs for this step (decided on the device, so that a step can be queued
 // without the host knowing its colours): not after a capacity abort; gate 1 (one block) only
 // when every colour fits one block, gate 2 (the grid) only when one does not, gate 0 always.
+// Gates 4 and 5 split gate 1 by the contact count: 4 when the compact single-block form holds
+// them all (kCompactMax), 5 when it does not.  Gate 3 (the cluster form) runs for colours beyond
+// one block up to kDsmemMaxcol, and gate 6 (the grid, when the cluster form is launched beside
+// it) for larger ones.
+constexpr int kCompactMax = 768;      // contacts of the compact single-block form
+constexpr int kDsmemMaxcol = 1792;    // largest colour the cluster form takes in automatic mode
 __device__ __forceinline__ bool sweeps_gate(const int32_t *dd, int gate) {
     if (dd[kDdAbort]) return false;
     const int maxcol = dd[kDdMaxcol];
-    if (gate == 1 && maxcol > kBlk) return false;
-    if (gate == 2 && maxcol <= kBlk) return false;
+    const int nc = dd[kDdNc];
+    if ((gate == 1 || gate == 4 || gate == 5) && maxcol > kBlk) return false;
+    if (gate == 4 && nc > kCompactMax) return false;
+    if (gate == 5 && nc <= kCompactMax) return false;
+    if ((gate == 2 || gate == 3 || gate == 6) && maxcol <= kBlk) return false;
+    if (gate == 3 && maxcol > kDsmemMaxcol) return false;
+    if (gate == 6 && maxcol <= kDsmemMaxcol) return false;
     return true;
 }
 
@@ -1235,6 +1262,92 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_block_smem(int iters, const int
         bv.dv[i] = sb.dv[i];
         bv.dw[i] = sb.dw[i];
     }
+}
+
+// All sweeps of a step in one thread block with only the bodies that have contacts in shared
+// memory (sphere scenes with at most kCompactMax contacts, every colour within the block): a
+// scene of thousands of bodies and a few contacts sweeps at shared-memory latency, where the
+// whole-scene form cannot hold its bodies.  Each body gets a slot: the first of its contacts to
+// claim it (atomic compare-and-swap on slot_of, which holds -1 for every body outside this
+// kernel) loads its records; the claims are undone at the end.
+template <typename T, int MODEL>
+__global__ void __launch_bounds__(kBlk) k_sweeps_compact(int iters, const int32_t *dd, int gate,
+                                                         const int32_t *color_start, T dtinv,
+                                                         Cache<T> cc, BodyV<T> bv,
+                                                         int32_t *slot_of, int track_last,
+                                                         unsigned long long *delta) {
+    if (!sweeps_gate(dd, gate)) return;
+    const int nc = dd[kDdNc];
+    if (nc > kCompactMax) return;   // the gate of the host-driven launch (0) does not check it
+    const int ncolors = dd[kDdNcolors];
+    constexpr int bcap = 2 * kCompactMax;
+    extern __shared__ __align__(16) unsigned char smem[];
+    T4<T> *sh = (T4<T> *)smem;
+    int32_t *sbody = (int32_t *)(sh + 4 * bcap);     // slot -> body
+    int2 *sids = (int2 *)(sbody + bcap);              // contact -> its bodies' slots
+    int32_t *claim = (int32_t *)(sids + kCompactMax); // claim (2 k + side) -> slot
+    __shared__ int32_t cs[kMaxColors + 1];
+    __shared__ int nslots;
+    if (threadIdx.x == 0) nslots = 0;
+    for (int i = threadIdx.x; i <= ncolors; i += blockDim.x) cs[i] = color_start[i];
+    __syncthreads();
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+        const int2 id = cc.ids[k];
+        if (atomicCAS(&slot_of[id.x], -1, 2 * k) == -1) {
+            const int sl = atomicAdd(&nslots, 1);
+            claim[2 * k] = sl;
+            sbody[sl] = id.x;
+        }
+        if (id.y >= 0 && atomicCAS(&slot_of[id.y], -1, 2 * k + 1) == -1) {
+            const int sl = atomicAdd(&nslots, 1);
+            claim[2 * k + 1] = sl;
+            sbody[sl] = id.y;
+        }
+    }
+    __syncthreads();
+    const int ns = nslots;
+    for (int sl = threadIdx.x; sl < ns; sl += blockDim.x) {
+        const int32_t b = sbody[sl];
+        sh[sl] = bv.vr[b];
+        sh[bcap + sl] = bv.wr[b];
+        sh[2 * bcap + sl] = bv.dv[b];
+        sh[3 * bcap + sl] = bv.dw[b];
+    }
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+        const int2 id = cc.ids[k];
+        const int s1 = claim[__ldcg(slot_of + id.x)];
+        const int s2 = id.y >= 0 ? claim[__ldcg(slot_of + id.y)] : -1;
+        sids[k] = make_int2(s1, s2);
+    }
+    __syncthreads();
+    BodyV<T> sb;
+    sb.vr = sh;
+    sb.wr = sh + bcap;
+    sb.dv = sh + 2 * bcap;
+    sb.dw = sh + 3 * bcap;
+    const CompactContacts<T> ccs{sids, cc.rec, cc.p, cc.dc};
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int e = cs[col + 1];
+            for (int k = cs[col] + threadIdx.x; k < e; k += blockDim.x)
+                sweep_contact<T, MODEL, false, false, BodyV<T>, CompactContacts<T>>(k, dtinv, ccs, sb,
+                                                                                    track, delta);
+            __syncthreads();
+        }
+    }
+    for (int sl = threadIdx.x; sl < ns; sl += blockDim.x) {
+        const int32_t b = sbody[sl];
+        bv.dv[b] = sh[2 * bcap + sl];
+        bv.dw[b] = sh[3 * bcap + sl];
+        slot_of[b] = -1;
+    }
+}
+
+template <typename T>
+constexpr size_t compact_smem() {
+    return (size_t)4 * 2 * kCompactMax * sizeof(T4<T>) + (size_t)2 * kCompactMax * 4 +
+           (size_t)kCompactMax * 8 + (size_t)2 * kCompactMax * 4;
 }
 
 // All sweeps of a step inside one thread-block cluster: the colours are separated by the
@@ -1515,6 +1628,8 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         dfree(c, b.dd);
         dfree(c, b.rem);
         dfree(c, b.bar2);
+        dfree(c, b.slot_of);
+        b.slot_of = nullptr;
         if (b.color_start) cudaFreeHost(b.color_start);
         if (b.h_dd) cudaFreeHost(b.h_dd);
         b.flags = nullptr;
@@ -1544,6 +1659,8 @@ int nbgs_alloc(Ctx *c, int64_t cap) {
         PEB_CUDA(c, cudaMallocHost(&b.h_dd, kDdCount * sizeof(int32_t)));
         memset(b.h_dd, 0, kDdCount * sizeof(int32_t));
         PEB_CUDA(c, dmalloc(c, &b.rem, kMaxRounds * sizeof(int32_t)));
+        PEB_CUDA(c, dmalloc(c, &b.slot_of, (size_t)nbod * sizeof(int32_t)));
+        PEB_CUDA(c, cudaMemsetAsync(b.slot_of, 0xff, (size_t)nbod * sizeof(int32_t), c->stream));
         PEB_CUDA(c, dmalloc(c, &b.bar2, 2 * sizeof(unsigned int)));
         PEB_CUDA(c, cudaMemsetAsync(b.bar2, 0, 2 * sizeof(unsigned int), c->stream));
     }
@@ -1739,6 +1856,40 @@ int sweeps_in_cluster(Ctx *c, int model, int iters, int ncolors, int maxcol, int
 }
 
 template <typename VT>
+auto compact_kernel(int m) -> decltype(&k_sweeps_compact<VT, 0>) {
+    switch (m) {
+        case 1: return k_sweeps_compact<VT, 1>;
+        case 2: return k_sweeps_compact<VT, 2>;
+        case 3: return k_sweeps_compact<VT, 3>;
+        case 4: return k_sweeps_compact<VT, 4>;
+        case 5: return k_sweeps_compact<VT, 5>;
+        default: return k_sweeps_compact<VT, 0>;
+    }
+}
+
+// Launches k_sweeps_compact (sphere scenes); *done reports it.
+template <typename VT>
+int launch_sweeps_compact(Ctx *c, int model, int iters, int gate, VT dtinv, const Cache<VT> &cc,
+                          const BodyV<VT> &bv, int track, unsigned long long *dl, bool *done) {
+    NbgsBuf &nb = c->nb;
+    *done = false;
+    if (nb.gen || !nb.slot_of || nb.compact_off) return PE_B200_OK;
+    auto kern = compact_kernel<VT>(model);
+    constexpr size_t bytes = compact_smem<VT>();
+    if (cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        nb.compact_off = true;
+        return PE_B200_OK;
+    }
+    kern<<<1, kBlk, bytes, c->stream>>>(iters, nb.dd, gate, nb.cstart_dev, dtinv, cc, bv,
+                                         nb.slot_of, track, dl);
+    PEB_LAUNCHED(c);
+    *done = true;
+    return PE_B200_OK;
+}
+
+template <typename VT>
 auto dsmem_kernel(int m, bool stage) -> decltype(&k_sweeps_dsmem<VT, 0, false>) {
     if (stage && m == 0) return k_sweeps_dsmem<VT, 0, true>;
     if (stage && m == 1) return k_sweeps_dsmem<VT, 1, true>;
@@ -1894,6 +2045,15 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
                          unsigned long long *dl) {
     NbgsBuf &nb = c->nb;
     int32_t *dd = nb.dd;
+    const int mode = c->tune.nbgs_sweeps;
+    // every colour within one block: the compact form for a few contacts, else the whole-scene
+    // single-block form
+    bool compact = false;
+    if (!gen && mode != 2) {
+        int rc = launch_sweeps_compact<VT>(c, model, iters, 4, dtinv, cc, bv, 0, dl, &compact);
+        if (rc) return rc;
+    }
+    const int block_gate = compact ? 5 : 1;
     const size_t smem = (size_t)(gen ? 7 : 4) * nb.nbod * sizeof(T4<VT>);
     bool smem_ok = smem <= kBlockSmemMax;
     if (smem_ok) {
@@ -1902,26 +2062,29 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kBlockSmemMax) == cudaSuccess;
         if (smem_ok) {
-            kern<<<1, kBlk, smem, c->stream>>>(iters, dd, 1, nb.cstart_dev, cap, dtinv, cc, bv,
-                                               nb.nbod, 0, dl);
+            kern<<<1, kBlk, smem, c->stream>>>(iters, dd, block_gate, nb.cstart_dev, cap, dtinv, cc,
+                                               bv, nb.nbod, 0, dl);
             PEB_LAUNCHED(c);
         } else {
             cudaGetLastError();
         }
     }
     if (!smem_ok) {
-        block_kernel<VT>(model, gen)<<<1, kBlk, 0, c->stream>>>(iters, dd, 1, nb.cstart_dev, cap,
-                                                                dtinv, cc, bv, n, 0, dl);
+        block_kernel<VT>(model, gen)<<<1, kBlk, 0, c->stream>>>(iters, dd, block_gate,
+                                                                nb.cstart_dev, cap, dtinv, cc, bv,
+                                                                n, 0, dl);
         PEB_LAUNCHED(c);
     }
-    const int mode = c->tune.nbgs_sweeps;
+    int grid_gate = 2;
     if (mode == 0 || mode == 5) {
-        // the colours that do not fit one block: in one cluster's shared memory, if the bodies
-        // fit there
+        // the colours beyond one block: in one cluster's shared memory, if the bodies fit there
+        // (automatic: up to kDsmemMaxcol contacts per colour, the grid form beyond)
         bool done = false;
-        int rc = launch_sweeps_dsmem<VT>(c, model, iters, 2, cap, dtinv, cc, bv, 0, dl, &done);
+        int rc = launch_sweeps_dsmem<VT>(c, model, iters, mode == 5 ? 2 : 3, cap, dtinv, cc, bv, 0,
+                                         dl, &done);
         if (rc) return rc;
-        if (done) return PE_B200_OK;
+        if (done && mode == 5) return PE_B200_OK;
+        if (done) grid_gate = 6;
     }
     auto kern = persistent_kernel<VT>(model, gen);
     int occ = 0;
@@ -1935,7 +2098,7 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
     const unsigned g = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>(grid, (int64_t)(4.0e9 / ((double)std::max(iters, 1) * kMaxColors))));
     PEB_CUDA(c, cudaMemsetAsync(nb.bar, 0, sizeof(unsigned int), c->stream));
-    int iters_a = iters, gate_a = 2, track_a = 0;
+    int iters_a = iters, gate_a = grid_gate, track_a = 0;
     int64_t cap_a = cap, n_a = n;
     VT dtinv_a = dtinv;
     int32_t *cs = nb.cstart_dev;
@@ -2200,6 +2363,17 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
                                             c->want_residual ? 1 : 0, dl, &done);
             if (rc) return rc;
         }
+        if (!done && (mode == 0 || mode == 4) && maxcol <= kBlk && !gen && nc <= kCompactMax) {
+            // a few contacts: one block with their bodies in shared memory
+            int rc = launch_sweeps_compact<VT>(c, model, iters, 0, VT(1.0 / dt), cc, bv,
+                                              c->want_residual ? 1 : 0, dl, &done);
+            if (rc) return rc;
+        }
+        if (!done && mode == 0 && maxcol > kBlk && maxcol <= kDsmemMaxcol) {
+            int rc = launch_sweeps_dsmem<VT>(c, model, iters, 0, cap, VT(1.0 / dt), cc, bv,
+                                            c->want_residual ? 1 : 0, dl, &done);
+            if (rc) return rc;
+        }
         if (!done && (mode == 0 || mode == 4) && maxcol <= kBlk) {
             // every colour fits one block: all sweeps in one block, colours separated by
             // __syncthreads (automatic, or asked for with 4)
@@ -2332,6 +2506,7 @@ void nbgs_free(Ctx *c) {
     dfree(c, b.dd);
     dfree(c, b.rem);
     dfree(c, b.bar2);
+    dfree(c, b.slot_of);
     if (b.color_start) cudaFreeHost(b.color_start);
     if (b.h_dd) cudaFreeHost(b.h_dd);
     nbgs_graph_free(c);
