@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the pe-on-one-core leg (minutes of set-up at 1M spheres)")
     ap.add_argument("--tuning", default=None,
-                    help="dem_variant,rebuild_per_sm,skin instead of running the autotuner")
+                    help="dem_variant,rebuild_per_sm,skin[,dem_split] instead of running the "
+                         "autotuner")
     ap.add_argument("--profile-case", default=None, choices=sorted(PROFILE_CASES),
                     help="run one small case of one stage for a profiler (prints a short JSON "
                          "line, not a bench line); see profile_case()")
@@ -475,7 +476,8 @@ def end_to_end(ss, kind, precision, tuning, dt, steps, torch, dev, dist):
         e2 = engine_from_staged(staged, kind, precision,
                                 skin=tuning["skin"] if tuning is not None else 0.0)
         if tuning is not None:
-            e2.set_tuning(tuning["dem_variant"], tuning["rebuild_per_sm"], tuning["skin"])
+            e2.set_tuning(tuning["dem_variant"], tuning["rebuild_per_sm"], tuning["skin"],
+                          dem_split=tuning.get("dem_split", 0))
         t1 = time.perf_counter()
         e2.step(dt, steps)
         t2 = time.perf_counter()
@@ -531,8 +533,9 @@ def our_arm(args):
     # the state is restored)
     tuning = None
     if kind == "dem" and args.tuning:
-        v, r, sk = args.tuning.split(",")
-        e.set_tuning(int(v), int(r), float(sk))
+        parts = args.tuning.split(",")
+        v, r, sk = parts[:3]
+        e.set_tuning(int(v), int(r), float(sk), dem_split=int(parts[3]) if len(parts) > 3 else 0)
         tuning = dict(e.tuning(), source="--tuning")
     elif kind == "dem":
         tuning = e.autotune(dt, 100)

@@ -259,6 +259,10 @@ typedef struct {
                                 FP32 position copy in cell order, with an exact FP64 test for the
                                 close ones; 1 every candidate through its FP64 record (the same
                                 results) */
+    int32_t dem_split;       /* DEM list step: 0 the marked spheres' forces, then the integration
+                                of every sphere; 1 the marked spheres (forces and integration) on a
+                                second stream beside the integration of the others (the same
+                                results) */
 } pe_b200_tuning;
 int pe_b200_get_tuning(pe_b200_ctx *ctx, pe_b200_tuning *out);
 int pe_b200_set_tuning(pe_b200_ctx *ctx, const pe_b200_tuning *t);

@@ -56,7 +56,7 @@ class Material(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("dem_variant", C.c_int32), ("rebuild_per_sm", C.c_int32), ("skin", C.c_double),
                 ("ms_per_step", C.c_double), ("variants", C.c_int32), ("nbgs_sweeps", C.c_int32),
-                ("dem_grid", C.c_int32)]
+                ("dem_grid", C.c_int32), ("dem_split", C.c_int32)]
 
 
 class PeB200Error(RuntimeError):

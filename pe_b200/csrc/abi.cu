@@ -508,6 +508,9 @@ int pe_b200_destroy(pe_b200_ctx *h) {
     free_device(c);
     dfree(c, c->d_err);
     if (c->h_err) cudaFreeHost(c->h_err);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PE_B200_OK;
@@ -831,6 +834,7 @@ int pe_b200_get_tuning(pe_b200_ctx *h, pe_b200_tuning *out) {
     out->variants = dem_variant_count();
     out->nbgs_sweeps = c->tune.nbgs_sweeps;
     out->dem_grid = c->tune.dem_grid;
+    out->dem_split = c->tune.dem_split;
     return PE_B200_OK;
 }
 
@@ -844,6 +848,7 @@ int pe_b200_set_tuning(pe_b200_ctx *h, const pe_b200_tuning *t) {
     tu.rebuild_per_sm = t->rebuild_per_sm;
     tu.nbgs_sweeps = t->nbgs_sweeps;
     tu.dem_grid = t->dem_grid;
+    tu.dem_split = t->dem_split;
     return set_tuning(c, tu, c->nl.enabled ? t->skin : c->nl.skin);
 }
 

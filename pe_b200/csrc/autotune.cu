@@ -66,8 +66,12 @@ int set_list_skin(Ctx *c, double skin) {
 
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
     if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < -1 ||
-        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 5 || t.dem_grid < 0 || t.dem_grid > 1)
+        t.nbgs_sweeps < 0 || t.nbgs_sweeps > 5 || t.dem_grid < 0 || t.dem_grid > 1 ||
+        t.dem_split < 0 || t.dem_split > 1)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
+    // captured list-step graphs bake the form in
+    if (t.dem_split != c->tune.dem_split) c->epoch++;
+    c->tune.dem_split = t.dem_split;
     // captured hard-contact graphs bake the sweep form in
     if (t.nbgs_sweeps != c->tune.nbgs_sweeps) c->epoch++;
     c->tune.nbgs_sweeps = t.nbgs_sweeps;
@@ -153,6 +157,11 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
         t.rebuild_per_sm = r;
         rc = consider(t, best_skin);
     }
+    if (!rc) {
+        Tuning t = best;
+        t.dem_split = 1 - best.dem_split;
+        rc = consider(t, best_skin);
+    }
     // leave the state as it was at entry, with the winning shapes
     if (!rc) rc = copy_bodies(c, c->cur, snap);
     if (!rc) rc = set_tuning(c, best, best_skin);
@@ -171,6 +180,7 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
         out->variants = dem_variant_count();
         out->nbgs_sweeps = best.nbgs_sweeps;
         out->dem_grid = c->tune.dem_grid;
+        out->dem_split = best.dem_split;
     }
     return PE_B200_OK;
 }

@@ -732,13 +732,16 @@ constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]))
 // k_dem_move then integrates every sphere, reading facc for the marked ones, so the common
 // sphere of a sparse scene runs a short kernel without the contact code's registers.
 
-// forces on the marked spheres (a grid-stride loop over the marked list)
-template <typename VT, bool HERTZ, bool ONE = false>
+// forces on the marked spheres (a grid-stride loop over the marked list).  SPLIT: the kernel
+// also integrates them, on a second stream beside k_dem_move, which then leaves them out; else
+// it stores their forces for k_dem_move, which runs after it.
+template <typename VT, bool HERTZ, bool ONE = false, bool SPLIT = false, bool TRACKQ = false>
 __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
     using T = VT;
     // launched early behind the rebuild kernel: nothing is read before it has finished
     pdl_wait();
     pdl_trigger();
+    const bool rebuilt = a0.nl_flags[4] != 0;
     const DemArgs<VT> a = list_view(a0);
     const int32_t na = a.act[a.n];
     for (int32_t m = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x); m < na;
@@ -775,18 +778,36 @@ __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
             }
         }
         wall_forces<T, VT>(a, s, pi, vi, wi, mi, acc);
-        const int64_t cap = a.n;
-        a.facc[m] = acc.F.x;
-        a.facc[cap + m] = acc.F.y;
-        a.facc[2 * cap + m] = acc.F.z;
-        a.facc[3 * cap + m] = acc.T_.x;
-        a.facc[4 * cap + m] = acc.T_.y;
-        a.facc[5 * cap + m] = acc.T_.z;
+        if constexpr (SPLIT) {
+            // the integration of k_dem_move for this sphere
+            uint32_t ext = ld_ext(a.vw, a.n, t);
+            V3<T> v, w;
+            const double4 o = integrate_core<VT, TRACKQ>(a, t, t, pi, vi, wi, mi, acc, v, w, ext);
+            a.pr_out[t] = o;
+            st_vw(a.vw_out, a.n, t, v, w, ext);
+            if (rebuilt) {
+                a.tag_out[t] = tagi;
+                a.uid_out[t] = a.uid[t];
+            }
+            const float vx = float(v.x), vy = float(v.y), vz = float(v.z);
+            const float d = a.disp[t] + sqrtf(vx * vx + vy * vy + vz * vz) * float(a.dt) * 1.0001f;
+            a.disp[t] = d;
+            if (!(d < a.half_skin)) atomicOr(&a.nl_flags[0], 1);
+        } else {
+            const int64_t cap = a.n;
+            a.facc[m] = acc.F.x;
+            a.facc[cap + m] = acc.F.y;
+            a.facc[2 * cap + m] = acc.F.z;
+            a.facc[3 * cap + m] = acc.T_.x;
+            a.facc[4 * cap + m] = acc.T_.y;
+            a.facc[5 * cap + m] = acc.T_.z;
+        }
     }
 }
 
-// integration of every sphere with the forces of k_dem_contacts
-template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool ONE = false>
+// integration of every sphere with the forces of k_dem_contacts (SPLIT: of the unmarked ones;
+// k_dem_contacts integrates the marked ones)
+template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool ONE = false, bool SPLIT = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -813,6 +834,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
         Acc<T> acc;
         acc.F = v3(T(0), T(0), T(0));
         acc.T_ = acc.F;
+        if (!(SPLIT && marked)) {
         if (marked) {
             const int64_t cap = a.n;
             acc.F = v3(a.facc[m], a.facc[cap + m], a.facc[2 * cap + m]);
@@ -839,6 +861,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
         const float d = disp0 + sqrtf(vx * vx + vy * vy + vz * vz) * float(a.dt) * 1.0001f;
         a.disp[t] = d;
         moved = !(d < a.half_skin);   // also catches NaN
+        }
     }
     if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(&a.nl_flags[0], 1);
     // after an overflow every step rebuilds until the host has grown the list buffer
@@ -1096,12 +1119,51 @@ int list_rebuild(Ctx *c) {
     return PE_B200_OK;
 }
 
+// the second stream and the two events of the split list step, created on first use
+bool split_streams(Ctx *c) {
+    if (c->side) return true;
+    if (c->split_failed) return false;
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        c->split_failed = true;
+        return false;
+    }
+    return true;
+}
+
 template <typename VT, bool TRACKQ, int V, bool HERTZ>
 void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
     static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
     const bool one = c->nscenes == 1 && c->mats_dev.size() == 1 && !TRACKQ && !HERTZ;
+    if (c->tune.dem_split && split_streams(c)) {
+        // the marked spheres (forces and integration) on the second stream, beside the
+        // integration of the others: both start once the rebuild kernel has finished, and the
+        // next step waits for both
+        const unsigned gc = (unsigned)std::min<int64_t>(grid_for(c->n, 128), 8 * (int64_t)c->sm_count);
+        const unsigned gm = (unsigned)grid_for(c->n, B);
+        cudaEventRecord(c->ev_fork, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        DemArgs<VT> b = a;
+        if (one) {
+            b.s0 = c->scenes[0];
+            b.m0 = c->mats_dev[0];
+            k_dem_contacts<VT, HERTZ, true, true, TRACKQ><<<gc, 128, 0, c->side>>>(b);
+            k_dem_move<VT, TRACKQ, B, M, true, true><<<gm, B, 0, c->stream>>>(b);
+        } else {
+            k_dem_contacts<VT, HERTZ, false, true, TRACKQ><<<gc, 128, 0, c->side>>>(b);
+            k_dem_move<VT, TRACKQ, B, M, false, true><<<gm, B, 0, c->stream>>>(b);
+        }
+        c->launches++;
+        cudaEventRecord(c->ev_join, c->side);
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        return;
+    }
     // each kernel is scheduled while the one before it finishes (a rebuild that has nothing to
     // do lets the contact kernel start at once)
     cudaLaunchAttribute at[1];

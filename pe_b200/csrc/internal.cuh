@@ -176,6 +176,7 @@ struct Tuning {
     int32_t nbgs_sweeps = 0;    // 0 automatic, 1 one cluster, 2 cooperative grid, 3 per colour,
                                 // 4 one block, 5 bodies in one cluster's shared memory
     int32_t dem_grid = 0;       // grid step: 0 sorted FP32 candidate copy, 1 FP64 records only
+    int32_t dem_split = 0;      // list step: 1 the marked spheres on a second stream (dem.cu)
 };
 
 // a captured CUDA graph of `steps` DEM list steps (dem.cu); valid while the buffers it was
@@ -214,6 +215,11 @@ struct Ctx {
     pe_b200_params p;
     std::string err;
     cudaStream_t stream = nullptr;
+    // the split list step's second stream (higher priority: it runs the marked spheres' chain)
+    // and its fork and join events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool split_failed = false;
     int device = 0;
     int sm_count = 148;
     int64_t launches = 0;

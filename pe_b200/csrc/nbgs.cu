@@ -49,7 +49,8 @@ enum : int {
     kDdNc = 5,       // contact count written by the host (scenes with moving boxes)
     kDdSink = 6,     // error bits nobody reads (a capacity overflow that aborts instead)
     kDdSeen = 7,     // the largest contact count of the call's steps (reset per call)
-    kDdCount = 8
+    kDdRounds = 8,   // the step colours by the parallel rounds (more contacts than one thread takes)
+    kDdCount = 10
 };
 
 struct CountF {
@@ -435,9 +436,10 @@ __global__ void k_raw(int64_t n, VisitArgs a, const int32_t *off, int64_t cap, c
 // Kernels over the contacts read their count from device memory (ncp) and loop with a grid
 // stride, so a step can be queued without the host knowing the count; none runs when the
 // step was aborted for capacity (dd[kDdAbort]).
-__global__ void k_degree(const int32_t *ncp, const int32_t *dd, const int32_t *b1,
-                         const int32_t *b2, int32_t *deg) {
-    if (dd[kDdAbort]) return;
+// (cond, may be null: the step needs the body -> contacts adjacency, i.e. the parallel rounds)
+__global__ void k_degree(const int32_t *ncp, const int32_t *dd, const int32_t *cond,
+                         const int32_t *b1, const int32_t *b2, int32_t *deg) {
+    if (dd[kDdAbort] || (cond && !*cond)) return;
     const int64_t nc = *ncp;
     GRID_STRIDE(c, nc) {
         atomicAdd(&deg[b1[c]], 1);
@@ -445,9 +447,9 @@ __global__ void k_degree(const int32_t *ncp, const int32_t *dd, const int32_t *b
     }
 }
 
-__global__ void k_adj_fill(const int32_t *ncp, const int32_t *dd, const int32_t *b1,
-                           const int32_t *b2, int32_t *fill, int32_t *adj) {
-    if (dd[kDdAbort]) return;
+__global__ void k_adj_fill(const int32_t *ncp, const int32_t *dd, const int32_t *cond,
+                           const int32_t *b1, const int32_t *b2, int32_t *fill, int32_t *adj) {
+    if (dd[kDdAbort] || (cond && !*cond)) return;
     const int64_t nc = *ncp;
     GRID_STRIDE(c, nc) {
         adj[atomicAdd(&fill[b1[c]], 1)] = (int32_t)c;
@@ -473,8 +475,9 @@ __global__ void k_any_contact(int64_t n, VisitArgs a, int32_t *dd) {
     }
 }
 
-__global__ void k_guard(const int32_t *total, int64_t limit, int32_t *dd) {
+__global__ void k_guard(const int32_t *total, int64_t limit, int64_t serial_max, int32_t *dd) {
     const int32_t t = *total;
+    dd[kDdRounds] = t > serial_max ? 1 : 0;
     if (t > limit) dd[kDdAbort] = 1;
     if (t > dd[kDdNeed]) dd[kDdNeed] = t;
     if (t > dd[kDdSeen]) dd[kDdSeen] = t;
@@ -1136,7 +1139,7 @@ __device__ __forceinline__ void sweep_contact(int64_t k, T dtinv, const CC &cc,
 // one block up to kDsmemMaxcol, and gate 6 (the grid, when the cluster form is launched beside
 // it) for larger ones.
 constexpr int kCompactMax = 768;      // contacts of the compact single-block form
-constexpr int kDsmemMaxcol = 1792;    // largest colour the cluster form takes in automatic mode
+constexpr int kDsmemMaxcol = 3072;    // largest colour the cluster form takes in automatic mode
 __device__ __forceinline__ bool sweeps_gate(const int32_t *dd, int gate) {
     if (dd[kDdAbort]) return false;
     const int maxcol = dd[kDdMaxcol];
@@ -2112,6 +2115,15 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
     return PE_B200_OK;
 }
 
+// contacts one thread colours (more take the parallel rounds): scenes with moving boxes, or
+// sphere scenes with the colour masks in shared memory or in global memory
+inline int64_t colour_serial_max(const Ctx *c) {
+    const bool gen = c->mb.m > 0;
+    const size_t masks = (size_t)(c->n + c->mb.m) * (gen ? 4 : 1) * sizeof(uint64_t);
+    return gen ? kSerialColourMax
+               : (masks <= 48 * 1024 ? kSerialColourMaxSpheres : kSerialColourMaxGlobal);
+}
+
 // One hard-contact step: sort, permute, detect, colour, cache, sweep, integrate.
 // queued: the step is queued without the host waiting on the device (sphere scenes without a
 // residual request, automatic/grid/single-block sweep forms): the contact count stays on the
@@ -2190,7 +2202,7 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
         } else {
             PEB_CUDA(c, cudaMemsetAsync(dd + kDdNc, 0, sizeof(int32_t), c->stream));
         }
-        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.cap, dd);
+        k_guard<<<1, 1, 0, c->stream>>>(ncp, nb.cap, colour_serial_max(c), dd);
         PEB_LAUNCHED(c);
     } else {
         int32_t total_b = 0;
@@ -2247,23 +2259,28 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
     const bool any = queued ? !nb.plan_none : nc > 0;
     if (any) {
         prof_begin(c, ST_COLOR);
-        PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)nbod + 1) * sizeof(int32_t), c->stream));
-        k_degree<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, raw.b1, raw.b2, nb.body_cnt);
-        PEB_LAUNCHED(c);
-        rc = scan_exclusive(c, nb.body_cnt, nb.body_cnt, nbod);
-        if (rc) return rc;
-        int32_t *fill = nb.cnt;  // reuse: counts are consumed
-        PEB_CUDA(c, cudaMemcpyAsync(fill, nb.body_cnt, ((size_t)nbod + 1) * sizeof(int32_t),
-                                    cudaMemcpyDeviceToDevice, c->stream));
-        k_adj_fill<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, raw.b1, raw.b2, fill, nb.body_adj);
-        PEB_LAUNCHED(c);
+        const size_t masks = (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t);
+        const bool in_smem = masks <= 48 * 1024;
+        const int64_t serial_max = colour_serial_max(c);
+        // the body -> contacts adjacency of the parallel rounds (skipped on the device, or by the
+        // host, when one thread colours the step)
+        const int32_t *rounds = queued ? dd + kDdRounds : nullptr;
+        if (queued || nc > serial_max) {
+            PEB_CUDA(c, cudaMemsetAsync(nb.body_cnt, 0, ((size_t)nbod + 1) * sizeof(int32_t), c->stream));
+            k_degree<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, rounds, raw.b1, raw.b2, nb.body_cnt);
+            PEB_LAUNCHED(c);
+            rc = scan_exclusive_cond(c, nb.body_cnt, nb.body_cnt, nbod, rounds);
+            if (rc) return rc;
+            int32_t *fill = nb.cnt;  // reuse: counts are consumed
+            PEB_CUDA(c, cudaMemcpyAsync(fill, nb.body_cnt, ((size_t)nbod + 1) * sizeof(int32_t),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            k_adj_fill<<<cgrid, kBlk, 0, c->stream>>>(ncp, dd, rounds, raw.b1, raw.b2, fill,
+                                                      nb.body_adj);
+            PEB_LAUNCHED(c);
+        }
         PEB_CUDA(c, cudaMemsetAsync(nb.color, 0xff, (size_t)(queued ? cap : nc) * sizeof(int32_t), c->stream));
         const int words = gen ? 4 : 1;
         PEB_CUDA(c, cudaMemsetAsync(nb.used, 0, (size_t)nbod * words * sizeof(uint64_t), c->stream));
-        const size_t masks = (size_t)nbod * (gen ? 4 : 1) * sizeof(uint64_t);
-        const bool in_smem = masks <= 48 * 1024;
-        const int64_t serial_max = gen ? kSerialColourMax
-                                       : (in_smem ? kSerialColourMaxSpheres : kSerialColourMaxGlobal);
         if (queued) {
             // one thread for a few contacts; otherwise every round in one cooperative launch
             k_color_serial<1><<<1, 256, in_smem ? masks : 0, c->stream>>>(

@@ -262,12 +262,12 @@ class Engine:
         return {k: getattr(t, k) for k, _ in _abi.Tuning._fields_}
 
     def set_tuning(self, dem_variant: int = 0, rebuild_per_sm: int = 0, skin: float = 0.0,
-                   nbgs_sweeps: int = 0, dem_grid: int = 0):
+                   nbgs_sweeps: int = 0, dem_grid: int = 0, dem_split: int = 0):
         """skin <= 0 keeps the current skin."""
         if skin <= 0:
             skin = self.tuning()["skin"]
         t = _abi.Tuning(dem_variant=dem_variant, rebuild_per_sm=rebuild_per_sm, skin=skin,
-                        nbgs_sweeps=nbgs_sweeps, dem_grid=dem_grid)
+                        nbgs_sweeps=nbgs_sweeps, dem_grid=dem_grid, dem_split=dem_split)
         self._check(self._L.pe_b200_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, dt: float, trial_steps: int = 100) -> dict:
