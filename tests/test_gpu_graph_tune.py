@@ -331,20 +331,21 @@ def test_hard_contact_graphs_are_kept_across_calls():
 def test_split_list_step_matches_two_kernel_form(precision, track):
     """The split list step (the marked spheres' forces and integration on a second stream, the
     other spheres' integration beside them) gives the results of the two-kernel form bit for bit,
-    step by step and through graph replays, over many rebuilds (a small skin)."""
-    s = scenes.dem_lattice(4, side=12)
-    out = []
-    for split, gs in ((0, 0), (1, 0), (1, 16)):
-        e = Engine(solver=_abi.DEM, precision=precision, track_orientation=track,
-                   skin=0.004).load_scene(s)
-        e.set_graph_steps(gs)
-        e.set_tuning(0, 0, 0.0, dem_split=split)
-        e.step(s.dt, 3)
-        e.step(s.dt, 61)
-        out.append(e.download())
-        st = e.neighbor_list_stats()
-        e.close()
-        assert st["rebuilds"] > 3
-    for o in out[1:]:
-        for a, b in zip(o, out[0]):
-            assert np.array_equal(a, b)
+    step by step and through graph replays, over several rebuilds (a small skin): on a sparse
+    lattice (few spheres marked) and on an agitated dense packing (every sphere marked)."""
+    for s in (scenes.dem_lattice(4, side=12), scenes.dem_dense(4, 16, 16, 8)):
+        out = []
+        for split, gs in ((0, 0), (1, 0), (1, 16)):
+            e = Engine(solver=_abi.DEM, precision=precision, track_orientation=track,
+                       skin=0.004).load_scene(s)
+            e.set_graph_steps(gs)
+            e.set_tuning(0, 0, 0.0, dem_split=split)
+            e.step(s.dt, 3)
+            e.step(s.dt, 61)
+            out.append(e.download())
+            st = e.neighbor_list_stats()
+            e.close()
+            assert st["rebuilds"] >= 1
+        for o in out[1:]:
+            for a, b in zip(o, out[0]):
+                assert np.array_equal(a, b)
