@@ -548,9 +548,11 @@ def our_arm(args):
                                                       torch, dev, dist)
     e2e_value = nsph_total(ss, dist, torch, dev) * args.steps / e2e_s
     clocks = Clocks(uuid)
+    nl0 = e.neighbor_list_stats() if kind == "dem" else None
     clocks.start()
     ms, launches, prof = timed_steps(e, dt, args.steps, args.warmup, torch, flush, stream, dist)
     clk = clocks.stop()
+    nl1 = e.neighbor_list_stats() if kind == "dem" else None
     # the cpu_baseline leg: pe on one host core over the same scene, started once the headline
     # and end-to-end measurements are done (pe's set-up of a 1M-sphere scene takes minutes and
     # its host load slowed the end-to-end set-up) and collected after the other GPU lines
@@ -585,7 +587,12 @@ def our_arm(args):
         st = e.stats()
         algo = 100 * (128.0 * st["contacts"] + 80.0 * nsph)
         kname = "k_sweep<float> (100 sweeps)"
-    nls = e.neighbor_list_stats() if kind == "dem" else None
+    nls = None
+    if kind == "dem":
+        # rebuilds of the warm-up, timed and stage-timed steps (the autotuner's trials before
+        # them rebuild too)
+        nls = dict(nl1, rebuilds_in_measured_steps=nl1["rebuilds"] - nl0["rebuilds"],
+                   measured_steps=args.warmup + args.steps + min(args.steps, 200))
     kavg = kms / max(kcnt, 1)
     achieved = algo / (kavg / 1e3) / 1e9 if kavg > 0 else None
     traffic = read_traffic(args.workload)
