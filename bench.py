@@ -764,6 +764,24 @@ def nbgs_extra(torch, flush, dev):
                     rec["contact_free_ms_per_step"] = mcf / 16
                     rec["contact_free_contacts_after"] = f.stats()["contacts"]
                     f.close()
+                    # the configured run whole: its 200 steps in one call (graph replays of
+                    # 16) after one untimed step that allocates, L2 flushed before it
+                    f = make_engine([sc], "hcsits", prec)
+                    fst = torch.cuda.ExternalStream(f.stream_ptr(), device=dev)
+                    f.step(sc.dt, 1)
+                    torch.cuda.synchronize()
+                    flush[0].add_(1)
+                    flush[2].add_(flush[1].sum())
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    with torch.cuda.stream(fst):
+                        a.record(fst)
+                        f.step(sc.dt, sc.steps)
+                        b.record(fst)
+                    torch.cuda.synchronize()
+                    rec["configured_run_ms_per_step"] = a.elapsed_time(b) / sc.steps
+                    rec["configured_run_steps"] = sc.steps
+                    rec["configured_run_contacts_at_end"] = f.stats()["contacts"]
+                    f.close()
                 if mu > 0:
                     e.set_residual(True)
                     e.step(sc.dt)
