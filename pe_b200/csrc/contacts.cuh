@@ -47,18 +47,16 @@ __device__ __forceinline__ void visit_contacts(const VisitArgs &a, int32_t b, F 
             const int64_t c0 = cell_key(s, x0, y, z);
             const int64_t c1 = c0 + (x1 - x0) + 1;
             const int e = a.cell_start[c1];
-            for (int slot = a.cell_start[c0]; slot < e; ++slot) {
-                const int32_t j = a.sorted ? a.sorted[slot] : slot;
-                if (j == b) continue;
-                const int32_t uidj = a.uid[j];
-                if (!(uidi < uidj)) continue;  // the pair belongs to body 1
-                const double4 pj = a.pr[j];
+            // one candidate, in slot order
+            auto pair = [&](int32_t j, int32_t uidj, const double4 &pj) {
+                if (j == b) return;
+                if (!(uidi < uidj)) return;  // the pair belongs to body 1
                 const double nx = pi.x - pj.x, ny = pi.y - pj.y, nz = pi.z - pj.z;
                 const double rs = pi.w + pj.w + 2.0 * kContactThreshold;
-                if (nx * nx + ny * ny + nz * nz > rs * rs * (1.0 + 1e-12)) continue;
+                if (nx * nx + ny * ny + nz * nz > rs * rs * (1.0 + 1e-12)) return;
                 const double len = length_rn(nx, ny, nz);
                 const double dist = __dsub_rn(__dsub_rn(len, pi.w), pj.w);
-                if (!(dist < kContactThreshold)) continue;
+                if (!(dist < kContactThreshold)) return;
                 ContactGeom g;
                 g.other = j;
                 g.wall = -1;
@@ -74,6 +72,25 @@ __device__ __forceinline__ void visit_contacts(const VisitArgs &a, int32_t b, F 
                 g.nx = ux; g.ny = uy; g.nz = uz;
                 g.dist = dist;
                 f(g);
+            };
+            int slot = a.cell_start[c0];
+            // four candidates' ids and records in flight at a time (visited in slot order)
+            for (; slot + 4 <= e; slot += 4) {
+                int32_t jj[4], uu[4];
+                double4 pp[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) jj[q] = a.sorted ? a.sorted[slot + q] : slot + q;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uu[q] = a.uid[jj[q]];
+                    pp[q] = a.pr[jj[q]];
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pair(jj[q], uu[q], pp[q]);
+            }
+            for (; slot < e; ++slot) {
+                const int32_t j = a.sorted ? a.sorted[slot] : slot;
+                pair(j, a.uid[j], a.pr[j]);
             }
         }
     }
