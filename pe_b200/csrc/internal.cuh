@@ -82,6 +82,7 @@ struct NbgsBuf {
     unsigned int *bar2 = nullptr;             // grid barrier of the colouring rounds
     int32_t *slot_of = nullptr;               // per body: -1, or its claim in the compact sweep
     bool compact_off = false;                 // the compact sweep form cannot be launched
+    bool staged_off = false;                  // nor the grid form with staged contacts
     bool on_device = false;                   // the last step's counts are only on the device
     bool plan_none = false;                   // queued steps planned without contacts
     bool warm = false;                        // a queued step has run on these buffers

@@ -1189,6 +1189,75 @@ __global__ void __launch_bounds__(kBlk) k_sweeps_persistent(int iters, const int
     }
 }
 
+// The grid form with each block's contacts staged in its shared memory (relaxation models 0 and
+// 1, sphere scenes): block b sweeps the b-th of G equal chunks of every colour, so it handles
+// the same contacts in every sweep, and their records (ids, the solver records the model reads,
+// the impulse) are copied into its shared memory before the sweeps (as many as fit, scap; the
+// rest are read from global memory) and the impulses written back after.  A colour's contact
+// then starts with its bodies' loads instead of first loading its own record from L2.
+template <typename T, int MODEL>
+__global__ void __launch_bounds__(kBlk) k_sweeps_grid_staged(int iters, const int32_t *dd,
+                                                             int gate, const int32_t *color_start,
+                                                             T dtinv, Cache<T> cc, BodyV<T> bv,
+                                                             int scap, int track_last,
+                                                             unsigned long long *delta,
+                                                             unsigned int *bar, int32_t *err) {
+    static_assert(MODEL <= 1, "staged records: relaxation models 0 and 1");
+    constexpr int NREC = MODEL == 0 ? 3 : 7;
+    if (!sweeps_gate(dd, gate)) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int32_t lo_s[kMaxColors], n_s[kMaxColors], off_s[kMaxColors];
+    const int ncolors = dd[kDdNcolors];
+    const int G = gridDim.x, r = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int64_t b0 = color_start[col], len = color_start[col + 1] - b0;
+            const int lo = (int)(b0 + len * r / G), hi = (int)(b0 + len * (r + 1) / G);
+            lo_s[col] = lo;
+            n_s[col] = hi - lo;
+            off_s[col] = off;
+            off += hi - lo;
+        }
+    }
+    SmemContacts<T, NREC> sc;
+    sc.rec = (T4<T> *)smem;
+    sc.p = sc.rec + (int64_t)NREC * scap;
+    sc.ids = (int2 *)(sc.p + scap);
+    __syncthreads();
+    for (int col = 0; col < ncolors; ++col)
+        for (int i = threadIdx.x; i < n_s[col]; i += blockDim.x) {
+            const int local = off_s[col] + i;
+            if (local >= scap) break;
+            const int64_t k = lo_s[col] + i;
+            sc.ids[local] = cc.ids[k];
+            for (int q = 0; q < NREC; ++q) sc.rec[(int64_t)NREC * local + q] = cc.rec[(int64_t)kRec * k + q];
+            sc.p[local] = cc.p[k];
+        }
+    __syncthreads();
+    unsigned int episode = 0;   // bar[0] was zeroed before the launch
+    for (int it = 0; it < iters; ++it) {
+        const int track = (track_last && it == iters - 1) ? 1 : 0;
+        for (int col = 0; col < ncolors; ++col) {
+            const int n = n_s[col], lo = lo_s[col], off = off_s[col];
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                if (off + i < scap)
+                    sweep_contact<T, MODEL, true, false, BodyV<T>, SmemContacts<T, NREC>>(
+                        off + i, dtinv, sc, bv, track, delta);
+                else
+                    sweep_contact<T, MODEL, true, false>(lo + i, dtinv, cc, bv, track, delta);
+            }
+            if (!grid_sync_counted(bar, episode, err)) return;
+        }
+    }
+    for (int col = 0; col < ncolors; ++col)
+        for (int i = threadIdx.x; i < n_s[col]; i += blockDim.x) {
+            const int local = off_s[col] + i;
+            if (local >= scap) break;
+            cc.p[lo_s[col] + i] = sc.p[local];
+        }
+}
+
 // All sweeps of a step in one thread block, when every colour fits the block: the colours are
 // separated by __syncthreads, and the body and impulse updates of a colour, made on this SM,
 // are read back through its L1 by the next.  Scenes whose contacts crowd on few bodies (box
@@ -1858,6 +1927,59 @@ int sweeps_in_cluster(Ctx *c, int model, int iters, int ncolors, int maxcol, int
     return PE_B200_OK;
 }
 
+// Launches k_sweeps_grid_staged (sphere scenes, relaxation models 0 and 1) as one cooperative
+// grid of `blocks` blocks (at most one per SM: each holds as many staged contacts as its shared
+// memory takes); *done reports it.
+template <typename VT>
+int launch_sweeps_grid_staged(Ctx *c, int model, int iters, int gate, VT dtinv,
+                              const Cache<VT> &cc, const BodyV<VT> &bv, int track,
+                              unsigned long long *dl, int64_t blocks, bool *done) {
+    NbgsBuf &nb = c->nb;
+    *done = false;
+    if (nb.gen || model > 1 || nb.staged_off || nb.coop_disabled) return PE_B200_OK;
+    auto kern = model == 0 ? k_sweeps_grid_staged<VT, 0> : k_sweeps_grid_staged<VT, 1>;
+    const int64_t rec_bytes = (model == 0 ? 3 : 7) * (int64_t)sizeof(T4<VT>) +
+                              (int64_t)sizeof(T4<VT>) + (int64_t)sizeof(int2);
+    if (nb.ds_optin == 0) cudaDeviceGetAttribute(&nb.ds_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    const int64_t room = (int64_t)nb.ds_optin - (3 * kMaxColors * 4 + 1024);
+    const int64_t scap = room / rec_bytes;
+    const size_t bytes = (size_t)(scap * rec_bytes);
+    if (scap < 256 || cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        nb.staged_off = true;
+        return PE_B200_OK;
+    }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlk, bytes) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        nb.staged_off = true;
+        return PE_B200_OK;
+    }
+    // the barrier counter counts iters x colours x blocks arrivals: past 2^32 the grid shrinks
+    const int64_t g = std::max<int64_t>(
+        1, std::min<int64_t>(std::min<int64_t>(blocks, (int64_t)occ * c->sm_count),
+                             (int64_t)(4.0e9 / ((double)std::max(iters, 1) * kMaxColors))));
+    PEB_CUDA(c, cudaMemsetAsync(nb.bar, 0, sizeof(unsigned int), c->stream));
+    int iters_a = iters, gate_a = gate, scap_a = (int)scap, track_a = track;
+    VT dtinv_a = dtinv;
+    const int32_t *dd = nb.dd, *cs = nb.cstart_dev;
+    Cache<VT> cc_a = cc;
+    BodyV<VT> bv_a = bv;
+    void *args[] = {&iters_a, &dd, &gate_a, &cs, &dtinv_a, &cc_a, &bv_a, &scap_a, &track_a, &dl,
+                    &nb.bar, &c->d_err};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)g),
+                                                      dim3(kBlk), args, bytes, c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        nb.staged_off = true;
+        return PE_B200_OK;
+    }
+    c->launches++;
+    *done = true;
+    return PE_B200_OK;
+}
+
 template <typename VT>
 auto compact_kernel(int m) -> decltype(&k_sweeps_compact<VT, 0>) {
     switch (m) {
@@ -2088,6 +2210,13 @@ int launch_sweeps_queued(Ctx *c, int model, bool gen, int iters, int64_t cap, VT
         if (rc) return rc;
         if (done && mode == 5) return PE_B200_OK;
         if (done) grid_gate = 6;
+    }
+    if (!gen && model <= 1) {
+        bool done = false;
+        int rc = launch_sweeps_grid_staged<VT>(c, model, iters, grid_gate, dtinv, cc, bv, 0, dl,
+                                               queued_sweep_blocks(c), &done);
+        if (rc) return rc;
+        if (done) return PE_B200_OK;
     }
     auto kern = persistent_kernel<VT>(model, gen);
     int occ = 0;
@@ -2418,6 +2547,14 @@ int nbgs_step_t(Ctx *c, double dt, bool queued) {
                 PEB_LAUNCHED(c);
             }
             done = true;
+        }
+        if (!done && mode != 3 && !gen && model <= 1) {
+            // the grid form with each block's contacts staged in its shared memory
+            int rc = launch_sweeps_grid_staged<VT>(c, model, iters, 0, VT(1.0 / dt), cc, bv,
+                                                  c->want_residual ? 1 : 0, dl,
+                                                  std::max<int64_t>(1, (maxcol + kBlk - 1) / kBlk),
+                                                  &done);
+            if (rc) return rc;
         }
         if (!done && !nb.coop_disabled && mode != 3) {
             // all sweeps in one cooperative launch (colours separated by grid barriers); as few
