@@ -34,6 +34,7 @@
 #include <climits>
 
 #include "internal.cuh"
+#include "rebuild.cuh"
 
 namespace peb {
 
@@ -732,20 +733,16 @@ constexpr int kDemShapeCount = (int)(sizeof(kDemShapes) / sizeof(kDemShapes[0]))
 // k_dem_move then integrates every sphere, reading facc for the marked ones, so the common
 // sphere of a sparse scene runs a short kernel without the contact code's registers.
 
-// forces on the marked spheres (a grid-stride loop over the marked list).  SPLIT: the kernel
-// also integrates them, on a second stream beside k_dem_move, which then leaves them out; else
-// it stores their forces for k_dem_move, which runs after it.
-template <typename VT, bool HERTZ, bool ONE = false, bool SPLIT = false, bool TRACKQ = false>
-__global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
+// Forces on the marked spheres m = first, first + stride, ... (a grid-stride loop over the
+// marked list), the state read through `a` (the rebuild's copy when the step rebuilt).  SPLIT:
+// they are integrated too, on a second stream beside k_dem_move, which then leaves them out;
+// else their forces are stored for k_dem_move, which runs after.
+template <typename VT, bool HERTZ, bool ONE, bool SPLIT, bool TRACKQ>
+__device__ __forceinline__ void contacts_loop(const DemArgs<VT> &a, bool rebuilt, int64_t first,
+                                              int64_t stride) {
     using T = VT;
-    // launched early behind the rebuild kernel: nothing is read before it has finished
-    pdl_wait();
-    pdl_trigger();
-    const bool rebuilt = a0.nl_flags[4] != 0;
-    const DemArgs<VT> a = list_view(a0);
     const int32_t na = a.act[a.n];
-    for (int32_t m = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x); m < na;
-         m += (int32_t)(gridDim.x * blockDim.x)) {
+    for (int32_t m = (int32_t)first; m < na; m += (int32_t)stride) {
         const int64_t t = a.alist[m];
         const double4 pi = a.pr[t];
         const uint32_t tagi = a.tag[t];
@@ -803,6 +800,44 @@ __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
             a.facc[5 * cap + m] = acc.T_.z;
         }
     }
+}
+
+template <typename VT, bool HERTZ, bool ONE = false, bool SPLIT = false, bool TRACKQ = false>
+__global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
+    // launched early behind the rebuild kernel: nothing is read before it has finished
+    pdl_wait();
+    pdl_trigger();
+    const bool rebuilt = a0.nl_flags[4] != 0;
+    const DemArgs<VT> a = list_view(a0);
+    contacts_loop<VT, HERTZ, ONE, SPLIT, TRACKQ>(a, rebuilt, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                                                 (int64_t)gridDim.x * blockDim.x);
+}
+
+// The list step's rebuild check (and, when requested, the rebuild) and the forces on the marked
+// spheres in one cooperative kernel: a step without a rebuild goes straight from the flag to
+// the forces, without a kernel boundary between them.  The flag is read by every thread before
+// any block writes it; after a rebuild a grid barrier makes the lists and marks visible first.
+template <typename VT, bool HERTZ, bool ONE>
+__global__ void __launch_bounds__(kRbBlock) k_rebuild_contacts(RebuildArgs<VT> ra, DemArgs<VT> da) {
+    pdl_wait();
+    const bool rebuilt = ra.flags[0] != 0;
+    if (rebuilt) {
+        if (!rebuild_stages(ra)) return;
+        if (!grid_sync(ra.bar, ra.err)) return;
+    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ra.flags[4] = 0;   // the integration reads the current state
+    }
+    pdl_trigger();
+    DemArgs<VT> a = da;
+    if (rebuilt) {
+        a.pr = da.alt_pr;
+        a.vw = da.alt_vw;
+        a.tag = da.alt_tag;
+        a.uid = da.alt_uid;
+        a.q = da.alt_q;
+    }
+    contacts_loop<VT, HERTZ, ONE, false, false>(a, rebuilt, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                                                (int64_t)gridDim.x * blockDim.x);
 }
 
 // integration of every sphere with the forces of k_dem_contacts (SPLIT: of the unmarked ones;
@@ -1136,7 +1171,7 @@ bool split_streams(Ctx *c) {
 }
 
 template <typename VT, bool TRACKQ, int V, bool HERTZ>
-void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
+void launch_list_shape(Ctx *c, const DemArgs<VT> &a, bool contacts_done) {
     static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
@@ -1194,22 +1229,100 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a) {
         DemArgs<VT> b = a;
         b.s0 = c->scenes[0];
         b.m0 = c->mats_dev[0];
-        cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, true>, b);
-        c->launches++;
+        if (!contacts_done) {
+            cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, true>, b);
+            c->launches++;
+        }
         cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, true>, b);
     } else {
-        cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, false>, a);
-        c->launches++;
+        if (!contacts_done) {
+            cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, false>, a);
+            c->launches++;
+        }
         cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, false>, a);
     }
+}
+
+// The fused rebuild-and-contacts kernel for one law and record source: cooperative, and
+// scheduled while the force kernel before it finishes.  *fused false: not launched (the kernel
+// cannot be resident, or the driver refused it), the step runs the separate kernels.
+template <typename VT, bool HERTZ, bool ONE>
+int launch_rebuild_contacts_t(Ctx *c, const DemArgs<VT> &a, bool *fused) {
+    ListBuf &L = c->nl;
+    static int occ = 0;
+    if (occ == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rebuild_contacts<VT, HERTZ, ONE>,
+                                                          kRbBlock, 0) != cudaSuccess || occ < 1) {
+            cudaGetLastError();
+            occ = 0;
+            L.fuse_off = true;
+            return PE_B200_OK;
+        }
+    }
+    RebuildArgs<VT> ra;
+    unsigned grid = 0;
+    int rc = rebuild_setup<VT>(c, occ, ra, &grid);
+    if (rc) return rc;
+    DemArgs<VT> b = a;
+    if (ONE) {
+        b.s0 = c->scenes[0];
+        b.m0 = c->mats_dev[0];
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kRbBlock);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = L.rebuild_pdl_off ? 1 : 2;
+    if (cudaLaunchKernelEx(&cfg, k_rebuild_contacts<VT, HERTZ, ONE>, ra, b) != cudaSuccess) {
+        cudaGetLastError();
+        L.fuse_off = true;
+        return PE_B200_OK;
+    }
+    c->launches++;
+    *fused = true;
+    return PE_B200_OK;
+}
+
+template <typename VT>
+int launch_rebuild_contacts(Ctx *c, const DemArgs<VT> &a, bool *fused) {
+    *fused = false;
+    const bool track = c->p.track_orientation != 0;
+    const bool one = c->nscenes == 1 && c->mats_dev.size() == 1 && !track && !a.hertz;
+    if (a.hertz) return launch_rebuild_contacts_t<VT, true, false>(c, a, fused);
+    return one ? launch_rebuild_contacts_t<VT, false, true>(c, a, fused)
+               : launch_rebuild_contacts_t<VT, false, false>(c, a, fused);
 }
 
 template <typename VT>
 int list_step(Ctx *c, double dt) {
     ListBuf &L = c->nl;
+    DemArgs<VT> a = dem_args<VT>(c, dt);
+    a.sorted = nullptr;   // the grid fallback sees the state in cell order
+    a.alt_pr = L.tmp.pr;
+    a.alt_vw = (const VT *)L.tmp.vw;
+    a.alt_tag = L.tmp.tag;
+    a.alt_uid = L.tmp.uid;
+    a.alt_q = L.tmp.q;
+    a.tag_out = c->cur.tag;   // tags and ids stay in place (reordered there after a rebuild)
+    a.uid_out = c->cur.uid;
     prof_begin(c, ST_REBUILD);
     int rc = PE_B200_OK;
-    if (!L.coop_disabled && c->tune.rebuild_per_sm >= 0) {
+    // the rebuild check and the contact forces in one kernel (not while profiling, whose stage
+    // timers keep the two apart)
+    bool fused = false;
+    if (!L.coop_disabled && c->tune.rebuild_per_sm >= 0 && !c->tune.dem_split && !c->prof &&
+        !L.fuse_off) {
+        rc = launch_rebuild_contacts<VT>(c, a, &fused);
+        if (rc) return rc;
+    }
+    if (fused) {
+    } else if (!L.coop_disabled && c->tune.rebuild_per_sm >= 0) {
         rc = dem_list_rebuild_persistent(c);
         if (rc != PE_B200_OK) {
             // no cooperative launch here: the rebuild kernels run one by one and return at
@@ -1224,30 +1337,21 @@ int list_step(Ctx *c, double dt) {
     }
     prof_end(c, ST_REBUILD);
     if (rc) return rc;
-    DemArgs<VT> a = dem_args<VT>(c, dt);
-    a.sorted = nullptr;   // the grid fallback sees the state in cell order
-    a.alt_pr = L.tmp.pr;
-    a.alt_vw = (const VT *)L.tmp.vw;
-    a.alt_tag = L.tmp.tag;
-    a.alt_uid = L.tmp.uid;
-    a.alt_q = L.tmp.q;
-    a.tag_out = c->cur.tag;   // tags and ids stay in place (reordered there after a rebuild)
-    a.uid_out = c->cur.uid;
     prof_begin(c, ST_DEM);
     // the Hertz law and orientation tracking run the default launch shape
     if (a.hertz)
-        c->p.track_orientation ? launch_list_shape<VT, true, 0, true>(c, a)
-                               : launch_list_shape<VT, false, 0, true>(c, a);
+        c->p.track_orientation ? launch_list_shape<VT, true, 0, true>(c, a, fused)
+                               : launch_list_shape<VT, false, 0, true>(c, a, fused);
     else if (c->p.track_orientation)
-        launch_list_shape<VT, true, 0, false>(c, a);
+        launch_list_shape<VT, true, 0, false>(c, a, fused);
     else
         switch (c->tune.dem_variant) {
-            case 1: launch_list_shape<VT, false, 1, false>(c, a); break;
-            case 2: launch_list_shape<VT, false, 2, false>(c, a); break;
-            case 3: launch_list_shape<VT, false, 3, false>(c, a); break;
-            case 4: launch_list_shape<VT, false, 4, false>(c, a); break;
-            case 5: launch_list_shape<VT, false, 5, false>(c, a); break;
-            default: launch_list_shape<VT, false, 0, false>(c, a); break;
+            case 1: launch_list_shape<VT, false, 1, false>(c, a, fused); break;
+            case 2: launch_list_shape<VT, false, 2, false>(c, a, fused); break;
+            case 3: launch_list_shape<VT, false, 3, false>(c, a, fused); break;
+            case 4: launch_list_shape<VT, false, 4, false>(c, a, fused); break;
+            case 5: launch_list_shape<VT, false, 5, false>(c, a, fused); break;
+            default: launch_list_shape<VT, false, 0, false>(c, a, fused); break;
         }
     PEB_LAUNCHED(c);
     prof_end(c, ST_DEM);

@@ -165,6 +165,7 @@ struct ListBuf {
     int32_t *rb_blk = nullptr;
     int64_t rb_blk_cap = 0;
     bool coop_disabled = false;
+    bool fuse_off = false;   // the fused rebuild-and-contacts kernel cannot be launched here
     bool rebuild_pdl_off = false;  // the rebuild's cooperative launch without the early start
     bool warm = false;          // a list step has run since the buffers were (re)allocated
     int since_check = 1 << 20;  // steps since the last queued read-back of flags

@@ -349,3 +349,26 @@ def test_split_list_step_matches_two_kernel_form(precision, track):
         for o in out[1:]:
             for a, b in zip(o, out[0]):
                 assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", [_abi.MIXED, _abi.FP64])
+@pytest.mark.parametrize("model", [0, 1])
+def test_nbgs_compact_form_agrees(precision, model):
+    """A scene of 32k spheres whose first few contacts appear after free fall: the compact
+    single-block form (only the bodies with contacts in shared memory, asked for with 4), the
+    whole-scene single-block form (what the queued grid mode runs for colours this small) and one
+    launch per colour give identical results."""
+    s = scenes.nbgs_box(0, mu=0.5 if model else 0.0)
+    out = []
+    for mode in (4, 2, 3):
+        e = Engine(solver=_abi.HCSITS, precision=precision, relaxation_model=model,
+                   max_iterations=40).load_scene(s)
+        e.set_tuning(nbgs_sweeps=mode)
+        e.step(s.dt, s.steps)
+        st = e.stats()
+        assert 0 < st["contacts"] <= 768
+        out.append(e.download())
+        e.close()
+    for o in out[1:]:
+        for a, b in zip(o, out[0]):
+            assert np.array_equal(a, b)
