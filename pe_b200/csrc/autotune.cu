@@ -69,8 +69,12 @@ int set_tuning(Ctx *c, const Tuning &t, double skin) {
         t.nbgs_sweeps < 0 || t.nbgs_sweeps > 5 || t.dem_grid < 0 || t.dem_grid > 1 ||
         t.dem_split < 0 || t.dem_split > 1)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
-    // captured list-step graphs bake the form in
-    if (t.dem_split != c->tune.dem_split) c->epoch++;
+    // captured list-step graphs bake the form in; the new form's first step runs outside a
+    // capture (the split form creates its second stream there)
+    if (t.dem_split != c->tune.dem_split) {
+        c->epoch++;
+        c->nl.warm = false;
+    }
     c->tune.dem_split = t.dem_split;
     // captured hard-contact graphs bake the sweep form in
     if (t.nbgs_sweeps != c->tune.nbgs_sweeps) c->epoch++;

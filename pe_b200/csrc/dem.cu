@@ -1410,6 +1410,21 @@ int dem_list_alloc(Ctx *c) {
     if (!L.ev) PEB_CUDA(c, cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming));
     PEB_CUDA(c, dmalloc(c, &L.rb_bar, 2 * sizeof(unsigned int)));
     PEB_CUDA(c, cudaMemsetAsync(L.rb_bar, 0, 2 * sizeof(unsigned int), c->stream));
+    // the per-block partial sums of every rebuild kernel (fused or not, any CTAs per SM), sized
+    // once for the largest cooperative grid of kRbBlock threads: a step never allocates, so a
+    // step captured into a graph never frees or allocates a buffer (a stream-ordered free in a
+    // capture must name a graph allocation)
+    {
+        int tpsm = 2048;
+        if (cudaDeviceGetAttribute(&tpsm, cudaDevAttrMaxThreadsPerMultiProcessor, c->device) !=
+            cudaSuccess || tpsm < kRbBlock) {
+            cudaGetLastError();
+            tpsm = 2048;
+        }
+        const int64_t blk = (int64_t)(tpsm / kRbBlock) * std::max(c->sm_count, 1) + 1;
+        PEB_CUDA(c, dmalloc(c, &L.rb_blk, (size_t)blk * sizeof(int32_t)));
+        L.rb_blk_cap = blk;
+    }
     PEB_CUDA(c, dmalloc(c, &L.tmp.pr, n * sizeof(double4)));
     PEB_CUDA(c, dmalloc(c, &L.tmp.vw, n * (size_t)c->vw_bytes));
     PEB_CUDA(c, dmalloc(c, &L.tmp.tag, n * sizeof(uint32_t)));

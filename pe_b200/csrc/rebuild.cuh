@@ -327,19 +327,18 @@ __device__ bool rebuild_stages(const RebuildArgs<VT> &a) {
 }
 
 // The rebuild's arguments for the context's current state and list buffers, and the grid of a
-// rebuild kernel with `occ` resident blocks per SM (the block partial sums sized for it).
+// rebuild kernel with `occ` resident blocks per SM (at most the blocks the partial sums hold).
 template <typename VT>
 int rebuild_setup(Ctx *c, int occ, RebuildArgs<VT> &a, unsigned *grid_out) {
     ListBuf &L = c->nl;
     const int64_t want = std::max<int64_t>(1, (c->n + kRbBlock - 1) / kRbBlock);
     const int per_sm = c->tune.rebuild_per_sm > 0 ? std::min(occ, c->tune.rebuild_per_sm) : occ;
-    const unsigned grid = (unsigned)std::min<int64_t>(want, (int64_t)per_sm * c->sm_count);
-    if (L.rb_blk_cap < (int64_t)grid + 1) {
-        dfree(c, L.rb_blk);
-        L.rb_blk = nullptr;
-        PEB_CUDA(c, dmalloc(c, &L.rb_blk, ((size_t)grid + 1) * sizeof(int32_t)));
-        L.rb_blk_cap = grid + 1;
-    }
+    // the partial-sum buffer is allocated with the list buffers for the largest resident grid;
+    // a grid never outgrows it (nothing is allocated here, inside a graph capture or not)
+    if (!L.rb_blk || L.rb_blk_cap < 2)
+        return set_err(c, PE_B200_ERR_STATE, "rebuild buffers not allocated");
+    const unsigned grid = (unsigned)std::min<int64_t>(
+        std::min<int64_t>(want, (int64_t)per_sm * c->sm_count), L.rb_blk_cap - 1);
     a.n = c->n;
     a.ncell = c->ncell;
     a.scenes = c->d_scenes;

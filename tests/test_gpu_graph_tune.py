@@ -351,6 +351,37 @@ def test_split_list_step_matches_two_kernel_form(precision, track):
                 assert np.array_equal(a, b)
 
 
+def test_list_forms_switched_between_graph_replays_on_a_large_scene():
+    """One context of 196,608 spheres switches, between graph replays, from the fused
+    rebuild-and-contacts form to the split form and back, at the rebuild grids of every CTA
+    count per SM.  The scene needs more rebuild blocks than either kernel keeps resident, so the
+    two forms' cooperative grids differ (the fused kernel holds fewer CTAs per SM); the rebuild's
+    per-block buffer must serve both without being reallocated (a step captured into a graph
+    allocates nothing).  The result is that of a fresh context stepping in the two-kernel form
+    without graphs, bit for bit."""
+    s = scenes.dem_dense(4, 64, 64, 48)
+    plan = ((0, 0), (1, 0), (0, 4), (1, 4), (0, 1), (1, 2))   # (dem_split, rebuild_per_sm)
+    e = Engine(solver=_abi.DEM, precision=_abi.MIXED, skin=0.004).load_scene(s)
+    e.set_graph_steps(16)
+    e.step(s.dt, 3)
+    for split, per_sm in plan:
+        e.set_tuning(0, per_sm, 0.0, dem_split=split)
+        e.step(s.dt, 32)
+    got = e.download()
+    gs = e.graph_stats()
+    st = e.neighbor_list_stats()
+    e.close()
+    assert gs["replays"] >= len(plan) and st["rebuilds"] >= 2
+    r = Engine(solver=_abi.DEM, precision=_abi.MIXED, skin=0.004).load_scene(s)
+    r.set_graph_steps(0)
+    r.set_tuning(0, -1, 0.0)
+    r.step(s.dt, 3 + 32 * len(plan))
+    want = r.download()
+    r.close()
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("precision", [_abi.MIXED, _abi.FP64])
 @pytest.mark.parametrize("model", [0, 1])
 def test_nbgs_compact_form_agrees(precision, model):
