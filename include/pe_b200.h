@@ -261,8 +261,11 @@ typedef struct {
                                 results) */
     int32_t dem_split;       /* DEM list step: 0 the marked spheres' forces, then the integration
                                 of every sphere; 1 the marked spheres (forces and integration) on a
-                                second stream beside the integration of the others (the same
-                                results) */
+                                second stream beside the integration of the others; 2 the same
+                                overlap on one stream: the kernel that checks for (and runs) the
+                                rebuild lets the integration of the unmarked spheres start, then
+                                computes and integrates the marked ones (orientation tracking
+                                runs form 0).  All forms give the same results */
 } pe_b200_tuning;
 int pe_b200_get_tuning(pe_b200_ctx *ctx, pe_b200_tuning *out);
 int pe_b200_set_tuning(pe_b200_ctx *ctx, const pe_b200_tuning *t);

@@ -8,6 +8,8 @@
 //   rebuild_per_sm  CTAs per SM of the persistent rebuild kernel (rebuild.cu); -1 rebuilds with
 //                   one launch per stage instead (the same lists, entry for entry)
 //   skin            neighbour-list skin (cells are re-planned to 2 r_max + skin)
+//   dem_split       form of the list step: the contact forces before the integration, on a
+//                   second stream beside it, or overlapped with it on one stream (dem.cu)
 // Each trial restores the state saved at entry, forces a list rebuild, runs a few untimed steps
 // (graph capture included), then times `trial` steps with CUDA events after forcing one more
 // rebuild, so a trial's time charges at least one rebuild per `trial` steps.  Coordinate
@@ -67,7 +69,7 @@ int set_list_skin(Ctx *c, double skin) {
 int set_tuning(Ctx *c, const Tuning &t, double skin) {
     if (t.dem_variant < 0 || t.dem_variant >= dem_variant_count() || t.rebuild_per_sm < -1 ||
         t.nbgs_sweeps < 0 || t.nbgs_sweeps > 5 || t.dem_grid < 0 || t.dem_grid > 1 ||
-        t.dem_split < 0 || t.dem_split > 1)
+        t.dem_split < 0 || t.dem_split > 2)
         return set_err(c, PE_B200_ERR_ARG, "invalid tuning");
     // captured list-step graphs bake the form in; the new form's first step runs outside a
     // capture (the split form creates its second stream there)
@@ -161,9 +163,11 @@ int autotune(Ctx *c, double dt, int32_t trial, pe_b200_tuning *out) {
         t.rebuild_per_sm = r;
         rc = consider(t, best_skin);
     }
-    if (!rc) {
+    const int32_t split0 = best.dem_split;
+    for (int32_t f = 0; f <= 2; ++f) {
+        if (rc || f == split0) continue;
         Tuning t = best;
-        t.dem_split = 1 - best.dem_split;
+        t.dem_split = f;
         rc = consider(t, best_skin);
     }
     // leave the state as it was at entry, with the winning shapes

@@ -404,6 +404,23 @@ __device__ __forceinline__ uint32_t ld_ext(const VT *vw, int64_t n, int64_t i) {
     else return 0u;
 }
 
+// the same loads through L2 only (data another kernel, still running, has made visible)
+__device__ __forceinline__ double4 ld_cg(const double4 *p) {
+    const double2 lo = __ldcg(reinterpret_cast<const double2 *>(p));
+    const double2 hi = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+template <typename T>
+__device__ __forceinline__ V3<T> ld_vw_cg(const T *vw, int64_t n, int64_t i, int which) {
+    const T *p = vw + 3 * which * n + i;
+    return v3(__ldcg(p), __ldcg(p + n), __ldcg(p + 2 * n));
+}
+template <typename VT>
+__device__ __forceinline__ uint32_t ld_ext_cg(const VT *vw, int64_t n, int64_t i) {
+    if constexpr (sizeof(VT) == 4) return __ldcg(reinterpret_cast<const uint32_t *>(vw + 6 * n) + i);
+    else return 0u;
+}
+
 template <typename VT, bool TRACKQ>
 __device__ __forceinline__ double4 integrate(const DemArgs<VT> &a, int64_t b, int64_t t,
                                              const double4 &pi, V3<VT> vi, V3<VT> wi,
@@ -817,7 +834,10 @@ __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
 // spheres in one cooperative kernel: a step without a rebuild goes straight from the flag to
 // the forces, without a kernel boundary between them.  The flag is read by every thread before
 // any block writes it; after a rebuild a grid barrier makes the lists and marks visible first.
-template <typename VT, bool HERTZ, bool ONE>
+// SPLIT (the overlapped form): the kernel also integrates the marked spheres, and k_dem_move,
+// released at the trigger below, integrates the others meanwhile; it reads the rebuild flag
+// and the marks without waiting for this kernel, so they are made visible before the trigger.
+template <typename VT, bool HERTZ, bool ONE, bool SPLIT = false>
 __global__ void __launch_bounds__(kRbBlock) k_rebuild_contacts(RebuildArgs<VT> ra, DemArgs<VT> da) {
     pdl_wait();
     const bool rebuilt = ra.flags[0] != 0;
@@ -826,6 +846,10 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild_contacts(RebuildArgs<VT> r
         if (!grid_sync(ra.bar, ra.err)) return;
     } else if (blockIdx.x == 0 && threadIdx.x == 0) {
         ra.flags[4] = 0;   // the integration reads the current state
+    }
+    if constexpr (SPLIT) {
+        __threadfence();
+        __syncthreads();
     }
     pdl_trigger();
     DemArgs<VT> a = da;
@@ -836,36 +860,50 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild_contacts(RebuildArgs<VT> r
         a.uid = da.alt_uid;
         a.q = da.alt_q;
     }
-    contacts_loop<VT, HERTZ, ONE, false, false>(a, rebuilt, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+    contacts_loop<VT, HERTZ, ONE, SPLIT, false>(a, rebuilt, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
                                                 (int64_t)gridDim.x * blockDim.x);
 }
 
 // integration of every sphere with the forces of k_dem_contacts (SPLIT: of the unmarked ones;
-// k_dem_contacts integrates the marked ones)
+// the contact kernel integrates the marked ones).  SPLIT does not wait for the kernel before it
+// (the contact kernel of the overlapped form, which lets it start once the rebuild flag and
+// the marks are final): the flag, the marks and, after a rebuild, the copy in cell order are
+// read through L2, and one block waits for the contact kernel before it exits, so that the
+// next step, which waits for this kernel, also finds the marked spheres integrated.
+// Launched after a finished kernel (the two-stream form), the waits return at once.
 template <typename VT, bool TRACKQ, int BLOCK, int MINB, bool ONE = false, bool SPLIT = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
     using T = VT;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // launched early behind the contact kernel; the next step's rebuild may be scheduled from
-    // here on (it waits for this kernel in turn)
-    pdl_wait();
+    // This body's records of the current state are loaded before waiting for the kernel before
+    // this one (launched early behind it): the previous step's integration wrote them and had
+    // completed before that kernel could let this one start, and that kernel does not write
+    // them.  The first wave's loads so overlap the contact kernel.  After a rebuild they are
+    // read again from the copy in cell order, and the path length (zeroed by the rebuild)
+    // starts from zero.
+    const bool in = t < a0.n;
+    double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
+    uint32_t tagi = 0u, ext = 0u;
+    V3<T> vi = v3(T(0), T(0), T(0)), wi = vi;
+    float disp0 = 0.f;
+    if (in) {
+        pi = a0.pr[t];
+        tagi = ONE ? 0u : a0.tag[t];
+        vi = ld_vw(a0.vw, a0.n, t, 0);
+        wi = ld_vw(a0.vw, a0.n, t, 1);
+        ext = ld_ext(a0.vw, a0.n, t);
+        disp0 = a0.disp[t];
+    }
+    // the next step's rebuild may be scheduled from here on (it waits for this kernel in turn)
+    if constexpr (!SPLIT) pdl_wait();
     pdl_trigger();
-    // whether this step rebuilt the lists (its state is then the copy in cell order); loaded
-    // beside the current state, which is read at once and read again from the copy only after
-    // a rebuild, so that the common step's loads do not wait for the flag
-    const bool rebuilt = a0.nl_flags[4] != 0;
+    // whether this step rebuilt the lists (its state is then the copy in cell order)
+    const bool rebuilt = (SPLIT ? __ldcg(&a0.nl_flags[4]) : a0.nl_flags[4]) != 0;
     DemArgs<VT> a = a0;
     bool moved = false;
-    if (t < a.n) {
-        // every load of this body's own records first: they are independent, and none may
-        // wait behind this thread's stores
-        double4 pi = a0.pr[t];
-        uint32_t tagi = ONE ? 0u : a0.tag[t];
-        V3<T> vi = ld_vw(a0.vw, a.n, t, 0), wi = ld_vw(a0.vw, a.n, t, 1);
-        uint32_t ext = ld_ext(a0.vw, a.n, t);
-        const int32_t m = a.act[t];
-        const bool marked = a.act[t + 1] > m;
-        const float disp0 = a.disp[t];
+    if (in) {
+        const int32_t m = SPLIT ? __ldcg(&a.act[t]) : a.act[t];
+        const bool marked = (SPLIT ? __ldcg(&a.act[t + 1]) : a.act[t + 1]) > m;
         Acc<T> acc;
         acc.F = v3(T(0), T(0), T(0));
         acc.T_ = acc.F;
@@ -876,15 +914,25 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
             acc.T_ = v3(a.facc[3 * cap + m], a.facc[4 * cap + m], a.facc[5 * cap + m]);
         }
         if (rebuilt) {
-            pi = a0.alt_pr[t];
-            tagi = a0.alt_tag[t];
-            vi = ld_vw(a0.alt_vw, a.n, t, 0);
-            wi = ld_vw(a0.alt_vw, a.n, t, 1);
-            ext = ld_ext(a0.alt_vw, a.n, t);
+            if constexpr (SPLIT) {
+                pi = ld_cg(&a0.alt_pr[t]);
+                tagi = __ldcg(&a0.alt_tag[t]);
+                vi = ld_vw_cg(a0.alt_vw, a.n, t, 0);
+                wi = ld_vw_cg(a0.alt_vw, a.n, t, 1);
+                ext = ld_ext_cg(a0.alt_vw, a.n, t);
+                a.uid_out[t] = __ldcg(&a0.alt_uid[t]);
+            } else {
+                pi = a0.alt_pr[t];
+                tagi = a0.alt_tag[t];
+                vi = ld_vw(a0.alt_vw, a.n, t, 0);
+                wi = ld_vw(a0.alt_vw, a.n, t, 1);
+                ext = ld_ext(a0.alt_vw, a.n, t);
+                a.uid_out[t] = a0.alt_uid[t];
+            }
+            disp0 = 0.f;
             a.q = a0.alt_q;
-            // the reordered tags and ids replace the current ones
+            // the reordered tags replace the current ones (the ids just above)
             a.tag_out[t] = tagi;
-            a.uid_out[t] = a0.alt_uid[t];
         }
         const MatDev &mi = ONE ? a.m0 : a.mats[tagi & 0xffffu];
         V3<T> v, w;
@@ -900,7 +948,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dem_move(DemArgs<VT> a0) {
     }
     if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(&a.nl_flags[0], 1);
     // after an overflow every step rebuilds until the host has grown the list buffer
-    if (t == 0 && a.nl_flags[1] != 0) atomicOr(&a.nl_flags[0], 1);
+    if (t == 0 && (SPLIT ? __ldcg(&a.nl_flags[1]) : a.nl_flags[1]) != 0) atomicOr(&a.nl_flags[0], 1);
+    // a grid completes when its last block exits: one block waiting for the contact kernel is
+    // enough (the last one, which starts last, so the others do not hold their SM slots)
+    if constexpr (SPLIT) {
+        if (blockIdx.x == gridDim.x - 1) pdl_wait();
+    }
 }
 
 template <typename VT>
@@ -1170,13 +1223,15 @@ bool split_streams(Ctx *c) {
     return true;
 }
 
+// contacts_done: the fused rebuild-and-contacts kernel has run (1: it stored the marked spheres'
+// forces; 2: the overlapped form, it integrates them too)
 template <typename VT, bool TRACKQ, int V, bool HERTZ>
-void launch_list_shape(Ctx *c, const DemArgs<VT> &a, bool contacts_done) {
+void launch_list_shape(Ctx *c, const DemArgs<VT> &a, int contacts_done) {
     static_assert(V >= 0 && V < kDemShapeCount, "launch shape index");
     constexpr int B = kDemShapes[V].block;
     constexpr int M = sizeof(VT) == 4 ? kDemShapes[V].minb_f32 : kDemShapes[V].minb_f64;
     const bool one = c->nscenes == 1 && c->mats_dev.size() == 1 && !TRACKQ && !HERTZ;
-    if (c->tune.dem_split && split_streams(c)) {
+    if (c->tune.dem_split == 1 && !contacts_done && split_streams(c)) {
         // the marked spheres (forces and integration) on the second stream, beside the
         // integration of the others: both start once the rebuild kernel has finished, and the
         // next step waits for both
@@ -1233,25 +1288,28 @@ void launch_list_shape(Ctx *c, const DemArgs<VT> &a, bool contacts_done) {
             cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, true>, b);
             c->launches++;
         }
-        cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, true>, b);
+        if (contacts_done == 2) cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, true, true>, b);
+        else cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, true>, b);
     } else {
         if (!contacts_done) {
             cudaLaunchKernelEx(&cc, k_dem_contacts<VT, HERTZ, false>, a);
             c->launches++;
         }
-        cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, false>, a);
+        if (contacts_done == 2) cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, false, true>, a);
+        else cudaLaunchKernelEx(&cm, k_dem_move<VT, TRACKQ, B, M, false>, a);
     }
 }
 
 // The fused rebuild-and-contacts kernel for one law and record source: cooperative, and
-// scheduled while the force kernel before it finishes.  *fused false: not launched (the kernel
-// cannot be resident, or the driver refused it), the step runs the separate kernels.
-template <typename VT, bool HERTZ, bool ONE>
-int launch_rebuild_contacts_t(Ctx *c, const DemArgs<VT> &a, bool *fused) {
+// scheduled while the force kernel before it finishes.  *fused 0: not launched (the kernel
+// cannot be resident, or the driver refused it), the step runs the separate kernels; 1 or 2
+// (SPLIT, the overlapped form): launched.
+template <typename VT, bool HERTZ, bool ONE, bool SPLIT>
+int launch_rebuild_contacts_t(Ctx *c, const DemArgs<VT> &a, int *fused) {
     ListBuf &L = c->nl;
     static int occ = 0;
     if (occ == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rebuild_contacts<VT, HERTZ, ONE>,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rebuild_contacts<VT, HERTZ, ONE, SPLIT>,
                                                           kRbBlock, 0) != cudaSuccess || occ < 1) {
             cudaGetLastError();
             occ = 0;
@@ -1279,24 +1337,30 @@ int launch_rebuild_contacts_t(Ctx *c, const DemArgs<VT> &a, bool *fused) {
     at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = L.rebuild_pdl_off ? 1 : 2;
-    if (cudaLaunchKernelEx(&cfg, k_rebuild_contacts<VT, HERTZ, ONE>, ra, b) != cudaSuccess) {
+    if (cudaLaunchKernelEx(&cfg, k_rebuild_contacts<VT, HERTZ, ONE, SPLIT>, ra, b) != cudaSuccess) {
         cudaGetLastError();
         L.fuse_off = true;
         return PE_B200_OK;
     }
     c->launches++;
-    *fused = true;
+    *fused = SPLIT ? 2 : 1;
     return PE_B200_OK;
 }
 
+// ovl: the overlapped form (sphere orientations not tracked)
 template <typename VT>
-int launch_rebuild_contacts(Ctx *c, const DemArgs<VT> &a, bool *fused) {
-    *fused = false;
+int launch_rebuild_contacts(Ctx *c, const DemArgs<VT> &a, bool ovl, int *fused) {
+    *fused = 0;
     const bool track = c->p.track_orientation != 0;
     const bool one = c->nscenes == 1 && c->mats_dev.size() == 1 && !track && !a.hertz;
-    if (a.hertz) return launch_rebuild_contacts_t<VT, true, false>(c, a, fused);
-    return one ? launch_rebuild_contacts_t<VT, false, true>(c, a, fused)
-               : launch_rebuild_contacts_t<VT, false, false>(c, a, fused);
+    if (ovl && !track) {
+        if (a.hertz) return launch_rebuild_contacts_t<VT, true, false, true>(c, a, fused);
+        return one ? launch_rebuild_contacts_t<VT, false, true, true>(c, a, fused)
+                   : launch_rebuild_contacts_t<VT, false, false, true>(c, a, fused);
+    }
+    if (a.hertz) return launch_rebuild_contacts_t<VT, true, false, false>(c, a, fused);
+    return one ? launch_rebuild_contacts_t<VT, false, true, false>(c, a, fused)
+               : launch_rebuild_contacts_t<VT, false, false, false>(c, a, fused);
 }
 
 template <typename VT>
@@ -1314,11 +1378,11 @@ int list_step(Ctx *c, double dt) {
     prof_begin(c, ST_REBUILD);
     int rc = PE_B200_OK;
     // the rebuild check and the contact forces in one kernel (not while profiling, whose stage
-    // timers keep the two apart)
-    bool fused = false;
-    if (!L.coop_disabled && c->tune.rebuild_per_sm >= 0 && !c->tune.dem_split && !c->prof &&
+    // timers keep the two apart, nor in the two-stream form)
+    int fused = 0;
+    if (!L.coop_disabled && c->tune.rebuild_per_sm >= 0 && c->tune.dem_split != 1 && !c->prof &&
         !L.fuse_off) {
-        rc = launch_rebuild_contacts<VT>(c, a, &fused);
+        rc = launch_rebuild_contacts<VT>(c, a, c->tune.dem_split == 2, &fused);
         if (rc) return rc;
     }
     if (fused) {

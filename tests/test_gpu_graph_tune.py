@@ -327,17 +327,19 @@ def test_hard_contact_graphs_are_kept_across_calls():
 
 
 @pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
-@pytest.mark.parametrize("track", [False, True])
-def test_split_list_step_matches_two_kernel_form(precision, track):
+@pytest.mark.parametrize("track,law", [(False, 0), (True, 0), (False, 1)])
+def test_split_list_step_matches_two_kernel_form(precision, track, law):
     """The split list step (the marked spheres' forces and integration on a second stream, the
-    other spheres' integration beside them) gives the results of the two-kernel form bit for bit,
-    step by step and through graph replays, over several rebuilds (a small skin): on a sparse
-    lattice (few spheres marked) and on an agitated dense packing (every sphere marked)."""
+    other spheres' integration beside them) and the overlapped form (the same on one stream: the
+    integration of the unmarked spheres starts while the marked ones are computed) give the
+    results of the two-kernel form bit for bit, step by step and through graph replays, over
+    several rebuilds (a small skin): on a sparse lattice (few spheres marked) and on an agitated
+    dense packing (every sphere marked)."""
     for s in (scenes.dem_lattice(4, side=12), scenes.dem_dense(4, 16, 16, 8)):
         out = []
-        for split, gs in ((0, 0), (1, 0), (1, 16)):
+        for split, gs in ((0, 0), (1, 0), (1, 16), (2, 0), (2, 16)):
             e = Engine(solver=_abi.DEM, precision=precision, track_orientation=track,
-                       skin=0.004).load_scene(s)
+                       skin=0.004, force_model=law).load_scene(s)
             e.set_graph_steps(gs)
             e.set_tuning(0, 0, 0.0, dem_split=split)
             e.step(s.dt, 3)
@@ -352,15 +354,15 @@ def test_split_list_step_matches_two_kernel_form(precision, track):
 
 
 def test_list_forms_switched_between_graph_replays_on_a_large_scene():
-    """One context of 196,608 spheres switches, between graph replays, from the fused
-    rebuild-and-contacts form to the split form and back, at the rebuild grids of every CTA
-    count per SM.  The scene needs more rebuild blocks than either kernel keeps resident, so the
+    """One context of 196,608 spheres switches, between graph replays, between the fused
+    rebuild-and-contacts form, the two-stream split form and the overlapped form (dem_split 0, 1,
+    2), at the rebuild grids of several CTA counts per SM.  The scene needs more rebuild blocks than either kernel keeps resident, so the
     two forms' cooperative grids differ (the fused kernel holds fewer CTAs per SM); the rebuild's
     per-block buffer must serve both without being reallocated (a step captured into a graph
     allocates nothing).  The result is that of a fresh context stepping in the two-kernel form
     without graphs, bit for bit."""
     s = scenes.dem_dense(4, 64, 64, 48)
-    plan = ((0, 0), (1, 0), (0, 4), (1, 4), (0, 1), (1, 2))   # (dem_split, rebuild_per_sm)
+    plan = ((0, 0), (1, 0), (2, 0), (0, 4), (1, 4), (2, 4), (0, 1), (2, 2), (1, 2))
     e = Engine(solver=_abi.DEM, precision=_abi.MIXED, skin=0.004).load_scene(s)
     e.set_graph_steps(16)
     e.step(s.dt, 3)
