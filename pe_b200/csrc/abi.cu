@@ -148,6 +148,11 @@ void free_device(Ctx *c) {
     dfree(c, c->cell_count);
     dfree(c, c->cell_start);
     dfree(c, c->scan_tmp);
+    dfree(c, c->gs_bar);
+    dfree(c, c->gs_blk);
+    c->gs_bar = nullptr;
+    c->gs_blk = nullptr;
+    c->gs_blk_cap = 0;
     dfree(c, c->posf);
     c->posf = nullptr;
     dfree(c, c->near);

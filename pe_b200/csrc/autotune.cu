@@ -59,7 +59,9 @@ int set_list_skin(Ctx *c, double skin) {
     PEB_CUDA(c, dmalloc(c, &c->cell_count, ((size_t)c->ncell + 1) * sizeof(int32_t)));
     PEB_CUDA(c, dmalloc(c, &c->cell_start, ((size_t)c->ncell + 2) * sizeof(int32_t)));
     PEB_CUDA(c, cudaMemsetAsync(c->cell_count, 0, ((size_t)c->ncell + 1) * sizeof(int32_t), c->stream));
-    int rc = upload_tables(c);
+    int rc = scan_reserve(c, c->ncell + 1);
+    if (rc) return rc;
+    rc = upload_tables(c);
     if (rc) return rc;
     c->binned = false;
     c->epoch++;

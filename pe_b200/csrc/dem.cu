@@ -848,8 +848,12 @@ __global__ void __launch_bounds__(kRbBlock) k_rebuild_contacts(RebuildArgs<VT> r
         ra.flags[4] = 0;   // the integration reads the current state
     }
     if constexpr (SPLIT) {
-        __threadfence();
-        __syncthreads();
+        // after a rebuild the grid barrier has ordered every write of it; without one only the
+        // flag written just above is new: block 0 fences it before any of its threads triggers
+        if (blockIdx.x == 0) {
+            if (threadIdx.x == 0) __threadfence();
+            __syncthreads();
+        }
     }
     pdl_trigger();
     DemArgs<VT> a = da;

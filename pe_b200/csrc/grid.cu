@@ -8,7 +8,11 @@
 //   scan   (exclusive prefix sum over cells -> cell_start)
 //   scatter(slot of body i = cell_start[key[i]] + rank[i])
 //   fixup  (order each cell by body index, so the result is independent of atomic order)
-#include "internal.cuh"
+// Outside graph captures the three run in one cooperative kernel (k_grid_sort) with bounded grid
+// barriers between them, which also clears the counts for the next step; in a capture, and with
+// rebuild_per_sm = -1 (no cooperative launches), they run as separate kernels.  Both give the
+// same arrays.
+#include "rebuild.cuh"
 
 namespace peb {
 
@@ -100,15 +104,10 @@ __global__ void k_scatter(int64_t n, const int32_t *__restrict__ key,
     sorted[start[key[i]] + rank[i]] = (int32_t)i;
 }
 
-// insertion sort of each cell's slots by body index (cells hold a handful of bodies); with
-// posf, the cell's bodies' positions relative to their scene's grid origin and radii in FP32,
-// in slot order (the candidate records of the grid DEM step)
-__global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
-                        int32_t *__restrict__ sorted, const double4 *__restrict__ pr,
-                        const uint32_t *__restrict__ tag, const SceneInfo *__restrict__ scenes,
-                        float4 *__restrict__ posf) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
+// one cell's insertion sort by body index, and its FP32 position records (posf non-null)
+__device__ __forceinline__ void fixup_cell(int64_t c, const int32_t *start, int32_t *sorted,
+                                           const double4 *pr, const uint32_t *tag,
+                                           const SceneInfo *scenes, float4 *posf) {
     const int b = start[c], e = start[c + 1];
     if (e == b) return;
     for (int i = b + 1; i < e; ++i) {
@@ -128,6 +127,43 @@ __global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
         posf[i] = make_float4(float(p.x - s.lo[0]), float(p.y - s.lo[1]), float(p.z - s.lo[2]),
                               float(p.w));
     }
+}
+
+// insertion sort of each cell's slots by body index (cells hold a handful of bodies); with
+// posf, the cell's bodies' positions relative to their scene's grid origin and radii in FP32,
+// in slot order (the candidate records of the grid DEM step)
+__global__ void k_fixup(int64_t ncell, const int32_t *__restrict__ start,
+                        int32_t *__restrict__ sorted, const double4 *__restrict__ pr,
+                        const uint32_t *__restrict__ tag, const SceneInfo *__restrict__ scenes,
+                        float4 *__restrict__ posf) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    fixup_cell(c, start, sorted, pr, tag, scenes, posf);
+}
+
+struct GridSortArgs {
+    int64_t n, ncell;
+    int32_t *cell_count, *cell_start, *key, *rank, *sorted;
+    const double4 *pr;
+    const uint32_t *tag;
+    const SceneInfo *scenes;
+    float4 *posf;
+    unsigned int *bar;
+    int32_t *blk, *err;
+};
+
+// the whole sort in one cooperative grid: scan | scatter, clear the counts | per-cell order
+__global__ void __launch_bounds__(kRbBlock) k_grid_sort(GridSortArgs g) {
+    if (!grid_scan_raw(g.blk, g.bar, g.err, g.cell_count, g.cell_start, g.ncell)) return;
+    if (!grid_sync(g.bar, g.err)) return;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t i = g0; i < g.n; i += stride) g.sorted[g.cell_start[g.key[i]] + g.rank[i]] = (int32_t)i;
+    // the scan has read every count: cleared for the step kernel, which bins for the next sort
+    for (int64_t c = g0; c <= g.ncell; c += stride) g.cell_count[c] = 0;
+    if (!grid_sync(g.bar, g.err)) return;
+    for (int64_t c = g0; c < g.ncell; c += stride)
+        fixup_cell(c, g.cell_start, g.sorted, g.pr, g.tag, g.scenes, g.posf);
 }
 
 }  // namespace
@@ -212,6 +248,22 @@ int scan_exclusive_cond(Ctx *c, const int32_t *in, int32_t *out, int64_t n, cons
 
 int grid_alloc(Ctx *c) {
     const size_t n = (size_t)c->n;
+    if (!c->gs_bar) {
+        PEB_CUDA(c, dmalloc(c, &c->gs_bar, 2 * sizeof(unsigned int)));
+        PEB_CUDA(c, cudaMemsetAsync(c->gs_bar, 0, 2 * sizeof(unsigned int), c->stream));
+        int tpsm = 2048;
+        if (cudaDeviceGetAttribute(&tpsm, cudaDevAttrMaxThreadsPerMultiProcessor, c->device) !=
+            cudaSuccess || tpsm < kRbBlock) {
+            cudaGetLastError();
+            tpsm = 2048;
+        }
+        c->gs_blk_cap = (int64_t)(tpsm / kRbBlock) * std::max(c->sm_count, 1) + 1;
+        PEB_CUDA(c, dmalloc(c, &c->gs_blk, (size_t)c->gs_blk_cap * sizeof(int32_t)));
+    }
+    // the scan scratch of every scan a step runs (cells, bodies and moving boxes, list counts),
+    // sized here so that no step allocates it inside a graph capture
+    int rc = scan_reserve(c, std::max<int64_t>(c->ncell + 1, 2 * c->n + 1024));
+    if (rc) return rc;
     PEB_CUDA(c, dmalloc(c, &c->key, n * sizeof(int32_t) + 16));
     PEB_CUDA(c, dmalloc(c, &c->rank, n * sizeof(int32_t) + 16));
     PEB_CUDA(c, dmalloc(c, &c->sorted, n * sizeof(int32_t) + 16));
@@ -237,6 +289,56 @@ int grid_bin_current(Ctx *c) {
 // cell_count is cleared for the producing kernel of this step.
 int grid_sort(Ctx *c, bool with_pos) {
     prof_begin(c, ST_SORT);
+    // one cooperative kernel for steps launched one by one; inside a graph capture the separate
+    // kernels (cheap to launch from a graph) measured faster than the kernel's grid barriers
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        cap = cudaStreamCaptureStatusActive;
+    }
+    if (cap == cudaStreamCaptureStatusNone && !c->gs_coop_off && c->gs_blk &&
+        c->tune.rebuild_per_sm >= 0 && c->ncell > 0) {
+        static int occ = 0;
+        if (occ == 0 &&
+            (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_grid_sort, kRbBlock, 0) !=
+                 cudaSuccess || occ < 1)) {
+            cudaGetLastError();
+            occ = 0;
+            c->gs_coop_off = true;
+        }
+        if (occ > 0) {
+            const int64_t work = std::max<int64_t>(c->ncell, c->n);
+            const int64_t want = std::max<int64_t>(1, (work + kRbBlock - 1) / kRbBlock);
+            const unsigned grid = (unsigned)std::min<int64_t>(
+                std::min<int64_t>(want, (int64_t)occ * c->sm_count), c->gs_blk_cap - 1);
+            GridSortArgs g;
+            g.n = c->n;
+            g.ncell = c->ncell;
+            g.cell_count = c->cell_count;
+            g.cell_start = c->cell_start;
+            g.key = c->key;
+            g.rank = c->rank;
+            g.sorted = c->sorted;
+            g.pr = c->cur.pr;
+            g.tag = c->cur.tag;
+            g.scenes = c->d_scenes;
+            g.posf = with_pos ? c->posf : nullptr;
+            g.bar = c->gs_bar;
+            g.blk = c->gs_blk;
+            g.err = c->d_err;
+            void *args[] = {&g};
+            if (cudaLaunchCooperativeKernel((const void *)k_grid_sort, dim3(grid), dim3(kRbBlock),
+                                            args, 0, c->stream) == cudaSuccess) {
+                c->launches++;
+                prof_end(c, ST_SORT);
+                return PE_B200_OK;
+            }
+            // refused (e.g. a shared device that allows no cooperative launches): the separate
+            // kernels from now on
+            cudaGetLastError();
+            c->gs_coop_off = true;
+        }
+    }
     int rc = scan_exclusive(c, c->cell_count, c->cell_start, c->ncell);
     if (rc) return rc;
     if (c->n > 0) {

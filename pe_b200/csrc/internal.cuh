@@ -249,6 +249,12 @@ struct Ctx {
     int32_t *cell_count = nullptr, *cell_start = nullptr;
     int32_t *scan_tmp = nullptr;
     int64_t scan_tmp_cap = 0;
+    // the one-kernel grid sort (grid.cu): barrier counters, per-block partial sums for the
+    // largest resident grid, and whether cooperative launches were refused here
+    unsigned int *gs_bar = nullptr;
+    int32_t *gs_blk = nullptr;
+    int64_t gs_blk_cap = 0;
+    bool gs_coop_off = false;
     float4 *posf = nullptr;         // grid step: FP32 positions relative to the grid origin and
                                     // radii, in the sort's slot order (grid_sort)
     int32_t *near = nullptr;        // grid step: per slot the count of candidates that passed

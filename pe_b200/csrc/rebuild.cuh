@@ -79,31 +79,33 @@ __device__ int block_incl_scan(int v, int *total) {
     return r;
 }
 
-// exclusive scan of in[0, m) into out[0, m], out[m] = total; blocks own contiguous chunks
-template <typename VT>
-__device__ bool grid_scan(const RebuildArgs<VT> &a, const int32_t *in, int32_t *out, int64_t m) {
+// exclusive scan of in[0, m) into out[0, m], out[m] = total, by every block of a cooperative
+// grid of kRbBlock threads; blocks own contiguous chunks, blk holds gridDim.x + 1 partial sums.
+// The caller puts a grid barrier after it before reading out.
+__device__ bool grid_scan_raw(int32_t *blk, unsigned int *bar, int32_t *err, const int32_t *in,
+                              int32_t *out, int64_t m) {
     const int64_t per = (m + gridDim.x - 1) / gridDim.x;
     const int64_t b0 = (int64_t)blockIdx.x * per;
     const int64_t b1 = (b0 + per < m) ? b0 + per : m;
     int s = 0;
     for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) s += in[i];
     s = block_sum(s);
-    if (threadIdx.x == 0) a.blk[blockIdx.x] = s;
-    if (!grid_sync(a.bar, a.err)) return false;
+    if (threadIdx.x == 0) blk[blockIdx.x] = s;
+    if (!grid_sync(bar, err)) return false;
     if (blockIdx.x == 0) {
         int run = 0;
         for (int64_t base = 0; base < gridDim.x; base += blockDim.x) {
             const int64_t i = base + threadIdx.x;
-            const int v = (i < gridDim.x) ? a.blk[i] : 0;
+            const int v = (i < gridDim.x) ? blk[i] : 0;
             int tot;
             const int incl = block_incl_scan(v, &tot);
-            if (i < gridDim.x) a.blk[i] = run + incl - v;
+            if (i < gridDim.x) blk[i] = run + incl - v;
             run += tot;
         }
         if (threadIdx.x == 0) out[m] = run;
     }
-    if (!grid_sync(a.bar, a.err)) return false;
-    int run = a.blk[blockIdx.x];
+    if (!grid_sync(bar, err)) return false;
+    int run = blk[blockIdx.x];
     for (int64_t base = b0; base < b1; base += blockDim.x) {
         const int64_t i = base + threadIdx.x;
         const int v = (i < b1) ? in[i] : 0;
@@ -113,6 +115,12 @@ __device__ bool grid_scan(const RebuildArgs<VT> &a, const int32_t *in, int32_t *
         run += tot;
     }
     return true;
+}
+
+template <typename VT>
+__device__ __forceinline__ bool grid_scan(const RebuildArgs<VT> &a, const int32_t *in, int32_t *out,
+                                          int64_t m) {
+    return grid_scan_raw(a.blk, a.bar, a.err, in, out, m);
 }
 
 // The cells within reach of body t (state in cell order): at most 3 x 3 rows of at most 3
