@@ -269,8 +269,21 @@ def engine_from_staged(st, kind, precision, iters=100, lists=True, skin=0.0):
     return e
 
 
-def timed_steps(e, dt, steps, warmup, torch, flush_buf, stream, dist=None):
-    """Per-step CUDA events on the library's stream; the L2 flush between steps is untimed."""
+def spin_up(torch, flush_buf, stream, ms=20.0):
+    """About `ms` of untimed GPU work (the flush kernels, no step of the workload), so that a
+    short timed region does not start while the GPU's clocks are still rising after host-side
+    work left it idle."""
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, int(ms / 0.085))):
+            flush_buf[0].add_(1)
+            flush_buf[2].add_(flush_buf[1].sum())
+    torch.cuda.synchronize()
+
+
+def timed_steps(e, dt, steps, warmup, torch, flush_buf, stream, dist=None, per_step=None):
+    """Per-step CUDA events on the library's stream; the L2 flush between steps is untimed.
+    per_step (a list) receives the timed steps' times in ms."""
+    spin_up(torch, flush_buf, stream)
     for _ in range(warmup):
         e.step(dt)
     torch.cuda.synchronize()
@@ -291,7 +304,10 @@ def timed_steps(e, dt, steps, warmup, torch, flush_buf, stream, dist=None):
                 e.step(dt)
                 evs[k][1].record(stream)
         torch.cuda.synchronize()
-        return sum(a.elapsed_time(b) for a, b in evs)
+        t = [a.elapsed_time(b) for a, b in evs]
+        if per_step is not None and not per_step:
+            per_step.extend(t)
+        return sum(t)
 
     # the headline pass runs without the library's stage timers (their events cost time)
     launches0 = e.kernel_launches()
@@ -311,6 +327,7 @@ def timed_steps(e, dt, steps, warmup, torch, flush_buf, stream, dist=None):
 
 def timed_chunks(e, dt, chunks, chunk, warmup, torch, flush_buf, stream):
     """Steps in chunks of `chunk` (each one CUDA-graph replay), L2 flushed between chunks."""
+    spin_up(torch, flush_buf, stream)
     e.set_graph_steps(chunk)
     e.step(dt, chunk * max(1, warmup))
     torch.cuda.synchronize()
@@ -550,7 +567,9 @@ def our_arm(args):
     clocks = Clocks(uuid)
     nl0 = e.neighbor_list_stats() if kind == "dem" else None
     clocks.start()
-    ms, launches, prof = timed_steps(e, dt, args.steps, args.warmup, torch, flush, stream, dist)
+    step_ms = []
+    ms, launches, prof = timed_steps(e, dt, args.steps, args.warmup, torch, flush, stream, dist,
+                                     per_step=step_ms)
     clk = clocks.stop()
     nl1 = e.neighbor_list_stats() if kind == "dem" else None
     # the cpu_baseline leg: pe on one host core over the same scene, started once the headline
@@ -638,6 +657,10 @@ def our_arm(args):
                                        if args.workload == "ensemble_512" else
                                        f"replicas x{world}")},
             "clocks": clk, "gpu_launches": launches,
+            "step_ms": {"min": min(step_ms), "median": float(np.median(step_ms)),
+                        "max": max(step_ms), "first": step_ms[0],
+                        "note": "this rank's timed steps, each between two L2 flushes; ~20 ms "
+                                "of untimed flush kernels run before the warm-up steps"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
                     "note": "new context, upload from pinned host arrays, steps, download into "
