@@ -293,7 +293,7 @@ int pe_b200_autotune(pe_b200_ctx *ctx, double dt, int32_t trial_steps, pe_b200_t
  *   for a material index outside [0, nmat)); stream: cudaStream_t to run on (NULL: the legacy
  *   default stream).
  * The call is synchronous: it returns after the step has finished on the device, copies its
- * tables from host memory and reads its status back, so it cannot be recorded into a CUDA graph.
+ * tables from host memory and reads its status back.
  * Limits: n <= PE_B200_STATIC_MAX_SPHERES, <= 64 materials, <= 64 planes, <= 64 boxes (larger
  * requests return PE_B200_ERR_ARG before any work); the grid is coarsened to at most
  * PE_B200_STATIC_MAX_CELLS cells, whatever the domain's width.  All calls on a device share the

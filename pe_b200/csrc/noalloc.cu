@@ -24,7 +24,7 @@
 //     (again after cudaDeviceReset, which unloads the module: the cache is keyed on the CUDA
 //     context's unique id, not on the device ordinal);
 //   - a call is synchronous: it copies its small tables from host memory and waits for its
-//     stream before returning, so it cannot be recorded into a CUDA graph.
+//     stream before returning.
 #include <cuda.h>
 #include <math.h>
 
