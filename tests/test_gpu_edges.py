@@ -33,9 +33,11 @@ def test_no_bodies(solver, lists):
 
 
 @pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
-def test_one_sphere_falls_onto_the_floor(precision):
+@pytest.mark.parametrize("form", [0, 2])
+def test_one_sphere_falls_onto_the_floor(precision, form):
     s = scene_of([[4.0, 4.0, 0.52]], [[0.3, 0.0, -1.0]], [0.5], "one")
     e = Engine(solver=_abi.DEM, precision=precision).load_scene(s)
+    e.set_tuning(0, 0, 0.0, dem_split=form)
     e.step(s.dt, 600)
     x, v, _ = e.download()
     e.close()
@@ -47,9 +49,11 @@ def test_one_sphere_falls_onto_the_floor(precision):
 
 
 @pytest.mark.parametrize("n", [2, 31, 33, 127, 129, 257, 1001])
-def test_partial_warps_blocks_and_tiles(n):
+@pytest.mark.parametrize("form", [0, 2])
+def test_partial_warps_blocks_and_tiles(n, form):
     s = scenes.small_random(100 + n, n=n, overlap=0.03)
     e = Engine(solver=_abi.DEM, precision=_abi.FP64).load_scene(s)
+    e.set_tuning(0, 0, 0.0, dem_split=form)
     e.step(s.dt, 30)
     x, v, _ = e.download()
     e.close()

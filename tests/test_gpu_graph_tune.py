@@ -106,11 +106,14 @@ def test_lists_cover_pairs_beyond_one_cell(skin):
 
 
 @pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
-def test_list_overflow_falls_back_to_the_grid(precision):
+@pytest.mark.parametrize("form", [0, 2])
+def test_list_overflow_falls_back_to_the_grid(precision, form):
     """A list buffer far too small for the first rebuild: that step searches the grid, the
-    library grows the buffer, and the trajectory is the grid path's."""
+    library grows the buffer, and the trajectory is the grid path's (in the fused and the
+    overlapped list-step forms)."""
     s = scenes.dem_lattice(3, side=8)
     e = Engine(solver=_abi.DEM, precision=precision, max_contacts=64).load_scene(s)
+    e.set_tuning(0, 0, 0.0, dem_split=form)
     e.step(s.dt, 30)
     x, v, _ = e.download()
     st = e.neighbor_list_stats()
@@ -351,6 +354,30 @@ def test_split_list_step_matches_two_kernel_form(precision, track, law):
         for o in out[1:]:
             for a, b in zip(o, out[0]):
                 assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", [_abi.FP64, _abi.MIXED])
+def test_list_forms_agree_on_batched_scenes(precision):
+    """Six scenes of different sizes in one context, some with fixed boxes, each scene its own
+    material (the kernels read every sphere's scene and material through its tag): the three
+    list-step forms give the same results bit for bit, step by step and through graph
+    replays."""
+    ss = [scenes.small_random(s, n=64 + 16 * s, with_boxes=bool(s % 2)) for s in range(6)]
+    for s in ss:
+        s.dt = ss[0].dt
+    out = []
+    for split, gs in ((0, 0), (1, 0), (2, 0), (2, 8)):
+        e = Engine(solver=_abi.DEM, precision=precision, skin=0.01)
+        e.load_scenes(ss)
+        e.set_graph_steps(gs)
+        e.set_tuning(0, 0, 0.0, dem_split=split)
+        e.step(ss[0].dt, 3)
+        e.step(ss[0].dt, 45)
+        out.append(e.download())
+        e.close()
+    for o in out[1:]:
+        for a, b in zip(o, out[0]):
+            assert np.array_equal(a, b)
 
 
 def test_list_forms_switched_between_graph_replays_on_a_large_scene():
