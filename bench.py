@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dem_large_1m",
-                    choices=["dem_large_1m", "dem_lattice_4096", "nbgs_box_32768", "ensemble_512"])
+                    choices=["dem_large_1m", "dem_dense_1m", "dem_lattice_4096", "nbgs_box_32768",
+                             "ensemble_512"])
     ap.add_argument("--no-extras", action="store_true", help="headline measurement only")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the pe-on-one-core leg (minutes of set-up at 1M spheres)")
@@ -68,6 +69,8 @@ def build_workload(name, seed=0, rank=0, world=1):
     share one fixed job and exchange nothing."""
     if name == "dem_large_1m":
         return [scenes.dem_large(seed)], "dem"
+    if name == "dem_dense_1m":
+        return [scenes.dem_dense(seed)], "dem"
     if name == "dem_lattice_4096":
         return [scenes.dem_lattice(seed)], "dem"
     if name == "nbgs_box_32768":

@@ -21,9 +21,11 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fopenm
               "-I" + INCLUDE]
 # per-file flags: the box fine detection rounds every product and sum separately, as pe's FP64
 # code does (its case selection compares depths that tie for aligned boxes); so do the
-# hard-contact kernels, whose sweep forms must give the same bits in every kernel they are
-# compiled into (contracted multiply-adds are chosen per kernel by the compiler)
-FILE_FLAGS = {"boxes.cu": ["-fmad=false"], "nbgs.cu": ["-fmad=false"]}
+# hard-contact kernels and the DEM step and list rebuild kernels, whose forms must give the same
+# bits in every kernel they are compiled into (contracted multiply-adds are chosen per kernel by
+# the compiler, and a kernel's launch bounds changed its choices)
+FILE_FLAGS = {"boxes.cu": ["-fmad=false"], "nbgs.cu": ["-fmad=false"], "dem.cu": ["-fmad=false"],
+              "rebuild.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

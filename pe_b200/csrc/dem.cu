@@ -837,8 +837,17 @@ __global__ void __launch_bounds__(128) k_dem_contacts(DemArgs<VT> a0) {
 // SPLIT (the overlapped form): the kernel also integrates the marked spheres, and k_dem_move,
 // released at the trigger below, integrates the others meanwhile; it reads the rebuild flag
 // and the marks without waiting for this kernel, so they are made visible before the trigger.
+// resident blocks per SM the registers of the overlapped form's mixed-precision linear-law
+// kernels must allow: 4 (64 registers) took the contact-dense 1M step from 134 to 109 us (more
+// warps on the neighbours' loads); 5 and 6 spill too much (118, 147 us); the sparse step is the
+// same at all four.  The FP64 and Hertz kernels would spill kilobytes at 64 and keep their own.
+#ifndef PEB_FUSED_MINB
+#define PEB_FUSED_MINB 4
+#endif
 template <typename VT, bool HERTZ, bool ONE, bool SPLIT = false>
-__global__ void __launch_bounds__(kRbBlock) k_rebuild_contacts(RebuildArgs<VT> ra, DemArgs<VT> da) {
+__global__ void __launch_bounds__(kRbBlock,
+                                  (SPLIT && sizeof(VT) == 4 && !HERTZ) ? PEB_FUSED_MINB : 1)
+    k_rebuild_contacts(RebuildArgs<VT> ra, DemArgs<VT> da) {
     pdl_wait();
     const bool rebuilt = ra.flags[0] != 0;
     if (rebuilt) {
