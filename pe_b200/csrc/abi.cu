@@ -516,6 +516,9 @@ int pe_b200_destroy(pe_b200_ctx *h) {
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->dl) cudaStreamDestroy(c->dl);
+    if (c->ev_dl0) cudaEventDestroy(c->ev_dl0);
+    if (c->ev_dl1) cudaEventDestroy(c->ev_dl1);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PE_B200_OK;

@@ -222,6 +222,10 @@ struct Ctx {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool split_failed = false;
+    // a second stream for the copies of a download (transfer.cu), created on first use
+    cudaStream_t dl = nullptr;
+    cudaEvent_t ev_dl0 = nullptr, ev_dl1 = nullptr;
+    bool dl_failed = false;
     int device = 0;
     int sm_count = 148;
     int64_t launches = 0;

@@ -163,6 +163,26 @@ int pack_bodies(Ctx *c, const double *x, const double *v, const double *w, const
     return PE_B200_OK;
 }
 
+// the download's second stream and its two events, created on first use (false: not
+// available, the copies stay on the context's stream)
+static bool download_streams(Ctx *c) {
+    if (c->dl) return true;
+    if (c->dl_failed) return false;
+    if (cudaStreamCreateWithFlags(&c->dl, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_dl0, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_dl1, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->dl) cudaStreamDestroy(c->dl);
+        if (c->ev_dl0) cudaEventDestroy(c->ev_dl0);
+        if (c->ev_dl1) cudaEventDestroy(c->ev_dl1);
+        c->dl = nullptr;
+        c->ev_dl0 = c->ev_dl1 = nullptr;
+        c->dl_failed = true;
+        return false;
+    }
+    return true;
+}
+
 int unpack_bodies(Ctx *c, double *x, double *v, double *w, double *q) {
     const int64_t n = c->n;
     if (n == 0) return PE_B200_OK;
@@ -179,10 +199,39 @@ int unpack_bodies(Ctx *c, double *x, double *v, double *w, double *q) {
                                                   s.x, s.v, s.w, s.r);
     PEB_LAUNCHED(c);
     const size_t v3b = 3 * (size_t)n * sizeof(double);
-    if (x) PEB_CUDA(c, cudaMemcpyAsync(x, s.x, v3b, cudaMemcpyDeviceToHost, c->stream));
-    if (v) PEB_CUDA(c, cudaMemcpyAsync(v, s.v, v3b, cudaMemcpyDeviceToHost, c->stream));
-    if (w) PEB_CUDA(c, cudaMemcpyAsync(w, s.w, v3b, cudaMemcpyDeviceToHost, c->stream));
-    if (q) PEB_CUDA(c, cudaMemcpyAsync(q, s.r, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    struct Part {
+        void *host;
+        const void *dev;
+        size_t bytes;
+    };
+    Part parts[4];
+    int np = 0;
+    if (x) parts[np++] = {x, s.x, v3b};
+    if (v) parts[np++] = {v, s.v, v3b};
+    if (w) parts[np++] = {w, s.w, v3b};
+    if (q) parts[np++] = {q, s.r, 4 * (size_t)n * sizeof(double)};
+    size_t total = 0;
+    for (int k = 0; k < np; ++k) total += parts[k].bytes;
+    if (total >= ((size_t)8 << 20) && download_streams(c)) {
+        // large downloads: every array's second half on a second stream, so that two copy
+        // engines move the halves at once; the context's stream waits for both
+        PEB_CUDA(c, cudaEventRecord(c->ev_dl0, c->stream));
+        PEB_CUDA(c, cudaStreamWaitEvent(c->dl, c->ev_dl0, 0));
+        for (int k = 0; k < np; ++k) {
+            const size_t half = (parts[k].bytes / 2) & ~(size_t)255;
+            PEB_CUDA(c, cudaMemcpyAsync(parts[k].host, parts[k].dev, half, cudaMemcpyDeviceToHost,
+                                        c->stream));
+            PEB_CUDA(c, cudaMemcpyAsync((char *)parts[k].host + half,
+                                        (const char *)parts[k].dev + half, parts[k].bytes - half,
+                                        cudaMemcpyDeviceToHost, c->dl));
+        }
+        PEB_CUDA(c, cudaEventRecord(c->ev_dl1, c->dl));
+        PEB_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_dl1, 0));
+    } else {
+        for (int k = 0; k < np; ++k)
+            PEB_CUDA(c, cudaMemcpyAsync(parts[k].host, parts[k].dev, parts[k].bytes,
+                                        cudaMemcpyDeviceToHost, c->stream));
+    }
     PEB_CUDA(c, cudaStreamSynchronize(c->stream));
     return PE_B200_OK;
 }
